@@ -1,0 +1,285 @@
+/*
+ * qcb200.h -- C ABI of libqcb200, a B200-native (sm_100a) implementation of the
+ * bit-packed tableau / Pauli-frame hot path of QuantumClifford.jl v0.11.7.
+ *
+ * The library replaces the device methods that the reference's CUDA package
+ * extension supplies (the files of ext/QuantumCliffordGPUExt) and the KernelAbstractions
+ * `mul_left!` (ext/QuantumCliffordKAExt/mul_leftright.jl).  A Julia extension
+ * binds these symbols with `ccall`; every signature uses plain pointers, sizes
+ * and POD structs only.
+ *
+ * Conventions
+ *  - Qubit and record-bit indices inside qcb_op are 1-based, exactly as in the
+ *    Julia operation structs (sCNOT(1,2), sMZ(3,1), ...).  A record bit of 0
+ *    means "do not record" (reference: sMZ(q) / sMRZ(q) with bit 0).
+ *  - Row indices passed to tableau calls are 1-based (Julia convention).
+ *  - Every call returns an int status (QCB_OK == 0).  qcb_last_error() gives
+ *    the message of the last failing call on the calling host thread.
+ *  - Calls are asynchronous on the given stream (NULL = the legacy default
+ *    stream), except calls that return host values (phases, ranks, projection
+ *    results), which synchronise that stream before returning.
+ *  - Host buffers are borrowed for the duration of the call only; all device
+ *    memory is owned by the library behind opaque handles.
+ */
+#ifndef QCB200_H
+#define QCB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum qcb_status {
+  QCB_OK = 0,
+  QCB_EDIM = 1,        /* DimensionMismatch (src/throws.jl:8-14)                 */
+  QCB_EBOUNDS = 2,     /* BoundsError: qubit / bit / row index out of range       */
+  QCB_EZEROQUBIT = 3,  /* ArgumentError(NoZeroQubit) (src/throws.jl:1)           */
+  QCB_EARG = 4,        /* ArgumentError, e.g. two-qubit gate with q1 == q2
+                          (src/symbolic_cliffords.jl:351)                        */
+  QCB_EOOM = 5,        /* device allocation failed                               */
+  QCB_EBUDGET = 6,     /* request exceeds the configured HBM budget              */
+  QCB_ETIMEOUT = 7,    /* a device-side bounded wait expired                     */
+  QCB_ECUDA = 8,       /* CUDA runtime error                                     */
+  QCB_EBADSTRUCT = 9,  /* BadDataStructure (src/project_trace_reset.jl:352-354)  */
+  QCB_EUNSUPPORTED = 10,
+  QCB_ENOTREADY = 11   /* asynchronous result not yet available                  */
+};
+
+/* ------------------------------------------------------------------ ops   */
+/* Operation codes.  Gate truth tables follow src/symbolic_cliffords.jl
+ * (`@qubitop1` at :105-118, `@qubitop2` at :358-395).                       */
+enum qcb_opcode {
+  QCB_OP_NOP = 0,
+  /* single-qubit symbolic Cliffords */
+  QCB_OP_I = 1, QCB_OP_H = 2, QCB_OP_S = 3, QCB_OP_SDAG = 4,
+  QCB_OP_X = 5, QCB_OP_Y = 6, QCB_OP_Z = 7,
+  QCB_OP_SQRTX = 8, QCB_OP_INVSQRTX = 9, QCB_OP_SQRTY = 10, QCB_OP_INVSQRTY = 11,
+  QCB_OP_HXY = 12, QCB_OP_HYZ = 13, QCB_OP_CXYZ = 14, QCB_OP_CZYX = 15,
+  /* two-qubit symbolic Cliffords */
+  QCB_OP_CNOT = 32, QCB_OP_CPHASE = 33, QCB_OP_SWAP = 34,
+  QCB_OP_ZCX = 35, QCB_OP_ZCY = 36, QCB_OP_ZCZ = 37,
+  QCB_OP_XCX = 38, QCB_OP_XCY = 39, QCB_OP_XCZ = 40,
+  QCB_OP_YCX = 41, QCB_OP_YCY = 42, QCB_OP_YCZ = 43,
+  /* measurements (frame semantics: src/pauli_frames.jl:74-116) */
+  QCB_OP_MZ = 64, QCB_OP_MRZ = 65, QCB_OP_MX = 66, QCB_OP_MRX = 67,
+  /* noise */
+  QCB_OP_PAULI_NOISE = 96, /* PauliError(q, px, py, pz): NoiseOp(PauliNoise)   */
+  QCB_OP_DEPOL1 = 97,      /* NoiseOp(DepolarizationNoise(p), (q1,))           */
+  QCB_OP_DEPOL2 = 98       /* NoiseOp(DepolarizationNoise(p), (q1, q2))        */
+};
+
+/* One circuit operation (40 bytes, 8-byte aligned).
+ *  - q1, q2: 1-based qubits (q2 only for two-qubit gates and DEPOL2).
+ *  - bit:    1-based record bit for MZ/MRZ/MX/MRX; 0 = not recorded.
+ *  - p:      PAULI_NOISE: p[0]=px, p[1]=py, p[2]=pz  (src/noise.jl:56-60);
+ *            DEPOL1/DEPOL2: p[0] = depolarisation probability p as in
+ *            DepolarizationNoise(p) (src/noise.jl:34-53): with probability p a
+ *            uniformly random k-qubit Pauli, identity included, is applied.  */
+typedef struct qcb_op {
+  uint32_t opcode;
+  uint32_t q1;
+  uint32_t q2;
+  uint32_t bit;
+  double p[3];
+} qcb_op;
+
+/* Where the randomness of a frame run comes from. */
+enum qcb_noise_mode {
+  QCB_NOISE_PHILOX = 0, /* on-device Philox-4x32-10, geometric-skip noise     */
+  QCB_NOISE_MASK = 1    /* caller-supplied events (bit-exact parity mode)      */
+};
+
+/* A noise event for mask mode: at noise op `op_index` (0-based index into
+ * the op array given to qcb_program_compile), frame `shot` (0-based) suffers
+ * Pauli `pauli`.  PAULI_NOISE: 1 = X, 2 = Z, 3 = Y.  DEPOL1/DEPOL2: the index
+ * of the Pauli in base 4, first qubit least significant, digits 0=I 1=X 2=Z
+ * 3=Y (src/noise.jl:99-129).                                                */
+typedef struct qcb_event {
+  uint32_t op_index;
+  uint32_t pauli;
+  uint64_t shot;
+} qcb_event;
+
+typedef struct qcb_noise_source {
+  uint32_t mode;         /* qcb_noise_mode                                   */
+  uint32_t reserved;
+  uint64_t seed;         /* PHILOX: key                                      */
+  uint64_t shot_offset;  /* global index of this frame's shot 0; a multiple
+                            of 32.  Shards of one run use disjoint offsets.  */
+  /* MASK mode only (host pointers, borrowed for the call): */
+  const qcb_event* events;
+  uint64_t n_events;
+  /* One bit plane per MRZ/MRX op in program order: plane k, word w, bit b is
+   * the `rand(Bool)` of that reset for shot 32*w+b (src/pauli_frames.jl:112).
+   * Shape [n_resets][ceil(frames/32)] uint32.  NULL = all zero.            */
+  const uint32_t* reset_planes;
+} qcb_noise_source;
+
+typedef struct qcb_program_info {
+  uint32_t nqubits;       /* highest qubit used                             */
+  uint32_t nbits;         /* highest record bit used                        */
+  uint32_t n_ops;         /* ops given                                      */
+  uint32_t n_updates;     /* Clifford + measurement ops per frame           */
+  uint32_t n_noise_sites; /* noise sites (one per qubit of PauliError)      */
+  uint32_t n_resets;      /* MRZ/MRX ops                                    */
+  uint32_t n_segments;    /* fused segments in the device program           */
+  uint32_t n_flushes;     /* noise flush points                             */
+} qcb_program_info;
+
+typedef struct qcb_program qcb_program;
+typedef struct qcb_frame qcb_frame;
+typedef struct qcb_tableau qcb_tableau;
+
+/* ------------------------------------------------------------ library     */
+int qcb_init(int device);
+const char* qcb_version(void);
+int qcb_last_error(char* buf, size_t len);
+const char* qcb_status_string(int status);
+int qcb_device_synchronize(void);
+/* Count of this library's kernel launches since load (for launch accounting). */
+uint64_t qcb_launch_count(void);
+
+/* ------------------------------------------------------------ programs    */
+/* Compile a circuit into a device program (replaces the per-op dispatch of
+ * pftrajectories(frame, circuit), src/pauli_frames.jl:234-239, and
+ * compactify_circuit, src/sumtypes.jl:190-237).  Validates indices like the
+ * Julia constructors do.                                                    */
+int qcb_program_compile(const qcb_op* ops, size_t n_ops, qcb_program** out);
+int qcb_program_info_get(const qcb_program* prog, qcb_program_info* info);
+int qcb_program_destroy(qcb_program* prog);
+
+/* ------------------------------------------------------------ Pauli frames */
+/* PauliFrame(frames, qubits, measurements) (src/pauli_frames.jl:30-37): an
+ * (qubits+1)-qubit frame (hidden ancilla included), zero x/z bits, an
+ * all-false record of `nbits` bits.  initZ! is a separate call.             */
+int qcb_frame_create(uint64_t frames, uint32_t qubits, uint32_t nbits, qcb_frame** out);
+int qcb_frame_destroy(qcb_frame* f);
+int qcb_frame_shape(const qcb_frame* f, uint64_t* frames, uint32_t* qubits, uint32_t* nbits);
+/* initZ! (src/pauli_frames.jl:47-56) from Philox (seed, shot_offset).       */
+int qcb_frame_init_z(qcb_frame* f, uint64_t seed, uint64_t shot_offset, void* stream);
+/* initZ! from caller bit planes [qubits+1][ceil(frames/32)] (mask mode).   */
+int qcb_frame_init_z_planes(qcb_frame* f, const uint32_t* z_planes, void* stream);
+/* Zero the x/z bits and the record.                                        */
+int qcb_frame_clear(qcb_frame* f, void* stream);
+
+/* pftrajectories(frame, circuit) (src/pauli_frames.jl:234-239).            */
+int qcb_pftrajectories(qcb_frame* f, const qcb_program* prog,
+                       const qcb_noise_source* noise, void* stream);
+
+/* apply!(frame, op) for a short op list (compiled on the fly).             */
+int qcb_frame_apply_ops(qcb_frame* f, const qcb_op* ops, size_t n_ops,
+                        const qcb_noise_source* noise, void* stream);
+
+/* Reference-layout transfers.  `xzs` is the parent of the Adjoint matrix of
+ * a fastcolumn frame: frames x W' uint64, frames contiguous per word, with
+ * W' = 2*ceil((qubits+1)/64) (X words first, then Z words;
+ * src/fastmemlayout.jl:45-60, src/pauli_frames.jl:30-37).  Padding bits are
+ * written as zero.                                                          */
+int qcb_frame_download_xzs(const qcb_frame* f, uint64_t* xzs, void* stream);
+int qcb_frame_upload_xzs(qcb_frame* f, const uint64_t* xzs, void* stream);
+/* measurements(frame) (src/pauli_frames.jl:280): Bool matrix frames x nbits,
+ * column-major (one byte per bit).                                         */
+int qcb_frame_download_measurements(const qcb_frame* f, uint8_t* bools, void* stream);
+/* The record as shot-packed bit planes [nbits][ceil(frames/32)] uint32.    */
+int qcb_frame_download_record_planes(const qcb_frame* f, uint32_t* planes, void* stream);
+/* x/z planes [qubits+1][ceil(frames/32)] uint32 each (device layout).      */
+int qcb_frame_download_planes(const qcb_frame* f, uint32_t* x_planes, uint32_t* z_planes, void* stream);
+
+/* pftrajectories(circuit; trajectories) (src/pauli_frames.jl:193-227) as one
+ * host call: fresh frame, Philox initZ!, run, record copied back as
+ * shot-packed planes [nbits][ceil(frames/32)].  The frame is kept on the
+ * device for reuse between calls with the same shape.                       */
+int qcb_pftrajectories_host(const qcb_op* ops, size_t n_ops, uint64_t frames,
+                            uint64_t seed, uint64_t shot_offset,
+                            uint32_t* record_planes, void* stream);
+
+/* pftrajectories(circuit; trajectories) on a preallocated frame: initZ!
+ * (Philox, seed / shot_offset) fused with the run; x starts at zero.  The
+ * record keeps the previous contents of bits the program does not write.   */
+int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t seed,
+                             uint64_t shot_offset, void* stream);
+
+/* Launch-shape overrides used by the tuner ("walker_threads",
+ * "canon_cluster", "project_cluster"); 0 restores the automatic choice.    */
+int qcb_tune_set(const char* key, int64_t value);
+
+/* ------------------------------------------------------------ tableaux    */
+/* A Tableau in the reference layout (src/QuantumClifford.jl:145-151): `rows`
+ * Pauli rows over `nqubits`; row r is W = 2*ceil(nqubits/64) uint64 words,
+ * X words then Z words; phases are uint8 mod 4.  A PauliOperator is a
+ * one-row tableau.                                                          */
+int qcb_tableau_create(uint32_t rows, uint32_t nqubits, qcb_tableau** out);
+int qcb_tableau_destroy(qcb_tableau* t);
+int qcb_tableau_shape(const qcb_tableau* t, uint32_t* rows, uint32_t* nqubits);
+int qcb_tableau_upload(qcb_tableau* t, const uint8_t* phases, const uint64_t* xzs, void* stream);
+int qcb_tableau_download(const qcb_tableau* t, uint8_t* phases, uint64_t* xzs, void* stream);
+int qcb_tableau_copy(qcb_tableau* dst, const qcb_tableau* src, void* stream);
+
+/* mul_left!(r::PauliOperator, l::PauliOperator; phases)
+ * (src/mul_leftright.jl:137-142, 75-126): r <- l * r.  r and l are one-row
+ * tableaux of equal size.  The new phase of r is written to *phase_out
+ * (may be NULL).                                                            */
+int qcb_mul_left_pauli(qcb_tableau* r, const qcb_tableau* l, int phases,
+                       uint8_t* phase_out, void* stream);
+/* mul_left!(s::Tableau, m, i; phases) (src/mul_leftright.jl:177-181).      */
+int qcb_mul_left_row(qcb_tableau* s, uint32_t m, uint32_t i, int phases, void* stream);
+/* mul_left!(s::Tableau, p::PauliOperator; phases) (src/mul_leftright.jl:223-229). */
+int qcb_mul_left_tableau_pauli(qcb_tableau* s, const qcb_tableau* p, int phases, void* stream);
+/* prodphase / comm of row i of l and row j of r (src/QuantumClifford.jl:723-859). */
+int qcb_prodphase(const qcb_tableau* l, uint32_t i, const qcb_tableau* r, uint32_t j,
+                  uint8_t* out, void* stream);
+int qcb_comm(const qcb_tableau* l, uint32_t i, const qcb_tableau* r, uint32_t j,
+             uint8_t* out, void* stream);
+
+/* canonicalize!(state; phases, ranks) (src/canonicalization.jl:92-133) on rows
+ * [row0, row0+nrows) of t (1-based row0; the stabilizer view).  rx, rz get
+ * the last pivot indices of the X and Z stage (relative to the view), as
+ * with ranks=true.                                                          */
+int qcb_canonicalize(qcb_tableau* t, uint32_t row0, uint32_t nrows, int phases,
+                     int32_t* rx, int32_t* rz, void* stream);
+
+/* Tableau kinds for project!. */
+enum qcb_state_kind {
+  QCB_STABILIZER = 0,         /* rows = the stabilizer                       */
+  QCB_MIXED_STABILIZER = 1,   /* rows >= rank; *rank_io = rank               */
+  QCB_DESTABILIZER = 2,       /* rows = 2n' (destabilizers then stabilizers) */
+  QCB_MIXED_DESTABILIZER = 3  /* rows = 2*nqubits; *rank_io = rank           */
+};
+
+/* project!(state, pauli; keep_result, phases) (src/project_trace_reset.jl:231-439).
+ * `paulis` holds k one-row Paulis (a k-row tableau); they are projected in
+ * order on the same state.  anticom[j] gets the anticommuting index (0 if
+ * none); result[j] gets the measurement phase 0..3, or -1 for `nothing`.
+ * For the mixed kinds *rank_io is read and updated.  A status of
+ * QCB_EBADSTRUCT reports BadDataStructure for projection j = *n_done.       */
+int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* paulis,
+                int keep_result, int phases, int32_t* anticom, int32_t* result,
+                uint32_t* n_done, void* stream);
+
+/* generate!(pauli, stabilizer; phases) (src/project_trace_reset.jl:37-81) on
+ * a canonical stabilizer.  Writes the remaining Pauli (identity up to phase)
+ * back into `pauli`; *ok = 0 when the Pauli cannot be generated.  used_rows
+ * (capacity cap, may be NULL) gets the 1-based rows used, *n_used their count. */
+int qcb_generate(qcb_tableau* pauli, const qcb_tableau* stab, int phases, int32_t* ok,
+                 int32_t* used_rows, uint32_t cap, uint32_t* n_used, void* stream);
+
+/* apply!(state, gates) for symbolic gates with phases
+ * (src/symbolic_cliffords.jl:62-74, 293-316), applied in order.             */
+int qcb_apply_gates(qcb_tableau* t, const qcb_op* ops, size_t n_ops, int phases, void* stream);
+
+/* Dense apply!(state, c::CliffordOperator; phases) (src/dense_cliffords.jl:135-169).
+ * `c` is the 2n-row tableau of the Clifford operator (images of X_1..X_n,
+ * then Z_1..Z_n).                                                           */
+int qcb_apply_dense(qcb_tableau* t, const qcb_tableau* c, int phases, void* stream);
+
+/* ------------------------------------------------------------ diagnostics */
+/* Philox-4x32-10 block (counter, key) -> out, computed on the device.       */
+int qcb_debug_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QCB200_H */

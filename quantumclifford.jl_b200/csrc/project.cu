@@ -1,0 +1,413 @@
+// project.cu -- project! for Stabilizer, MixedStabilizer, Destabilizer and
+// MixedDestabilizer tableaux (src/project_trace_reset.jl:231-439).
+//
+// One thread-block cluster projects a list of Paulis in order on one state.
+// The tableau stays in global memory (it is L2 resident at these sizes).  Per
+// Pauli:
+//   1. every CTA computes comm(pauli, row) for its share of the rows (warp per
+//      row, parity of popcounts) into a flag array, and the first
+//      anticommuting row of each range the reference scans;
+//   2. after a cluster barrier every CTA reads all CTAs' minima through
+//      distributed shared memory, so all take the same branch;
+//   3. the row swaps of the MixedDestabilizer logical branch are done by CTA 0
+//      (flags swapped with the rows), then every CTA left-multiplies its
+//      anticommuting rows by the pivot row exactly as anticomm_update_rows
+//      (:319-335) does (comm is evaluated on the rows before any update, and
+//      the pivot row is never updated, so the row updates are independent);
+//   4. CTA 0 does the row copies, rank update and the result.
+// The commuting branch of Stabilizer / MixedStabilizer needs canonicalize! +
+// generate!; the kernel stops there and the host runs those kernels before
+// resuming with the next Pauli.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "qcb_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace qcb {
+
+int canonicalize_view(uint64_t* xzs, uint8_t* ph, uint32_t rows, uint32_t n, uint32_t W, int phases,
+                      int32_t* d_out, cudaStream_t st);
+int generate_dev(uint64_t* pauli, uint8_t* pph, const uint64_t* xzs, const uint8_t* ph, uint32_t rows,
+                 uint32_t W, int phases, int32_t* d_ok, int32_t* d_used, uint32_t cap, uint32_t* d_nused,
+                 cudaStream_t st);
+
+__device__ __forceinline__ void mul_step_p(uint64_t x1, uint64_t z1, uint64_t& x2, uint64_t& z2,
+                                           uint64_t& c1, uint64_t& c2) {
+  const uint64_t nx = x1 ^ x2, nz = z1 ^ z2;
+  const uint64_t x1z2 = x1 & z2;
+  const uint64_t anti = (x2 & z1) ^ x1z2;
+  c2 ^= (c1 ^ nx ^ nz ^ x1z2) & anti;
+  c1 ^= anti;
+  x2 = nx;
+  z2 = nz;
+}
+
+enum : int32_t { PST_OK = 0, PST_NEED_CANON = 1, PST_BADSTRUCT = 2 };
+
+struct ProjArgs {
+  uint64_t* xzs;
+  uint8_t* ph;
+  uint32_t rows, n, W;
+  int kind;
+  int32_t* rank;         // device rank (mixed kinds)
+  const uint64_t* paulis;
+  const uint8_t* pph;
+  uint32_t j0, k;        // project Paulis [j0, k)
+  int keep_result, phases;
+  int32_t* anticom;
+  int32_t* result;
+  int32_t* status;       // [0] = status, [1] = index reached
+  uint8_t* flags;        // rows
+};
+
+constexpr uint32_t PROJ_THREADS = 1024;
+
+// row m <- row i * row m (mul_left!(tab, m, i)), warp-cooperative.
+__device__ __forceinline__ void warp_rowmul(uint64_t* xzs, uint8_t* ph, uint32_t W, uint32_t m,
+                                            const uint64_t* piv, uint32_t pph, bool phases,
+                                            uint32_t lane) {
+  const uint32_t len = W / 2;
+  uint64_t* row = xzs + (size_t)m * W;
+  uint64_t c1 = 0, c2 = 0;
+  for (uint32_t w = lane; w < len; w += 32) {
+    uint64_t x2 = row[w], z2 = row[len + w];
+    mul_step_p(piv[w], piv[len + w], x2, z2, c1, c2);
+    row[w] = x2;
+    row[len + w] = z2;
+  }
+  if (phases) {
+    const uint32_t s =
+        __reduce_add_sync(0xFFFFFFFFu, (uint32_t)(__popcll(c1) + 2 * __popcll(c2)) & 3u) & 3u;
+    if (lane == 0) ph[m] = (uint8_t)((s + ph[m] + pph) & 3u);
+  }
+}
+
+__global__ void __launch_bounds__(PROJ_THREADS) project_kernel(const ProjArgs a) {
+  cg::cluster_group cl = cg::this_cluster();
+  const uint32_t me = cl.block_rank(), CS = cl.num_blocks();
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t gw = me * nwarps + warp, NW = CS * nwarps;
+  const uint32_t W = a.W, len = W / 2;
+  extern __shared__ __align__(16) uint64_t smem[];
+  uint64_t* P = smem;            // W words: the Pauli
+  uint64_t* piv = smem + W;      // W words: the pivot row
+  __shared__ uint32_t mins[3];   // first anticommuting: stab range, logical X, logical Z
+  __shared__ int32_t dec[8];     // decision broadcast
+
+  const uint32_t rows = a.rows;
+  for (uint32_t j = a.j0; j < a.k; j++) {
+    const uint64_t* pj = a.paulis + (size_t)j * W;
+    for (uint32_t w = tid; w < W; w += blockDim.x) P[w] = pj[w];
+    if (tid < 3) mins[tid] = 0xFFFFFFFFu;
+    const uint32_t pphase = a.pph[j];
+    int32_t r = a.kind == QCB_STABILIZER ? (int32_t)rows : (a.kind == QCB_DESTABILIZER ? (int32_t)(rows / 2) : *a.rank);
+    __syncthreads();
+    const uint32_t nn = (a.kind == QCB_DESTABILIZER || a.kind == QCB_MIXED_DESTABILIZER) ? rows / 2 : rows;
+    // 1. comm flags for every row and the first anticommuting rows
+    for (uint32_t m = gw; m < rows; m += NW) {
+      const uint64_t* row = a.xzs + (size_t)m * W;
+      uint64_t acc = 0;
+      for (uint32_t w = lane; w < len; w += 32) acc ^= (P[len + w] & row[w]) ^ (P[w] & row[len + w]);
+      const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)__popcll(acc)) & 1u;
+      if (lane == 0) {
+        a.flags[m] = (uint8_t)c;
+        if (c) {
+          if (a.kind == QCB_STABILIZER || a.kind == QCB_MIXED_STABILIZER) {
+            if (m < (uint32_t)r) atomicMin(&mins[0], m);
+          } else {
+            if (m >= nn && m < nn + (uint32_t)r) atomicMin(&mins[0], m - nn);
+            if (a.kind == QCB_MIXED_DESTABILIZER) {
+              if (m >= (uint32_t)r && m < nn) atomicMin(&mins[1], m);
+              if (m >= nn + (uint32_t)r) atomicMin(&mins[2], m);
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    cl.sync();
+    // 2. uniform decision
+    if (tid == 0) {
+      uint32_t m0 = 0xFFFFFFFFu, m1 = 0xFFFFFFFFu, m2 = 0xFFFFFFFFu;
+      for (uint32_t q = 0; q < CS; q++) {
+        uint32_t* rm = cl.map_shared_rank(mins, q);
+        m0 = min(m0, rm[0]); m1 = min(m1, rm[1]); m2 = min(m2, rm[2]);
+      }
+      // dec: [0] branch, [1] pivot row, [2] anticom (1-based), [3] update r, [4] update anticommutes
+      int32_t branch = 0, pivrow = -1, anticom = 0;
+      if (m0 != 0xFFFFFFFFu) {
+        branch = 1;  // anticommutes with a stabilizer row
+        anticom = (int32_t)m0 + 1;
+      } else if (a.kind == QCB_MIXED_DESTABILIZER && (m1 != 0xFFFFFFFFu || m2 != 0xFFFFFFFFu)) {
+        branch = 2;  // anticommutes with a logical operator
+        anticom = (int32_t)(m1 != 0xFFFFFFFFu ? m1 : m2) + 1;  // 1-based anticomlog
+      } else {
+        branch = 0;
+      }
+      if (branch == 1) {
+        pivrow = (a.kind == QCB_STABILIZER || a.kind == QCB_MIXED_STABILIZER) ? anticom - 1 : (int32_t)nn + anticom - 1;
+      } else if (branch == 2) {
+        pivrow = (int32_t)nn + r;  // row n+r+1 (1-based) after the swaps
+      }
+      dec[0] = branch; dec[1] = pivrow; dec[2] = anticom;
+    }
+    __syncthreads();
+    const int32_t branch = dec[0];
+    if (branch == 0) {
+      // commutes with every stabilizer row
+      bool stop = false;
+      if (a.kind == QCB_STABILIZER || a.kind == QCB_MIXED_STABILIZER) {
+        if (a.keep_result || a.kind == QCB_MIXED_STABILIZER) stop = true;
+        else if (me == 0 && tid == 0) { a.anticom[j] = 0; a.result[j] = -1; }
+      } else if (a.kind == QCB_DESTABILIZER && nn != a.n) {
+        if (me == 0 && tid == 0) { a.status[0] = PST_BADSTRUCT; a.status[1] = (int32_t)j; }
+        cl.sync();
+        return;
+      } else if (me == 0 && warp == 0) {
+        int32_t res = -1;
+        if (a.keep_result) {
+          // new_pauli = product of the stabilizer rows whose destabilizer
+          // anticommutes with the Pauli, phase starting from the Pauli's
+          uint64_t c1 = 0, c2 = 0;
+          uint32_t extra = pphase;
+          uint64_t* buf = piv;  // the pivot buffer is free in this branch
+          for (uint32_t w = lane; w < W; w += 32) buf[w] = 0;
+          __syncwarp();
+          for (uint32_t i = 0; i < (uint32_t)r; i++) {
+            if (!a.flags[i]) continue;  // comm(pauli, destabilizer row i)
+            const uint64_t* srow = a.xzs + (size_t)(nn + i) * W;
+            for (uint32_t w = lane; w < len; w += 32) {
+              uint64_t x2 = buf[w], z2 = buf[len + w];
+              mul_step_p(srow[w], srow[len + w], x2, z2, c1, c2);
+              buf[w] = x2;
+              buf[len + w] = z2;
+            }
+            __syncwarp();
+            extra += a.ph[nn + i];
+          }
+          const uint32_t s =
+              __reduce_add_sync(0xFFFFFFFFu, (uint32_t)(__popcll(c1) + 2 * __popcll(c2)) & 3u) & 3u;
+          res = a.phases ? (int32_t)((s + extra) & 3u) : (int32_t)(pphase & 3u);
+        }
+        if (lane == 0) { a.anticom[j] = 0; a.result[j] = res; }
+      }
+      if (stop) {
+        if (me == 0 && tid == 0) { a.status[0] = PST_NEED_CANON; a.status[1] = (int32_t)j; }
+        cl.sync();
+        return;
+      }
+      cl.sync();
+      continue;
+    }
+    // 3. swaps (MixedDestabilizer logical branch), done by CTA 0
+    if (branch == 2) {
+      if (me == 0) {
+        const uint32_t al = (uint32_t)dec[2];  // 1-based anticomlog
+        auto swaprow = [&](uint32_t u, uint32_t v) {  // 0-based
+          if (u == v) return;
+          uint64_t* ru = a.xzs + (size_t)u * W;
+          uint64_t* rv = a.xzs + (size_t)v * W;
+          for (uint32_t w = tid; w < W; w += blockDim.x) { uint64_t t = ru[w]; ru[w] = rv[w]; rv[w] = t; }
+          if (tid == 0) {
+            uint8_t t = a.ph[u]; a.ph[u] = a.ph[v]; a.ph[v] = t;
+            uint8_t f = a.flags[u]; a.flags[u] = a.flags[v]; a.flags[v] = f;
+          }
+          __syncthreads();
+        };
+        const uint32_t ru = (uint32_t)r;
+        if (al <= nn) {
+          swaprow(ru + nn, al - 1);
+          if (nn != ru + 1 && al != ru + 1) swaprow(ru, al + nn - 1);
+        } else {
+          swaprow(ru, al - nn - 1);
+          swaprow(ru + nn, al - 1);
+        }
+      }
+      cl.sync();
+    }
+    // 4. row updates (anticomm_update_rows or the Stabilizer loop)
+    const uint32_t pivrow = (uint32_t)dec[1];
+    for (uint32_t w = tid; w < W; w += blockDim.x) piv[w] = a.xzs[(size_t)pivrow * W + w];
+    __syncthreads();
+    const uint32_t pph = a.ph[pivrow];
+    if (a.kind == QCB_STABILIZER || a.kind == QCB_MIXED_STABILIZER) {
+      const uint32_t ac = (uint32_t)dec[2];
+      for (uint32_t m = ac + gw; m < (uint32_t)r; m += NW)
+        if (a.flags[m]) warp_rowmul(a.xzs, a.ph, W, m, piv, pph, a.phases != 0, lane);
+    } else {
+      const uint32_t ru = branch == 2 ? (uint32_t)r + 1 : (uint32_t)r;
+      const uint32_t ac = branch == 2 ? (uint32_t)r + 1 : (uint32_t)dec[2];
+      for (uint32_t m = gw; m < 2 * nn; m += NW) {
+        if (!a.flags[m] || m == pivrow) continue;
+        if (m >= ru && m < nn) warp_rowmul(a.xzs, a.ph, W, m, piv, pph, a.phases != 0, lane);
+        else if (m >= nn + ac && m < 2 * nn) warp_rowmul(a.xzs, a.ph, W, m, piv, pph, a.phases != 0, lane);
+        else if (m < ru && m != ac - 1) warp_rowmul(a.xzs, a.ph, W, m, piv, pph, false, lane);
+      }
+    }
+    cl.sync();
+    // 5. row copies, rank, outputs (CTA 0)
+    if (me == 0) {
+      if (a.kind == QCB_STABILIZER || a.kind == QCB_MIXED_STABILIZER) {
+        const uint32_t ac = (uint32_t)dec[2];
+        for (uint32_t w = tid; w < W; w += blockDim.x) a.xzs[(size_t)(ac - 1) * W + w] = P[w];
+        if (tid == 0) { a.ph[ac - 1] = (uint8_t)pphase; a.anticom[j] = (int32_t)ac; a.result[j] = -1; }
+      } else {
+        const uint32_t ac = branch == 2 ? (uint32_t)r + 1 : (uint32_t)dec[2];
+        // destabilizer[ac] = stabilizer[ac]; stabilizer[ac] = pauli
+        for (uint32_t w = tid; w < W; w += blockDim.x) {
+          a.xzs[(size_t)(ac - 1) * W + w] = a.xzs[(size_t)(nn + ac - 1) * W + w];
+        }
+        __syncthreads();
+        for (uint32_t w = tid; w < W; w += blockDim.x) a.xzs[(size_t)(nn + ac - 1) * W + w] = P[w];
+        if (tid == 0) {
+          a.ph[ac - 1] = a.ph[nn + ac - 1];
+          a.ph[nn + ac - 1] = (uint8_t)pphase;
+          if (branch == 2) *a.rank = r + 1;
+          a.anticom[j] = (int32_t)(branch == 2 ? r + 1 : (int32_t)ac);
+          a.result[j] = -1;
+        }
+      }
+    }
+    cl.sync();
+  }
+  if (me == 0 && tid == 0) { a.status[0] = PST_OK; a.status[1] = (int32_t)a.k; }
+}
+
+static uint32_t g_proj_cs = 8;
+
+}  // namespace qcb
+
+using namespace qcb;
+
+extern "C" {
+
+int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* paulis, int keep_result,
+                int phases, int32_t* anticom, int32_t* result, uint32_t* n_done, void* stream) {
+  if (!t || !paulis || !anticom || !result) return fail(QCB_EARG, "null argument");
+  if (paulis->nqubits != t->nqubits) return fail(QCB_EDIM, "project!: the Pauli and the state act on different numbers of qubits");
+  if (kind < 0 || kind > 3) return fail(QCB_EARG, "project!: bad state kind");
+  const bool mixed = kind == QCB_MIXED_STABILIZER || kind == QCB_MIXED_DESTABILIZER;
+  if (mixed && !rank_io) return fail(QCB_EARG, "project!: rank required for mixed states");
+  if ((kind == QCB_DESTABILIZER || kind == QCB_MIXED_DESTABILIZER) && (t->rows % 2))
+    return fail(QCB_EDIM, "project!: destabilizer tableaux have an even number of rows");
+  if (kind == QCB_MIXED_DESTABILIZER && t->rows != 2 * t->nqubits)
+    return fail(QCB_EDIM, "project!: MixedDestabilizer tableaux have 2n rows");
+  if (mixed && (*rank_io < 0 || (uint32_t)*rank_io > (kind == QCB_MIXED_STABILIZER ? t->rows : t->rows / 2)))
+    return fail(QCB_EBOUNDS, "project!: rank out of range");
+  cudaStream_t st = S(stream);
+  const uint32_t k = paulis->rows;
+  if (n_done) *n_done = 0;
+  if (!k) return QCB_OK;
+  int32_t *d_anti = nullptr, *d_res = nullptr, *d_stat = nullptr, *d_rank = nullptr, *d_cout = nullptr;
+  uint8_t* d_flags = nullptr;
+  uint64_t* d_tmp = nullptr;
+  uint8_t* d_tmpph = nullptr;
+  QCB_CUDA(cudaMallocAsync(&d_anti, (size_t)k * 4, st));
+  QCB_CUDA(cudaMallocAsync(&d_res, (size_t)k * 4, st));
+  QCB_CUDA(cudaMallocAsync(&d_stat, 64, st));
+  QCB_CUDA(cudaMallocAsync(&d_rank, 4, st));
+  QCB_CUDA(cudaMallocAsync(&d_cout, 16, st));
+  QCB_CUDA(cudaMallocAsync(&d_flags, std::max<uint32_t>(t->rows, 1), st));
+  QCB_CUDA(cudaMallocAsync(&d_tmp, (size_t)t->W * 8 + 16, st));
+  QCB_CUDA(cudaMallocAsync(&d_tmpph, 16, st));
+  int32_t rank = mixed ? *rank_io : 0;
+  QCB_CUDA(cudaMemcpyAsync(d_rank, &rank, 4, cudaMemcpyHostToDevice, st));
+
+  const size_t sm = (size_t)2 * t->W * 8;
+  const uint32_t cs = g_proj_cs;
+  QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(sm, 1024)));
+  int status = QCB_OK;
+  uint32_t j0 = 0;
+  std::vector<int32_t> h_anti(k, 0), h_res(k, -1);
+  while (j0 < k) {
+    ProjArgs a{};
+    a.xzs = t->xzs; a.ph = t->phases; a.rows = t->rows; a.n = t->nqubits; a.W = t->W;
+    a.kind = kind; a.rank = d_rank; a.paulis = paulis->xzs; a.pph = paulis->phases;
+    a.j0 = j0; a.k = k; a.keep_result = keep_result; a.phases = phases;
+    a.anticom = d_anti; a.result = d_res; a.status = d_stat; a.flags = d_flags;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(PROJ_THREADS);
+    cfg.dynamicSmemBytes = std::max<size_t>(sm, 1024);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    QCB_CUDA(cudaLaunchKernelEx(&cfg, project_kernel, a));
+    QCB_LAUNCHED();
+    int32_t hs[2];
+    QCB_CUDA(cudaMemcpyAsync(hs, d_stat, 8, cudaMemcpyDeviceToHost, st));
+    QCB_CUDA(cudaStreamSynchronize(st));
+    if (hs[0] == PST_OK) break;
+    const uint32_t j = (uint32_t)hs[1];
+    if (hs[0] == PST_BADSTRUCT) {
+      status = fail(QCB_EBADSTRUCT,
+                    "`Destabilizer` can not efficiently (faster than n^3) detect whether you are projecting on a "
+                    "stabilized or a logical operator. Switch to one of the `Mixed*` data structures.");
+      if (n_done) *n_done = j;
+      j0 = k;
+      break;
+    }
+    // PST_NEED_CANON: canonicalize the stabilizer view, then generate!
+    int32_t r_now = rank;
+    if (kind == QCB_MIXED_STABILIZER) QCB_CUDA(cudaMemcpy(&r_now, d_rank, 4, cudaMemcpyDeviceToHost));
+    const uint32_t nr = kind == QCB_STABILIZER ? t->rows : (uint32_t)r_now;
+    if (int s = canonicalize_view(t->xzs, t->phases, nr, t->nqubits, t->W, phases, d_cout, st)) { status = s; break; }
+    QCB_CUDA(cudaMemcpyAsync(d_tmp, paulis->xzs + (size_t)j * t->W, (size_t)t->W * 8, cudaMemcpyDeviceToDevice, st));
+    QCB_CUDA(cudaMemcpyAsync(d_tmpph, paulis->phases + j, 1, cudaMemcpyDeviceToDevice, st));
+    if (int s = generate_dev(d_tmp, d_tmpph, t->xzs, t->phases, nr, t->W, phases, d_cout + 2, nullptr, 0,
+                             (uint32_t*)(d_cout + 3), st)) { status = s; break; }
+    int32_t cout[4];
+    uint8_t gph = 0;
+    QCB_CUDA(cudaMemcpyAsync(cout, d_cout, 16, cudaMemcpyDeviceToHost, st));
+    QCB_CUDA(cudaMemcpyAsync(&gph, d_tmpph, 1, cudaMemcpyDeviceToHost, st));
+    QCB_CUDA(cudaStreamSynchronize(st));
+    int32_t anti = 0, res = -1;
+    if (cout[2]) {
+      res = gph;
+    } else {
+      anti = cout[1] + 1;
+      if (kind == QCB_MIXED_STABILIZER && anti == r_now + 1) {
+        // ms.tab[rank+1] = pauli; rank += 1  (src/project_trace_reset.jl:310-317)
+        if ((uint32_t)r_now >= t->rows) { status = fail(QCB_EBOUNDS, "MixedStabilizer tableau is full"); break; }
+        QCB_CUDA(cudaMemcpyAsync(t->xzs + (size_t)r_now * t->W, paulis->xzs + (size_t)j * t->W, (size_t)t->W * 8,
+                                 cudaMemcpyDeviceToDevice, st));
+        QCB_CUDA(cudaMemcpyAsync(t->phases + r_now, paulis->phases + j, 1, cudaMemcpyDeviceToDevice, st));
+        r_now += 1;
+        QCB_CUDA(cudaMemcpyAsync(d_rank, &r_now, 4, cudaMemcpyHostToDevice, st));
+      }
+    }
+    QCB_CUDA(cudaMemcpyAsync(d_anti + j, &anti, 4, cudaMemcpyHostToDevice, st));
+    QCB_CUDA(cudaMemcpyAsync(d_res + j, &res, 4, cudaMemcpyHostToDevice, st));
+    QCB_CUDA(cudaStreamSynchronize(st));
+    j0 = j + 1;
+  }
+  if (status == QCB_OK || status == QCB_EBADSTRUCT) {
+    QCB_CUDA(cudaMemcpyAsync(h_anti.data(), d_anti, (size_t)k * 4, cudaMemcpyDeviceToHost, st));
+    QCB_CUDA(cudaMemcpyAsync(h_res.data(), d_res, (size_t)k * 4, cudaMemcpyDeviceToHost, st));
+    if (mixed) QCB_CUDA(cudaMemcpyAsync(&rank, d_rank, 4, cudaMemcpyDeviceToHost, st));
+    QCB_CUDA(cudaStreamSynchronize(st));
+    std::copy(h_anti.begin(), h_anti.end(), anticom);
+    std::copy(h_res.begin(), h_res.end(), result);
+    if (mixed) *rank_io = rank;
+    if (status == QCB_OK && n_done) *n_done = k;
+  }
+  cudaFreeAsync(d_anti, st); cudaFreeAsync(d_res, st); cudaFreeAsync(d_stat, st);
+  cudaFreeAsync(d_rank, st); cudaFreeAsync(d_cout, st); cudaFreeAsync(d_flags, st);
+  cudaFreeAsync(d_tmp, st); cudaFreeAsync(d_tmpph, st);
+  cudaStreamSynchronize(st);
+  return status;
+}
+
+}  // extern "C"
+
+namespace qcb {
+void set_project_cluster(uint32_t cs) { g_proj_cs = cs ? cs : 8; }
+}

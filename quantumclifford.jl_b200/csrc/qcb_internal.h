@@ -1,0 +1,132 @@
+// qcb_internal.h -- shared internals of libqcb200 (host + device).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "../../include/qcb200.h"
+
+namespace qcb {
+
+// ------------------------------------------------------------ errors
+void set_error(int status, const std::string& msg);
+int fail(int status, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+extern std::atomic<uint64_t> g_launches;
+
+#define QCB_CUDA(call)                                        \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return ::qcb::cuda_fail(e_, #call); \
+  } while (0)
+
+// Check the launch that was just issued and count it.
+#define QCB_LAUNCHED()                                                 \
+  do {                                                                 \
+    ::qcb::g_launches.fetch_add(1, std::memory_order_relaxed);         \
+    cudaError_t e_ = cudaGetLastError();                               \
+    if (e_ != cudaSuccess) return ::qcb::cuda_fail(e_, "kernel launch"); \
+  } while (0)
+
+inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+
+int device_sm_count();
+int device_max_smem_optin();
+
+// ------------------------------------------------------------ Philox
+enum : uint32_t { TAG_INITZ = 0x51A7u, TAG_RESET = 0x5E5Eu, TAG_NOISE = 0x4E01u };
+
+// Philox-4x32-10 (Salmon et al., SC'11), published multipliers and Weyl
+// increments.  Counter = (index, column lo, column hi, tag), key = seed.
+__host__ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2,
+                                                       uint32_t c3, uint32_t k0, uint32_t k1,
+                                                       uint32_t out[4]) {
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+  for (int r = 0; r < 10; r++) {
+#ifdef __CUDA_ARCH__
+    uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+    uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+#else
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+    uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+// ------------------------------------------------------------ programs
+// Device program: a stream of 16-byte aligned records.
+//   header (4 words): [kind<<24 | count, aux0, aux1, aux2]
+//   operands: padded to a multiple of 4 words.
+enum SegKind : uint32_t {
+  SEG_END = 0,
+  SEG_CNOT = 1,   // count gates, 2 words each (c, t), padded to 4 gates
+  SEG_H = 2,      // 1 word each (q), padded to 4
+  SEG_S = 3,      // 1 word each (q), padded to 4
+  SEG_G1 = 4,     // 2 words each (opcode, q), padded to 2
+  SEG_G2 = 5,     // 4 words each (opcode, q1, q2, 0)
+  SEG_MZ = 6,     // 2 words each (q, bit or NONE), padded to 2
+  SEG_MRZ = 7,    // 4 words each (q, bit or NONE, reset index, is_pad)
+  SEG_FLUSH = 8,  // header only: aux0 = site begin, aux1 = site end
+  SEG_CZ = 9      // 2 words each (a, b), padded to 4 gates
+};
+constexpr uint32_t BIT_NONE = 0xFFFFFFFFu;
+
+// A noise site.  kind = opcode (PAULI_NOISE / DEPOL1 / DEPOL2); a, b =
+// operand (slot or qubit); thresholds for the event kind.
+struct Site {
+  uint32_t kind, a, b, pad;
+  double t0, t1, t2;  // PAULI: X if v<t0, Z if v<t1, Y if v<t2;  DEPOL: t0 = p_eff
+  double pad2;
+};
+
+struct Program {
+  qcb_program_info info;
+  uint32_t nq;         // qubits referenced (max index)
+  uint32_t nslots;     // distinct qubits referenced (smem slots); scratch = nslots
+  std::vector<uint32_t> slot_qubit;   // slot -> 0-based qubit
+  std::vector<uint32_t> stream_slot;  // operands in slot space; scratch slot = nslots
+  std::vector<Site> sites_slot;
+  std::vector<int64_t> site_of_op;    // op index -> site (or -1)
+  std::vector<uint32_t> site_arity;
+  double pmax = 0, inv_log1m = 0;
+  // device copies
+  uint32_t* d_stream_slot = nullptr;
+  Site* d_sites_slot = nullptr;
+  uint32_t* d_slot_qubit = nullptr;
+  uint32_t* d_qubit_slot = nullptr;   // [nq_alloc] qubit -> slot or NONE
+  uint32_t qubit_slot_len = 0;
+  uint64_t hash = 0;
+};
+
+}  // namespace qcb
+
+struct qcb_program : qcb::Program {};
+
+struct qcb_frame {
+  uint64_t frames;
+  uint32_t qubits;   // user qubits (frame has qubits+1)
+  uint32_t nq1;      // qubits + 1
+  uint32_t nbits;
+  uint64_t ncols;    // ceil(frames/32)
+  uint64_t pitch;    // words per plane (>= ncols, multiple of 32)
+  uint32_t* planes;  // [(2*(nq1+1))][pitch]: plane 2q = x(q), 2q+1 = z(q); last pair = scratch
+  uint32_t* record;  // [nbits][pitch]
+};
+
+struct qcb_tableau {
+  uint32_t rows;
+  uint32_t nqubits;
+  uint32_t W;        // words per row = 2*ceil(n/64)
+  uint64_t* xzs;     // rows x W, row-contiguous
+  uint8_t* phases;   // rows
+  uint32_t* scratch; // small device scratch (phase accumulators, flags)
+};

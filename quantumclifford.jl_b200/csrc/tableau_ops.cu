@@ -1,0 +1,434 @@
+// tableau_ops.cu -- row algebra on device tableaux.
+//
+//  mul_left!  (src/mul_leftright.jl:75-142, 171-229): r <- l * r with the
+//             phase of the product.  The phase is the sum over bit lanes of
+//             independent mod-4 counters (cnt1 = low bit, cnt2 = high bit),
+//             so any partition of the words into threads sums exactly:
+//             phase = (sum popc(cnt1) + 2 * sum popc(cnt2)) mod 4.
+//  prodphase / comm (src/QuantumClifford.jl:723-859).
+//  symbolic gates with phases (src/symbolic_cliffords.jl:62-74, 293-316).
+//  dense apply! (src/dense_cliffords.jl:135-169).
+#include <algorithm>
+
+#include "qcb_internal.h"
+
+namespace qcb {
+
+// Stim phase-counter step on one word pair (src/mul_leftright.jl:90-96).
+template <class T>
+__device__ __forceinline__ void mul_step(T x1, T z1, T& x2, T& z2, uint64_t& c1, uint64_t& c2) {
+  const uint64_t nx = x1 ^ x2, nz = z1 ^ z2;
+  const uint64_t x1z2 = (uint64_t)x1 & (uint64_t)z2;
+  const uint64_t anti = ((uint64_t)x2 & (uint64_t)z1) ^ x1z2;
+  c2 ^= (c1 ^ nx ^ nz ^ x1z2) & anti;
+  c1 ^= anti;
+  x2 = (T)nx;
+  z2 = (T)nz;
+}
+
+__device__ __forceinline__ uint32_t cnt_phase(uint64_t c1, uint64_t c2) {
+  return (uint32_t)(__popcll(c1) + 2 * __popcll(c2));
+}
+
+// Grid-stride mul_left! over two long Paulis.  VEC = 2 uses 128-bit loads
+// (needs len even and 16-byte aligned halves).  Each block adds its phase
+// sum (mod 4) into acc[0].
+template <int VEC, bool PH>
+__global__ void __launch_bounds__(256) mul_left_long_kernel(uint64_t* __restrict__ r,
+                                                            const uint64_t* __restrict__ l,
+                                                            uint64_t len, uint32_t* acc) {
+  uint64_t c1a = 0, c2a = 0, c1b = 0, c2b = 0;
+  const uint64_t nvec = len / VEC;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nvec; i += stride) {
+    if (VEC == 2) {
+      const ulonglong2 lx = __ldcs((const ulonglong2*)l + i);
+      const ulonglong2 lz = __ldcs((const ulonglong2*)(l + len) + i);
+      ulonglong2 rx = __ldcs((const ulonglong2*)r + i);
+      ulonglong2 rz = __ldcs((const ulonglong2*)(r + len) + i);
+      if (PH) {
+        mul_step(lx.x, lz.x, rx.x, rz.x, c1a, c2a);
+        mul_step(lx.y, lz.y, rx.y, rz.y, c1b, c2b);
+      } else {
+        rx.x ^= lx.x; rx.y ^= lx.y; rz.x ^= lz.x; rz.y ^= lz.y;
+      }
+      __stcs((ulonglong2*)r + i, rx);
+      __stcs((ulonglong2*)(r + len) + i, rz);
+    } else {
+      const uint64_t lx = __ldcs(l + i), lz = __ldcs(l + len + i);
+      uint64_t rx = __ldcs(r + i), rz = __ldcs(r + len + i);
+      if (PH) mul_step(lx, lz, rx, rz, c1a, c2a);
+      else { rx ^= lx; rz ^= lz; }
+      __stcs(r + i, rx);
+      __stcs(r + len + i, rz);
+    }
+  }
+  if (!PH) return;
+  uint32_t v = (cnt_phase(c1a, c2a) + cnt_phase(c1b, c2b)) & 3u;
+  v = __reduce_add_sync(0xFFFFFFFFu, v) & 3u;
+  __shared__ uint32_t wsum[32];
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) wsum[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t s = lane < (blockDim.x >> 5) ? wsum[lane] : 0u;
+    s = __reduce_add_sync(0xFFFFFFFFu, s) & 3u;
+    if (lane == 0 && s) atomicAdd(acc, s);
+  }
+}
+
+// r.phase <- (s + r.phase + l.phase) & 3 (src/mul_leftright.jl:140); clears acc.
+__global__ void mul_left_finish_kernel(uint8_t* r_phase, const uint8_t* l_phase, uint32_t* acc,
+                                       int phases) {
+  const uint32_t s = acc[0] & 3u;
+  if (phases) r_phase[0] = (uint8_t)((s + r_phase[0] + l_phase[0]) & 3u);
+  acc[0] = 0;
+}
+
+// Row-level ops: one warp per target row; lanes stride over the words.
+template <bool PH>
+__device__ __forceinline__ uint32_t warp_mul_left_row(uint64_t* r, const uint64_t* l, uint32_t len,
+                                                      uint32_t lane) {
+  uint64_t c1 = 0, c2 = 0;
+  for (uint32_t w = lane; w < len; w += 32) {
+    uint64_t rx = r[w], rz = r[len + w];
+    const uint64_t lx = l[w], lz = l[len + w];
+    if (PH) mul_step(lx, lz, rx, rz, c1, c2);
+    else { rx ^= lx; rz ^= lz; }
+    r[w] = rx;
+    r[len + w] = rz;
+  }
+  if (!PH) return 0;
+  return __reduce_add_sync(0xFFFFFFFFu, cnt_phase(c1, c2) & 3u) & 3u;
+}
+
+// mul_left!(s::Tableau, p::PauliOperator) (src/mul_leftright.jl:221-227).
+__global__ void mul_left_tab_pauli_kernel(uint64_t* xzs, uint8_t* ph, uint32_t rows, uint32_t W,
+                                          const uint64_t* p, const uint8_t* pph, int phases) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= rows) return;
+  uint64_t* r = xzs + (uint64_t)warp * W;
+  if (phases) {
+    const uint32_t s = warp_mul_left_row<true>(r, p, W / 2, lane);
+    if (lane == 0) ph[warp] = (uint8_t)((s + ph[warp] + pph[0]) & 3u);
+  } else {
+    warp_mul_left_row<false>(r, p, W / 2, lane);
+  }
+}
+
+// mul_left!(s::Tableau, m, i) (src/mul_leftright.jl:177-181), 0-based rows.
+__global__ void mul_left_row_kernel(uint64_t* xzs, uint8_t* ph, uint32_t W, uint32_t m, uint32_t i,
+                                    int phases) {
+  const uint32_t lane = threadIdx.x & 31;
+  if (threadIdx.x >= 32) return;
+  uint64_t* r = xzs + (uint64_t)m * W;
+  const uint64_t* l = xzs + (uint64_t)i * W;
+  if (phases) {
+    const uint32_t s = warp_mul_left_row<true>(r, l, W / 2, lane);
+    if (lane == 0) ph[m] = (uint8_t)((s + ph[m] + ph[i]) & 3u);
+  } else {
+    warp_mul_left_row<false>(r, l, W / 2, lane);
+  }
+}
+
+// prodphase (src/QuantumClifford.jl:723-733) and comm (:791-798) of two rows.
+__global__ void prodphase_comm_kernel(const uint64_t* l, uint8_t lph, const uint64_t* r, uint8_t rph,
+                                      uint32_t len, int what, uint8_t* out) {
+  const uint32_t lane = threadIdx.x & 31;
+  if (threadIdx.x >= 32) return;
+  int32_t acc = 0;
+  uint64_t cm = 0;
+  for (uint32_t w = lane; w < len; w += 32) {
+    const uint64_t x1 = l[w], x2 = r[w], z1 = l[len + w], z2 = r[len + w];
+    acc += __popcll((~z2 & x2 & ~x1 & z1) | (z2 & ~x2 & x1 & z1) | (z2 & x2 & x1 & ~z1));
+    acc -= __popcll((z2 & x2 & ~x1 & z1) | (~z2 & x2 & x1 & z1) | (z2 & ~x2 & x1 & ~z1));
+    cm ^= (z1 & x2) ^ (x1 & z2);
+  }
+  const int32_t tot = __reduce_add_sync(0xFFFFFFFFu, acc);
+  const uint32_t par = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)__popcll(cm)) & 1u;
+  if (lane == 0) {
+    if (what == 0) out[0] = (uint8_t)(((uint32_t)tot + lph + rph) & 3u);
+    else out[0] = (uint8_t)par;
+  }
+}
+
+// ---------------------------------------------------------- symbolic gates
+// Bit-sliced truth tables with the phase flag (src/symbolic_cliffords.jl
+// :105-118 and :358-395).
+__device__ __forceinline__ uint64_t g1(uint32_t op, uint64_t& x, uint64_t& z) {
+  const uint64_t X = x, Z = z;
+  switch (op) {
+    case QCB_OP_H: x = Z; z = X; return X & Z;
+    case QCB_OP_HXY: z = X ^ Z; return ~X & Z;
+    case QCB_OP_HYZ: x = X ^ Z; return X & ~Z;
+    case QCB_OP_S: z = X ^ Z; return X & Z;
+    case QCB_OP_SDAG: z = X ^ Z; return X & ~Z;
+    case QCB_OP_X: return Z;
+    case QCB_OP_Y: return X ^ Z;
+    case QCB_OP_Z: return X;
+    case QCB_OP_SQRTX: x = X ^ Z; return ~X & Z;
+    case QCB_OP_INVSQRTX: x = X ^ Z; return X & Z;
+    case QCB_OP_SQRTY: x = Z; z = X; return X & ~Z;
+    case QCB_OP_INVSQRTY: x = Z; z = X; return Z & ~X;
+    case QCB_OP_CXYZ: x = X ^ Z; z = X; return 0;
+    case QCB_OP_CZYX: x = Z; z = X ^ Z; return 0;
+    default: return 0;
+  }
+}
+
+__device__ __forceinline__ uint64_t g2(uint32_t op, uint64_t& x1, uint64_t& z1, uint64_t& x2,
+                                       uint64_t& z2) {
+  const uint64_t a = x1, b = z1, c = x2, d = z2;
+  switch (op) {
+    case QCB_OP_SWAP: x1 = c; z1 = d; x2 = a; z2 = b; return 0;
+    case QCB_OP_CNOT: z1 = b ^ d; x2 = c ^ a; return (a & b & c & d) | (a & d & ~(b | c));
+    case QCB_OP_CPHASE: z1 = b ^ c; z2 = d ^ a; return (a & b & c & ~d) | (a & ~b & c & d);
+    case QCB_OP_ZCX: z1 = b ^ d; x2 = c ^ a; return (a & d) & ~(b ^ c);
+    case QCB_OP_ZCY: z1 = c ^ b ^ d; x2 = c ^ a; z2 = d ^ a; return a & (c ^ b) & (c ^ d);
+    case QCB_OP_ZCZ: z1 = b ^ c; z2 = d ^ a; return (b ^ d) & (a & c);
+    case QCB_OP_XCX: x1 = d ^ a; x2 = c ^ b; return (b & d) & (a ^ c);
+    case QCB_OP_XCY: x1 = a ^ c ^ d; x2 = b ^ c; z2 = d ^ b; return b & (c ^ d) & ~(c ^ a);
+    case QCB_OP_XCZ: x1 = a ^ c; z2 = d ^ b; return (c & b) & ~(a ^ d);
+    case QCB_OP_YCX: x1 = a ^ d; z1 = d ^ b; x2 = a ^ b ^ c; return d & (a ^ b) & ~(c ^ a);
+    case QCB_OP_YCY:
+      x1 = a ^ d ^ c; z1 = b ^ c ^ d; x2 = a ^ c ^ b; z2 = a ^ b ^ d;
+      return (a & ~b & ~c & d) | (~a & b & c & ~d);
+    case QCB_OP_YCZ: x1 = a ^ c; z1 = c ^ b; z2 = d ^ a ^ b; return c & (a ^ b) & (d ^ a);
+    default: return 0;
+  }
+}
+
+struct GateOp {
+  uint32_t op, q1, q2, pad;
+};
+
+// Thread per row; the whole gate list is applied to that row in order.
+__global__ void apply_gates_kernel(uint64_t* xzs, uint8_t* ph, uint32_t rows, uint32_t W,
+                                   const GateOp* ops, uint32_t nops, int phases) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  uint64_t* row = xzs + (uint64_t)r * W;
+  const uint32_t len = W / 2;
+  uint32_t p = ph[r];
+  for (uint32_t k = 0; k < nops; k++) {
+    const GateOp g = ops[k];
+    if (g.op < QCB_OP_CNOT) {
+      const uint32_t q = g.q1, w = q >> 6, s = q & 63;
+      uint64_t x = (row[w] >> s) & 1, z = (row[len + w] >> s) & 1;
+      const uint64_t f = g1(g.op, x, z) & 1;
+      row[w] = (row[w] & ~(1ull << s)) | ((x & 1) << s);
+      row[len + w] = (row[len + w] & ~(1ull << s)) | ((z & 1) << s);
+      if (phases && f) p = (p + 2) & 3;
+    } else {
+      const uint32_t w1 = g.q1 >> 6, s1 = g.q1 & 63, w2 = g.q2 >> 6, s2 = g.q2 & 63;
+      uint64_t x1 = (row[w1] >> s1) & 1, z1 = (row[len + w1] >> s1) & 1;
+      uint64_t x2 = (row[w2] >> s2) & 1, z2 = (row[len + w2] >> s2) & 1;
+      const uint64_t f = g2(g.op, x1, z1, x2, z2) & 1;
+      row[w1] = (row[w1] & ~(1ull << s1)) | ((x1 & 1) << s1);
+      row[len + w1] = (row[len + w1] & ~(1ull << s1)) | ((z1 & 1) << s1);
+      row[w2] = (row[w2] & ~(1ull << s2)) | ((x2 & 1) << s2);
+      row[len + w2] = (row[len + w2] & ~(1ull << s2)) | ((z2 & 1) << s2);
+      if (phases && f) p = (p + 2) & 3;
+    }
+  }
+  ph[r] = (uint8_t)p;
+}
+
+// ---------------------------------------------------------- dense apply!
+// One warp per state row.  The ordered product over qubits of the Clifford's
+// images (src/dense_cliffords.jl:152-169) is accumulated in registers; the
+// phase counters run across all the multiplications (each multiplication adds
+// +-1 per anticommuting lane, independent of the current counter value), so
+// one reduction at the end gives the exact total.
+template <int MAXW>
+__global__ void __launch_bounds__(256) apply_dense_kernel(uint64_t* xzs, uint8_t* ph, uint32_t rows,
+                                                          uint32_t W, uint32_t n,
+                                                          const uint64_t* __restrict__ c,
+                                                          const uint8_t* __restrict__ cph,
+                                                          int phases) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= rows) return;
+  const uint32_t len = W / 2;
+  constexpr int PER = (MAXW / 2 + 31) / 32;  // words per lane per half
+  uint64_t bx[PER], bz[PER], c1[PER], c2[PER];
+#pragma unroll
+  for (int k = 0; k < PER; k++) { bx[k] = bz[k] = c1[k] = c2[k] = 0; }
+  uint64_t* row = xzs + (uint64_t)warp * W;
+  uint32_t extra = 0;  // sum of Clifford-row phases and -1 corrections (mod 4)
+  for (uint32_t wq = 0; wq < len; wq++) {
+    const uint64_t xw = row[wq], zw = row[len + wq];  // broadcast loads
+    uint64_t both = xw | zw;
+    while (both) {
+      const uint32_t b = __ffsll((long long)both) - 1;
+      both &= both - 1;
+      const uint32_t q = wq * 64 + b;
+      if (q >= n) break;
+      const bool x = (xw >> b) & 1, z = (zw >> b) & 1;
+      if (x && z) extra += 3;  // phase -= 1
+      if (x) {
+        const uint64_t* cr = c + (uint64_t)q * W;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+          const uint32_t w = lane + 32 * k;
+          if (w < len) mul_step<uint64_t>(__ldg(cr + w), __ldg(cr + len + w), bx[k], bz[k], c1[k], c2[k]);
+        }
+        extra += cph[q];
+      }
+      if (z) {
+        const uint64_t* cr = c + (uint64_t)(q + n) * W;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+          const uint32_t w = lane + 32 * k;
+          if (w < len) mul_step<uint64_t>(__ldg(cr + w), __ldg(cr + len + w), bx[k], bz[k], c1[k], c2[k]);
+        }
+        extra += cph[q + n];
+      }
+    }
+  }
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < PER; k++) s += cnt_phase(c1[k], c2[k]);
+  s = __reduce_add_sync(0xFFFFFFFFu, s & 3u) & 3u;
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    const uint32_t w = lane + 32 * k;
+    if (w < len) { row[w] = bx[k]; row[len + w] = bz[k]; }
+  }
+  if (lane == 0) ph[warp] = phases ? (uint8_t)((s + extra + ph[warp]) & 3u) : (uint8_t)0;
+}
+
+}  // namespace qcb
+
+using namespace qcb;
+
+extern "C" {
+
+int qcb_mul_left_pauli(qcb_tableau* r, const qcb_tableau* l, int phases, uint8_t* phase_out,
+                       void* stream) {
+  if (!r || !l) return fail(QCB_EARG, "null argument");
+  if (r->nqubits != l->nqubits)
+    return fail(QCB_EDIM, "The two Pauli operators should have the same length!");
+  if (r->rows < 1 || l->rows < 1) return fail(QCB_EDIM, "empty Pauli");
+  const uint64_t len = r->W / 2;
+  cudaStream_t st = S(stream);
+  const int sms = device_sm_count();
+  const bool vec = (len % 2 == 0);
+  const uint64_t work = vec ? len / 2 : len;
+  uint32_t blocks = (uint32_t)std::min<uint64_t>((work + 255) / 256, (uint64_t)sms * 8);
+  if (blocks == 0) blocks = 1;
+  if (len) {
+    if (vec) {
+      if (phases) mul_left_long_kernel<2, true><<<blocks, 256, 0, st>>>(r->xzs, l->xzs, len, r->scratch);
+      else mul_left_long_kernel<2, false><<<blocks, 256, 0, st>>>(r->xzs, l->xzs, len, r->scratch);
+    } else {
+      if (phases) mul_left_long_kernel<1, true><<<blocks, 256, 0, st>>>(r->xzs, l->xzs, len, r->scratch);
+      else mul_left_long_kernel<1, false><<<blocks, 256, 0, st>>>(r->xzs, l->xzs, len, r->scratch);
+    }
+    QCB_LAUNCHED();
+  }
+  mul_left_finish_kernel<<<1, 1, 0, st>>>(r->phases, l->phases, r->scratch, phases);
+  QCB_LAUNCHED();
+  if (phase_out) {
+    QCB_CUDA(cudaMemcpyAsync(phase_out, r->phases, 1, cudaMemcpyDeviceToHost, st));
+    QCB_CUDA(cudaStreamSynchronize(st));
+  }
+  return QCB_OK;
+}
+
+int qcb_mul_left_row(qcb_tableau* s, uint32_t m, uint32_t i, int phases, void* stream) {
+  if (!s) return fail(QCB_EARG, "null tableau");
+  if (m < 1 || i < 1 || m > s->rows || i > s->rows) return fail(QCB_EBOUNDS, "row index out of bounds");
+  mul_left_row_kernel<<<1, 32, 0, S(stream)>>>(s->xzs, s->phases, s->W, m - 1, i - 1, phases);
+  QCB_LAUNCHED();
+  return QCB_OK;
+}
+
+int qcb_mul_left_tableau_pauli(qcb_tableau* s, const qcb_tableau* p, int phases, void* stream) {
+  if (!s || !p) return fail(QCB_EARG, "null argument");
+  if (s->nqubits != p->nqubits) return fail(QCB_EDIM, "The tableau and the Pauli operator must have the same number of qubits");
+  if (!s->rows) return QCB_OK;
+  const uint32_t threads = 256, blocks = (s->rows * 32 + threads - 1) / threads;
+  mul_left_tab_pauli_kernel<<<blocks, threads, 0, S(stream)>>>(s->xzs, s->phases, s->rows, s->W,
+                                                               p->xzs, p->phases, phases);
+  QCB_LAUNCHED();
+  return QCB_OK;
+}
+
+static int pc_common(const qcb_tableau* l, uint32_t i, const qcb_tableau* r, uint32_t j, uint8_t* out,
+                     void* stream, int what) {
+  if (!l || !r || !out) return fail(QCB_EARG, "null argument");
+  if (l->nqubits != r->nqubits) return fail(QCB_EDIM, "operands must have the same number of qubits");
+  if (i < 1 || i > l->rows || j < 1 || j > r->rows) return fail(QCB_EBOUNDS, "row index out of bounds");
+  cudaStream_t st = S(stream);
+  uint8_t lph = 0, rph = 0;
+  QCB_CUDA(cudaMemcpyAsync(&lph, l->phases + (i - 1), 1, cudaMemcpyDeviceToHost, st));
+  QCB_CUDA(cudaMemcpyAsync(&rph, r->phases + (j - 1), 1, cudaMemcpyDeviceToHost, st));
+  QCB_CUDA(cudaStreamSynchronize(st));
+  uint8_t* d = (uint8_t*)l->scratch + 64;
+  prodphase_comm_kernel<<<1, 32, 0, st>>>(l->xzs + (uint64_t)(i - 1) * l->W, lph,
+                                          r->xzs + (uint64_t)(j - 1) * r->W, rph, l->W / 2, what, d);
+  QCB_LAUNCHED();
+  QCB_CUDA(cudaMemcpyAsync(out, d, 1, cudaMemcpyDeviceToHost, st));
+  QCB_CUDA(cudaStreamSynchronize(st));
+  return QCB_OK;
+}
+
+int qcb_prodphase(const qcb_tableau* l, uint32_t i, const qcb_tableau* r, uint32_t j, uint8_t* out,
+                  void* stream) {
+  return pc_common(l, i, r, j, out, stream, 0);
+}
+
+int qcb_comm(const qcb_tableau* l, uint32_t i, const qcb_tableau* r, uint32_t j, uint8_t* out,
+             void* stream) {
+  return pc_common(l, i, r, j, out, stream, 1);
+}
+
+int qcb_apply_gates(qcb_tableau* t, const qcb_op* ops, size_t n_ops, int phases, void* stream) {
+  if (!t) return fail(QCB_EARG, "null tableau");
+  std::vector<GateOp> g;
+  g.reserve(n_ops);
+  for (size_t k = 0; k < n_ops; k++) {
+    const qcb_op& o = ops[k];
+    const bool one = o.opcode >= QCB_OP_I && o.opcode <= QCB_OP_CZYX;
+    const bool two = o.opcode >= QCB_OP_CNOT && o.opcode <= QCB_OP_YCZ;
+    if (!one && !two) return fail(QCB_EUNSUPPORTED, "qcb_apply_gates: op " + std::to_string(k) + " is not a symbolic Clifford gate");
+    if (o.q1 == 0 || (two && o.q2 == 0)) return fail(QCB_EZEROQUBIT, "qubit indices start at 1 (NoZeroQubit)");
+    if (two && o.q1 == o.q2) return fail(QCB_EARG, "Failed to create a two qubit gate because the two qubits it acts on have the same index. The qubit indices have to be different.");
+    if (o.q1 > t->nqubits || (two && o.q2 > t->nqubits)) return fail(QCB_EBOUNDS, "gate qubit index exceeds the tableau's qubits");
+    g.push_back({o.opcode, o.q1 - 1, two ? o.q2 - 1 : 0, 0});
+  }
+  if (g.empty() || !t->rows) return QCB_OK;
+  cudaStream_t st = S(stream);
+  GateOp* d = nullptr;
+  QCB_CUDA(cudaMallocAsync(&d, g.size() * sizeof(GateOp), st));
+  QCB_CUDA(cudaMemcpyAsync(d, g.data(), g.size() * sizeof(GateOp), cudaMemcpyHostToDevice, st));
+  apply_gates_kernel<<<(t->rows + 127) / 128, 128, 0, st>>>(t->xzs, t->phases, t->rows, t->W, d,
+                                                            (uint32_t)g.size(), phases);
+  QCB_LAUNCHED();
+  QCB_CUDA(cudaFreeAsync(d, st));
+  QCB_CUDA(cudaStreamSynchronize(st));  // the host vector must outlive the copy
+  return QCB_OK;
+}
+
+int qcb_apply_dense(qcb_tableau* t, const qcb_tableau* c, int phases, void* stream) {
+  if (!t || !c) return fail(QCB_EARG, "null argument");
+  if (t->nqubits != c->nqubits || c->rows != 2 * c->nqubits)
+    return fail(QCB_EDIM, "The tableau and the Clifford operator need to act on the same number of qubits.");
+  if (!t->rows) return QCB_OK;
+  const uint32_t threads = 256, blocks = (t->rows * 32 + threads - 1) / threads;
+  cudaStream_t st = S(stream);
+  const uint32_t W = t->W;
+  if (W <= 64)
+    apply_dense_kernel<64><<<blocks, threads, 0, st>>>(t->xzs, t->phases, t->rows, W, t->nqubits, c->xzs, c->phases, phases);
+  else if (W <= 128)
+    apply_dense_kernel<128><<<blocks, threads, 0, st>>>(t->xzs, t->phases, t->rows, W, t->nqubits, c->xzs, c->phases, phases);
+  else if (W <= 256)
+    apply_dense_kernel<256><<<blocks, threads, 0, st>>>(t->xzs, t->phases, t->rows, W, t->nqubits, c->xzs, c->phases, phases);
+  else
+    return fail(QCB_EUNSUPPORTED, "qcb_apply_dense: at most 8192 qubits");
+  QCB_LAUNCHED();
+  return QCB_OK;
+}
+
+}  // extern "C"

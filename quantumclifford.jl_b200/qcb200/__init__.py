@@ -1,0 +1,28 @@
+"""qcb200 -- host-side mirror of QuantumClifford.jl's bit-packed tableau /
+Pauli-frame API over libqcb200 (the B200 C ABI in include/qcb200.h).
+
+Julia names map to Python ones with ``!`` spelled as a trailing underscore:
+``mul_left!`` -> ``mul_left_``, ``canonicalize!`` -> ``canonicalize_``,
+``project!`` -> ``project_``, ``apply!`` -> ``apply_``, ``pauliframe!`` ->
+``pauliframe_``.
+"""
+from ._lib import (  # noqa: F401
+    QCBError, DimensionMismatch, BoundsError, ArgumentError, BadDataStructure, lib, check, ensure_init,
+    exported_symbols, LIB_PATH, OP_DTYPE, EVENT_DTYPE,
+)
+from .ops import (  # noqa: F401
+    Op, OP, sId1, sHadamard, sPhase, sInvPhase, sX, sY, sZ, sSQRTX, sInvSQRTX, sSQRTY, sInvSQRTY,
+    sHadamardXY, sHadamardYZ, sCXYZ, sCZYX, sCNOT, sCPHASE, sSWAP, sZCX, sZCY, sZCZ, sXCX, sXCY, sXCZ,
+    sYCX, sYCY, sYCZ, sMZ, sMRZ, sMX, sMRX, PauliError, NoiseOp, PauliNoise, UnbiasedUncorrelatedNoise,
+    DepolarizationNoise, to_array, count_updates, affected_counts,
+)
+from .frames import (  # noqa: F401
+    PauliFrame, Program, Masks, sample_masks, pftrajectories, pauliframe_, measurements,
+    pftrajectories_record, unpack_record,
+)
+from .tableau import (  # noqa: F401
+    Tableau, PauliOperator, Stabilizer, MixedStabilizer, Destabilizer, MixedDestabilizer, CliffordOperator,
+    P, S, T, tCNOT, tensor_pow, one_destabilizer, one_mixed_destabilizer, random_clifford_ops,
+    mul_left_, mul_left_row_, prodphase, comm, canonicalize_, project_, generate_, apply_, DeviceTableau,
+)
+from . import circuits  # noqa: F401

@@ -1,0 +1,404 @@
+"""Tableaux, Pauli operators and the tableau hot path on the device.
+
+Host objects use the reference layout (src/QuantumClifford.jl:145-151,
+src/pauli_operator.jl:42-48): a row is ``W = 2*ceil(n/64)`` uint64 words, X
+words then Z words; phases are uint8 mod 4 (0: +, 1: +i, 2: -, 3: -i).
+``to_gpu`` moves them into library-owned device tableaux; the in-place
+operations (``mul_left_``, ``canonicalize_``, ``project_``, ``generate_``,
+``apply_``) run only on device objects, through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+import re
+from typing import Optional
+
+import numpy as np
+
+from . import ops as _ops
+from ._lib import check, ensure_init, lib, ptr
+
+KIND = {"Stabilizer": 0, "MixedStabilizer": 1, "Destabilizer": 2, "MixedDestabilizer": 3}
+
+
+def nwords(n: int) -> int:
+    return 2 * ((n + 63) // 64)
+
+
+class DeviceTableau:
+    """Owner of a qcb_tableau handle."""
+
+    def __init__(self, rows: int, nqubits: int):
+        ensure_init()
+        h = ctypes.c_void_p()
+        check(lib().qcb_tableau_create(int(rows), int(nqubits), ctypes.byref(h)))
+        self.handle = h
+        self.rows, self.nqubits, self.W = int(rows), int(nqubits), nwords(nqubits)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            lib().qcb_tableau_destroy(h)
+            self.handle = None
+
+    def upload(self, phases: np.ndarray, xzs: np.ndarray):
+        ph = np.ascontiguousarray(phases, dtype=np.uint8)
+        xz = np.ascontiguousarray(xzs, dtype=np.uint64)
+        assert ph.shape == (self.rows,) and xz.shape == (self.rows, self.W)
+        check(lib().qcb_tableau_upload(self.handle, ptr(ph) if ph.size else None, ptr(xz) if xz.size else None, None))
+
+    def download(self):
+        ph = np.empty(self.rows, dtype=np.uint8)
+        xz = np.empty((self.rows, self.W), dtype=np.uint64)
+        check(lib().qcb_tableau_download(self.handle, ptr(ph) if ph.size else None, ptr(xz) if xz.size else None, None))
+        return ph, xz
+
+
+class Tableau:
+    """Rows of Pauli operators (host numpy arrays, reference layout), optionally
+    mirrored by a device tableau (``self.dev``)."""
+
+    def __init__(self, phases, nqubits: int, xzs):
+        self.phases = np.ascontiguousarray(phases, dtype=np.uint8)
+        self.nqubits = int(nqubits)
+        self.xzs = np.ascontiguousarray(xzs, dtype=np.uint64).reshape(len(self.phases), nwords(nqubits))
+        self.dev: Optional[DeviceTableau] = None
+
+    # ----- construction helpers
+    @classmethod
+    def zeros(cls, rows: int, n: int) -> "Tableau":
+        return cls(np.zeros(rows, np.uint8), n, np.zeros((rows, nwords(n)), np.uint64))
+
+    @classmethod
+    def from_bits(cls, phases, xs: np.ndarray, zs: np.ndarray) -> "Tableau":
+        xs = np.asarray(xs, dtype=bool)
+        zs = np.asarray(zs, dtype=bool)
+        rows, n = xs.shape
+        t = cls.zeros(rows, n)
+        t.phases[:] = np.asarray(phases, dtype=np.uint8) & 3
+        half = nwords(n) // 2
+        for q in range(n):
+            w, b = q >> 6, np.uint64(1 << (q & 63))
+            t.xzs[xs[:, q], w] |= b
+            t.xzs[zs[:, q], half + w] |= b
+        return t
+
+    def bits(self):
+        half = self.xzs.shape[1] // 2
+        q = np.arange(self.nqubits)
+        w, b = q >> 6, (q & 63).astype(np.uint64)
+        xs = ((self.xzs[:, w] >> b) & np.uint64(1)).astype(bool)
+        zs = ((self.xzs[:, half + w] >> b) & np.uint64(1)).astype(bool)
+        return xs, zs
+
+    def __len__(self):
+        return len(self.phases)
+
+    def copy(self) -> "Tableau":
+        t = Tableau(self.phases.copy(), self.nqubits, self.xzs.copy())
+        return t
+
+    def __eq__(self, other) -> bool:
+        return (
+            isinstance(other, Tableau)
+            and self.nqubits == other.nqubits
+            and np.array_equal(self.phases, other.phases)
+            and np.array_equal(self.xzs, other.xzs)
+        )
+
+    def __str__(self) -> str:
+        xs, zs = self.bits()
+        out = []
+        for r in range(len(self)):
+            s = {0: "+ ", 1: "+i", 2: "- ", 3: "-i"}[int(self.phases[r])]
+            s += "".join("_XZY"[int(x) + 2 * int(z)] for x, z in zip(xs[r], zs[r]))
+            out.append(s)
+        return "\n".join(out)
+
+    # ----- device mirror
+    def to_gpu(self) -> "Tableau":
+        if self.dev is None or self.dev.rows != len(self) or self.dev.nqubits != self.nqubits:
+            self.dev = DeviceTableau(len(self), self.nqubits)
+        self.dev.upload(self.phases, self.xzs)
+        return self
+
+    def to_cpu(self) -> "Tableau":
+        if self.dev is not None:
+            self.phases[:], self.xzs[:] = self.dev.download()
+        return self
+
+    def _need_dev(self) -> DeviceTableau:
+        if self.dev is None:
+            raise TypeError("this object lives on the host; call to_gpu() first (libqcb200 has no CPU path)")
+        return self.dev
+
+
+_PAULI_RE = re.compile(r"^\s*([+-]?)\s*(i?)\s*([XYZI_]+)\s*$")
+
+
+def _parse_pauli(s: str):
+    m = _PAULI_RE.match(s)
+    if not m:
+        raise ValueError(f"not a Pauli string: {s!r}")
+    sign, im, body = m.groups()
+    ph = (2 if sign == "-" else 0) + (1 if im else 0)
+    xs = np.array([c in "XY" for c in body], dtype=bool)
+    zs = np.array([c in "ZY" for c in body], dtype=bool)
+    return ph & 3, xs, zs
+
+
+class PauliOperator(Tableau):
+    """A one-row tableau (src/pauli_operator.jl:42-48)."""
+
+    @classmethod
+    def from_str(cls, s: str) -> "PauliOperator":
+        ph, xs, zs = _parse_pauli(s)
+        t = Tableau.from_bits([ph], xs[None, :], zs[None, :])
+        p = cls(t.phases, t.nqubits, t.xzs)
+        return p
+
+    @property
+    def phase(self) -> int:
+        return int(self.phases[0])
+
+    @property
+    def xz(self) -> np.ndarray:
+        return self.xzs[0]
+
+
+def P(s: str) -> PauliOperator:
+    """P"..." string macro."""
+    return PauliOperator.from_str(s)
+
+
+def T(s: str) -> Tableau:
+    """A tableau from whitespace/newline separated Pauli strings (S"..." / T"...")."""
+    parts = re.findall(r"[+-]?\s*i?\s*[XYZI_]+", s)
+    rows = [_parse_pauli(p) for p in parts]
+    n = len(rows[0][1])
+    return Tableau.from_bits([r[0] for r in rows], np.stack([r[1] for r in rows]), np.stack([r[2] for r in rows]))
+
+
+class Stabilizer:
+    """Stabilizer / MixedStabilizer / Destabilizer / MixedDestabilizer wrapper:
+    a tableau plus the kind (and rank for the mixed kinds)."""
+
+    kind = "Stabilizer"
+
+    def __init__(self, tab: Tableau, rank: Optional[int] = None):
+        self.tab = tab
+        self.rank = rank
+
+    def to_gpu(self):
+        self.tab.to_gpu()
+        return self
+
+    def to_cpu(self):
+        self.tab.to_cpu()
+        return self
+
+    def copy(self):
+        return type(self)(self.tab.copy(), self.rank)
+
+    @property
+    def nqubits(self) -> int:
+        return self.tab.nqubits
+
+    def __eq__(self, other):
+        return type(self) is type(other) and self.tab == other.tab and self.rank == other.rank
+
+    def __str__(self):
+        return str(self.tab)
+
+
+class MixedStabilizer(Stabilizer):
+    kind = "MixedStabilizer"
+
+
+class Destabilizer(Stabilizer):
+    kind = "Destabilizer"
+
+
+class MixedDestabilizer(Stabilizer):
+    kind = "MixedDestabilizer"
+
+
+def S(s: str) -> Stabilizer:
+    return Stabilizer(T(s))
+
+
+def one_destabilizer(n: int) -> Destabilizer:
+    """one(Destabilizer, n): destabilizers X_i, stabilizers Z_i."""
+    xs = np.vstack([np.eye(n, dtype=bool), np.zeros((n, n), bool)])
+    zs = np.vstack([np.zeros((n, n), bool), np.eye(n, dtype=bool)])
+    return Destabilizer(Tableau.from_bits(np.zeros(2 * n), xs, zs))
+
+
+def one_mixed_destabilizer(r: int, n: int) -> MixedDestabilizer:
+    """one(MixedDestabilizer, r, n): X_i destabs / logical X, Z_i stabs / logical Z."""
+    d = one_destabilizer(n)
+    return MixedDestabilizer(d.tab, r)
+
+
+def random_clifford_ops(n: int, depth: int, rng: np.random.Generator) -> list:
+    """A random circuit of H, S and CNOT layers (used to make random states;
+    the reference draws uniform Cliffords with Bravyi-Maslov, src/randoms.jl)."""
+    ops = []
+    for _ in range(depth):
+        for q in range(1, n + 1):
+            g = rng.integers(0, 3)
+            if g == 0:
+                ops.append(_ops.sHadamard(q))
+            elif g == 1:
+                ops.append(_ops.sPhase(q))
+        perm = rng.permutation(n) + 1
+        for k in range(0, n - 1, 2):
+            ops.append(_ops.sCNOT(int(perm[k]), int(perm[k + 1])))
+    return ops
+
+
+# ------------------------------------------------------------------ hot path
+def _tab(x) -> Tableau:
+    return x.tab if isinstance(x, Stabilizer) else x
+
+
+def mul_left_(r, l, *, phases: bool = True):
+    """mul_left!(r, l): r <- l * r for device PauliOperators
+    (src/mul_leftright.jl:137-142).  Returns r."""
+    rt, lt = _tab(r), _tab(l)
+    ph = ctypes.c_uint8()
+    check(lib().qcb_mul_left_pauli(rt._need_dev().handle, lt._need_dev().handle, int(phases), ctypes.byref(ph), None))
+    rt.phases[0] = ph.value if phases else rt.phases[0]
+    return r
+
+
+def mul_left_row_(s, m: int, i: int, *, phases: bool = True):
+    """mul_left!(s::Tableau, m, i) (1-based rows)."""
+    check(lib().qcb_mul_left_row(_tab(s)._need_dev().handle, int(m), int(i), int(phases), None))
+    return s
+
+
+def prodphase(l, r, i: int = 1, j: int = 1) -> int:
+    out = ctypes.c_uint8()
+    check(lib().qcb_prodphase(_tab(l)._need_dev().handle, i, _tab(r)._need_dev().handle, j, ctypes.byref(out), None))
+    return out.value
+
+
+def comm(l, r, i: int = 1, j: int = 1) -> int:
+    out = ctypes.c_uint8()
+    check(lib().qcb_comm(_tab(l)._need_dev().handle, i, _tab(r)._need_dev().handle, j, ctypes.byref(out), None))
+    return out.value
+
+
+def canonicalize_(state, *, phases: bool = True, ranks: bool = False):
+    """canonicalize!(state; phases, ranks) (src/canonicalization.jl:92-133) on
+    the stabilizer view of a device state."""
+    t = _tab(state)
+    dev = t._need_dev()
+    rows = len(t)
+    row0 = 1
+    if isinstance(state, (Destabilizer, MixedDestabilizer)):
+        n = rows // 2
+        row0, rows = n + 1, (state.rank if isinstance(state, MixedDestabilizer) else n)
+    elif isinstance(state, MixedStabilizer):
+        rows = state.rank
+    rx, rz = ctypes.c_int32(), ctypes.c_int32()
+    check(lib().qcb_canonicalize(dev.handle, row0, rows, int(phases), ctypes.byref(rx), ctypes.byref(rz), None))
+    if ranks:
+        return state, rx.value, rz.value
+    return state
+
+
+def project_(state, paulis, *, keep_result: bool = True, phases: bool = True):
+    """project!(state, pauli; keep_result, phases) (src/project_trace_reset.jl:231-439).
+
+    ``paulis``: one PauliOperator or a device Tableau of k Paulis projected in
+    order.  Returns (state, anticom, result) with result None for `nothing`
+    (lists when k > 1)."""
+    t = _tab(state)
+    dev = t._need_dev()
+    single = isinstance(paulis, PauliOperator)
+    pt = _tab(paulis)
+    if pt.dev is None:
+        pt.to_gpu()
+    k = len(pt)
+    kind = KIND[state.kind if isinstance(state, Stabilizer) else "Stabilizer"]
+    rank = ctypes.c_int32(state.rank if getattr(state, "rank", None) is not None else 0)
+    anti = np.zeros(k, dtype=np.int32)
+    res = np.zeros(k, dtype=np.int32)
+    done = ctypes.c_uint32()
+    check(lib().qcb_project(dev.handle, kind, ctypes.byref(rank), pt.dev.handle, int(keep_result), int(phases),
+                            ptr(anti), ptr(res), ctypes.byref(done), None))
+    if isinstance(state, (MixedStabilizer, MixedDestabilizer)):
+        state.rank = rank.value
+    results = [None if v < 0 else int(v) for v in res]
+    if single:
+        return state, int(anti[0]), results[0]
+    return state, [int(a) for a in anti], results
+
+
+def generate_(pauli: PauliOperator, stab, *, phases: bool = True, saveindices: bool = True):
+    """generate!(pauli, stabilizer) (src/project_trace_reset.jl:37-81) on device
+    objects.  Returns None (nothing) or (pauli, used_indices)."""
+    ok = ctypes.c_int32()
+    cap = len(_tab(stab))
+    used = np.zeros(max(cap, 1), dtype=np.int32)
+    nu = ctypes.c_uint32()
+    check(lib().qcb_generate(pauli._need_dev().handle, _tab(stab)._need_dev().handle, int(phases), ctypes.byref(ok),
+                             ptr(used), cap, ctypes.byref(nu), None))
+    if not ok.value:
+        return None
+    pauli.to_cpu()
+    return (pauli, [int(u) for u in used[: nu.value]]) if saveindices else pauli
+
+
+def apply_(state, op, *, phases: bool = True):
+    """apply!(state, gate) for symbolic gates / gate lists, or dense
+    apply!(state, c::CliffordOperator) when ``op`` is a CliffordOperator."""
+    t = _tab(state)
+    dev = t._need_dev()
+    if isinstance(op, CliffordOperator):
+        if op.tab.dev is None:
+            op.tab.to_gpu()
+        check(lib().qcb_apply_dense(dev.handle, op.tab.dev.handle, int(phases), None))
+        return state
+    arr = _ops.to_array([op] if isinstance(op, _ops.Op) else op)
+    check(lib().qcb_apply_gates(dev.handle, ptr(arr), len(arr), int(phases), None))
+    return state
+
+
+class CliffordOperator:
+    """Dense Clifford operator: a 2n-row tableau of the images of
+    X_1..X_n, Z_1..Z_n (src/dense_cliffords.jl:42-56)."""
+
+    def __init__(self, tab: Tableau):
+        assert len(tab) == 2 * tab.nqubits
+        self.tab = tab
+
+    def to_gpu(self):
+        self.tab.to_gpu()
+        return self
+
+
+def tCNOT() -> CliffordOperator:
+    """C"XX IX ZI ZZ" (src/dense_cliffords.jl:222-244)."""
+    return CliffordOperator(T("XX IX ZI ZZ"))
+
+
+def tensor_pow(c: CliffordOperator, k: int) -> CliffordOperator:
+    """tensor_pow (src/linalg.jl:303-309): k copies of c on disjoint qubits."""
+    m = c.tab.nqubits
+    n = m * k
+    xs0, zs0 = c.tab.bits()
+    xs = np.zeros((2 * n, n), bool)
+    zs = np.zeros((2 * n, n), bool)
+    ph = np.zeros(2 * n, np.uint8)
+    for b in range(k):
+        for r in range(m):
+            for half in range(2):
+                src = half * m + r
+                dst = half * n + b * m + r
+                xs[dst, b * m:(b + 1) * m] = xs0[src]
+                zs[dst, b * m:(b + 1) * m] = zs0[src]
+                ph[dst] = c.tab.phases[src]
+    return CliffordOperator(Tableau.from_bits(ph, xs, zs))

@@ -1,0 +1,217 @@
+"""GPU parity tests for the Pauli-frame engine (through the C ABI).
+
+Bit-exact against the CPU oracle:
+  * mask mode (shared seeded event file) against the reference-structured
+    restatement: record and final frame (coding bits; reference padding bits
+    are random and are not compared);
+  * Philox mode against the oracle's restatement of the device procedure.
+Statistical: Philox mode against the reference-structured per-frame draws,
+per-detector rates within 5 sigma.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import qcb200
+from qcb200 import circuits, ops as O
+
+pytestmark = pytest.mark.gpu
+
+
+def coding(xzs, nq1):
+    return xzs & oracle.coding_mask(nq1)[:, None]
+
+
+def run_mask(qcb, circ, frames, seed=0, qubits=None, nbits=None):
+    arr = O.to_array(circ)
+    qmax, bmax = O.affected_counts(arr)
+    qubits = qubits or qmax
+    nbits = nbits or bmax
+    masks = qcb.sample_masks(arr, frames, qubits=qubits, seed=seed)
+    f = qcb.PauliFrame(frames, qubits, nbits, masks=masks)
+    qcb.pftrajectories(f, arr, masks=masks)
+    ox, om = oracle.pftrajectories_mask(arr, frames, qubits, nbits, masks.init_z, masks.reset_planes, masks.events)
+    return f, ox, om
+
+
+def test_device_philox_matches_oracle(qcb):
+    import ctypes
+
+    for ctr, key in [([0, 0, 0, 0], [0, 0]), ([1, 2, 3, 4], [5, 6]), ([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2)]:
+        c = (ctypes.c_uint32 * 4)(*ctr)
+        k = (ctypes.c_uint32 * 2)(*key)
+        out = (ctypes.c_uint32 * 4)()
+        qcb.check(qcb.lib().qcb_debug_philox(c, k, out))
+        assert list(out) == list(oracle.philox(ctr, key))
+
+
+@pytest.mark.parametrize("frames", [10_000, 1, 31, 33, 1000])
+def test_repetition_code_mask_mode_bit_exact(qcb, frames):
+    circ = circuits.repetition_code_memory(7, 7, 1e-3 if frames == 10_000 else 0.2)
+    f, ox, om = run_mask(qcb, circ, frames, seed=frames)
+    assert np.array_equal(f.measurements(), om)
+    assert np.array_equal(coding(f.xzs(), 14), coding(ox, 14))
+
+
+def test_surface_code_d11_mask_mode_bit_exact(qcb):
+    circ = circuits.rotated_surface_code_memory(11, 11, 1e-3)
+    f, ox, om = run_mask(qcb, circ, 10_000, seed=5)
+    assert np.array_equal(f.measurements(), om)
+    assert np.array_equal(coding(f.xzs(), 242), coding(ox, 242))
+
+
+def random_circuit(n, length, rng, p=0.05, nbits_start=1):
+    g1 = ["H", "S", "SDAG", "X", "Y", "Z", "SQRTX", "INVSQRTX", "SQRTY", "INVSQRTY", "HXY", "HYZ", "CXYZ", "CZYX", "I"]
+    g2 = ["CNOT", "CPHASE", "SWAP", "ZCX", "ZCY", "ZCZ", "XCX", "XCY", "XCZ", "YCX", "YCY", "YCZ"]
+    c, bit = [], nbits_start
+    for _ in range(length):
+        k = rng.integers(0, 10)
+        q = int(rng.integers(1, n + 1))
+        if k < 3:
+            c.append(O.Op(O.OP[g1[rng.integers(len(g1))]], q))
+        elif k < 6:
+            q2 = int(rng.integers(1, n + 1))
+            if q2 != q:
+                c.append(O.Op(O.OP[g2[rng.integers(len(g2))]], q, q2))
+        elif k == 6:
+            meas = ["MZ", "MRZ", "MX", "MRX"][rng.integers(4)]
+            b = bit if rng.random() < 0.8 else 0
+            c.append(O.Op(O.OP[meas], q, 0, b))
+            bit += 1
+        elif k == 7:
+            c += O.PauliError(q, *(rng.random(3) * p))
+        elif k == 8:
+            q2 = int(rng.integers(1, n + 1))
+            if q2 != q:
+                c += O.NoiseOp(O.DepolarizationNoise(p * 3), (q, q2))
+        else:
+            c += O.NoiseOp(O.DepolarizationNoise(p * 2), (q,))
+    c.append(O.sMZ(1, bit))
+    return c
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_circuits_mask_mode_bit_exact(qcb, seed):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(2, 70))
+    circ = random_circuit(n, 400, rng)
+    frames = int(rng.integers(1, 3000))
+    f, ox, om = run_mask(qcb, circ, frames, seed=seed)
+    assert np.array_equal(f.measurements(), om)
+    assert np.array_equal(coding(f.xzs(), f.qubits + 1), coding(ox, f.qubits + 1))
+
+
+def test_tall_frame_uses_hbm_walker_bit_exact(qcb):
+    # more touched qubits than a shared-memory tile of 64 columns can hold
+    rng = np.random.default_rng(9)
+    circ = random_circuit(1200, 3000, rng, p=0.02)
+    circ += [O.sCNOT(q, q + 1) for q in range(1, 1200, 2)]
+    f, ox, om = run_mask(qcb, circ, 700, seed=9)
+    assert np.array_equal(f.measurements(), om)
+    assert np.array_equal(coding(f.xzs(), f.qubits + 1), coding(ox, f.qubits + 1))
+
+
+@pytest.mark.parametrize("which", ["rep", "surface5", "random"])
+def test_philox_mode_bit_exact_against_oracle_replica(qcb, which):
+    rng = np.random.default_rng(1)
+    if which == "rep":
+        circ, frames = circuits.repetition_code_memory(7, 7, 0.05), 10_000
+    elif which == "surface5":
+        circ, frames = circuits.rotated_surface_code_memory(5, 5, 0.02), 4096
+    else:
+        circ, frames = random_circuit(40, 500, rng, p=0.1), 3000
+    arr = O.to_array(circ)
+    qmax, bmax = O.affected_counts(arr)
+    seed = 0x1234_5678_9ABC
+    f = qcb.pftrajectories(arr, trajectories=frames, seed=seed)
+    ox, om = oracle.pftrajectories_philox(arr, frames, qmax, bmax, seed)
+    assert np.array_equal(f.measurements(), om)
+    assert np.array_equal(coding(f.xzs(), qmax + 1), coding(ox, qmax + 1))
+
+
+def test_shot_offset_shards_compose(qcb):
+    circ = O.to_array(circuits.rotated_surface_code_memory(3, 3, 0.05))
+    qmax, bmax = O.affected_counts(circ)
+    full = qcb.PauliFrame(4096, qmax, bmax, seed=77)
+    qcb.pftrajectories(full, circ, seed=77)
+    parts = []
+    for k in range(2):
+        f = qcb.PauliFrame(2048, qmax, bmax, seed=77, shot_offset=2048 * k)
+        qcb.pftrajectories(f, circ, seed=77)
+        parts.append(f.measurements())
+    assert np.array_equal(full.measurements(), np.vstack(parts))
+
+
+def test_host_call_matches_frame_api(qcb):
+    circ = O.to_array(circuits.rotated_surface_code_memory(5, 5, 1e-2))
+    planes = qcb.pftrajectories_record(circ, 5000, seed=3)
+    f = qcb.pftrajectories(circ, trajectories=5000, seed=3)
+    assert np.array_equal(qcb.unpack_record(planes, 5000), f.measurements())
+    assert np.array_equal(planes, f.record_planes())
+
+
+def test_single_op_apply_equals_program(qcb):
+    rng = np.random.default_rng(3)
+    circ = O.flatten(random_circuit(12, 120, rng))
+    arr = O.to_array(circ)
+    qmax, bmax = O.affected_counts(arr)
+    masks = qcb.sample_masks(arr, 500, qubits=qmax, seed=2)
+    whole = qcb.PauliFrame(500, qmax, bmax, masks=masks)
+    qcb.pftrajectories(whole, arr, masks=masks)
+    step = qcb.PauliFrame(500, qmax, bmax, masks=masks)
+    # apply op by op: remap events and reset planes to each single-op call
+    resets = 0
+    for k, op in enumerate(circ):
+        ev = masks.events[masks.events["op_index"] == k].copy()
+        ev["op_index"] = 0
+        nres = 1 if op.opcode in (O.OP["MRZ"], O.OP["MRX"]) else 0
+        rp = masks.reset_planes[resets:resets + nres]
+        resets += nres
+        step.apply(op, masks=qcb.Masks(masks.init_z, rp, ev))
+    assert np.array_equal(step.measurements(), whole.measurements())
+    x1, z1 = step.planes()
+    x2, z2 = whole.planes()
+    assert np.array_equal(x1, x2) and np.array_equal(z1, z2)
+
+
+def test_reference_layout_roundtrip(qcb):
+    rng = np.random.default_rng(4)
+    frames, qubits = 777, 130
+    wp = 2 * ((qubits + 1 + 63) // 64)
+    xzs = rng.integers(0, 2**63, size=(wp, frames), dtype=np.uint64) & oracle.coding_mask(qubits + 1)[:, None]
+    f = qcb.PauliFrame(frames, qubits, 3, init=False)
+    f.set_xzs(xzs)
+    assert np.array_equal(f.xzs(), xzs)
+
+
+def test_errors_are_reported_like_the_reference(qcb):
+    f = qcb.PauliFrame(64, 3, 2)
+    with pytest.raises(qcb.BoundsError):
+        qcb.pftrajectories(f, [O.sCNOT(1, 5)])  # qubit 5 > 3 + hidden ancilla
+    with pytest.raises(qcb.BoundsError):
+        qcb.pftrajectories(f, [O.sMZ(1, 3)])
+    qcb.pftrajectories(f, [O.sCNOT(1, 4)])  # the hidden ancilla is addressable
+    bad = np.zeros(1, dtype=qcb.EVENT_DTYPE)
+    with pytest.raises(qcb.ArgumentError):
+        qcb.pftrajectories(f, [O.sX(1)], masks=qcb.Masks(np.zeros((4, 2), np.uint32), np.zeros((0, 2), np.uint32), bad))
+
+
+def test_philox_statistics_match_reference_draws(qcb):
+    """Per-detector rates of the d=5 memory circuit at 1e6 shots: Philox mode
+    against the reference-structured per-frame draws, within 5 sigma."""
+    d, frames = 5, 1_000_000
+    circ = O.to_array(circuits.rotated_surface_code_memory(d, d, 5e-3))
+    qmax, bmax = O.affected_counts(circ)
+    planes = qcb.pftrajectories_record(circ, frames, seed=2024)
+    dev = circuits.surface_code_detectors(qcb.unpack_record(planes, frames), d)
+    _, om = oracle.pftrajectories_rng(circ, frames, qmax, bmax, seed=99, threads=8)
+    ref = circuits.surface_code_detectors(om, d)
+    p1, p2 = dev.mean(axis=0), ref.mean(axis=0)
+    pbar = (p1 + p2) / 2
+    sigma = np.sqrt(2 * pbar * (1 - pbar) / frames) + 1e-12
+    z = np.abs(p1 - p2) / sigma
+    assert z.max() < 5, (z.max(), p1[:5], p2[:5])
+    assert p1.mean() > 0.005  # the noise is actually there
+    # individual data measurements are uniformly random (initZ! / reset randomisation)
+    rec = qcb.unpack_record(planes[-d * d:], frames)
+    assert abs(rec.mean() - 0.5) < 0.01

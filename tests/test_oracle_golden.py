@@ -1,0 +1,327 @@
+"""Pins the CPU oracle against the reference's own known answers.
+
+Every expected value below is written in the reference's doctests or tests
+(file:line cited per case) or follows from its definitions; the pure-Python
+restatement in tests/refpy.py (a different phase method) cross-checks the
+rest on random inputs.
+"""
+import numpy as np
+import pytest
+
+import refpy
+from qcb200 import P, S, T, ops as O
+from qcb200.tableau import Tableau, nwords, one_destabilizer, random_clifford_ops
+
+
+def tab_args(t):
+    t = t.tab if hasattr(t, "tab") else t
+    return t.phases.copy(), t.xzs.copy(), t.nqubits
+
+
+def as_tab(ph, xzs, n):
+    return Tableau(ph, n, xzs)
+
+
+def test_philox_known_answers(orc):
+    # Random123 known-answer vectors for Philox-4x32-10
+    assert list(orc.philox([0, 0, 0, 0], [0, 0])) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert list(orc.philox([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2)) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    assert list(orc.philox([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0])) == [
+        0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+def test_prodphase_and_comm_doctests(orc):
+    # src/QuantumClifford.jl:712-721
+    zzz, xxx = P("ZZZ"), P("XXX")
+    assert orc.prodphase(zzz.xz, 0, xxx.xz, 0) == 3
+    assert orc.prodphase(xxx.xz, 0, zzz.xz, 0) == 1
+    # test/test_paulis.jl:40
+    assert orc.prodphase(P("XX").xz, 0, P("YY").xz, 0) == 2
+    # src/QuantumClifford.jl:776-787 (comm doctest); test/test_paulis.jl:38-39
+    assert orc.comm(P("ZZ").xz, P("XX").xz) == 0
+    assert orc.comm(P("IZ").xz, P("XX").xz) == 1
+    assert orc.comm(P("XX").xz, P("YY").xz) == 0
+    assert orc.comm(P("XZ").xz, P("YZ").xz) == 1
+
+
+def test_pauli_products_doctests(orc):
+    # P"ZZZ"*P"XXX" == -iYYY (src/QuantumClifford.jl:712-715): mul_left!(copy(r), l) = l*r
+    r, ph = orc.mul_left_pauli(P("XXX").xz, 0, P("ZZZ").xz, 0)
+    assert ph == 3 and np.array_equal(r, P("YYY").xz)
+    # P"XX"*P"ZZ" == -YY (src/QuantumClifford.jl:776-779)
+    r, ph = orc.mul_left_pauli(P("ZZ").xz, 0, P("XX").xz, 0)
+    assert ph == 2 and np.array_equal(r, P("YY").xz)
+
+
+def canon(s, phases=True):
+    ph, xz, n = tab_args(s)
+    ph, xz, rx, rz = __import__("oracle").canonicalize(ph, xz, n, phases)
+    return as_tab(ph, xz, n), rx, rz
+
+
+def test_canonicalize_doctests(orc):
+    # src/canonicalization.jl:9-86
+    t, _, _ = canon(S("XXXX ZZII IZZI IIZZ"))
+    assert t == T("+ XXXX + Z__Z + _Z_Z + __ZZ")
+    t, _, _ = canon(S("XXXX IZZI IIZZ"))
+    assert t == T("+ XXXX + _Z_Z + __ZZ")
+    t, _, _ = canon(S("XXXX ZZII IZZI IZIZ IIZZ"))
+    assert t == T("+ XXXX + Z__Z + _Z_Z + __ZZ + ____")
+    s = S("-ZX XZ")
+    t, _, _ = canon(s, phases=False)
+    assert t == T("- XZ + ZX")
+    t, _, _ = canon(s)
+    assert t == T("+ XZ - ZX")
+    t, rx, rz = canon(S("XXXX ZZII IZIZ ZIIZ"))
+    assert (rx, rz) == (1, 3)
+    assert t == T("+ XXXX + Z__Z + _Z_Z + ____")
+
+
+def test_canonicalize_ten_qubit_golden(orc):
+    # test/test_stabcanon.jl:5-26
+    s = S("""- XZZZZ_____
+            - _YZY___YX_
+            - __XXZ__YX_
+            + Z_Z_Y__YXZ
+            + _____Z____
+            + __________
+            + __________
+            + ______YYX_
+            + __________
+            + __________""")
+    want = T("""- XZZZZ_____
+            - _YZY___YX_
+            - __XXZ__YX_
+            + Z_Z_Y__YXZ
+            + ______YYX_
+            + _____Z____
+            + __________
+            + __________
+            + __________
+            + __________""")
+    t, _, _ = canon(s)
+    assert t == want
+
+
+def proj(kind, state, pauli, rank=0, keep_result=True, phases=True):
+    import oracle
+
+    ph, xz, n = tab_args(state)
+    st, ph, xz, rank, a, r = oracle.project(kind, ph, xz, n, pauli.xz, pauli.phase, rank, keep_result, phases)
+    return st, as_tab(ph, xz, n), rank, a, (None if r < 0 else r)
+
+
+def test_project_doctests(orc):
+    # src/project_trace_reset.jl:110-137
+    ghz, _, _ = canon(S("XXXX ZZII IZZI IIZZ"))
+    st, t, _, a, r = proj("Stabilizer", ghz, P("ZIII"))
+    assert t == T("+ Z___ + Z__Z + _Z_Z + __ZZ") and (a, r) == (1, None)
+    t2, _, _ = canon(t)
+    assert t2 == T("Z___ _Z__ __Z_ ___Z")
+    # :139-160
+    s, _, _ = canon(S("ZII IXI IIY"))
+    assert s == T("+ _X_ + __Y + Z__")
+    st, t, _, a, r = proj("Stabilizer", s, P("-ZII"))
+    assert t == T("+ _X_ + __Y + Z__") and (a, r) == (0, 2)
+    # :162-178: incomplete tableau, projector not generated -> anticom = rank + 1
+    st, t, _, a, r = proj("Stabilizer", S("XZI IZI"), P("IIX"))
+    assert t == T("+ X__ + _Z_") and (a, r) == (3, None)
+    # :186-197  one(MixedStabilizer, 2, 3)
+    ms = T("Z__ _Z_ __Z")
+    st, t, rank, a, r = proj("MixedStabilizer", ms, P("IIX"), rank=2)
+    assert rank == 3 and a == 3 and r is None
+    assert as_tab(t.phases[:3], t.xzs[:3], 3) == T("+ Z__ + _Z_ + __X")
+    # :199-225  one(MixedDestabilizer, 2, 3)
+    md = one_destabilizer(3).tab
+    st, t, rank, a, r = proj("MixedDestabilizer", md, P("IIX"), rank=2)
+    assert rank == 3 and a == 3 and r is None
+    assert as_tab(t.phases[:3], t.xzs[:3], 3) == T("+ X__ + _X_ + __Z")
+    assert as_tab(t.phases[3:], t.xzs[3:], 3) == T("+ Z__ + _Z_ + __X")
+
+
+def test_projection_tests(orc):
+    # test/test_projections.jl:9-25
+    s = S("XXX ZZI IZZ")
+    st, t, _, a, r = proj("Stabilizer", s, P("ZII"))
+    t2, _, _ = canon(t)
+    assert a == 1 and r is None and t2 == T("ZII IZI IIZ")
+    st, t, _, a, r = proj("Stabilizer", s, P("-XXX"))
+    c, _, _ = canon(s)
+    assert a == 0 and r == 2 and t == c
+    st, t, _, a, r = proj("Stabilizer", s, P("-XXX"), keep_result=False)
+    assert a == 0 and r is None and t == s.tab
+    # test/test_projections.jl:66-96 (Stabilizer and MixedStabilizer parts)
+    s = S(" XXX -ZZI")
+    st, t, _, a, r = proj("Stabilizer", s, P("IZZ"))
+    assert a == 3 and r is None
+    big = Tableau.zeros(3, 3)
+    big.phases[:2], big.xzs[:2] = s.tab.phases, s.tab.xzs
+    st, t, rank, a, r = proj("MixedStabilizer", big, P("IZZ"), rank=2)
+    assert rank == 3 and a == 3 and r is None
+    st, t, _, a, r = proj("Stabilizer", s, P("ZZI"))
+    assert a == 0 and r == 2
+    st, t, rank, a, r = proj("MixedStabilizer", big, P("ZZI"), rank=2)
+    assert rank == 2 and a == 0 and r == 2
+
+
+def test_generate_doctests(orc):
+    import oracle
+
+    # src/project_trace_reset.jl:10-35
+    ghz, _, _ = canon(S("XXXX ZZII IZZI IIZZ"))
+    p = P("-ZIZI")
+    ok, rest, ph, used = oracle.generate(p.xz, p.phase, ghz.phases, ghz.xzs, 4)
+    assert ok and not rest.any() and ph == 2 and used == [2, 4]
+    c, _, _ = canon(S("ZII"))
+    assert not oracle.generate(P("XII").xz, 0, c.phases, c.xzs, 3)[0]
+    c, _, _ = canon(S("XII"))
+    assert oracle.generate(P("XII").xz, 0, c.phases, c.xzs, 3)[0]
+
+
+def test_dense_tcnot_doctest(orc):
+    import oracle
+
+    # src/dense_cliffords.jl:4-22: tCNOT * S"XI IZ" == S"XX ZZ"
+    c = T("XX IX ZI ZZ")
+    s = T("XI IZ")
+    ph, xz = oracle.apply_dense(s.phases, s.xzs, 2, c.phases, c.xzs)
+    assert as_tab(ph, xz, 2) == T("+ XX + ZZ")
+
+
+def _to_py(t):
+    xs, zs = t.bits()
+    return [(int(t.phases[r]), [int(v) for v in xs[r]], [int(v) for v in zs[r]]) for r in range(len(t))]
+
+
+def _from_py(rows, n):
+    import numpy as np
+
+    return Tableau.from_bits([r[0] for r in rows], np.array([r[1] for r in rows], bool).reshape(len(rows), n),
+                             np.array([r[2] for r in rows], bool).reshape(len(rows), n))
+
+
+@pytest.mark.parametrize("n", [1, 2, 10, 63, 64, 65, 127, 128, 129])
+def test_mul_left_against_table_method(orc, n):
+    import oracle
+
+    rng = np.random.default_rng(n)
+    for _ in range(10):
+        a = Tableau.from_bits(rng.integers(0, 4, 1), rng.random((1, n)) < 0.5, rng.random((1, n)) < 0.5)
+        b = Tableau.from_bits(rng.integers(0, 4, 1), rng.random((1, n)) < 0.5, rng.random((1, n)) < 0.5)
+        r, ph = oracle.mul_left_pauli(b.xzs[0], b.phases[0], a.xzs[0], a.phases[0])
+        want = refpy.mul(_to_py(a)[0], _to_py(b)[0])
+        got = _to_py(as_tab([ph], r[None, :], n))[0]
+        assert got == (want[0], want[1], want[2])
+        assert oracle.comm(a.xzs[0], b.xzs[0]) == refpy.comm(_to_py(a)[0], _to_py(b)[0])
+        # prodphase is the phase of the product
+        assert oracle.prodphase(a.xzs[0], a.phases[0], b.xzs[0], b.phases[0]) == want[0]
+
+
+def random_stabilizer_tab(n, rng, depth=None):
+    d = one_destabilizer(n)
+    ops = O.to_array(random_clifford_ops(n, depth or max(4, n // 2), rng))
+    import oracle
+
+    ph, xz = oracle.apply_gates(d.tab.phases, d.tab.xzs, n, ops)
+    full = as_tab(ph, xz, n)
+    return full, as_tab(ph[n:], xz[n:], n)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 10, 17])
+@pytest.mark.parametrize("phases", [True, False])
+def test_canonicalize_against_table_method(orc, n, phases):
+    rng = np.random.default_rng(100 + n)
+    for rows in (n, max(1, n // 2), n + 2):
+        _, st = random_stabilizer_tab(n, rng)
+        t = Tableau.zeros(rows, n)
+        k = min(rows, n)
+        t.phases[:k], t.xzs[:k] = st.phases[:k], st.xzs[:k]
+        if rows > n:  # redundant rows: products of existing ones
+            for r in range(n, rows):
+                t.xzs[r] = t.xzs[r - n] ^ t.xzs[(r - n + 1) % n]
+        got, rx, rz = canon(t, phases)
+        want, wrx, wrz = refpy.canonicalize(_to_py(t), n, phases)
+        assert (rx, rz) == (wrx, wrz)
+        assert got == _from_py(want, n)
+
+
+GATES1 = ["I", "H", "S", "SDAG", "X", "Y", "Z", "SQRTX", "INVSQRTX", "SQRTY", "INVSQRTY", "HXY", "HYZ", "CXYZ", "CZYX"]
+GATES2 = ["CNOT", "CPHASE", "SWAP", "ZCX", "ZCY", "ZCZ", "XCX", "XCY", "XCZ", "YCX", "YCY", "YCZ"]
+
+
+@pytest.mark.parametrize("gate", GATES1 + GATES2)
+def test_symbolic_gates_match_their_dense_form(orc, gate):
+    """test/test_symcliff.jl:8-60: a symbolic gate and the dense operator built
+    from its action on the generators act identically (phases included)."""
+    import oracle
+
+    n = 3
+    code = O.OP[gate]
+    q = [2, 3] if gate in GATES2 else [2]
+    op = np.zeros(1, dtype=oracle.OP_DTYPE)
+    op[0] = (code, q[0], q[1] if len(q) > 1 else 0, 0, (0, 0, 0))
+    ident = one_destabilizer(n).tab  # rows X_1..X_n, Z_1..Z_n: the images define the operator
+    cph, cxz = oracle.apply_gates(ident.phases, ident.xzs, n, op)
+    rng = np.random.default_rng(7)
+    for _ in range(5):
+        _, st = random_stabilizer_tab(n, rng)
+        st.phases[:] = rng.integers(0, 4, n)
+        a_ph, a_xz = oracle.apply_gates(st.phases, st.xzs, n, op)
+        d_ph, d_xz = oracle.apply_dense(st.phases, st.xzs, n, cph, cxz)
+        assert np.array_equal(a_xz, d_xz)
+        assert np.array_equal(a_ph, d_ph)
+
+
+def test_frame_ghz_correlations(orc):
+    """test/test_pauliframe.jl:30-52: GHZ records have row sums 0 or 3 and
+    mean 1/2."""
+    import oracle
+
+    circ = O.to_array([O.sHadamard(1), O.sCNOT(1, 2), O.sCNOT(1, 3), O.sMZ(1, 1), O.sMZ(2, 2), O.sMZ(3, 3)])
+    n = 200_000
+    _, m = oracle.pftrajectories_rng(circ, n, 3, 3, seed=11, threads=4)
+    tot = m.sum(axis=1)
+    assert np.all(tot % 3 == 0)
+    frac = tot.sum() / 3 / n
+    assert 0.49 < frac < 0.51
+
+
+def test_frame_repetition_syndrome(orc):
+    """test/test_pauliframe.jl:2-27: an X error on qubit 2 flips both syndromes."""
+    import oracle
+
+    circ = O.to_array([O.sX(1), O.sCNOT(1, 2), O.sCNOT(1, 3)] + O.PauliError(2, 0.75) +
+                      [O.sCNOT(1, 4), O.sCNOT(2, 4), O.sCNOT(2, 5), O.sCNOT(3, 5), O.sMZ(4, 1), O.sMZ(5, 2)])
+    xzs, m = oracle.pftrajectories_rng(circ, 100, 5, 2, seed=3)
+    half = xzs.shape[0] // 2
+    for f in range(100):
+        x2 = (xzs[0, f] >> np.uint64(1)) & np.uint64(1)
+        z2 = (xzs[half, f] >> np.uint64(1)) & np.uint64(1)
+        if x2 and not z2:
+            x4 = (xzs[0, f] >> np.uint64(3)) & np.uint64(1)
+            x5 = (xzs[0, f] >> np.uint64(4)) & np.uint64(1)
+            assert x4 and x5 and m[f, 0] and m[f, 1]
+
+
+def test_frame_reset_semantics(orc):
+    """sMRZ records x, clears x and randomises z; sMZ with bit 0 is a no-op;
+    sMX applies sHadamard and does not undo it (src/pauli_frames.jl:74-116)."""
+    import oracle
+
+    S_ = 64
+    circ = O.to_array([O.sX(1), O.sMRZ(1, 1), O.sMZ(1, 2)])
+    init_z = np.zeros((2, 2), np.uint32)
+    reset = np.full((1, 2), 0xFFFFFFFF, np.uint32)
+    ev = np.zeros(0, dtype=oracle.EVENT_DTYPE)
+    xzs, m = oracle.pftrajectories_mask(circ, S_, 1, 2, init_z, reset, ev)
+    # sX does not change frames; record is x = 0; after reset z is all ones
+    assert not m.any()
+    assert np.all(xzs[1] & np.uint64(1))
+    # x error then measurement
+    circ = O.to_array(O.PauliError(1, 1.0, 0, 0) + [O.sMZ(1, 1), O.sMZ(1, 0), O.sMX(1, 2)])
+    ev = np.zeros(S_, dtype=oracle.EVENT_DTYPE)
+    ev["op_index"], ev["pauli"], ev["shot"] = 0, 1, np.arange(S_)
+    xzs, m = oracle.pftrajectories_mask(circ, S_, 1, 2, init_z, np.zeros((0, 2), np.uint32), ev)
+    assert m[:, 0].all() and not m[:, 1].any()
+    # after sMX the H stays applied: x moved to z
+    assert np.all(xzs[1] & np.uint64(1)) and not np.any(xzs[0] & np.uint64(1))

@@ -168,7 +168,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--shots", type=int, default=SHOTS_PER_GPU)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--walker-threads", type=int, default=0)
+    ap.add_argument("--walker-tile", type=int, default=0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -195,8 +195,8 @@ def main():
 
     qcb200.ensure_init(local)
     L = lib()
-    if args.walker_threads:
-        check(L.qcb_tune_set(b"walker_threads", args.walker_threads))
+    if args.walker_tile:
+        check(L.qcb_tune_set(b"walker_tile", args.walker_tile))
     arr = O.to_array(circuits.rotated_surface_code_memory(D, ROUNDS, P_NOISE))
     upd = O.count_updates(arr)
     assert upd == 7601

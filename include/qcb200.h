@@ -202,7 +202,7 @@ int qcb_pftrajectories_host(const qcb_op* ops, size_t n_ops, uint64_t frames,
 int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t seed,
                              uint64_t shot_offset, void* stream);
 
-/* Launch-shape overrides used by the tuner ("walker_threads",
+/* Launch-shape overrides used by the tuner ("walker_tile",
  * "canon_cluster", "project_cluster"); 0 restores the automatic choice.    */
 int qcb_tune_set(const char* key, int64_t value);
 
@@ -278,6 +278,14 @@ int qcb_apply_dense(qcb_tableau* t, const qcb_tableau* c, int phases, void* stre
 /* ------------------------------------------------------------ diagnostics */
 /* Philox-4x32-10 block (counter, key) -> out, computed on the device.       */
 int qcb_debug_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+/* Compile on the host only (no device needed) and copy out the device
+ * program: the record stream (uint32 words), the noise-site table (64 bytes
+ * per site), and per slot the frame qubit and the final x<->z relabel flag.
+ * Buffers may be NULL or too small, in which case only the sizes are set.   */
+int qcb_debug_program_dump(const qcb_op* ops, size_t n_ops, uint32_t* stream, size_t stream_cap,
+                           size_t* stream_len, uint8_t* sites, size_t sites_cap, size_t* n_sites,
+                           uint32_t* slot_qubit, uint32_t* slot_swap, size_t slots_cap, size_t* n_slots,
+                           qcb_program_info* info);
 
 #ifdef __cplusplus
 }

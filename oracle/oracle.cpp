@@ -702,23 +702,34 @@ static inline void philox_block(u64 seed, u32 idx, u64 col, u32 tag, u32 out[4])
 // Noise-site thresholds, as the program compiler lays them out.
 struct Site { u32 opcode, q1, q2; double t0, t1, t2, peff; };
 
-// Per-column event process: geometric skip over trials t = site*32 + lane at
-// rate pmax, then the event kind from a second uniform scaled by pmax.
-struct ColumnNoise {
-  u64 seed, col; double inv_log1m; double pmax; u32 draw = 0; u64 next_t = 0; double v = 0;
-  bool dead = false;
-  void step(bool first) {
+// Event streams: the noise sites are cut into chunks of NOISE_CHUNK sites;
+// each (chunk g, 32-shot column) has its own counter-based stream over the
+// trials tau = (site - g*CHUNK)*32 + lane, with geometric gaps at rate pmax
+// and the event kind from a second uniform scaled by pmax.
+static const u32 NOISE_CHUNK = 32;
+
+struct Event { u32 site, lane; double v; };
+
+static void chunk_events(u64 seed, u64 col, u32 g, double pmax, double inv_log1m, u32 nsites,
+                         std::vector<Event>& out) {
+  const long long span = (long long)NOISE_CHUNK * 32;
+  long long tau = -1;
+  for (u32 draw = 0;; draw++) {
+    u32 ctr[4] = {draw, (u32)col, g, TAG_NOISE};
+    u32 key[2] = {(u32)seed, (u32)(seed >> 32)};
     u32 o[4];
-    philox_block(seed, draw++, col, TAG_NOISE, o);
+    oracle_philox4x32_10(ctr, key, o);
     u64 u53 = ((u64)o[0] << 21) | (o[1] >> 11);
     double u = ((double)u53 + 0.5) * 0x1.0p-53;
-    double g = pmax >= 1.0 ? 0.0 : std::floor(std::log(u) * inv_log1m);
-    v = (double)o[2] * 0x1.0p-32 * pmax;
-    if (g > 9.0e18) { dead = true; return; }
-    u64 gi = (u64)g;
-    next_t = first ? gi : next_t + 1 + gi;
+    double gap = pmax >= 1.0 ? 0.0 : std::floor(std::log(u) * inv_log1m);
+    if (gap >= (double)span) break;
+    tau += 1 + (long long)gap;
+    if (tau >= span) break;
+    u32 site = g * NOISE_CHUNK + (u32)(tau >> 5);
+    if (site >= nsites) break;
+    out.push_back({site, (u32)(tau & 31), (double)o[2] * 0x1.0p-32 * pmax});
   }
-};
+}
 
 // Returns the Pauli code of the event (0 = thinned away).
 static inline u32 site_code(const Site& s, double v) {
@@ -768,11 +779,16 @@ void oracle_pftrajectories_philox(u64* xzs, u8* meas, u64 S, u32 nq1, u32 nbits,
   double inv_log1m = pmax > 0 && pmax < 1.0 ? 1.0 / std::log1p(-pmax) : 0.0;
   u64 words = (S + 31) / 32;
   u64 col0 = shot_offset / 32;
+  const u32 nsites = (u32)sites.size();
+  const u32 nchunks = (nsites + NOISE_CHUNK - 1) / NOISE_CHUNK;
   for (u64 w = 0; w < words; w++) {
     u64 col = col0 + w;
-    ColumnNoise cn{seed, col, inv_log1m, pmax};
-    bool have_noise = pmax > 0 && !sites.empty();
-    if (have_noise) cn.step(true);
+    // all events of this column, grouped by site
+    std::vector<Event> evs;
+    if (pmax > 0)
+      for (u32 g = 0; g < nchunks; g++) chunk_events(seed, col, g, pmax, inv_log1m, nsites, evs);
+    std::vector<std::vector<const Event*>> by_site(nsites);
+    for (const Event& e : evs) by_site[e.site].push_back(&e);
     u64 f0 = w * 32, f1 = std::min<u64>(S, f0 + 32);
     size_t reset_index = 0;
     u32 rcache[4]; u32 rblock = 0xFFFFFFFFu;
@@ -781,23 +797,18 @@ void oracle_pftrajectories_philox(u64* xzs, u8* meas, u64 S, u32 nq1, u32 nbits,
       u32 oc = op.opcode;
       if (is_noise(oc)) {
         long s = site_of_op[k];
-        // events of this site in this column (trials s*32 .. s*32+31)
-        while (have_noise && !cn.dead && cn.next_t < (u64)(s + 1) * 32) {
-          if (cn.next_t >= (u64)s * 32) {
-            u32 lane = (u32)(cn.next_t & 31);
-            u64 f = f0 + lane;
-            u32 code = site_code(sites[(size_t)s], cn.v);
-            if (code && f < f1) {
-              const Site& st = sites[(size_t)s];
-              if (st.opcode == QCB_OP_DEPOL2) {
-                frame_flip(F, st.q1, f, code & 3);
-                frame_flip(F, st.q2, f, (code >> 2) & 3);
-              } else {
-                frame_flip(F, st.q1, f, code & 3);
-              }
+        for (const Event* e : by_site[(size_t)s]) {
+          u64 f = f0 + e->lane;
+          u32 code = site_code(sites[(size_t)s], e->v);
+          if (code && f < f1) {
+            const Site& st = sites[(size_t)s];
+            if (st.opcode == QCB_OP_DEPOL2) {
+              frame_flip(F, st.q1, f, code & 3);
+              frame_flip(F, st.q2, f, (code >> 2) & 3);
+            } else {
+              frame_flip(F, st.q1, f, code & 3);
             }
           }
-          cn.step(false);
         }
         continue;
       }

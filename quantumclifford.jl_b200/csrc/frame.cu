@@ -38,10 +38,11 @@ struct WalkArgs {
   uint64_t pitch;
   uint64_t ncols;
   const uint32_t* slot_qubit;
+  const uint32_t* slot_swap;
   uint32_t nslots;
-  uint32_t scratch_plane;  // qubit index of the scratch plane pair
   uint32_t nq1;
   uint32_t fresh;          // 1: start from x = 0, z = Philox initZ!
+  uint32_t tile;           // shot columns per tile (multiple of 32)
   const uint32_t* qubit_slot;
   uint32_t qubit_slot_len;
   uint32_t nsites;
@@ -57,51 +58,6 @@ struct WalkArgs {
   uint64_t reset_pitch;
 };
 
-// Column storage: shared memory tile or HBM planes.
-struct SmemCol {
-  uint32_t* b;   // sm + tid
-  uint32_t nt;
-  __device__ __forceinline__ uint32_t& x(uint32_t s) const { return b[(2 * s) * nt]; }
-  __device__ __forceinline__ uint32_t& z(uint32_t s) const { return b[(2 * s + 1) * nt]; }
-};
-struct GlobCol {
-  uint32_t* b;   // planes + c
-  const uint32_t* po;  // slot -> plane pair (shared memory table)
-  uint64_t p;
-  __device__ __forceinline__ uint32_t& x(uint32_t s) const { return b[(uint64_t)(2 * po[s]) * p]; }
-  __device__ __forceinline__ uint32_t& z(uint32_t s) const { return b[(uint64_t)(2 * po[s] + 1) * p]; }
-};
-
-__device__ __forceinline__ uint32_t sel4(const uint32_t o[4], uint32_t i) {
-  uint32_t a = (i & 1) ? o[1] : o[0];
-  uint32_t b = (i & 1) ? o[3] : o[2];
-  return (i & 2) ? b : a;
-}
-
-struct NoiseState {
-  uint64_t t;
-  double v;
-  uint32_t draw;
-  bool alive;
-};
-
-__device__ __forceinline__ void noise_step(NoiseState& ns, const WalkArgs& a, uint64_t col,
-                                           bool first) {
-  uint32_t o[4];
-  philox4x32_10(ns.draw++, (uint32_t)col, (uint32_t)(col >> 32), TAG_NOISE, (uint32_t)a.seed,
-                (uint32_t)(a.seed >> 32), o);
-  uint64_t u53 = ((uint64_t)o[0] << 21) | (o[1] >> 11);
-  double u = __dmul_rn(__dadd_rn((double)u53, 0.5), 0x1.0p-53);
-  double g = a.pmax >= 1.0 ? 0.0 : floor(__dmul_rn(log(u), a.inv_log1m));
-  ns.v = __dmul_rn(__dmul_rn((double)o[2], 0x1.0p-32), a.pmax);
-  if (g > 9.0e18) {
-    ns.alive = false;
-    return;
-  }
-  uint64_t gi = (uint64_t)g;
-  ns.t = first ? gi : ns.t + 1 + gi;
-}
-
 __device__ __forceinline__ uint32_t site_code(const Site& s, double v) {
   if (s.kind == QCB_OP_PAULI_NOISE) {
     if (v < s.t0) return 1;
@@ -109,7 +65,7 @@ __device__ __forceinline__ uint32_t site_code(const Site& s, double v) {
     if (v < s.t2) return 3;
     return 0;
   }
-  uint32_t np = s.kind == QCB_OP_DEPOL2 ? 15u : 3u;
+  const uint32_t np = s.kind == QCB_OP_DEPOL2 ? 15u : 3u;
   if (v < s.t0) {
     uint32_t k = (uint32_t)(__dmul_rn(v / s.t0, (double)np));
     if (k >= np) k = np - 1;
@@ -118,31 +74,14 @@ __device__ __forceinline__ uint32_t site_code(const Site& s, double v) {
   return 0;
 }
 
-template <class Col>
-__device__ __forceinline__ void flip(const Col& C, uint32_t s, uint32_t digit, uint32_t bit) {
-  if (digit & 1) C.x(s) ^= bit;
-  if (digit & 2) C.z(s) ^= bit;
-}
-
-template <class Col>
-__device__ __forceinline__ void apply_event(const Col& C, const Site& s, uint32_t code,
-                                            uint32_t bit) {
-  if (s.kind == QCB_OP_DEPOL2) {
-    flip(C, s.a, code & 3, bit);
-    flip(C, s.b, (code >> 2) & 3, bit);
-  } else {
-    flip(C, s.a, code & 3, bit);
-  }
-}
-
-// Bit-sliced single-qubit gate (src/symbolic_cliffords.jl:105-118), frames
+// Bit-sliced single-qubit gate (src/symbolic_cliffords.jl:105-118); frames
 // track no phase (src/pauli_frames.jl:58-61).
 __device__ __forceinline__ void gate1_xz(uint32_t op, uint32_t& x, uint32_t& z) {
-  uint32_t X = x, Z = z;
+  const uint32_t X = x, Z = z;
   switch (op) {
     case QCB_OP_H: case QCB_OP_SQRTY: case QCB_OP_INVSQRTY: x = Z; z = X; break;
-    case QCB_OP_HXY: case QCB_OP_S: case QCB_OP_SDAG: x = X; z = X ^ Z; break;
-    case QCB_OP_HYZ: case QCB_OP_SQRTX: case QCB_OP_INVSQRTX: x = X ^ Z; z = Z; break;
+    case QCB_OP_HXY: case QCB_OP_S: case QCB_OP_SDAG: z = X ^ Z; break;
+    case QCB_OP_HYZ: case QCB_OP_SQRTX: case QCB_OP_INVSQRTX: x = X ^ Z; break;
     case QCB_OP_CXYZ: x = X ^ Z; z = X; break;
     case QCB_OP_CZYX: x = Z; z = X ^ Z; break;
     default: break;  // I, X, Y, Z: no change to the frame bits
@@ -152,7 +91,7 @@ __device__ __forceinline__ void gate1_xz(uint32_t op, uint32_t& x, uint32_t& z) 
 // Bit-sliced two-qubit gate maps (src/symbolic_cliffords.jl:358-395).
 __device__ __forceinline__ void gate2_xz(uint32_t op, uint32_t& x1, uint32_t& z1, uint32_t& x2,
                                          uint32_t& z2) {
-  uint32_t a = x1, b = z1, c = x2, d = z2;
+  const uint32_t a = x1, b = z1, c = x2, d = z2;
   switch (op) {
     case QCB_OP_SWAP: x1 = c; z1 = d; x2 = a; z2 = b; break;
     case QCB_OP_CNOT: case QCB_OP_ZCX: z1 = b ^ d; x2 = c ^ a; break;
@@ -168,223 +107,294 @@ __device__ __forceinline__ void gate2_xz(uint32_t op, uint32_t& x1, uint32_t& z1
   }
 }
 
-template <class Col, bool PHILOX>
-__device__ __forceinline__ void walk_column(const WalkArgs& a, const Col& C, uint64_t c) {
-  const uint64_t col = a.col0 + c;
-  const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
-  const uint32_t clo = (uint32_t)col, chi = (uint32_t)(col >> 32);
-  uint32_t* rec = a.rec + c;
-  const uint64_t pitch = a.pitch;
-
-  NoiseState ns{0, 0.0, 0, false};
-  uint64_t ep = 0, ee = 0;
-  if (PHILOX) {
-    if (a.nsites && a.pmax > 0.0) {
-      ns.alive = true;
-      noise_step(ns, a, col, true);
-    }
-  } else {
-    ep = a.ev_off[c];
-    ee = a.ev_off[c + 1];
+// The frame tile.  SMEM: plane p of tile column cl at sm[p*T + cl].
+// Global: plane p maps to frame plane pmap[p] (a shared-memory table).
+template <bool SMEM>
+struct Tile {
+  uint32_t* sm;
+  uint32_t* planes;
+  const uint32_t* pmap;
+  uint64_t pitch;
+  uint32_t T;
+  __device__ __forceinline__ uint32_t* at(uint32_t p, uint32_t cl, uint64_t cg) const {
+    if (SMEM) return sm + p * T + cl;
+    return planes + (uint64_t)pmap[p] * pitch + cg;
   }
-  uint32_t rblk = 0xFFFFFFFFu;
-  uint32_t rc[4] = {0, 0, 0, 0};
+};
 
-  const uint4* pc = a.prog;
-  while (true) {
-    const uint4 h = __ldg(pc++);
-    const uint32_t kind = h.x >> 24, cnt = h.x & 0xFFFFFFu;
-    if (kind == SEG_END) break;
-    switch (kind) {
-      case SEG_CNOT: {
-        for (uint32_t i = 0; i < cnt; i += 4) {
-          const uint4 o0 = __ldg(pc), o1 = __ldg(pc + 1);
-          pc += 2;
-          uint32_t xc0 = C.x(o0.x), zc0 = C.z(o0.x), xt0 = C.x(o0.y), zt0 = C.z(o0.y);
-          uint32_t xc1 = C.x(o0.z), zc1 = C.z(o0.z), xt1 = C.x(o0.w), zt1 = C.z(o0.w);
-          uint32_t xc2 = C.x(o1.x), zc2 = C.z(o1.x), xt2 = C.x(o1.y), zt2 = C.z(o1.y);
-          uint32_t xc3 = C.x(o1.z), zc3 = C.z(o1.z), xt3 = C.x(o1.w), zt3 = C.z(o1.w);
-          C.x(o0.y) = xt0 ^ xc0; C.z(o0.x) = zc0 ^ zt0;
-          C.x(o0.w) = xt1 ^ xc1; C.z(o0.z) = zc1 ^ zt1;
-          C.x(o1.y) = xt2 ^ xc2; C.z(o1.x) = zc2 ^ zt2;
-          C.x(o1.w) = xt3 ^ xc3; C.z(o1.z) = zc3 ^ zt3;
-        }
-        break;
-      }
-      case SEG_CZ: {
-        for (uint32_t i = 0; i < cnt; i += 4) {
-          const uint4 o0 = __ldg(pc), o1 = __ldg(pc + 1);
-          pc += 2;
-          uint32_t xa0 = C.x(o0.x), za0 = C.z(o0.x), xb0 = C.x(o0.y), zb0 = C.z(o0.y);
-          uint32_t xa1 = C.x(o0.z), za1 = C.z(o0.z), xb1 = C.x(o0.w), zb1 = C.z(o0.w);
-          uint32_t xa2 = C.x(o1.x), za2 = C.z(o1.x), xb2 = C.x(o1.y), zb2 = C.z(o1.y);
-          uint32_t xa3 = C.x(o1.z), za3 = C.z(o1.z), xb3 = C.x(o1.w), zb3 = C.z(o1.w);
-          C.z(o0.x) = za0 ^ xb0; C.z(o0.y) = zb0 ^ xa0;
-          C.z(o0.z) = za1 ^ xb1; C.z(o0.w) = zb1 ^ xa1;
-          C.z(o1.x) = za2 ^ xb2; C.z(o1.y) = zb2 ^ xa2;
-          C.z(o1.z) = za3 ^ xb3; C.z(o1.w) = zb3 ^ xa3;
-        }
-        break;
-      }
-      case SEG_H: {
-        for (uint32_t i = 0; i < cnt; i += 4) {
-          const uint4 o = __ldg(pc++);
-          uint32_t x0 = C.x(o.x), z0 = C.z(o.x), x1 = C.x(o.y), z1 = C.z(o.y);
-          uint32_t x2 = C.x(o.z), z2 = C.z(o.z), x3 = C.x(o.w), z3 = C.z(o.w);
-          C.x(o.x) = z0; C.z(o.x) = x0; C.x(o.y) = z1; C.z(o.y) = x1;
-          C.x(o.z) = z2; C.z(o.z) = x2; C.x(o.w) = z3; C.z(o.w) = x3;
-        }
-        break;
-      }
-      case SEG_S: {
-        for (uint32_t i = 0; i < cnt; i += 4) {
-          const uint4 o = __ldg(pc++);
-          uint32_t x0 = C.x(o.x), z0 = C.z(o.x), x1 = C.x(o.y), z1 = C.z(o.y);
-          uint32_t x2 = C.x(o.z), z2 = C.z(o.z), x3 = C.x(o.w), z3 = C.z(o.w);
-          C.z(o.x) = z0 ^ x0; C.z(o.y) = z1 ^ x1; C.z(o.z) = z2 ^ x2; C.z(o.w) = z3 ^ x3;
-        }
-        break;
-      }
-      case SEG_G1: {
-        for (uint32_t i = 0; i < cnt; i += 2) {
-          const uint4 o = __ldg(pc++);
-          uint32_t x0 = C.x(o.y), z0 = C.z(o.y), x1 = C.x(o.w), z1 = C.z(o.w);
-          gate1_xz(o.x, x0, z0);
-          gate1_xz(o.z, x1, z1);
-          C.x(o.y) = x0; C.z(o.y) = z0; C.x(o.w) = x1; C.z(o.w) = z1;
-        }
-        break;
-      }
-      case SEG_G2: {
-        for (uint32_t i = 0; i < cnt; i++) {
-          const uint4 o = __ldg(pc++);
-          uint32_t x1 = C.x(o.y), z1 = C.z(o.y), x2 = C.x(o.z), z2 = C.z(o.z);
-          gate2_xz(o.x, x1, z1, x2, z2);
-          C.x(o.y) = x1; C.z(o.y) = z1; C.x(o.z) = x2; C.z(o.z) = z2;
-        }
-        break;
-      }
-      case SEG_MZ: {
-        for (uint32_t i = 0; i < cnt; i += 2) {
-          const uint4 o = __ldg(pc++);
-          uint32_t x0 = C.x(o.x), x1 = C.x(o.z);
-          if (o.y != BIT_NONE) rec[(uint64_t)o.y * pitch] = x0;
-          if (o.w != BIT_NONE) rec[(uint64_t)o.w * pitch] = x1;
-        }
-        break;
-      }
-      case SEG_MRZ: {
-        for (uint32_t i = 0; i < cnt; i++) {
-          const uint4 o = __ldg(pc++);  // (q, bit, reset index, 0)
-          uint32_t x = C.x(o.x), z = C.z(o.x);
-          uint32_t rb;
-          if (PHILOX) {
-            if ((o.z >> 2) != rblk) {
-              rblk = o.z >> 2;
-              philox4x32_10(rblk, clo, chi, TAG_RESET, k0, k1, rc);
-            }
-            rb = sel4(rc, o.z & 3);
-          } else {
-            rb = a.reset_planes ? __ldg(a.reset_planes + (uint64_t)o.z * a.reset_pitch + c) : 0u;
-          }
-          if (o.y != BIT_NONE) rec[(uint64_t)o.y * pitch] = x;
-          C.x(o.x) = 0u;
-          C.z(o.x) = z ^ rb;
-        }
-        break;
-      }
-      case SEG_FLUSH: {
-        const uint64_t lim = (uint64_t)h.z * 32u;
-        if (PHILOX) {
-          while (ns.alive && ns.t < lim) {
-            const uint32_t site = (uint32_t)(ns.t >> 5);
-            const Site s = a.sites[site];
-            const uint32_t code = site_code(s, ns.v);
-            if (code) apply_event(C, s, code, 1u << (ns.t & 31));
-            noise_step(ns, a, col, false);
-          }
-        } else {
-          while (ep < ee) {
-            const uint64_t d = __ldg(a.ev_data + ep);
-            const uint64_t t = d >> 8;
-            if (t >= lim) break;
-            const Site s = a.sites[(uint32_t)(t >> 5)];
-            apply_event(C, s, (uint32_t)(d & 0xFF), 1u << (t & 31));
-            ep++;
-          }
-        }
-        break;
-      }
-      default:
-        return;
+// One noise stream: sites [g*CH, (g+1)*CH) of one shot column, trials
+// tau = (site - g*CH)*32 + lane, geometric gaps at p_max.  Only the events of
+// sites in [lo, hi) are applied (a stream can straddle two flushes; the
+// counter-based generator lets the second flush replay it from the start).
+template <bool SMEM>
+__device__ __forceinline__ void noise_chunk(const WalkArgs& a, const Tile<SMEM>& F, uint32_t cl, uint64_t cg,
+                                            uint32_t col_lo, uint32_t g, uint32_t lo, uint32_t hi) {
+  const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
+  const int64_t span = (int64_t)NOISE_CHUNK * 32;
+  int64_t tau = -1;
+  for (uint32_t draw = 0;; draw++) {
+    uint32_t o[4];
+    philox4x32_10(draw, col_lo, g, TAG_NOISE, k0, k1, o);
+    const uint64_t u53 = ((uint64_t)o[0] << 21) | (o[1] >> 11);
+    const double u = __dmul_rn(__dadd_rn((double)u53, 0.5), 0x1.0p-53);
+    const double gap = a.pmax >= 1.0 ? 0.0 : floor(__dmul_rn(log(u), a.inv_log1m));
+    if (gap >= (double)span) break;
+    tau += 1 + (int64_t)gap;
+    if (tau >= span) break;
+    const uint32_t site = g * NOISE_CHUNK + (uint32_t)(tau >> 5);
+    if (site >= hi) break;
+    if (site < lo) continue;
+    const double v = __dmul_rn(__dmul_rn((double)o[2], 0x1.0p-32), a.pmax);
+    const Site s = a.sites[site];
+    const uint32_t code = site_code(s, v);
+    if (!code) continue;
+    const uint32_t bit = 1u << (tau & 31);
+    if (code & 1) atomicXor(F.at(s.xa, cl, cg), bit);
+    if (code & 2) atomicXor(F.at(s.za, cl, cg), bit);
+    if (s.kind == QCB_OP_DEPOL2) {
+      if (code & 4) atomicXor(F.at(s.xb, cl, cg), bit);
+      if (code & 8) atomicXor(F.at(s.zb, cl, cg), bit);
     }
   }
 }
 
+// The walker: one CTA owns a tile of T shot columns (T x 32 shots) and runs
+// the whole program on it.  Thread (rr, cl) = (tid / T, tid % T) handles
+// column cl and every R-th op of a segment, so a warp covers 32 columns of one
+// op (conflict-free shared accesses, uniform operand loads); one barrier per
+// segment orders the segments.
 template <bool SMEM, bool PHILOX>
-__global__ void __launch_bounds__(256) walker_kernel(const WalkArgs a) {
+__global__ void __launch_bounds__(1024, 1) walker_kernel(const WalkArgs a) {
   extern __shared__ __align__(16) uint32_t sm[];
-  const uint32_t NT = blockDim.x, tid = threadIdx.x;
+  const uint32_t tid = threadIdx.x, T = a.tile, R = blockDim.x / T;
+  const uint32_t cl = tid % T, rr = tid / T;
+  const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
+  const uint64_t pitch = a.pitch;
   if (!SMEM) {
-    for (uint32_t s = tid; s <= a.nslots; s += NT) sm[s] = s < a.nslots ? a.slot_qubit[s] : a.scratch_plane;
+    for (uint32_t p = tid; p < 2 * a.nslots; p += blockDim.x) sm[p] = 2 * a.slot_qubit[p >> 1] + (p & 1);
     __syncthreads();
   }
-  const uint64_t ntiles = (a.ncols + NT - 1) / NT;
+  const uint64_t ntiles = (a.ncols + T - 1) / T;
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const uint64_t c = tile * NT + tid;
-    if (c >= a.ncols) break;
-    const uint64_t col = a.col0 + c;
-    const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
-    if (SMEM) {
-      SmemCol C{sm + tid, NT};
-      if (a.fresh) {
-        for (uint32_t q = 0; q < a.nq1; q += 4) {
-          uint32_t o[4];
-          philox4x32_10(q >> 2, (uint32_t)col, (uint32_t)(col >> 32), TAG_INITZ, k0, k1, o);
+    const uint64_t c0 = tile * T, cg = c0 + cl;
+    const bool act = rr < R && cg < a.ncols;
+    const uint64_t col = a.col0 + cg;
+    const uint32_t clo = (uint32_t)col, chi = (uint32_t)(col >> 32);
+    const Tile<SMEM> F{sm, a.planes, sm, pitch, T};
+
+    // ---- initial frame
+    if (a.fresh) {
+      for (uint32_t qb = rr; qb * 4 < a.nq1; qb += R) {
+        if (!act) break;
+        uint32_t o[4];
+        philox4x32_10(qb, clo, chi, TAG_INITZ, k0, k1, o);
 #pragma unroll
-          for (uint32_t j = 0; j < 4; j++) {
-            const uint32_t qq = q + j;
-            if (qq >= a.nq1) break;
-            const uint32_t s = qq < a.qubit_slot_len ? __ldg(a.qubit_slot + qq) : BIT_NONE;
-            if (s != BIT_NONE) {
-              C.x(s) = 0u;
-              C.z(s) = o[j];
-            } else {
-              a.planes[(uint64_t)(2 * qq) * a.pitch + c] = 0u;
-              a.planes[(uint64_t)(2 * qq + 1) * a.pitch + c] = o[j];
+        for (uint32_t j = 0; j < 4; j++) {
+          const uint32_t q = qb * 4 + j;
+          if (q >= a.nq1) break;
+          const uint32_t s = (SMEM && q < a.qubit_slot_len) ? __ldg(a.qubit_slot + q) : BIT_NONE;
+          if (SMEM && s != BIT_NONE) {
+            *F.at(2 * s, cl, cg) = 0u;
+            *F.at(2 * s + 1, cl, cg) = o[j];
+          } else {
+            a.planes[(uint64_t)(2 * q) * pitch + cg] = 0u;
+            a.planes[(uint64_t)(2 * q + 1) * pitch + cg] = o[j];
+          }
+        }
+      }
+    } else if (SMEM) {
+      for (uint32_t s = rr; s < a.nslots; s += R) {
+        if (!act) break;
+        const uint32_t q = __ldg(a.slot_qubit + s);
+        *F.at(2 * s, cl, cg) = a.planes[(uint64_t)(2 * q) * pitch + cg];
+        *F.at(2 * s + 1, cl, cg) = a.planes[(uint64_t)(2 * q + 1) * pitch + cg];
+      }
+    }
+    uint64_t ep = 0, ee = 0;
+    if (!PHILOX && rr == 0 && act) {
+      ep = a.ev_off[cg];
+      ee = a.ev_off[cg + 1];
+    }
+    __syncthreads();
+
+    // ---- the program
+    const uint4* pc = a.prog;
+    while (true) {
+      const uint4 h = __ldg(pc++);
+      const uint32_t kind = h.x >> 24, cnt = h.x & 0xFFFFFFu;
+      if (kind == SEG_END) break;
+      switch (kind) {
+        case SEG_CNOT: {
+          const uint4* e = pc;
+          pc += cnt;
+          if (!act) break;
+          uint32_t j = rr;
+          for (; j + R < cnt; j += 2 * R) {
+            const uint4 o = __ldg(e + j), u = __ldg(e + j + R);
+            uint32_t *pxc = F.at(o.x, cl, cg), *pzc = F.at(o.y, cl, cg), *pxt = F.at(o.z, cl, cg), *pzt = F.at(o.w, cl, cg);
+            uint32_t *qxc = F.at(u.x, cl, cg), *qzc = F.at(u.y, cl, cg), *qxt = F.at(u.z, cl, cg), *qzt = F.at(u.w, cl, cg);
+            const uint32_t xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
+            const uint32_t yxc = *qxc, yzc = *qzc, yxt = *qxt, yzt = *qzt;
+            *pxt = xt ^ xc; *pzc = zc ^ zt;
+            *qxt = yxt ^ yxc; *qzc = yzc ^ yzt;
+          }
+          for (; j < cnt; j += R) {
+            const uint4 o = __ldg(e + j);
+            uint32_t *pxc = F.at(o.x, cl, cg), *pzc = F.at(o.y, cl, cg), *pxt = F.at(o.z, cl, cg), *pzt = F.at(o.w, cl, cg);
+            const uint32_t xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
+            *pxt = xt ^ xc; *pzc = zc ^ zt;
+          }
+          break;
+        }
+        case SEG_CZ: {
+          const uint4* e = pc;
+          pc += cnt;
+          if (!act) break;
+          for (uint32_t j = rr; j < cnt; j += R) {
+            const uint4 o = __ldg(e + j);
+            uint32_t *pxa = F.at(o.x, cl, cg), *pza = F.at(o.y, cl, cg), *pxb = F.at(o.z, cl, cg), *pzb = F.at(o.w, cl, cg);
+            const uint32_t xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
+            *pza = za ^ xb; *pzb = zb ^ xa;
+          }
+          break;
+        }
+        case SEG_S:
+        case SEG_G1: {
+          const uint4* e = pc;
+          pc += cnt;
+          if (!act) break;
+          for (uint32_t j = rr; j < cnt; j += R) {
+            const uint4 o = __ldg(e + j);
+            uint32_t *px = F.at(o.x, cl, cg), *pz = F.at(o.y, cl, cg);
+            uint32_t x = *px, z = *pz;
+            if (kind == SEG_S) z ^= x;
+            else gate1_xz(o.z, x, z);
+            *px = x; *pz = z;
+          }
+          break;
+        }
+        case SEG_G2: {
+          const uint4* e = pc;
+          pc += 2 * cnt;
+          if (!act) break;
+          for (uint32_t j = rr; j < cnt; j += R) {
+            const uint4 o = __ldg(e + 2 * j), o2 = __ldg(e + 2 * j + 1);
+            uint32_t *pxa = F.at(o.y, cl, cg), *pza = F.at(o.z, cl, cg), *pxb = F.at(o.w, cl, cg), *pzb = F.at(o2.x, cl, cg);
+            uint32_t xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
+            gate2_xz(o.x, xa, za, xb, zb);
+            *pxa = xa; *pza = za; *pxb = xb; *pzb = zb;
+          }
+          break;
+        }
+        case SEG_MZ: {
+          const uint2* e = (const uint2*)pc;
+          pc += (cnt * 2 + 3) / 4;
+          if (!act) break;
+          for (uint32_t j = rr; j < cnt; j += R) {
+            const uint2 o = __ldg(e + j);
+            a.rec[(uint64_t)o.y * pitch + cg] = *F.at(o.x, cl, cg);
+          }
+          break;
+        }
+        case SEG_MRZ: {
+          const uint4* e = pc;
+          pc += 4 * cnt;
+          if (!act) break;
+          for (uint32_t g = rr; g < cnt; g += R) {
+            uint4 ent[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) ent[i] = __ldg(e + 4 * g + i);
+            uint32_t o[4] = {0, 0, 0, 0};
+            if (PHILOX) {
+              uint32_t blk = 0;
+#pragma unroll
+              for (int i = 0; i < 4; i++)
+                if (ent[i].w != MRZ_PAD) blk = ent[i].w >> 2;
+              philox4x32_10(blk, clo, chi, TAG_RESET, k0, k1, o);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              if (ent[i].w == MRZ_PAD) continue;
+              uint32_t* px = F.at(ent[i].x, cl, cg);
+              uint32_t* pz = F.at(ent[i].y, cl, cg);
+              const uint32_t x = *px, z = *pz;
+              uint32_t rb;
+              if (PHILOX) rb = o[i];
+              else rb = a.reset_planes ? __ldg(a.reset_planes + (uint64_t)ent[i].w * a.reset_pitch + cg) : 0u;
+              if (ent[i].z != BIT_NONE) a.rec[(uint64_t)ent[i].z * pitch + cg] = x;
+              *px = 0u;
+              *pz = z ^ rb;
             }
           }
+          break;
         }
-      } else {
-        for (uint32_t s = 0; s < a.nslots; s++) {
-          const uint32_t q = __ldg(a.slot_qubit + s);
-          C.x(s) = a.planes[(uint64_t)(2 * q) * a.pitch + c];
-          C.z(s) = a.planes[(uint64_t)(2 * q + 1) * a.pitch + c];
-        }
-      }
-      walk_column<SmemCol, PHILOX>(a, C, c);
-      for (uint32_t s = 0; s < a.nslots; s++) {
-        const uint32_t q = __ldg(a.slot_qubit + s);
-        a.planes[(uint64_t)(2 * q) * a.pitch + c] = C.x(s);
-        a.planes[(uint64_t)(2 * q + 1) * a.pitch + c] = C.z(s);
-      }
-    } else {
-      GlobCol C{a.planes + c, sm, a.pitch};
-      if (a.fresh) {
-        for (uint32_t q = 0; q < a.nq1; q += 4) {
-          uint32_t o[4];
-          philox4x32_10(q >> 2, (uint32_t)col, (uint32_t)(col >> 32), TAG_INITZ, k0, k1, o);
-#pragma unroll
-          for (uint32_t j = 0; j < 4; j++) {
-            const uint32_t qq = q + j;
-            if (qq >= a.nq1) break;
-            a.planes[(uint64_t)(2 * qq) * a.pitch + c] = 0u;
-            a.planes[(uint64_t)(2 * qq + 1) * a.pitch + c] = o[j];
+        case SEG_FLUSH: {
+          // cnt runs of site indices (begin, end), two runs per record
+          const uint2* runs = (const uint2*)pc;
+          pc += (cnt + 1) / 2;
+          if (!act) break;
+          if (PHILOX) {
+            if (a.pmax > 0.0) {
+              // (run, chunk) tasks, dealt round-robin over the R threads of a column
+              uint32_t idx = 0;
+              for (uint32_t r = 0; r < cnt; r++) {
+                const uint2 run = __ldg(runs + r);
+                const uint32_t g0 = run.x / NOISE_CHUNK, g1 = (run.y - 1) / NOISE_CHUNK;
+                for (uint32_t g = g0; g <= g1; g++, idx++)
+                  if (idx % R == rr) noise_chunk<SMEM>(a, F, cl, cg, clo, g, run.x, run.y);
+              }
+            }
+          } else if (rr == 0) {
+            // this column's events are sorted by trial; runs are not visited in
+            // site order, so find the first event of each run
+            for (uint32_t r = 0; r < cnt; r++) {
+              const uint2 run = __ldg(runs + r);
+              const uint64_t lo_t = (uint64_t)run.x * 32u, lim = (uint64_t)run.y * 32u;
+              uint64_t lo = ep, hi = ee;
+              while (lo < hi) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if ((__ldg(a.ev_data + mid) >> 8) < lo_t) lo = mid + 1;
+                else hi = mid;
+              }
+              for (uint64_t k = lo; k < ee; k++) {
+                const uint64_t d = __ldg(a.ev_data + k);
+                const uint64_t t = d >> 8;
+                if (t >= lim) break;
+                const Site s = a.sites[(uint32_t)(t >> 5)];
+                const uint32_t code = (uint32_t)(d & 0xFF), bit = 1u << (t & 31);
+                if (code & 1) *F.at(s.xa, cl, cg) ^= bit;
+                if (code & 2) *F.at(s.za, cl, cg) ^= bit;
+                if (s.kind == QCB_OP_DEPOL2) {
+                  if (code & 4) *F.at(s.xb, cl, cg) ^= bit;
+                  if (code & 8) *F.at(s.zb, cl, cg) ^= bit;
+                }
+              }
+            }
           }
+          break;
         }
+        default:
+          break;
       }
-      walk_column<GlobCol, PHILOX>(a, C, c);
+      __syncthreads();
     }
+
+    // ---- write the frame back, undoing the x<->z relabels
+    for (uint32_t s = rr; s < a.nslots; s += R) {
+      if (!act) break;
+      const uint32_t q = __ldg(a.slot_qubit + s), sw = __ldg(a.slot_swap + s);
+      if (SMEM) {
+        a.planes[(uint64_t)(2 * q) * pitch + cg] = *F.at(2 * s + sw, cl, cg);
+        a.planes[(uint64_t)(2 * q + 1) * pitch + cg] = *F.at(2 * s + 1 - sw, cl, cg);
+      } else if (sw) {
+        uint32_t* px = a.planes + (uint64_t)(2 * q) * pitch + cg;
+        uint32_t* pz = a.planes + (uint64_t)(2 * q + 1) * pitch + cg;
+        const uint32_t x = *px, z = *pz;
+        *px = z;
+        *pz = x;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -544,46 +554,56 @@ namespace qcb {
 // qubits of a tile of >= 64 columns fit, else HBM planes).
 struct WalkConfig {
   bool smem;
-  uint32_t nt;
+  uint32_t T;     // tile columns
+  uint32_t nth;   // threads per CTA
   uint32_t grid;
   size_t smem_bytes;
 };
 
-static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f, uint32_t nt_hint) {
+static uint32_t g_tile_override = 0;
+
+// Shared-memory tile when 2 planes x 32 columns of every touched qubit fit,
+// else the same walker on the HBM planes.
+static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   WalkConfig wc{};
-  const size_t per_thread = (size_t)(p->nslots + 1) * 2 * 4;
+  const size_t per_col = (size_t)2 * std::max<uint32_t>(p->nslots, 1) * 4;
   const size_t maxsm = (size_t)device_max_smem_optin();
-  uint32_t nt = 0;
-  for (uint32_t cand = 256; cand >= 64; cand -= 32)
-    if (per_thread * cand <= maxsm) { nt = cand; break; }
-  if (nt_hint && per_thread * nt_hint <= maxsm) nt = nt_hint;
-  if (nt >= 64) {
+  uint32_t T = 0;
+  if (g_tile_override && per_col * g_tile_override <= maxsm) {
+    T = g_tile_override;
+  } else {
+    const uint32_t cands[] = {64, 96, 32};
+    for (uint32_t c : cands)
+      if (per_col * c <= maxsm) { T = c; break; }
+  }
+  if (T) {
     wc.smem = true;
-    wc.nt = nt;
-    wc.smem_bytes = per_thread * nt;
+    wc.T = T;
+    wc.nth = T == 96 ? 768u : 1024u;
+    wc.smem_bytes = per_col * T;
   } else {
     wc.smem = false;
-    wc.nt = 128;
-    wc.smem_bytes = (size_t)(p->nslots + 1) * 4;
+    wc.T = 128;
+    wc.nth = 1024;
+    wc.smem_bytes = (size_t)2 * p->nslots * 4;
   }
-  uint64_t tiles = (f->ncols + wc.nt - 1) / wc.nt;
+  const uint64_t tiles = (f->ncols + wc.T - 1) / wc.T;
   wc.grid = (uint32_t)std::min<uint64_t>(tiles ? tiles : 1, 1u << 30);
   return wc;
 }
 
-static uint32_t g_nt_override = 0;
-
 int launch_walker(qcb_frame* f, const qcb_program* p, WalkArgs& a, bool philox, bool fresh,
                   cudaStream_t st) {
-  WalkConfig wc = walk_config(p, f, g_nt_override);
+  WalkConfig wc = walk_config(p, f);
   a.fresh = fresh ? 1 : 0;
+  a.tile = wc.T;
   if (!f->ncols) return QCB_OK;
   void (*kern)(const WalkArgs);
   if (wc.smem) kern = philox ? walker_kernel<true, true> : walker_kernel<true, false>;
   else kern = philox ? walker_kernel<false, true> : walker_kernel<false, false>;
   if (wc.smem_bytes > 48 * 1024)
     QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wc.smem_bytes));
-  kern<<<wc.grid, wc.nt, wc.smem_bytes, st>>>(a);
+  kern<<<wc.grid, wc.nth, wc.smem_bytes, st>>>(a);
   QCB_LAUNCHED();
   return QCB_OK;
 }
@@ -596,8 +616,8 @@ static void fill_common(WalkArgs& a, qcb_frame* f, const qcb_program* p) {
   a.pitch = f->pitch;
   a.ncols = f->ncols;
   a.slot_qubit = p->d_slot_qubit;
+  a.slot_swap = p->d_slot_swap;
   a.nslots = p->nslots;
-  a.scratch_plane = f->nq1;
   a.nq1 = f->nq1;
   a.qubit_slot = p->d_qubit_slot;
   a.qubit_slot_len = p->qubit_slot_len;
@@ -808,7 +828,7 @@ extern "C" int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* p, uint
 
 // Internal hooks for the batched runner and the tuner.
 namespace qcb {
-void set_walker_nt(uint32_t nt) { g_nt_override = nt; }
+void set_walker_tile(uint32_t t) { g_tile_override = t; }
 int run_program_fresh(qcb_frame* f, const qcb_program* p, uint64_t seed, uint64_t shot_offset,
                       cudaStream_t st) {
   qcb_noise_source n{};

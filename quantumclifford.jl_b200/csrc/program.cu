@@ -2,16 +2,29 @@
 //
 // Replaces the per-op dispatch of pftrajectories(frame, circuit)
 // (src/pauli_frames.jl:234-239) and compactify_circuit (src/sumtypes.jl:190-237).
-// Ops are validated like the Julia constructors (NoZeroQubit, q1 == q2),
-// sMX / sMRX are lowered to sHadamard + sMZ / sMRZ (src/pauli_frames.jl:74-83),
-// and the remaining ops are grouped into segments: runs of one gate kind on
-// pairwise-disjoint qubits, which the walker kernel executes with independent
-// loads in flight.  Noise ops do not break segments; they are collected into
-// a pending set and applied at a FLUSH record placed before the first later
-// op that touches one of their qubits.  Moving a Pauli flip past gates that act
-// on other qubits is exact, so the result equals op-by-op execution.
+//
+//  * Ops are validated like the Julia constructors (NoZeroQubit, q1 == q2).
+//  * sMX / sMRX are lowered to sHadamard + sMZ / sMRZ (src/pauli_frames.jl:74-83).
+//  * Frames carry no phases (src/pauli_frames.jl:58-61), so sX/sY/sZ/sId1 do
+//    nothing and are dropped, and the gates whose frame action is x <-> z
+//    (sHadamard, sSQRTY, sInvSQRTY) cost nothing at run time: the compiler
+//    keeps a per-qubit "swapped" flag and emits every later operand as the
+//    physical plane that currently holds x or z.  The final flags are applied
+//    when the frame is written back.
+//  * The remaining ops are grouped into segments: runs of one kind on
+//    pairwise-disjoint qubits.  Inside a segment all (op, shot column) pairs
+//    are independent, so a thread block executes them in parallel and
+//    synchronises once per segment.
+//  * Noise ops do not break segments.  Their sites (with the planes current
+//    at the noise op) are collected and applied at a FLUSH record placed before
+//    the first later op that reads or writes one of their qubits; moving a
+//    Pauli flip past ops on other qubits (or past a relabelling) is exact.
+//  * Resets are grouped four at a time so that one Philox block serves four
+//    resets of a shot column.
 #include <cmath>
 #include <cstring>
+#include <algorithm>
+#include <unordered_map>
 #include <unordered_set>
 
 #include "qcb_internal.h"
@@ -22,14 +35,20 @@ static bool is1q(uint32_t o) { return o >= QCB_OP_I && o <= QCB_OP_CZYX; }
 static bool is2q(uint32_t o) { return o >= QCB_OP_CNOT && o <= QCB_OP_YCZ; }
 static bool isnoise(uint32_t o) { return o >= QCB_OP_PAULI_NOISE && o <= QCB_OP_DEPOL2; }
 static bool ismeas(uint32_t o) { return o >= QCB_OP_MZ && o <= QCB_OP_MRX; }
+// frame action x <-> z
+static bool is_relabel(uint32_t o) { return o == QCB_OP_H || o == QCB_OP_SQRTY || o == QCB_OP_INVSQRTY; }
+// no frame action
+static bool is_frame_noop(uint32_t o) { return o == QCB_OP_I || o == QCB_OP_X || o == QCB_OP_Y || o == QCB_OP_Z; }
 
 struct LOp {  // lowered op (0-based qubits)
-  uint32_t kind;   // SegKind for gates/measurements; 0 for noise
+  uint32_t kind;   // SegKind; SEG_END marks noise, SEG_H marks a relabel
   uint32_t opcode;
   uint32_t q1, q2;
   uint32_t bit;    // 0-based record row or BIT_NONE
   uint32_t reset;  // reset index (MRZ)
-  int64_t site;    // noise site (noise ops)
+  int64_t site;    // noise site
+  size_t src;      // index in the caller's op array
+  uint32_t xa = 0, za = 0, xb = 0, zb = 0;  // planes, fixed when the op joins a segment
 };
 
 static uint64_t fnv1a(const void* p, size_t n, uint64_t h = 1469598103934665603ull) {
@@ -38,54 +57,14 @@ static uint64_t fnv1a(const void* p, size_t n, uint64_t h = 1469598103934665603u
   return h;
 }
 
-static void emit_segment(std::vector<uint32_t>& out, uint32_t kind, const std::vector<LOp>& ops,
-                         const std::vector<uint32_t>& map, uint32_t scratch) {
-  auto M = [&](uint32_t q) { return map.empty() ? q : map[q]; };
-  uint32_t cnt = (uint32_t)ops.size();
-  out.push_back((kind << 24) | cnt);
-  out.push_back(0); out.push_back(0); out.push_back(0);
-  switch (kind) {
-    case SEG_CNOT: case SEG_CZ: {
-      for (auto& o : ops) { out.push_back(M(o.q1)); out.push_back(M(o.q2)); }
-      // pad with gates on the scratch slot to a multiple of 4 gates
-      for (uint32_t i = cnt; i % 4; i++) { out.push_back(scratch); out.push_back(scratch); }
-      break;
-    }
-    case SEG_H: case SEG_S: {
-      for (auto& o : ops) out.push_back(M(o.q1));
-      for (uint32_t i = cnt; i % 4; i++) out.push_back(scratch);
-      break;
-    }
-    case SEG_G1: {
-      for (auto& o : ops) { out.push_back(o.opcode); out.push_back(M(o.q1)); }
-      for (uint32_t i = cnt; i % 2; i++) { out.push_back(QCB_OP_I); out.push_back(scratch); }
-      break;
-    }
-    case SEG_G2: {
-      for (auto& o : ops) {
-        out.push_back(o.opcode); out.push_back(M(o.q1)); out.push_back(M(o.q2)); out.push_back(0);
-      }
-      break;
-    }
-    case SEG_MZ: {
-      for (auto& o : ops) { out.push_back(M(o.q1)); out.push_back(o.bit); }
-      for (uint32_t i = cnt; i % 2; i++) { out.push_back(scratch); out.push_back(BIT_NONE); }
-      break;
-    }
-    case SEG_MRZ: {
-      for (auto& o : ops) {
-        out.push_back(M(o.q1)); out.push_back(o.bit); out.push_back(o.reset); out.push_back(0);
-      }
-      break;
-    }
-    default: break;
-  }
-}
-
-static void emit_flush(std::vector<uint32_t>& out, uint32_t sb, uint32_t se) {
-  out.push_back((SEG_FLUSH << 24));
-  out.push_back(sb); out.push_back(se); out.push_back(0);
-}
+struct Emitter {
+  std::vector<uint32_t>& out;
+  std::vector<uint8_t>& swp;     // per slot: x currently lives in plane 2s+1
+  std::vector<uint32_t>& slot;   // qubit -> slot
+  uint32_t px(uint32_t q) const { uint32_t s = slot[q]; return 2 * s + (swp[s] ? 1 : 0); }
+  uint32_t pz(uint32_t q) const { uint32_t s = slot[q]; return 2 * s + (swp[s] ? 0 : 1); }
+  void pad4() { while (out.size() % 4) out.push_back(0); }
+};
 
 int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   std::memset(&P.info, 0, sizeof(P.info));
@@ -97,8 +76,8 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   uint64_t nsites = 0;
   for (size_t k = 0; k < n_ops; k++) {
     const qcb_op& op = ops[k];
-    uint32_t oc = op.opcode;
-    bool two = is2q(oc) || oc == QCB_OP_DEPOL2;
+    const uint32_t oc = op.opcode;
+    const bool two = is2q(oc) || oc == QCB_OP_DEPOL2;
     if (!(is1q(oc) || is2q(oc) || isnoise(oc) || ismeas(oc) || oc == QCB_OP_NOP))
       return fail(QCB_EUNSUPPORTED, "op " + std::to_string(k) + ": unknown opcode " + std::to_string(oc));
     if (oc == QCB_OP_NOP) continue;
@@ -112,38 +91,40 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
       return fail(QCB_EBOUNDS, "op " + std::to_string(k) + ": qubit index too large");
     nq = std::max(nq, op.q1);
     if (two) nq = std::max(nq, op.q2);
-    uint32_t q1 = op.q1 - 1, q2 = two ? op.q2 - 1 : 0;
+    const uint32_t q1 = op.q1 - 1, q2 = two ? op.q2 - 1 : 0;
     if (is1q(oc)) {
-      uint32_t kind = oc == QCB_OP_H ? SEG_H : oc == QCB_OP_S ? SEG_S : SEG_G1;
-      low.push_back({kind, oc, q1, 0, BIT_NONE, 0, -1});
       P.info.n_updates++;
+      if (is_frame_noop(oc)) continue;
+      const uint32_t kind = is_relabel(oc) ? SEG_H : (oc == QCB_OP_S || oc == QCB_OP_SDAG || oc == QCB_OP_HXY) ? SEG_S : SEG_G1;
+      low.push_back({kind, oc, q1, 0, BIT_NONE, 0, -1, k});
     } else if (is2q(oc)) {
-      uint32_t kind = oc == QCB_OP_CNOT ? SEG_CNOT : oc == QCB_OP_CPHASE ? SEG_CZ : SEG_G2;
-      low.push_back({kind, oc, q1, q2, BIT_NONE, 0, -1});
       P.info.n_updates++;
+      const uint32_t kind = (oc == QCB_OP_CNOT || oc == QCB_OP_ZCX) ? SEG_CNOT
+                            : (oc == QCB_OP_CPHASE || oc == QCB_OP_ZCZ) ? SEG_CZ : SEG_G2;
+      low.push_back({kind, oc, q1, q2, BIT_NONE, 0, -1, k});
     } else if (ismeas(oc)) {
       nbits = std::max(nbits, op.bit);
-      uint32_t bit = op.bit ? op.bit - 1 : BIT_NONE;
+      const uint32_t bit = op.bit ? op.bit - 1 : BIT_NONE;
       P.info.n_updates++;
       if (oc == QCB_OP_MZ) {
         if (op.bit == 0) continue;  // src/pauli_frames.jl:86
-        low.push_back({SEG_MZ, oc, q1, 0, bit, 0, -1});
+        low.push_back({SEG_MZ, oc, q1, 0, bit, 0, -1, k});
       } else if (oc == QCB_OP_MX) {
         if (op.bit == 0) continue;  // src/pauli_frames.jl:75
-        low.push_back({SEG_H, QCB_OP_H, q1, 0, BIT_NONE, 0, -1});
-        low.push_back({SEG_MZ, QCB_OP_MZ, q1, 0, bit, 0, -1});
+        low.push_back({SEG_H, QCB_OP_H, q1, 0, BIT_NONE, 0, -1, k});
+        low.push_back({SEG_MZ, QCB_OP_MZ, q1, 0, bit, 0, -1, k});
       } else if (oc == QCB_OP_MRZ) {
-        low.push_back({SEG_MRZ, oc, q1, 0, bit, nresets++, -1});
+        low.push_back({SEG_MRZ, oc, q1, 0, bit, nresets++, -1, k});
       } else {  // MRX
-        low.push_back({SEG_H, QCB_OP_H, q1, 0, BIT_NONE, 0, -1});
-        low.push_back({SEG_MRZ, QCB_OP_MRZ, q1, 0, bit, nresets++, -1});
+        low.push_back({SEG_H, QCB_OP_H, q1, 0, BIT_NONE, 0, -1, k});
+        low.push_back({SEG_MRZ, QCB_OP_MRZ, q1, 0, bit, nresets++, -1, k});
       }
     } else {  // noise
       for (int i = 0; i < 3; i++)
         if (!(op.p[i] >= 0.0) || !std::isfinite(op.p[i]))
           return fail(QCB_EARG, "op " + std::to_string(k) + ": noise probabilities must be finite and >= 0");
       P.site_of_op[k] = (int64_t)nsites;
-      low.push_back({0, oc, q1, q2, BIT_NONE, 0, (int64_t)nsites});
+      low.push_back({SEG_END, oc, q1, q2, BIT_NONE, 0, (int64_t)nsites, k});
       nsites++;
     }
   }
@@ -154,7 +135,7 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   P.info.n_noise_sites = (uint32_t)nsites;
   P.nq = nq;
 
-  // slot assignment: qubits in order of first use
+  // slots: qubits in order of first use (relabels included)
   std::vector<uint32_t> qslot(nq + 1, BIT_NONE);
   P.slot_qubit.clear();
   auto touch = [&](uint32_t q) {
@@ -165,82 +146,181 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     if (o.kind == SEG_CNOT || o.kind == SEG_CZ || o.kind == SEG_G2 || o.opcode == QCB_OP_DEPOL2) touch(o.q2);
   }
   P.nslots = (uint32_t)P.slot_qubit.size();
-  std::vector<uint32_t> slotmap(qslot.begin(), qslot.end());
-
-  // site table (operands in slot space)
-  P.sites_slot.clear(); P.site_arity.clear();
-  double pmax = 0;
-  for (size_t k = 0; k < n_ops; k++) {
-    if (P.site_of_op[k] < 0) continue;
-    const qcb_op& op = ops[k];
-    Site s{};
-    s.kind = op.opcode;
-    s.a = slotmap[op.q1 - 1];
-    s.b = op.opcode == QCB_OP_DEPOL2 ? slotmap[op.q2 - 1] : 0;
-    double pe;
-    if (op.opcode == QCB_OP_PAULI_NOISE) {
-      s.t0 = op.p[0]; s.t1 = op.p[0] + op.p[2]; s.t2 = op.p[0] + op.p[2] + op.p[1];
-      pe = s.t2;
-      P.site_arity.push_back(1);
-    } else {
-      double np = op.opcode == QCB_OP_DEPOL2 ? 15.0 : 3.0;
-      s.t0 = op.p[0] * np / (np + 1.0);
-      pe = s.t0;
-      P.site_arity.push_back(op.opcode == QCB_OP_DEPOL2 ? 2 : 1);
-    }
-    if (pe > 1.0) pe = 1.0;
-    pmax = std::max(pmax, pe);
-    P.sites_slot.push_back(s);
-  }
-  P.pmax = pmax;
-  P.inv_log1m = (pmax > 0 && pmax < 1.0) ? 1.0 / std::log1p(-pmax) : 0.0;
-
-  // segmentation
+  std::vector<uint8_t> swp(P.nslots, 0);
+  Emitter E{P.stream_slot, swp, qslot};
   P.stream_slot.clear();
+  P.sites_slot.assign(nsites, Site{});
+  P.site_arity.assign(nsites, 1);
+
+  double pmax = 0;
+  uint32_t nseg = 0, nflush = 0;
+
+  // Emits one segment of ops of one kind (all at one level: disjoint qubits).
+  auto emit_seg = [&](uint32_t kind, std::vector<LOp>& seg) {
+    if (seg.empty()) return;
+    auto& out = P.stream_slot;
+    const size_t hdr = out.size();
+    out.push_back(0); out.push_back(0); out.push_back(0); out.push_back(0);
+    uint32_t cnt = 0;
+    switch (kind) {
+      case SEG_CNOT:
+      case SEG_CZ:  // (x_a, z_a, x_b, z_b)
+        for (auto& o : seg) { out.push_back(o.xa); out.push_back(o.za); out.push_back(o.xb); out.push_back(o.zb); }
+        cnt = (uint32_t)seg.size();
+        break;
+      case SEG_S:  // (x, z, opcode, 0)
+      case SEG_G1:
+        for (auto& o : seg) { out.push_back(o.xa); out.push_back(o.za); out.push_back(o.opcode); out.push_back(0); }
+        cnt = (uint32_t)seg.size();
+        break;
+      case SEG_G2:  // (opcode, x_a, z_a, x_b), (z_b, 0, 0, 0)
+        for (auto& o : seg) {
+          out.push_back(o.opcode); out.push_back(o.xa); out.push_back(o.za); out.push_back(o.xb);
+          out.push_back(o.zb); out.push_back(0); out.push_back(0); out.push_back(0);
+        }
+        cnt = (uint32_t)seg.size();
+        break;
+      case SEG_MZ:  // (x, bit)
+        for (auto& o : seg) { out.push_back(o.xa); out.push_back(o.bit); }
+        cnt = (uint32_t)seg.size();
+        E.pad4();
+        break;
+      case SEG_MRZ: {  // groups of 4 entries (x, z, bit, reset | PAD): entry i of a group holds
+                       // reset 4*block + i, so one Philox block serves the group
+        std::sort(seg.begin(), seg.end(), [](const LOp& a, const LOp& b) { return a.reset < b.reset; });
+        size_t i = 0;
+        while (i < seg.size()) {
+          const uint32_t blk = seg[i].reset >> 2;
+          const LOp* ent[4] = {nullptr, nullptr, nullptr, nullptr};
+          while (i < seg.size() && (seg[i].reset >> 2) == blk) { ent[seg[i].reset & 3] = &seg[i]; i++; }
+          for (int k = 0; k < 4; k++) {
+            const LOp* o = ent[k];
+            if (o) { out.push_back(o->xa); out.push_back(o->za); out.push_back(o->bit); out.push_back(o->reset); }
+            else { out.push_back(0); out.push_back(0); out.push_back(BIT_NONE); out.push_back(MRZ_PAD); }
+          }
+          cnt++;
+        }
+        break;
+      }
+      default: break;
+    }
+    out[hdr] = (kind << 24) | cnt;
+    nseg++;
+  };
+  // One FLUSH record per set of sites: header [FLUSH<<24 | nranges], then the
+  // runs of consecutive site indices as (begin, end) pairs, padded to 16 bytes.
+  auto emit_flush = [&](const std::vector<std::pair<uint32_t, uint32_t>>& runs) {
+    if (runs.empty()) return;
+    auto& out = P.stream_slot;
+    out.push_back((SEG_FLUSH << 24) | (uint32_t)runs.size());
+    out.push_back(0); out.push_back(0); out.push_back(0);
+    for (auto& r : runs) { out.push_back(r.first); out.push_back(r.second); }
+    E.pad4();
+    nflush++;
+  };
+
+  // Scheduling, in program order.  The open segment collects ops of one kind
+  // on pairwise-disjoint qubits.  A noise op goes to the open segment's
+  // pre-flush (applied before the segment) when the segment does not touch its
+  // qubits -- every earlier op on them is in an emitted segment -- and
+  // otherwise to the post-flush, which is applied before the next segment.  An
+  // op that touches a qubit with post-flush noise, overlaps the segment or has
+  // another kind closes the segment.  Flips commute with ops on other qubits,
+  // so the result equals op-by-op execution, and a circuit written in layers
+  // (noise after each gate, measurement flips before each reset) gets one
+  // flush per layer.
   std::vector<LOp> cur;
   uint32_t cur_kind = SEG_END;
-  std::unordered_set<uint32_t> cur_q, pend_q;
-  uint32_t pend_begin = 0, pend_end = 0;
-  uint32_t nseg = 0, nflush = 0;
-  auto close_seg = [&]() {
-    if (cur.empty()) return;
-    emit_segment(P.stream_slot, cur_kind, cur, slotmap, P.nslots);
-    nseg++;
-    cur.clear(); cur_q.clear(); cur_kind = SEG_END;
-  };
-  auto flush = [&]() {
-    if (pend_end > pend_begin) {
-      emit_flush(P.stream_slot, pend_begin, pend_end);
-      nflush++;
+  std::unordered_set<uint32_t> cur_q, post_q;
+  std::vector<uint32_t> pre, post;
+  auto emit_sites = [&](std::vector<uint32_t>& st) {
+    std::sort(st.begin(), st.end());
+    std::vector<std::pair<uint32_t, uint32_t>> runs;
+    size_t i = 0;
+    while (i < st.size()) {  // runs of consecutive site indices
+      size_t j = i + 1;
+      while (j < st.size() && st[j] == st[j - 1] + 1) j++;
+      runs.push_back({st[i], st[j - 1] + 1});
+      i = j;
     }
-    pend_begin = pend_end;
-    pend_q.clear();
+    emit_flush(runs);
+    st.clear();
+  };
+  auto close_seg = [&]() {
+    emit_sites(pre);
+    emit_seg(cur_kind, cur);
+    cur.clear();
+    cur_q.clear();
+    cur_kind = SEG_END;
+    pre.swap(post);
+    post_q.clear();
   };
   for (auto& o : low) {
-    bool two = o.kind == SEG_CNOT || o.kind == SEG_CZ || o.kind == SEG_G2;
-    if (o.kind == 0) {  // noise
-      pend_q.insert(o.q1);
-      if (o.opcode == QCB_OP_DEPOL2) pend_q.insert(o.q2);
-      pend_end = (uint32_t)o.site + 1;
+    if (o.kind == SEG_END) {  // noise: record the site with the current planes
+      const qcb_op& op = ops[o.src];
+      Site& s = P.sites_slot[(size_t)o.site];
+      s.kind = op.opcode;
+      s.xa = E.px(o.q1); s.za = E.pz(o.q1);
+      bool touches = cur_q.count(o.q1) > 0;
+      if (op.opcode == QCB_OP_DEPOL2) {
+        s.xb = E.px(o.q2); s.zb = E.pz(o.q2);
+        touches = touches || cur_q.count(o.q2) > 0;
+        P.site_arity[(size_t)o.site] = 2;
+      }
+      double pe;
+      if (op.opcode == QCB_OP_PAULI_NOISE) {
+        s.t0 = op.p[0]; s.t1 = op.p[0] + op.p[2]; s.t2 = op.p[0] + op.p[2] + op.p[1];
+        pe = s.t2;
+      } else {
+        const double np = op.opcode == QCB_OP_DEPOL2 ? 15.0 : 3.0;
+        s.t0 = op.p[0] * np / (np + 1.0);
+        pe = s.t0;
+      }
+      if (pe > 1.0) pe = 1.0;
+      pmax = std::max(pmax, pe);
+      if (touches) {
+        post.push_back((uint32_t)o.site);
+        post_q.insert(o.q1);
+        if (op.opcode == QCB_OP_DEPOL2) post_q.insert(o.q2);
+      } else {
+        pre.push_back((uint32_t)o.site);
+      }
       continue;
     }
-    bool hit = pend_q.count(o.q1) || (two && pend_q.count(o.q2));
-    if (hit) { close_seg(); flush(); }
-    bool overlap = cur_q.count(o.q1) || (two && cur_q.count(o.q2));
-    if (o.kind != cur_kind || overlap || cur.size() >= (1u << 20)) close_seg();
+    if (o.kind == SEG_H) {  // relabel x <-> z of this qubit, no run-time work
+      swp[qslot[o.q1]] ^= 1;
+      continue;
+    }
+    const bool two = o.kind == SEG_CNOT || o.kind == SEG_CZ || o.kind == SEG_G2;
+    const bool hit = post_q.count(o.q1) || (two && post_q.count(o.q2));
+    const bool overlap = cur_q.count(o.q1) || (two && cur_q.count(o.q2));
+    bool same_bit = false;
+    if (o.bit != BIT_NONE)
+      for (auto& c : cur) same_bit = same_bit || c.bit == o.bit;
+    if (!cur.empty() && (hit || overlap || same_bit || o.kind != cur_kind || cur.size() >= (1u << 20)))
+      close_seg();
     cur_kind = o.kind;
-    cur.push_back(o);
+    LOp c = o;  // planes current at this op
+    c.xa = E.px(o.q1); c.za = E.pz(o.q1);
+    if (two) { c.xb = E.px(o.q2); c.zb = E.pz(o.q2); }
+    cur.push_back(c);
     cur_q.insert(o.q1);
     if (two) cur_q.insert(o.q2);
   }
   close_seg();
-  flush();
+  emit_sites(pre);
   P.stream_slot.push_back(SEG_END << 24); P.stream_slot.push_back(0);
   P.stream_slot.push_back(0); P.stream_slot.push_back(0);
   P.info.n_segments = nseg;
   P.info.n_flushes = nflush;
+  P.slot_swap.assign(swp.begin(), swp.end());
+  P.pmax = pmax;
+  P.inv_log1m = (pmax > 0 && pmax < 1.0) ? 1.0 / std::log1p(-pmax) : 0.0;
   P.hash = fnv1a(ops, n_ops * sizeof(qcb_op));
+  return QCB_OK;
+}
 
+int upload(Program& P) {
   // device copies
   auto up = [&](auto** dptr, const auto& vec) -> cudaError_t {
     size_t bytes = vec.size() * sizeof(vec[0]);
@@ -252,9 +332,12 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   cudaError_t e = up(&P.d_stream_slot, P.stream_slot);
   if (e == cudaSuccess) e = up(&P.d_sites_slot, P.sites_slot);
   if (e == cudaSuccess) e = up(&P.d_slot_qubit, P.slot_qubit);
-  std::vector<uint32_t> qs(qslot.begin(), qslot.end());
+  std::vector<uint32_t> qs(P.nq + 1, BIT_NONE);
+  for (uint32_t s = 0; s < P.nslots; s++) qs[P.slot_qubit[s]] = s;
   P.qubit_slot_len = (uint32_t)qs.size();
   if (e == cudaSuccess) e = up(&P.d_qubit_slot, qs);
+  std::vector<uint32_t> sw(P.slot_swap.begin(), P.slot_swap.end());
+  if (e == cudaSuccess) e = up(&P.d_slot_swap, sw);
   if (e != cudaSuccess) return cuda_fail(e, "qcb_program_compile upload");
   return QCB_OK;
 }
@@ -262,10 +345,12 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
 void release(Program& P) {
   cudaFree(P.d_stream_slot);
   cudaFree(P.d_sites_slot);
-  cudaFree(P.d_slot_qubit); cudaFree(P.d_qubit_slot);
+  cudaFree(P.d_slot_qubit);
+  cudaFree(P.d_qubit_slot);
+  cudaFree(P.d_slot_swap);
   P.d_stream_slot = nullptr;
   P.d_sites_slot = nullptr;
-  P.d_slot_qubit = P.d_qubit_slot = nullptr;
+  P.d_slot_qubit = P.d_qubit_slot = P.d_slot_swap = nullptr;
 }
 
 }  // namespace qcb
@@ -280,8 +365,33 @@ int qcb_program_compile(const qcb_op* ops, size_t n_ops, qcb_program** out) {
   if (n_ops && !ops) return fail(QCB_EARG, "qcb_program_compile: null ops");
   qcb_program* p = new qcb_program();
   int st = compile(ops, n_ops, *p);
+  if (st == QCB_OK) st = upload(*p);
   if (st != QCB_OK) { release(*p); delete p; return st; }
   *out = p;
+  return QCB_OK;
+}
+
+int qcb_debug_program_dump(const qcb_op* ops, size_t n_ops, uint32_t* stream, size_t stream_cap,
+                           size_t* stream_len, uint8_t* sites, size_t sites_cap, size_t* n_sites,
+                           uint32_t* slot_qubit, uint32_t* slot_swap, size_t slots_cap, size_t* n_slots,
+                           qcb_program_info* info) {
+  Program P;
+  int st = compile(ops, n_ops, P);
+  if (st != QCB_OK) return st;
+  if (stream_len) *stream_len = P.stream_slot.size();
+  if (n_sites) *n_sites = P.sites_slot.size();
+  if (n_slots) *n_slots = P.nslots;
+  if (info) *info = P.info;
+  if (stream && stream_cap >= P.stream_slot.size())
+    std::memcpy(stream, P.stream_slot.data(), P.stream_slot.size() * 4);
+  if (sites && sites_cap >= P.sites_slot.size() * sizeof(Site))
+    std::memcpy(sites, P.sites_slot.data(), P.sites_slot.size() * sizeof(Site));
+  if (slots_cap >= P.nslots) {
+    for (uint32_t s = 0; s < P.nslots; s++) {
+      if (slot_qubit) slot_qubit[s] = P.slot_qubit[s];
+      if (slot_swap) slot_swap[s] = P.slot_swap[s];
+    }
+  }
   return QCB_OK;
 }
 

@@ -63,29 +63,34 @@ __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1,
 }
 
 // ------------------------------------------------------------ programs
-// Device program: a stream of 16-byte aligned records.
-//   header (4 words): [kind<<24 | count, aux0, aux1, aux2]
-//   operands: padded to a multiple of 4 words.
+// Device program: a stream of 16-byte records.  Operands are physical plane
+// indices of the frame tile (plane 2s / 2s+1 of slot s, swapped while the
+// qubit is relabelled by an odd number of x<->z gates).
+//   header (4 words): [kind<<24 | count, aux0, aux1, aux2], then operands.
 enum SegKind : uint32_t {
   SEG_END = 0,
-  SEG_CNOT = 1,   // count gates, 2 words each (c, t), padded to 4 gates
-  SEG_H = 2,      // 1 word each (q), padded to 4
-  SEG_S = 3,      // 1 word each (q), padded to 4
-  SEG_G1 = 4,     // 2 words each (opcode, q), padded to 2
-  SEG_G2 = 5,     // 4 words each (opcode, q1, q2, 0)
-  SEG_MZ = 6,     // 2 words each (q, bit or NONE), padded to 2
-  SEG_MRZ = 7,    // 4 words each (q, bit or NONE, reset index, is_pad)
-  SEG_FLUSH = 8,  // header only: aux0 = site begin, aux1 = site end
-  SEG_CZ = 9      // 2 words each (a, b), padded to 4 gates
+  SEG_CNOT = 1,   // count entries (x_c, z_c, x_t, z_t)
+  SEG_H = 2,      // compile-time only (relabel); never emitted
+  SEG_S = 3,      // entries (x, z, opcode, 0): z ^= x
+  SEG_G1 = 4,     // entries (x, z, opcode, 0)
+  SEG_G2 = 5,     // entries (opcode, x_a, z_a, x_b), (z_b, 0, 0, 0)
+  SEG_MZ = 6,     // entries (x, bit), padded to a multiple of 4 words
+  SEG_MRZ = 7,    // count groups of 4 entries (x, z, bit or NONE, reset or PAD)
+  SEG_FLUSH = 8,  // count runs of sites (begin, end), padded to a multiple of 4 words
+  SEG_CZ = 9      // entries (x_a, z_a, x_b, z_b)
 };
 constexpr uint32_t BIT_NONE = 0xFFFFFFFFu;
+constexpr uint32_t MRZ_PAD = 0xFFFFFFFFu;
+// Noise sites per independent Philox event stream (per shot column).
+constexpr uint32_t NOISE_CHUNK = 32;
 
-// A noise site.  kind = opcode (PAULI_NOISE / DEPOL1 / DEPOL2); a, b =
-// operand (slot or qubit); thresholds for the event kind.
+// A noise site: kind = opcode (PAULI_NOISE / DEPOL1 / DEPOL2), the planes of
+// its qubit(s) at the noise op, and the thresholds for the event kind.
 struct Site {
-  uint32_t kind, a, b, pad;
+  uint32_t kind, xa, za, xb;
+  uint32_t zb, pad0, pad1, pad2;
   double t0, t1, t2;  // PAULI: X if v<t0, Z if v<t1, Y if v<t2;  DEPOL: t0 = p_eff
-  double pad2;
+  double pad3;
 };
 
 struct Program {
@@ -97,11 +102,13 @@ struct Program {
   std::vector<Site> sites_slot;
   std::vector<int64_t> site_of_op;    // op index -> site (or -1)
   std::vector<uint32_t> site_arity;
+  std::vector<uint8_t> slot_swap;     // final x<->z relabel per slot
   double pmax = 0, inv_log1m = 0;
   // device copies
   uint32_t* d_stream_slot = nullptr;
   Site* d_sites_slot = nullptr;
   uint32_t* d_slot_qubit = nullptr;
+  uint32_t* d_slot_swap = nullptr;
   uint32_t* d_qubit_slot = nullptr;   // [nq_alloc] qubit -> slot or NONE
   uint32_t qubit_slot_len = 0;
   uint64_t hash = 0;

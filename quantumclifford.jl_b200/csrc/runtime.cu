@@ -47,7 +47,7 @@ __global__ void philox_probe_kernel(uint4 ctr, uint2 key, uint32_t* out) {
   for (int i = 0; i < 4; i++) out[i] = o[i];
 }
 
-void set_walker_nt(uint32_t nt);
+void set_walker_tile(uint32_t t);
 void set_canon_cluster(uint32_t cs);
 void set_project_cluster(uint32_t cs);
 
@@ -104,9 +104,9 @@ int qcb_tune_set(const char* key, int64_t value) {
   if (!key) return fail(QCB_EARG, "qcb_tune_set: null key");
   const std::string k(key);
   if (value < 0 || value > 1024) return fail(QCB_EARG, "qcb_tune_set: value out of range");
-  if (k == "walker_threads") {
-    if (value && (value % 32 || value < 32)) return fail(QCB_EARG, "walker_threads must be a multiple of 32");
-    set_walker_nt((uint32_t)value);
+  if (k == "walker_tile") {
+    if (value && (value % 32 || value > 256)) return fail(QCB_EARG, "walker_tile must be a multiple of 32, at most 256");
+    set_walker_tile((uint32_t)value);
   } else if (k == "canon_cluster") {
     if (value && (value > 16 || (value & (value - 1)))) return fail(QCB_EARG, "canon_cluster must be 1, 2, 4, 8 or 16");
     set_canon_cluster((uint32_t)value);
@@ -145,6 +145,7 @@ int qcb_tableau_create(uint32_t rows, uint32_t nqubits, qcb_tableau** out) {
   if (e == cudaSuccess) e = cudaMalloc(&t->scratch, 4096);
   if (e == cudaSuccess) e = cudaMemset(t->xzs, 0, (words ? words : 1) * 8);
   if (e == cudaSuccess) e = cudaMemset(t->phases, 0, rows ? rows : 1);
+  if (e == cudaSuccess) e = cudaMemset(t->scratch, 0, 4096);
   if (e != cudaSuccess) {
     cudaFree(t->xzs); cudaFree(t->phases); cudaFree(t->scratch);
     delete t;

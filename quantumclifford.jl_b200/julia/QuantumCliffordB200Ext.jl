@@ -1,0 +1,242 @@
+# QuantumCliffordB200Ext -- Julia package extension that routes QuantumClifford's
+# bit-packed tableau / Pauli-frame hot path to libqcb200 (B200, sm_100a) through
+# `ccall`.  It plays the role ext/QuantumCliffordGPUExt plays for CUDA.jl arrays:
+# methods are selected by dispatch on the device-backed storage types defined here.
+#
+# Not exercised in this repository (no Julia toolchain here); the same C ABI is
+# exercised by the Python mirror in ../qcb200 and its tests.
+module QuantumCliffordB200Ext
+
+using QuantumClifford
+import QuantumClifford: apply!, pftrajectories, mul_left!, canonicalize!, project!,
+    measurements, PauliFrame, Stabilizer, MixedDestabilizer, Destabilizer, MixedStabilizer,
+    PauliOperator, Tableau, nqubits, tab, CliffordOperator, AbstractOperation
+
+const libqcb = get(ENV, "QCB200_LIB", joinpath(@__DIR__, "..", "lib", "libqcb200.so"))
+
+# ---------------------------------------------------------------- errors
+const QCB_OK = Cint(0)
+
+function _check(st::Cint)
+    st == QCB_OK && return nothing
+    buf = Vector{UInt8}(undef, 4096)
+    ccall((:qcb_last_error, libqcb), Cint, (Ptr{UInt8}, Csize_t), buf, length(buf))
+    msg = unsafe_string(pointer(buf))
+    st == 1 && throw(DimensionMismatch(msg))
+    st == 2 && throw(BoundsError(msg))
+    (st == 3 || st == 4) && throw(ArgumentError(msg))
+    st == 9 && throw(QuantumClifford.BadDataStructure(msg, :project!, :Destabilizer))
+    error("libqcb200 status $st: $msg")
+end
+
+# ---------------------------------------------------------------- ops
+struct QcbOp            # mirrors `qcb_op` (40 bytes)
+    opcode::UInt32
+    q1::UInt32
+    q2::UInt32
+    bit::UInt32
+    p::NTuple{3,Float64}
+end
+
+const OPC = Dict{DataType,UInt32}(
+    sId1 => 1, sHadamard => 2, sPhase => 3, sInvPhase => 4, sX => 5, sY => 6, sZ => 7,
+    sSQRTX => 8, sInvSQRTX => 9, sSQRTY => 10, sInvSQRTY => 11, sHadamardXY => 12, sHadamardYZ => 13,
+    sCXYZ => 14, sCZYX => 15, sCNOT => 32, sCPHASE => 33, sSWAP => 34, sZCX => 35, sZCY => 36,
+    sZCZ => 37, sXCX => 38, sXCY => 39, sXCZ => 40, sYCX => 41, sYCY => 42, sYCZ => 43,
+    sMZ => 64, sMRZ => 65, sMX => 66, sMRX => 67)
+
+_qcbops(op::AbstractSingleQubitOperator) = [QcbOp(OPC[typeof(op)], op.q, 0, 0, (0.0, 0.0, 0.0))]
+_qcbops(op::AbstractTwoQubitOperator) = [QcbOp(OPC[typeof(op)], op.q1, op.q2, 0, (0.0, 0.0, 0.0))]
+_qcbops(op::Union{sMZ,sMRZ,sMX,sMRX}) = [QcbOp(OPC[typeof(op)], op.qubit, 0, op.bit, (0.0, 0.0, 0.0))]
+function _qcbops(op::NoiseOp)
+    n = op.noise
+    if n isa UnbiasedUncorrelatedNoise
+        return [QcbOp(96, q, 0, 0, (n.p / 3, n.p / 3, n.p / 3)) for q in op.indices]
+    elseif n isa PauliNoise
+        return [QcbOp(96, q, 0, 0, (n.px, n.py, n.pz)) for q in op.indices]
+    elseif n isa DepolarizationNoise && length(op.indices) == 1
+        return [QcbOp(97, op.indices[1], 0, 0, (n.p, 0.0, 0.0))]
+    elseif n isa DepolarizationNoise && length(op.indices) == 2
+        return [QcbOp(98, op.indices[1], op.indices[2], 0, (n.p, 0.0, 0.0))]
+    end
+    throw(ArgumentError("noise model $(typeof(n)) is not supported on the B200 path"))
+end
+_qcbops(circuit::AbstractVector) = reduce(vcat, (_qcbops(op) for op in circuit); init=QcbOp[])
+
+# ---------------------------------------------------------------- programs
+mutable struct B200Program
+    handle::Ptr{Cvoid}
+    function B200Program(circuit)
+        ops = _qcbops(circuit)
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        _check(ccall((:qcb_program_compile, libqcb), Cint, (Ptr{QcbOp}, Csize_t, Ref{Ptr{Cvoid}}), ops, length(ops), h))
+        p = new(h[])
+        finalizer(x -> ccall((:qcb_program_destroy, libqcb), Cint, (Ptr{Cvoid},), x.handle), p)
+    end
+end
+
+const _programs = IdDict{Any,B200Program}()   # circuits compiled once
+_program(circuit) = get!(() -> B200Program(circuit), _programs, circuit)
+
+# ---------------------------------------------------------------- frames
+"""Device Pauli frame; `to_b200(PauliFrame(...))` or `B200Frame(frames, qubits, bits)`."""
+mutable struct B200Frame
+    handle::Ptr{Cvoid}
+    frames::Int
+    qubits::Int
+    nbits::Int
+    seed::UInt64
+end
+
+function B200Frame(frames::Integer, qubits::Integer, bits::Integer; seed::Integer=rand(UInt64))
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    _check(ccall((:qcb_frame_create, libqcb), Cint, (UInt64, UInt32, UInt32, Ref{Ptr{Cvoid}}), frames, qubits, bits, h))
+    f = B200Frame(h[], frames, qubits, bits, UInt64(seed))
+    finalizer(x -> ccall((:qcb_frame_destroy, libqcb), Cint, (Ptr{Cvoid},), x.handle), f)
+    _check(ccall((:qcb_frame_init_z, libqcb), Cint, (Ptr{Cvoid}, UInt64, UInt64, Ptr{Cvoid}), f.handle, f.seed, 0, C_NULL))
+    f
+end
+
+struct NoiseSource   # mirrors `qcb_noise_source`
+    mode::UInt32
+    reserved::UInt32
+    seed::UInt64
+    shot_offset::UInt64
+    events::Ptr{Cvoid}
+    n_events::UInt64
+    reset_planes::Ptr{UInt32}
+end
+
+function pftrajectories(f::B200Frame, circuit)
+    src = Ref(NoiseSource(0, 0, f.seed, 0, C_NULL, 0, C_NULL))
+    _check(ccall((:qcb_pftrajectories, libqcb), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{NoiseSource}, Ptr{Cvoid}),
+                 f.handle, _program(circuit).handle, src, C_NULL))
+    f.seed += 0x9E3779B97F4A7C15   # next call draws fresh randomness
+    f
+end
+
+apply!(f::B200Frame, op::AbstractOperation) = pftrajectories(f, [op])
+
+function measurements(f::B200Frame)
+    m = Matrix{Bool}(undef, f.frames, f.nbits)
+    _check(ccall((:qcb_frame_download_measurements, libqcb), Cint, (Ptr{Cvoid}, Ptr{Bool}, Ptr{Cvoid}),
+                 f.handle, m, C_NULL))
+    m
+end
+
+"""The frame tableau back in the reference fastcolumn layout (UInt64)."""
+function QuantumClifford.PauliFrame(f::B200Frame)
+    W = 2 * cld(f.qubits + 1, 64)
+    xzs = Matrix{UInt64}(undef, f.frames, W)          # frames contiguous per word
+    _check(ccall((:qcb_frame_download_xzs, libqcb), Cint, (Ptr{Cvoid}, Ptr{UInt64}, Ptr{Cvoid}), f.handle, xzs, C_NULL))
+    stab = Stabilizer(Tableau(zeros(UInt8, f.frames), f.qubits + 1, collect(xzs')))
+    PauliFrame(fastcolumn(stab), measurements(f))
+end
+
+to_b200(f::PauliFrame; seed::Integer=rand(UInt64)) = begin
+    g = B200Frame(length(f), nqubits(f), size(f.measurements, 2); seed)
+    xzs = collect(permutedims(tab(f.frame).xzs))     # frames x W, frames contiguous per word
+    _check(ccall((:qcb_frame_upload_xzs, libqcb), Cint, (Ptr{Cvoid}, Ptr{UInt64}, Ptr{Cvoid}), g.handle, xzs, C_NULL))
+    g
+end
+
+"""pftrajectories(circuit; trajectories) on the device in one call."""
+function pftrajectories_b200(circuit; trajectories=5000, seed::Integer=rand(UInt64))
+    qmax = maximum((maximum(affectedqubits(g), init=1) for g in circuit))
+    bmax = maximum((maximum(affectedbits(g), init=1) for g in circuit))
+    f = B200Frame(trajectories, qmax, bmax; seed)
+    pftrajectories(f, circuit)
+end
+
+# ---------------------------------------------------------------- tableaux
+mutable struct B200Tableau
+    handle::Ptr{Cvoid}
+    rows::Int
+    nqubits::Int
+end
+
+function B200Tableau(t::Tableau)
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    _check(ccall((:qcb_tableau_create, libqcb), Cint, (UInt32, UInt32, Ref{Ptr{Cvoid}}), length(t), t.nqubits, h))
+    d = B200Tableau(h[], length(t), t.nqubits)
+    finalizer(x -> ccall((:qcb_tableau_destroy, libqcb), Cint, (Ptr{Cvoid},), x.handle), d)
+    xzs = convert(Matrix{UInt64}, t.xzs)          # (W, rows) column-major: rows contiguous
+    _check(ccall((:qcb_tableau_upload, libqcb), Cint, (Ptr{Cvoid}, Ptr{UInt8}, Ptr{UInt64}, Ptr{Cvoid}),
+                 d.handle, convert(Vector{UInt8}, t.phases), xzs, C_NULL))
+    d
+end
+B200Tableau(p::PauliOperator) = B200Tableau(Tableau([p]))
+
+function download!(t::Tableau, d::B200Tableau)
+    ph = Vector{UInt8}(undef, d.rows)
+    xzs = Matrix{UInt64}(undef, size(t.xzs)...)
+    _check(ccall((:qcb_tableau_download, libqcb), Cint, (Ptr{Cvoid}, Ptr{UInt8}, Ptr{UInt64}, Ptr{Cvoid}),
+                 d.handle, ph, xzs, C_NULL))
+    t.phases .= ph
+    t.xzs .= xzs
+    t
+end
+
+"""A state whose tableau lives on the B200: `to_b200(s)`, `to_cpu(s)`."""
+struct B200State{S}
+    host::S             # host object (shape, kind, rank)
+    dev::B200Tableau
+end
+to_b200(s::Union{Stabilizer,Destabilizer,MixedStabilizer,MixedDestabilizer}) = B200State(copy(s), B200Tableau(tab(s)))
+to_b200(p::PauliOperator) = B200State(copy(p), B200Tableau(p))
+to_cpu(s::B200State) = (download!(tab(s.host), s.dev); s.host)
+
+_kind(::Stabilizer) = 0
+_kind(::MixedStabilizer) = 1
+_kind(::Destabilizer) = 2
+_kind(::MixedDestabilizer) = 3
+
+function mul_left!(r::B200State{<:PauliOperator}, l::B200State{<:PauliOperator}; phases::Val{B}=Val(true)) where B
+    ph = Ref{UInt8}(0)
+    _check(ccall((:qcb_mul_left_pauli, libqcb), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Ref{UInt8}, Ptr{Cvoid}),
+                 r.dev.handle, l.dev.handle, B, ph, C_NULL))
+    B && (r.host.phase[] = ph[])
+    r
+end
+
+function canonicalize!(s::B200State; phases::Bool=true, ranks::Bool=false)
+    h = s.host
+    n = nqubits(h)
+    row0, rows = h isa Union{Destabilizer,MixedDestabilizer} ? (n + 1, h isa MixedDestabilizer ? h.rank : n) :
+                 (1, h isa MixedStabilizer ? h.rank : length(tab(h)))
+    rx, rz = Ref{Int32}(0), Ref{Int32}(0)
+    _check(ccall((:qcb_canonicalize, libqcb), Cint, (Ptr{Cvoid}, UInt32, UInt32, Cint, Ref{Int32}, Ref{Int32}, Ptr{Cvoid}),
+                 s.dev.handle, row0, rows, phases, rx, rz, C_NULL))
+    ranks ? (s, Int(rx[]), Int(rz[])) : s
+end
+
+function project!(s::B200State, p::B200State{<:PauliOperator}; keep_result::Bool=true, phases::Bool=true)
+    h = s.host
+    rank = Ref{Int32}(h isa Union{MixedStabilizer,MixedDestabilizer} ? h.rank : 0)
+    anti, res, done = Ref{Int32}(0), Ref{Int32}(0), Ref{UInt32}(0)
+    _check(ccall((:qcb_project, libqcb), Cint,
+                 (Ptr{Cvoid}, Cint, Ref{Int32}, Ptr{Cvoid}, Cint, Cint, Ref{Int32}, Ref{Int32}, Ref{UInt32}, Ptr{Cvoid}),
+                 s.dev.handle, _kind(h), rank, p.dev.handle, keep_result, phases, anti, res, done, C_NULL))
+    h isa Union{MixedStabilizer,MixedDestabilizer} && (h.rank = rank[])
+    s, Int(anti[]), res[] < 0 ? nothing : UInt8(res[])
+end
+
+function apply!(s::B200State, gate::AbstractSymbolicOperator; phases::Bool=true)
+    ops = _qcbops(gate)
+    _check(ccall((:qcb_apply_gates, libqcb), Cint, (Ptr{Cvoid}, Ptr{QcbOp}, Csize_t, Cint, Ptr{Cvoid}),
+                 s.dev.handle, ops, length(ops), phases, C_NULL))
+    s
+end
+
+function apply!(s::B200State, c::CliffordOperator; phases::Bool=true)
+    cd = B200Tableau(tab(c))
+    _check(ccall((:qcb_apply_dense, libqcb), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Ptr{Cvoid}),
+                 s.dev.handle, cd.handle, phases, C_NULL))
+    s
+end
+
+function __init__()
+    _check(ccall((:qcb_init, libqcb), Cint, (Cint,), 0))
+end
+
+end # module

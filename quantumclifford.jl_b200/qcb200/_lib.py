@@ -159,6 +159,8 @@ def lib():
         "qcb_apply_gates": ([vp, vp, sz, ctypes.c_int, vp], ctypes.c_int),
         "qcb_apply_dense": ([vp, vp, ctypes.c_int, vp], ctypes.c_int),
         "qcb_debug_philox": ([vp, vp, vp], ctypes.c_int),
+        "qcb_debug_program_dump": ([vp, sz, vp, sz, P(sz), vp, sz, P(sz), vp, vp, sz, P(sz), P(qcb_program_info)],
+                                   ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

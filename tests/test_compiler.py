@@ -1,0 +1,60 @@
+"""CPU tests of the circuit compiler: the device program, interpreted on the
+host (tests/stream_emu.py), must reproduce the oracle bit for bit in mask
+mode.  No GPU is involved: qcb_debug_program_dump compiles on the host."""
+import numpy as np
+import pytest
+
+import oracle
+import qcb200
+import stream_emu
+from qcb200 import circuits, ops as O
+
+from test_gpu_frames import random_circuit  # noqa: E402  (shared generator; its GPU tests are marked)
+
+
+def check_circuit(circ, frames, seed):
+    arr = O.to_array(circ)
+    qmax, bmax = O.affected_counts(arr)
+    masks = qcb200.sample_masks(arr, frames, qubits=qmax, seed=seed)
+    X, Z, rec, info = stream_emu.run_mask(arr, frames, qmax, bmax, masks)
+    ox, om = oracle.pftrajectories_mask(arr, frames, qmax, bmax, masks.init_z, masks.reset_planes, masks.events)
+    got = qcb200.unpack_record(rec, frames)
+    assert np.array_equal(got, om)
+    xzs = stream_emu.planes_to_xzs(X, Z, frames)
+    m = oracle.coding_mask(qmax + 1)[:, None]
+    assert np.array_equal(xzs & m, ox & m)
+    return info
+
+
+def test_repetition_code():
+    info = check_circuit(circuits.repetition_code_memory(7, 7, 0.1), 300, 1)
+    assert info["n_updates"] == 133
+
+
+def test_surface_code_program_shape():
+    info = check_circuit(circuits.rotated_surface_code_memory(5, 5, 0.02), 200, 2)
+    # per round: four CNOT layers and the reset layer, a handful of flushes
+    assert info["n_segments"] <= 5 * 6 + 2
+    assert info["n_flushes"] <= 5 * 6 + 2
+
+
+def test_surface_code_d11_segments():
+    _, _, _, _, info = stream_emu.dump(circuits.rotated_surface_code_memory(11, 11, 1e-3))
+    assert info["n_updates"] == 7601
+    assert info["n_segments"] <= 11 * 6 + 2, info
+    assert info["n_flushes"] <= 11 * 6 + 2, info
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_circuits(seed):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(2, 40))
+    check_circuit(random_circuit(n, 300, rng, p=0.1), int(rng.integers(1, 200)), seed)
+
+
+def test_relabels_and_noise_interleave():
+    # noise between relabels on the same qubit, and measurements of relabelled qubits
+    c = [O.sHadamard(1)] + O.PauliError(1, 0.3) + [O.sHadamard(1)] + O.PauliError(1, 0.3, 0.1, 0.2)
+    c += [O.sCNOT(1, 2), O.sSQRTY(2)] + O.NoiseOp(O.DepolarizationNoise(0.5), (1, 2))
+    c += [O.sMX(2, 1), O.sMRX(1, 2), O.sMZ(2, 3), O.sX(1), O.sMRZ(1, 4), O.sMZ(1, 2)]
+    check_circuit(c, 500, 3)

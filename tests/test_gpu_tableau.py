@@ -38,8 +38,8 @@ def test_mul_left_pauli(qcb, n, phases):
     rng = np.random.default_rng(n)
     for _ in range(3):
         a, b = rand_tab(1, n, rng), rand_tab(1, n, rng)
-        ra = qcb.PauliOperator(b.phases, n, b.xzs).to_gpu()
-        la = qcb.PauliOperator(a.phases, n, a.xzs).to_gpu()
+        ra = qcb.PauliOperator(b.phases.copy(), n, b.xzs.copy()).to_gpu()
+        la = qcb.PauliOperator(a.phases.copy(), n, a.xzs.copy()).to_gpu()
         qcb.mul_left_(ra, la, phases=phases)
         ra.to_cpu()
         r, ph = oracle.mul_left_pauli(b.xzs[0], b.phases[0], a.xzs[0], a.phases[0], phases)
@@ -268,6 +268,7 @@ def test_dense_apply(qcb, n):
     else:
         c = qcb.CliffordOperator(dev_random_destabilizer(qcb, n, rng).tab)
         c.tab.phases[:] = rng.integers(0, 4, 2 * n)
+        c.to_gpu()  # the device copy must see the new phases
     for phases in (True, False):
         s = qcb.Stabilizer(state.copy()).to_gpu()
         qcb.apply_(s, c, phases=phases)

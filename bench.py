@@ -201,7 +201,7 @@ def main():
     upd = O.count_updates(arr)
     assert upd == 7601
     shots = args.shots
-    offset = rank * ((shots + 31) // 32 * 32)
+    offset = rank * ((shots + 1023) // 1024 * 1024)  # Philox shot groups are 1024 shots
     prog = qcb200.Program(arr)
     qmax, bmax = O.affected_counts(arr)
     frame = qcb200.PauliFrame(shots, qmax, bmax, init=False)

@@ -279,7 +279,7 @@ int qcb_apply_dense(qcb_tableau* t, const qcb_tableau* c, int phases, void* stre
 /* Philox-4x32-10 block (counter, key) -> out, computed on the device.       */
 int qcb_debug_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* Compile on the host only (no device needed) and copy out the device
- * program: the record stream (uint32 words), the noise-site table (64 bytes
+ * program: the record stream (uint32 words), the noise-site table (80 bytes
  * per site), and per slot the frame qubit and the final x<->z relabel flag.
  * Buffers may be NULL or too small, in which case only the sizes are set.   */
 int qcb_debug_program_dump(const qcb_op* ops, size_t n_ops, uint32_t* stream, size_t stream_cap,

@@ -689,8 +689,9 @@ void oracle_frame_init_z(u64* xzs, u64 S, u32 nq1, const u32* z_planes, u64 seed
 // -------------------------------------------------- Philox-mode replica
 // The device's Philox-mode sampling procedure restated on the CPU, so that
 // the on-device generator can be checked bit for bit (the reference's own
-// streams are checked statistically).  Counters: (index, column lo, column hi,
-// tag), key = seed; column = global 32-shot word index.
+// streams are checked statistically).  initZ! and reset counters are
+// (index, column lo, column hi, tag) with column = global 32-shot word index;
+// noise counters are (site, 1024-shot group, block, tag); key = seed.
 enum { TAG_INITZ = 0x51A7u, TAG_RESET = 0x5E5Eu, TAG_NOISE = 0x4E01u };
 
 static inline void philox_block(u64 seed, u32 idx, u64 col, u32 tag, u32 out[4]) {
@@ -699,40 +700,28 @@ static inline void philox_block(u64 seed, u32 idx, u64 col, u32 tag, u32 out[4])
   oracle_philox4x32_10(ctr, key, out);
 }
 
-// Noise-site thresholds, as the program compiler lays them out.
-struct Site { u32 opcode, q1, q2; double t0, t1, t2, peff; };
+// Noise sites as the program compiler lays them out: event probability p_eff,
+// kind thresholds, Binomial(GROUP, p_eff) count parameters.
+static const u32 NOISE_GROUP = 1024;
+struct Site { u32 opcode, q1, q2; double t0, t1, t2, peff, q0, r; bool dense; };
 
-// Event streams: the noise sites are cut into chunks of NOISE_CHUNK sites;
-// each (chunk g, 32-shot column) has its own counter-based stream over the
-// trials tau = (site - g*CHUNK)*32 + lane, with geometric gaps at rate pmax
-// and the event kind from a second uniform scaled by pmax.
-static const u32 NOISE_CHUNK = 32;
-
-struct Event { u32 site, lane; double v; };
-
-static void chunk_events(u64 seed, u64 col, u32 g, double pmax, double inv_log1m, u32 nsites,
-                         std::vector<Event>& out) {
-  const long long span = (long long)NOISE_CHUNK * 32;
-  long long tau = -1;
-  for (u32 draw = 0;; draw++) {
-    u32 ctr[4] = {draw, (u32)col, g, TAG_NOISE};
-    u32 key[2] = {(u32)seed, (u32)(seed >> 32)};
-    u32 o[4];
-    oracle_philox4x32_10(ctr, key, o);
-    u64 u53 = ((u64)o[0] << 21) | (o[1] >> 11);
-    double u = ((double)u53 + 0.5) * 0x1.0p-53;
-    double gap = pmax >= 1.0 ? 0.0 : std::floor(std::log(u) * inv_log1m);
-    if (gap >= (double)span) break;
-    tau += 1 + (long long)gap;
-    if (tau >= span) break;
-    u32 site = g * NOISE_CHUNK + (u32)(tau >> 5);
-    if (site >= nsites) break;
-    out.push_back({site, (u32)(tau & 31), (double)o[2] * 0x1.0p-32 * pmax});
+static Site make_site(const qcb_op& op) {
+  Site s{op.opcode, op.q1 - 1, op.q2 ? op.q2 - 1 : 0, 0, 0, 0, 0, 0, 0, false};
+  if (op.opcode == QCB_OP_PAULI_NOISE) {
+    s.t0 = op.p[0]; s.t1 = op.p[0] + op.p[2]; s.t2 = op.p[0] + op.p[2] + op.p[1];
+    s.peff = s.t2;
+  } else {
+    double np = op.opcode == QCB_OP_DEPOL2 ? 15.0 : 3.0;
+    s.peff = op.p[0] * np / (np + 1.0);
+    s.t0 = s.t1 = s.t2 = s.peff;
   }
+  if (s.peff > 1.0) s.peff = 1.0;
+  s.dense = s.peff * NOISE_GROUP > 16.0;
+  if (s.peff < 1.0) { s.q0 = std::pow(1.0 - s.peff, (double)NOISE_GROUP); s.r = s.peff / (1.0 - s.peff); }
+  return s;
 }
 
-// Returns the Pauli code of the event (0 = thinned away).
-static inline u32 site_code(const Site& s, double v) {
+static inline u32 event_code(const Site& s, double v) {
   if (s.opcode == QCB_OP_PAULI_NOISE) {
     if (v < s.t0) return 1;
     if (v < s.t1) return 2;
@@ -741,104 +730,139 @@ static inline u32 site_code(const Site& s, double v) {
   }
   u32 np = s.opcode == QCB_OP_DEPOL2 ? 15u : 3u;
   if (v < s.peff) {
-    u32 k = (u32)(v / s.peff * (double)np);
+    u32 k = (u32)((v / s.peff) * (double)np);
     if (k >= np) k = np - 1;
     return k + 1;
   }
   return 0;
 }
 
+struct Event { u32 pos, code; };
+
+// Events of one site on one group of NOISE_GROUP shots: Philox blocks
+// (site, group, block, TAG_NOISE); sparse sites draw the Binomial count by
+// inverse CDF and place the events on distinct uniform positions, dense sites
+// draw one uniform per shot.
+static void site_group_events(const Site& s, u32 site, u64 group, u64 seed, std::vector<Event>& out) {
+  if (!(s.peff > 0.0)) return;
+  u32 key[2] = {(u32)seed, (u32)(seed >> 32)};
+  u32 o[4];
+  if (s.dense) {
+    for (u32 blk = 0; blk < NOISE_GROUP / 4; blk++) {
+      u32 ctr[4] = {site, (u32)group, blk, TAG_NOISE};
+      oracle_philox4x32_10(ctr, key, o);
+      for (u32 j = 0; j < 4; j++) {
+        u32 code = event_code(s, (double)o[j] * 0x1.0p-32);
+        if (code) out.push_back({blk * 4 + j, code});
+      }
+    }
+    return;
+  }
+  u32 ctr0[4] = {site, (u32)group, 0u, TAG_NOISE};
+  oracle_philox4x32_10(ctr0, key, o);
+  double u = ((double)o[0] + 0.5) * 0x1.0p-32;
+  u32 k = 0;
+  double pk = s.q0, cum = s.q0;
+  while (u > cum && k < NOISE_GROUP) {
+    pk = (pk * ((double)(NOISE_GROUP - k) * s.r)) / (double)(k + 1);
+    k++;
+    cum = cum + pk;
+  }
+  u32 blk = 0, widx = 1;
+  std::vector<bool> used(NOISE_GROUP, false);
+  auto word = [&](u32 i) {
+    if ((i >> 2) != blk) {
+      blk = i >> 2;
+      u32 ctr[4] = {site, (u32)group, blk, TAG_NOISE};
+      oracle_philox4x32_10(ctr, key, o);
+    }
+    return o[i & 3];
+  };
+  for (u32 e = 0; e < k; e++) {
+    u32 pos, tw;
+    while (true) {
+      pos = word(widx) & (NOISE_GROUP - 1);
+      widx++;
+      tw = word(widx);
+      widx++;
+      if (!used[pos]) { used[pos] = true; break; }
+    }
+    u32 code = event_code(s, ((double)tw * 0x1.0p-32) * s.peff);
+    if (code) out.push_back({pos, code});
+  }
+}
+
 // Runs the op list on the frame in Philox mode exactly as the device does.
 // Frame x/z must be preset (x=0 and Z from oracle_philox_init_z for a fresh
-// frame).  shot_offset: global shot of frame 0 (multiple of 32).
+// frame).  shot_offset: global shot of frame 0 (multiple of 1024).
 void oracle_pftrajectories_philox(u64* xzs, u8* meas, u64 S, u32 nq1, u32 nbits,
                                   const qcb_op* ops, size_t nops, u64 seed, u64 shot_offset) {
   Frame F{xzs, meas, S, nq1, nbits, 2 * (size_t)((nq1 + 63) / 64)};
-  // site table in program order
   std::vector<Site> sites;
   std::vector<long> site_of_op(nops, -1);
-  double pmax = 0;
   for (size_t k = 0; k < nops; k++) {
-    const qcb_op& op = ops[k];
-    if (!is_noise(op.opcode)) continue;
-    Site s{op.opcode, op.q1 - 1, op.q2 ? op.q2 - 1 : 0, 0, 0, 0, 0};
-    double pe;
-    if (op.opcode == QCB_OP_PAULI_NOISE) {
-      s.t0 = op.p[0]; s.t1 = op.p[0] + op.p[2]; s.t2 = op.p[0] + op.p[2] + op.p[1];
-      pe = s.t2;
-    } else {
-      double np = op.opcode == QCB_OP_DEPOL2 ? 15.0 : 3.0;
-      s.peff = op.p[0] * np / (np + 1.0);
-      pe = s.peff;
-    }
-    if (pe > 1.0) pe = 1.0;
-    pmax = std::max(pmax, pe);
+    if (!is_noise(ops[k].opcode)) continue;
     site_of_op[k] = (long)sites.size();
-    sites.push_back(s);
+    sites.push_back(make_site(ops[k]));
   }
-  double inv_log1m = pmax > 0 && pmax < 1.0 ? 1.0 / std::log1p(-pmax) : 0.0;
-  u64 words = (S + 31) / 32;
-  u64 col0 = shot_offset / 32;
-  const u32 nsites = (u32)sites.size();
-  const u32 nchunks = (nsites + NOISE_CHUNK - 1) / NOISE_CHUNK;
-  for (u64 w = 0; w < words; w++) {
-    u64 col = col0 + w;
-    // all events of this column, grouped by site
-    std::vector<Event> evs;
-    if (pmax > 0)
-      for (u32 g = 0; g < nchunks; g++) chunk_events(seed, col, g, pmax, inv_log1m, nsites, evs);
-    std::vector<std::vector<const Event*>> by_site(nsites);
-    for (const Event& e : evs) by_site[e.site].push_back(&e);
-    u64 f0 = w * 32, f1 = std::min<u64>(S, f0 + 32);
-    size_t reset_index = 0;
-    u32 rcache[4]; u32 rblock = 0xFFFFFFFFu;
-    for (size_t k = 0; k < nops; k++) {
-      const qcb_op& op = ops[k];
-      u32 oc = op.opcode;
-      if (is_noise(oc)) {
-        long s = site_of_op[k];
-        for (const Event* e : by_site[(size_t)s]) {
-          u64 f = f0 + e->lane;
-          u32 code = site_code(sites[(size_t)s], e->v);
-          if (code && f < f1) {
-            const Site& st = sites[(size_t)s];
+  const u64 words = (S + 31) / 32, col0 = shot_offset / 32;
+  for (u64 g0 = 0; g0 < words; g0 += 32) {  // groups of 32 columns = 1024 shots
+    const u64 group = (col0 + g0) / 32;
+    std::vector<std::vector<Event>> ev(sites.size());
+    for (u32 s = 0; s < (u32)sites.size(); s++) site_group_events(sites[s], s, group, seed, ev[s]);
+    for (u64 w = g0; w < std::min<u64>(words, g0 + 32); w++) {
+      const u64 col = col0 + w;
+      const u64 f0 = w * 32, f1 = std::min<u64>(S, f0 + 32);
+      size_t reset_index = 0;
+      u32 rcache[4];
+      u32 rblock = 0xFFFFFFFFu;
+      for (size_t k = 0; k < nops; k++) {
+        const qcb_op& op = ops[k];
+        const u32 oc = op.opcode;
+        if (is_noise(oc)) {
+          const Site& st = sites[(size_t)site_of_op[k]];
+          for (const Event& e : ev[(size_t)site_of_op[k]]) {
+            const u64 f = (g0 + (e.pos >> 5)) * 32 + (e.pos & 31);
+            if (f < f0 || f >= f1) continue;
             if (st.opcode == QCB_OP_DEPOL2) {
-              frame_flip(F, st.q1, f, code & 3);
-              frame_flip(F, st.q2, f, (code >> 2) & 3);
+              frame_flip(F, st.q1, f, e.code & 3);
+              frame_flip(F, st.q2, f, (e.code >> 2) & 3);
             } else {
-              frame_flip(F, st.q1, f, code & 3);
+              frame_flip(F, st.q1, f, e.code & 3);
             }
           }
+          continue;
         }
-        continue;
-      }
-      if (oc == QCB_OP_MRZ || oc == QCB_OP_MRX) {
-        u32 q = op.q1 - 1; u64 m = 1ull << (q & 63);
-        if (oc == QCB_OP_MRX) {
-          for (u64 f = f0; f < f1; f++) {
-            u64 x = (F.xw(q, f) & m) ? 1 : 0, z = (F.zw(q, f) & m) ? 1 : 0;
-            F.xw(q, f) = (F.xw(q, f) & ~m) | (z ? m : 0);
-            F.zw(q, f) = (F.zw(q, f) & ~m) | (x ? m : 0);
+        if (oc == QCB_OP_MRZ || oc == QCB_OP_MRX) {
+          const u32 q = op.q1 - 1;
+          const u64 m = 1ull << (q & 63);
+          if (oc == QCB_OP_MRX) {
+            for (u64 f = f0; f < f1; f++) {
+              const u64 x = (F.xw(q, f) & m) ? 1 : 0, z = (F.zw(q, f) & m) ? 1 : 0;
+              F.xw(q, f) = (F.xw(q, f) & ~m) | (z ? m : 0);
+              F.zw(q, f) = (F.zw(q, f) & ~m) | (x ? m : 0);
+            }
           }
+          if (rblock != (u32)(reset_index >> 2)) {
+            rblock = (u32)(reset_index >> 2);
+            philox_block(seed, rblock, col, TAG_RESET, rcache);
+          }
+          const u32 rb = rcache[reset_index & 3];
+          if (op.bit != 0) {
+            u8* c = F.meas + (size_t)(op.bit - 1) * F.S;
+            for (u64 f = f0; f < f1; f++) c[f] = (F.xw(q, f) & m) ? 1 : 0;
+          }
+          for (u64 f = f0; f < f1; f++) {
+            F.xw(q, f) &= ~m;
+            if ((rb >> (f - f0)) & 1) F.zw(q, f) ^= m;
+          }
+          reset_index++;
+          continue;
         }
-        if (rblock != (u32)(reset_index >> 2)) {
-          rblock = (u32)(reset_index >> 2);
-          philox_block(seed, rblock, col, TAG_RESET, rcache);
-        }
-        u32 rb = rcache[reset_index & 3];
-        if (op.bit != 0) {
-          u8* c = F.meas + (size_t)(op.bit - 1) * F.S;
-          for (u64 f = f0; f < f1; f++) c[f] = (F.xw(q, f) & m) ? 1 : 0;
-        }
-        for (u64 f = f0; f < f1; f++) {
-          F.xw(q, f) &= ~m;
-          if ((rb >> (f - f0)) & 1) F.zw(q, f) ^= m;
-        }
-        reset_index++;
-        continue;
+        NoiseFeed nf;
+        nf.mode = SRC_MASK;
+        frame_op(F, op, k, f0, f1, nf, nullptr, 0);
       }
-      NoiseFeed nf; nf.mode = SRC_MASK;
-      frame_op(F, op, k, f0, f1, nf, nullptr, 0);
     }
   }
 }

@@ -32,7 +32,8 @@
 namespace qcb {
 
 struct WalkArgs {
-  const uint4* prog;
+  const uint4* prog;        // windowed stream (PROG_WINDOW_WORDS words per window)
+  uint32_t nwin;            // windows in the stream
   uint32_t* planes;
   uint32_t* rec;
   uint64_t pitch;
@@ -41,38 +42,21 @@ struct WalkArgs {
   const uint32_t* slot_swap;
   uint32_t nslots;
   uint32_t nq1;
-  uint32_t fresh;          // 1: start from x = 0, z = Philox initZ!
-  uint32_t tile;           // shot columns per tile (multiple of 32)
+  uint32_t fresh;           // 1: start from x = 0, z = Philox initZ!
+  uint32_t tile;            // shot columns per tile (multiple of 32)
   const uint32_t* qubit_slot;
   uint32_t qubit_slot_len;
-  uint32_t nsites;
   uint64_t seed;
-  uint64_t col0;           // global column index of column 0
-  const Site* sites;
+  uint64_t col0;            // global column index of column 0
+  const NoiseClass* classes;
   double pmax;
-  double inv_log1m;
+  int32_t* err;             // set to QCB_ETIMEOUT when a staging wait gives up
   // mask mode
   const uint64_t* ev_off;
   const uint64_t* ev_data;  // (trial << 8) | code, sorted per column
   const uint32_t* reset_planes;
   uint64_t reset_pitch;
 };
-
-__device__ __forceinline__ uint32_t site_code(const Site& s, double v) {
-  if (s.kind == QCB_OP_PAULI_NOISE) {
-    if (v < s.t0) return 1;
-    if (v < s.t1) return 2;
-    if (v < s.t2) return 3;
-    return 0;
-  }
-  const uint32_t np = s.kind == QCB_OP_DEPOL2 ? 15u : 3u;
-  if (v < s.t0) {
-    uint32_t k = (uint32_t)(__dmul_rn(v / s.t0, (double)np));
-    if (k >= np) k = np - 1;
-    return k + 1;
-  }
-  return 0;
-}
 
 // Bit-sliced single-qubit gate (src/symbolic_cliffords.jl:105-118); frames
 // track no phase (src/pauli_frames.jl:58-61).
@@ -122,60 +106,199 @@ struct Tile {
   }
 };
 
-// One noise stream: sites [g*CH, (g+1)*CH) of one shot column, trials
-// tau = (site - g*CH)*32 + lane, geometric gaps at p_max.  Only the events of
-// sites in [lo, hi) are applied (a stream can straddle two flushes; the
-// counter-based generator lets the second flush replay it from the start).
+__device__ __forceinline__ uint32_t sel4(const uint32_t o[4], uint32_t i) {
+  const uint32_t a = (i & 1) ? o[1] : o[0];
+  const uint32_t b = (i & 1) ? o[3] : o[2];
+  return (i & 2) ? b : a;
+}
+
+// ---------------------------------------------------------------- staging
+// The program is staged window by window into two shared-memory buffers with
+// bulk copies (cp.async.bulk, completion on an mbarrier), one window ahead of
+// the walk.  Waits are bounded: on expiry the kernel records QCB_ETIMEOUT.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void stage_window(uint32_t* dst, const uint4* src, uint32_t bytes, uint64_t* bar) {
+  const uint32_t b = smem_addr(bar);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(b)
+      : "memory");
+}
+
+// Returns false when the wait gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t b = smem_addr(bar);
+  for (uint32_t it = 0; it < (1u << 22); it++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(b), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------- noise
+// Event kind of a uniform v in [0, p_eff) (or [0, 1) in dense mode, where
+// v >= p_eff means no event): PauliNoise X / Z / Y by the thresholds,
+// DepolarizationNoise a uniform non-identity Pauli index.
+__device__ __forceinline__ uint32_t event_code(uint32_t kind, const NoiseClass& c, double v) {
+  if (kind == QCB_OP_PAULI_NOISE) {
+    if (v < c.t0) return 1;
+    if (v < c.t1) return 2;
+    if (v < c.t2) return 3;
+    return 0;
+  }
+  const uint32_t np = kind == QCB_OP_DEPOL2 ? 15u : 3u;
+  if (v < c.peff) {
+    uint32_t k = (uint32_t)(__dmul_rn(__ddiv_rn(v, c.peff), (double)np));
+    if (k >= np) k = np - 1;
+    return k + 1;
+  }
+  return 0;
+}
+
+// Flip the event's Pauli into the tile at group-relative shot `pos`.
+// e = (site, kind | class<<8, x_a | z_a<<16, x_b | z_b<<16).
 template <bool SMEM>
-__device__ __forceinline__ void noise_chunk(const WalkArgs& a, const Tile<SMEM>& F, uint32_t cl, uint64_t cg,
-                                            uint32_t col_lo, uint32_t g, uint32_t lo, uint32_t hi) {
-  const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
-  const int64_t span = (int64_t)NOISE_CHUNK * 32;
-  int64_t tau = -1;
-  for (uint32_t draw = 0;; draw++) {
-    uint32_t o[4];
-    philox4x32_10(draw, col_lo, g, TAG_NOISE, k0, k1, o);
-    const uint64_t u53 = ((uint64_t)o[0] << 21) | (o[1] >> 11);
-    const double u = __dmul_rn(__dadd_rn((double)u53, 0.5), 0x1.0p-53);
-    const double gap = a.pmax >= 1.0 ? 0.0 : floor(__dmul_rn(log(u), a.inv_log1m));
-    if (gap >= (double)span) break;
-    tau += 1 + (int64_t)gap;
-    if (tau >= span) break;
-    const uint32_t site = g * NOISE_CHUNK + (uint32_t)(tau >> 5);
-    if (site >= hi) break;
-    if (site < lo) continue;
-    const double v = __dmul_rn(__dmul_rn((double)o[2], 0x1.0p-32), a.pmax);
-    const Site s = a.sites[site];
-    const uint32_t code = site_code(s, v);
-    if (!code) continue;
-    const uint32_t bit = 1u << (tau & 31);
-    if (code & 1) atomicXor(F.at(s.xa, cl, cg), bit);
-    if (code & 2) atomicXor(F.at(s.za, cl, cg), bit);
-    if (s.kind == QCB_OP_DEPOL2) {
-      if (code & 4) atomicXor(F.at(s.xb, cl, cg), bit);
-      if (code & 8) atomicXor(F.at(s.zb, cl, cg), bit);
-    }
+__device__ __forceinline__ void apply_code(const Tile<SMEM>& F, const uint4& e, uint32_t code, uint32_t gl,
+                                           uint32_t pos, uint64_t c0, uint64_t ncols) {
+  const uint32_t cl = gl * 32 + (pos >> 5);
+  const uint64_t cg = c0 + cl;
+  if (cg >= ncols) return;
+  const uint32_t bit = 1u << (pos & 31);
+  if (code & 1) atomicXor(F.at(e.z & 0xFFFFu, cl, cg), bit);
+  if (code & 2) atomicXor(F.at(e.z >> 16, cl, cg), bit);
+  if ((e.y & 0xFFu) == QCB_OP_DEPOL2) {
+    if (code & 4) atomicXor(F.at(e.w & 0xFFFFu, cl, cg), bit);
+    if (code & 8) atomicXor(F.at(e.w >> 16, cl, cg), bit);
   }
 }
 
-// The walker: one CTA owns a tile of T shot columns (T x 32 shots) and runs
-// the whole program on it.  Thread (rr, cl) = (tid / T, tid % T) handles
-// column cl and every R-th op of a segment, so a warp covers 32 columns of one
-// op (conflict-free shared accesses, uniform operand loads); one barrier per
-// segment orders the segments.
+// The events of one noise site on one group of NOISE_GROUP shots (group G of
+// the run, = 32 consecutive shot columns).  Its random words come from Philox
+// blocks (site, G, block index, TAG_NOISE).
+//  sparse: word 0 gives the event count k ~ Binomial(NOISE_GROUP, p_eff) by
+//          inverse CDF; each event then takes a position word (uniform in the
+//          group, redrawn if the shot already has an event of this site) and
+//          a kind word (uniform in [0, p_eff)).  Given k the positions are a
+//          uniform k-subset, so every shot gets an event independently with
+//          probability p_eff, as the reference's per-frame draws.
+//  dense:  word j is the per-shot uniform of shot j.
+template <bool SMEM>
+__device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<SMEM>& F, const uint4& e,
+                                                  uint64_t G, uint32_t gl, uint64_t c0) {
+  const uint32_t site = e.x, kind = e.y & 0xFFu;
+  const NoiseClass c = a.classes[e.y >> 8];
+  if (!(c.peff > 0.0)) return;
+  const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
+  const uint32_t glo = (uint32_t)G;
+  uint32_t o[4];
+  if (c.dense) {
+    for (uint32_t blk = 0; blk < NOISE_GROUP / 4; blk++) {
+      philox4x32_10(site, glo, blk, TAG_NOISE, k0, k1, o);
+#pragma unroll
+      for (uint32_t j = 0; j < 4; j++) {
+        const double u = __dmul_rn((double)o[j], 0x1.0p-32);
+        const uint32_t code = event_code(kind, c, u);
+        if (code) apply_code<SMEM>(F, e, code, gl, blk * 4 + j, c0, a.ncols);
+      }
+    }
+    return;
+  }
+  philox4x32_10(site, glo, 0u, TAG_NOISE, k0, k1, o);
+  const double u = __dmul_rn(__dadd_rn((double)o[0], 0.5), 0x1.0p-32);
+  uint32_t k = 0;
+  double pk = c.q0, cum = c.q0;
+  while (u > cum && k < NOISE_GROUP) {
+    pk = __ddiv_rn(__dmul_rn(pk, __dmul_rn((double)(NOISE_GROUP - k), c.r)), (double)(k + 1));
+    k++;
+    cum = __dadd_rn(cum, pk);
+  }
+  if (k == 0) return;
+  uint32_t blk = 0, widx = 1;
+  uint32_t p0 = 0xFFFFFFFFu, p1 = 0xFFFFFFFFu, p2 = 0xFFFFFFFFu, p3 = 0xFFFFFFFFu;
+  uint32_t bm[NOISE_GROUP / 32];  // used positions when k > 4
+  if (k > 4)
+    for (uint32_t i = 0; i < NOISE_GROUP / 32; i++) bm[i] = 0;
+  for (uint32_t ev = 0; ev < k; ev++) {
+    uint32_t pos, tw;
+    while (true) {
+      // words widx (position) and widx + 1 (kind)
+      if ((widx >> 2) != blk) { blk = widx >> 2; philox4x32_10(site, glo, blk, TAG_NOISE, k0, k1, o); }
+      pos = sel4(o, widx & 3) & (NOISE_GROUP - 1);
+      widx++;
+      if ((widx >> 2) != blk) { blk = widx >> 2; philox4x32_10(site, glo, blk, TAG_NOISE, k0, k1, o); }
+      tw = sel4(o, widx & 3);
+      widx++;
+      bool dup;
+      if (k > 4) {
+        dup = (bm[pos >> 5] >> (pos & 31)) & 1u;
+        if (!dup) bm[pos >> 5] |= 1u << (pos & 31);
+      } else {
+        dup = pos == p0 || pos == p1 || pos == p2 || pos == p3;
+        if (!dup) { if (ev == 0) p0 = pos; else if (ev == 1) p1 = pos; else if (ev == 2) p2 = pos; else p3 = pos; }
+      }
+      if (!dup) break;
+    }
+    const double v = __dmul_rn(__dmul_rn((double)tw, 0x1.0p-32), c.peff);
+    const uint32_t code = event_code(kind, c, v);
+    if (code) apply_code<SMEM>(F, e, code, gl, pos, c0, a.ncols);
+  }
+}
+
+// ---------------------------------------------------------------- walker
+// One CTA owns a tile of T shot columns (T x 32 shots) and runs the whole
+// program on it.  Thread (rr, cl) = (tid / T, tid % T) handles column cl and
+// every R-th op of a segment, so a warp covers 32 columns of one op
+// (conflict-free shared accesses, broadcast operand reads from the staged
+// window); one barrier per segment orders the segments.
 template <bool SMEM, bool PHILOX>
-__global__ void __launch_bounds__(1024, 1) walker_kernel(const WalkArgs a) {
-  extern __shared__ __align__(16) uint32_t sm[];
+__global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
+  extern __shared__ __align__(128) uint32_t sm[];
   const uint32_t tid = threadIdx.x, T = a.tile, R = blockDim.x / T;
   const uint32_t cl = tid % T, rr = tid / T;
   const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
   const uint64_t pitch = a.pitch;
-  if (!SMEM) {
+  // layout: [frame tile | pmap] [window 0] [window 1] [2 mbarriers]
+  const uint32_t tile_words = SMEM ? 2 * a.nslots * T : 2 * a.nslots;
+  uint32_t* win0 = sm + ((tile_words + 31) & ~31u);
+  uint32_t* win1 = win0 + PROG_WINDOW_WORDS;
+  uint64_t* bars = (uint64_t*)(win1 + PROG_WINDOW_WORDS);
+  if (!SMEM)
     for (uint32_t p = tid; p < 2 * a.nslots; p += blockDim.x) sm[p] = 2 * a.slot_qubit[p >> 1] + (p & 1);
-    __syncthreads();
-  }
   const uint64_t ntiles = (a.ncols + T - 1) / T;
-  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  const uint64_t my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint64_t total_win = my_tiles * a.nwin;  // windows this CTA walks
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // window k of the flattened (tile, window) sequence lives in buffer k & 1
+  auto issue = [&](uint64_t k) {
+    if (k >= total_win) return;
+    const uint32_t w = (uint32_t)(k % a.nwin);
+    stage_window((k & 1) ? win1 : win0, a.prog + (size_t)w * (PROG_WINDOW_WORDS / 4), PROG_WINDOW_WORDS * 4,
+                 &bars[k & 1]);
+  };
+  if (tid == 0) { issue(0); issue(1); }
+  uint64_t kwin = 0;
+  bool failed = false;
+
+  for (uint64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
     const uint64_t c0 = tile * T, cg = c0 + cl;
     const bool act = rr < R && cg < a.ncols;
     const uint64_t col = a.col0 + cg;
@@ -215,44 +338,65 @@ __global__ void __launch_bounds__(1024, 1) walker_kernel(const WalkArgs a) {
       ep = a.ev_off[cg];
       ee = a.ev_off[cg + 1];
     }
-    __syncthreads();
 
-    // ---- the program
-    const uint4* pc = a.prog;
-    while (true) {
-      const uint4 h = __ldg(pc++);
+    // ---- the program, window by window
+    const uint32_t* wp = nullptr;
+    bool need_window = true;
+    bool done = false;
+    while (!done) {
+      if (need_window) {
+        const bool ok = mbar_wait(&bars[kwin & 1], (uint32_t)((kwin >> 1) & 1));
+        if (__syncthreads_or(!ok)) {  // every thread takes the same branch
+          if (tid == 0) atomicExch(a.err, QCB_ETIMEOUT);
+          failed = true;
+          break;
+        }
+        wp = (kwin & 1) ? win1 : win0;
+        need_window = false;
+      }
+      __syncthreads();  // the tile init / the previous record is complete
+      const uint4 h = *(const uint4*)wp;
       const uint32_t kind = h.x >> 24, cnt = h.x & 0xFFFFFFu;
-      if (kind == SEG_END) break;
+      const uint32_t* e = wp + 4;
       switch (kind) {
+        case SEG_END:
+          done = true;
+          break;
+        case SEG_WIN:
+          break;
         case SEG_CNOT: {
-          const uint4* e = pc;
-          pc += cnt;
+          wp = e + ((cnt * 2 + 3) & ~3u);
           if (!act) break;
+          const uint2* en = (const uint2*)e;
           uint32_t j = rr;
           for (; j + R < cnt; j += 2 * R) {
-            const uint4 o = __ldg(e + j), u = __ldg(e + j + R);
-            uint32_t *pxc = F.at(o.x, cl, cg), *pzc = F.at(o.y, cl, cg), *pxt = F.at(o.z, cl, cg), *pzt = F.at(o.w, cl, cg);
-            uint32_t *qxc = F.at(u.x, cl, cg), *qzc = F.at(u.y, cl, cg), *qxt = F.at(u.z, cl, cg), *qzt = F.at(u.w, cl, cg);
+            const uint2 o = en[j], u = en[j + R];
+            uint32_t *pxc = F.at(o.x & 0xFFFFu, cl, cg), *pzc = F.at(o.x >> 16, cl, cg);
+            uint32_t *pxt = F.at(o.y & 0xFFFFu, cl, cg), *pzt = F.at(o.y >> 16, cl, cg);
+            uint32_t *qxc = F.at(u.x & 0xFFFFu, cl, cg), *qzc = F.at(u.x >> 16, cl, cg);
+            uint32_t *qxt = F.at(u.y & 0xFFFFu, cl, cg), *qzt = F.at(u.y >> 16, cl, cg);
             const uint32_t xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
             const uint32_t yxc = *qxc, yzc = *qzc, yxt = *qxt, yzt = *qzt;
             *pxt = xt ^ xc; *pzc = zc ^ zt;
             *qxt = yxt ^ yxc; *qzc = yzc ^ yzt;
           }
           for (; j < cnt; j += R) {
-            const uint4 o = __ldg(e + j);
-            uint32_t *pxc = F.at(o.x, cl, cg), *pzc = F.at(o.y, cl, cg), *pxt = F.at(o.z, cl, cg), *pzt = F.at(o.w, cl, cg);
+            const uint2 o = en[j];
+            uint32_t *pxc = F.at(o.x & 0xFFFFu, cl, cg), *pzc = F.at(o.x >> 16, cl, cg);
+            uint32_t *pxt = F.at(o.y & 0xFFFFu, cl, cg), *pzt = F.at(o.y >> 16, cl, cg);
             const uint32_t xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
             *pxt = xt ^ xc; *pzc = zc ^ zt;
           }
           break;
         }
         case SEG_CZ: {
-          const uint4* e = pc;
-          pc += cnt;
+          wp = e + ((cnt * 2 + 3) & ~3u);
           if (!act) break;
+          const uint2* en = (const uint2*)e;
           for (uint32_t j = rr; j < cnt; j += R) {
-            const uint4 o = __ldg(e + j);
-            uint32_t *pxa = F.at(o.x, cl, cg), *pza = F.at(o.y, cl, cg), *pxb = F.at(o.z, cl, cg), *pzb = F.at(o.w, cl, cg);
+            const uint2 o = en[j];
+            uint32_t *pxa = F.at(o.x & 0xFFFFu, cl, cg), *pza = F.at(o.x >> 16, cl, cg);
+            uint32_t *pxb = F.at(o.y & 0xFFFFu, cl, cg), *pzb = F.at(o.y >> 16, cl, cg);
             const uint32_t xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
             *pza = za ^ xb; *pzb = zb ^ xa;
           }
@@ -260,68 +404,69 @@ __global__ void __launch_bounds__(1024, 1) walker_kernel(const WalkArgs a) {
         }
         case SEG_S:
         case SEG_G1: {
-          const uint4* e = pc;
-          pc += cnt;
+          wp = e + ((cnt * 2 + 3) & ~3u);
           if (!act) break;
+          const uint2* en = (const uint2*)e;
           for (uint32_t j = rr; j < cnt; j += R) {
-            const uint4 o = __ldg(e + j);
-            uint32_t *px = F.at(o.x, cl, cg), *pz = F.at(o.y, cl, cg);
+            const uint2 o = en[j];
+            uint32_t *px = F.at(o.x & 0xFFFFu, cl, cg), *pz = F.at(o.x >> 16, cl, cg);
             uint32_t x = *px, z = *pz;
             if (kind == SEG_S) z ^= x;
-            else gate1_xz(o.z, x, z);
+            else gate1_xz(o.y, x, z);
             *px = x; *pz = z;
           }
           break;
         }
         case SEG_G2: {
-          const uint4* e = pc;
-          pc += 2 * cnt;
+          wp = e + cnt * 4;
           if (!act) break;
+          const uint4* en = (const uint4*)e;
           for (uint32_t j = rr; j < cnt; j += R) {
-            const uint4 o = __ldg(e + 2 * j), o2 = __ldg(e + 2 * j + 1);
-            uint32_t *pxa = F.at(o.y, cl, cg), *pza = F.at(o.z, cl, cg), *pxb = F.at(o.w, cl, cg), *pzb = F.at(o2.x, cl, cg);
+            const uint4 o = en[j];
+            uint32_t *pxa = F.at(o.x & 0xFFFFu, cl, cg), *pza = F.at(o.x >> 16, cl, cg);
+            uint32_t *pxb = F.at(o.y & 0xFFFFu, cl, cg), *pzb = F.at(o.y >> 16, cl, cg);
             uint32_t xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
-            gate2_xz(o.x, xa, za, xb, zb);
+            gate2_xz(o.z, xa, za, xb, zb);
             *pxa = xa; *pza = za; *pxb = xb; *pzb = zb;
           }
           break;
         }
         case SEG_MZ: {
-          const uint2* e = (const uint2*)pc;
-          pc += (cnt * 2 + 3) / 4;
+          wp = e + ((cnt * 2 + 3) & ~3u);
           if (!act) break;
+          const uint2* en = (const uint2*)e;
           for (uint32_t j = rr; j < cnt; j += R) {
-            const uint2 o = __ldg(e + j);
+            const uint2 o = en[j];
             a.rec[(uint64_t)o.y * pitch + cg] = *F.at(o.x, cl, cg);
           }
           break;
         }
         case SEG_MRZ: {
-          const uint4* e = pc;
-          pc += 4 * cnt;
+          wp = e + cnt * 16;
           if (!act) break;
+          const uint4* en = (const uint4*)e;
           for (uint32_t g = rr; g < cnt; g += R) {
             uint4 ent[4];
 #pragma unroll
-            for (int i = 0; i < 4; i++) ent[i] = __ldg(e + 4 * g + i);
+            for (int i = 0; i < 4; i++) ent[i] = en[4 * g + i];
             uint32_t o[4] = {0, 0, 0, 0};
             if (PHILOX) {
               uint32_t blk = 0;
 #pragma unroll
               for (int i = 0; i < 4; i++)
-                if (ent[i].w != MRZ_PAD) blk = ent[i].w >> 2;
+                if (ent[i].z != MRZ_PAD) blk = ent[i].z >> 2;
               philox4x32_10(blk, clo, chi, TAG_RESET, k0, k1, o);
             }
 #pragma unroll
             for (int i = 0; i < 4; i++) {
-              if (ent[i].w == MRZ_PAD) continue;
-              uint32_t* px = F.at(ent[i].x, cl, cg);
-              uint32_t* pz = F.at(ent[i].y, cl, cg);
+              if (ent[i].z == MRZ_PAD) continue;
+              uint32_t* px = F.at(ent[i].x & 0xFFFFu, cl, cg);
+              uint32_t* pz = F.at(ent[i].x >> 16, cl, cg);
               const uint32_t x = *px, z = *pz;
               uint32_t rb;
               if (PHILOX) rb = o[i];
-              else rb = a.reset_planes ? __ldg(a.reset_planes + (uint64_t)ent[i].w * a.reset_pitch + cg) : 0u;
-              if (ent[i].z != BIT_NONE) a.rec[(uint64_t)ent[i].z * pitch + cg] = x;
+              else rb = a.reset_planes ? __ldg(a.reset_planes + (uint64_t)ent[i].z * a.reset_pitch + cg) : 0u;
+              if (ent[i].y != BIT_NONE) a.rec[(uint64_t)ent[i].y * pitch + cg] = x;
               *px = 0u;
               *pz = z ^ rb;
             }
@@ -329,27 +474,25 @@ __global__ void __launch_bounds__(1024, 1) walker_kernel(const WalkArgs a) {
           break;
         }
         case SEG_FLUSH: {
-          // cnt runs of site indices (begin, end), two runs per record
-          const uint2* runs = (const uint2*)pc;
-          pc += (cnt + 1) / 2;
-          if (!act) break;
+          wp = e + cnt * 4;
+          const uint4* en = (const uint4*)e;
           if (PHILOX) {
             if (a.pmax > 0.0) {
-              // (run, chunk) tasks, dealt round-robin over the R threads of a column
-              uint32_t idx = 0;
-              for (uint32_t r = 0; r < cnt; r++) {
-                const uint2 run = __ldg(runs + r);
-                const uint32_t g0 = run.x / NOISE_CHUNK, g1 = (run.y - 1) / NOISE_CHUNK;
-                for (uint32_t g = g0; g <= g1; g++, idx++)
-                  if (idx % R == rr) noise_chunk<SMEM>(a, F, cl, cg, clo, g, run.x, run.y);
+              // (site, shot group) tasks over all threads of the CTA; a group is
+              // 32 tile columns
+              const uint32_t ng = T / 32;
+              const uint64_t G0 = (a.col0 + c0) / 32;
+              const uint32_t ntask = cnt * ng;
+              for (uint32_t t = tid; t < ntask; t += blockDim.x) {
+                const uint32_t i = t / ng, gl = t - i * ng;
+                sample_site_group<SMEM>(a, F, en[i], G0 + gl, gl, c0);
               }
             }
-          } else if (rr == 0) {
-            // this column's events are sorted by trial; runs are not visited in
-            // site order, so find the first event of each run
-            for (uint32_t r = 0; r < cnt; r++) {
-              const uint2 run = __ldg(runs + r);
-              const uint64_t lo_t = (uint64_t)run.x * 32u, lim = (uint64_t)run.y * 32u;
+          } else if (rr == 0 && act) {
+            // this column's events are sorted by trial (site*32 + lane)
+            for (uint32_t i = 0; i < cnt; i++) {
+              const uint4 st = en[i];
+              const uint64_t lo_t = (uint64_t)st.x * 32u, lim = lo_t + 32u;
               uint64_t lo = ep, hi = ee;
               while (lo < hi) {
                 const uint64_t mid = (lo + hi) >> 1;
@@ -360,13 +503,12 @@ __global__ void __launch_bounds__(1024, 1) walker_kernel(const WalkArgs a) {
                 const uint64_t d = __ldg(a.ev_data + k);
                 const uint64_t t = d >> 8;
                 if (t >= lim) break;
-                const Site s = a.sites[(uint32_t)(t >> 5)];
                 const uint32_t code = (uint32_t)(d & 0xFF), bit = 1u << (t & 31);
-                if (code & 1) *F.at(s.xa, cl, cg) ^= bit;
-                if (code & 2) *F.at(s.za, cl, cg) ^= bit;
-                if (s.kind == QCB_OP_DEPOL2) {
-                  if (code & 4) *F.at(s.xb, cl, cg) ^= bit;
-                  if (code & 8) *F.at(s.zb, cl, cg) ^= bit;
+                if (code & 1) *F.at(st.z & 0xFFFFu, cl, cg) ^= bit;
+                if (code & 2) *F.at(st.z >> 16, cl, cg) ^= bit;
+                if ((st.y & 0xFFu) == QCB_OP_DEPOL2) {
+                  if (code & 4) *F.at(st.w & 0xFFFFu, cl, cg) ^= bit;
+                  if (code & 8) *F.at(st.w >> 16, cl, cg) ^= bit;
                 }
               }
             }
@@ -374,10 +516,21 @@ __global__ void __launch_bounds__(1024, 1) walker_kernel(const WalkArgs a) {
           break;
         }
         default:
+          done = true;
           break;
       }
-      __syncthreads();
+      if (kind == SEG_WIN || kind == SEG_END) {
+        __syncthreads();  // every thread is done with this window
+        if (tid == 0) issue(kwin + 2);
+        kwin++;
+        need_window = true;
+        if (kind == SEG_END) break;
+      } else if (h.y & FLAG_NO_BARRIER) {
+        // a part of a split record: the next part needs no barrier, but the
+        // loop head has one; harmless
+      }
     }
+    if (failed) break;
 
     // ---- write the frame back, undoing the x<->z relabels
     for (uint32_t s = rr; s < a.nslots; s += R) {
@@ -395,6 +548,12 @@ __global__ void __launch_bounds__(1024, 1) walker_kernel(const WalkArgs a) {
       }
     }
     __syncthreads();
+  }
+  // no bulk copy may still be in flight when the CTA exits
+  if (failed) {
+    __syncthreads();
+    if (tid == 0)
+      for (uint64_t k = kwin; k < kwin + 2 && k < total_win; k++) mbar_wait(&bars[k & 1], (uint32_t)((k >> 1) & 1));
   }
 }
 
@@ -473,6 +632,14 @@ static int check_frame(const qcb_frame* f) {
   return QCB_OK;
 }
 
+// After a synchronising call: report a device-side wait that gave up.
+static int frame_device_status(const qcb_frame* f) {
+  int32_t h = 0;
+  if (cudaMemcpy(&h, f->err, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return QCB_OK;
+  if (h) return fail(h, "a device-side wait of the frame walker expired; the frame contents are not valid");
+  return QCB_OK;
+}
+
 extern "C" {
 
 int qcb_frame_create(uint64_t frames, uint32_t qubits, uint32_t nbits, qcb_frame** out) {
@@ -490,10 +657,12 @@ int qcb_frame_create(uint64_t frames, uint32_t qubits, uint32_t nbits, qcb_frame
   size_t rbytes = (size_t)std::max<uint32_t>(nbits, 1) * f->pitch * 4;
   cudaError_t e = cudaMalloc(&f->planes, pbytes);
   if (e == cudaSuccess) e = cudaMalloc(&f->record, rbytes);
+  if (e == cudaSuccess) e = cudaMalloc(&f->err, 16);
+  if (e == cudaSuccess) e = cudaMemset(f->err, 0, 16);
   if (e == cudaSuccess) e = cudaMemset(f->planes, 0, pbytes);
   if (e == cudaSuccess) e = cudaMemset(f->record, 0, rbytes);
   if (e != cudaSuccess) {
-    cudaFree(f->planes); cudaFree(f->record);
+    cudaFree(f->planes); cudaFree(f->record); cudaFree(f->err);
     delete f;
     return cuda_fail(e, "qcb_frame_create");
   }
@@ -505,6 +674,7 @@ int qcb_frame_destroy(qcb_frame* f) {
   if (!f) return QCB_OK;
   cudaFree(f->planes);
   cudaFree(f->record);
+  cudaFree(f->err);
   delete f;
   return QCB_OK;
 }
@@ -567,25 +737,27 @@ static uint32_t g_tile_override = 0;
 static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   WalkConfig wc{};
   const size_t per_col = (size_t)2 * std::max<uint32_t>(p->nslots, 1) * 4;
+  const size_t stage = (size_t)2 * PROG_WINDOW_WORDS * 4 + 16 + 128;  // windows, mbarriers, alignment
   const size_t maxsm = (size_t)device_max_smem_optin();
+  const size_t budget = maxsm > stage ? maxsm - stage : 0;
   uint32_t T = 0;
-  if (g_tile_override && per_col * g_tile_override <= maxsm) {
+  if (g_tile_override && per_col * g_tile_override <= budget) {
     T = g_tile_override;
   } else {
-    const uint32_t cands[] = {64, 96, 32};
+    const uint32_t cands[] = {96, 64, 32};
     for (uint32_t c : cands)
-      if (per_col * c <= maxsm) { T = c; break; }
+      if (per_col * c <= budget) { T = c; break; }
   }
   if (T) {
     wc.smem = true;
     wc.T = T;
-    wc.nth = T == 96 ? 768u : 1024u;
-    wc.smem_bytes = per_col * T;
+    wc.nth = (768u / T) * T;  // the kernel is compiled for at most 768 threads
+    wc.smem_bytes = per_col * T + stage;
   } else {
     wc.smem = false;
     wc.T = 128;
-    wc.nth = 1024;
-    wc.smem_bytes = (size_t)2 * p->nslots * 4;
+    wc.nth = 768;
+    wc.smem_bytes = (size_t)2 * p->nslots * 4 + stage;
   }
   const uint64_t tiles = (f->ncols + wc.T - 1) / wc.T;
   wc.grid = (uint32_t)std::min<uint64_t>(tiles ? tiles : 1, 1u << 30);
@@ -621,10 +793,11 @@ static void fill_common(WalkArgs& a, qcb_frame* f, const qcb_program* p) {
   a.nq1 = f->nq1;
   a.qubit_slot = p->d_qubit_slot;
   a.qubit_slot_len = p->qubit_slot_len;
-  a.nsites = p->info.n_noise_sites;
-  a.sites = p->d_sites_slot;
+  a.prog = (const uint4*)p->d_stream_slot;
+  a.nwin = (uint32_t)(p->stream_slot.size() / PROG_WINDOW_WORDS);
+  a.classes = p->d_classes;
   a.pmax = p->pmax;
-  a.inv_log1m = p->inv_log1m;
+  a.err = f->err;
 }
 
 static int check_run(const qcb_frame* f, const qcb_program* p, const qcb_noise_source* n) {
@@ -635,8 +808,9 @@ static int check_run(const qcb_frame* f, const qcb_program* p, const qcb_noise_s
   if (p->info.nbits > f->nbits)
     return fail(QCB_EBOUNDS, "program records bit " + std::to_string(p->info.nbits) +
                                  " but the frame has " + std::to_string(f->nbits));
-  if (n->shot_offset % 32) return fail(QCB_EARG, "shot_offset must be a multiple of 32");
   if (n->mode != QCB_NOISE_PHILOX && n->mode != QCB_NOISE_MASK) return fail(QCB_EARG, "bad noise mode");
+  if (n->shot_offset % (n->mode == QCB_NOISE_PHILOX ? NOISE_GROUP : 32))
+    return fail(QCB_EARG, "shot_offset must be a multiple of 1024 (Philox mode) or 32 (mask mode)");
   return QCB_OK;
 }
 
@@ -760,7 +934,7 @@ int qcb_frame_download_measurements(const qcb_frame* f, uint8_t* bools, void* st
   QCB_CUDA(cudaMemcpyAsync(bools, d, bytes, cudaMemcpyDeviceToHost, S(stream)));
   QCB_CUDA(cudaFreeAsync(d, S(stream)));
   QCB_CUDA(cudaStreamSynchronize(S(stream)));
-  return QCB_OK;
+  return frame_device_status(f);
 }
 
 int qcb_frame_download_record_planes(const qcb_frame* f, uint32_t* planes, void* stream) {
@@ -769,7 +943,7 @@ int qcb_frame_download_record_planes(const qcb_frame* f, uint32_t* planes, void*
   QCB_CUDA(cudaMemcpy2DAsync(planes, f->ncols * 4, f->record, f->pitch * 4, f->ncols * 4, f->nbits,
                              cudaMemcpyDeviceToHost, S(stream)));
   QCB_CUDA(cudaStreamSynchronize(S(stream)));
-  return QCB_OK;
+  return frame_device_status(f);
 }
 
 int qcb_frame_download_planes(const qcb_frame* f, uint32_t* xp, uint32_t* zp, void* stream) {

@@ -24,6 +24,8 @@
 #include <cmath>
 #include <cstring>
 #include <algorithm>
+#include <map>
+#include <tuple>
 #include <unordered_map>
 #include <unordered_set>
 
@@ -65,6 +67,32 @@ struct Emitter {
   uint32_t pz(uint32_t q) const { uint32_t s = slot[q]; return 2 * s + (swp[s] ? 0 : 1); }
   void pad4() { while (out.size() % 4) out.push_back(0); }
 };
+
+// Event probabilities of a noise site.  PauliNoise (src/pauli_frames.jl:157-174):
+// X below px, Z below px+pz, Y below px+pz+py.  DepolarizationNoise(p) on k
+// qubits (src/noise.jl:122-132): a uniform Pauli of the 4^k with probability p,
+// so a non-identity one with p_eff = p (4^k-1)/4^k, uniform over those.
+void fill_site_probabilities(Site& s, const qcb_op& op) {
+  if (op.opcode == QCB_OP_PAULI_NOISE) {
+    s.t0 = op.p[0];
+    s.t1 = op.p[0] + op.p[2];
+    s.t2 = op.p[0] + op.p[2] + op.p[1];
+    s.peff = s.t2;
+  } else {
+    const double np = op.opcode == QCB_OP_DEPOL2 ? 15.0 : 3.0;
+    s.peff = op.p[0] * np / (np + 1.0);
+    s.t0 = s.t1 = s.t2 = s.peff;
+  }
+  if (s.peff > 1.0) s.peff = 1.0;
+  s.dense = s.peff * NOISE_GROUP > NOISE_DENSE_LAMBDA ? 1u : 0u;
+  if (s.peff < 1.0) {
+    s.q0 = std::pow(1.0 - s.peff, (double)NOISE_GROUP);
+    s.r = s.peff / (1.0 - s.peff);
+  } else {
+    s.q0 = 0.0;
+    s.r = 0.0;
+  }
+}
 
 int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   std::memset(&P.info, 0, sizeof(P.info));
@@ -154,39 +182,46 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
 
   double pmax = 0;
   uint32_t nseg = 0, nflush = 0;
+  if (2ull * P.nslots > 65536) return fail(QCB_EUNSUPPORTED, "at most 32768 distinct qubits per program");
 
-  // Emits one segment of ops of one kind (all at one level: disjoint qubits).
+  // Noise probability classes: sites with equal probabilities share one entry.
+  std::vector<NoiseClass> classes;
+  std::map<std::tuple<double, double, double, double>, uint32_t> class_of;
+  auto class_id = [&](const Site& s) -> uint32_t {
+    auto key = std::make_tuple(s.t0, s.t1, s.t2, s.peff);
+    auto it = class_of.find(key);
+    if (it != class_of.end()) return it->second;
+    NoiseClass c{s.t0, s.t1, s.t2, s.peff, s.q0, s.r, s.dense, 0};
+    classes.push_back(c);
+    return class_of[key] = (uint32_t)(classes.size() - 1);
+  };
+
+  // Records before windowing: fixed-size entries of one kind.
+  struct Rec { uint32_t kind, entry_words; std::vector<uint32_t> w; };
+  std::vector<Rec> recs;
+  auto pk = [](uint32_t a, uint32_t b) { return a | (b << 16); };
   auto emit_seg = [&](uint32_t kind, std::vector<LOp>& seg) {
     if (seg.empty()) return;
-    auto& out = P.stream_slot;
-    const size_t hdr = out.size();
-    out.push_back(0); out.push_back(0); out.push_back(0); out.push_back(0);
-    uint32_t cnt = 0;
+    Rec r{kind, 2, {}};
     switch (kind) {
       case SEG_CNOT:
-      case SEG_CZ:  // (x_a, z_a, x_b, z_b)
-        for (auto& o : seg) { out.push_back(o.xa); out.push_back(o.za); out.push_back(o.xb); out.push_back(o.zb); }
-        cnt = (uint32_t)seg.size();
+      case SEG_CZ:  // (x_a | z_a << 16, x_b | z_b << 16)
+        for (auto& o : seg) { r.w.push_back(pk(o.xa, o.za)); r.w.push_back(pk(o.xb, o.zb)); }
         break;
-      case SEG_S:  // (x, z, opcode, 0)
-      case SEG_G1:
-        for (auto& o : seg) { out.push_back(o.xa); out.push_back(o.za); out.push_back(o.opcode); out.push_back(0); }
-        cnt = (uint32_t)seg.size();
+      case SEG_S:
+      case SEG_G1:  // (x | z << 16, opcode)
+        for (auto& o : seg) { r.w.push_back(pk(o.xa, o.za)); r.w.push_back(o.opcode); }
         break;
-      case SEG_G2:  // (opcode, x_a, z_a, x_b), (z_b, 0, 0, 0)
-        for (auto& o : seg) {
-          out.push_back(o.opcode); out.push_back(o.xa); out.push_back(o.za); out.push_back(o.xb);
-          out.push_back(o.zb); out.push_back(0); out.push_back(0); out.push_back(0);
-        }
-        cnt = (uint32_t)seg.size();
+      case SEG_G2:  // (x_a | z_a << 16, x_b | z_b << 16, opcode, 0)
+        r.entry_words = 4;
+        for (auto& o : seg) { r.w.push_back(pk(o.xa, o.za)); r.w.push_back(pk(o.xb, o.zb)); r.w.push_back(o.opcode); r.w.push_back(0); }
         break;
       case SEG_MZ:  // (x, bit)
-        for (auto& o : seg) { out.push_back(o.xa); out.push_back(o.bit); }
-        cnt = (uint32_t)seg.size();
-        E.pad4();
+        for (auto& o : seg) { r.w.push_back(o.xa); r.w.push_back(o.bit); }
         break;
-      case SEG_MRZ: {  // groups of 4 entries (x, z, bit, reset | PAD): entry i of a group holds
-                       // reset 4*block + i, so one Philox block serves the group
+      case SEG_MRZ: {  // groups of 4 entries (x | z << 16, bit, reset | PAD, 0); entry i of a group
+                       // holds reset 4*block + i, so one Philox block serves the group
+        r.entry_words = 16;
         std::sort(seg.begin(), seg.end(), [](const LOp& a, const LOp& b) { return a.reset < b.reset; });
         size_t i = 0;
         while (i < seg.size()) {
@@ -195,28 +230,32 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
           while (i < seg.size() && (seg[i].reset >> 2) == blk) { ent[seg[i].reset & 3] = &seg[i]; i++; }
           for (int k = 0; k < 4; k++) {
             const LOp* o = ent[k];
-            if (o) { out.push_back(o->xa); out.push_back(o->za); out.push_back(o->bit); out.push_back(o->reset); }
-            else { out.push_back(0); out.push_back(0); out.push_back(BIT_NONE); out.push_back(MRZ_PAD); }
+            if (o) { r.w.push_back(pk(o->xa, o->za)); r.w.push_back(o->bit); r.w.push_back(o->reset); r.w.push_back(0); }
+            else { r.w.push_back(0); r.w.push_back(BIT_NONE); r.w.push_back(MRZ_PAD); r.w.push_back(0); }
           }
-          cnt++;
         }
         break;
       }
       default: break;
     }
-    out[hdr] = (kind << 24) | cnt;
+    recs.push_back(std::move(r));
     nseg++;
   };
-  // One FLUSH record per set of sites: header [FLUSH<<24 | nranges], then the
-  // runs of consecutive site indices as (begin, end) pairs, padded to 16 bytes.
-  auto emit_flush = [&](const std::vector<std::pair<uint32_t, uint32_t>>& runs) {
-    if (runs.empty()) return;
-    auto& out = P.stream_slot;
-    out.push_back((SEG_FLUSH << 24) | (uint32_t)runs.size());
-    out.push_back(0); out.push_back(0); out.push_back(0);
-    for (auto& r : runs) { out.push_back(r.first); out.push_back(r.second); }
-    E.pad4();
+  // FLUSH: one entry per site (site, kind | class << 8, x_a | z_a << 16, x_b | z_b << 16).
+  auto emit_sites = [&](std::vector<uint32_t>& st) {
+    if (st.empty()) return;
+    std::sort(st.begin(), st.end());
+    Rec r{SEG_FLUSH, 4, {}};
+    for (uint32_t si : st) {
+      const Site& s = P.sites_slot[si];
+      r.w.push_back(si);
+      r.w.push_back(s.kind | (class_id(s) << 8));
+      r.w.push_back(pk(s.xa, s.za));
+      r.w.push_back(pk(s.xb, s.zb));
+    }
+    recs.push_back(std::move(r));
     nflush++;
+    st.clear();
   };
 
   // Scheduling, in program order.  The open segment collects ops of one kind
@@ -224,33 +263,21 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   // pre-flush (applied before the segment) when the segment does not touch its
   // qubits -- every earlier op on them is in an emitted segment -- and
   // otherwise to the post-flush, which is applied before the next segment.  An
-  // op that touches a qubit with post-flush noise, overlaps the segment or has
-  // another kind closes the segment.  Flips commute with ops on other qubits,
-  // so the result equals op-by-op execution, and a circuit written in layers
-  // (noise after each gate, measurement flips before each reset) gets one
-  // flush per layer.
+  // op that touches a qubit with post-flush noise, overlaps the segment, writes
+  // a record bit the segment writes, or has another kind closes the segment.
+  // Flips commute with ops on other qubits, so the result equals op-by-op
+  // execution, and a circuit written in layers (noise after each gate,
+  // measurement flips before each reset) gets one flush per layer.
   std::vector<LOp> cur;
   uint32_t cur_kind = SEG_END;
-  std::unordered_set<uint32_t> cur_q, post_q;
+  std::unordered_set<uint32_t> cur_q, post_q, cur_bits;
   std::vector<uint32_t> pre, post;
-  auto emit_sites = [&](std::vector<uint32_t>& st) {
-    std::sort(st.begin(), st.end());
-    std::vector<std::pair<uint32_t, uint32_t>> runs;
-    size_t i = 0;
-    while (i < st.size()) {  // runs of consecutive site indices
-      size_t j = i + 1;
-      while (j < st.size() && st[j] == st[j - 1] + 1) j++;
-      runs.push_back({st[i], st[j - 1] + 1});
-      i = j;
-    }
-    emit_flush(runs);
-    st.clear();
-  };
   auto close_seg = [&]() {
     emit_sites(pre);
     emit_seg(cur_kind, cur);
     cur.clear();
     cur_q.clear();
+    cur_bits.clear();
     cur_kind = SEG_END;
     pre.swap(post);
     post_q.clear();
@@ -267,17 +294,8 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
         touches = touches || cur_q.count(o.q2) > 0;
         P.site_arity[(size_t)o.site] = 2;
       }
-      double pe;
-      if (op.opcode == QCB_OP_PAULI_NOISE) {
-        s.t0 = op.p[0]; s.t1 = op.p[0] + op.p[2]; s.t2 = op.p[0] + op.p[2] + op.p[1];
-        pe = s.t2;
-      } else {
-        const double np = op.opcode == QCB_OP_DEPOL2 ? 15.0 : 3.0;
-        s.t0 = op.p[0] * np / (np + 1.0);
-        pe = s.t0;
-      }
-      if (pe > 1.0) pe = 1.0;
-      pmax = std::max(pmax, pe);
+      fill_site_probabilities(s, op);
+      pmax = std::max(pmax, s.peff);
       if (touches) {
         post.push_back((uint32_t)o.site);
         post_q.insert(o.q1);
@@ -294,11 +312,8 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     const bool two = o.kind == SEG_CNOT || o.kind == SEG_CZ || o.kind == SEG_G2;
     const bool hit = post_q.count(o.q1) || (two && post_q.count(o.q2));
     const bool overlap = cur_q.count(o.q1) || (two && cur_q.count(o.q2));
-    bool same_bit = false;
-    if (o.bit != BIT_NONE)
-      for (auto& c : cur) same_bit = same_bit || c.bit == o.bit;
-    if (!cur.empty() && (hit || overlap || same_bit || o.kind != cur_kind || cur.size() >= (1u << 20)))
-      close_seg();
+    const bool same_bit = o.bit != BIT_NONE && cur_bits.count(o.bit);
+    if (!cur.empty() && (hit || overlap || same_bit || o.kind != cur_kind)) close_seg();
     cur_kind = o.kind;
     LOp c = o;  // planes current at this op
     c.xa = E.px(o.q1); c.za = E.pz(o.q1);
@@ -306,16 +321,47 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     cur.push_back(c);
     cur_q.insert(o.q1);
     if (two) cur_q.insert(o.q2);
+    if (o.bit != BIT_NONE) cur_bits.insert(o.bit);
   }
   close_seg();
   emit_sites(pre);
-  P.stream_slot.push_back(SEG_END << 24); P.stream_slot.push_back(0);
-  P.stream_slot.push_back(0); P.stream_slot.push_back(0);
+
+  // Windowing: the kernel stages the stream into shared memory one window of
+  // PROG_WINDOW_WORDS at a time, so no record may straddle a window.  A record
+  // too long for the space left is split into parts (entries of one segment
+  // or flush are independent; every part but the last is marked so that no
+  // barrier follows it); a window ends with a WIN record, the stream with END.
+  auto& out = P.stream_slot;
+  out.clear();
+  auto room = [&]() { return PROG_WINDOW_WORDS - (uint32_t)(out.size() % PROG_WINDOW_WORDS) - 4; };
+  auto next_window = [&]() {
+    out.push_back(SEG_WIN << 24); out.push_back(0); out.push_back(0); out.push_back(0);
+    while (out.size() % PROG_WINDOW_WORDS) out.push_back(0);
+  };
+  for (auto& r : recs) {
+    const uint32_t n = (uint32_t)(r.w.size() / r.entry_words);
+    uint32_t done = 0;
+    while (done < n) {
+      if (room() < 4 + ((r.entry_words + 3) & ~3u)) next_window();
+      const uint32_t fit = (room() - 4) / r.entry_words;
+      // room() - 4 is a multiple of 4 words, so the padded part fits too
+      const uint32_t take = std::min(n - done, fit);
+      const bool last = done + take == n;
+      out.push_back((r.kind << 24) | take);
+      out.push_back(last ? 0u : FLAG_NO_BARRIER); out.push_back(0); out.push_back(0);
+      out.insert(out.end(), r.w.begin() + (size_t)done * r.entry_words, r.w.begin() + (size_t)(done + take) * r.entry_words);
+      while (out.size() % 4) out.push_back(0);
+      done += take;
+    }
+  }
+  out.push_back(SEG_END << 24); out.push_back(0); out.push_back(0); out.push_back(0);
+  while (out.size() % PROG_WINDOW_WORDS) out.push_back(0);
+  P.classes = classes;
   P.info.n_segments = nseg;
   P.info.n_flushes = nflush;
   P.slot_swap.assign(swp.begin(), swp.end());
   P.pmax = pmax;
-  P.inv_log1m = (pmax > 0 && pmax < 1.0) ? 1.0 / std::log1p(-pmax) : 0.0;
+  P.inv_log1m = 0;
   P.hash = fnv1a(ops, n_ops * sizeof(qcb_op));
   return QCB_OK;
 }
@@ -330,7 +376,7 @@ int upload(Program& P) {
     return e;
   };
   cudaError_t e = up(&P.d_stream_slot, P.stream_slot);
-  if (e == cudaSuccess) e = up(&P.d_sites_slot, P.sites_slot);
+  if (e == cudaSuccess) e = up(&P.d_classes, P.classes);
   if (e == cudaSuccess) e = up(&P.d_slot_qubit, P.slot_qubit);
   std::vector<uint32_t> qs(P.nq + 1, BIT_NONE);
   for (uint32_t s = 0; s < P.nslots; s++) qs[P.slot_qubit[s]] = s;
@@ -344,12 +390,12 @@ int upload(Program& P) {
 
 void release(Program& P) {
   cudaFree(P.d_stream_slot);
-  cudaFree(P.d_sites_slot);
+  cudaFree(P.d_classes);
   cudaFree(P.d_slot_qubit);
   cudaFree(P.d_qubit_slot);
   cudaFree(P.d_slot_swap);
   P.d_stream_slot = nullptr;
-  P.d_sites_slot = nullptr;
+  P.d_classes = nullptr;
   P.d_slot_qubit = P.d_qubit_slot = P.d_slot_swap = nullptr;
 }
 

@@ -76,21 +76,41 @@ enum SegKind : uint32_t {
   SEG_G2 = 5,     // entries (opcode, x_a, z_a, x_b), (z_b, 0, 0, 0)
   SEG_MZ = 6,     // entries (x, bit), padded to a multiple of 4 words
   SEG_MRZ = 7,    // count groups of 4 entries (x, z, bit or NONE, reset or PAD)
-  SEG_FLUSH = 8,  // count runs of sites (begin, end), padded to a multiple of 4 words
-  SEG_CZ = 9      // entries (x_a, z_a, x_b, z_b)
+  SEG_FLUSH = 8,  // count sites (site, kind | class << 8, x_a | z_a << 16, x_b | z_b << 16)
+  SEG_CZ = 9,     // entries (x_a, z_a, x_b, z_b)
+  SEG_WIN = 10    // the stream continues in the next window
 };
+// Entry layouts in the windowed stream (planes are 16-bit):
+//   CNOT/CZ (x_a | z_a<<16, x_b | z_b<<16); S/G1 (x | z<<16, opcode);
+//   G2 (x_a | z_a<<16, x_b | z_b<<16, opcode, 0); MZ (x, bit);
+//   MRZ groups of 4 x (x | z<<16, bit, reset or PAD, 0); FLUSH as above.
+// Header word 1 bit 0: no barrier after this record (a record split across
+// windows; its parts are independent).
 constexpr uint32_t BIT_NONE = 0xFFFFFFFFu;
 constexpr uint32_t MRZ_PAD = 0xFFFFFFFFu;
-// Noise sites per independent Philox event stream (per shot column).
-constexpr uint32_t NOISE_CHUNK = 32;
+constexpr uint32_t FLAG_NO_BARRIER = 1u;
+// Program window staged into shared memory by the walker (words).
+constexpr uint32_t PROG_WINDOW_WORDS = 2048;
+
+// Probabilities shared by noise sites (one entry per distinct set).
+struct NoiseClass {
+  double t0, t1, t2, peff, q0, r;
+  uint32_t dense, pad;
+};
+// Noise is sampled per (site, group of NOISE_GROUP consecutive shots).
+constexpr uint32_t NOISE_GROUP = 1024;
+// Sites with p_eff * NOISE_GROUP above this draw every shot (dense mode).
+constexpr double NOISE_DENSE_LAMBDA = 16.0;
 
 // A noise site: kind = opcode (PAULI_NOISE / DEPOL1 / DEPOL2), the planes of
-// its qubit(s) at the noise op, and the thresholds for the event kind.
+// its qubit(s) at the noise op, the total event probability p_eff and the
+// thresholds for the event kind, and the Binomial(NOISE_GROUP, p_eff)
+// parameters of the event count: q0 = (1-p_eff)^NOISE_GROUP, r = p_eff/(1-p_eff).
 struct Site {
   uint32_t kind, xa, za, xb;
-  uint32_t zb, pad0, pad1, pad2;
-  double t0, t1, t2;  // PAULI: X if v<t0, Z if v<t1, Y if v<t2;  DEPOL: t0 = p_eff
-  double pad3;
+  uint32_t zb, dense, pad0, pad1;
+  double t0, t1, t2;  // PAULI: X if v<t0, Z if v<t1, Y if v<t2
+  double peff, q0, r;
 };
 
 struct Program {
@@ -103,10 +123,11 @@ struct Program {
   std::vector<int64_t> site_of_op;    // op index -> site (or -1)
   std::vector<uint32_t> site_arity;
   std::vector<uint8_t> slot_swap;     // final x<->z relabel per slot
+  std::vector<NoiseClass> classes;
   double pmax = 0, inv_log1m = 0;
   // device copies
   uint32_t* d_stream_slot = nullptr;
-  Site* d_sites_slot = nullptr;
+  NoiseClass* d_classes = nullptr;
   uint32_t* d_slot_qubit = nullptr;
   uint32_t* d_slot_swap = nullptr;
   uint32_t* d_qubit_slot = nullptr;   // [nq_alloc] qubit -> slot or NONE
@@ -127,6 +148,7 @@ struct qcb_frame {
   uint64_t pitch;    // words per plane (>= ncols, multiple of 32)
   uint32_t* planes;  // [(2*(nq1+1))][pitch]: plane 2q = x(q), 2q+1 = z(q); last pair = scratch
   uint32_t* record;  // [nbits][pitch]
+  int32_t* err;      // device status word of the walker (QCB_ETIMEOUT on a stuck wait)
 };
 
 struct qcb_tableau {

@@ -17,12 +17,13 @@ import qcb200
 from qcb200 import ops as O
 from qcb200._lib import check, lib, ptr, qcb_program_info
 
-SEG_END, SEG_CNOT, SEG_H, SEG_S, SEG_G1, SEG_G2, SEG_MZ, SEG_MRZ, SEG_FLUSH, SEG_CZ = range(10)
+SEG_END, SEG_CNOT, SEG_H, SEG_S, SEG_G1, SEG_G2, SEG_MZ, SEG_MRZ, SEG_FLUSH, SEG_CZ, SEG_WIN = range(11)
 BIT_NONE = 0xFFFFFFFF
 MRZ_PAD = 0xFFFFFFFF
 SITE_DTYPE = np.dtype([("kind", "<u4"), ("xa", "<u4"), ("za", "<u4"), ("xb", "<u4"), ("zb", "<u4"),
-                       ("pad", "<u4", (3,)), ("t", "<f8", (3,)), ("pad2", "<f8")])
-assert SITE_DTYPE.itemsize == 64
+                       ("dense", "<u4"), ("pad", "<u4", (2,)), ("t", "<f8", (3,)), ("peff", "<f8"), ("q0", "<f8"),
+                       ("r", "<f8")])
+assert SITE_DTYPE.itemsize == 80
 
 
 def dump(arr):
@@ -103,6 +104,9 @@ def run_mask(arr, frames, qubits, nbits, masks):
     for e in masks.events:
         s = int(site_of_op[int(e["op_index"])])
         ev_by_site.setdefault(s, []).append((int(e["shot"]), int(e["pauli"])))
+    WIN = 2048
+    lo16 = lambda v: int(v) & 0xFFFF
+    hi16 = lambda v: int(v) >> 16
     pc = 0
     while True:
         h = stream[pc: pc + 4]
@@ -110,10 +114,14 @@ def run_mask(arr, frames, qubits, nbits, masks):
         kind, cnt = int(h[0]) >> 24, int(h[0]) & 0xFFFFFF
         if kind == SEG_END:
             break
+        if kind == SEG_WIN:
+            pc = (pc - 4) // WIN * WIN + WIN
+            continue
         if kind in (SEG_CNOT, SEG_CZ):
-            e = stream[pc: pc + 4 * cnt].reshape(cnt, 4)
-            pc += 4 * cnt
-            for xa, za, xb, zb in e:
+            e = stream[pc: pc + 2 * cnt].reshape(cnt, 2)
+            pc += (2 * cnt + 3) // 4 * 4
+            for a_, b_ in e:
+                xa, za, xb, zb = lo16(a_), hi16(a_), lo16(b_), hi16(b_)
                 if kind == SEG_CNOT:
                     T[xb] ^= T[xa]
                     T[za] ^= T[zb]
@@ -121,17 +129,19 @@ def run_mask(arr, frames, qubits, nbits, masks):
                     T[za] ^= T[xb]
                     T[zb] ^= T[xa]
         elif kind in (SEG_S, SEG_G1):
-            e = stream[pc: pc + 4 * cnt].reshape(cnt, 4)
-            pc += 4 * cnt
-            for x, z, op, _ in e:
+            e = stream[pc: pc + 2 * cnt].reshape(cnt, 2)
+            pc += (2 * cnt + 3) // 4 * 4
+            for a_, op in e:
+                x, z = lo16(a_), hi16(a_)
                 if kind == SEG_S:
                     T[z] ^= T[x]
                 else:
                     T[x], T[z] = gate1(int(op), T[x], T[z])
         elif kind == SEG_G2:
-            e = stream[pc: pc + 8 * cnt].reshape(cnt, 8)
-            pc += 8 * cnt
-            for op, xa, za, xb, zb, *_ in e:
+            e = stream[pc: pc + 4 * cnt].reshape(cnt, 4)
+            pc += 4 * cnt
+            for a_, b_, op, _ in e:
+                xa, za, xb, zb = lo16(a_), hi16(a_), lo16(b_), hi16(b_)
                 T[xa], T[za], T[xb], T[zb] = gate2(int(op), T[xa].copy(), T[za].copy(), T[xb].copy(), T[zb].copy())
         elif kind == SEG_MZ:
             e = stream[pc: pc + 2 * cnt].reshape(cnt, 2)
@@ -141,29 +151,29 @@ def run_mask(arr, frames, qubits, nbits, masks):
         elif kind == SEG_MRZ:
             e = stream[pc: pc + 16 * cnt].reshape(cnt * 4, 4)
             pc += 16 * cnt
-            for x, z, bit, r in e:
+            for a_, bit, r, _ in e:
                 if r == MRZ_PAD:
                     continue
+                x, z = lo16(a_), hi16(a_)
                 if bit != BIT_NONE:
                     rec[bit] = T[x]
                 T[x] = 0
                 T[z] ^= masks.reset_planes[r]
         elif kind == SEG_FLUSH:
-            runs = stream[pc: pc + 2 * cnt].reshape(cnt, 2)
-            pc += (2 * cnt + 3) // 4 * 4
-            for s in (s for sb, se in runs for s in range(int(sb), int(se))):
-                st = sites[s]
-                for shot, code in ev_by_site.get(s, []):
+            e = stream[pc: pc + 4 * cnt].reshape(cnt, 4)
+            pc += 4 * cnt
+            for site, kc, pa, pb in e:
+                for shot, code in ev_by_site.get(int(site), []):
                     w, b = shot >> 5, np.uint32(1 << (shot & 31))
                     if code & 1:
-                        T[st["xa"], w] ^= b
+                        T[lo16(pa), w] ^= b
                     if code & 2:
-                        T[st["za"], w] ^= b
-                    if st["kind"] == O.OP["DEPOL2"]:
+                        T[hi16(pa), w] ^= b
+                    if (int(kc) & 0xFF) == O.OP["DEPOL2"]:
                         if code & 4:
-                            T[st["xb"], w] ^= b
+                            T[lo16(pb), w] ^= b
                         if code & 8:
-                            T[st["zb"], w] ^= b
+                            T[hi16(pb), w] ^= b
         else:
             raise ValueError(f"unknown record kind {kind}")
     for s in range(nslots):

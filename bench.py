@@ -39,9 +39,9 @@ METRIC = "frame-gate updates/s, d=11 surface code"
 UNIT = "updates/s"
 WORKLOAD = "rotated surface-code memory d=11, 11 rounds, p=1e-3, 1e6 shots per GPU, plain one-circuit launch"
 
-# Model bytes of the plane traffic an op-per-launch schedule must move
-# (CNOT 6, H 4, sMRZ 5, sMZ 2 bits/shot, initZ 1 bit per
-# qubit): 11*(120*4 + 440*6 + 120*5) + 121*2 + 241 = 41,403 bits per shot.
+# Model bytes: the plane traffic an op-per-launch schedule must move (bits
+# per shot read + written: CNOT 6, H 4, sMRZ 5, sMZ 2, initZ 1 per qubit):
+# 11*(120*4 + 440*6 + 120*5) + 121*2 + 241 = 41,403 bits per shot.
 MODEL_BITS_PER_SHOT = 11 * (120 * 4 + 440 * 6 + 120 * 5) + 121 * 2 + 241
 # Compulsory HBM traffic of the fused kernel per shot: the record
 # (1,441 bits) and the final frame (242 qubits x 2 bits).
@@ -264,6 +264,10 @@ def main():
     model_bytes = MODEL_BITS_PER_SHOT / 8 * shots
     hbm_bytes = (RECORD_BITS + FRAME_BITS) / 8 * shots
     achieved = model_bytes / (kernel_ms / 1e3) / 1e9
+    # the walker moves the model bytes through shared memory: 128 B per SM
+    # per clock at the sampled SM clock
+    props = torch.cuda.get_device_properties(local)
+    smem_gbs = props.multi_processor_count * 128 * (clk.get("sm_mhz") or 1965.0) * 1e6 / 1e9
     traffic = None
     tr_path = os.path.join(ROOT, "profiles", "walker_d11_traffic.json")
     if os.path.exists(tr_path):
@@ -287,7 +291,8 @@ def main():
                      "basis": "model plane bytes of an op-per-launch schedule (5,175 B/shot); the walker keeps the "
                               "frame on chip, so its compulsory DRAM bytes are the record + final frame",
                      "compulsory_dram_bytes_per_launch": hbm_bytes,
-                     "compulsory_dram_frac": hbm_bytes / (kernel_ms / 1e3) / 1e9 / peak},
+                     "compulsory_dram_frac": hbm_bytes / (kernel_ms / 1e3) / 1e9 / peak,
+                     "smem_peak_gbs": smem_gbs, "smem_frac": achieved / smem_gbs},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

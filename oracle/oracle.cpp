@@ -700,51 +700,62 @@ static inline void philox_block(u64 seed, u32 idx, u64 col, u32 tag, u32 out[4])
   oracle_philox4x32_10(ctr, key, out);
 }
 
-// Noise sites as the program compiler lays them out: event probability p_eff,
-// kind thresholds, Binomial(GROUP, p_eff) count parameters.
-static const u32 NOISE_GROUP = 1024;
-struct Site { u32 opcode, q1, q2; double t0, t1, t2, peff, q0, r; bool dense; };
+// Noise sites as the program compiler lays them out, in fixed point:
+//  dense sites (p_eff * GROUP > 16) draw one 32-bit word w per shot: PauliNoise
+//  X if w < d0, Z if w < d1, Y if w < d2 (units 2^-32); Depolarization an
+//  event if w < d2, Pauli index 1 + w*np/d2.
+//  sparse sites draw a count word (Binomial(GROUP, p_eff) by inverse CDF
+//  against round(P(K<=k) * 2^32)) and one word per event: position w % GROUP,
+//  kind word v = w >> 10 (units 2^-22): PauliNoise X if v < s0, Z if v < s1,
+//  else Y; Depolarization Pauli index 1 + (v*np >> 22).
+static const u32 NOISE_GROUP = 1024, CDF_MAX = 128, KIND_BITS = 22;
+struct Site {
+  u32 opcode, q1, q2, np;
+  bool dense;
+  u64 d0, d1, d2, s0, s1;
+  std::vector<u32> cdf;
+};
 
-static Site make_site(const qcb_op& op) {
-  Site s{op.opcode, op.q1 - 1, op.q2 ? op.q2 - 1 : 0, 0, 0, 0, 0, 0, 0, false};
-  if (op.opcode == QCB_OP_PAULI_NOISE) {
-    s.t0 = op.p[0]; s.t1 = op.p[0] + op.p[2]; s.t2 = op.p[0] + op.p[2] + op.p[1];
-    s.peff = s.t2;
-  } else {
-    double np = op.opcode == QCB_OP_DEPOL2 ? 15.0 : 3.0;
-    s.peff = op.p[0] * np / (np + 1.0);
-    s.t0 = s.t1 = s.t2 = s.peff;
-  }
-  if (s.peff > 1.0) s.peff = 1.0;
-  s.dense = s.peff * NOISE_GROUP > 16.0;
-  if (s.peff < 1.0) { s.q0 = std::pow(1.0 - s.peff, (double)NOISE_GROUP); s.r = s.peff / (1.0 - s.peff); }
-  return s;
+static u64 to_fixed(double x, u32 bits) {
+  double one = std::ldexp(1.0, (int)bits), f = std::floor(x * one + 0.5);
+  if (!(f > 0.0)) return 0;
+  return f >= one ? (1ull << bits) : (u64)f;
 }
 
-static inline u32 event_code(const Site& s, double v) {
-  if (s.opcode == QCB_OP_PAULI_NOISE) {
-    if (v < s.t0) return 1;
-    if (v < s.t1) return 2;
-    if (v < s.t2) return 3;
-    return 0;
+static Site make_site(const qcb_op& op) {
+  Site s{op.opcode, op.q1 - 1, op.q2 ? op.q2 - 1 : 0, op.opcode == QCB_OP_DEPOL2 ? 15u : 3u, false, 0, 0, 0, 0, 0, {}};
+  double t0, t1, t2, peff;
+  if (op.opcode == QCB_OP_PAULI_NOISE) {
+    t0 = op.p[0]; t1 = op.p[0] + op.p[2]; t2 = op.p[0] + op.p[2] + op.p[1];
+    peff = t2;
+  } else {
+    double np = op.opcode == QCB_OP_DEPOL2 ? 15.0 : 3.0;
+    peff = op.p[0] * np / (np + 1.0);
+    t0 = t1 = t2 = peff;
   }
-  u32 np = s.opcode == QCB_OP_DEPOL2 ? 15u : 3u;
-  if (v < s.peff) {
-    u32 k = (u32)((v / s.peff) * (double)np);
-    if (k >= np) k = np - 1;
-    return k + 1;
+  if (peff > 1.0) peff = 1.0;
+  s.dense = peff * NOISE_GROUP > 16.0;
+  if (s.dense) {
+    s.d0 = to_fixed(t0, 32); s.d1 = to_fixed(t1, 32); s.d2 = to_fixed(std::min(t2, 1.0), 32);
+  } else if (peff > 0.0) {
+    s.s0 = to_fixed(t0 / peff, KIND_BITS); s.s1 = to_fixed(t1 / peff, KIND_BITS);
+    double r = peff / (1.0 - peff), pk = std::pow(1.0 - peff, (double)NOISE_GROUP), cum = pk;
+    for (u32 k = 0; k < CDF_MAX; k++) {
+      u64 f = to_fixed(cum, 32);
+      if (f >> 32) break;
+      s.cdf.push_back((u32)f);
+      pk = pk * ((double)(NOISE_GROUP - k) * r) / (double)(k + 1);
+      cum = cum + pk;
+    }
   }
-  return 0;
+  return s;
 }
 
 struct Event { u32 pos, code; };
 
-// Events of one site on one group of NOISE_GROUP shots: Philox blocks
-// (site, group, block, TAG_NOISE); sparse sites draw the Binomial count by
-// inverse CDF and place the events on distinct uniform positions, dense sites
-// draw one uniform per shot.
+// Events of one site on one group of NOISE_GROUP shots: word i of Philox block
+// (site, group, i/4, TAG_NOISE) lane i%4.
 static void site_group_events(const Site& s, u32 site, u64 group, u64 seed, std::vector<Event>& out) {
-  if (!(s.peff > 0.0)) return;
   u32 key[2] = {(u32)seed, (u32)(seed >> 32)};
   u32 o[4];
   if (s.dense) {
@@ -752,43 +763,38 @@ static void site_group_events(const Site& s, u32 site, u64 group, u64 seed, std:
       u32 ctr[4] = {site, (u32)group, blk, TAG_NOISE};
       oracle_philox4x32_10(ctr, key, o);
       for (u32 j = 0; j < 4; j++) {
-        u32 code = event_code(s, (double)o[j] * 0x1.0p-32);
+        u64 w = o[j];
+        u32 code = 0;
+        if (s.opcode == QCB_OP_PAULI_NOISE) code = w < s.d0 ? 1 : w < s.d1 ? 2 : w < s.d2 ? 3 : 0;
+        else if (w < s.d2) code = 1 + (u32)(w * s.np / s.d2);
         if (code) out.push_back({blk * 4 + j, code});
       }
     }
     return;
   }
+  if (s.cdf.empty()) return;
   u32 ctr0[4] = {site, (u32)group, 0u, TAG_NOISE};
   oracle_philox4x32_10(ctr0, key, o);
-  double u = ((double)o[0] + 0.5) * 0x1.0p-32;
   u32 k = 0;
-  double pk = s.q0, cum = s.q0;
-  while (u > cum && k < NOISE_GROUP) {
-    pk = (pk * ((double)(NOISE_GROUP - k) * s.r)) / (double)(k + 1);
-    k++;
-    cum = cum + pk;
-  }
-  u32 blk = 0, widx = 1;
-  std::vector<bool> used(NOISE_GROUP, false);
+  while (k < s.cdf.size() && o[0] >= s.cdf[k]) k++;
   auto word = [&](u32 i) {
-    if ((i >> 2) != blk) {
-      blk = i >> 2;
-      u32 ctr[4] = {site, (u32)group, blk, TAG_NOISE};
-      oracle_philox4x32_10(ctr, key, o);
-    }
-    return o[i & 3];
+    u32 ctr[4] = {site, (u32)group, i >> 2, TAG_NOISE}, b[4];
+    oracle_philox4x32_10(ctr, key, b);
+    return b[i & 3];
   };
+  // event e starts from word 1+e; in order, an event whose position repeats
+  // an earlier event's takes the next unused word (k+1, k+2, ...), at most
+  // 64 times, after which the last draw is kept
+  std::vector<bool> used(NOISE_GROUP, false);
+  u32 next = k + 1;
   for (u32 e = 0; e < k; e++) {
-    u32 pos, tw;
-    while (true) {
-      pos = word(widx) & (NOISE_GROUP - 1);
-      widx++;
-      tw = word(widx);
-      widx++;
-      if (!used[pos]) { used[pos] = true; break; }
-    }
-    u32 code = event_code(s, ((double)tw * 0x1.0p-32) * s.peff);
-    if (code) out.push_back({pos, code});
+    u32 w = word(1 + e);
+    for (u32 r = 0; r < 64 && used[w % NOISE_GROUP]; r++) w = word(next++);
+    used[w % NOISE_GROUP] = true;
+    u32 v = w >> 10, code;
+    if (s.opcode == QCB_OP_PAULI_NOISE) code = v < s.s0 ? 1 : v < s.s1 ? 2 : 3;
+    else code = 1 + ((v * s.np) >> KIND_BITS);
+    out.push_back({w % NOISE_GROUP, code});
   }
 }
 

@@ -15,12 +15,12 @@
 // qubit in shared memory (or in the HBM planes when the frame is too tall),
 // and only the record and the final frame go to HBM.
 //
-// Noise (Philox mode).  Each column draws its own counter-based stream
-// (key = seed, counter = (draw, column, tag)).  Noise sites are visited in
-// program order; over the trials t = site*32 + lane the column samples the
-// gaps between events geometrically at rate p_max, then picks the event kind
-// (or thins it away) from a second uniform scaled by p_max.  Events of sites
-// [b, e) are applied at the FLUSH record the compiler placed for them.
+// Noise (Philox mode).  Counter-based streams (key = seed): initZ! and reset
+// draws per (index, shot column); noise per (site, group of 1024 shots), where
+// one word gives the group's Binomial event count and one word per event its
+// shot and kind, in integer fixed point (sample_site_group).  The sites of a
+// FLUSH record are sampled there, as (site, group) tasks spread over the
+// whole CTA, and flipped into the tile with shared-memory atomics.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -49,6 +49,7 @@ struct WalkArgs {
   uint64_t seed;
   uint64_t col0;            // global column index of column 0
   const NoiseClass* classes;
+  const uint32_t* cdf;      // Binomial count tables of the sparse classes
   double pmax;
   int32_t* err;             // set to QCB_ETIMEOUT when a staging wait gives up
   // mask mode
@@ -150,31 +151,32 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // ---------------------------------------------------------------- noise
-// Event kind of a uniform v in [0, p_eff) (or [0, 1) in dense mode, where
-// v >= p_eff means no event): PauliNoise X / Z / Y by the thresholds,
-// DepolarizationNoise a uniform non-identity Pauli index.
-__device__ __forceinline__ uint32_t event_code(uint32_t kind, const NoiseClass& c, double v) {
-  if (kind == QCB_OP_PAULI_NOISE) {
-    if (v < c.t0) return 1;
-    if (v < c.t1) return 2;
-    if (v < c.t2) return 3;
-    return 0;
-  }
-  const uint32_t np = kind == QCB_OP_DEPOL2 ? 15u : 3u;
-  if (v < c.peff) {
-    uint32_t k = (uint32_t)(__dmul_rn(__ddiv_rn(v, c.peff), (double)np));
-    if (k >= np) k = np - 1;
-    return k + 1;
-  }
-  return 0;
+// Event codes: bit 0 flips x of the site's first qubit, bit 1 its z, bits 2
+// and 3 the same for the second qubit; 0 is no event.  PauliNoise gives X = 1,
+// Z = 2, Y = 3; DepolarizationNoise a uniform non-identity Pauli index.
+// Dense draw: one 32-bit word per shot (thresholds in units of 2^-32).
+__device__ __forceinline__ uint32_t dense_code(uint32_t kind, const NoiseClass& c, uint32_t w) {
+  if (kind == QCB_OP_PAULI_NOISE) return w < c.thr0 ? 1u : w < c.thr1 ? 2u : w < c.thr2 ? 3u : 0u;
+  if (w >= c.thr2) return 0u;
+  return 1u + (uint32_t)(((uint64_t)w * c.np) / c.thr2);
 }
 
-// Flip the event's Pauli into the tile at group-relative shot `pos`.
+// Sparse event: the kind of an event that happens, from a 22-bit word v.
+__device__ __forceinline__ uint32_t sparse_code(uint32_t kind, const NoiseClass& c, uint32_t v) {
+  if (kind == QCB_OP_PAULI_NOISE) return v < c.thr0 ? 1u : v < c.thr1 ? 2u : 3u;
+  return 1u + ((v * c.np) >> NOISE_KIND_BITS);
+}
+
+// Flip the event's Pauli into the tile at group shot `pos`; lc0 is the tile
+// column of the group's first column (a group may straddle tiles: columns
+// outside [0, T) belong to a neighbouring tile, which draws the same events).
 // e = (site, kind | class<<8, x_a | z_a<<16, x_b | z_b<<16).
 template <bool SMEM>
-__device__ __forceinline__ void apply_code(const Tile<SMEM>& F, const uint4& e, uint32_t code, uint32_t gl,
+__device__ __forceinline__ void apply_code(const Tile<SMEM>& F, const uint4& e, uint32_t code, int32_t lc0,
                                            uint32_t pos, uint64_t c0, uint64_t ncols) {
-  const uint32_t cl = gl * 32 + (pos >> 5);
+  const int32_t lc = lc0 + (int32_t)(pos >> 5);
+  if (lc < 0 || lc >= (int32_t)F.T) return;
+  const uint32_t cl = (uint32_t)lc;
   const uint64_t cg = c0 + cl;
   if (cg >= ncols) return;
   const uint32_t bit = 1u << (pos & 31);
@@ -186,75 +188,95 @@ __device__ __forceinline__ void apply_code(const Tile<SMEM>& F, const uint4& e, 
   }
 }
 
+// Word i of the noise stream of (site, group G): lane i % 4 of Philox block
+// (site, G, i / 4, TAG_NOISE).
+__device__ __forceinline__ uint32_t noise_word(uint32_t site, uint32_t glo, uint32_t i, uint32_t k0,
+                                               uint32_t k1) {
+  uint32_t o[4];
+  philox4x32_10(site, glo, i >> 2, TAG_NOISE, k0, k1, o);
+  return sel4(o, i & 3);
+}
+
+// Events with at most this many per (site, group) stay in registers.
+constexpr uint32_t NOISE_KREG = 8;
+// Redraws of one event's position before its last draw is kept (a collision
+// has probability below k/NOISE_GROUP per draw, so the cap is never reached
+// in practice; it only bounds the loop).
+constexpr uint32_t NOISE_REDRAWS = 64;
+
 // The events of one noise site on one group of NOISE_GROUP shots (group G of
-// the run, = 32 consecutive shot columns).  Its random words come from Philox
-// blocks (site, G, block index, TAG_NOISE).
+// the run, = 32 consecutive shot columns), from the words of noise_word.
 //  sparse: word 0 gives the event count k ~ Binomial(NOISE_GROUP, p_eff) by
-//          inverse CDF; each event then takes a position word (uniform in the
-//          group, redrawn if the shot already has an event of this site) and
-//          a kind word (uniform in [0, p_eff)).  Given k the positions are a
-//          uniform k-subset, so every shot gets an event independently with
+//          inverse CDF against the class's fixed-point table.  Event e starts
+//          from word 1 + e: position w & (NOISE_GROUP-1), kind from w >> 10.
+//          Then, for e = 1, 2, ... in order, while event e's position equals
+//          that of an earlier event, its word is replaced by the next unused
+//          word k+1, k+2, ...  This is sequential rejection sampling, so given
+//          k the positions are a uniform k-subset and the kinds are
+//          independent: every shot gets an event independently with
 //          probability p_eff, as the reference's per-frame draws.
-//  dense:  word j is the per-shot uniform of shot j.
+//  dense:  word j is the per-shot draw of shot j.
 template <bool SMEM>
 __device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<SMEM>& F, const uint4& e,
-                                                  uint64_t G, uint32_t gl, uint64_t c0) {
+                                                  uint64_t G, int32_t lc0, uint64_t c0) {
   const uint32_t site = e.x, kind = e.y & 0xFFu;
   const NoiseClass c = a.classes[e.y >> 8];
-  if (!(c.peff > 0.0)) return;
   const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
   const uint32_t glo = (uint32_t)G;
+  constexpr uint32_t PMASK = NOISE_GROUP - 1;
   uint32_t o[4];
   if (c.dense) {
     for (uint32_t blk = 0; blk < NOISE_GROUP / 4; blk++) {
       philox4x32_10(site, glo, blk, TAG_NOISE, k0, k1, o);
 #pragma unroll
       for (uint32_t j = 0; j < 4; j++) {
-        const double u = __dmul_rn((double)o[j], 0x1.0p-32);
-        const uint32_t code = event_code(kind, c, u);
-        if (code) apply_code<SMEM>(F, e, code, gl, blk * 4 + j, c0, a.ncols);
+        const uint32_t code = dense_code(kind, c, o[j]);
+        if (code) apply_code<SMEM>(F, e, code, lc0, blk * 4 + j, c0, a.ncols);
       }
     }
     return;
   }
+  if (!c.cdf_len) return;
   philox4x32_10(site, glo, 0u, TAG_NOISE, k0, k1, o);
-  const double u = __dmul_rn(__dadd_rn((double)o[0], 0.5), 0x1.0p-32);
+  const uint32_t* tb = a.cdf + c.cdf_off;
   uint32_t k = 0;
-  double pk = c.q0, cum = c.q0;
-  while (u > cum && k < NOISE_GROUP) {
-    pk = __ddiv_rn(__dmul_rn(pk, __dmul_rn((double)(NOISE_GROUP - k), c.r)), (double)(k + 1));
-    k++;
-    cum = __dadd_rn(cum, pk);
-  }
+  while (k < c.cdf_len && o[0] >= __ldg(tb + k)) k++;
   if (k == 0) return;
-  uint32_t blk = 0, widx = 1;
-  uint32_t p0 = 0xFFFFFFFFu, p1 = 0xFFFFFFFFu, p2 = 0xFFFFFFFFu, p3 = 0xFFFFFFFFu;
-  uint32_t bm[NOISE_GROUP / 32];  // used positions when k > 4
-  if (k > 4)
-    for (uint32_t i = 0; i < NOISE_GROUP / 32; i++) bm[i] = 0;
-  for (uint32_t ev = 0; ev < k; ev++) {
-    uint32_t pos, tw;
-    while (true) {
-      // words widx (position) and widx + 1 (kind)
-      if ((widx >> 2) != blk) { blk = widx >> 2; philox4x32_10(site, glo, blk, TAG_NOISE, k0, k1, o); }
-      pos = sel4(o, widx & 3) & (NOISE_GROUP - 1);
-      widx++;
-      if ((widx >> 2) != blk) { blk = widx >> 2; philox4x32_10(site, glo, blk, TAG_NOISE, k0, k1, o); }
-      tw = sel4(o, widx & 3);
-      widx++;
-      bool dup;
-      if (k > 4) {
-        dup = (bm[pos >> 5] >> (pos & 31)) & 1u;
-        if (!dup) bm[pos >> 5] |= 1u << (pos & 31);
-      } else {
-        dup = pos == p0 || pos == p1 || pos == p2 || pos == p3;
-        if (!dup) { if (ev == 0) p0 = pos; else if (ev == 1) p1 = pos; else if (ev == 2) p2 = pos; else p3 = pos; }
+  uint32_t next = k + 1;  // next unused word
+  if (k <= NOISE_KREG) {
+    uint32_t w[NOISE_KREG];
+#pragma unroll
+    for (uint32_t ev = 0; ev < NOISE_KREG; ev++) {
+      if (ev < k) {
+        if (((ev + 1) & 3) == 0) philox4x32_10(site, glo, (ev + 1) >> 2, TAG_NOISE, k0, k1, o);
+        w[ev] = o[(ev + 1) & 3];
       }
-      if (!dup) break;
     }
-    const double v = __dmul_rn(__dmul_rn((double)tw, 0x1.0p-32), c.peff);
-    const uint32_t code = event_code(kind, c, v);
-    if (code) apply_code<SMEM>(F, e, code, gl, pos, c0, a.ncols);
+#pragma unroll
+    for (uint32_t ev = 1; ev < NOISE_KREG; ev++) {
+      if (ev < k) {
+        for (uint32_t r = 0; r < NOISE_REDRAWS; r++) {
+          bool dup = false;
+#pragma unroll
+          for (uint32_t j = 0; j < ev; j++) dup |= ((w[ev] ^ w[j]) & PMASK) == 0;
+          if (!dup) break;
+          w[ev] = noise_word(site, glo, next++, k0, k1);
+        }
+      }
+    }
+#pragma unroll
+    for (uint32_t ev = 0; ev < NOISE_KREG; ev++)
+      if (ev < k) apply_code<SMEM>(F, e, sparse_code(kind, c, w[ev] >> 10), lc0, w[ev] & PMASK, c0, a.ncols);
+    return;
+  }
+  uint32_t bm[NOISE_GROUP / 32];  // positions taken so far
+  for (uint32_t i = 0; i < NOISE_GROUP / 32; i++) bm[i] = 0;
+  for (uint32_t ev = 0; ev < k; ev++) {
+    uint32_t wv = noise_word(site, glo, 1 + ev, k0, k1);
+    for (uint32_t r = 0; r < NOISE_REDRAWS && ((bm[(wv & PMASK) >> 5] >> (wv & 31)) & 1u); r++)
+      wv = noise_word(site, glo, next++, k0, k1);
+    bm[(wv & PMASK) >> 5] |= 1u << (wv & 31);
+    apply_code<SMEM>(F, e, sparse_code(kind, c, wv >> 10), lc0, wv & PMASK, c0, a.ncols);
   }
 }
 
@@ -478,14 +500,17 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
           const uint4* en = (const uint4*)e;
           if (PHILOX) {
             if (a.pmax > 0.0) {
-              // (site, shot group) tasks over all threads of the CTA; a group is
-              // 32 tile columns
-              const uint32_t ng = T / 32;
-              const uint64_t G0 = (a.col0 + c0) / 32;
+              // (site, shot group) tasks over all threads of the CTA; a group
+              // is 32 run columns and may straddle the tile's edges
+              const uint64_t gc0 = a.col0 + c0;
+              const uint64_t gc1 = a.col0 + min(c0 + T, a.ncols);
+              const uint64_t G0 = gc0 / 32;
+              const uint32_t ng = (uint32_t)((gc1 - 1) / 32 - G0 + 1);
               const uint32_t ntask = cnt * ng;
               for (uint32_t t = tid; t < ntask; t += blockDim.x) {
                 const uint32_t i = t / ng, gl = t - i * ng;
-                sample_site_group<SMEM>(a, F, en[i], G0 + gl, gl, c0);
+                const int32_t lc0 = (int32_t)((int64_t)((G0 + gl) * 32) - (int64_t)gc0);
+                sample_site_group<SMEM>(a, F, en[i], G0 + gl, lc0, c0);
               }
             }
           } else if (rr == 0 && act) {
@@ -732,6 +757,16 @@ struct WalkConfig {
 
 static uint32_t g_tile_override = 0;
 
+// Tile width for ncols columns with tiles of at most tmax columns: the fewest
+// waves of one CTA per SM, then the narrowest tile that still needs no more
+// waves, so that the last wave is as full as the others.
+static uint32_t balanced_tile(uint64_t ncols, uint32_t tmax) {
+  const uint64_t nsm = (uint64_t)std::max(device_sm_count(), 1);
+  const uint64_t waves = std::max<uint64_t>(1, (ncols + nsm * tmax - 1) / (nsm * tmax));
+  const uint64_t t = (ncols + nsm * waves - 1) / (nsm * waves);
+  return (uint32_t)std::min<uint64_t>(tmax, std::max<uint64_t>(t, 16));
+}
+
 // Shared-memory tile when 2 planes x 32 columns of every touched qubit fit,
 // else the same walker on the HBM planes.
 static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
@@ -743,10 +778,8 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   uint32_t T = 0;
   if (g_tile_override && per_col * g_tile_override <= budget) {
     T = g_tile_override;
-  } else {
-    const uint32_t cands[] = {96, 64, 32};
-    for (uint32_t c : cands)
-      if (per_col * c <= budget) { T = c; break; }
+  } else if (budget / per_col >= 32) {
+    T = balanced_tile(f->ncols, (uint32_t)std::min<size_t>(256, budget / per_col));
   }
   if (T) {
     wc.smem = true;
@@ -755,8 +788,8 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
     wc.smem_bytes = per_col * T + stage;
   } else {
     wc.smem = false;
-    wc.T = 128;
-    wc.nth = 768;
+    wc.T = balanced_tile(f->ncols, 128);
+    wc.nth = (768u / wc.T) * wc.T;
     wc.smem_bytes = (size_t)2 * p->nslots * 4 + stage;
   }
   const uint64_t tiles = (f->ncols + wc.T - 1) / wc.T;
@@ -796,6 +829,7 @@ static void fill_common(WalkArgs& a, qcb_frame* f, const qcb_program* p) {
   a.prog = (const uint4*)p->d_stream_slot;
   a.nwin = (uint32_t)(p->stream_slot.size() / PROG_WINDOW_WORDS);
   a.classes = p->d_classes;
+  a.cdf = p->d_cdf;
   a.pmax = p->pmax;
   a.err = f->err;
 }

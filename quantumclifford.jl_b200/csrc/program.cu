@@ -94,6 +94,47 @@ void fill_site_probabilities(Site& s, const qcb_op& op) {
   }
 }
 
+// round(x * 2^bits), clamped to [0, 2^bits]; x * 2^bits is exact.
+static uint64_t fixed_point(double x, uint32_t bits) {
+  const double one = std::ldexp(1.0, (int)bits);
+  const double f = std::floor(x * one + 0.5);
+  if (!(f > 0.0)) return 0;
+  return f >= one ? (uint64_t)1 << bits : (uint64_t)f;
+}
+
+// Fixed-point thresholds of a site's class (layout in qcb_internal.h).
+static NoiseClass noise_class(const Site& s) {
+  NoiseClass c{};
+  c.dense = s.dense;
+  c.np = s.kind == QCB_OP_DEPOL2 ? 15u : 3u;
+  if (s.dense) {
+    c.thr0 = fixed_point(s.t0, 32);
+    c.thr1 = fixed_point(s.t1, 32);
+    c.thr2 = fixed_point(std::min(s.t2, 1.0), 32);
+  } else if (s.peff > 0.0) {
+    // kind given an event: X with px / p_eff, Z with pz / p_eff, else Y
+    c.thr0 = fixed_point(s.t0 / s.peff, NOISE_KIND_BITS);
+    c.thr1 = fixed_point(s.t1 / s.peff, NOISE_KIND_BITS);
+    c.thr2 = (uint64_t)1 << NOISE_KIND_BITS;
+  }
+  return c;
+}
+
+// Count thresholds of Binomial(NOISE_GROUP, p): entry k = round(P(K <= k) *
+// 2^32), appended while below 2^32 (at most NOISE_CDF_MAX entries).  The pmf
+// follows P(k+1) = P(k) (N-k)/(k+1) p/(1-p) from P(0) = (1-p)^N.
+static void binomial_count_table(double p, std::vector<uint32_t>& out) {
+  const double r = p / (1.0 - p);
+  double pk = std::pow(1.0 - p, (double)NOISE_GROUP), cum = pk;
+  for (uint32_t k = 0; k < NOISE_CDF_MAX; k++) {
+    const uint64_t f = fixed_point(cum, 32);
+    if (f >> 32) break;
+    out.push_back((uint32_t)f);
+    pk = pk * ((double)(NOISE_GROUP - k) * r) / (double)(k + 1);
+    cum = cum + pk;
+  }
+}
+
 int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   std::memset(&P.info, 0, sizeof(P.info));
   P.info.n_ops = (uint32_t)n_ops;
@@ -184,14 +225,27 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   uint32_t nseg = 0, nflush = 0;
   if (2ull * P.nslots > 65536) return fail(QCB_EUNSUPPORTED, "at most 32768 distinct qubits per program");
 
-  // Noise probability classes: sites with equal probabilities share one entry.
+  // Noise classes: sites of one opcode with equal probabilities share one
+  // entry; sparse classes with equal p_eff share one count table.
   std::vector<NoiseClass> classes;
-  std::map<std::tuple<double, double, double, double>, uint32_t> class_of;
+  std::vector<uint32_t> cdf;
+  std::map<std::tuple<uint32_t, double, double, double, double>, uint32_t> class_of;
+  std::map<double, std::pair<uint32_t, uint32_t>> table_of;
   auto class_id = [&](const Site& s) -> uint32_t {
-    auto key = std::make_tuple(s.t0, s.t1, s.t2, s.peff);
+    auto key = std::make_tuple(s.kind, s.t0, s.t1, s.t2, s.peff);
     auto it = class_of.find(key);
     if (it != class_of.end()) return it->second;
-    NoiseClass c{s.t0, s.t1, s.t2, s.peff, s.q0, s.r, s.dense, 0};
+    NoiseClass c = noise_class(s);
+    if (!c.dense && s.peff > 0.0) {
+      auto t = table_of.find(s.peff);
+      if (t == table_of.end()) {
+        const uint32_t off = (uint32_t)cdf.size();
+        binomial_count_table(s.peff, cdf);
+        t = table_of.emplace(s.peff, std::make_pair(off, (uint32_t)cdf.size() - off)).first;
+      }
+      c.cdf_off = t->second.first;
+      c.cdf_len = t->second.second;
+    }
     classes.push_back(c);
     return class_of[key] = (uint32_t)(classes.size() - 1);
   };
@@ -357,11 +411,11 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   out.push_back(SEG_END << 24); out.push_back(0); out.push_back(0); out.push_back(0);
   while (out.size() % PROG_WINDOW_WORDS) out.push_back(0);
   P.classes = classes;
+  P.cdf = cdf;
   P.info.n_segments = nseg;
   P.info.n_flushes = nflush;
   P.slot_swap.assign(swp.begin(), swp.end());
   P.pmax = pmax;
-  P.inv_log1m = 0;
   P.hash = fnv1a(ops, n_ops * sizeof(qcb_op));
   return QCB_OK;
 }
@@ -377,6 +431,7 @@ int upload(Program& P) {
   };
   cudaError_t e = up(&P.d_stream_slot, P.stream_slot);
   if (e == cudaSuccess) e = up(&P.d_classes, P.classes);
+  if (e == cudaSuccess) e = up(&P.d_cdf, P.cdf);
   if (e == cudaSuccess) e = up(&P.d_slot_qubit, P.slot_qubit);
   std::vector<uint32_t> qs(P.nq + 1, BIT_NONE);
   for (uint32_t s = 0; s < P.nslots; s++) qs[P.slot_qubit[s]] = s;
@@ -391,11 +446,13 @@ int upload(Program& P) {
 void release(Program& P) {
   cudaFree(P.d_stream_slot);
   cudaFree(P.d_classes);
+  cudaFree(P.d_cdf);
   cudaFree(P.d_slot_qubit);
   cudaFree(P.d_qubit_slot);
   cudaFree(P.d_slot_swap);
   P.d_stream_slot = nullptr;
   P.d_classes = nullptr;
+  P.d_cdf = nullptr;
   P.d_slot_qubit = P.d_qubit_slot = P.d_slot_swap = nullptr;
 }
 

@@ -92,11 +92,25 @@ constexpr uint32_t FLAG_NO_BARRIER = 1u;
 // Program window staged into shared memory by the walker (words).
 constexpr uint32_t PROG_WINDOW_WORDS = 2048;
 
-// Probabilities shared by noise sites (one entry per distinct set).
+// Sampling parameters shared by the noise sites of one opcode with equal
+// probabilities, in fixed point so that the device does integer work only.
+//  dense  (one 32-bit word w per shot): PauliNoise X if w < thr0, Z if
+//         w < thr1, Y if w < thr2; Depolarization an event if w < thr2, of
+//         Pauli index 1 + w*np/thr2.  Thresholds in units of 2^-32.
+//  sparse (one word per group gives the event count k: the first k with
+//         w < cdf[cdf_off + k], else cdf_len; each event is one word w with
+//         position w & (NOISE_GROUP-1) and kind word v = w >> 10):
+//         PauliNoise X if v < thr0, Z if v < thr1, else Y; Depolarization
+//         Pauli index 1 + (v*np >> 22).  Thresholds in units of 2^-22.
 struct NoiseClass {
-  double t0, t1, t2, peff, q0, r;
-  uint32_t dense, pad;
+  uint64_t thr0, thr1, thr2;
+  uint32_t dense, np, cdf_off, cdf_len;
 };
+// Longest Binomial count table (counts above it are clamped to it; sparse
+// classes have NOISE_GROUP*p_eff <= NOISE_DENSE_LAMBDA, so the clamped tail
+// has probability below 2^-60).
+constexpr uint32_t NOISE_CDF_MAX = 128;
+constexpr uint32_t NOISE_KIND_BITS = 22;
 // Noise is sampled per (site, group of NOISE_GROUP consecutive shots).
 constexpr uint32_t NOISE_GROUP = 1024;
 // Sites with p_eff * NOISE_GROUP above this draw every shot (dense mode).
@@ -124,10 +138,12 @@ struct Program {
   std::vector<uint32_t> site_arity;
   std::vector<uint8_t> slot_swap;     // final x<->z relabel per slot
   std::vector<NoiseClass> classes;
-  double pmax = 0, inv_log1m = 0;
+  std::vector<uint32_t> cdf;          // Binomial count thresholds of the sparse classes
+  double pmax = 0;
   // device copies
   uint32_t* d_stream_slot = nullptr;
   NoiseClass* d_classes = nullptr;
+  uint32_t* d_cdf = nullptr;
   uint32_t* d_slot_qubit = nullptr;
   uint32_t* d_slot_swap = nullptr;
   uint32_t* d_qubit_slot = nullptr;   // [nq_alloc] qubit -> slot or NONE

@@ -105,7 +105,7 @@ int qcb_tune_set(const char* key, int64_t value) {
   const std::string k(key);
   if (value < 0 || value > 1024) return fail(QCB_EARG, "qcb_tune_set: value out of range");
   if (k == "walker_tile") {
-    if (value && (value % 32 || value > 256)) return fail(QCB_EARG, "walker_tile must be a multiple of 32, at most 256");
+    if (value && (value < 8 || value > 256)) return fail(QCB_EARG, "walker_tile must be 0 (automatic) or 8..256");
     set_walker_tile((uint32_t)value);
   } else if (k == "canon_cluster") {
     if (value && (value > 16 || (value & (value - 1)))) return fail(QCB_EARG, "canon_cluster must be 1, 2, 4, 8 or 16");

@@ -129,6 +129,37 @@ def test_philox_mode_bit_exact_against_oracle_replica(qcb, which):
     assert np.array_equal(coding(f.xzs(), qmax + 1), coding(ox, qmax + 1))
 
 
+@pytest.mark.parametrize("tile", [0, 16, 40, 106, 256])
+@pytest.mark.parametrize("d,p", [(5, 0.004), (3, 0.015), (3, 1e-4)])
+def test_philox_sparse_noise_any_tile_width(qcb, tile, d, p):
+    # sparse sites (p_eff * 1024 <= 16): Binomial counts, distinct positions,
+    # several events per group at p = 0.015; tiles of 16/40/106 columns cut
+    # 1024-shot groups, which both neighbouring tiles draw
+    arr = O.to_array(circuits.rotated_surface_code_memory(d, d, p))
+    qmax, bmax = O.affected_counts(arr)
+    frames = 9 * 1024 + 100
+    qcb.check(qcb.lib().qcb_tune_set(b"walker_tile", tile))
+    try:
+        f = qcb.pftrajectories(arr, trajectories=frames, seed=99)
+    finally:
+        qcb.check(qcb.lib().qcb_tune_set(b"walker_tile", 0))
+    ox, om = oracle.pftrajectories_philox(arr, frames, qmax, bmax, 99)
+    assert np.array_equal(f.measurements(), om)
+    assert np.array_equal(coding(f.xzs(), qmax + 1), coding(ox, qmax + 1))
+
+
+@pytest.mark.parametrize("tile", [16, 40, 106])
+def test_mask_mode_any_tile_width(qcb, tile):
+    circ = circuits.rotated_surface_code_memory(3, 3, 0.01)
+    qcb.check(qcb.lib().qcb_tune_set(b"walker_tile", tile))
+    try:
+        f, ox, om = run_mask(qcb, circ, 5000, seed=tile)
+    finally:
+        qcb.check(qcb.lib().qcb_tune_set(b"walker_tile", 0))
+    assert np.array_equal(f.measurements(), om)
+    assert np.array_equal(coding(f.xzs(), f.qubits + 1), coding(ox, f.qubits + 1))
+
+
 def test_shot_offset_shards_compose(qcb):
     circ = O.to_array(circuits.rotated_surface_code_memory(3, 3, 0.05))
     qmax, bmax = O.affected_counts(circ)

@@ -88,7 +88,7 @@ typedef struct qcb_op {
 
 /* Where the randomness of a frame run comes from. */
 enum qcb_noise_mode {
-  QCB_NOISE_PHILOX = 0, /* on-device Philox-4x32-10, geometric-skip noise     */
+  QCB_NOISE_PHILOX = 0, /* on-device Philox-4x32-10 per site and shot group   */
   QCB_NOISE_MASK = 1    /* caller-supplied events (bit-exact parity mode)      */
 };
 
@@ -224,6 +224,25 @@ int qcb_tableau_copy(qcb_tableau* dst, const qcb_tableau* src, void* stream);
  * (may be NULL).                                                            */
 int qcb_mul_left_pauli(qcb_tableau* r, const qcb_tableau* l, int phases,
                        uint8_t* phase_out, void* stream);
+/* No counterpart in the reference.  Batched mul_left! (the semantics of
+ * qcb_mul_left_pauli) on caller-owned device memory, allocating nothing:
+ * for i < count, Pauli r_i <- l_i * r_i, where pair i is row i of two
+ * count-row tableaux in the reference layout (r_xz + i*W, W =
+ * 2*ceil(nqubits/64) uint64 words, X words then Z words; phases uint8,
+ * updated in place when `phases` is nonzero, left untouched otherwise).
+ * For callers that hold their Paulis in memory of another allocator and call
+ * from a loop where a device allocation (and the device-wide synchronisation
+ * a free implies) is not acceptable.  The phase accumulators live in one
+ * static device array of QCB_NOALLOC_MAX_PAIRS words per device: count above
+ * it fails with QCB_EARG.  The array starts at zero and every call leaves it
+ * at zero.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress, with that device current) and clears it, so make it
+ * before any latency-critical use.  Calls that overlap in time on one device
+ * (other streams or host threads) share the array and race: serialise them. */
+#define QCB_NOALLOC_MAX_PAIRS 4096
+int qcb_mul_left_pauli_batch_noalloc(uint64_t* r_xz, uint8_t* r_phases, const uint64_t* l_xz,
+                                     const uint8_t* l_phases, uint32_t nqubits, uint32_t count,
+                                     int phases, void* stream);
 /* mul_left!(s::Tableau, m, i; phases) (src/mul_leftright.jl:177-181).      */
 int qcb_mul_left_row(qcb_tableau* s, uint32_t m, uint32_t i, int phases, void* stream);
 /* mul_left!(s::Tableau, p::PauliOperator; phases) (src/mul_leftright.jl:223-229). */

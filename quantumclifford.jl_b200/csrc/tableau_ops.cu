@@ -9,6 +9,7 @@
 //  symbolic gates with phases (src/symbolic_cliffords.jl:62-74, 293-316).
 //  dense apply! (src/dense_cliffords.jl:135-169).
 #include <algorithm>
+#include <mutex>
 
 #include "qcb_internal.h"
 
@@ -298,6 +299,70 @@ __global__ void __launch_bounds__(256) apply_dense_kernel(uint64_t* xzs, uint8_t
   if (lane == 0) ph[warp] = phases ? (uint8_t)((s + extra + ph[warp]) & 3u) : (uint8_t)0;
 }
 
+// ---------------------------------------------------------------- no-alloc batch
+// Phase accumulators of qcb_mul_left_pauli_batch_noalloc, one per pair.  Zero
+// between calls: the finish kernel clears what it read.
+static __device__ __align__(256) uint32_t g_noalloc_acc[QCB_NOALLOC_MAX_PAIRS];
+
+// Pair blockIdx.y of a batch: the grid-stride loop of mul_left_long_kernel
+// over that pair's words, the phase sum added into acc[pair].
+template <int VEC, bool PH>
+__global__ void __launch_bounds__(256) mul_left_batch_kernel(uint64_t* __restrict__ r,
+                                                             const uint64_t* __restrict__ l,
+                                                             uint64_t len, uint32_t* acc) {
+  const uint32_t pair = blockIdx.y;
+  r += (uint64_t)pair * 2 * len;
+  l += (uint64_t)pair * 2 * len;
+  uint64_t c1a = 0, c2a = 0, c1b = 0, c2b = 0;
+  const uint64_t nvec = len / VEC;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nvec; i += stride) {
+    if (VEC == 2) {
+      const ulonglong2 lx = __ldcs((const ulonglong2*)l + i);
+      const ulonglong2 lz = __ldcs((const ulonglong2*)(l + len) + i);
+      ulonglong2 rx = __ldcs((const ulonglong2*)r + i);
+      ulonglong2 rz = __ldcs((const ulonglong2*)(r + len) + i);
+      if (PH) {
+        mul_step(lx.x, lz.x, rx.x, rz.x, c1a, c2a);
+        mul_step(lx.y, lz.y, rx.y, rz.y, c1b, c2b);
+      } else {
+        rx.x ^= lx.x; rx.y ^= lx.y; rz.x ^= lz.x; rz.y ^= lz.y;
+      }
+      __stcs((ulonglong2*)r + i, rx);
+      __stcs((ulonglong2*)(r + len) + i, rz);
+    } else {
+      const uint64_t lx = __ldcs(l + i), lz = __ldcs(l + len + i);
+      uint64_t rx = __ldcs(r + i), rz = __ldcs(r + len + i);
+      if (PH) mul_step(lx, lz, rx, rz, c1a, c2a);
+      else { rx ^= lx; rz ^= lz; }
+      __stcs(r + i, rx);
+      __stcs(r + len + i, rz);
+    }
+  }
+  if (!PH) return;
+  uint32_t v = (cnt_phase(c1a, c2a) + cnt_phase(c1b, c2b)) & 3u;
+  v = __reduce_add_sync(0xFFFFFFFFu, v) & 3u;
+  __shared__ uint32_t wsum[32];
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) wsum[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t s = lane < (blockDim.x >> 5) ? wsum[lane] : 0u;
+    s = __reduce_add_sync(0xFFFFFFFFu, s) & 3u;
+    if (lane == 0 && s) atomicAdd(acc + pair, s);
+  }
+}
+
+// r_phase[i] <- (s_i + r_phase[i] + l_phase[i]) & 3 (src/mul_leftright.jl:140)
+// when phases; clears acc[i] either way.
+__global__ void mul_left_batch_finish_kernel(uint8_t* r_phase, const uint8_t* l_phase, uint32_t* acc,
+                                             uint32_t count, int phases) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  if (phases) r_phase[i] = (uint8_t)(((acc[i] & 3u) + r_phase[i] + l_phase[i]) & 3u);
+  acc[i] = 0;
+}
+
 }  // namespace qcb
 
 using namespace qcb;
@@ -427,6 +492,63 @@ int qcb_apply_dense(qcb_tableau* t, const qcb_tableau* c, int phases, void* stre
     apply_dense_kernel<256><<<blocks, threads, 0, st>>>(t->xzs, t->phases, t->rows, W, t->nqubits, c->xzs, c->phases, phases);
   else
     return fail(QCB_EUNSUPPORTED, "qcb_apply_dense: at most 8192 qubits");
+  QCB_LAUNCHED();
+  return QCB_OK;
+}
+
+// The no-alloc scratch of the current device: looked up once per device with
+// that device current, cleared once, then reused by every call.
+static std::mutex g_noalloc_mu;
+static uint32_t* g_noalloc_ptr[64] = {};
+
+static int noalloc_scratch(uint32_t** out) {
+  int dev = 0;
+  QCB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(QCB_EARG, "device ordinal out of range for the no-alloc scratch");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    uint32_t* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_acc);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+    e = cudaMemset(p, 0, sizeof(uint32_t) * QCB_NOALLOC_MAX_PAIRS);
+    if (e != cudaSuccess) return cuda_fail(e, "clearing the no-alloc scratch");
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(e, "clearing the no-alloc scratch");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return QCB_OK;
+}
+
+int qcb_mul_left_pauli_batch_noalloc(uint64_t* r_xz, uint8_t* r_phases, const uint64_t* l_xz,
+                                     const uint8_t* l_phases, uint32_t nqubits, uint32_t count,
+                                     int phases, void* stream) {
+  if (count == 0) return QCB_OK;
+  if (count > QCB_NOALLOC_MAX_PAIRS)
+    return fail(QCB_EARG, "qcb_mul_left_pauli_batch_noalloc: count " + std::to_string(count) +
+                              " exceeds the no-alloc scratch of " + std::to_string(QCB_NOALLOC_MAX_PAIRS) +
+                              " pairs; split the batch");
+  if (!r_xz || !l_xz) return fail(QCB_EARG, "qcb_mul_left_pauli_batch_noalloc: null Pauli words");
+  if (phases && (!r_phases || !l_phases)) return fail(QCB_EARG, "qcb_mul_left_pauli_batch_noalloc: null phases");
+  uint32_t* acc = nullptr;
+  if (int st = noalloc_scratch(&acc)) return st;
+  const uint64_t len = ((uint64_t)nqubits + 63) / 64;
+  cudaStream_t st = S(stream);
+  const bool vec = len % 2 == 0 && (((uintptr_t)r_xz | (uintptr_t)l_xz) & 15u) == 0;
+  const uint64_t work = vec ? len / 2 : len;
+  const uint32_t bx = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((work + 255) / 256, (uint64_t)device_sm_count() * 8));
+  if (len) {
+    const dim3 grid(bx, count);
+    if (vec) {
+      if (phases) mul_left_batch_kernel<2, true><<<grid, 256, 0, st>>>(r_xz, l_xz, len, acc);
+      else mul_left_batch_kernel<2, false><<<grid, 256, 0, st>>>(r_xz, l_xz, len, acc);
+    } else {
+      if (phases) mul_left_batch_kernel<1, true><<<grid, 256, 0, st>>>(r_xz, l_xz, len, acc);
+      else mul_left_batch_kernel<1, false><<<grid, 256, 0, st>>>(r_xz, l_xz, len, acc);
+    }
+    QCB_LAUNCHED();
+  }
+  mul_left_batch_finish_kernel<<<(count + 255) / 256, 256, 0, st>>>(r_phases, l_phases, acc, count, phases);
   QCB_LAUNCHED();
   return QCB_OK;
 }

@@ -149,6 +149,8 @@ def lib():
         "qcb_tableau_download": ([vp, vp, vp, vp], ctypes.c_int),
         "qcb_tableau_copy": ([vp, vp, vp], ctypes.c_int),
         "qcb_mul_left_pauli": ([vp, vp, ctypes.c_int, vp, vp], ctypes.c_int),
+        "qcb_mul_left_pauli_batch_noalloc": ([vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp],
+                                             ctypes.c_int),
         "qcb_mul_left_row": ([vp, u32, u32, ctypes.c_int, vp], ctypes.c_int),
         "qcb_mul_left_tableau_pauli": ([vp, vp, ctypes.c_int, vp], ctypes.c_int),
         "qcb_prodphase": ([vp, u32, vp, u32, vp, vp], ctypes.c_int),

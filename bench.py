@@ -160,6 +160,179 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+# Published single-thread reference times (README of the reference, Ryzen 9
+# 7950X, Julia 1.9.1), the denominators of vs_baseline for the tableau lines.
+REF_MS = {"mul_left": 13.355, "canonicalize_1000": 8.536, "dense_apply": 17.010,
+          "sCNOT": 3.043e-3, "project": 21.971e-3}
+
+
+def bench_tableau(args):
+    """Config-3 tableau kernels, one JSON line each: device time per call
+    (CUDA events around the call only; state copies happen outside), the
+    result checked against the oracle on the same input, and the oracle
+    single-threaded on the host as cpu_baseline.  Random states come from
+    seeded random H/S/CNOT circuits applied to the identity."""
+    import torch
+    import numpy as np
+    import qcb200
+    from qcb200 import tableau as Q
+    from qcb200._lib import check, lib, ptr
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the checker and the timed CPU baseline only
+
+    qcb200.ensure_init(0)
+    L = lib()
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    peak, peak_kind = load_peaks()
+    rng = np.random.default_rng(2024)
+
+    def device_ms(fn, reps, setup=None, warm=3):
+        ts = []
+        for i in range(warm + reps):
+            if setup:
+                setup()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i >= warm:
+                ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    def cpu_ms(fn, reps=3):
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        return statistics.median(ts)
+
+    def emit(metric, key, ms, config, cpu, extra=None):
+        out = {"metric": metric, "value": ms, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": 3,
+               "ms_per_step": ms, "higher_is_better": False, "scaling": "none",
+               "vs_baseline": (ms / REF_MS[key]) if key in REF_MS else None, "dtype": "u64 bit rows + u8 phases",
+               "data": "synthetic (seeded)", "config": config, "gpu_launches": None,
+               "cpu_baseline": {"value": cpu, "unit": "ms", "cores": 1, "kind": "port",
+                                "sample": "the oracle on the same input, one thread"}}
+        if extra:
+            out.update(extra)
+        print(json.dumps(out), flush=True)
+
+    def random_destabilizer(n, depth=12):
+        d = Q.one_destabilizer(n).to_gpu()
+        Q.apply_(d, Q.random_clifford_ops(n, depth, rng))
+        d.to_cpu()
+        return d
+
+    # ---- mul_left! of two 1e9-qubit Paulis (HBM: read 2 x 250 MB, write 250 MB)
+    n = 10**9
+    W = Q.nwords(n)
+    rx = rng.integers(0, 2**64, size=(1, W), dtype=np.uint64)
+    lx = rng.integers(0, 2**64, size=(1, W), dtype=np.uint64)
+    r = Q.Tableau(np.array([1], np.uint8), n, rx).to_gpu()
+    l = Q.Tableau(np.array([2], np.uint8), n, lx).to_gpu()
+    ms = device_ms(lambda: check(L.qcb_mul_left_pauli(r.dev.handle, l.dev.handle, 1, None, sp)), args.steps)
+    # correctness of one call against the oracle on a 1e8-qubit slice (X and Z halves)
+    m = 10**8
+    Wm = Q.nwords(m)
+    a = Q.Tableau(np.array([1], np.uint8), m, rx[:, :Wm].copy()).to_gpu()
+    b = Q.Tableau(np.array([2], np.uint8), m, lx[:, :Wm].copy()).to_gpu()
+    Q.mul_left_(a, b)
+    a.to_cpu()
+    ox, oph = oracle.mul_left_pauli(rx[0, :Wm], 1, lx[0, :Wm], 2)
+    assert np.array_equal(a.xzs[0], ox) and int(a.phases[0]) == oph
+    cpu = cpu_ms(lambda: oracle.mul_left_pauli(rx[0, :Wm], 1, lx[0, :Wm], 2)) * (n / m)
+    traffic = 3 * W * 8
+    emit("mul_left! of two 1e9-qubit Paulis", "mul_left", ms,
+         {"workload": "mul_left! r <- l * r, n = 1e9 qubits (250 MB per Pauli), phases on", "l2": "750 MB > L2"},
+         cpu, {"roofline": {"bound": "hbm", "achieved": traffic / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                            "frac": traffic / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+                            "algorithmic_bytes_per_launch": traffic}})
+    del r, l, a, b
+
+    # ---- canonicalize! of random full-rank stabilizers
+    for n in (1000, 2000, 4000):
+        d = random_destabilizer(n)
+        src = Q.Tableau(d.tab.phases[n:].copy(), n, d.tab.xzs[n:].copy())
+        work = Q.Tableau(src.phases.copy(), n, src.xzs.copy()).to_gpu()
+        pristine = Q.DeviceTableau(n, n)
+        pristine.upload(src.phases, src.xzs)
+        ms = device_ms(lambda: check(L.qcb_canonicalize(work.dev.handle, 1, n, 1, None, None, sp)), args.steps,
+                       setup=lambda: check(L.qcb_tableau_copy(work.dev.handle, pristine.handle, sp)))
+        work.to_cpu()
+        oph, oxz, _, _ = oracle.canonicalize(src.phases, src.xzs, n)
+        assert np.array_equal(work.xzs, oxz) and np.array_equal(work.phases, oph)
+        cpu = cpu_ms(lambda: oracle.canonicalize(src.phases, src.xzs, n), reps=1 if n > 2000 else 3)
+        emit(f"canonicalize! of a random {n}-qubit stabilizer", f"canonicalize_{n}", ms,
+             {"workload": f"canonicalize!(random_stabilizer({n})), phases on", "rows": n}, cpu)
+
+    # ---- project! of 1000 random Paulis in sequence on a random 1000-qubit Destabilizer
+    n, k = 1000, 1000
+    d = random_destabilizer(n)
+    xs = np.zeros((k, n), bool)
+    zs = np.zeros((k, n), bool)
+    for i in range(k):
+        w = int(rng.integers(1, n + 1))
+        q = rng.choice(n, w, replace=False)
+        kinds = rng.integers(1, 4, size=w)
+        xs[i, q] = kinds & 1 == 1
+        zs[i, q] = kinds & 2 == 2
+    P = Q.Tableau.from_bits(np.zeros(k, np.uint8), xs, zs).to_gpu()
+    state = Q.Destabilizer(Q.Tableau(d.tab.phases.copy(), n, d.tab.xzs.copy())).to_gpu()
+    pristine = Q.DeviceTableau(2 * n, n)
+    pristine.upload(d.tab.phases, d.tab.xzs)
+    rank = ctypes.c_int32(0)
+    anti = np.zeros(k, np.int32)
+    res = np.zeros(k, np.int32)
+    done = ctypes.c_uint32()
+    ms = device_ms(lambda: check(L.qcb_project(state.tab.dev.handle, Q.KIND["Destabilizer"], ctypes.byref(rank),
+                                               P.dev.handle, 1, 1, ptr(anti), ptr(res), ctypes.byref(done), sp)),
+                   max(3, args.steps // 4), setup=lambda: check(L.qcb_tableau_copy(state.tab.dev.handle, pristine.handle, sp)))
+    # oracle: the same sequence
+    def oracle_chain():
+        ph, xz = d.tab.phases.copy(), d.tab.xzs.copy()
+        outs = []
+        for i in range(k):
+            st, ph, xz, _, a_, r_ = oracle.project("Destabilizer", ph, xz, n, P.xzs[i], 0)
+            outs.append((a_, r_))
+        return outs
+    t0 = time.perf_counter()
+    outs = oracle_chain()
+    cpu = (time.perf_counter() - t0) * 1e3 / k
+    assert [o[0] for o in outs] == list(anti) and [o[1] for o in outs] == list(res)
+    emit("project! of a random Pauli on a random 1000-qubit Destabilizer", "project", ms / k,
+         {"workload": "1000 random Paulis (weight ~ U{1..n}) projected in sequence by one call, per projection",
+          "rows": 2 * n}, cpu)
+
+    # ---- dense apply! of tensor_pow(tCNOT, 500) to a random 1000-qubit stabilizer
+    n = 1000
+    d = random_destabilizer(n)
+    src = Q.Tableau(d.tab.phases[n:].copy(), n, d.tab.xzs[n:].copy())
+    work = Q.Tableau(src.phases.copy(), n, src.xzs.copy()).to_gpu()
+    pristine = Q.DeviceTableau(n, n)
+    pristine.upload(src.phases, src.xzs)
+    c = Q.tensor_pow(Q.tCNOT(), 500).to_gpu()
+    ms = device_ms(lambda: check(L.qcb_apply_dense(work.dev.handle, c.tab.dev.handle, 1, sp)), args.steps,
+                   setup=lambda: check(L.qcb_tableau_copy(work.dev.handle, pristine.handle, sp)))
+    work.to_cpu()
+    oph, oxz = oracle.apply_dense(src.phases, src.xzs, n, c.tab.phases, c.tab.xzs)
+    assert np.array_equal(work.xzs, oxz) and np.array_equal(work.phases, oph)
+    cpu = cpu_ms(lambda: oracle.apply_dense(src.phases, src.xzs, n, c.tab.phases, c.tab.xzs))
+    emit("dense apply! of tensor_pow(tCNOT, 500) to a random 1000-qubit stabilizer", "dense_apply", ms,
+         {"workload": "apply!(random_stabilizer(1000), tensor_pow(tCNOT, 500)), phases on"}, cpu)
+
+    # ---- one symbolic sCNOT(32, 504) on a random 1000-qubit stabilizer
+    from qcb200 import ops as O
+    gate = O.to_array([O.sCNOT(32, 504)])
+    ms = device_ms(lambda: check(L.qcb_apply_gates(work.dev.handle, ptr(gate), 1, 1, sp)), max(args.steps, 50))
+    cpu = cpu_ms(lambda: oracle.apply_gates(src.phases, src.xzs, n, gate), reps=20)
+    emit("symbolic apply! of sCNOT(32, 504) to a random 1000-qubit stabilizer", "sCNOT", ms,
+         {"workload": "apply!(random_stabilizer(1000), sCNOT(32, 504)): one launch"}, cpu)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -169,6 +342,7 @@ def main():
     ap.add_argument("--shots", type=int, default=SHOTS_PER_GPU)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--walker-tile", type=int, default=0)
+    ap.add_argument("--workload", default="frames", choices=["frames", "tableau"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -178,6 +352,10 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "tableau":
+        if rank == 0:
+            bench_tableau(args)
+        return
 
     import torch
     import torch.distributed as dist

@@ -202,17 +202,23 @@ __device__ __forceinline__ uint64_t g2(uint32_t op, uint64_t& x1, uint64_t& z1, 
 struct GateOp {
   uint32_t op, q1, q2, pad;
 };
+// Gates passed to one launch by value (kernel parameter space, 2 KB), so a
+// gate list needs no device allocation, no copy and no synchronisation.
+constexpr uint32_t GATE_BATCH = 128;
+struct GateBatch {
+  GateOp op[GATE_BATCH];
+};
 
-// Thread per row; the whole gate list is applied to that row in order.
+// Thread per row; the batch's gates are applied to that row in order.
 __global__ void apply_gates_kernel(uint64_t* xzs, uint8_t* ph, uint32_t rows, uint32_t W,
-                                   const GateOp* ops, uint32_t nops, int phases) {
+                                   const __grid_constant__ GateBatch ops, uint32_t nops, int phases) {
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= rows) return;
   uint64_t* row = xzs + (uint64_t)r * W;
   const uint32_t len = W / 2;
   uint32_t p = ph[r];
   for (uint32_t k = 0; k < nops; k++) {
-    const GateOp g = ops[k];
+    const GateOp g = ops.op[k];
     if (g.op < QCB_OP_CNOT) {
       const uint32_t q = g.q1, w = q >> 6, s = q & 63;
       uint64_t x = (row[w] >> s) & 1, z = (row[len + w] >> s) & 1;
@@ -465,14 +471,13 @@ int qcb_apply_gates(qcb_tableau* t, const qcb_op* ops, size_t n_ops, int phases,
   }
   if (g.empty() || !t->rows) return QCB_OK;
   cudaStream_t st = S(stream);
-  GateOp* d = nullptr;
-  QCB_CUDA(cudaMallocAsync(&d, g.size() * sizeof(GateOp), st));
-  QCB_CUDA(cudaMemcpyAsync(d, g.data(), g.size() * sizeof(GateOp), cudaMemcpyHostToDevice, st));
-  apply_gates_kernel<<<(t->rows + 127) / 128, 128, 0, st>>>(t->xzs, t->phases, t->rows, t->W, d,
-                                                            (uint32_t)g.size(), phases);
-  QCB_LAUNCHED();
-  QCB_CUDA(cudaFreeAsync(d, st));
-  QCB_CUDA(cudaStreamSynchronize(st));  // the host vector must outlive the copy
+  for (size_t k0 = 0; k0 < g.size(); k0 += GATE_BATCH) {
+    const uint32_t n = (uint32_t)std::min<size_t>(GATE_BATCH, g.size() - k0);
+    GateBatch b{};
+    std::copy(g.begin() + k0, g.begin() + k0 + n, b.op);
+    apply_gates_kernel<<<(t->rows + 127) / 128, 128, 0, st>>>(t->xzs, t->phases, t->rows, t->W, b, n, phases);
+    QCB_LAUNCHED();
+  }
   return QCB_OK;
 }
 

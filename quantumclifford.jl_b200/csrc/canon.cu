@@ -109,11 +109,12 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a)
         if (lane == 0) slot[step & 1] = b;
       }
       cl.sync();
-      if (tid == 0) {
-        uint32_t k = 0xFFFFFFFFu;
-        for (uint32_t q = 0; q < CS; q++) k = min(k, *cl.map_shared_rank(&slot[step & 1], q));
-        ctl[0] = k;
-        if (k != 0xFFFFFFFFu) {
+      if (warp == 0) {
+        // the cluster's candidates, one CTA per lane
+        uint32_t k = lane < CS ? *cl.map_shared_rank(&slot[step & 1], lane) : 0xFFFFFFFFu;
+        k = __reduce_min_sync(0xFFFFFFFFu, k);
+        if (lane == 0) ctl[0] = k;
+        if (lane == 0 && k != 0xFFFFFFFFu) {
           // rowswap!(state, k, i) on logical positions
           const uint32_t pstar = inv[k], aphys = inv[i];
           inv[i] = pstar;
@@ -294,7 +295,8 @@ static size_t canon_smem(uint32_t rows, uint32_t W, uint32_t RB, bool smem_rows)
   return (b + 15) / 16 * 16;
 }
 
-static uint32_t g_canon_cs = 0;  // tuner override (0 = automatic)
+static uint32_t g_canon_cs = 0;       // tuner override (0 = automatic)
+static uint32_t g_canon_threads = 0;  // tuner override (0 = automatic)
 
 static CanonPlan canon_plan(uint32_t rows, uint32_t W) {
   const size_t maxsm = (size_t)device_max_smem_optin();
@@ -338,7 +340,7 @@ int canonicalize_view(uint64_t* xzs, uint8_t* ph, uint32_t rows, uint32_t n, uin
   if (p.cs > 8) QCB_CUDA(cudaFuncSetAttribute(canon_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(p.cs);
-  cfg.blockDim = dim3(CANON_THREADS);
+  cfg.blockDim = dim3(g_canon_threads ? g_canon_threads : CANON_THREADS);
   cfg.dynamicSmemBytes = p.smem_bytes;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -370,6 +372,7 @@ int generate_dev(uint64_t* pauli, uint8_t* pph, const uint64_t* xzs, const uint8
 }
 
 void set_canon_cluster(uint32_t cs) { g_canon_cs = cs; }
+void set_canon_threads(uint32_t n) { g_canon_threads = n; }
 
 }  // namespace qcb
 

@@ -92,7 +92,7 @@ __device__ __forceinline__ void gate2_xz(uint32_t op, uint32_t& x1, uint32_t& z1
   }
 }
 
-// The frame tile.  SMEM: plane p of tile column cl at sm[p*T + cl].
+// The frame tile.  SMEM: plane p of tile column cl at sm[p*T + cl] (T even).
 // Global: plane p maps to frame plane pmap[p] (a shared-memory table).
 template <bool SMEM>
 struct Tile {
@@ -101,9 +101,14 @@ struct Tile {
   const uint32_t* pmap;
   uint64_t pitch;
   uint32_t T;
-  __device__ __forceinline__ uint32_t* at(uint32_t p, uint32_t cl, uint64_t cg) const {
+  // word of plane p at tile column cl (frame column cg)
+  __device__ __forceinline__ uint32_t* at32(uint32_t p, uint32_t cl, uint64_t cg) const {
     if (SMEM) return sm + p * T + cl;
     return planes + (uint64_t)pmap[p] * pitch + cg;
+  }
+  // the two words of plane p at the even tile column cw (frame column cg)
+  __device__ __forceinline__ uint2* at2(uint32_t p, uint32_t cw, uint64_t cg) const {
+    return (uint2*)at32(p, cw, cg);
   }
 };
 
@@ -180,11 +185,11 @@ __device__ __forceinline__ void apply_code(const Tile<SMEM>& F, const uint4& e, 
   const uint64_t cg = c0 + cl;
   if (cg >= ncols) return;
   const uint32_t bit = 1u << (pos & 31);
-  if (code & 1) atomicXor(F.at(e.z & 0xFFFFu, cl, cg), bit);
-  if (code & 2) atomicXor(F.at(e.z >> 16, cl, cg), bit);
+  if (code & 1) atomicXor(F.at32(e.z & 0xFFFFu, cl, cg), bit);
+  if (code & 2) atomicXor(F.at32(e.z >> 16, cl, cg), bit);
   if ((e.y & 0xFFu) == QCB_OP_DEPOL2) {
-    if (code & 4) atomicXor(F.at(e.w & 0xFFFFu, cl, cg), bit);
-    if (code & 8) atomicXor(F.at(e.w >> 16, cl, cg), bit);
+    if (code & 4) atomicXor(F.at32(e.w & 0xFFFFu, cl, cg), bit);
+    if (code & 8) atomicXor(F.at32(e.w >> 16, cl, cg), bit);
   }
 }
 
@@ -281,16 +286,20 @@ __device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<
 }
 
 // ---------------------------------------------------------------- walker
-// One CTA owns a tile of T shot columns (T x 32 shots) and runs the whole
-// program on it.  Thread (rr, cl) = (tid / T, tid % T) handles column cl and
-// every R-th op of a segment, so a warp covers 32 columns of one op
-// (conflict-free shared accesses, broadcast operand reads from the staged
-// window); one barrier per segment orders the segments.
+__device__ __forceinline__ uint2 xor2(uint2 a, uint2 b) { return make_uint2(a.x ^ b.x, a.y ^ b.y); }
+
+// One CTA owns a tile of T shot columns (T even; T x 32 shots) and runs the
+// whole program on it.  Thread (rr, cp) = (tid / TP, tid % TP), TP = T / 2,
+// handles the column pair (2cp, 2cp + 1) -- one 64-bit shared-memory word per
+// plane, so each op's operand decode and address arithmetic serve two columns
+// -- and every R-th op of a segment; a warp covers consecutive pairs of one
+// op (broadcast operand reads from the staged window).  One barrier per
+// record orders the records.
 template <bool SMEM, bool PHILOX>
 __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
   extern __shared__ __align__(128) uint32_t sm[];
-  const uint32_t tid = threadIdx.x, T = a.tile, R = blockDim.x / T;
-  const uint32_t cl = tid % T, rr = tid / T;
+  const uint32_t tid = threadIdx.x, T = a.tile, TP = T / 2, R = blockDim.x / TP;
+  const uint32_t cp = tid % TP, rr = tid / TP, cw = 2 * cp;  // cw: tile column of the pair
   const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
   const uint64_t pitch = a.pitch;
   // layout: [frame tile | pmap] [window 0] [window 1] [2 mbarriers]
@@ -321,29 +330,32 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
   bool failed = false;
 
   for (uint64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-    const uint64_t c0 = tile * T, cg = c0 + cl;
+    const uint64_t c0 = tile * T, cg = c0 + cw;  // the pair's first column in the frame
     const bool act = rr < R && cg < a.ncols;
-    const uint64_t col = a.col0 + cg;
+    const bool two = cg + 1 < a.ncols;          // its second column exists
+    const uint64_t col = a.col0 + cg, col1 = col + 1;
     const uint32_t clo = (uint32_t)col, chi = (uint32_t)(col >> 32);
+    const uint32_t clo1 = (uint32_t)col1, chi1 = (uint32_t)(col1 >> 32);
     const Tile<SMEM> F{sm, a.planes, sm, pitch, T};
 
     // ---- initial frame
     if (a.fresh) {
       for (uint32_t qb = rr; qb * 4 < a.nq1; qb += R) {
         if (!act) break;
-        uint32_t o[4];
+        uint32_t o[4], u[4];
         philox4x32_10(qb, clo, chi, TAG_INITZ, k0, k1, o);
+        philox4x32_10(qb, clo1, chi1, TAG_INITZ, k0, k1, u);
 #pragma unroll
         for (uint32_t j = 0; j < 4; j++) {
           const uint32_t q = qb * 4 + j;
           if (q >= a.nq1) break;
           const uint32_t s = (SMEM && q < a.qubit_slot_len) ? __ldg(a.qubit_slot + q) : BIT_NONE;
           if (SMEM && s != BIT_NONE) {
-            *F.at(2 * s, cl, cg) = 0u;
-            *F.at(2 * s + 1, cl, cg) = o[j];
+            *F.at2(2 * s, cw, cg) = make_uint2(0u, 0u);
+            *F.at2(2 * s + 1, cw, cg) = make_uint2(o[j], u[j]);
           } else {
-            a.planes[(uint64_t)(2 * q) * pitch + cg] = 0u;
-            a.planes[(uint64_t)(2 * q + 1) * pitch + cg] = o[j];
+            *(uint2*)(a.planes + (uint64_t)(2 * q) * pitch + cg) = make_uint2(0u, 0u);
+            *(uint2*)(a.planes + (uint64_t)(2 * q + 1) * pitch + cg) = make_uint2(o[j], u[j]);
           }
         }
       }
@@ -351,14 +363,16 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
       for (uint32_t s = rr; s < a.nslots; s += R) {
         if (!act) break;
         const uint32_t q = __ldg(a.slot_qubit + s);
-        *F.at(2 * s, cl, cg) = a.planes[(uint64_t)(2 * q) * pitch + cg];
-        *F.at(2 * s + 1, cl, cg) = a.planes[(uint64_t)(2 * q + 1) * pitch + cg];
+        *F.at2(2 * s, cw, cg) = *(const uint2*)(a.planes + (uint64_t)(2 * q) * pitch + cg);
+        *F.at2(2 * s + 1, cw, cg) = *(const uint2*)(a.planes + (uint64_t)(2 * q + 1) * pitch + cg);
       }
     }
-    uint64_t ep = 0, ee = 0;
+    // mask mode: the events of the pair's columns, [ep[h], ep[h + 1]) for column h
+    uint64_t ep[3] = {0, 0, 0};
     if (!PHILOX && rr == 0 && act) {
-      ep = a.ev_off[cg];
-      ee = a.ev_off[cg + 1];
+      ep[0] = a.ev_off[cg];
+      ep[1] = a.ev_off[cg + 1];
+      ep[2] = two ? a.ev_off[cg + 2] : ep[1];
     }
 
     // ---- the program, window by window
@@ -393,21 +407,21 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
           uint32_t j = rr;
           for (; j + R < cnt; j += 2 * R) {
             const uint2 o = en[j], u = en[j + R];
-            uint32_t *pxc = F.at(o.x & 0xFFFFu, cl, cg), *pzc = F.at(o.x >> 16, cl, cg);
-            uint32_t *pxt = F.at(o.y & 0xFFFFu, cl, cg), *pzt = F.at(o.y >> 16, cl, cg);
-            uint32_t *qxc = F.at(u.x & 0xFFFFu, cl, cg), *qzc = F.at(u.x >> 16, cl, cg);
-            uint32_t *qxt = F.at(u.y & 0xFFFFu, cl, cg), *qzt = F.at(u.y >> 16, cl, cg);
-            const uint32_t xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
-            const uint32_t yxc = *qxc, yzc = *qzc, yxt = *qxt, yzt = *qzt;
-            *pxt = xt ^ xc; *pzc = zc ^ zt;
-            *qxt = yxt ^ yxc; *qzc = yzc ^ yzt;
+            uint2 *pxc = F.at2(o.x & 0xFFFFu, cw, cg), *pzc = F.at2(o.x >> 16, cw, cg);
+            uint2 *pxt = F.at2(o.y & 0xFFFFu, cw, cg), *pzt = F.at2(o.y >> 16, cw, cg);
+            uint2 *qxc = F.at2(u.x & 0xFFFFu, cw, cg), *qzc = F.at2(u.x >> 16, cw, cg);
+            uint2 *qxt = F.at2(u.y & 0xFFFFu, cw, cg), *qzt = F.at2(u.y >> 16, cw, cg);
+            const uint2 xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
+            const uint2 yxc = *qxc, yzc = *qzc, yxt = *qxt, yzt = *qzt;
+            *pxt = xor2(xt, xc); *pzc = xor2(zc, zt);
+            *qxt = xor2(yxt, yxc); *qzc = xor2(yzc, yzt);
           }
           for (; j < cnt; j += R) {
             const uint2 o = en[j];
-            uint32_t *pxc = F.at(o.x & 0xFFFFu, cl, cg), *pzc = F.at(o.x >> 16, cl, cg);
-            uint32_t *pxt = F.at(o.y & 0xFFFFu, cl, cg), *pzt = F.at(o.y >> 16, cl, cg);
-            const uint32_t xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
-            *pxt = xt ^ xc; *pzc = zc ^ zt;
+            uint2 *pxc = F.at2(o.x & 0xFFFFu, cw, cg), *pzc = F.at2(o.x >> 16, cw, cg);
+            uint2 *pxt = F.at2(o.y & 0xFFFFu, cw, cg), *pzt = F.at2(o.y >> 16, cw, cg);
+            const uint2 xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
+            *pxt = xor2(xt, xc); *pzc = xor2(zc, zt);
           }
           break;
         }
@@ -417,10 +431,10 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
           const uint2* en = (const uint2*)e;
           for (uint32_t j = rr; j < cnt; j += R) {
             const uint2 o = en[j];
-            uint32_t *pxa = F.at(o.x & 0xFFFFu, cl, cg), *pza = F.at(o.x >> 16, cl, cg);
-            uint32_t *pxb = F.at(o.y & 0xFFFFu, cl, cg), *pzb = F.at(o.y >> 16, cl, cg);
-            const uint32_t xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
-            *pza = za ^ xb; *pzb = zb ^ xa;
+            uint2 *pxa = F.at2(o.x & 0xFFFFu, cw, cg), *pza = F.at2(o.x >> 16, cw, cg);
+            uint2 *pxb = F.at2(o.y & 0xFFFFu, cw, cg), *pzb = F.at2(o.y >> 16, cw, cg);
+            const uint2 xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
+            *pza = xor2(za, xb); *pzb = xor2(zb, xa);
           }
           break;
         }
@@ -431,10 +445,14 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
           const uint2* en = (const uint2*)e;
           for (uint32_t j = rr; j < cnt; j += R) {
             const uint2 o = en[j];
-            uint32_t *px = F.at(o.x & 0xFFFFu, cl, cg), *pz = F.at(o.x >> 16, cl, cg);
-            uint32_t x = *px, z = *pz;
-            if (kind == SEG_S) z ^= x;
-            else gate1_xz(o.y, x, z);
+            uint2 *px = F.at2(o.x & 0xFFFFu, cw, cg), *pz = F.at2(o.x >> 16, cw, cg);
+            uint2 x = *px, z = *pz;
+            if (kind == SEG_S) {
+              z = xor2(z, x);
+            } else {
+              gate1_xz(o.y, x.x, z.x);
+              gate1_xz(o.y, x.y, z.y);
+            }
             *px = x; *pz = z;
           }
           break;
@@ -445,10 +463,11 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
           const uint4* en = (const uint4*)e;
           for (uint32_t j = rr; j < cnt; j += R) {
             const uint4 o = en[j];
-            uint32_t *pxa = F.at(o.x & 0xFFFFu, cl, cg), *pza = F.at(o.x >> 16, cl, cg);
-            uint32_t *pxb = F.at(o.y & 0xFFFFu, cl, cg), *pzb = F.at(o.y >> 16, cl, cg);
-            uint32_t xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
-            gate2_xz(o.z, xa, za, xb, zb);
+            uint2 *pxa = F.at2(o.x & 0xFFFFu, cw, cg), *pza = F.at2(o.x >> 16, cw, cg);
+            uint2 *pxb = F.at2(o.y & 0xFFFFu, cw, cg), *pzb = F.at2(o.y >> 16, cw, cg);
+            uint2 xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
+            gate2_xz(o.z, xa.x, za.x, xb.x, zb.x);
+            gate2_xz(o.z, xa.y, za.y, xb.y, zb.y);
             *pxa = xa; *pza = za; *pxb = xb; *pzb = zb;
           }
           break;
@@ -459,7 +478,7 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
           const uint2* en = (const uint2*)e;
           for (uint32_t j = rr; j < cnt; j += R) {
             const uint2 o = en[j];
-            a.rec[(uint64_t)o.y * pitch + cg] = *F.at(o.x, cl, cg);
+            *(uint2*)(a.rec + (uint64_t)o.y * pitch + cg) = *F.at2(o.x, cw, cg);
           }
           break;
         }
@@ -471,26 +490,29 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
             uint4 ent[4];
 #pragma unroll
             for (int i = 0; i < 4; i++) ent[i] = en[4 * g + i];
-            uint32_t o[4] = {0, 0, 0, 0};
+            uint32_t o[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
             if (PHILOX) {
               uint32_t blk = 0;
 #pragma unroll
               for (int i = 0; i < 4; i++)
                 if (ent[i].z != MRZ_PAD) blk = ent[i].z >> 2;
               philox4x32_10(blk, clo, chi, TAG_RESET, k0, k1, o);
+              philox4x32_10(blk, clo1, chi1, TAG_RESET, k0, k1, u);
             }
 #pragma unroll
             for (int i = 0; i < 4; i++) {
               if (ent[i].z == MRZ_PAD) continue;
-              uint32_t* px = F.at(ent[i].x & 0xFFFFu, cl, cg);
-              uint32_t* pz = F.at(ent[i].x >> 16, cl, cg);
-              const uint32_t x = *px, z = *pz;
-              uint32_t rb;
-              if (PHILOX) rb = o[i];
-              else rb = a.reset_planes ? __ldg(a.reset_planes + (uint64_t)ent[i].z * a.reset_pitch + cg) : 0u;
-              if (ent[i].y != BIT_NONE) a.rec[(uint64_t)ent[i].y * pitch + cg] = x;
-              *px = 0u;
-              *pz = z ^ rb;
+              uint2* px = F.at2(ent[i].x & 0xFFFFu, cw, cg);
+              uint2* pz = F.at2(ent[i].x >> 16, cw, cg);
+              const uint2 x = *px, z = *pz;
+              uint2 rb = make_uint2(o[i], u[i]);
+              if (!PHILOX) {
+                const uint32_t* rp = a.reset_planes + (uint64_t)ent[i].z * a.reset_pitch + cg;
+                rb = a.reset_planes ? make_uint2(__ldg(rp), two ? __ldg(rp + 1) : 0u) : make_uint2(0u, 0u);
+              }
+              if (ent[i].y != BIT_NONE) *(uint2*)(a.rec + (uint64_t)ent[i].y * pitch + cg) = x;
+              *px = make_uint2(0u, 0u);
+              *pz = xor2(z, rb);
             }
           }
           break;
@@ -514,26 +536,30 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
               }
             }
           } else if (rr == 0 && act) {
-            // this column's events are sorted by trial (site*32 + lane)
-            for (uint32_t i = 0; i < cnt; i++) {
-              const uint4 st = en[i];
-              const uint64_t lo_t = (uint64_t)st.x * 32u, lim = lo_t + 32u;
-              uint64_t lo = ep, hi = ee;
-              while (lo < hi) {
-                const uint64_t mid = (lo + hi) >> 1;
-                if ((__ldg(a.ev_data + mid) >> 8) < lo_t) lo = mid + 1;
-                else hi = mid;
-              }
-              for (uint64_t k = lo; k < ee; k++) {
-                const uint64_t d = __ldg(a.ev_data + k);
-                const uint64_t t = d >> 8;
-                if (t >= lim) break;
-                const uint32_t code = (uint32_t)(d & 0xFF), bit = 1u << (t & 31);
-                if (code & 1) *F.at(st.z & 0xFFFFu, cl, cg) ^= bit;
-                if (code & 2) *F.at(st.z >> 16, cl, cg) ^= bit;
-                if ((st.y & 0xFFu) == QCB_OP_DEPOL2) {
-                  if (code & 4) *F.at(st.w & 0xFFFFu, cl, cg) ^= bit;
-                  if (code & 8) *F.at(st.w >> 16, cl, cg) ^= bit;
+            // each column's events are sorted by trial (site*32 + lane)
+            for (uint32_t hc = 0; hc < 2; hc++) {
+              const uint64_t eb = ep[hc], ee = ep[hc + 1];
+              if (eb == ee) continue;
+              for (uint32_t i = 0; i < cnt; i++) {
+                const uint4 st = en[i];
+                const uint64_t lo_t = (uint64_t)st.x * 32u, lim = lo_t + 32u;
+                uint64_t lo = eb, hi = ee;
+                while (lo < hi) {
+                  const uint64_t mid = (lo + hi) >> 1;
+                  if ((__ldg(a.ev_data + mid) >> 8) < lo_t) lo = mid + 1;
+                  else hi = mid;
+                }
+                for (uint64_t k = lo; k < ee; k++) {
+                  const uint64_t d = __ldg(a.ev_data + k);
+                  const uint64_t t = d >> 8;
+                  if (t >= lim) break;
+                  const uint32_t code = (uint32_t)(d & 0xFF), bit = 1u << (t & 31);
+                  if (code & 1) *F.at32(st.z & 0xFFFFu, cw + hc, cg + hc) ^= bit;
+                  if (code & 2) *F.at32(st.z >> 16, cw + hc, cg + hc) ^= bit;
+                  if ((st.y & 0xFFu) == QCB_OP_DEPOL2) {
+                    if (code & 4) *F.at32(st.w & 0xFFFFu, cw + hc, cg + hc) ^= bit;
+                    if (code & 8) *F.at32(st.w >> 16, cw + hc, cg + hc) ^= bit;
+                  }
                 }
               }
             }
@@ -550,9 +576,6 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
         kwin++;
         need_window = true;
         if (kind == SEG_END) break;
-      } else if (h.y & FLAG_NO_BARRIER) {
-        // a part of a split record: the next part needs no barrier, but the
-        // loop head has one; harmless
       }
     }
     if (failed) break;
@@ -561,15 +584,15 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
     for (uint32_t s = rr; s < a.nslots; s += R) {
       if (!act) break;
       const uint32_t q = __ldg(a.slot_qubit + s), sw = __ldg(a.slot_swap + s);
+      uint2* gx = (uint2*)(a.planes + (uint64_t)(2 * q) * pitch + cg);
+      uint2* gz = (uint2*)(a.planes + (uint64_t)(2 * q + 1) * pitch + cg);
       if (SMEM) {
-        a.planes[(uint64_t)(2 * q) * pitch + cg] = *F.at(2 * s + sw, cl, cg);
-        a.planes[(uint64_t)(2 * q + 1) * pitch + cg] = *F.at(2 * s + 1 - sw, cl, cg);
+        *gx = *F.at2(2 * s + sw, cw, cg);
+        *gz = *F.at2(2 * s + 1 - sw, cw, cg);
       } else if (sw) {
-        uint32_t* px = a.planes + (uint64_t)(2 * q) * pitch + cg;
-        uint32_t* pz = a.planes + (uint64_t)(2 * q + 1) * pitch + cg;
-        const uint32_t x = *px, z = *pz;
-        *px = z;
-        *pz = x;
+        const uint2 x = *gx, z = *gz;
+        *gx = z;
+        *gz = x;
       }
     }
     __syncthreads();
@@ -757,13 +780,15 @@ struct WalkConfig {
 
 static uint32_t g_tile_override = 0;
 
-// Tile width for ncols columns with tiles of at most tmax columns: the fewest
-// waves of one CTA per SM, then the narrowest tile that still needs no more
-// waves, so that the last wave is as full as the others.
+// Tile width (even: threads own column pairs) for ncols columns with tiles of
+// at most tmax columns: the fewest waves of one CTA per SM, then the narrowest
+// tile that still needs no more waves, so that the last wave is as full as
+// the others.
 static uint32_t balanced_tile(uint64_t ncols, uint32_t tmax) {
+  tmax &= ~1u;
   const uint64_t nsm = (uint64_t)std::max(device_sm_count(), 1);
   const uint64_t waves = std::max<uint64_t>(1, (ncols + nsm * tmax - 1) / (nsm * tmax));
-  const uint64_t t = (ncols + nsm * waves - 1) / (nsm * waves);
+  const uint64_t t = ((ncols + nsm * waves - 1) / (nsm * waves) + 1) & ~1ull;
   return (uint32_t)std::min<uint64_t>(tmax, std::max<uint64_t>(t, 16));
 }
 
@@ -784,12 +809,12 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   if (T) {
     wc.smem = true;
     wc.T = T;
-    wc.nth = (768u / T) * T;  // the kernel is compiled for at most 768 threads
+    wc.nth = (768u / (T / 2)) * (T / 2);  // column pairs; the kernel's launch bound is 768
     wc.smem_bytes = per_col * T + stage;
   } else {
     wc.smem = false;
     wc.T = balanced_tile(f->ncols, 128);
-    wc.nth = (768u / wc.T) * wc.T;
+    wc.nth = (768u / (wc.T / 2)) * (wc.T / 2);
     wc.smem_bytes = (size_t)2 * p->nslots * 4 + stage;
   }
   const uint64_t tiles = (f->ncols + wc.T - 1) / wc.T;

@@ -106,7 +106,7 @@ int qcb_tune_set(const char* key, int64_t value) {
   const std::string k(key);
   if (value < 0 || value > 1024) return fail(QCB_EARG, "qcb_tune_set: value out of range");
   if (k == "walker_tile") {
-    if (value && (value < 8 || value > 256)) return fail(QCB_EARG, "walker_tile must be 0 (automatic) or 8..256");
+    if (value && (value < 8 || value > 256 || value % 2)) return fail(QCB_EARG, "walker_tile must be 0 (automatic) or even, 8..256");
     set_walker_tile((uint32_t)value);
   } else if (k == "canon_threads") {
     if (value && (value < 64 || value > 1024 || value % 32)) return fail(QCB_EARG, "canon_threads must be 0 or 64..1024, a multiple of 32");

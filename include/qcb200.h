@@ -58,6 +58,10 @@ enum qcb_opcode {
   QCB_OP_X = 5, QCB_OP_Y = 6, QCB_OP_Z = 7,
   QCB_OP_SQRTX = 8, QCB_OP_INVSQRTX = 9, QCB_OP_SQRTY = 10, QCB_OP_INVSQRTY = 11,
   QCB_OP_HXY = 12, QCB_OP_HYZ = 13, QCB_OP_CXYZ = 14, QCB_OP_CZYX = 15,
+  /* SingleQubitOperator(q1, xx, xz, zx, zz, px, pz) (src/symbolic_cliffords.jl
+   * :168-206): its flags packed in q2, bit 0 xx, 1 xz, 2 zx, 3 zz, 4 px, 5 pz.
+   * x' = (x & xx) ^ (z & zx), z' = (x & xz) ^ (z & zz).                      */
+  QCB_OP_SQO = 16,
   /* two-qubit symbolic Cliffords */
   QCB_OP_CNOT = 32, QCB_OP_CPHASE = 33, QCB_OP_SWAP = 34,
   QCB_OP_ZCX = 35, QCB_OP_ZCY = 36, QCB_OP_ZCZ = 37,
@@ -65,6 +69,11 @@ enum qcb_opcode {
   QCB_OP_YCX = 41, QCB_OP_YCY = 42, QCB_OP_YCZ = 43,
   /* measurements (frame semantics: src/pauli_frames.jl:74-116) */
   QCB_OP_MZ = 64, QCB_OP_MRZ = 65, QCB_OP_MX = 66, QCB_OP_MRX = 67,
+  /* ClassicalXOR(bits, store) (src/misc_ops.jl:198-205; frame semantics
+   * src/pauli_frames.jl:63-72): record bit `bit` <- XOR of n = q1 record bits
+   * (1 <= n <= 30), which follow in the next ceil(n/3) ops of opcode
+   * QCB_OP_XOR_BITS, three 1-based bits each in q1, q2, bit (0 = none).      */
+  QCB_OP_XOR = 68, QCB_OP_XOR_BITS = 69,
   /* noise */
   QCB_OP_PAULI_NOISE = 96, /* PauliError(q, px, py, pz): NoiseOp(PauliNoise)   */
   QCB_OP_DEPOL1 = 97,      /* NoiseOp(DepolarizationNoise(p), (q1,))           */

@@ -85,6 +85,16 @@ extern "C" void oracle_philox4x32_10(const u32 ctr_in[4], const u32 key_in[2], u
 // Returns the phase flag word (lanes whose phase gains +2).
 static inline u64 gate1(u32 op, u64& x, u64& z) {
   u64 X = x, Z = z, ph = 0;
+  if ((op & 0xFF) == QCB_OP_SQO) {
+    // SingleQubitOperator (src/symbolic_cliffords.jl:178-206); flags in op >> 8:
+    // xx, xz, zx, zz, px, pz
+    u32 f = op >> 8;
+    bool xx = f & 1, xz = f & 2, zx = f & 4, zz = f & 8, px = f & 16, pz = f & 32;
+    bool anticom = (!zz && xz && !xx && zx) || (zz && !xz && xx && zx) || (zz && xz && xx && !zx);
+    x = (xx ? X : 0) ^ (zx ? Z : 0);
+    z = (xz ? X : 0) ^ (zz ? Z : 0);
+    return (px ? X : 0) ^ (pz ? Z : 0) ^ (anticom ? (X & Z) : 0);
+  }
   switch (op) {
     case QCB_OP_I: break;
     case QCB_OP_H: x = Z; z = X; ph = X & Z; break;
@@ -148,7 +158,11 @@ static inline u64 gate2(u32 op, u64& x1, u64& z1, u64& x2, u64& z2) {
   return ph;
 }
 
-static inline bool is1q(u32 op) { return op >= QCB_OP_I && op <= QCB_OP_CZYX; }
+static inline bool is1q(u32 op) { return op >= QCB_OP_I && op <= QCB_OP_SQO; }
+// gate code of a 1-qubit op: SingleQubitOperator carries its flags (q2) along
+static inline u32 code1(const qcb_op& op) {
+  return op.opcode == QCB_OP_SQO ? op.opcode | ((op.q2 & 63u) << 8) : op.opcode;
+}
 static inline bool is2q(u32 op) { return op >= QCB_OP_CNOT && op <= QCB_OP_YCZ; }
 
 // ---------------------------------------------------------------- Pauli rows
@@ -443,7 +457,7 @@ int oracle_apply_gates(u64* xzs, u8* ph, size_t rows, u32 n, const qcb_op* ops, 
       for (size_t r = 0; r < rows; r++) {
         u64* row = xzs + r * W;
         u64 x = (row[wi] & m) ? 1 : 0, z = (row[len + wi] & m) ? 1 : 0;
-        u64 f = gate1(op.opcode, x, z) & 1;
+        u64 f = gate1(code1(op), x, z) & 1;
         row[wi] = (row[wi] & ~m) | (x & 1 ? m : 0);
         row[len + wi] = (row[len + wi] & ~m) | (z & 1 ? m : 0);
         if (phases && f) ph[r] = (u8)((ph[r] + 2) & 3);
@@ -528,6 +542,26 @@ static inline void frame_flip(Frame& F, u32 q, u64 f, u32 digit) {
 }
 
 // One op on frames [f0, f1).  reset_index = index of this op among resets.
+// ClassicalXOR (src/pauli_frames.jl:63-72): per frame, record bit `store`
+// <- XOR of the listed bits, all read before the store is written.  ops[k] is
+// the QCB_OP_XOR header; returns the number of QCB_OP_XOR_BITS ops it used.
+static size_t frame_xor(Frame& F, const qcb_op* ops, size_t nops, size_t k, u64 f0, u64 f1) {
+  const qcb_op& op = ops[k];
+  const u32 n = op.q1;
+  const size_t npay = (n + 2) / 3;
+  std::vector<u32> bits;
+  for (size_t j = 1; j <= npay && k + j < nops; j++)
+    for (u32 b : {ops[k + j].q1, ops[k + j].q2, ops[k + j].bit})
+      if (b && bits.size() < n) bits.push_back(b - 1);
+  u8* dst = F.meas + (size_t)(op.bit - 1) * F.S;
+  for (u64 f = f0; f < f1; f++) {
+    u8 v = 0;
+    for (u32 b : bits) v ^= F.meas[(size_t)b * F.S + f];
+    dst[f] = v;
+  }
+  return npay;
+}
+
 static void frame_op(Frame& F, const qcb_op& op, size_t op_index, u64 f0, u64 f1,
                      NoiseFeed& nf, Xoshiro* rng, size_t reset_index) {
   u32 oc = op.opcode;
@@ -537,7 +571,7 @@ static void frame_op(Frame& F, const qcb_op& op, size_t op_index, u64 f0, u64 f1
     for (u64 f = f0; f < f1; f++) {
       u64& xw = F.xw(q, f); u64& zw = F.zw(q, f);
       u64 x = (xw & m) ? 1 : 0, z = (zw & m) ? 1 : 0;
-      gate1(oc, x, z);
+      gate1(code1(op), x, z);
       xw = (xw & ~m) | ((x & 1) ? m : 0);
       zw = (zw & ~m) | ((z & 1) ? m : 0);
     }
@@ -655,6 +689,10 @@ void oracle_pftrajectories(u64* xzs, u8* meas, u64 S, u32 nq1, u32 nbits, const 
     Xoshiro rng(seed * 0x9E3779B97F4A7C15ull + (u64)ti + 1);
     size_t reset_index = 0;
     for (size_t k = 0; k < nops; k++) {
+      if (ops[k].opcode == QCB_OP_XOR) {
+        k += frame_xor(F, ops, nops, k, b, e);
+        continue;
+      }
       frame_op(F, ops[k], k, b, e, nf, &rng, reset_index);
       if (is_reset(ops[k].opcode)) reset_index++;
     }
@@ -825,6 +863,10 @@ void oracle_pftrajectories_philox(u64* xzs, u8* meas, u64 S, u32 nq1, u32 nbits,
       for (size_t k = 0; k < nops; k++) {
         const qcb_op& op = ops[k];
         const u32 oc = op.opcode;
+        if (oc == QCB_OP_XOR) {
+          k += frame_xor(F, ops, nops, k, f0, f1);
+          continue;
+        }
         if (is_noise(oc)) {
           const Site& st = sites[(size_t)site_of_op[k]];
           for (const Event& e : ev[(size_t)site_of_op[k]]) {

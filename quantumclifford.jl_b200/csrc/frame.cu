@@ -63,6 +63,13 @@ struct WalkArgs {
 // track no phase (src/pauli_frames.jl:58-61).
 __device__ __forceinline__ void gate1_xz(uint32_t op, uint32_t& x, uint32_t& z) {
   const uint32_t X = x, Z = z;
+  if ((op & 0xFFu) == QCB_OP_SQO) {  // SingleQubitOperator, flags in bits 8..13
+    const uint32_t xx = 0u - ((op >> 8) & 1u), xz = 0u - ((op >> 9) & 1u);
+    const uint32_t zx = 0u - ((op >> 10) & 1u), zz = 0u - ((op >> 11) & 1u);
+    x = (X & xx) ^ (Z & zx);
+    z = (X & xz) ^ (Z & zz);
+    return;
+  }
   switch (op) {
     case QCB_OP_H: case QCB_OP_SQRTY: case QCB_OP_INVSQRTY: x = Z; z = X; break;
     case QCB_OP_HXY: case QCB_OP_S: case QCB_OP_SDAG: z = X ^ Z; break;
@@ -514,6 +521,18 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
               *px = make_uint2(0u, 0u);
               *pz = xor2(z, rb);
             }
+          }
+          break;
+        }
+        case SEG_XOR: {
+          wp = e + cnt * 32;
+          if (!act) break;
+          for (uint32_t j = rr; j < cnt; j += R) {
+            const uint32_t* x = e + 32 * j;  // (store, n, b_0 .. b_{n-1})
+            const uint32_t n = min(x[1], XOR_MAX_BITS);
+            uint2 v = make_uint2(0u, 0u);
+            for (uint32_t i = 0; i < n; i++) v = xor2(v, *(const uint2*)(a.rec + (uint64_t)x[2 + i] * pitch + cg));
+            *(uint2*)(a.rec + (uint64_t)x[0] * pitch + cg) = v;
           }
           break;
         }

@@ -33,7 +33,7 @@
 
 namespace qcb {
 
-static bool is1q(uint32_t o) { return o >= QCB_OP_I && o <= QCB_OP_CZYX; }
+static bool is1q(uint32_t o) { return o >= QCB_OP_I && o <= QCB_OP_SQO; }
 static bool is2q(uint32_t o) { return o >= QCB_OP_CNOT && o <= QCB_OP_YCZ; }
 static bool isnoise(uint32_t o) { return o >= QCB_OP_PAULI_NOISE && o <= QCB_OP_DEPOL2; }
 static bool ismeas(uint32_t o) { return o >= QCB_OP_MZ && o <= QCB_OP_MRX; }
@@ -51,6 +51,7 @@ struct LOp {  // lowered op (0-based qubits)
   int64_t site;    // noise site
   size_t src;      // index in the caller's op array
   uint32_t xa = 0, za = 0, xb = 0, zb = 0;  // planes, fixed when the op joins a segment
+  std::vector<uint32_t> xin;  // ClassicalXOR: 0-based input record rows
 };
 
 static uint64_t fnv1a(const void* p, size_t n, uint64_t h = 1469598103934665603ull) {
@@ -147,9 +148,36 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     const qcb_op& op = ops[k];
     const uint32_t oc = op.opcode;
     const bool two = is2q(oc) || oc == QCB_OP_DEPOL2;
-    if (!(is1q(oc) || is2q(oc) || isnoise(oc) || ismeas(oc) || oc == QCB_OP_NOP))
+    if (!(is1q(oc) || is2q(oc) || isnoise(oc) || ismeas(oc) || oc == QCB_OP_NOP || oc == QCB_OP_XOR ||
+          oc == QCB_OP_XOR_BITS))
       return fail(QCB_EUNSUPPORTED, "op " + std::to_string(k) + ": unknown opcode " + std::to_string(oc));
     if (oc == QCB_OP_NOP) continue;
+    if (oc == QCB_OP_XOR_BITS)
+      return fail(QCB_EARG, "op " + std::to_string(k) + ": ClassicalXOR input bits without their QCB_OP_XOR");
+    if (oc == QCB_OP_XOR) {  // ClassicalXOR: the input bits follow in XOR_BITS ops
+      const uint32_t n = op.q1;
+      if (n < 1 || n > XOR_MAX_BITS)
+        return fail(QCB_EUNSUPPORTED, "op " + std::to_string(k) + ": ClassicalXOR of " + std::to_string(n) +
+                                          " bits (1.." + std::to_string(XOR_MAX_BITS) + " supported)");
+      if (op.bit == 0) return fail(QCB_EBOUNDS, "op " + std::to_string(k) + ": ClassicalXOR store bit 0");
+      const size_t npay = (n + 2) / 3;
+      if (k + npay >= n_ops)
+        return fail(QCB_EARG, "op " + std::to_string(k) + ": ClassicalXOR is missing its input bits");
+      LOp x{SEG_XOR, oc, 0, 0, op.bit - 1, 0, -1, k};
+      for (size_t j = 1; j <= npay; j++) {
+        const qcb_op& pl = ops[k + j];
+        if (pl.opcode != QCB_OP_XOR_BITS)
+          return fail(QCB_EARG, "op " + std::to_string(k + j) + ": expected the ClassicalXOR's input bits");
+        for (uint32_t b : {pl.q1, pl.q2, pl.bit})
+          if (b && x.xin.size() < n) x.xin.push_back(b - 1);
+      }
+      if (x.xin.size() != n) return fail(QCB_EARG, "op " + std::to_string(k) + ": ClassicalXOR input bit 0");
+      nbits = std::max(nbits, op.bit);
+      for (uint32_t b : x.xin) nbits = std::max(nbits, b + 1);
+      low.push_back(std::move(x));
+      k += npay;
+      continue;
+    }
     if (op.q1 == 0 || (two && op.q2 == 0))
       return fail(QCB_EZEROQUBIT, "op " + std::to_string(k) + ": qubit indices start at 1 (NoZeroQubit)");
     if (two && op.q1 == op.q2)
@@ -164,6 +192,13 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     if (is1q(oc)) {
       P.info.n_updates++;
       if (is_frame_noop(oc)) continue;
+      if (oc == QCB_OP_SQO) {  // by its bit map: nothing, x <-> z, z ^= x, or generic
+        const uint32_t m = op.q2 & 15u;
+        if (m == 9u) continue;  // xx, zz: identity on frames
+        const uint32_t kind = m == 6u ? SEG_H : m == 11u ? SEG_S : SEG_G1;
+        low.push_back({kind, QCB_OP_SQO | ((op.q2 & 63u) << 8), q1, 0, BIT_NONE, 0, -1, k});
+        continue;
+      }
       const uint32_t kind = is_relabel(oc) ? SEG_H : (oc == QCB_OP_S || oc == QCB_OP_SDAG || oc == QCB_OP_HXY) ? SEG_S : SEG_G1;
       low.push_back({kind, oc, q1, 0, BIT_NONE, 0, -1, k});
     } else if (is2q(oc)) {
@@ -211,6 +246,7 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     if (qslot[q] == BIT_NONE) { qslot[q] = (uint32_t)P.slot_qubit.size(); P.slot_qubit.push_back(q); }
   };
   for (auto& o : low) {
+    if (o.kind == SEG_XOR) continue;  // no qubits
     touch(o.q1);
     if (o.kind == SEG_CNOT || o.kind == SEG_CZ || o.kind == SEG_G2 || o.opcode == QCB_OP_DEPOL2) touch(o.q2);
   }
@@ -273,6 +309,14 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
       case SEG_MZ:  // (x, bit)
         for (auto& o : seg) { r.w.push_back(o.xa); r.w.push_back(o.bit); }
         break;
+      case SEG_XOR:  // (store, n, b_0 .. b_{n-1}, 0 ...)
+        r.entry_words = 32;
+        for (auto& o : seg) {
+          r.w.push_back(o.bit);
+          r.w.push_back((uint32_t)o.xin.size());
+          for (uint32_t i = 0; i < 30; i++) r.w.push_back(i < o.xin.size() ? o.xin[i] : 0u);
+        }
+        break;
       case SEG_MRZ: {  // groups of 4 entries (x | z << 16, bit, reset | PAD, 0); entry i of a group
                        // holds reset 4*block + i, so one Philox block serves the group
         r.entry_words = 16;
@@ -324,7 +368,7 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   // measurement flips before each reset) gets one flush per layer.
   std::vector<LOp> cur;
   uint32_t cur_kind = SEG_END;
-  std::unordered_set<uint32_t> cur_q, post_q, cur_bits;
+  std::unordered_set<uint32_t> cur_q, post_q, cur_bits, cur_reads;
   std::vector<uint32_t> pre, post;
   auto close_seg = [&]() {
     emit_sites(pre);
@@ -332,6 +376,7 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     cur.clear();
     cur_q.clear();
     cur_bits.clear();
+    cur_reads.clear();
     cur_kind = SEG_END;
     pre.swap(post);
     post_q.clear();
@@ -361,6 +406,18 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     }
     if (o.kind == SEG_H) {  // relabel x <-> z of this qubit, no run-time work
       swp[qslot[o.q1]] ^= 1;
+      continue;
+    }
+    if (o.kind == SEG_XOR) {
+      // record rows only: a segment of XORs may not read a row it stores, nor
+      // store a row it reads or stores already
+      bool dep = cur_bits.count(o.bit) || cur_reads.count(o.bit);
+      for (uint32_t b : o.xin) dep = dep || cur_bits.count(b);
+      if (!cur.empty() && (dep || cur_kind != SEG_XOR)) close_seg();
+      cur_kind = SEG_XOR;
+      cur.push_back(o);
+      cur_bits.insert(o.bit);
+      for (uint32_t b : o.xin) cur_reads.insert(b);
       continue;
     }
     const bool two = o.kind == SEG_CNOT || o.kind == SEG_CZ || o.kind == SEG_G2;

@@ -78,8 +78,12 @@ enum SegKind : uint32_t {
   SEG_MRZ = 7,    // count groups of 4 entries (x, z, bit or NONE, reset or PAD)
   SEG_FLUSH = 8,  // count sites (site, kind | class << 8, x_a | z_a << 16, x_b | z_b << 16)
   SEG_CZ = 9,     // entries (x_a, z_a, x_b, z_b)
-  SEG_WIN = 10    // the stream continues in the next window
+  SEG_WIN = 10,   // the stream continues in the next window
+  SEG_XOR = 11    // entries of 32 words (store, n, b_0 .. b_{n-1}, 0 ...): record row
+                  // store <- XOR of record rows b_i (ClassicalXOR)
 };
+// Inputs of one ClassicalXOR entry.
+constexpr uint32_t XOR_MAX_BITS = 30;
 // Entry layouts in the windowed stream (planes are 16-bit):
 //   CNOT/CZ (x_a | z_a<<16, x_b | z_b<<16); S/G1 (x | z<<16, opcode);
 //   G2 (x_a | z_a<<16, x_b | z_b<<16, opcode, 0); MZ (x, bit);

@@ -158,6 +158,19 @@ __global__ void prodphase_comm_kernel(const uint64_t* l, uint8_t lph, const uint
 // :105-118 and :358-395).
 __device__ __forceinline__ uint64_t g1(uint32_t op, uint64_t& x, uint64_t& z) {
   const uint64_t X = x, Z = z;
+  if ((op & 0xFFu) == QCB_OP_SQO) {
+    // SingleQubitOperator (src/symbolic_cliffords.jl:178-206), flags in bits
+    // 8..13: +2 for px & x, for pz & z, and for x & z when the map sends Y to
+    // minus the product of the images of X and Z
+    const uint32_t f = op >> 8;
+    const bool bxx = f & 1u, bxz = f & 2u, bzx = f & 4u, bzz = f & 8u;
+    const uint64_t xx = 0ull - (uint64_t)bxx, xz = 0ull - (uint64_t)bxz;
+    const uint64_t zx = 0ull - (uint64_t)bzx, zz = 0ull - (uint64_t)bzz;
+    const bool anticom = (!bzz && bxz && !bxx && bzx) || (bzz && !bxz && bxx && bzx) || (bzz && bxz && bxx && !bzx);
+    x = (X & xx) ^ (Z & zx);
+    z = (X & xz) ^ (Z & zz);
+    return ((f & 16u) ? X : 0ull) ^ ((f & 32u) ? Z : 0ull) ^ (anticom ? (X & Z) : 0ull);
+  }
   switch (op) {
     case QCB_OP_H: x = Z; z = X; return X & Z;
     case QCB_OP_HXY: z = X ^ Z; return ~X & Z;
@@ -219,7 +232,7 @@ __global__ void apply_gates_kernel(uint64_t* xzs, uint8_t* ph, uint32_t rows, ui
   uint32_t p = ph[r];
   for (uint32_t k = 0; k < nops; k++) {
     const GateOp g = ops.op[k];
-    if (g.op < QCB_OP_CNOT) {
+    if ((g.op & 0xFFu) < QCB_OP_CNOT) {  // SingleQubitOperator carries flags above bit 8
       const uint32_t q = g.q1, w = q >> 6, s = q & 63;
       uint64_t x = (row[w] >> s) & 1, z = (row[len + w] >> s) & 1;
       const uint64_t f = g1(g.op, x, z) & 1;
@@ -461,13 +474,14 @@ int qcb_apply_gates(qcb_tableau* t, const qcb_op* ops, size_t n_ops, int phases,
   g.reserve(n_ops);
   for (size_t k = 0; k < n_ops; k++) {
     const qcb_op& o = ops[k];
-    const bool one = o.opcode >= QCB_OP_I && o.opcode <= QCB_OP_CZYX;
+    const bool one = o.opcode >= QCB_OP_I && o.opcode <= QCB_OP_SQO;
     const bool two = o.opcode >= QCB_OP_CNOT && o.opcode <= QCB_OP_YCZ;
     if (!one && !two) return fail(QCB_EUNSUPPORTED, "qcb_apply_gates: op " + std::to_string(k) + " is not a symbolic Clifford gate");
     if (o.q1 == 0 || (two && o.q2 == 0)) return fail(QCB_EZEROQUBIT, "qubit indices start at 1 (NoZeroQubit)");
     if (two && o.q1 == o.q2) return fail(QCB_EARG, "Failed to create a two qubit gate because the two qubits it acts on have the same index. The qubit indices have to be different.");
     if (o.q1 > t->nqubits || (two && o.q2 > t->nqubits)) return fail(QCB_EBOUNDS, "gate qubit index exceeds the tableau's qubits");
-    g.push_back({o.opcode, o.q1 - 1, two ? o.q2 - 1 : 0, 0});
+    const uint32_t code = o.opcode == QCB_OP_SQO ? o.opcode | ((o.q2 & 63u) << 8) : o.opcode;
+    g.push_back({code, o.q1 - 1, two ? o.q2 - 1 : 0, 0});
   }
   if (g.empty() || !t->rows) return QCB_OK;
   cudaStream_t st = S(stream);

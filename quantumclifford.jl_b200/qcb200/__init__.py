@@ -12,8 +12,8 @@ from ._lib import (  # noqa: F401
 )
 from .ops import (  # noqa: F401
     Op, OP, sId1, sHadamard, sPhase, sInvPhase, sX, sY, sZ, sSQRTX, sInvSQRTX, sSQRTY, sInvSQRTY,
-    sHadamardXY, sHadamardYZ, sCXYZ, sCZYX, sCNOT, sCPHASE, sSWAP, sZCX, sZCY, sZCZ, sXCX, sXCY, sXCZ,
-    sYCX, sYCY, sYCZ, sMZ, sMRZ, sMX, sMRX, PauliError, NoiseOp, PauliNoise, UnbiasedUncorrelatedNoise,
+    sHadamardXY, sHadamardYZ, sCXYZ, sCZYX, SingleQubitOperator, sCNOT, sCPHASE, sSWAP, sZCX, sZCY, sZCZ, sXCX, sXCY, sXCZ,
+    sYCX, sYCY, sYCZ, sMZ, sMRZ, sMX, sMRX, ClassicalXOR, PauliMeasurement, PauliError, NoiseOp, PauliNoise, UnbiasedUncorrelatedNoise,
     DepolarizationNoise, to_array, count_updates, affected_counts,
 )
 from .frames import (  # noqa: F401

@@ -17,9 +17,9 @@ from ._lib import OP_DTYPE, ArgumentError, QCB_EARG, QCB_EZEROQUBIT
 # opcodes (enum qcb_opcode)
 OP = dict(
     NOP=0, I=1, H=2, S=3, SDAG=4, X=5, Y=6, Z=7, SQRTX=8, INVSQRTX=9, SQRTY=10, INVSQRTY=11,
-    HXY=12, HYZ=13, CXYZ=14, CZYX=15,
+    HXY=12, HYZ=13, CXYZ=14, CZYX=15, SQO=16,
     CNOT=32, CPHASE=33, SWAP=34, ZCX=35, ZCY=36, ZCZ=37, XCX=38, XCY=39, XCZ=40, YCX=41, YCY=42, YCZ=43,
-    MZ=64, MRZ=65, MX=66, MRX=67,
+    MZ=64, MRZ=65, MX=66, MRX=67, XOR=68, XOR_BITS=69,
     PAULI_NOISE=96, DEPOL1=97, DEPOL2=98,
 )
 
@@ -97,6 +97,82 @@ sHadamardXY = _one("HXY")
 sHadamardYZ = _one("HYZ")
 sCXYZ = _one("CXYZ")
 sCZYX = _one("CZYX")
+
+
+def SingleQubitOperator(q, xx=None, xz=None, zx=None, zz=None, px=None, pz=None) -> Op:
+    """SingleQubitOperator(q, xx, xz, zx, zz, px, pz) (src/symbolic_cliffords.jl
+    :168-206): X -> (xx, xz) with sign px, Z -> (zx, zz) with sign pz.  Also
+    SingleQubitOperator(gate) for a named single-qubit gate (the reference's
+    conversion table, :207-221), and SingleQubitOperator(op, qubit)."""
+    if isinstance(q, Op):
+        if q.opcode == OP["SQO"]:
+            return Op(OP["SQO"], _q(xx if xx is not None else q.q1), q.q2)
+        f = _SQO_OF[q.opcode]
+        return Op(OP["SQO"], _q(xx if xx is not None else q.q1), f)
+    f = sum(int(bool(b)) << i for i, b in enumerate((xx, xz, zx, zz, px, pz)))
+    return Op(OP["SQO"], _q(q), f)
+
+
+def _sqo_flags(xx, xz, zx, zz, px, pz):
+    return sum(int(b) << i for i, b in enumerate((xx, xz, zx, zz, px, pz)))
+
+
+T_, F_ = True, False
+_SQO_OF = {  # src/symbolic_cliffords.jl:207-221
+    OP["H"]: _sqo_flags(F_, T_, T_, F_, F_, F_), OP["S"]: _sqo_flags(T_, T_, F_, T_, F_, F_),
+    OP["SDAG"]: _sqo_flags(T_, T_, F_, T_, T_, F_), OP["I"]: _sqo_flags(T_, F_, F_, T_, F_, F_),
+    OP["X"]: _sqo_flags(T_, F_, F_, T_, F_, T_), OP["Y"]: _sqo_flags(T_, F_, F_, T_, T_, T_),
+    OP["Z"]: _sqo_flags(T_, F_, F_, T_, T_, F_), OP["CXYZ"]: _sqo_flags(T_, T_, T_, F_, F_, F_),
+    OP["CZYX"]: _sqo_flags(F_, T_, T_, T_, F_, F_), OP["HXY"]: _sqo_flags(T_, T_, F_, T_, F_, T_),
+    OP["HYZ"]: _sqo_flags(T_, F_, T_, T_, T_, F_), OP["SQRTX"]: _sqo_flags(T_, F_, T_, T_, F_, T_),
+    OP["INVSQRTX"]: _sqo_flags(T_, F_, T_, T_, F_, F_), OP["SQRTY"]: _sqo_flags(F_, T_, T_, F_, T_, F_),
+    OP["INVSQRTY"]: _sqo_flags(F_, T_, T_, F_, F_, T_),
+}
+
+
+def ClassicalXOR(bits, store) -> list:
+    """ClassicalXOR(bits, store) (src/misc_ops.jl:198-205): record bit `store`
+    <- XOR of record bits `bits` (1-based, at most 30).  The C ABI form: one
+    XOR op (q1 = len(bits), bit = store) and the bits, three per XOR_BITS op."""
+    bits = [int(b) for b in bits]
+    if not 1 <= len(bits) <= 30:
+        raise ArgumentError(QCB_EARG, "ClassicalXOR takes 1 to 30 bits")
+    if store <= 0 or min(bits) <= 0:
+        raise ArgumentError(QCB_EARG, "record bits start at 1")
+    ops = [Op(OP["XOR"], len(bits), 0, int(store))]
+    for i in range(0, len(bits), 3):
+        b = bits[i:i + 3] + [0] * (3 - len(bits[i:i + 3]))
+        ops.append(Op(OP["XOR_BITS"], b[0], b[1], b[2]))
+    return ops
+
+
+def PauliMeasurement(pauli, bit: int) -> list:
+    """PauliMeasurement(pauli, bit) on a Pauli frame (src/pauli_frames.jl
+    :118-134): through the hidden ancilla n+1 of an n-qubit Pauli, sXCZ / sCNOT
+    / sYCX from each qubit with X / Z / Y onto it, then sMRZ(n+1, bit) (the
+    sign's sX does not change a frame).  `pauli` is a string like "XIZY" (a
+    leading sign is accepted) or an object with `bits()`/`nqubits` (a one-row
+    Tableau)."""
+    if isinstance(pauli, str):
+        body = pauli.strip().lstrip("+-").lstrip("i")
+        letters = [ch for ch in body if ch in "IXYZ_"]
+    else:
+        xs, zs = pauli.bits()
+        letters = ["_XZY"[int(x) + 2 * int(z)] for x, z in zip(xs[0], zs[0])]
+    n = len(letters)
+    anc = n + 1
+    ops = []
+    for q, ch in enumerate(letters, start=1):
+        if ch == "X":
+            ops.append(Op(OP["XCZ"], q, anc))
+        elif ch == "Z":
+            ops.append(Op(OP["CNOT"], q, anc))
+        elif ch == "Y":
+            ops.append(Op(OP["YCX"], q, anc))
+    ops.append(Op(OP["MRZ"], anc, 0, int(bit)))
+    return ops
+
+
 # two-qubit symbolic gates (src/symbolic_cliffords.jl:358-395)
 sCNOT = _two("CNOT")
 sCPHASE = _two("CPHASE")
@@ -203,14 +279,23 @@ def to_array(circuit: Iterable) -> np.ndarray:
 
 
 def affected_counts(arr: np.ndarray) -> tuple[int, int]:
-    """(qmax, bmax) as _create_pauliframe computes them (init = 1)."""
+    """(qmax, bmax) as _create_pauliframe computes them (init = 1): the highest
+    qubit of any op and the highest record bit (src/affectedqubits.jl)."""
     if len(arr) == 0:
         return 1, 1
-    qmax = int(max(1, arr["q1"].max(), arr["q2"].max()))
-    bmax = int(max(1, arr["bit"].max()))
+    oc = arr["opcode"]
+    one_q = ((oc >= OP["I"]) & (oc < OP["XOR"])) | (oc >= OP["PAULI_NOISE"])  # ops with a qubit q1
+    two_q = ((oc >= OP["CNOT"]) & (oc <= OP["YCZ"])) | (oc == OP["DEPOL2"])   # and a second qubit q2
+    pay = oc == OP["XOR_BITS"]                                                  # record bits in q1, q2, bit
+
+    def top(v):
+        return int(v.max()) if len(v) else 0
+
+    qmax = max(1, top(arr["q1"][one_q]), top(arr["q2"][two_q]))
+    bmax = max(1, top(arr["bit"][(oc >= OP["MZ"]) & (oc <= OP["XOR_BITS"])]), top(arr["q1"][pay]), top(arr["q2"][pay]))
     return qmax, bmax
 
 
 def count_updates(arr: np.ndarray) -> int:
     """Clifford gates + measurements (noise not counted)."""
-    return int(np.count_nonzero((arr["opcode"] > 0) & (arr["opcode"] < OP["PAULI_NOISE"])))
+    return int(np.count_nonzero((arr["opcode"] > 0) & (arr["opcode"] < OP["XOR"])))

@@ -17,7 +17,7 @@ import qcb200
 from qcb200 import ops as O
 from qcb200._lib import check, lib, ptr, qcb_program_info
 
-SEG_END, SEG_CNOT, SEG_H, SEG_S, SEG_G1, SEG_G2, SEG_MZ, SEG_MRZ, SEG_FLUSH, SEG_CZ, SEG_WIN = range(11)
+SEG_END, SEG_CNOT, SEG_H, SEG_S, SEG_G1, SEG_G2, SEG_MZ, SEG_MRZ, SEG_FLUSH, SEG_CZ, SEG_WIN, SEG_XOR = range(12)
 BIT_NONE = 0xFFFFFFFF
 MRZ_PAD = 0xFFFFFFFF
 SITE_DTYPE = np.dtype([("kind", "<u4"), ("xa", "<u4"), ("za", "<u4"), ("xb", "<u4"), ("zb", "<u4"),
@@ -46,6 +46,10 @@ def dump(arr):
 
 def gate1(op, x, z):
     X, Z = x.copy(), z.copy()
+    if (op & 0xFF) == O.OP["SQO"]:
+        f = op >> 8
+        m = lambda b: np.uint32(0xFFFFFFFF if (f >> b) & 1 else 0)
+        return (X & m(0)) ^ (Z & m(2)), (X & m(1)) ^ (Z & m(3))
     if op in (O.OP["H"], O.OP["SQRTY"], O.OP["INVSQRTY"]):
         return Z, X
     if op in (O.OP["HXY"], O.OP["S"], O.OP["SDAG"]):
@@ -159,6 +163,14 @@ def run_mask(arr, frames, qubits, nbits, masks):
                     rec[bit] = T[x]
                 T[x] = 0
                 T[z] ^= masks.reset_planes[r]
+        elif kind == SEG_XOR:
+            e = stream[pc: pc + 32 * cnt].reshape(cnt, 32)
+            pc += 32 * cnt
+            for row in e:
+                v = np.zeros(words, np.uint32)
+                for b in row[2: 2 + int(row[1])]:
+                    v ^= rec[b]
+                rec[row[0]] = v
         elif kind == SEG_FLUSH:
             e = stream[pc: pc + 4 * cnt].reshape(cnt, 4)
             pc += 4 * cnt

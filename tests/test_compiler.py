@@ -9,7 +9,7 @@ import qcb200
 import stream_emu
 from qcb200 import circuits, ops as O
 
-from test_gpu_frames import random_circuit  # noqa: E402  (shared generator; its GPU tests are marked)
+from test_gpu_frames import random_circuit, xor_chain_circuit  # noqa: E402  (shared generator; its GPU tests are marked)
 
 
 def check_circuit(circ, frames, seed):
@@ -58,3 +58,8 @@ def test_relabels_and_noise_interleave():
     c += [O.sCNOT(1, 2), O.sSQRTY(2)] + O.NoiseOp(O.DepolarizationNoise(0.5), (1, 2))
     c += [O.sMX(2, 1), O.sMRX(1, 2), O.sMZ(2, 3), O.sX(1), O.sMRZ(1, 4), O.sMZ(1, 2)]
     check_circuit(c, 500, 3)
+
+
+def test_classical_xor_chains():
+    info = check_circuit(xor_chain_circuit(np.random.default_rng(21)), 150, 4)
+    assert info["n_flushes"] >= 1

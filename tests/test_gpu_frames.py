@@ -60,6 +60,15 @@ def test_surface_code_d11_mask_mode_bit_exact(qcb):
     assert np.array_equal(coding(f.xzs(), 242), coding(ox, 242))
 
 
+# the invertible bit maps (xx, xz, zx, zz) of a single-qubit Clifford
+SQO_MAPS = [(1, 0, 0, 1), (0, 1, 1, 0), (1, 1, 0, 1), (1, 0, 1, 1), (0, 1, 1, 1), (1, 1, 1, 0)]
+
+
+def random_sqo(q, rng):
+    m = SQO_MAPS[rng.integers(len(SQO_MAPS))]
+    return O.SingleQubitOperator(q, *m, bool(rng.integers(2)), bool(rng.integers(2)))
+
+
 def random_circuit(n, length, rng, p=0.05, nbits_start=1):
     g1 = ["H", "S", "SDAG", "X", "Y", "Z", "SQRTX", "INVSQRTX", "SQRTY", "INVSQRTY", "HXY", "HYZ", "CXYZ", "CZYX", "I"]
     g2 = ["CNOT", "CPHASE", "SWAP", "ZCX", "ZCY", "ZCZ", "XCX", "XCY", "XCZ", "YCX", "YCY", "YCZ"]
@@ -68,7 +77,10 @@ def random_circuit(n, length, rng, p=0.05, nbits_start=1):
         k = rng.integers(0, 10)
         q = int(rng.integers(1, n + 1))
         if k < 3:
-            c.append(O.Op(O.OP[g1[rng.integers(len(g1))]], q))
+            if rng.random() < 0.25:
+                c.append(random_sqo(q, rng))
+            else:
+                c.append(O.Op(O.OP[g1[rng.integers(len(g1))]], q))
         elif k < 6:
             q2 = int(rng.integers(1, n + 1))
             if q2 != q:
@@ -84,6 +96,13 @@ def random_circuit(n, length, rng, p=0.05, nbits_start=1):
             q2 = int(rng.integers(1, n + 1))
             if q2 != q:
                 c += O.NoiseOp(O.DepolarizationNoise(p * 3), (q, q2))
+        elif k == 9 and rng.random() < 0.5:
+            if bit > 2 and rng.random() < 0.5:  # a detector-like XOR of earlier bits
+                k_in = int(rng.integers(1, min(bit - 1, 12) + 1))
+                c += O.ClassicalXOR([int(b) for b in rng.integers(1, bit, size=k_in)], bit)
+            else:  # a random Pauli measured through the ancilla n+1
+                c += O.PauliMeasurement("".join("IXZY"[int(v)] for v in rng.integers(0, 4, size=n)), bit)
+            bit += 1
         else:
             c += O.NoiseOp(O.DepolarizationNoise(p * 2), (q,))
     c.append(O.sMZ(1, bit))
@@ -97,6 +116,31 @@ def test_random_circuits_mask_mode_bit_exact(qcb, seed):
     circ = random_circuit(n, 400, rng)
     frames = int(rng.integers(1, 3000))
     f, ox, om = run_mask(qcb, circ, frames, seed=seed)
+    assert np.array_equal(f.measurements(), om)
+    assert np.array_equal(coding(f.xzs(), f.qubits + 1), coding(ox, f.qubits + 1))
+
+
+def xor_chain_circuit(rng):
+    """Stores among their own inputs, chains of XORs reading earlier stores,
+    30-input XORs, XORs between measurements of the same round."""
+    c = []
+    for r in range(6):
+        for q in range(1, 33):
+            c.append(O.Op(O.OP["H"], q))
+            c += O.PauliError(q, 0.1, 0.05, 0.02)
+            c.append(O.sMZ(q, 32 * r + q))
+        c += O.ClassicalXOR(list(range(32 * r + 1, 32 * r + 31)), 32 * r + 2)
+        c += O.ClassicalXOR([32 * r + 2, 32 * r + 3], 32 * r + 3)
+        c += O.ClassicalXOR([32 * r + 3], 200 + r)
+        for _ in range(4):
+            ins = [int(b) for b in rng.integers(1, 32 * r + 33, size=int(rng.integers(1, 31)))]
+            c += O.ClassicalXOR(ins, int(rng.choice(ins)))
+        c += O.PauliMeasurement("Z" + "I" * 31, 210 + r)
+    return c
+
+
+def test_classical_xor_chains_bit_exact(qcb):
+    f, ox, om = run_mask(qcb, xor_chain_circuit(np.random.default_rng(21)), 2500, seed=4)
     assert np.array_equal(f.measurements(), om)
     assert np.array_equal(coding(f.xzs(), f.qubits + 1), coding(ox, f.qubits + 1))
 
@@ -191,14 +235,19 @@ def test_single_op_apply_equals_program(qcb):
     qcb.pftrajectories(whole, arr, masks=masks)
     step = qcb.PauliFrame(500, qmax, bmax, masks=masks)
     # apply op by op: remap events and reset planes to each single-op call
+    # (a ClassicalXOR goes with its XOR_BITS payload ops)
     resets = 0
-    for k, op in enumerate(circ):
+    k = 0
+    while k < len(circ):
+        op = circ[k]
+        n = 1 + ((op.q1 + 2) // 3 if op.opcode == O.OP["XOR"] else 0)
         ev = masks.events[masks.events["op_index"] == k].copy()
         ev["op_index"] = 0
         nres = 1 if op.opcode in (O.OP["MRZ"], O.OP["MRX"]) else 0
         rp = masks.reset_planes[resets:resets + nres]
         resets += nres
-        step.apply(op, masks=qcb.Masks(masks.init_z, rp, ev))
+        step.apply(circ[k:k + n], masks=qcb.Masks(masks.init_z, rp, ev))
+        k += n
     assert np.array_equal(step.measurements(), whole.measurements())
     x1, z1 = step.planes()
     x2, z2 = whole.planes()

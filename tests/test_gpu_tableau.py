@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
+from test_gpu_frames import random_sqo  # noqa: E402
 import qcb200
 from qcb200 import ops as O
 from qcb200.tableau import Tableau, one_destabilizer, random_clifford_ops
@@ -94,7 +95,10 @@ def test_symbolic_gates_with_phases(qcb, n):
     g1 = ["I", "H", "S", "SDAG", "X", "Y", "Z", "SQRTX", "INVSQRTX", "SQRTY", "INVSQRTY", "HXY", "HYZ", "CXYZ", "CZYX"]
     g2 = ["CNOT", "CPHASE", "SWAP", "ZCX", "ZCY", "ZCZ", "XCX", "XCY", "XCZ", "YCX", "YCY", "YCZ"]
     for _ in range(300):
-        if rng.random() < 0.5:
+        u = rng.random()
+        if u < 0.15:
+            gates.append(random_sqo(int(rng.integers(1, n + 1)), rng))
+        elif u < 0.5:
             gates.append(O.Op(O.OP[g1[rng.integers(len(g1))]], int(rng.integers(1, n + 1))))
         else:
             a, b = rng.choice(np.arange(1, n + 1), 2, replace=False)

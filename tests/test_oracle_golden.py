@@ -272,6 +272,27 @@ def test_symbolic_gates_match_their_dense_form(orc, gate):
         assert np.array_equal(a_ph, d_ph)
 
 
+@pytest.mark.parametrize("gate", GATES1)
+def test_single_qubit_operator_of_each_named_gate_acts_like_it(orc, gate):
+    """SingleQubitOperator(g) (the reference's table, src/symbolic_cliffords.jl
+    :207-221) acts like g on random tableaux, phases included
+    (test/test_symcliff.jl compares them the same way)."""
+    import oracle
+
+    n = 3
+    named = np.zeros(1, dtype=oracle.OP_DTYPE)
+    named[0] = (O.OP[gate], 2, 0, 0, (0, 0, 0))
+    sqo = O.to_array([O.SingleQubitOperator(O.Op(O.OP[gate], 2))])
+    rng = np.random.default_rng(13)
+    for _ in range(5):
+        _, st = random_stabilizer_tab(n, rng)
+        st.phases[:] = rng.integers(0, 4, n)
+        a_ph, a_xz = oracle.apply_gates(st.phases, st.xzs, n, named)
+        b_ph, b_xz = oracle.apply_gates(st.phases, st.xzs, n, sqo)
+        assert np.array_equal(a_xz, b_xz)
+        assert np.array_equal(a_ph, b_ph)
+
+
 def test_frame_ghz_correlations(orc):
     """test/test_pauliframe.jl:30-52: GHZ records have row sums 0 or 3 and
     mean 1/2."""

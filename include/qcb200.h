@@ -287,6 +287,50 @@ int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* p
                 int keep_result, int phases, int32_t* anticom, int32_t* result,
                 uint32_t* n_done, void* stream);
 
+/* projectX!(state, qubit) / projectZ! / projectY! (src/project_trace_reset.jl
+ * :440-573): k single-qubit projections in order, basis 1 = X, 2 = Z, 3 = Y,
+ * qubits 1-based.  On a MixedDestabilizer this is project_cond! (a one-bit
+ * anticommutation test per row; the new stabilizer row is the projector with
+ * phase 0); on the other kinds project! with single_x/z/y, as the reference
+ * dispatches.  Outputs as for qcb_project.                                  */
+int qcb_project_qubit(qcb_tableau* t, int kind, int32_t* rank_io, uint32_t basis,
+                      const uint32_t* qubits, size_t k, int keep_result, int phases,
+                      int32_t* anticom, int32_t* result, uint32_t* n_done, void* stream);
+
+/* projectrand!(state, pauli) / projectXrand! / projectZrand! / projectYrand!
+ * (src/project_trace_reset.jl:575-636): the projections of qcb_project (when
+ * `paulis` is non-NULL) or of qcb_project_qubit (basis, qubits, k), with
+ * keep_result and phases on; a projection whose outcome is undetermined
+ * (`nothing`) sets the new stabilizer row's phase to rand_phases[j] (0 or 2,
+ * drawn by the caller, one per projection) and reports it as the result.    */
+int qcb_projectrand(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* paulis,
+                    uint32_t basis, const uint32_t* qubits, size_t k, const uint8_t* rand_phases,
+                    int32_t* anticom, int32_t* result, uint32_t* n_done, void* stream);
+
+/* canonicalize!(state; phases, ranks) (src/canonicalization.jl:92-133) on a
+ * whole state of the given kind (rank for the mixed kinds): for Destabilizer
+ * and MixedDestabilizer the row swaps and products also act on the paired
+ * destabilizer rows, as rowswap!/mul_left! on those states do
+ * (src/QuantumClifford.jl:907-927, src/mul_leftright.jl:200-219).          */
+int qcb_canonicalize_state(qcb_tableau* t, int kind, int32_t rank, int phases,
+                           int32_t* rx, int32_t* rz, void* stream);
+
+/* canonicalize_rref!(state, colindices; phases) (src/canonicalization.jl
+ * :150-185): cols are 1-based qubits in order; *i_out gets the reference's
+ * returned index i (1-based; rows i+1.. hold the pivots).                   */
+int qcb_canonicalize_rref(qcb_tableau* t, int kind, int32_t rank, const uint32_t* cols,
+                          size_t ncols, int phases, int32_t* i_out, void* stream);
+
+/* canonicalize_gott!(stabilizer; phases) (src/canonicalization.jl:206-272)
+ * without backtracking: r, s and the permutations xperm, zperm (1-based,
+ * nqubits entries each, may be NULL) that were applied with permutesystems!. */
+int qcb_canonicalize_gott(qcb_tableau* t, int phases, int32_t* r, int32_t* s,
+                          uint32_t* xperm, uint32_t* zperm, void* stream);
+
+/* permutesystems!(s, perm) (src/linalg.jl:7-17): every row becomes row[perm]
+ * (new qubit j is old qubit perm[j], 1-based, nqubits entries); phases stay. */
+int qcb_permutesystems(qcb_tableau* t, const uint32_t* perm, void* stream);
+
 /* generate!(pauli, stabilizer; phases) (src/project_trace_reset.jl:37-81) on
  * a canonical stabilizer.  Writes the remaining Pauli (identity up to phase)
  * back into `pauli`; *ok = 0 when the Pauli cannot be generated.  used_rows

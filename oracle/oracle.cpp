@@ -445,6 +445,241 @@ int oracle_project(int kind, u64* xzs, u8* ph, size_t rows, u32 n, int* rank_io,
   return QCB_OK;
 }
 
+// ---------------------------------------------------------------- states
+// The stabilizer view of a state is rows [off, off + rows) of its tableau;
+// the Destabilizer kinds pair stabilizer row off + i with destabilizer row i.
+struct StateView {
+  Tab t;
+  size_t off, rows;
+  bool destab;
+};
+
+static StateView state_view(int kind, u64* xzs, u8* ph, size_t tab_rows, u32 n, int rank) {
+  size_t W = 2 * ((n + 63) / 64);
+  StateView s{Tab{xzs, ph, W, n}, 0, tab_rows, false};
+  if (kind == QCB_MIXED_STABILIZER) s.rows = (size_t)rank;
+  if (kind == QCB_DESTABILIZER) { s.off = tab_rows / 2; s.rows = tab_rows / 2; s.destab = true; }
+  if (kind == QCB_MIXED_DESTABILIZER) { s.off = tab_rows / 2; s.rows = (size_t)rank; s.destab = true; }
+  return s;
+}
+
+// rowswap!(state, i, j) (src/QuantumClifford.jl:899-927), 0-based view rows.
+static void st_rowswap(StateView& s, size_t i, size_t j, bool P) {
+  if (s.destab) tab_rowswap(s.t, i, j, P);
+  tab_rowswap(s.t, s.off + i, s.off + j, P);
+}
+
+// mul_left!(state, m, i) (src/mul_leftright.jl:195-219): stabilizer m <- i * m;
+// the Destabilizer kinds also set destabilizer i <- m * i without phases.
+static void st_mul_left(StateView& s, size_t m, size_t i, bool P) {
+  if (s.destab) tab_mul_left(s.t, i, m, false);
+  tab_mul_left(s.t, s.off + m, s.off + i, P);
+}
+
+static bool st_bit(const StateView& s, size_t r, u32 j, int z) {
+  return z ? s.t.zbit(s.off + r, j) : s.t.xbit(s.off + r, j);
+}
+
+// _canonicalize!(state) (src/canonicalization.jl:95-133) on a state of any kind.
+void oracle_canonicalize_state(int kind, u64* xzs, u8* ph, size_t tab_rows, u32 n, int rank, int phases,
+                               int* rx_out, int* rz_out) {
+  StateView s = state_view(kind, xzs, ph, tab_rows, n, rank);
+  bool P = phases != 0;
+  size_t i = 0;
+  for (int stage = 0; stage < 2; stage++) {
+    for (u32 j = 0; j < n; j++) {
+      size_t k = s.rows;
+      for (size_t ii = i; ii < s.rows; ii++)
+        if (st_bit(s, ii, j, stage)) { k = ii; break; }
+      if (k == s.rows) continue;
+      st_rowswap(s, k, i, P);
+      for (size_t m = 0; m < s.rows; m++)
+        if (st_bit(s, m, j, stage) && m != i) st_mul_left(s, m, i, P);
+      i++;
+    }
+    if (stage == 0 && rx_out) *rx_out = (int)i;
+  }
+  if (rz_out) *rz_out = (int)i;
+}
+
+// _canonicalize_rref!(state, colindices) (src/canonicalization.jl:153-183).
+// cols are 1-based qubits; returns the reference's (1-based) `i`.
+int oracle_canonicalize_rref(int kind, u64* xzs, u8* ph, size_t tab_rows, u32 n, int rank,
+                             const u32* cols, size_t ncols, int phases) {
+  StateView s = state_view(kind, xzs, ph, tab_rows, n, rank);
+  bool P = phases != 0;
+  long i = (long)s.rows;  // 1-based
+  for (size_t c = 0; c < ncols; c++) {
+    u32 j = cols[c] - 1;
+    for (int z = 0; z < 2; z++) {
+      long k = 0;  // findfirst over 1:i
+      for (long ii = 1; ii <= i; ii++)
+        if (st_bit(s, (size_t)ii - 1, j, z)) { k = ii; break; }
+      if (k == 0) continue;
+      st_rowswap(s, (size_t)k - 1, (size_t)i - 1, P);
+      for (size_t m = 0; m < s.rows; m++)
+        if (st_bit(s, m, j, z) && (long)m != i - 1) st_mul_left(s, m, (size_t)i - 1, P);
+      i -= 1;
+    }
+  }
+  return (int)i;
+}
+
+// permutesystems!(s, perm) (src/linalg.jl:7-17): every row becomes row[perm]
+// (new qubit j is old qubit perm[j], 1-based); phases stay.
+void oracle_permutesystems(u64* xzs, size_t rows, u32 n, const u32* perm) {
+  size_t W = 2 * ((n + 63) / 64), len = W / 2;
+  std::vector<u64> old(W);
+  for (size_t r = 0; r < rows; r++) {
+    u64* row = xzs + r * W;
+    std::memcpy(old.data(), row, W * 8);
+    for (size_t w = 0; w < W; w++) row[w] = 0;
+    for (u32 j = 0; j < n; j++) {
+      u32 q = perm[j] - 1;
+      row[j >> 6] |= ((old[q >> 6] >> (q & 63)) & 1) << (j & 63);
+      row[len + (j >> 6)] |= ((old[len + (q >> 6)] >> (q & 63)) & 1) << (j & 63);
+    }
+  }
+}
+
+// gott_standard_form_indices (src/canonicalization.jl:187-204) on the X
+// (half = 0) or Z (half = 1) bits; perm (1-based, length n); returns the rank.
+static size_t gott_indices(const u64* xzs, size_t rows, u32 n, int half, size_t skip, u32* perm) {
+  size_t W = 2 * ((n + 63) / 64), len = W / 2;
+  std::vector<u32> good;
+  for (size_t r = skip; r < rows; r++) {
+    // unsafe_bitfindnext_(row bits, skip+1) (src/QuantumClifford.jl:960-977)
+    long found = -1;
+    for (u32 b = (u32)skip; b < 64 * len; b++)
+      if ((xzs[r * W + half * len + (b >> 6)] >> (b & 63)) & 1) { found = b; break; }
+    if (found < 0) break;
+    if (std::find(good.begin(), good.end(), (u32)found + 1) != good.end()) continue;
+    good.push_back((u32)found + 1);
+  }
+  size_t k = 0;
+  if (good.empty()) {
+    for (u32 j = 1; j <= n; j++) perm[k++] = j;
+    return 0;
+  }
+  for (u32 j = 1; j <= (u32)skip; j++) perm[k++] = j;
+  for (u32 g : good) perm[k++] = g;
+  for (u32 j = (u32)skip + 1; j <= good.back(); j++)
+    if (std::find(good.begin(), good.end(), j) == good.end()) perm[k++] = j;
+  for (u32 j = good.back() + 1; j <= n; j++) perm[k++] = j;
+  return good.size();
+}
+
+// _canonicalize_gott!(stabilizer) (src/canonicalization.jl:223-272) without
+// backtracking: returns r, s and the two permutations (1-based, length n).
+void oracle_canonicalize_gott(u64* xzs, u8* ph, size_t rows, u32 n, int phases, int* r_out, int* s_out,
+                              u32* xperm, u32* zperm) {
+  StateView s = state_view(QCB_STABILIZER, xzs, ph, rows, n, 0);
+  bool P = phases != 0;
+  size_t i = 0;
+  for (u32 j = 0; j < n; j++) {
+    size_t k = rows;
+    for (size_t ii = i; ii < rows; ii++)
+      if (st_bit(s, ii, j, 0)) { k = ii; break; }
+    if (k == rows) continue;
+    st_rowswap(s, k, i, P);
+    for (size_t m = 0; m < rows; m++)
+      if (st_bit(s, m, j, 0) && m != i) st_mul_left(s, m, i, P);
+    i++;
+  }
+  size_t r = gott_indices(xzs, rows, n, 0, 0, xperm);
+  oracle_permutesystems(xzs, rows, n, xperm);
+  i = r;
+  for (u32 j = (u32)r; j < n; j++) {
+    size_t k = rows;
+    for (size_t ii = i; ii < rows; ii++)
+      if (st_bit(s, ii, j, 1)) { k = ii; break; }
+    if (k == rows) continue;
+    st_rowswap(s, k, i, P);
+    for (size_t m = 0; m < rows; m++)
+      if (st_bit(s, m, j, 1) && m != i) st_mul_left(s, m, i, P);
+    i++;
+  }
+  size_t sz = gott_indices(xzs, rows, n, 1, r, zperm);
+  oracle_permutesystems(xzs, rows, n, zperm);
+  *r_out = (int)r;
+  *s_out = (int)sz;
+}
+
+// project_cond! (src/project_trace_reset.jl:493-573) behind projectX! /
+// projectZ! / projectY! on a MixedDestabilizer: basis 1 = X (condition isZ,
+// projector bits (1,0)), 2 = Z (isX, (0,1)), 3 = Y (isXorZ, (1,1)); qubit is
+// 1-based.  anticom: 1-based or 0; result: 0..3 or -1 for `nothing`.
+void oracle_project_cond(u64* xzs, u8* ph, size_t tab_rows, u32 n, int* rank_io, u32 qubit, int basis,
+                         int keep_result, int phases, int* anticom_out, int* result_out) {
+  size_t W = 2 * ((n + 63) / 64);
+  Tab t{xzs, ph, W, n};
+  bool P = phases != 0;
+  const u32 q = qubit - 1;
+  auto IS = [&](size_t row) -> bool {
+    bool x = t.xbit(row, q), z = t.zbit(row, q);
+    return basis == 1 ? z : (basis == 2 ? x : (x != z));
+  };
+  auto set_projector = [&](size_t row) {  // zero!(tab, row); tab[row, qubit] = RESET
+    for (size_t w = 0; w < W; w++) t.row(row)[w] = 0;
+    t.ph[row] = 0;
+    if (basis & 1) t.row(row)[q >> 6] |= 1ull << (q & 63);
+    if (basis & 2) t.row(row)[W / 2 + (q >> 6)] |= 1ull << (q & 63);
+  };
+  // anticomm_update_rows_cond (:480-495), 1-based r and anticommutes
+  auto update = [&](size_t r, size_t nn, size_t a) {
+    size_t piv = nn + a - 1;
+    for (size_t i = r; i < nn; i++)
+      if (IS(i)) tab_mul_left(t, i, piv, P);
+    for (size_t i = nn + a; i < 2 * nn; i++)
+      if (IS(i)) tab_mul_left(t, i, piv, P);
+    for (size_t i = 0; i < r; i++)
+      if (i != a - 1 && IS(i)) tab_mul_left(t, i, piv, false);
+  };
+  size_t nn = n, r = (size_t)*rank_io;
+  (void)tab_rows;
+  int anticommutes = 0, result = -1;
+  for (size_t i = 0; i < r; i++)
+    if (IS(nn + i)) { anticommutes = (int)i + 1; break; }
+  if (anticommutes == 0) {
+    size_t anticomlog = 0;
+    for (size_t i = r; i < nn; i++)
+      if (IS(i)) { anticomlog = i + 1; break; }
+    if (anticomlog == 0)
+      for (size_t i = nn + r; i < 2 * nn; i++)
+        if (IS(i)) { anticomlog = i + 1; break; }
+    if (anticomlog != 0) {
+      if (anticomlog <= nn) {
+        tab_rowswap(t, r + nn, anticomlog - 1, true);
+        if (nn != r + 1 && anticomlog != r + 1) tab_rowswap(t, r, anticomlog + nn - 1, true);
+      } else {
+        tab_rowswap(t, r, anticomlog - nn - 1, true);
+        tab_rowswap(t, r + nn, anticomlog - 1, true);
+      }
+      update(r + 1, nn, r + 1);
+      *rank_io += 1;
+      anticommutes = *rank_io;
+      tab_setrow(t, r, t.row(nn + r), ph[nn + r]);
+      set_projector(nn + r);
+    } else if (keep_result) {
+      std::vector<u64> np(W, 0);
+      u8 nph = 0;
+      for (size_t i = 0; i < r; i++)
+        if (IS(i)) {
+          u8 e = row_mul_left(np.data(), t.row(nn + i), W, P);
+          if (P) nph = (u8)((e + nph + ph[nn + i]) & 3);
+        }
+      result = nph;
+    }
+  } else {
+    update(r, nn, (size_t)anticommutes);
+    size_t a = (size_t)anticommutes - 1;
+    tab_setrow(t, a, t.row(nn + a), ph[nn + a]);
+    set_projector(nn + a);
+  }
+  *anticom_out = anticommutes;
+  *result_out = result;
+}
+
 // Symbolic gate application with phases (src/symbolic_cliffords.jl:62-74, 293-316).
 int oracle_apply_gates(u64* xzs, u8* ph, size_t rows, u32 n, const qcb_op* ops, size_t nops,
                        int phases) {

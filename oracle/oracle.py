@@ -56,6 +56,12 @@ def L():
             "oracle_frame_init_z": ([vp, u64, u32, vp, u64], None),
             "oracle_pftrajectories_philox": ([vp, vp, u64, u32, u32, vp, sz, u64, u64], None),
             "oracle_philox_init_z": ([vp, u64, u32, u64, u64], None),
+            "oracle_canonicalize_state": ([i, vp, vp, sz, u32, i, i, P(ctypes.c_int), P(ctypes.c_int)], None),
+            "oracle_canonicalize_rref": ([i, vp, vp, sz, u32, i, vp, sz, i], i),
+            "oracle_permutesystems": ([vp, sz, u32, vp], None),
+            "oracle_canonicalize_gott": ([vp, vp, sz, u32, i, P(ctypes.c_int), P(ctypes.c_int), vp, vp], None),
+            "oracle_project_cond": ([vp, vp, sz, u32, P(ctypes.c_int), u32, i, i, i, P(ctypes.c_int),
+                                     P(ctypes.c_int)], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(_L, name)
@@ -104,6 +110,58 @@ def canonicalize(phases, xzs, n, use_phases=True):
     rx, rz = ctypes.c_int(), ctypes.c_int()
     L().oracle_canonicalize(_p(xz), _p(ph), len(ph), n, int(use_phases), ctypes.byref(rx), ctypes.byref(rz))
     return ph, xz, rx.value, rz.value
+
+
+def canonicalize_state(kind, phases, xzs, n, rank=0, use_phases=True):
+    """_canonicalize!(state) on a whole state tableau (the Destabilizer kinds
+    carry their destabilizer rows along).  Returns (phases, xzs, rx, rz)."""
+    ph = np.array(phases, dtype=np.uint8, copy=True)
+    xz = np.array(xzs, dtype=np.uint64, copy=True)
+    rx, rz = ctypes.c_int(), ctypes.c_int()
+    L().oracle_canonicalize_state(KIND[kind] if isinstance(kind, str) else kind, _p(xz), _p(ph), len(ph), n,
+                                  int(rank), int(use_phases), ctypes.byref(rx), ctypes.byref(rz))
+    return ph, xz, rx.value, rz.value
+
+
+def canonicalize_rref(kind, phases, xzs, n, cols, rank=0, use_phases=True):
+    """_canonicalize_rref!(state, cols) with 1-based cols.  Returns (phases, xzs, i)."""
+    ph = np.array(phases, dtype=np.uint8, copy=True)
+    xz = np.array(xzs, dtype=np.uint64, copy=True)
+    c = np.ascontiguousarray(cols, dtype=np.uint32)
+    i = L().oracle_canonicalize_rref(KIND[kind] if isinstance(kind, str) else kind, _p(xz), _p(ph), len(ph), n,
+                                     int(rank), _p(c), len(c), int(use_phases))
+    return ph, xz, int(i)
+
+
+def permutesystems(xzs, n, perm):
+    xz = np.array(xzs, dtype=np.uint64, copy=True)
+    pm = np.ascontiguousarray(perm, dtype=np.uint32)
+    L().oracle_permutesystems(_p(xz), xz.shape[0], n, _p(pm))
+    return xz
+
+
+def canonicalize_gott(phases, xzs, n, use_phases=True):
+    """_canonicalize_gott!(stabilizer).  Returns (phases, xzs, r, s, xperm, zperm), perms 1-based."""
+    ph = np.array(phases, dtype=np.uint8, copy=True)
+    xz = np.array(xzs, dtype=np.uint64, copy=True)
+    r, s = ctypes.c_int(), ctypes.c_int()
+    xp = np.zeros(max(n, 1), np.uint32)
+    zp = np.zeros(max(n, 1), np.uint32)
+    L().oracle_canonicalize_gott(_p(xz), _p(ph), len(ph), n, int(use_phases), ctypes.byref(r), ctypes.byref(s),
+                                 _p(xp), _p(zp))
+    return ph, xz, r.value, s.value, xp[:n], zp[:n]
+
+
+def project_cond(phases, xzs, n, rank, qubit, basis, keep_result=True, use_phases=True):
+    """project_cond! behind projectX!/projectZ!/projectY! (basis 1/2/3) on a
+    MixedDestabilizer.  Returns (phases, xzs, rank, anticom, result), result -1 = nothing."""
+    ph = np.array(phases, dtype=np.uint8, copy=True)
+    xz = np.array(xzs, dtype=np.uint64, copy=True)
+    r = ctypes.c_int(rank)
+    a, res = ctypes.c_int(), ctypes.c_int()
+    L().oracle_project_cond(_p(xz), _p(ph), len(ph), n, ctypes.byref(r), int(qubit), int(basis), int(keep_result),
+                            int(use_phases), ctypes.byref(a), ctypes.byref(res))
+    return ph, xz, r.value, a.value, res.value
 
 
 def generate(p_xz, p_ph, phases, xzs, n, use_phases=True):

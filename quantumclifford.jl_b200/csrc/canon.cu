@@ -40,16 +40,30 @@ __device__ __forceinline__ void mul_step_c(uint64_t x1, uint64_t z1, uint64_t& x
   z2 = nz;
 }
 
+// Elimination modes of canon_kernel.
+enum : uint32_t {
+  ELIM_BOTH = 0,  // canonicalize!: X stage then Z stage over all columns
+  ELIM_X = 1,     // canonicalize_gott! first stage: X stage only
+  ELIM_Z = 2,     // canonicalize_gott! second stage: Z stage from column c0, pivots from row i0
+  ELIM_RREF = 3   // canonicalize_rref!: X then Z per listed column, pivots from the last row upwards
+};
+
 struct CanonArgs {
-  uint64_t* xzs;   // first row of the view
+  uint64_t* xzs;   // first row of the stabilizer view
   uint8_t* ph;
+  uint64_t* dxzs;  // destabilizer rows paired with the view rows (Destabilizer kinds), or null
+  uint8_t* dph;
   uint32_t rows, n, W;
   uint32_t RB;     // rows per CTA
   int phases;
   int smem_rows;   // 1: rows staged in shared memory
-  uint64_t* gtmp;  // global mode: permuted output
+  uint64_t* gtmp;  // global mode: permuted output (view rows, then destabilizer rows)
   uint8_t* gtmp_ph;
-  int32_t* out;    // rx, rz
+  int32_t* out;    // [0] pivots of the X stage (ELIM_BOTH) or of the launch, [1] next pivot position
+  uint32_t mode, c0, i0;
+  const uint32_t* cols;  // ELIM_RREF columns, 0-based
+  uint32_t ncols;
+  int32_t* pivcols;      // column of every pivot in order, or null
 };
 
 constexpr uint32_t CANON_THREADS = 1024;
@@ -62,131 +76,244 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a)
   const uint32_t W = a.W, len = W / 2, WS = W + 1;
   const uint32_t r0 = me * a.RB;
   const uint32_t nloc = r0 < a.rows ? min(a.RB, a.rows - r0) : 0u;
+  const bool D = a.dxzs != nullptr;
 
   extern __shared__ __align__(16) uint64_t smem[];
-  uint64_t* piv = smem;                                   // W words
-  uint64_t* rowsbuf = piv + W + 1;                        // RB * WS words (smem mode)
-  uint8_t* bytes = (uint8_t*)(rowsbuf + (a.smem_rows ? (size_t)a.RB * WS : 0));
-  uint32_t* slot = (uint32_t*)bytes;                      // 2 candidate slots
-  uint32_t* red = slot + 2;                               // 32 warp minima
-  uint32_t* ctl = red + 32;                               // [0]=k [1]=pstar [2]=piv phase
-  uint32_t* inv = ctl + 4;                                // rows (replicated)
-  uint32_t* pos = inv + a.rows;                           // RB
-  uint8_t* lph = (uint8_t*)(pos + a.RB);                  // RB
+  uint64_t* piv = smem;                                               // W words
+  uint64_t* rowsbuf = piv + W + 1;                                    // RB * WS words (smem mode)
+  uint64_t* drows = rowsbuf + (a.smem_rows ? (size_t)a.RB * WS : 0);  // RB * WS words (smem mode, D)
+  uint64_t* part = drows + (a.smem_rows && D ? (size_t)a.RB * WS : 0);  // 2 x W words (D)
+  uint32_t* slot = (uint32_t*)(part + (D ? 2 * (size_t)W : 0));       // 2 candidate slots
+  uint32_t* red = slot + 2;                                           // 32 warp minima
+  uint32_t* ctl = red + 32;                                           // [0]=k [1]=pstar [2]=piv phase
+  uint32_t* inv = ctl + 4;                                            // rows (replicated)
+  uint32_t* pos = inv + a.rows;                                       // RB
+  uint8_t* lph = (uint8_t*)(pos + a.RB);                              // RB
+  uint8_t* dlph = lph + a.RB;                                         // RB (D)
 
   auto ROW = [&](uint32_t r) -> uint64_t* {
     return a.smem_rows ? rowsbuf + (size_t)r * WS : a.xzs + (size_t)(r0 + r) * W;
+  };
+  auto DROW = [&](uint32_t r) -> uint64_t* {
+    return a.smem_rows ? drows + (size_t)r * WS : a.dxzs + (size_t)(r0 + r) * W;
   };
 
   for (uint32_t r = tid; r < nloc; r += blockDim.x) {
     pos[r] = r0 + r;
     lph[r] = a.ph[r0 + r];
+    if (D) dlph[r] = a.dph[r0 + r];
   }
   if (a.smem_rows) {
     for (uint32_t r = warp; r < nloc; r += nwarps)
-      for (uint32_t w = lane; w < W; w += 32) rowsbuf[(size_t)r * WS + w] = a.xzs[(size_t)(r0 + r) * W + w];
+      for (uint32_t w = lane; w < W; w += 32) {
+        rowsbuf[(size_t)r * WS + w] = a.xzs[(size_t)(r0 + r) * W + w];
+        if (D) drows[(size_t)r * WS + w] = a.dxzs[(size_t)(r0 + r) * W + w];
+      }
   }
   for (uint32_t p = tid; p < a.rows; p += blockDim.x) inv[p] = p;
   cl.sync();
 
-  uint32_t i = 0, step = 0, rx = 0;
-  for (uint32_t stage = 0; stage < 2; stage++) {
-    for (uint32_t j = 0; j < a.n; j++, step++) {
-      const uint32_t wj = stage * len + (j >> 6);
-      const uint64_t bm = 1ull << (j & 63);
-      // local candidate: smallest position >= i with the bit set
-      uint32_t best = 0xFFFFFFFFu;
-      for (uint32_t r = tid; r < nloc; r += blockDim.x) {
-        const uint32_t p = pos[r];
-        if (p >= i && (ROW(r)[wj] & bm)) best = min(best, p);
+  // The destabilizer update of mul_left!(state, m, i) (destabilizer i <- m * i,
+  // no phase) XORs the destabilizer rows of every eliminated row into the
+  // pivot's.  Each CTA accumulates its rows' share in part[parity]; the pivot
+  // row's owner folds the cluster's shares in after the next cluster barrier
+  // (before it can read that row again).
+  bool pend = false;
+  uint32_t pend_par = 0, pend_owner = 0, pend_lr = 0;
+  auto fold_pending = [&]() {
+    if (pend && me == pend_owner) {
+      uint64_t* dst = DROW(pend_lr);
+      for (uint32_t w = tid; w < W; w += blockDim.x) {
+        uint64_t x = 0;
+        for (uint32_t q = 0; q < CS; q++) x ^= *cl.map_shared_rank(part + (size_t)pend_par * W + w, q);
+        dst[w] ^= x;
       }
-      best = __reduce_min_sync(0xFFFFFFFFu, best);
-      if (lane == 0) red[warp] = best;
-      __syncthreads();
-      if (warp == 0) {
-        uint32_t b = lane < nwarps ? red[lane] : 0xFFFFFFFFu;
-        b = __reduce_min_sync(0xFFFFFFFFu, b);
-        if (lane == 0) slot[step & 1] = b;
-      }
-      cl.sync();
-      if (warp == 0) {
-        // the cluster's candidates, one CTA per lane
-        uint32_t k = lane < CS ? *cl.map_shared_rank(&slot[step & 1], lane) : 0xFFFFFFFFu;
-        k = __reduce_min_sync(0xFFFFFFFFu, k);
-        if (lane == 0) ctl[0] = k;
-        if (lane == 0 && k != 0xFFFFFFFFu) {
-          // rowswap!(state, k, i) on logical positions
-          const uint32_t pstar = inv[k], aphys = inv[i];
-          inv[i] = pstar;
-          inv[k] = aphys;
-          if (pstar >= r0 && pstar < r0 + nloc) pos[pstar - r0] = i;
-          if (aphys >= r0 && aphys < r0 + nloc) pos[aphys - r0] = k;
-          ctl[1] = pstar;
-        }
-      }
-      __syncthreads();
-      const uint32_t k = ctl[0];
-      if (k == 0xFFFFFFFFu) continue;
-      const uint32_t pstar = ctl[1];
-      const uint32_t owner = pstar / a.RB, lr = pstar - owner * a.RB;
-      {
-        const uint64_t* src;
-        const uint8_t* srcph;
-        if (a.smem_rows) {
-          uint64_t* base = rowsbuf + (size_t)lr * WS;
-          uint8_t* pb = lph + lr;
-          src = owner == me ? base : cl.map_shared_rank(base, owner);
-          srcph = owner == me ? pb : cl.map_shared_rank(pb, owner);
-        } else {
-          src = a.xzs + (size_t)pstar * W;
-          uint8_t* pb = lph + lr;
-          srcph = owner == me ? pb : cl.map_shared_rank(pb, owner);
-        }
-        for (uint32_t w = tid; w < W; w += blockDim.x) piv[w] = src[w];
-        if (tid == 0) ctl[2] = *srcph;
-      }
-      __syncthreads();
-      const uint32_t pph = ctl[2];
-      for (uint32_t r = warp; r < nloc; r += nwarps) {
-        if (r0 + r == pstar) continue;
-        uint64_t* row = ROW(r);
-        if (!(row[wj] & bm)) continue;
-        uint64_t c1 = 0, c2 = 0;
-        for (uint32_t w = lane; w < len; w += 32) {
-          uint64_t x2 = row[w], z2 = row[len + w];
-          mul_step_c(piv[w], piv[len + w], x2, z2, c1, c2);
-          row[w] = x2;
-          row[len + w] = z2;
-        }
-        if (a.phases) {
-          const uint32_t s =
-              __reduce_add_sync(0xFFFFFFFFu, (uint32_t)(__popcll(c1) + 2 * __popcll(c2)) & 3u) & 3u;
-          if (lane == 0) lph[r] = (uint8_t)((s + lph[r] + pph) & 3u);
-        }
-      }
-      __syncthreads();
-      i++;
     }
-    if (stage == 0) rx = i;
+    pend = false;
+  };
+
+  const bool desc = a.mode == ELIM_RREF;
+  const uint32_t nsteps = desc ? 2 * a.ncols
+                               : (a.mode == ELIM_BOTH ? 2 * a.n : (a.mode == ELIM_X ? a.n : (a.n > a.c0 ? a.n - a.c0 : 0u)));
+  int32_t i = desc ? (int32_t)a.rows - 1 : (int32_t)a.i0;  // next pivot position
+  uint32_t rx = 0, step = 0, npiv = 0;
+  for (uint32_t t = 0; t < nsteps; t++) {
+    uint32_t stage, j;
+    if (desc) {
+      j = a.cols[t >> 1];
+      stage = t & 1;
+    } else if (a.mode == ELIM_BOTH) {
+      stage = t >= a.n;
+      j = stage ? t - a.n : t;
+      if (t == a.n) rx = (uint32_t)i;
+    } else if (a.mode == ELIM_X) {
+      stage = 0;
+      j = t;
+    } else {
+      stage = 1;
+      j = a.c0 + t;
+    }
+    // the search range [i, rows) (or [0, i] from the bottom) is empty
+    if (desc ? i < 0 : i >= (int32_t)a.rows) continue;
+    const uint32_t lo = desc ? 0u : (uint32_t)i, hi = desc ? (uint32_t)i : a.rows - 1;
+    const uint32_t wj = stage * len + (j >> 6);
+    const uint64_t bm = 1ull << (j & 63);
+    // local candidate: smallest position in [lo, hi] with the bit set
+    uint32_t best = 0xFFFFFFFFu;
+    for (uint32_t r = tid; r < nloc; r += blockDim.x) {
+      const uint32_t p = pos[r];
+      if (p >= lo && p <= hi && (ROW(r)[wj] & bm)) best = min(best, p);
+    }
+    best = __reduce_min_sync(0xFFFFFFFFu, best);
+    if (lane == 0) red[warp] = best;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t b = lane < nwarps ? red[lane] : 0xFFFFFFFFu;
+      b = __reduce_min_sync(0xFFFFFFFFu, b);
+      if (lane == 0) slot[step & 1] = b;
+    }
+    cl.sync();
+    fold_pending();
+    if (warp == 0) {
+      // the cluster's candidates, one CTA per lane
+      uint32_t k = lane < CS ? *cl.map_shared_rank(&slot[step & 1], lane) : 0xFFFFFFFFu;
+      k = __reduce_min_sync(0xFFFFFFFFu, k);
+      if (lane == 0) ctl[0] = k;
+      if (lane == 0 && k != 0xFFFFFFFFu) {
+        // rowswap!(state, k, i) on logical positions
+        const uint32_t pstar = inv[k], aphys = inv[i];
+        inv[i] = pstar;
+        inv[k] = aphys;
+        if (pstar >= r0 && pstar < r0 + nloc) pos[pstar - r0] = (uint32_t)i;
+        if (aphys >= r0 && aphys < r0 + nloc) pos[aphys - r0] = k;
+        ctl[1] = pstar;
+      }
+    }
+    __syncthreads();
+    step++;
+    const uint32_t k = ctl[0];
+    if (k == 0xFFFFFFFFu) continue;
+    const uint32_t pstar = ctl[1];
+    const uint32_t owner = pstar / a.RB, lr = pstar - owner * a.RB;
+    const uint32_t par = npiv & 1;
+    {
+      const uint64_t* src;
+      const uint8_t* srcph;
+      if (a.smem_rows) {
+        uint64_t* base = rowsbuf + (size_t)lr * WS;
+        uint8_t* pb = lph + lr;
+        src = owner == me ? base : cl.map_shared_rank(base, owner);
+        srcph = owner == me ? pb : cl.map_shared_rank(pb, owner);
+      } else {
+        src = a.xzs + (size_t)pstar * W;
+        uint8_t* pb = lph + lr;
+        srcph = owner == me ? pb : cl.map_shared_rank(pb, owner);
+      }
+      for (uint32_t w = tid; w < W; w += blockDim.x) {
+        piv[w] = src[w];
+        if (D) part[(size_t)par * W + w] = 0;
+      }
+      if (tid == 0) ctl[2] = *srcph;
+    }
+    __syncthreads();
+    const uint32_t pph = ctl[2];
+    for (uint32_t r = warp; r < nloc; r += nwarps) {
+      if (r0 + r == pstar) continue;
+      uint64_t* row = ROW(r);
+      if (!(row[wj] & bm)) continue;
+      uint64_t c1 = 0, c2 = 0;
+      for (uint32_t w = lane; w < len; w += 32) {
+        uint64_t x2 = row[w], z2 = row[len + w];
+        mul_step_c(piv[w], piv[len + w], x2, z2, c1, c2);
+        row[w] = x2;
+        row[len + w] = z2;
+      }
+      if (a.phases) {
+        const uint32_t s =
+            __reduce_add_sync(0xFFFFFFFFu, (uint32_t)(__popcll(c1) + 2 * __popcll(c2)) & 3u) & 3u;
+        if (lane == 0) lph[r] = (uint8_t)((s + lph[r] + pph) & 3u);
+      }
+      if (D) {
+        const uint64_t* dr = DROW(r);
+        for (uint32_t w = lane; w < W; w += 32)
+          atomicXor((unsigned long long*)(part + (size_t)par * W + w), (unsigned long long)dr[w]);
+      }
+    }
+    __syncthreads();
+    if (D) {
+      pend = true;
+      pend_par = par;
+      pend_owner = owner;
+      pend_lr = lr;
+    }
+    if (a.pivcols && me == 0 && tid == 0) a.pivcols[npiv] = (int32_t)j;
+    npiv++;
+    if (desc) i--; else i++;
   }
+  if (a.mode == ELIM_BOTH && a.n == 0) rx = (uint32_t)i;
   // every CTA is done reading remote shared memory before anyone leaves
   cl.sync();
+  if (D) {
+    fold_pending();
+    __syncthreads();
+    cl.sync();
+  }
   if (a.smem_rows) {
     for (uint32_t r = warp; r < nloc; r += nwarps) {
       const uint32_t p = pos[r];
-      for (uint32_t w = lane; w < W; w += 32) a.xzs[(size_t)p * W + w] = rowsbuf[(size_t)r * WS + w];
-      if (lane == 0 && a.phases) a.ph[p] = lph[r];
+      for (uint32_t w = lane; w < W; w += 32) {
+        a.xzs[(size_t)p * W + w] = rowsbuf[(size_t)r * WS + w];
+        if (D) a.dxzs[(size_t)p * W + w] = drows[(size_t)r * WS + w];
+      }
+      if (lane == 0 && a.phases) {
+        a.ph[p] = lph[r];
+        if (D) a.dph[p] = dlph[r];
+      }
     }
   } else {
     for (uint32_t r = warp; r < nloc; r += nwarps) {
       const uint32_t p = pos[r];
-      for (uint32_t w = lane; w < W; w += 32) a.gtmp[(size_t)p * W + w] = a.xzs[(size_t)(r0 + r) * W + w];
-      if (lane == 0) a.gtmp_ph[p] = a.phases ? lph[r] : a.ph[p];
+      for (uint32_t w = lane; w < W; w += 32) {
+        a.gtmp[(size_t)p * W + w] = a.xzs[(size_t)(r0 + r) * W + w];
+        if (D) a.gtmp[(size_t)(a.rows + p) * W + w] = a.dxzs[(size_t)(r0 + r) * W + w];
+      }
+      if (lane == 0) {
+        a.gtmp_ph[p] = a.phases ? lph[r] : a.ph[p];
+        if (D) a.gtmp_ph[a.rows + p] = a.phases ? dlph[r] : a.dph[p];
+      }
     }
   }
   if (me == 0 && tid == 0) {
-    a.out[0] = (int32_t)rx;
-    a.out[1] = (int32_t)i;
+    a.out[0] = (int32_t)(a.mode == ELIM_BOTH ? rx : npiv);
+    a.out[1] = i;
+  }
+}
+
+// permutesystems!(s, perm) (src/linalg.jl:7-17): every row becomes row[perm]
+// (new qubit j is old qubit perm[j], 0-based here); phases stay.  One warp per
+// row, the old row staged in shared memory.
+__global__ void permute_kernel(uint64_t* xzs, uint32_t rows, uint32_t n, uint32_t W, const uint32_t* perm) {
+  extern __shared__ __align__(16) uint64_t pbuf[];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t len = W / 2;
+  uint64_t* old = pbuf + (size_t)warp * W;
+  for (uint32_t m = blockIdx.x * nw + warp; m < rows; m += gridDim.x * nw) {
+    uint64_t* row = xzs + (size_t)m * W;
+    for (uint32_t w = lane; w < W; w += 32) old[w] = row[w];
+    __syncwarp();
+    for (uint32_t w = lane; w < len; w += 32) {
+      uint64_t x = 0, z = 0;
+      for (uint32_t b = 0; b < 64; b++) {
+        const uint32_t j = w * 64 + b;
+        if (j >= n) break;
+        const uint32_t q = perm[j];
+        x |= ((old[q >> 6] >> (q & 63)) & 1ull) << b;
+        z |= ((old[len + (q >> 6)] >> (q & 63)) & 1ull) << b;
+      }
+      row[w] = x;
+      row[len + w] = z;
+    }
+    __syncwarp();
   }
 }
 
@@ -288,22 +415,23 @@ struct CanonPlan {
   uint32_t RB;
 };
 
-static size_t canon_smem(uint32_t rows, uint32_t W, uint32_t RB, bool smem_rows) {
+static size_t canon_smem(uint32_t rows, uint32_t W, uint32_t RB, bool smem_rows, bool D) {
   size_t b = (size_t)(W + 1) * 8;
-  if (smem_rows) b += (size_t)RB * (W + 1) * 8;
-  b += (2 + 32 + 4) * 4 + (size_t)rows * 4 + (size_t)RB * 4 + RB + 16;
+  if (smem_rows) b += (size_t)RB * (W + 1) * 8 * (D ? 2 : 1);
+  if (D) b += (size_t)2 * W * 8;
+  b += (2 + 32 + 4) * 4 + (size_t)rows * 4 + (size_t)RB * 4 + (size_t)RB * (D ? 2 : 1) + 16;
   return (b + 15) / 16 * 16;
 }
 
 static uint32_t g_canon_cs = 0;       // tuner override (0 = automatic)
 static uint32_t g_canon_threads = 0;  // tuner override (0 = automatic)
 
-static CanonPlan canon_plan(uint32_t rows, uint32_t W) {
+static CanonPlan canon_plan(uint32_t rows, uint32_t W, bool D) {
   const size_t maxsm = (size_t)device_max_smem_optin();
   if (g_canon_cs) {
     const uint32_t cs = g_canon_cs, RB = std::max<uint32_t>(1, (rows + cs - 1) / cs);
-    const bool sm = canon_smem(rows, W, RB, true) <= maxsm;
-    return {cs, sm, canon_smem(rows, W, RB, sm), RB};
+    const bool sm = canon_smem(rows, W, RB, true, D) <= maxsm;
+    return {cs, sm, canon_smem(rows, W, RB, sm, D), RB};
   }
   // measured on B200 (random full-rank stabilizers, n = 1000 / 2000 / 4000):
   // 16 CTAs beat 8 / 4 / 2 / 1 at every size (3.4 / 8.8 / 47 ms); a small
@@ -313,28 +441,49 @@ static CanonPlan canon_plan(uint32_t rows, uint32_t W) {
   for (uint32_t ci = 0; ci < 5; ci++) {
     const uint32_t cs = cands[ci];
     const uint32_t RB = std::max<uint32_t>(1, (rows + cs - 1) / cs);
-    if (canon_smem(rows, W, RB, true) <= maxsm) return {cs, true, canon_smem(rows, W, RB, true), RB};
+    if (canon_smem(rows, W, RB, true, D) <= maxsm) return {cs, true, canon_smem(rows, W, RB, true, D), RB};
   }
   const uint32_t cs = 16, RB = std::max<uint32_t>(1, (rows + cs - 1) / cs);
-  return {cs, false, canon_smem(rows, W, RB, false), RB};
+  return {cs, false, canon_smem(rows, W, RB, false, D), RB};
 }
 
-int canonicalize_view(uint64_t* xzs, uint8_t* ph, uint32_t rows, uint32_t n, uint32_t W, int phases,
-                      int32_t* d_out, cudaStream_t st) {
-  if (rows == 0) {
-    QCB_CUDA(cudaMemsetAsync(d_out, 0, 8, st));
+// One elimination launch (any mode) on a stabilizer view and, for the
+// Destabilizer kinds, its destabilizer rows.  d_out receives [pivots, next i].
+struct ElimSpec {
+  uint64_t* xzs;
+  uint8_t* ph;
+  uint64_t* dxzs;
+  uint8_t* dph;
+  uint32_t rows, n, W;
+  int phases;
+  uint32_t mode, c0, i0;
+  const uint32_t* d_cols;
+  uint32_t ncols;
+  int32_t* d_pivcols;
+  int32_t* d_out;
+};
+
+static int eliminate(const ElimSpec& e, cudaStream_t st) {
+  if (e.rows == 0) {
+    const int32_t h[2] = {0, e.mode == ELIM_RREF ? -1 : (int32_t)e.i0};
+    QCB_CUDA(cudaMemcpyAsync(e.d_out, h, 8, cudaMemcpyHostToDevice, st));
+    QCB_CUDA(cudaStreamSynchronize(st));  // h is on this stack frame
     return QCB_OK;
   }
-  CanonPlan p = canon_plan(rows, W);
+  const bool D = e.dxzs != nullptr;
+  CanonPlan p = canon_plan(e.rows, e.W, D);
   if (p.smem_bytes > (size_t)device_max_smem_optin())
     return fail(QCB_EUNSUPPORTED, "canonicalize!: tableau too tall for the cluster's bookkeeping");
   CanonArgs a{};
-  a.xzs = xzs; a.ph = ph; a.rows = rows; a.n = n; a.W = W; a.RB = p.RB; a.phases = phases;
+  a.xzs = e.xzs; a.ph = e.ph; a.dxzs = e.dxzs; a.dph = e.dph;
+  a.rows = e.rows; a.n = e.n; a.W = e.W; a.RB = p.RB; a.phases = e.phases;
   a.smem_rows = p.smem_rows ? 1 : 0;
-  a.out = d_out;
+  a.out = e.d_out;
+  a.mode = e.mode; a.c0 = e.c0; a.i0 = e.i0; a.cols = e.d_cols; a.ncols = e.ncols; a.pivcols = e.d_pivcols;
+  const size_t nout = (size_t)e.rows * (D ? 2 : 1);
   if (!p.smem_rows) {
-    QCB_CUDA(cudaMallocAsync(&a.gtmp, (size_t)rows * W * 8, st));
-    QCB_CUDA(cudaMallocAsync(&a.gtmp_ph, rows, st));
+    QCB_CUDA(cudaMallocAsync(&a.gtmp, nout * e.W * 8, st));
+    QCB_CUDA(cudaMallocAsync(&a.gtmp_ph, nout, st));
   }
   QCB_CUDA(cudaFuncSetAttribute(canon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_bytes));
   if (p.cs > 8) QCB_CUDA(cudaFuncSetAttribute(canon_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -353,12 +502,68 @@ int canonicalize_view(uint64_t* xzs, uint8_t* ph, uint32_t rows, uint32_t n, uin
   QCB_CUDA(cudaLaunchKernelEx(&cfg, canon_kernel, a));
   QCB_LAUNCHED();
   if (!p.smem_rows) {
-    QCB_CUDA(cudaMemcpyAsync(xzs, a.gtmp, (size_t)rows * W * 8, cudaMemcpyDeviceToDevice, st));
-    QCB_CUDA(cudaMemcpyAsync(ph, a.gtmp_ph, rows, cudaMemcpyDeviceToDevice, st));
+    QCB_CUDA(cudaMemcpyAsync(e.xzs, a.gtmp, (size_t)e.rows * e.W * 8, cudaMemcpyDeviceToDevice, st));
+    QCB_CUDA(cudaMemcpyAsync(e.ph, a.gtmp_ph, e.rows, cudaMemcpyDeviceToDevice, st));
+    if (D) {
+      QCB_CUDA(cudaMemcpyAsync(e.dxzs, a.gtmp + (size_t)e.rows * e.W, (size_t)e.rows * e.W * 8,
+                               cudaMemcpyDeviceToDevice, st));
+      QCB_CUDA(cudaMemcpyAsync(e.dph, a.gtmp_ph + e.rows, e.rows, cudaMemcpyDeviceToDevice, st));
+    }
     QCB_CUDA(cudaFreeAsync(a.gtmp, st));
     QCB_CUDA(cudaFreeAsync(a.gtmp_ph, st));
   }
   return QCB_OK;
+}
+
+int canonicalize_view(uint64_t* xzs, uint8_t* ph, uint32_t rows, uint32_t n, uint32_t W, int phases,
+                      int32_t* d_out, cudaStream_t st) {
+  ElimSpec e{};
+  e.xzs = xzs; e.ph = ph; e.rows = rows; e.n = n; e.W = W; e.phases = phases;
+  e.mode = ELIM_BOTH; e.d_out = d_out;
+  return eliminate(e, st);
+}
+
+// permutesystems! with a 0-based device permutation.
+static int permute_dev(uint64_t* xzs, uint32_t rows, uint32_t n, uint32_t W, const uint32_t* d_perm,
+                       cudaStream_t st) {
+  if (!rows || !n) return QCB_OK;
+  const uint32_t threads = 256, wpb = threads / 32;
+  const size_t sm = (size_t)wpb * W * 8;
+  if (sm > 48 * 1024) QCB_CUDA(cudaFuncSetAttribute(permute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const uint32_t blocks = std::min<uint32_t>((rows + wpb - 1) / wpb, 4 * (uint32_t)device_sm_count());
+  permute_kernel<<<blocks, threads, sm, st>>>(xzs, rows, n, W, d_perm);
+  QCB_LAUNCHED();
+  return QCB_OK;
+}
+
+// The stabilizer view of a state of the given kind (src/QuantumClifford.jl
+// stabilizerview): rows [off, off + rows); the Destabilizer kinds pair view
+// row i with destabilizer row i.
+static int state_view(const qcb_tableau* t, int kind, int32_t rank, uint32_t* off, uint32_t* rows, bool* destab) {
+  *off = 0;
+  *rows = t->rows;
+  *destab = false;
+  switch (kind) {
+    case QCB_STABILIZER: return QCB_OK;
+    case QCB_MIXED_STABILIZER:
+      if (rank < 0 || (uint32_t)rank > t->rows) return fail(QCB_EBOUNDS, "rank out of range");
+      *rows = (uint32_t)rank;
+      return QCB_OK;
+    case QCB_DESTABILIZER:
+      if (t->rows % 2) return fail(QCB_EDIM, "destabilizer tableaux have an even number of rows");
+      *off = t->rows / 2;
+      *rows = t->rows / 2;
+      *destab = true;
+      return QCB_OK;
+    case QCB_MIXED_DESTABILIZER:
+      if (t->rows != 2 * t->nqubits) return fail(QCB_EDIM, "MixedDestabilizer tableaux have 2n rows");
+      if (rank < 0 || (uint32_t)rank > t->nqubits) return fail(QCB_EBOUNDS, "rank out of range");
+      *off = t->nqubits;
+      *rows = (uint32_t)rank;
+      *destab = true;
+      return QCB_OK;
+  }
+  return fail(QCB_EARG, "bad state kind");
 }
 
 int generate_dev(uint64_t* pauli, uint8_t* pph, const uint64_t* xzs, const uint8_t* ph, uint32_t rows,
@@ -395,6 +600,158 @@ int qcb_canonicalize(qcb_tableau* t, uint32_t row0, uint32_t nrows, int phases, 
     QCB_CUDA(cudaStreamSynchronize(st));
     if (rx) *rx = h[0];
     if (rz) *rz = h[1];
+  }
+  return QCB_OK;
+}
+
+int qcb_canonicalize_state(qcb_tableau* t, int kind, int32_t rank, int phases, int32_t* rx, int32_t* rz,
+                           void* stream) {
+  if (!t) return fail(QCB_EARG, "null tableau");
+  uint32_t off, rows;
+  bool destab;
+  if (int s = state_view(t, kind, rank, &off, &rows, &destab)) return s;
+  cudaStream_t st = S(stream);
+  ElimSpec e{};
+  e.xzs = t->xzs + (size_t)off * t->W; e.ph = t->phases + off;
+  if (destab) { e.dxzs = t->xzs; e.dph = t->phases; }
+  e.rows = rows; e.n = t->nqubits; e.W = t->W; e.phases = phases;
+  e.mode = ELIM_BOTH; e.d_out = (int32_t*)t->scratch + 16;
+  if (int s = eliminate(e, st)) return s;
+  if (rx || rz) {
+    int32_t h[2];
+    QCB_CUDA(cudaMemcpyAsync(h, e.d_out, 8, cudaMemcpyDeviceToHost, st));
+    QCB_CUDA(cudaStreamSynchronize(st));
+    if (rx) *rx = h[0];
+    if (rz) *rz = h[1];
+  }
+  return QCB_OK;
+}
+
+int qcb_canonicalize_rref(qcb_tableau* t, int kind, int32_t rank, const uint32_t* cols, size_t ncols, int phases,
+                          int32_t* i_out, void* stream) {
+  if (!t || (ncols && !cols)) return fail(QCB_EARG, "null argument");
+  uint32_t off, rows;
+  bool destab;
+  if (int s = state_view(t, kind, rank, &off, &rows, &destab)) return s;
+  std::vector<uint32_t> c0(ncols);
+  for (size_t k = 0; k < ncols; k++) {
+    if (cols[k] == 0) return fail(QCB_EZEROQUBIT, "qubit indices start at 1 (NoZeroQubit)");
+    if (cols[k] > t->nqubits) return fail(QCB_EBOUNDS, "canonicalize_rref!: column index exceeds the qubits");
+    c0[k] = cols[k] - 1;
+  }
+  cudaStream_t st = S(stream);
+  uint32_t* d_cols = nullptr;
+  if (ncols) {
+    QCB_CUDA(cudaMallocAsync(&d_cols, ncols * 4, st));
+    QCB_CUDA(cudaMemcpyAsync(d_cols, c0.data(), ncols * 4, cudaMemcpyHostToDevice, st));
+  }
+  ElimSpec e{};
+  e.xzs = t->xzs + (size_t)off * t->W; e.ph = t->phases + off;
+  if (destab) { e.dxzs = t->xzs; e.dph = t->phases; }
+  e.rows = rows; e.n = t->nqubits; e.W = t->W; e.phases = phases;
+  e.mode = ELIM_RREF; e.d_cols = d_cols; e.ncols = (uint32_t)ncols; e.d_out = (int32_t*)t->scratch + 16;
+  int s = eliminate(e, st);
+  int32_t h[2] = {0, 0};
+  if (s == QCB_OK) {
+    if (cudaMemcpyAsync(h, e.d_out, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess) s = fail(QCB_ECUDA, "copy");
+  }
+  if (d_cols) cudaFreeAsync(d_cols, st);
+  QCB_CUDA(cudaStreamSynchronize(st));
+  if (s == QCB_OK && i_out) *i_out = h[1] + 1;  // the reference's 1-based `i`
+  return s;
+}
+
+int qcb_permutesystems(qcb_tableau* t, const uint32_t* perm, void* stream) {
+  if (!t || !perm) return fail(QCB_EARG, "null argument");
+  const uint32_t n = t->nqubits;
+  std::vector<uint32_t> p0(n);
+  std::vector<uint8_t> seen(n, 0);
+  for (uint32_t j = 0; j < n; j++) {
+    if (perm[j] < 1 || perm[j] > n || seen[perm[j] - 1]) return fail(QCB_EARG, "permutesystems!: not a permutation");
+    seen[perm[j] - 1] = 1;
+    p0[j] = perm[j] - 1;
+  }
+  cudaStream_t st = S(stream);
+  if (!n || !t->rows) return QCB_OK;
+  uint32_t* d_perm = nullptr;
+  QCB_CUDA(cudaMallocAsync(&d_perm, (size_t)n * 4, st));
+  QCB_CUDA(cudaMemcpyAsync(d_perm, p0.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
+  int s = permute_dev(t->xzs, t->rows, n, t->W, d_perm, st);
+  cudaFreeAsync(d_perm, st);
+  QCB_CUDA(cudaStreamSynchronize(st));  // p0 lives on this stack frame
+  return s;
+}
+
+// gott_standard_form_indices (src/canonicalization.jl:187-204) from the
+// pivot columns of one stage: after the stage's elimination, row skip + a has
+// its first set bit at or after column skip at the a-th pivot column, and the
+// rows past the last pivot have none, so the row scan of the reference visits
+// exactly the pivot columns in order.  perm is 0-based.
+static void gott_perm(const std::vector<int32_t>& piv, uint32_t n, uint32_t skip, std::vector<uint32_t>& perm) {
+  perm.clear();
+  if (piv.empty()) {
+    for (uint32_t j = 0; j < n; j++) perm.push_back(j);
+    return;
+  }
+  std::vector<uint8_t> good(n, 0);
+  for (uint32_t j = 0; j < skip; j++) perm.push_back(j);
+  for (int32_t g : piv) { perm.push_back((uint32_t)g); good[g] = 1; }
+  const uint32_t last = (uint32_t)piv.back();
+  for (uint32_t j = skip; j <= last; j++)
+    if (!good[j]) perm.push_back(j);
+  for (uint32_t j = last + 1; j < n; j++) perm.push_back(j);
+}
+
+int qcb_canonicalize_gott(qcb_tableau* t, int phases, int32_t* r_out, int32_t* s_out, uint32_t* xperm,
+                          uint32_t* zperm, void* stream) {
+  if (!t) return fail(QCB_EARG, "null tableau");
+  const uint32_t n = t->nqubits;
+  cudaStream_t st = S(stream);
+  int32_t* d_piv = nullptr;
+  uint32_t* d_perm = nullptr;
+  QCB_CUDA(cudaMallocAsync(&d_piv, (size_t)std::max<uint32_t>(n, 1) * 4, st));
+  QCB_CUDA(cudaMallocAsync(&d_perm, (size_t)std::max<uint32_t>(n, 1) * 4, st));
+  std::vector<int32_t> piv;
+  std::vector<uint32_t> px, pz;
+  int32_t h[2] = {0, 0};
+  int s = QCB_OK;
+  uint32_t r = 0, sz = 0;
+  for (int stage = 0; stage < 2 && s == QCB_OK; stage++) {
+    ElimSpec e{};
+    e.xzs = t->xzs; e.ph = t->phases; e.rows = t->rows; e.n = n; e.W = t->W; e.phases = phases;
+    e.mode = stage == 0 ? ELIM_X : ELIM_Z;
+    e.c0 = stage == 0 ? 0 : r;
+    e.i0 = stage == 0 ? 0 : r;
+    e.d_pivcols = d_piv;
+    e.d_out = (int32_t*)t->scratch + 16;
+    if ((s = eliminate(e, st))) break;
+    if (cudaMemcpyAsync(h, e.d_out, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) { s = fail(QCB_ECUDA, "canonicalize_gott!: copy"); break; }
+    const uint32_t np = (uint32_t)(t->rows ? h[0] : 0);
+    piv.assign(np, 0);
+    if (np && (cudaMemcpyAsync(piv.data(), d_piv, (size_t)np * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+               cudaStreamSynchronize(st) != cudaSuccess)) { s = fail(QCB_ECUDA, "canonicalize_gott!: copy"); break; }
+    std::vector<uint32_t>& perm = stage == 0 ? px : pz;
+    gott_perm(piv, n, stage == 0 ? 0 : r, perm);
+    if (stage == 0) r = np; else sz = np;
+    if (n && t->rows) {
+      if (cudaMemcpyAsync(d_perm, perm.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        s = fail(QCB_ECUDA, "canonicalize_gott!: copy");
+        break;
+      }
+      if ((s = permute_dev(t->xzs, t->rows, n, t->W, d_perm, st))) break;
+      if (cudaStreamSynchronize(st) != cudaSuccess) { s = fail(QCB_ECUDA, "canonicalize_gott!: sync"); break; }
+    }
+  }
+  cudaFreeAsync(d_piv, st);
+  cudaFreeAsync(d_perm, st);
+  QCB_CUDA(cudaStreamSynchronize(st));
+  if (s != QCB_OK) return s;
+  if (r_out) *r_out = (int32_t)r;
+  if (s_out) *s_out = (int32_t)sz;
+  for (uint32_t j = 0; j < n; j++) {
+    if (xperm) xperm[j] = px[j] + 1;
+    if (zperm) zperm[j] = pz[j] + 1;
   }
   return QCB_OK;
 }

@@ -61,6 +61,9 @@ struct ProjArgs {
   int32_t* result;
   int32_t* status;       // [0] = status, [1] = index reached
   uint8_t* flags;        // rows
+  const uint32_t* qubits;  // projectX!/Y!/Z!: Pauli j is the single-qubit Pauli on qubits[j] (0-based), or null
+  uint32_t basis;          // with qubits: bit 0 = X component, bit 1 = Z component
+  const uint8_t* rand_ph;  // projectrand!: phase (0 or 2) given to the new stabilizer row of Pauli j, or null
 };
 
 constexpr uint32_t PROJ_THREADS = 1024;
@@ -99,32 +102,55 @@ __global__ void __launch_bounds__(PROJ_THREADS) project_kernel(const ProjArgs a)
 
   const uint32_t rows = a.rows;
   for (uint32_t j = a.j0; j < a.k; j++) {
-    const uint64_t* pj = a.paulis + (size_t)j * W;
-    for (uint32_t w = tid; w < W; w += blockDim.x) P[w] = pj[w];
+    const bool single = a.qubits != nullptr;
+    uint32_t wq = 0;
+    uint64_t bq = 0;
+    if (single) {
+      wq = a.qubits[j] >> 6;
+      bq = 1ull << (a.qubits[j] & 63);
+      for (uint32_t w = tid; w < W; w += blockDim.x)
+        P[w] = (((a.basis & 1u) && w == wq) ? bq : 0ull) | (((a.basis & 2u) && w == len + wq) ? bq : 0ull);
+    } else {
+      const uint64_t* pj = a.paulis + (size_t)j * W;
+      for (uint32_t w = tid; w < W; w += blockDim.x) P[w] = pj[w];
+    }
     if (tid < 3) mins[tid] = 0xFFFFFFFFu;
-    const uint32_t pphase = a.pph[j];
+    const uint32_t pphase = single ? 0u : a.pph[j];
     int32_t r = a.kind == QCB_STABILIZER ? (int32_t)rows : (a.kind == QCB_DESTABILIZER ? (int32_t)(rows / 2) : *a.rank);
     __syncthreads();
     const uint32_t nn = (a.kind == QCB_DESTABILIZER || a.kind == QCB_MIXED_DESTABILIZER) ? rows / 2 : rows;
     // 1. comm flags for every row and the first anticommuting rows
-    for (uint32_t m = gw; m < rows; m += NW) {
-      const uint64_t* row = a.xzs + (size_t)m * W;
-      uint64_t acc = 0;
-      for (uint32_t w = lane; w < len; w += 32) acc ^= (P[len + w] & row[w]) ^ (P[w] & row[len + w]);
-      const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)__popcll(acc)) & 1u;
-      if (lane == 0) {
-        a.flags[m] = (uint8_t)c;
-        if (c) {
-          if (a.kind == QCB_STABILIZER || a.kind == QCB_MIXED_STABILIZER) {
-            if (m < (uint32_t)r) atomicMin(&mins[0], m);
-          } else {
-            if (m >= nn && m < nn + (uint32_t)r) atomicMin(&mins[0], m - nn);
-            if (a.kind == QCB_MIXED_DESTABILIZER) {
-              if (m >= (uint32_t)r && m < nn) atomicMin(&mins[1], m);
-              if (m >= nn + (uint32_t)r) atomicMin(&mins[2], m);
-            }
+    auto note = [&](uint32_t m, uint32_t c) {
+      a.flags[m] = (uint8_t)c;
+      if (c) {
+        if (a.kind == QCB_STABILIZER || a.kind == QCB_MIXED_STABILIZER) {
+          if (m < (uint32_t)r) atomicMin(&mins[0], m);
+        } else {
+          if (m >= nn && m < nn + (uint32_t)r) atomicMin(&mins[0], m - nn);
+          if (a.kind == QCB_MIXED_DESTABILIZER) {
+            if (m >= (uint32_t)r && m < nn) atomicMin(&mins[1], m);
+            if (m >= nn + (uint32_t)r) atomicMin(&mins[2], m);
           }
         }
+      }
+    };
+    if (single) {
+      // comm with a single-qubit Pauli is one bit of the row (the isX / isZ /
+      // isXorZ tests of project_cond!, src/project_trace_reset.jl:476-479)
+      for (uint32_t m = me * blockDim.x + tid; m < rows; m += CS * blockDim.x) {
+        const uint64_t* row = a.xzs + (size_t)m * W;
+        uint32_t c = 0;
+        if (a.basis & 1u) c ^= (uint32_t)((row[len + wq] & bq) != 0);
+        if (a.basis & 2u) c ^= (uint32_t)((row[wq] & bq) != 0);
+        note(m, c);
+      }
+    } else {
+      for (uint32_t m = gw; m < rows; m += NW) {
+        const uint64_t* row = a.xzs + (size_t)m * W;
+        uint64_t acc = 0;
+        for (uint32_t w = lane; w < len; w += 32) acc ^= (P[len + w] & row[w]) ^ (P[w] & row[len + w]);
+        const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)__popcll(acc)) & 1u;
+        if (lane == 0) note(m, c);
       }
     }
     __syncthreads();
@@ -253,7 +279,13 @@ __global__ void __launch_bounds__(PROJ_THREADS) project_kernel(const ProjArgs a)
       if (a.kind == QCB_STABILIZER || a.kind == QCB_MIXED_STABILIZER) {
         const uint32_t ac = (uint32_t)dec[2];
         for (uint32_t w = tid; w < W; w += blockDim.x) a.xzs[(size_t)(ac - 1) * W + w] = P[w];
-        if (tid == 0) { a.ph[ac - 1] = (uint8_t)pphase; a.anticom[j] = (int32_t)ac; a.result[j] = -1; }
+        if (tid == 0) {
+          // projectrand!: the undetermined outcome gets a random sign
+          const int32_t rp = a.rand_ph ? (int32_t)a.rand_ph[j] : -1;
+          a.ph[ac - 1] = (uint8_t)(rp >= 0 ? rp : (int32_t)pphase);
+          a.anticom[j] = (int32_t)ac;
+          a.result[j] = rp;
+        }
       } else {
         const uint32_t ac = branch == 2 ? (uint32_t)r + 1 : (uint32_t)dec[2];
         // destabilizer[ac] = stabilizer[ac]; stabilizer[ac] = pauli
@@ -263,11 +295,12 @@ __global__ void __launch_bounds__(PROJ_THREADS) project_kernel(const ProjArgs a)
         __syncthreads();
         for (uint32_t w = tid; w < W; w += blockDim.x) a.xzs[(size_t)(nn + ac - 1) * W + w] = P[w];
         if (tid == 0) {
+          const int32_t rp = a.rand_ph ? (int32_t)a.rand_ph[j] : -1;
           a.ph[ac - 1] = a.ph[nn + ac - 1];
-          a.ph[nn + ac - 1] = (uint8_t)pphase;
+          a.ph[nn + ac - 1] = (uint8_t)(rp >= 0 ? rp : (int32_t)pphase);
           if (branch == 2) *a.rank = r + 1;
           a.anticom[j] = (int32_t)(branch == 2 ? r + 1 : (int32_t)ac);
-          a.result[j] = -1;
+          a.result[j] = rp;
         }
       }
     }
@@ -284,10 +317,14 @@ using namespace qcb;
 
 extern "C" {
 
-int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* paulis, int keep_result,
-                int phases, int32_t* anticom, int32_t* result, uint32_t* n_done, void* stream) {
-  if (!t || !paulis || !anticom || !result) return fail(QCB_EARG, "null argument");
-  if (paulis->nqubits != t->nqubits) return fail(QCB_EDIM, "project!: the Pauli and the state act on different numbers of qubits");
+// The k projections of one call: Paulis from a device tableau (pxzs, pph),
+// or single-qubit Paulis (qubits: 1-based host array, basis bit 0 = X,
+// bit 1 = Z); rand_host (host, 0 or 2 per projection) turns them into
+// projectrand!.
+static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64_t* pxzs, const uint8_t* pph,
+                        const uint32_t* qubits, uint32_t basis, uint32_t k, int keep_result, int phases,
+                        const uint8_t* rand_host, int32_t* anticom, int32_t* result, uint32_t* n_done, void* stream) {
+  if (!t || !anticom || !result) return fail(QCB_EARG, "null argument");
   if (kind < 0 || kind > 3) return fail(QCB_EARG, "project!: bad state kind");
   const bool mixed = kind == QCB_MIXED_STABILIZER || kind == QCB_MIXED_DESTABILIZER;
   if (mixed && !rank_io) return fail(QCB_EARG, "project!: rank required for mixed states");
@@ -298,9 +335,27 @@ int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* p
   if (mixed && (*rank_io < 0 || (uint32_t)*rank_io > (kind == QCB_MIXED_STABILIZER ? t->rows : t->rows / 2)))
     return fail(QCB_EBOUNDS, "project!: rank out of range");
   cudaStream_t st = S(stream);
-  const uint32_t k = paulis->rows;
   if (n_done) *n_done = 0;
   if (!k) return QCB_OK;
+  const uint32_t W = t->W, len = W / 2;
+  std::vector<uint32_t> q0;
+  if (qubits) {
+    q0.resize(k);
+    for (uint32_t j = 0; j < k; j++) {
+      if (qubits[j] == 0) return fail(QCB_EZEROQUBIT, "qubit indices start at 1 (NoZeroQubit)");
+      if (qubits[j] > t->nqubits) return fail(QCB_EBOUNDS, "project: qubit index exceeds the state's qubits");
+      q0[j] = qubits[j] - 1;
+    }
+  }
+  // the Pauli of projection j in host memory (single-qubit mode)
+  auto single_pauli = [&](uint32_t j) {
+    std::vector<uint64_t> hp(W, 0);
+    if (basis & 1u) hp[q0[j] >> 6] |= 1ull << (q0[j] & 63);
+    if (basis & 2u) hp[len + (q0[j] >> 6)] |= 1ull << (q0[j] & 63);
+    return hp;
+  };
+  uint32_t* d_q = nullptr;
+  uint8_t* d_rand = nullptr;
   int32_t *d_anti = nullptr, *d_res = nullptr, *d_stat = nullptr, *d_rank = nullptr, *d_cout = nullptr;
   uint8_t* d_flags = nullptr;
   uint64_t* d_tmp = nullptr;
@@ -313,6 +368,14 @@ int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* p
   QCB_CUDA(cudaMallocAsync(&d_flags, std::max<uint32_t>(t->rows, 1), st));
   QCB_CUDA(cudaMallocAsync(&d_tmp, (size_t)t->W * 8 + 16, st));
   QCB_CUDA(cudaMallocAsync(&d_tmpph, 16, st));
+  if (qubits) {
+    QCB_CUDA(cudaMallocAsync(&d_q, (size_t)k * 4, st));
+    QCB_CUDA(cudaMemcpyAsync(d_q, q0.data(), (size_t)k * 4, cudaMemcpyHostToDevice, st));
+  }
+  if (rand_host) {
+    QCB_CUDA(cudaMallocAsync(&d_rand, k, st));
+    QCB_CUDA(cudaMemcpyAsync(d_rand, rand_host, k, cudaMemcpyHostToDevice, st));
+  }
   int32_t rank = mixed ? *rank_io : 0;
   QCB_CUDA(cudaMemcpyAsync(d_rank, &rank, 4, cudaMemcpyHostToDevice, st));
 
@@ -325,9 +388,10 @@ int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* p
   while (j0 < k) {
     ProjArgs a{};
     a.xzs = t->xzs; a.ph = t->phases; a.rows = t->rows; a.n = t->nqubits; a.W = t->W;
-    a.kind = kind; a.rank = d_rank; a.paulis = paulis->xzs; a.pph = paulis->phases;
+    a.kind = kind; a.rank = d_rank; a.paulis = pxzs; a.pph = pph;
     a.j0 = j0; a.k = k; a.keep_result = keep_result; a.phases = phases;
     a.anticom = d_anti; a.result = d_res; a.status = d_stat; a.flags = d_flags;
+    a.qubits = d_q; a.basis = basis; a.rand_ph = d_rand;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(cs);
     cfg.blockDim = dim3(PROJ_THREADS);
@@ -360,8 +424,16 @@ int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* p
     if (kind == QCB_MIXED_STABILIZER) QCB_CUDA(cudaMemcpy(&r_now, d_rank, 4, cudaMemcpyDeviceToHost));
     const uint32_t nr = kind == QCB_STABILIZER ? t->rows : (uint32_t)r_now;
     if (int s = canonicalize_view(t->xzs, t->phases, nr, t->nqubits, t->W, phases, d_cout, st)) { status = s; break; }
-    QCB_CUDA(cudaMemcpyAsync(d_tmp, paulis->xzs + (size_t)j * t->W, (size_t)t->W * 8, cudaMemcpyDeviceToDevice, st));
-    QCB_CUDA(cudaMemcpyAsync(d_tmpph, paulis->phases + j, 1, cudaMemcpyDeviceToDevice, st));
+    std::vector<uint64_t> hp;
+    const uint8_t zero = 0;
+    if (qubits) {
+      hp = single_pauli(j);
+      QCB_CUDA(cudaMemcpyAsync(d_tmp, hp.data(), (size_t)W * 8, cudaMemcpyHostToDevice, st));
+      QCB_CUDA(cudaMemcpyAsync(d_tmpph, &zero, 1, cudaMemcpyHostToDevice, st));
+    } else {
+      QCB_CUDA(cudaMemcpyAsync(d_tmp, pxzs + (size_t)j * W, (size_t)W * 8, cudaMemcpyDeviceToDevice, st));
+      QCB_CUDA(cudaMemcpyAsync(d_tmpph, pph + j, 1, cudaMemcpyDeviceToDevice, st));
+    }
     if (int s = generate_dev(d_tmp, d_tmpph, t->xzs, t->phases, nr, t->W, phases, d_cout + 2, nullptr, 0,
                              (uint32_t*)(d_cout + 3), st)) { status = s; break; }
     int32_t cout[4];
@@ -377,11 +449,22 @@ int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* p
       if (kind == QCB_MIXED_STABILIZER && anti == r_now + 1) {
         // ms.tab[rank+1] = pauli; rank += 1  (src/project_trace_reset.jl:310-317)
         if ((uint32_t)r_now >= t->rows) { status = fail(QCB_EBOUNDS, "MixedStabilizer tableau is full"); break; }
-        QCB_CUDA(cudaMemcpyAsync(t->xzs + (size_t)r_now * t->W, paulis->xzs + (size_t)j * t->W, (size_t)t->W * 8,
-                                 cudaMemcpyDeviceToDevice, st));
-        QCB_CUDA(cudaMemcpyAsync(t->phases + r_now, paulis->phases + j, 1, cudaMemcpyDeviceToDevice, st));
+        if (qubits) {
+          QCB_CUDA(cudaMemcpyAsync(t->xzs + (size_t)r_now * W, hp.data(), (size_t)W * 8, cudaMemcpyHostToDevice, st));
+          QCB_CUDA(cudaMemcpyAsync(t->phases + r_now, &zero, 1, cudaMemcpyHostToDevice, st));
+        } else {
+          QCB_CUDA(cudaMemcpyAsync(t->xzs + (size_t)r_now * W, pxzs + (size_t)j * W, (size_t)W * 8,
+                                   cudaMemcpyDeviceToDevice, st));
+          QCB_CUDA(cudaMemcpyAsync(t->phases + r_now, pph + j, 1, cudaMemcpyDeviceToDevice, st));
+        }
         r_now += 1;
         QCB_CUDA(cudaMemcpyAsync(d_rank, &r_now, 4, cudaMemcpyHostToDevice, st));
+      }
+      if (rand_host && anti > 0) {
+        // projectrand!: the new stabilizer row anti gets a random sign
+        if ((uint32_t)anti > t->rows) { status = fail(QCB_EBOUNDS, "projectrand!: no stabilizer row to randomize"); break; }
+        QCB_CUDA(cudaMemcpyAsync(t->phases + (anti - 1), rand_host + j, 1, cudaMemcpyHostToDevice, st));
+        res = rand_host[j];
       }
     }
     QCB_CUDA(cudaMemcpyAsync(d_anti + j, &anti, 4, cudaMemcpyHostToDevice, st));
@@ -402,8 +485,47 @@ int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* p
   cudaFreeAsync(d_anti, st); cudaFreeAsync(d_res, st); cudaFreeAsync(d_stat, st);
   cudaFreeAsync(d_rank, st); cudaFreeAsync(d_cout, st); cudaFreeAsync(d_flags, st);
   cudaFreeAsync(d_tmp, st); cudaFreeAsync(d_tmpph, st);
+  if (d_q) cudaFreeAsync(d_q, st);
+  if (d_rand) cudaFreeAsync(d_rand, st);
   cudaStreamSynchronize(st);
   return status;
+}
+
+int qcb_project(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* paulis, int keep_result,
+                int phases, int32_t* anticom, int32_t* result, uint32_t* n_done, void* stream) {
+  if (!t || !paulis) return fail(QCB_EARG, "null argument");
+  if (paulis->nqubits != t->nqubits) return fail(QCB_EDIM, "project!: the Pauli and the state act on different numbers of qubits");
+  return project_impl(t, kind, rank_io, paulis->xzs, paulis->phases, nullptr, 0, paulis->rows, keep_result, phases,
+                      nullptr, anticom, result, n_done, stream);
+}
+
+int qcb_project_qubit(qcb_tableau* t, int kind, int32_t* rank_io, uint32_t basis, const uint32_t* qubits, size_t k,
+                      int keep_result, int phases, int32_t* anticom, int32_t* result, uint32_t* n_done,
+                      void* stream) {
+  if (basis < 1 || basis > 3) return fail(QCB_EARG, "project: basis is 1 (X), 2 (Z) or 3 (Y)");
+  if (k && !qubits) return fail(QCB_EARG, "null argument");
+  if (k > 0xFFFFFFFFull) return fail(QCB_EARG, "too many projections");
+  return project_impl(t, kind, rank_io, nullptr, nullptr, qubits, basis, (uint32_t)k, keep_result, phases, nullptr,
+                      anticom, result, n_done, stream);
+}
+
+int qcb_projectrand(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tableau* paulis, uint32_t basis,
+                    const uint32_t* qubits, size_t k, const uint8_t* rand_phases, int32_t* anticom, int32_t* result,
+                    uint32_t* n_done, void* stream) {
+  if (!rand_phases) return fail(QCB_EARG, "null argument");
+  if (paulis) {
+    if (paulis->nqubits != t->nqubits) return fail(QCB_EDIM, "project!: the Pauli and the state act on different numbers of qubits");
+    for (uint32_t j = 0; j < paulis->rows; j++)
+      if (rand_phases[j] != 0 && rand_phases[j] != 2) return fail(QCB_EARG, "projectrand!: random phases are 0 or 2");
+    return project_impl(t, kind, rank_io, paulis->xzs, paulis->phases, nullptr, 0, paulis->rows, 1, 1, rand_phases,
+                        anticom, result, n_done, stream);
+  }
+  if (basis < 1 || basis > 3) return fail(QCB_EARG, "project: basis is 1 (X), 2 (Z) or 3 (Y)");
+  if (k && !qubits) return fail(QCB_EARG, "null argument");
+  for (size_t j = 0; j < k; j++)
+    if (rand_phases[j] != 0 && rand_phases[j] != 2) return fail(QCB_EARG, "projectrand!: random phases are 0 or 2");
+  return project_impl(t, kind, rank_io, nullptr, nullptr, qubits, basis, (uint32_t)k, 1, 1, rand_phases, anticom,
+                      result, n_done, stream);
 }
 
 }  // extern "C"

@@ -48,6 +48,34 @@ const OPC = Dict{DataType,UInt32}(
 _qcbops(op::AbstractSingleQubitOperator) = [QcbOp(OPC[typeof(op)], op.q, 0, 0, (0.0, 0.0, 0.0))]
 _qcbops(op::AbstractTwoQubitOperator) = [QcbOp(OPC[typeof(op)], op.q1, op.q2, 0, (0.0, 0.0, 0.0))]
 _qcbops(op::Union{sMZ,sMRZ,sMX,sMRX}) = [QcbOp(OPC[typeof(op)], op.qubit, 0, op.bit, (0.0, 0.0, 0.0))]
+# SingleQubitOperator: opcode 16, the six Bool fields as flag bits 0..5 of q2
+_qcbops(op::SingleQubitOperator) = [QcbOp(16, op.q, op.xx | op.xz << 1 | op.zx << 2 | op.zz << 3 | op.px << 4 | op.pz << 5,
+                                          0, (0.0, 0.0, 0.0))]
+# ClassicalXOR: one op 68 (q1 = number of bits, bit = store), then the bits three per op 69
+function _qcbops(op::ClassicalXOR)
+    b = collect(op.bits)
+    ops = [QcbOp(68, length(b), 0, op.store, (0.0, 0.0, 0.0))]
+    for i in 1:3:length(b)
+        c = vcat(b[i:min(i + 2, end)], zeros(Int, 3))
+        push!(ops, QcbOp(69, c[1], c[2], c[3], (0.0, 0.0, 0.0)))
+    end
+    ops
+end
+# PauliMeasurement on a frame (src/pauli_frames.jl:118-134): couple each
+# qubit onto the ancilla n+1, then sMRZ(n+1, bit); the sign's sX does not
+# change a frame
+function _qcbops(op::PauliMeasurement)
+    n = nqubits(op.pauli)
+    ops = QcbOp[]
+    for q in 1:n
+        x, z = op.pauli[q]
+        x && !z && push!(ops, QcbOp(40, q, n + 1, 0, (0.0, 0.0, 0.0)))
+        !x && z && push!(ops, QcbOp(32, q, n + 1, 0, (0.0, 0.0, 0.0)))
+        x && z && push!(ops, QcbOp(41, q, n + 1, 0, (0.0, 0.0, 0.0)))
+    end
+    push!(ops, QcbOp(65, n + 1, 0, op.bit, (0.0, 0.0, 0.0)))
+    ops
+end
 function _qcbops(op::NoiseOp)
     n = op.noise
     if n isa UnbiasedUncorrelatedNoise

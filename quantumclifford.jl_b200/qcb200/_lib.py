@@ -157,6 +157,14 @@ def lib():
         "qcb_comm": ([vp, u32, vp, u32, vp, vp], ctypes.c_int),
         "qcb_canonicalize": ([vp, u32, u32, ctypes.c_int, P(i32), P(i32), vp], ctypes.c_int),
         "qcb_project": ([vp, ctypes.c_int, P(i32), vp, ctypes.c_int, ctypes.c_int, vp, vp, P(u32), vp], ctypes.c_int),
+        "qcb_project_qubit": ([vp, ctypes.c_int, P(i32), u32, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, vp, vp,
+                               P(u32), vp], ctypes.c_int),
+        "qcb_projectrand": ([vp, ctypes.c_int, P(i32), vp, u32, vp, ctypes.c_size_t, vp, vp, vp, P(u32), vp],
+                            ctypes.c_int),
+        "qcb_canonicalize_state": ([vp, ctypes.c_int, i32, ctypes.c_int, P(i32), P(i32), vp], ctypes.c_int),
+        "qcb_canonicalize_rref": ([vp, ctypes.c_int, i32, vp, ctypes.c_size_t, ctypes.c_int, P(i32), vp], ctypes.c_int),
+        "qcb_canonicalize_gott": ([vp, ctypes.c_int, P(i32), P(i32), vp, vp, vp], ctypes.c_int),
+        "qcb_permutesystems": ([vp, vp, vp], ctypes.c_int),
         "qcb_generate": ([vp, vp, ctypes.c_int, P(i32), vp, u32, P(u32), vp], ctypes.c_int),
         "qcb_apply_gates": ([vp, vp, sz, ctypes.c_int, vp], ctypes.c_int),
         "qcb_apply_dense": ([vp, vp, ctypes.c_int, vp], ctypes.c_int),

@@ -290,23 +290,152 @@ def comm(l, r, i: int = 1, j: int = 1) -> int:
     return out.value
 
 
+def _kind_rank(state):
+    kind = KIND[state.kind if isinstance(state, Stabilizer) else "Stabilizer"]
+    rank = state.rank if getattr(state, "rank", None) is not None else 0
+    return kind, rank
+
+
 def canonicalize_(state, *, phases: bool = True, ranks: bool = False):
-    """canonicalize!(state; phases, ranks) (src/canonicalization.jl:92-133) on
-    the stabilizer view of a device state."""
-    t = _tab(state)
-    dev = t._need_dev()
-    rows = len(t)
-    row0 = 1
-    if isinstance(state, (Destabilizer, MixedDestabilizer)):
-        n = rows // 2
-        row0, rows = n + 1, (state.rank if isinstance(state, MixedDestabilizer) else n)
-    elif isinstance(state, MixedStabilizer):
-        rows = state.rank
+    """canonicalize!(state; phases, ranks) (src/canonicalization.jl:92-133) on a
+    device state; the Destabilizer kinds carry their destabilizer rows along
+    (rowswap!/mul_left! on the state)."""
+    dev = _tab(state)._need_dev()
+    kind, rank = _kind_rank(state)
     rx, rz = ctypes.c_int32(), ctypes.c_int32()
-    check(lib().qcb_canonicalize(dev.handle, row0, rows, int(phases), ctypes.byref(rx), ctypes.byref(rz), None))
+    check(lib().qcb_canonicalize_state(dev.handle, kind, rank, int(phases), ctypes.byref(rx), ctypes.byref(rz), None))
     if ranks:
         return state, rx.value, rz.value
     return state
+
+
+def canonicalize_rref_(state, colindices=None, *, phases: bool = True):
+    """canonicalize_rref!(state[, colindices]; phases) (src/canonicalization.jl
+    :150-185).  Returns (state, i) with the reference's 1-based index i."""
+    dev = _tab(state)._need_dev()
+    kind, rank = _kind_rank(state)
+    if colindices is None:
+        colindices = range(1, state.nqubits + 1)
+    cols = np.ascontiguousarray(np.asarray(list(colindices), dtype=np.int64).astype(np.uint32))
+    i = ctypes.c_int32()
+    check(lib().qcb_canonicalize_rref(dev.handle, kind, rank, ptr(cols) if len(cols) else None, len(cols), int(phases),
+                                      ctypes.byref(i), None))
+    return state, i.value
+
+
+def canonicalize_gott_(stabilizer, *, phases: bool = True):
+    """canonicalize_gott!(stabilizer; phases) (src/canonicalization.jl:206-272).
+    Returns (stabilizer, r, s, xperm, zperm), permutations 1-based."""
+    if isinstance(stabilizer, Stabilizer) and stabilizer.kind != "Stabilizer":
+        raise TypeError("canonicalize_gott! takes a Stabilizer")
+    t = _tab(stabilizer)
+    dev = t._need_dev()
+    n = t.nqubits
+    r, sz = ctypes.c_int32(), ctypes.c_int32()
+    xp = np.zeros(max(n, 1), np.uint32)
+    zp = np.zeros(max(n, 1), np.uint32)
+    check(lib().qcb_canonicalize_gott(dev.handle, int(phases), ctypes.byref(r), ctypes.byref(sz), ptr(xp), ptr(zp),
+                                      None))
+    return stabilizer, r.value, sz.value, xp[:n].astype(np.int64), zp[:n].astype(np.int64)
+
+
+def permutesystems_(state, perm):
+    """permutesystems!(state, perm) (src/linalg.jl:7-17): qubit j of the result
+    is qubit perm[j] (1-based) of the input."""
+    dev = _tab(state)._need_dev()
+    p = np.ascontiguousarray(np.asarray(perm, dtype=np.int64).astype(np.uint32))
+    if len(p) != state.nqubits:
+        raise ValueError("permutesystems!: the permutation needs one entry per qubit")
+    check(lib().qcb_permutesystems(dev.handle, ptr(p) if len(p) else None, None))
+    return state
+
+
+_BASIS = {"X": 1, "Z": 2, "Y": 3}
+
+
+def _project_qubit(state, basis, qubit, keep_result, phases):
+    dev = _tab(state)._need_dev()
+    kind, rank0 = _kind_rank(state)
+    single = np.isscalar(qubit)
+    qs = np.ascontiguousarray(np.atleast_1d(np.asarray(qubit, dtype=np.int64)).astype(np.uint32))
+    k = len(qs)
+    rank = ctypes.c_int32(rank0)
+    anti = np.zeros(max(k, 1), dtype=np.int32)
+    res = np.zeros(max(k, 1), dtype=np.int32)
+    done = ctypes.c_uint32()
+    check(lib().qcb_project_qubit(dev.handle, kind, ctypes.byref(rank), _BASIS[basis], ptr(qs) if k else None, k,
+                                  int(keep_result), int(phases), ptr(anti), ptr(res), ctypes.byref(done), None))
+    if isinstance(state, (MixedStabilizer, MixedDestabilizer)):
+        state.rank = rank.value
+    results = [None if v < 0 else int(v) for v in res[:k]]
+    if single:
+        return state, int(anti[0]), results[0]
+    return state, [int(a) for a in anti[:k]], results
+
+
+def projectX_(state, qubit, *, keep_result: bool = True, phases: bool = True):
+    """projectX!(state, qubit) (src/project_trace_reset.jl:446-452); ``qubit``
+    may be a sequence (projected in order, one launch)."""
+    return _project_qubit(state, "X", qubit, keep_result, phases)
+
+
+def projectZ_(state, qubit, *, keep_result: bool = True, phases: bool = True):
+    """projectZ!(state, qubit) (src/project_trace_reset.jl:460-466)."""
+    return _project_qubit(state, "Z", qubit, keep_result, phases)
+
+
+def projectY_(state, qubit, *, keep_result: bool = True, phases: bool = True):
+    """projectY!(state, qubit) (src/project_trace_reset.jl:474-480)."""
+    return _project_qubit(state, "Y", qubit, keep_result, phases)
+
+
+def _projectrand(state, paulis, basis, qubit, rng):
+    dev = _tab(state)._need_dev()
+    kind, rank0 = _kind_rank(state)
+    rng = rng if rng is not None else np.random.default_rng()
+    if paulis is not None:
+        single = isinstance(paulis, PauliOperator)
+        pt = _tab(paulis)
+        if pt.dev is None:
+            pt.to_gpu()
+        k, qs, ph = len(pt), None, pt.dev.handle
+    else:
+        single = np.isscalar(qubit)
+        qs = np.ascontiguousarray(np.atleast_1d(np.asarray(qubit, dtype=np.int64)).astype(np.uint32))
+        k, ph = len(qs), None
+    rp = (2 * rng.integers(0, 2, size=max(k, 1))).astype(np.uint8)  # rand((0x0, 0x2))
+    rank = ctypes.c_int32(rank0)
+    anti = np.zeros(max(k, 1), dtype=np.int32)
+    res = np.zeros(max(k, 1), dtype=np.int32)
+    done = ctypes.c_uint32()
+    check(lib().qcb_projectrand(dev.handle, kind, ctypes.byref(rank), ph, _BASIS.get(basis, 0),
+                                ptr(qs) if qs is not None and k else None, k, ptr(rp), ptr(anti), ptr(res),
+                                ctypes.byref(done), None))
+    if isinstance(state, (MixedStabilizer, MixedDestabilizer)):
+        state.rank = rank.value
+    results = [int(v) for v in res[:k]]
+    return (state, results[0]) if single else (state, results)
+
+
+def projectrand_(state, pauli, *, rng=None):
+    """projectrand!(state, pauli) (src/project_trace_reset.jl:627-631): returns
+    (state, result) with an undetermined outcome drawn from {0x0, 0x2}."""
+    return _projectrand(state, pauli, None, None, rng)
+
+
+def projectXrand_(state, qubit, *, rng=None):
+    """projectXrand!(state, qubit) (src/project_trace_reset.jl:583-587)."""
+    return _projectrand(state, None, "X", qubit, rng)
+
+
+def projectZrand_(state, qubit, *, rng=None):
+    """projectZrand!(state, qubit) (src/project_trace_reset.jl:598-602)."""
+    return _projectrand(state, None, "Z", qubit, rng)
+
+
+def projectYrand_(state, qubit, *, rng=None):
+    """projectYrand!(state, qubit) (src/project_trace_reset.jl:613-617)."""
+    return _projectrand(state, None, "Y", qubit, rng)
 
 
 def project_(state, paulis, *, keep_result: bool = True, phases: bool = True):

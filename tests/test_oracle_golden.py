@@ -346,3 +346,155 @@ def test_frame_reset_semantics(orc):
     assert m[:, 0].all() and not m[:, 1].any()
     # after sMX the H stays applied: x moved to z
     assert np.all(xzs[1] & np.uint64(1)) and not np.any(xzs[0] & np.uint64(1))
+
+
+# ------------------------------------------------------------------ state kinds, rref, gott, projectX/Y/Z
+def random_mixed_destabilizer_tab(r, n, rng):
+    """A random valid MixedDestabilizer tableau of rank r (one(MixedDestabilizer,
+    r, n) under a random Clifford circuit): rows 0..n-1 destabilizers then
+    logical X, rows n..2n-1 stabilizers then logical Z."""
+    import oracle
+
+    d = one_destabilizer(n)
+    ops = O.to_array(random_clifford_ops(n, max(4, n // 2), rng))
+    return oracle.apply_gates(d.tab.phases, d.tab.xzs, n, ops)
+
+
+def symplectic_ok(xzs, n, r=None):
+    """The pairing checks of destab_looks_good / mixed_destab_looks_good
+    (src/misc.jl): rows i and n+j anticommute iff i == j, all other pairs
+    commute."""
+    import oracle
+
+    rows = xzs.shape[0]
+    for i in range(rows):
+        for j in range(i + 1, rows):
+            want = 1 if (rows == 2 * n and j == i + n) else 0
+            if oracle.comm(xzs[i], xzs[j]) != want:
+                return False
+    return True
+
+
+def stab_commutes(xzs):
+    import oracle
+
+    return all(oracle.comm(xzs[i], xzs[j]) == 0 for i in range(len(xzs)) for j in range(i + 1, len(xzs)))
+
+
+@pytest.mark.parametrize("n", [1, 3, 10, 64, 65, 100])
+@pytest.mark.parametrize("phases", [True, False])
+def test_canonicalize_state_kinds_agree(orc, n, phases):
+    # test/test_stabcanon.jl:44-72: canonicalize! and canonicalize_rref! give the
+    # same stabilizer view for Stabilizer, MixedStabilizer, Destabilizer and
+    # MixedDestabilizer, and the destabilizer kinds stay well formed
+    rng = np.random.default_rng(500 + n)
+    for r in sorted({n, max(1, n // 3), max(1, 2 * n // 3)}):
+        ph, xz = random_mixed_destabilizer_tab(r, n, rng)
+        sv = slice(n, n + r)
+        c_ph, c_xz, rx, rz = orc.canonicalize(ph[sv], xz[sv], n, phases)
+        kinds = [("MixedDestabilizer", ph, xz, r), ("MixedStabilizer", ph[sv], xz[sv], r)]
+        if r == n:
+            kinds += [("Destabilizer", ph, xz, 0), ("Stabilizer", ph[sv], xz[sv], 0)]
+        for kind, p0, x0, rank in kinds:
+            p1, x1, rx1, rz1 = orc.canonicalize_state(kind, p0, x0, n, rank, phases)
+            off = n if "Destabilizer" in kind else 0
+            assert np.array_equal(x1[off:off + r], c_xz) and (rx1, rz1) == (rx, rz), kind
+            if phases:
+                assert np.array_equal(p1[off:off + r], c_ph), kind
+            if "Destabilizer" in kind:
+                assert symplectic_ok(x1, n), kind
+            cols = np.arange(1, n + 1)
+            q1, y1, i1 = orc.canonicalize_rref(kind, p0, x0, n, cols, rank, phases)
+            if kind == "MixedDestabilizer":
+                want_view = y1[n:n + r].copy()
+                want_i = i1
+            else:
+                assert np.array_equal(y1[off:off + r], want_view) and i1 == want_i, kind
+            if "Destabilizer" in kind:
+                assert symplectic_ok(y1, n), kind
+            # canonicalize!(canonicalize_rref!(s)) == canonicalize!(s)
+            # (test/test_stabcanon.jl:76-87)
+            z_ph, z_xz, _, _ = orc.canonicalize(q1[off:off + r], y1[off:off + r], n, phases)
+            assert np.array_equal(z_xz, c_xz), kind
+
+
+def test_canonicalize_rref_partial_columns(orc):
+    # canonicalize_rref!(state, colindices) on a subset, as traceout! uses it
+    # (src/project_trace_reset.jl:643-660): pivots only in those columns, the
+    # rows below the returned i are free of them
+    rng = np.random.default_rng(7)
+    n = 12
+    ph, xz = random_mixed_destabilizer_tab(n, n, rng)
+    cols = [3, 7, 8, 12]
+    p1, x1, i = orc.canonicalize_rref("Stabilizer", ph[n:], xz[n:], n, cols)
+    assert n - 2 * len(cols) <= i <= n  # the reference's `i`: rows i+1..n hold the pivots
+    W = xz.shape[1]
+    for row in range(i):  # rows 1..i (1-based) have no X or Z on the columns
+        for c in cols:
+            q = c - 1
+            assert not (x1[row, q >> 6] >> np.uint64(q & 63)) & np.uint64(1)
+            assert not (x1[row, W // 2 + (q >> 6)] >> np.uint64(q & 63)) & np.uint64(1)
+    assert stab_commutes(x1)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 10, 63, 64, 65, 100])
+def test_canonicalize_gott_invariants(orc, n):
+    # test/test_stabcanon.jl:31-43: canonicalize!(permute(permute(s, p1), p2)) ==
+    # canonicalize!(gott(s)), the result still a stabilizer; plus the standard
+    # form it is named for (identity blocks in the X then Z pivot columns)
+    rng = np.random.default_rng(900 + n)
+    for rows in sorted({n, max(1, n // 3), max(1, 2 * n // 3)}):
+        ph, xz = random_mixed_destabilizer_tab(rows, n, rng)
+        s_ph, s_xz = ph[n:n + rows], xz[n:n + rows]
+        g_ph, g_xz, r, s, xp, zp = orc.canonicalize_gott(s_ph, s_xz, n)
+        assert sorted(xp) == list(range(1, n + 1)) and sorted(zp) == list(range(1, n + 1))
+        p = orc.permutesystems(orc.permutesystems(s_xz, n, xp), n, zp)
+        _, c1, _, _ = orc.canonicalize(s_ph, p, n)
+        _, cg, _, _ = orc.canonicalize(g_ph, g_xz, n)
+        assert np.array_equal(c1, cg)
+        assert stab_commutes(g_xz)
+        assert r + s <= rows
+        W = xz.shape[1]
+        bit = lambda row, half, q: int((g_xz[row, half * (W // 2) + (q >> 6)] >> np.uint64(q & 63)) & np.uint64(1))
+        for a in range(r):
+            assert [bit(a, 0, q) for q in range(r)] == [int(q == a) for q in range(r)]
+        for a in range(s):
+            assert [bit(r + a, 1, q) for q in range(r, r + s)] == [int(q == a) for q in range(s)]
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 10, 64, 65, 100])
+@pytest.mark.parametrize("phases", [True, False])
+def test_project_xyz_equals_project_single_pauli(orc, n, phases):
+    # test/test_projections.jl:291-317: project!(s, single_x(n, r)) ==
+    # projectX!(s, r) (and Y, Z) on MixedDestabilizer(random_destabilizer(n), n÷2),
+    # also after a first projection, with keep_result both ways
+    rng = np.random.default_rng(1300 + n)
+    W = nwords(n)
+    for trial in range(4):
+        rank = max(0, n // 2) if trial < 2 else n
+        ph, xz = random_mixed_destabilizer_tab(rank, n, rng)
+        for step in range(3):
+            q = int(rng.integers(1, n + 1))
+            basis = int(rng.integers(1, 4))
+            keep = bool(rng.integers(2)) if trial % 2 else True
+            p = np.zeros(W, np.uint64)
+            if basis & 1:
+                p[(q - 1) >> 6] |= np.uint64(1) << np.uint64((q - 1) & 63)
+            if basis & 2:
+                p[W // 2 + ((q - 1) >> 6)] |= np.uint64(1) << np.uint64((q - 1) & 63)
+            st, ph1, xz1, r1, a1, res1 = orc.project("MixedDestabilizer", ph, xz, n, p, 0, rank, keep, phases)
+            ph2, xz2, r2, a2, res2 = orc.project_cond(ph, xz, n, rank, q, basis, keep, phases)
+            assert st == 0
+            assert (r1, a1, res1) == (r2, a2, res2)
+            assert np.array_equal(xz1, xz2) and np.array_equal(ph1, ph2)
+            ph, xz, rank = ph2, xz2, r2
+
+
+def test_project_xyz_known_answers(orc):
+    # test/test_projections.jl:349-370: on S"XII -IZI IIY" the single-qubit
+    # projections agree with project! of the Pauli: X1 -> 0x0, Z2 -> 0x2, Y3 -> 0x0
+    # (destabilizers Z1, X2, Z3 pair with the three stabilizers)
+    t = T("+Z__ +_X_ +__Z +X__ -_Z_ +__Y")
+    for q, basis, want in [(1, 1, 0), (2, 2, 2), (3, 3, 0)]:
+        _, _, rank, a, res = orc.project_cond(t.phases, t.xzs, 3, 3, q, basis)
+        assert (rank, a, res) == (3, 0, want)

@@ -9,8 +9,11 @@ module QuantumCliffordB200Ext
 
 using QuantumClifford
 import QuantumClifford: apply!, pftrajectories, mul_left!, canonicalize!, project!,
+    canonicalize_rref!, canonicalize_gott!, permutesystems!, projectX!, projectY!, projectZ!,
+    projectXrand!, projectYrand!, projectZrand!,
     measurements, PauliFrame, Stabilizer, MixedDestabilizer, Destabilizer, MixedStabilizer,
-    PauliOperator, Tableau, nqubits, tab, CliffordOperator, AbstractOperation
+    PauliOperator, Tableau, nqubits, tab, CliffordOperator, AbstractOperation,
+    SingleQubitOperator, ClassicalXOR, PauliMeasurement
 
 const libqcb = get(ENV, "QCB200_LIB", joinpath(@__DIR__, "..", "lib", "libqcb200.so"))
 
@@ -227,16 +230,79 @@ function mul_left!(r::B200State{<:PauliOperator}, l::B200State{<:PauliOperator};
     r
 end
 
+_rank(h) = h isa Union{MixedStabilizer,MixedDestabilizer} ? Int32(h.rank) : Int32(0)
+
+# canonicalize! on the whole state: the Destabilizer kinds carry their
+# destabilizer rows through the row swaps and products
 function canonicalize!(s::B200State; phases::Bool=true, ranks::Bool=false)
     h = s.host
-    n = nqubits(h)
-    row0, rows = h isa Union{Destabilizer,MixedDestabilizer} ? (n + 1, h isa MixedDestabilizer ? h.rank : n) :
-                 (1, h isa MixedStabilizer ? h.rank : length(tab(h)))
     rx, rz = Ref{Int32}(0), Ref{Int32}(0)
-    _check(ccall((:qcb_canonicalize, libqcb), Cint, (Ptr{Cvoid}, UInt32, UInt32, Cint, Ref{Int32}, Ref{Int32}, Ptr{Cvoid}),
-                 s.dev.handle, row0, rows, phases, rx, rz, C_NULL))
+    _check(ccall((:qcb_canonicalize_state, libqcb), Cint, (Ptr{Cvoid}, Cint, Int32, Cint, Ref{Int32}, Ref{Int32}, Ptr{Cvoid}),
+                 s.dev.handle, _kind(h), _rank(h), phases, rx, rz, C_NULL))
     ranks ? (s, Int(rx[]), Int(rz[])) : s
 end
+
+function canonicalize_rref!(s::B200State, colindices; phases::Bool=true)
+    h = s.host
+    cols = UInt32.(collect(colindices))
+    i = Ref{Int32}(0)
+    _check(ccall((:qcb_canonicalize_rref, libqcb), Cint,
+                 (Ptr{Cvoid}, Cint, Int32, Ptr{UInt32}, Csize_t, Cint, Ref{Int32}, Ptr{Cvoid}),
+                 s.dev.handle, _kind(h), _rank(h), cols, length(cols), phases, i, C_NULL))
+    s, Int(i[])
+end
+canonicalize_rref!(s::B200State; phases::Bool=true) = canonicalize_rref!(s, 1:nqubits(s.host); phases)
+
+function canonicalize_gott!(s::B200State{<:Stabilizer}; phases::Bool=true)
+    n = nqubits(s.host)
+    r, sz = Ref{Int32}(0), Ref{Int32}(0)
+    xperm, zperm = Vector{UInt32}(undef, n), Vector{UInt32}(undef, n)
+    _check(ccall((:qcb_canonicalize_gott, libqcb), Cint,
+                 (Ptr{Cvoid}, Cint, Ref{Int32}, Ref{Int32}, Ptr{UInt32}, Ptr{UInt32}, Ptr{Cvoid}),
+                 s.dev.handle, phases, r, sz, xperm, zperm, C_NULL))
+    s, Int(r[]), Int(sz[]), Int.(xperm), Int.(zperm)
+end
+
+function permutesystems!(s::B200State, perm::AbstractVector)
+    p = UInt32.(perm)
+    _check(ccall((:qcb_permutesystems, libqcb), Cint, (Ptr{Cvoid}, Ptr{UInt32}, Ptr{Cvoid}), s.dev.handle, p, C_NULL))
+    s
+end
+
+# projectX! / projectZ! / projectY!: basis 1 / 2 / 3
+function _project_qubit!(s::B200State, basis, qubit::Int; keep_result::Bool=true, phases::Bool=true)
+    h = s.host
+    rank = Ref{Int32}(_rank(h))
+    anti, res, done = Ref{Int32}(0), Ref{Int32}(0), Ref{UInt32}(0)
+    q = Ref{UInt32}(qubit)
+    _check(ccall((:qcb_project_qubit, libqcb), Cint,
+                 (Ptr{Cvoid}, Cint, Ref{Int32}, UInt32, Ref{UInt32}, Csize_t, Cint, Cint, Ref{Int32}, Ref{Int32},
+                  Ref{UInt32}, Ptr{Cvoid}),
+                 s.dev.handle, _kind(h), rank, basis, q, 1, keep_result, phases, anti, res, done, C_NULL))
+    h isa Union{MixedStabilizer,MixedDestabilizer} && (h.rank = rank[])
+    s, Int(anti[]), res[] < 0 ? nothing : UInt8(res[])
+end
+projectX!(s::B200State, qubit::Int; kw...) = _project_qubit!(s, 1, qubit; kw...)
+projectZ!(s::B200State, qubit::Int; kw...) = _project_qubit!(s, 2, qubit; kw...)
+projectY!(s::B200State, qubit::Int; kw...) = _project_qubit!(s, 3, qubit; kw...)
+
+# projectXrand! and friends: the undetermined sign comes from the task RNG,
+# drawn here and handed to the device
+function _projectrand!(s::B200State, basis, qubit::Int)
+    h = s.host
+    rank = Ref{Int32}(_rank(h))
+    anti, res, done = Ref{Int32}(0), Ref{Int32}(0), Ref{UInt32}(0)
+    q, rp = Ref{UInt32}(qubit), Ref{UInt8}(rand((0x0, 0x2)))
+    _check(ccall((:qcb_projectrand, libqcb), Cint,
+                 (Ptr{Cvoid}, Cint, Ref{Int32}, Ptr{Cvoid}, UInt32, Ref{UInt32}, Csize_t, Ref{UInt8}, Ref{Int32},
+                  Ref{Int32}, Ref{UInt32}, Ptr{Cvoid}),
+                 s.dev.handle, _kind(h), rank, C_NULL, basis, q, 1, rp, anti, res, done, C_NULL))
+    h isa Union{MixedStabilizer,MixedDestabilizer} && (h.rank = rank[])
+    s, UInt8(res[])
+end
+projectXrand!(s::B200State, qubit::Int) = _projectrand!(s, 1, qubit)
+projectZrand!(s::B200State, qubit::Int) = _projectrand!(s, 2, qubit)
+projectYrand!(s::B200State, qubit::Int) = _projectrand!(s, 3, qubit)
 
 function project!(s::B200State, p::B200State{<:PauliOperator}; keep_result::Bool=true, phases::Bool=true)
     h = s.host

@@ -197,6 +197,29 @@ int qcb_frame_download_record_planes(const qcb_frame* f, uint32_t* planes, void*
 /* x/z planes [qubits+1][ceil(frames/32)] uint32 each (device layout).      */
 int qcb_frame_download_planes(const qcb_frame* f, uint32_t* x_planes, uint32_t* z_planes, void* stream);
 
+/* The decoder hand-off (src/ecc/decoder_pipeline.jl:163-170).
+ * measurements(frame)[:, bits]: the record columns `bits` (1-based, nsel of
+ * them) as a Bool matrix S x nsel, column-major (the reference's view of the
+ * syndrome or logical bits).  `reference` (nbits Bools, may be NULL) is
+ * XORed in: measurements(register, frame) (src/pauli_frames.jl:289).       */
+int qcb_frame_measurement_columns(const qcb_frame* f, const uint32_t* bits, size_t nsel,
+                                  const uint8_t* reference, uint8_t* bools, void* stream);
+/* The syndrome matrix for a decoder, shot-major and bit-packed: shot s owns
+ * words out[s*W .. s*W+W-1], W = ceil(nsel/64), bit b of word w = record bit
+ * bits[64w+b] of shot s (zero past nsel).  out is device memory when
+ * out_on_device, else host memory (the call then synchronises).           */
+int qcb_frame_syndrome_rows(const qcb_frame* f, const uint32_t* bits, size_t nsel, uint64_t* out,
+                            int out_on_device, void* stream);
+/* evaluate_guesses(measured_faults, guesses, faults_matrix)
+ * (src/ecc/decoder_pipeline.jl:172-190) with measured_faults =
+ * measurements(frame)[:, logical_bits]: guesses is the decoder's Bool matrix
+ * S x k and faults the Bool matrix nlog x k, both column-major (host);
+ * *fails gets the number of failed shots (the reference returns
+ * fails / nsamples).                                                       */
+int qcb_evaluate_guesses(const qcb_frame* f, const uint32_t* logical_bits, size_t nlog,
+                         const uint8_t* guesses, size_t k, const uint8_t* faults, uint64_t* fails,
+                         void* stream);
+
 /* pftrajectories(circuit; trajectories) (src/pauli_frames.jl:193-227) as one
  * host call: fresh frame, Philox initZ!, run, record copied back as
  * shot-packed planes [nbits][ceil(frames/32)].  The frame is kept on the

@@ -445,6 +445,26 @@ int oracle_project(int kind, u64* xzs, u8* ph, size_t rows, u32 n, int* rank_io,
   return QCB_OK;
 }
 
+// evaluate_guesses (src/ecc/decoder_pipeline.jl:172-190): Bool matrices in
+// Julia's column-major layout: measured S x nlog, guesses S x k, faults
+// nlog x k.  Returns the number of failed samples.
+u64 oracle_evaluate_guesses(const u8* measured, const u8* guesses, const u8* faults, u64 S, size_t nlog,
+                            size_t k) {
+  u64 fails = 0;
+  for (u64 i = 0; i < S; i++) {
+    for (size_t j = 0; j < nlog; j++) {
+      unsigned sum_mod = 0;
+      for (size_t c = 0; c < k; c++) sum_mod += (unsigned)(faults[c * nlog + j] & 1u) * (guesses[c * S + i] & 1u);
+      sum_mod %= 2;
+      if (sum_mod != (unsigned)(measured[j * S + i] & 1u)) {
+        fails += 1;
+        break;
+      }
+    }
+  }
+  return fails;
+}
+
 // ---------------------------------------------------------------- states
 // The stabilizer view of a state is rows [off, off + rows) of its tableau;
 // the Destabilizer kinds pair stabilizer row off + i with destabilizer row i.

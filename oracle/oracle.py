@@ -56,6 +56,7 @@ def L():
             "oracle_frame_init_z": ([vp, u64, u32, vp, u64], None),
             "oracle_pftrajectories_philox": ([vp, vp, u64, u32, u32, vp, sz, u64, u64], None),
             "oracle_philox_init_z": ([vp, u64, u32, u64, u64], None),
+            "oracle_evaluate_guesses": ([vp, vp, vp, u64, sz, sz], u64),
             "oracle_canonicalize_state": ([i, vp, vp, sz, u32, i, i, P(ctypes.c_int), P(ctypes.c_int)], None),
             "oracle_canonicalize_rref": ([i, vp, vp, sz, u32, i, vp, sz, i], i),
             "oracle_permutesystems": ([vp, sz, u32, vp], None),
@@ -162,6 +163,17 @@ def project_cond(phases, xzs, n, rank, qubit, basis, keep_result=True, use_phase
     L().oracle_project_cond(_p(xz), _p(ph), len(ph), n, ctypes.byref(r), int(qubit), int(basis), int(keep_result),
                             int(use_phases), ctypes.byref(a), ctypes.byref(res))
     return ph, xz, r.value, a.value, res.value
+
+
+def evaluate_guesses(measured_faults, guesses, faults_matrix):
+    """evaluate_guesses: fails / nsamples, on Bool matrices (samples x nlog,
+    samples x k, nlog x k)."""
+    m = np.asfortranarray(measured_faults, dtype=np.uint8)
+    g = np.asfortranarray(guesses, dtype=np.uint8)
+    f = np.asfortranarray(faults_matrix, dtype=np.uint8)
+    S = g.shape[0]
+    fails = L().oracle_evaluate_guesses(m.ctypes.data, g.ctypes.data, f.ctypes.data, S, f.shape[0], f.shape[1])
+    return fails / S, int(fails)
 
 
 def generate(p_xz, p_ph, phases, xzs, n, use_phases=True):

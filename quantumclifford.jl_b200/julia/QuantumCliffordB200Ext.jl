@@ -155,6 +155,29 @@ function measurements(f::B200Frame)
     m
 end
 
+# The decoder hand-off (src/ecc/decoder_pipeline.jl:163-190): the syndrome
+# columns for batchdecode, and evaluate_guesses on the device
+function measurements(f::B200Frame, bits::AbstractVector{<:Integer})
+    b = UInt32.(bits)
+    m = Matrix{Bool}(undef, f.frames, length(b))
+    _check(ccall((:qcb_frame_measurement_columns, libqcb), Cint,
+                 (Ptr{Cvoid}, Ptr{UInt32}, Csize_t, Ptr{UInt8}, Ptr{Bool}, Ptr{Cvoid}),
+                 f.handle, b, length(b), C_NULL, m, C_NULL))
+    m
+end
+
+function evaluate_guesses(f::B200Frame, logical_bits::AbstractVector{<:Integer}, guesses::AbstractMatrix{Bool},
+                          faults_submatrix::AbstractMatrix)
+    lb = UInt32.(logical_bits)
+    g = Matrix{Bool}(guesses)
+    F = Matrix{Bool}(faults_submatrix .% 2 .== 1)
+    fails = Ref{UInt64}(0)
+    _check(ccall((:qcb_evaluate_guesses, libqcb), Cint,
+                 (Ptr{Cvoid}, Ptr{UInt32}, Csize_t, Ptr{Bool}, Csize_t, Ptr{Bool}, Ref{UInt64}, Ptr{Cvoid}),
+                 f.handle, lb, length(lb), g, size(g, 2), F, fails, C_NULL))
+    fails[] / f.frames
+end
+
 """The frame tableau back in the reference fastcolumn layout (UInt64)."""
 function QuantumClifford.PauliFrame(f::B200Frame)
     W = 2 * cld(f.qubits + 1, 64)

@@ -193,6 +193,30 @@ class PauliFrame:
         check(lib().qcb_frame_upload_xzs(self.handle, ptr(a), None))
         return self
 
+    def measurement_columns(self, bits, reference=None) -> np.ndarray:
+        """measurements(frame)[:, bits] (Bool, frames x len(bits)); with
+        ``reference`` (the Register's record, one Bool per bit) it is
+        measurements(register, frame)[:, bits] (src/pauli_frames.jl:289)."""
+        b = np.ascontiguousarray(np.asarray(bits, dtype=np.int64).astype(np.uint32))
+        out = np.empty((len(b), self.frames), dtype=np.uint8)  # column-major frames x nsel
+        ref = None if reference is None else np.ascontiguousarray(np.asarray(reference, dtype=np.uint8))
+        if ref is not None and len(ref) != self.nbits:
+            raise ValueError("reference needs one entry per record bit")
+        if out.size:
+            check(lib().qcb_frame_measurement_columns(self.handle, ptr(b), len(b), ptr(ref) if ref is not None else None,
+                                                      ptr(out), None))
+        return out.T.astype(bool)
+
+    def syndrome_rows(self, bits) -> np.ndarray:
+        """The syndrome matrix a decoder consumes, shot-major and bit-packed:
+        uint64 [frames, ceil(len(bits)/64)], bit b of word w = record bit
+        bits[64w+b] of that shot."""
+        b = np.ascontiguousarray(np.asarray(bits, dtype=np.int64).astype(np.uint32))
+        out = np.zeros((self.frames, (len(b) + 63) // 64), dtype=np.uint64)
+        if out.size:
+            check(lib().qcb_frame_syndrome_rows(self.handle, ptr(b), len(b), ptr(out), 0, None))
+        return out
+
     def apply(self, op, *, seed: int = 0, masks: Optional[Masks] = None):
         """apply!(frame, op) for one op or a short op list."""
         arr = _ops.to_array([op] if isinstance(op, _ops.Op) else op)
@@ -225,6 +249,24 @@ pauliframe_ = pftrajectories
 
 def measurements(frame: PauliFrame) -> np.ndarray:
     return frame.measurements()
+
+
+def evaluate_guesses(frame: PauliFrame, logical_bits, guesses, faults_submatrix) -> float:
+    """evaluate_guesses(measured_faults, guesses, faults_matrix)
+    (src/ecc/decoder_pipeline.jl:172-190) with measured_faults =
+    measurements(frame)[:, logical_bits], on the device: the fraction of
+    shots whose guessed faults, through the faults matrix, miss a measured
+    logical bit.  ``guesses``: Bool frames x k (a decoder's batchdecode
+    output); ``faults_submatrix``: Bool nlog x k."""
+    lb = np.ascontiguousarray(np.asarray(logical_bits, dtype=np.int64).astype(np.uint32))
+    g = np.asfortranarray(np.asarray(guesses, dtype=np.uint8))
+    f = np.asfortranarray(np.asarray(faults_submatrix, dtype=np.uint8))
+    if g.shape[0] != frame.frames or f.shape != (len(lb), g.shape[1]):
+        raise ValueError("guesses must be frames x k and the faults matrix len(logical_bits) x k")
+    fails = ctypes.c_uint64()
+    check(lib().qcb_evaluate_guesses(frame.handle, ptr(lb) if len(lb) else None, len(lb), g.ctypes.data if g.size else None,
+                                     g.shape[1], f.ctypes.data if f.size else None, ctypes.byref(fails), None))
+    return fails.value / frame.frames if frame.frames else 0.0
 
 
 def pftrajectories_record(circuit, trajectories: int, seed: int = 0, shot_offset: int = 0,

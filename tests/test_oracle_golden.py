@@ -498,3 +498,21 @@ def test_project_xyz_known_answers(orc):
     for q, basis, want in [(1, 1, 0), (2, 2, 2), (3, 3, 0)]:
         _, _, rank, a, res = orc.project_cond(t.phases, t.xzs, 3, 3, q, basis)
         assert (rank, a, res) == (3, 0, want)
+
+
+def test_evaluate_guesses_restatement(orc):
+    # src/ecc/decoder_pipeline.jl:172-190 on small matrices, against the
+    # definition: a sample fails when any row of faults . guess (mod 2)
+    # differs from the measured logical bit
+    rng = np.random.default_rng(4)
+    for S, nlog, k in [(1, 1, 1), (50, 2, 7), (300, 4, 30)]:
+        m = rng.random((S, nlog)) < 0.5
+        g = rng.random((S, k)) < 0.5
+        f = rng.random((nlog, k)) < 0.5
+        frac, cnt = orc.evaluate_guesses(m, g, f)
+        want = int(np.count_nonzero(((g.astype(int) @ f.T.astype(int)) % 2 != m).any(axis=1)))
+        assert cnt == want and frac == want / S
+    # a perfect decoder never fails
+    g = rng.random((40, 6)) < 0.5
+    f = rng.random((3, 6)) < 0.5
+    assert orc.evaluate_guesses((g.astype(int) @ f.T.astype(int)) % 2 == 1, g, f)[1] == 0

@@ -197,6 +197,37 @@ int qcb_frame_download_record_planes(const qcb_frame* f, uint32_t* planes, void*
 /* x/z planes [qubits+1][ceil(frames/32)] uint32 each (device layout).      */
 int qcb_frame_download_planes(const qcb_frame* f, uint32_t* x_planes, uint32_t* z_planes, void* stream);
 
+/* ------------------------------------------------------------ batches
+ * Many sampling jobs drained from one persistent launch (no reference
+ * counterpart: the reference runs one pftrajectories per circuit).  Each job
+ * is a fresh run (initZ! + circuit, Philox mode) of `program` on `frame`, so
+ * its record equals that of qcb_pftrajectories_fresh with the same seed and
+ * shot_offset.  The (job, shot-tile) items are queued longest first and taken
+ * by one CTA per SM.  qcb_batch_run only clears the queue head and launches:
+ * it can be captured in a CUDA graph.  Frames and programs must outlive the
+ * batch; the frame tile of every job must fit one CTA's shared memory.      */
+typedef struct qcb_batch_job {
+  qcb_frame* frame;
+  const qcb_program* program;
+  uint64_t seed;
+  uint64_t shot_offset;   /* a multiple of 1024                                */
+  uint32_t tile;          /* shot columns per tile (even, 16..256); 0 = tuned
+                             width of the job's size class, else the widest  */
+  uint32_t reserved;
+} qcb_batch_job;
+typedef struct qcb_batch qcb_batch;
+int qcb_batch_create(const qcb_batch_job* jobs, size_t n_jobs, qcb_batch** out);
+int qcb_batch_run(qcb_batch* b, void* stream);
+/* Synchronising check of every job's device status word (QCB_ETIMEOUT when a
+ * device-side wait expired).                                                */
+int qcb_batch_status(const qcb_batch* b);
+int qcb_batch_destroy(qcb_batch* b);
+/* The autotuner: times the candidate tile widths (16..256 columns) for
+ * `program` on a scratch frame of two full waves each and records the fastest
+ * per frame column for the program's size class (its touched qubits), which
+ * qcb_batch_create then uses.  Synchronises the device.                     */
+int qcb_tune_tile(const qcb_program* program, uint32_t* tile, float* us_per_column, void* stream);
+
 /* The decoder hand-off (src/ecc/decoder_pipeline.jl:163-170).
  * measurements(frame)[:, bits]: the record columns `bits` (1-based, nsel of
  * them) as a Bool matrix S x nsel, column-major (the reference's view of the

@@ -68,6 +68,10 @@ struct CanonArgs {
 
 constexpr uint32_t CANON_THREADS = 1024;
 
+// D: destabilizer rows ride along; DESC: pivots from the last row upwards
+// (canonicalize_rref!).  Compile-time so that canonicalize! runs the lean
+// instance.
+template <bool D, bool DESC>
 __global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a) {
   cg::cluster_group cl = cg::this_cluster();
   const uint32_t me = cl.block_rank();
@@ -76,7 +80,6 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a)
   const uint32_t W = a.W, len = W / 2, WS = W + 1;
   const uint32_t r0 = me * a.RB;
   const uint32_t nloc = r0 < a.rows ? min(a.RB, a.rows - r0) : 0u;
-  const bool D = a.dxzs != nullptr;
 
   extern __shared__ __align__(16) uint64_t smem[];
   uint64_t* piv = smem;                                               // W words
@@ -132,7 +135,7 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a)
     pend = false;
   };
 
-  const bool desc = a.mode == ELIM_RREF;
+  constexpr bool desc = DESC;
   const uint32_t nsteps = desc ? 2 * a.ncols
                                : (a.mode == ELIM_BOTH ? 2 * a.n : (a.mode == ELIM_X ? a.n : (a.n > a.c0 ? a.n - a.c0 : 0u)));
   int32_t i = desc ? (int32_t)a.rows - 1 : (int32_t)a.i0;  // next pivot position
@@ -162,7 +165,8 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a)
     uint32_t best = 0xFFFFFFFFu;
     for (uint32_t r = tid; r < nloc; r += blockDim.x) {
       const uint32_t p = pos[r];
-      if (p >= lo && p <= hi && (ROW(r)[wj] & bm)) best = min(best, p);
+      const bool in = desc ? p <= hi : p >= lo;  // the other end of the range is the tableau's
+      if (in && (ROW(r)[wj] & bm)) best = min(best, p);
     }
     best = __reduce_min_sync(0xFFFFFFFFu, best);
     if (lane == 0) red[warp] = best;
@@ -485,8 +489,11 @@ static int eliminate(const ElimSpec& e, cudaStream_t st) {
     QCB_CUDA(cudaMallocAsync(&a.gtmp, nout * e.W * 8, st));
     QCB_CUDA(cudaMallocAsync(&a.gtmp_ph, nout, st));
   }
-  QCB_CUDA(cudaFuncSetAttribute(canon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_bytes));
-  if (p.cs > 8) QCB_CUDA(cudaFuncSetAttribute(canon_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  void (*kern)(const CanonArgs) =
+      D ? (e.mode == ELIM_RREF ? canon_kernel<true, true> : canon_kernel<true, false>)
+        : (e.mode == ELIM_RREF ? canon_kernel<false, true> : canon_kernel<false, false>);
+  QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_bytes));
+  if (p.cs > 8) QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(p.cs);
   cfg.blockDim = dim3(g_canon_threads ? g_canon_threads : CANON_THREADS);
@@ -499,7 +506,7 @@ static int eliminate(const ElimSpec& e, cudaStream_t st) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  QCB_CUDA(cudaLaunchKernelEx(&cfg, canon_kernel, a));
+  QCB_CUDA(cudaLaunchKernelEx(&cfg, kern, a));
   QCB_LAUNCHED();
   if (!p.smem_rows) {
     QCB_CUDA(cudaMemcpyAsync(e.xzs, a.gtmp, (size_t)e.rows * e.W * 8, cudaMemcpyDeviceToDevice, st));

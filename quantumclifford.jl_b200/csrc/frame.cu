@@ -24,6 +24,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <unordered_map>
 
@@ -295,20 +297,308 @@ __device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<
 // ---------------------------------------------------------------- walker
 __device__ __forceinline__ uint2 xor2(uint2 a, uint2 b) { return make_uint2(a.x ^ b.x, a.y ^ b.y); }
 
-// One CTA owns a tile of T shot columns (T even; T x 32 shots) and runs the
-// whole program on it.  Thread (rr, cp) = (tid / TP, tid % TP), TP = T / 2,
+// One tile of T shot columns (T even; T x 32 shots) walked through the whole
+// program by one CTA.  Thread (rr, cp) = (tid / TP, tid % TP), TP = T / 2,
 // handles the column pair (2cp, 2cp + 1) -- one 64-bit shared-memory word per
 // plane, so each op's operand decode and address arithmetic serve two columns
 // -- and every R-th op of a segment; a warp covers consecutive pairs of one
 // op (broadcast operand reads from the staged window).  One barrier per
-// record orders the records.
-template <bool SMEM, bool PHILOX>
-__global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
-  extern __shared__ __align__(128) uint32_t sm[];
+// record orders the records.  The program arrives window by window in the
+// two staging buffers (window kwin in buffer kwin & 1); after each window
+// thread 0 calls issue(kwin + 2) for the window two ahead.  Returns false
+// when a staging wait gave up (the job's status word then holds
+// QCB_ETIMEOUT).
+template <bool SMEM, bool PHILOX, class Issue>
+__device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint32_t* win0, uint32_t* win1,
+                                          uint64_t* bars, uint64_t& kwin, Issue& issue, uint64_t tile) {
   const uint32_t tid = threadIdx.x, T = a.tile, TP = T / 2, R = blockDim.x / TP;
   const uint32_t cp = tid % TP, rr = tid / TP, cw = 2 * cp;  // cw: tile column of the pair
   const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
   const uint64_t pitch = a.pitch;
+  const uint64_t c0 = tile * T, cg = c0 + cw;  // the pair's first column in the frame
+  const bool act = rr < R && cg < a.ncols;
+  const bool two = cg + 1 < a.ncols;          // its second column exists
+  const uint64_t col = a.col0 + cg, col1 = col + 1;
+  const uint32_t clo = (uint32_t)col, chi = (uint32_t)(col >> 32);
+  const uint32_t clo1 = (uint32_t)col1, chi1 = (uint32_t)(col1 >> 32);
+  const Tile<SMEM> F{sm, a.planes, sm, pitch, T};
+
+  // ---- initial frame
+  if (a.fresh) {
+    for (uint32_t qb = rr; qb * 4 < a.nq1; qb += R) {
+      if (!act) break;
+      uint32_t o[4], u[4];
+      philox4x32_10(qb, clo, chi, TAG_INITZ, k0, k1, o);
+      philox4x32_10(qb, clo1, chi1, TAG_INITZ, k0, k1, u);
+#pragma unroll
+      for (uint32_t j = 0; j < 4; j++) {
+        const uint32_t q = qb * 4 + j;
+        if (q >= a.nq1) break;
+        const uint32_t s = (SMEM && q < a.qubit_slot_len) ? __ldg(a.qubit_slot + q) : BIT_NONE;
+        if (SMEM && s != BIT_NONE) {
+          *F.at2(2 * s, cw, cg) = make_uint2(0u, 0u);
+          *F.at2(2 * s + 1, cw, cg) = make_uint2(o[j], u[j]);
+        } else {
+          *(uint2*)(a.planes + (uint64_t)(2 * q) * pitch + cg) = make_uint2(0u, 0u);
+          *(uint2*)(a.planes + (uint64_t)(2 * q + 1) * pitch + cg) = make_uint2(o[j], u[j]);
+        }
+      }
+    }
+  } else if (SMEM) {
+    for (uint32_t s = rr; s < a.nslots; s += R) {
+      if (!act) break;
+      const uint32_t q = __ldg(a.slot_qubit + s);
+      *F.at2(2 * s, cw, cg) = *(const uint2*)(a.planes + (uint64_t)(2 * q) * pitch + cg);
+      *F.at2(2 * s + 1, cw, cg) = *(const uint2*)(a.planes + (uint64_t)(2 * q + 1) * pitch + cg);
+    }
+  }
+  // mask mode: the events of the pair's columns, [ep[h], ep[h + 1]) for column h
+  uint64_t ep[3] = {0, 0, 0};
+  if (!PHILOX && rr == 0 && act) {
+    ep[0] = a.ev_off[cg];
+    ep[1] = a.ev_off[cg + 1];
+    ep[2] = two ? a.ev_off[cg + 2] : ep[1];
+  }
+
+  // ---- the program, window by window
+  const uint32_t* wp = nullptr;
+  bool need_window = true;
+  bool done = false;
+  while (!done) {
+    if (need_window) {
+      const bool ok = mbar_wait(&bars[kwin & 1], (uint32_t)((kwin >> 1) & 1));
+      if (__syncthreads_or(!ok)) {  // every thread takes the same branch
+        if (tid == 0) atomicExch(a.err, QCB_ETIMEOUT);
+        return false;
+      }
+      wp = (kwin & 1) ? win1 : win0;
+      need_window = false;
+    }
+    __syncthreads();  // the tile init / the previous record is complete
+    const uint4 h = *(const uint4*)wp;
+    const uint32_t kind = h.x >> 24, cnt = h.x & 0xFFFFFFu;
+    const uint32_t* e = wp + 4;
+    switch (kind) {
+      case SEG_END:
+        done = true;
+        break;
+      case SEG_WIN:
+        break;
+      case SEG_CNOT: {
+        wp = e + ((cnt * 2 + 3) & ~3u);
+        if (!act) break;
+        const uint2* en = (const uint2*)e;
+        uint32_t j = rr;
+        for (; j + R < cnt; j += 2 * R) {
+          const uint2 o = en[j], u = en[j + R];
+          uint2 *pxc = F.at2(o.x & 0xFFFFu, cw, cg), *pzc = F.at2(o.x >> 16, cw, cg);
+          uint2 *pxt = F.at2(o.y & 0xFFFFu, cw, cg), *pzt = F.at2(o.y >> 16, cw, cg);
+          uint2 *qxc = F.at2(u.x & 0xFFFFu, cw, cg), *qzc = F.at2(u.x >> 16, cw, cg);
+          uint2 *qxt = F.at2(u.y & 0xFFFFu, cw, cg), *qzt = F.at2(u.y >> 16, cw, cg);
+          const uint2 xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
+          const uint2 yxc = *qxc, yzc = *qzc, yxt = *qxt, yzt = *qzt;
+          *pxt = xor2(xt, xc); *pzc = xor2(zc, zt);
+          *qxt = xor2(yxt, yxc); *qzc = xor2(yzc, yzt);
+        }
+        for (; j < cnt; j += R) {
+          const uint2 o = en[j];
+          uint2 *pxc = F.at2(o.x & 0xFFFFu, cw, cg), *pzc = F.at2(o.x >> 16, cw, cg);
+          uint2 *pxt = F.at2(o.y & 0xFFFFu, cw, cg), *pzt = F.at2(o.y >> 16, cw, cg);
+          const uint2 xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
+          *pxt = xor2(xt, xc); *pzc = xor2(zc, zt);
+        }
+        break;
+      }
+      case SEG_CZ: {
+        wp = e + ((cnt * 2 + 3) & ~3u);
+        if (!act) break;
+        const uint2* en = (const uint2*)e;
+        for (uint32_t j = rr; j < cnt; j += R) {
+          const uint2 o = en[j];
+          uint2 *pxa = F.at2(o.x & 0xFFFFu, cw, cg), *pza = F.at2(o.x >> 16, cw, cg);
+          uint2 *pxb = F.at2(o.y & 0xFFFFu, cw, cg), *pzb = F.at2(o.y >> 16, cw, cg);
+          const uint2 xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
+          *pza = xor2(za, xb); *pzb = xor2(zb, xa);
+        }
+        break;
+      }
+      case SEG_S:
+      case SEG_G1: {
+        wp = e + ((cnt * 2 + 3) & ~3u);
+        if (!act) break;
+        const uint2* en = (const uint2*)e;
+        for (uint32_t j = rr; j < cnt; j += R) {
+          const uint2 o = en[j];
+          uint2 *px = F.at2(o.x & 0xFFFFu, cw, cg), *pz = F.at2(o.x >> 16, cw, cg);
+          uint2 x = *px, z = *pz;
+          if (kind == SEG_S) {
+            z = xor2(z, x);
+          } else {
+            gate1_xz(o.y, x.x, z.x);
+            gate1_xz(o.y, x.y, z.y);
+          }
+          *px = x; *pz = z;
+        }
+        break;
+      }
+      case SEG_G2: {
+        wp = e + cnt * 4;
+        if (!act) break;
+        const uint4* en = (const uint4*)e;
+        for (uint32_t j = rr; j < cnt; j += R) {
+          const uint4 o = en[j];
+          uint2 *pxa = F.at2(o.x & 0xFFFFu, cw, cg), *pza = F.at2(o.x >> 16, cw, cg);
+          uint2 *pxb = F.at2(o.y & 0xFFFFu, cw, cg), *pzb = F.at2(o.y >> 16, cw, cg);
+          uint2 xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
+          gate2_xz(o.z, xa.x, za.x, xb.x, zb.x);
+          gate2_xz(o.z, xa.y, za.y, xb.y, zb.y);
+          *pxa = xa; *pza = za; *pxb = xb; *pzb = zb;
+        }
+        break;
+      }
+      case SEG_MZ: {
+        wp = e + ((cnt * 2 + 3) & ~3u);
+        if (!act) break;
+        const uint2* en = (const uint2*)e;
+        for (uint32_t j = rr; j < cnt; j += R) {
+          const uint2 o = en[j];
+          *(uint2*)(a.rec + (uint64_t)o.y * pitch + cg) = *F.at2(o.x, cw, cg);
+        }
+        break;
+      }
+      case SEG_MRZ: {
+        wp = e + cnt * 16;
+        if (!act) break;
+        const uint4* en = (const uint4*)e;
+        for (uint32_t g = rr; g < cnt; g += R) {
+          uint4 ent[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) ent[i] = en[4 * g + i];
+          uint32_t o[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
+          if (PHILOX) {
+            uint32_t blk = 0;
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+              if (ent[i].z != MRZ_PAD) blk = ent[i].z >> 2;
+            philox4x32_10(blk, clo, chi, TAG_RESET, k0, k1, o);
+            philox4x32_10(blk, clo1, chi1, TAG_RESET, k0, k1, u);
+          }
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            if (ent[i].z == MRZ_PAD) continue;
+            uint2* px = F.at2(ent[i].x & 0xFFFFu, cw, cg);
+            uint2* pz = F.at2(ent[i].x >> 16, cw, cg);
+            const uint2 x = *px, z = *pz;
+            uint2 rb = make_uint2(o[i], u[i]);
+            if (!PHILOX) {
+              const uint32_t* rp = a.reset_planes + (uint64_t)ent[i].z * a.reset_pitch + cg;
+              rb = a.reset_planes ? make_uint2(__ldg(rp), two ? __ldg(rp + 1) : 0u) : make_uint2(0u, 0u);
+            }
+            if (ent[i].y != BIT_NONE) *(uint2*)(a.rec + (uint64_t)ent[i].y * pitch + cg) = x;
+            *px = make_uint2(0u, 0u);
+            *pz = xor2(z, rb);
+          }
+        }
+        break;
+      }
+      case SEG_XOR: {
+        wp = e + cnt * 32;
+        if (!act) break;
+        for (uint32_t j = rr; j < cnt; j += R) {
+          const uint32_t* x = e + 32 * j;  // (store, n, b_0 .. b_{n-1})
+          const uint32_t n = min(x[1], XOR_MAX_BITS);
+          uint2 v = make_uint2(0u, 0u);
+          for (uint32_t i = 0; i < n; i++) v = xor2(v, *(const uint2*)(a.rec + (uint64_t)x[2 + i] * pitch + cg));
+          *(uint2*)(a.rec + (uint64_t)x[0] * pitch + cg) = v;
+        }
+        break;
+      }
+      case SEG_FLUSH: {
+        wp = e + cnt * 4;
+        const uint4* en = (const uint4*)e;
+        if (PHILOX) {
+          if (a.pmax > 0.0) {
+            // (site, shot group) tasks over all threads of the CTA; a group
+            // is 32 run columns and may straddle the tile's edges
+            const uint64_t gc0 = a.col0 + c0;
+            const uint64_t gc1 = a.col0 + min(c0 + T, a.ncols);
+            const uint64_t G0 = gc0 / 32;
+            const uint32_t ng = (uint32_t)((gc1 - 1) / 32 - G0 + 1);
+            const uint32_t ntask = cnt * ng;
+            for (uint32_t t = tid; t < ntask; t += blockDim.x) {
+              const uint32_t i = t / ng, gl = t - i * ng;
+              const int32_t lc0 = (int32_t)((int64_t)((G0 + gl) * 32) - (int64_t)gc0);
+              sample_site_group<SMEM>(a, F, en[i], G0 + gl, lc0, c0);
+            }
+          }
+        } else if (rr == 0 && act) {
+          // each column's events are sorted by trial (site*32 + lane)
+          for (uint32_t hc = 0; hc < 2; hc++) {
+            const uint64_t eb = ep[hc], ee = ep[hc + 1];
+            if (eb == ee) continue;
+            for (uint32_t i = 0; i < cnt; i++) {
+              const uint4 st = en[i];
+              const uint64_t lo_t = (uint64_t)st.x * 32u, lim = lo_t + 32u;
+              uint64_t lo = eb, hi = ee;
+              while (lo < hi) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if ((__ldg(a.ev_data + mid) >> 8) < lo_t) lo = mid + 1;
+                else hi = mid;
+              }
+              for (uint64_t k = lo; k < ee; k++) {
+                const uint64_t d = __ldg(a.ev_data + k);
+                const uint64_t t = d >> 8;
+                if (t >= lim) break;
+                const uint32_t code = (uint32_t)(d & 0xFF), bit = 1u << (t & 31);
+                if (code & 1) *F.at32(st.z & 0xFFFFu, cw + hc, cg + hc) ^= bit;
+                if (code & 2) *F.at32(st.z >> 16, cw + hc, cg + hc) ^= bit;
+                if ((st.y & 0xFFu) == QCB_OP_DEPOL2) {
+                  if (code & 4) *F.at32(st.w & 0xFFFFu, cw + hc, cg + hc) ^= bit;
+                  if (code & 8) *F.at32(st.w >> 16, cw + hc, cg + hc) ^= bit;
+                }
+              }
+            }
+          }
+        }
+        break;
+      }
+      default:
+        done = true;
+        break;
+    }
+    if (kind == SEG_WIN || kind == SEG_END) {
+      __syncthreads();  // every thread is done with this window
+      if (tid == 0) issue(kwin + 2);
+      kwin++;
+      need_window = true;
+      if (kind == SEG_END) break;
+    }
+  }
+
+  // ---- write the frame back, undoing the x<->z relabels
+  for (uint32_t s = rr; s < a.nslots; s += R) {
+    if (!act) break;
+    const uint32_t q = __ldg(a.slot_qubit + s), sw = __ldg(a.slot_swap + s);
+    uint2* gx = (uint2*)(a.planes + (uint64_t)(2 * q) * pitch + cg);
+    uint2* gz = (uint2*)(a.planes + (uint64_t)(2 * q + 1) * pitch + cg);
+    if (SMEM) {
+      *gx = *F.at2(2 * s + sw, cw, cg);
+      *gz = *F.at2(2 * s + 1 - sw, cw, cg);
+    } else if (sw) {
+      const uint2 x = *gx, z = *gz;
+      *gx = z;
+      *gz = x;
+    }
+  }
+  __syncthreads();
+  return true;
+}
+
+// The plain launch: one program on one frame, CTA b walking tiles b, b + grid, ...
+template <bool SMEM, bool PHILOX>
+__global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
+  extern __shared__ __align__(128) uint32_t sm[];
+  const uint32_t tid = threadIdx.x, T = a.tile;
   // layout: [frame tile | pmap] [window 0] [window 1] [2 mbarriers]
   const uint32_t tile_words = SMEM ? 2 * a.nslots * T : 2 * a.nslots;
   uint32_t* win0 = sm + ((tile_words + 31) & ~31u);
@@ -335,292 +625,103 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
   if (tid == 0) { issue(0); issue(1); }
   uint64_t kwin = 0;
   bool failed = false;
-
-  for (uint64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-    const uint64_t c0 = tile * T, cg = c0 + cw;  // the pair's first column in the frame
-    const bool act = rr < R && cg < a.ncols;
-    const bool two = cg + 1 < a.ncols;          // its second column exists
-    const uint64_t col = a.col0 + cg, col1 = col + 1;
-    const uint32_t clo = (uint32_t)col, chi = (uint32_t)(col >> 32);
-    const uint32_t clo1 = (uint32_t)col1, chi1 = (uint32_t)(col1 >> 32);
-    const Tile<SMEM> F{sm, a.planes, sm, pitch, T};
-
-    // ---- initial frame
-    if (a.fresh) {
-      for (uint32_t qb = rr; qb * 4 < a.nq1; qb += R) {
-        if (!act) break;
-        uint32_t o[4], u[4];
-        philox4x32_10(qb, clo, chi, TAG_INITZ, k0, k1, o);
-        philox4x32_10(qb, clo1, chi1, TAG_INITZ, k0, k1, u);
-#pragma unroll
-        for (uint32_t j = 0; j < 4; j++) {
-          const uint32_t q = qb * 4 + j;
-          if (q >= a.nq1) break;
-          const uint32_t s = (SMEM && q < a.qubit_slot_len) ? __ldg(a.qubit_slot + q) : BIT_NONE;
-          if (SMEM && s != BIT_NONE) {
-            *F.at2(2 * s, cw, cg) = make_uint2(0u, 0u);
-            *F.at2(2 * s + 1, cw, cg) = make_uint2(o[j], u[j]);
-          } else {
-            *(uint2*)(a.planes + (uint64_t)(2 * q) * pitch + cg) = make_uint2(0u, 0u);
-            *(uint2*)(a.planes + (uint64_t)(2 * q + 1) * pitch + cg) = make_uint2(o[j], u[j]);
-          }
-        }
-      }
-    } else if (SMEM) {
-      for (uint32_t s = rr; s < a.nslots; s += R) {
-        if (!act) break;
-        const uint32_t q = __ldg(a.slot_qubit + s);
-        *F.at2(2 * s, cw, cg) = *(const uint2*)(a.planes + (uint64_t)(2 * q) * pitch + cg);
-        *F.at2(2 * s + 1, cw, cg) = *(const uint2*)(a.planes + (uint64_t)(2 * q + 1) * pitch + cg);
-      }
+  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    if (!walk_tile<SMEM, PHILOX>(a, sm, win0, win1, bars, kwin, issue, tile)) {
+      failed = true;
+      break;
     }
-    // mask mode: the events of the pair's columns, [ep[h], ep[h + 1]) for column h
-    uint64_t ep[3] = {0, 0, 0};
-    if (!PHILOX && rr == 0 && act) {
-      ep[0] = a.ev_off[cg];
-      ep[1] = a.ev_off[cg + 1];
-      ep[2] = two ? a.ev_off[cg + 2] : ep[1];
-    }
-
-    // ---- the program, window by window
-    const uint32_t* wp = nullptr;
-    bool need_window = true;
-    bool done = false;
-    while (!done) {
-      if (need_window) {
-        const bool ok = mbar_wait(&bars[kwin & 1], (uint32_t)((kwin >> 1) & 1));
-        if (__syncthreads_or(!ok)) {  // every thread takes the same branch
-          if (tid == 0) atomicExch(a.err, QCB_ETIMEOUT);
-          failed = true;
-          break;
-        }
-        wp = (kwin & 1) ? win1 : win0;
-        need_window = false;
-      }
-      __syncthreads();  // the tile init / the previous record is complete
-      const uint4 h = *(const uint4*)wp;
-      const uint32_t kind = h.x >> 24, cnt = h.x & 0xFFFFFFu;
-      const uint32_t* e = wp + 4;
-      switch (kind) {
-        case SEG_END:
-          done = true;
-          break;
-        case SEG_WIN:
-          break;
-        case SEG_CNOT: {
-          wp = e + ((cnt * 2 + 3) & ~3u);
-          if (!act) break;
-          const uint2* en = (const uint2*)e;
-          uint32_t j = rr;
-          for (; j + R < cnt; j += 2 * R) {
-            const uint2 o = en[j], u = en[j + R];
-            uint2 *pxc = F.at2(o.x & 0xFFFFu, cw, cg), *pzc = F.at2(o.x >> 16, cw, cg);
-            uint2 *pxt = F.at2(o.y & 0xFFFFu, cw, cg), *pzt = F.at2(o.y >> 16, cw, cg);
-            uint2 *qxc = F.at2(u.x & 0xFFFFu, cw, cg), *qzc = F.at2(u.x >> 16, cw, cg);
-            uint2 *qxt = F.at2(u.y & 0xFFFFu, cw, cg), *qzt = F.at2(u.y >> 16, cw, cg);
-            const uint2 xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
-            const uint2 yxc = *qxc, yzc = *qzc, yxt = *qxt, yzt = *qzt;
-            *pxt = xor2(xt, xc); *pzc = xor2(zc, zt);
-            *qxt = xor2(yxt, yxc); *qzc = xor2(yzc, yzt);
-          }
-          for (; j < cnt; j += R) {
-            const uint2 o = en[j];
-            uint2 *pxc = F.at2(o.x & 0xFFFFu, cw, cg), *pzc = F.at2(o.x >> 16, cw, cg);
-            uint2 *pxt = F.at2(o.y & 0xFFFFu, cw, cg), *pzt = F.at2(o.y >> 16, cw, cg);
-            const uint2 xc = *pxc, zc = *pzc, xt = *pxt, zt = *pzt;
-            *pxt = xor2(xt, xc); *pzc = xor2(zc, zt);
-          }
-          break;
-        }
-        case SEG_CZ: {
-          wp = e + ((cnt * 2 + 3) & ~3u);
-          if (!act) break;
-          const uint2* en = (const uint2*)e;
-          for (uint32_t j = rr; j < cnt; j += R) {
-            const uint2 o = en[j];
-            uint2 *pxa = F.at2(o.x & 0xFFFFu, cw, cg), *pza = F.at2(o.x >> 16, cw, cg);
-            uint2 *pxb = F.at2(o.y & 0xFFFFu, cw, cg), *pzb = F.at2(o.y >> 16, cw, cg);
-            const uint2 xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
-            *pza = xor2(za, xb); *pzb = xor2(zb, xa);
-          }
-          break;
-        }
-        case SEG_S:
-        case SEG_G1: {
-          wp = e + ((cnt * 2 + 3) & ~3u);
-          if (!act) break;
-          const uint2* en = (const uint2*)e;
-          for (uint32_t j = rr; j < cnt; j += R) {
-            const uint2 o = en[j];
-            uint2 *px = F.at2(o.x & 0xFFFFu, cw, cg), *pz = F.at2(o.x >> 16, cw, cg);
-            uint2 x = *px, z = *pz;
-            if (kind == SEG_S) {
-              z = xor2(z, x);
-            } else {
-              gate1_xz(o.y, x.x, z.x);
-              gate1_xz(o.y, x.y, z.y);
-            }
-            *px = x; *pz = z;
-          }
-          break;
-        }
-        case SEG_G2: {
-          wp = e + cnt * 4;
-          if (!act) break;
-          const uint4* en = (const uint4*)e;
-          for (uint32_t j = rr; j < cnt; j += R) {
-            const uint4 o = en[j];
-            uint2 *pxa = F.at2(o.x & 0xFFFFu, cw, cg), *pza = F.at2(o.x >> 16, cw, cg);
-            uint2 *pxb = F.at2(o.y & 0xFFFFu, cw, cg), *pzb = F.at2(o.y >> 16, cw, cg);
-            uint2 xa = *pxa, za = *pza, xb = *pxb, zb = *pzb;
-            gate2_xz(o.z, xa.x, za.x, xb.x, zb.x);
-            gate2_xz(o.z, xa.y, za.y, xb.y, zb.y);
-            *pxa = xa; *pza = za; *pxb = xb; *pzb = zb;
-          }
-          break;
-        }
-        case SEG_MZ: {
-          wp = e + ((cnt * 2 + 3) & ~3u);
-          if (!act) break;
-          const uint2* en = (const uint2*)e;
-          for (uint32_t j = rr; j < cnt; j += R) {
-            const uint2 o = en[j];
-            *(uint2*)(a.rec + (uint64_t)o.y * pitch + cg) = *F.at2(o.x, cw, cg);
-          }
-          break;
-        }
-        case SEG_MRZ: {
-          wp = e + cnt * 16;
-          if (!act) break;
-          const uint4* en = (const uint4*)e;
-          for (uint32_t g = rr; g < cnt; g += R) {
-            uint4 ent[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) ent[i] = en[4 * g + i];
-            uint32_t o[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
-            if (PHILOX) {
-              uint32_t blk = 0;
-#pragma unroll
-              for (int i = 0; i < 4; i++)
-                if (ent[i].z != MRZ_PAD) blk = ent[i].z >> 2;
-              philox4x32_10(blk, clo, chi, TAG_RESET, k0, k1, o);
-              philox4x32_10(blk, clo1, chi1, TAG_RESET, k0, k1, u);
-            }
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-              if (ent[i].z == MRZ_PAD) continue;
-              uint2* px = F.at2(ent[i].x & 0xFFFFu, cw, cg);
-              uint2* pz = F.at2(ent[i].x >> 16, cw, cg);
-              const uint2 x = *px, z = *pz;
-              uint2 rb = make_uint2(o[i], u[i]);
-              if (!PHILOX) {
-                const uint32_t* rp = a.reset_planes + (uint64_t)ent[i].z * a.reset_pitch + cg;
-                rb = a.reset_planes ? make_uint2(__ldg(rp), two ? __ldg(rp + 1) : 0u) : make_uint2(0u, 0u);
-              }
-              if (ent[i].y != BIT_NONE) *(uint2*)(a.rec + (uint64_t)ent[i].y * pitch + cg) = x;
-              *px = make_uint2(0u, 0u);
-              *pz = xor2(z, rb);
-            }
-          }
-          break;
-        }
-        case SEG_XOR: {
-          wp = e + cnt * 32;
-          if (!act) break;
-          for (uint32_t j = rr; j < cnt; j += R) {
-            const uint32_t* x = e + 32 * j;  // (store, n, b_0 .. b_{n-1})
-            const uint32_t n = min(x[1], XOR_MAX_BITS);
-            uint2 v = make_uint2(0u, 0u);
-            for (uint32_t i = 0; i < n; i++) v = xor2(v, *(const uint2*)(a.rec + (uint64_t)x[2 + i] * pitch + cg));
-            *(uint2*)(a.rec + (uint64_t)x[0] * pitch + cg) = v;
-          }
-          break;
-        }
-        case SEG_FLUSH: {
-          wp = e + cnt * 4;
-          const uint4* en = (const uint4*)e;
-          if (PHILOX) {
-            if (a.pmax > 0.0) {
-              // (site, shot group) tasks over all threads of the CTA; a group
-              // is 32 run columns and may straddle the tile's edges
-              const uint64_t gc0 = a.col0 + c0;
-              const uint64_t gc1 = a.col0 + min(c0 + T, a.ncols);
-              const uint64_t G0 = gc0 / 32;
-              const uint32_t ng = (uint32_t)((gc1 - 1) / 32 - G0 + 1);
-              const uint32_t ntask = cnt * ng;
-              for (uint32_t t = tid; t < ntask; t += blockDim.x) {
-                const uint32_t i = t / ng, gl = t - i * ng;
-                const int32_t lc0 = (int32_t)((int64_t)((G0 + gl) * 32) - (int64_t)gc0);
-                sample_site_group<SMEM>(a, F, en[i], G0 + gl, lc0, c0);
-              }
-            }
-          } else if (rr == 0 && act) {
-            // each column's events are sorted by trial (site*32 + lane)
-            for (uint32_t hc = 0; hc < 2; hc++) {
-              const uint64_t eb = ep[hc], ee = ep[hc + 1];
-              if (eb == ee) continue;
-              for (uint32_t i = 0; i < cnt; i++) {
-                const uint4 st = en[i];
-                const uint64_t lo_t = (uint64_t)st.x * 32u, lim = lo_t + 32u;
-                uint64_t lo = eb, hi = ee;
-                while (lo < hi) {
-                  const uint64_t mid = (lo + hi) >> 1;
-                  if ((__ldg(a.ev_data + mid) >> 8) < lo_t) lo = mid + 1;
-                  else hi = mid;
-                }
-                for (uint64_t k = lo; k < ee; k++) {
-                  const uint64_t d = __ldg(a.ev_data + k);
-                  const uint64_t t = d >> 8;
-                  if (t >= lim) break;
-                  const uint32_t code = (uint32_t)(d & 0xFF), bit = 1u << (t & 31);
-                  if (code & 1) *F.at32(st.z & 0xFFFFu, cw + hc, cg + hc) ^= bit;
-                  if (code & 2) *F.at32(st.z >> 16, cw + hc, cg + hc) ^= bit;
-                  if ((st.y & 0xFFu) == QCB_OP_DEPOL2) {
-                    if (code & 4) *F.at32(st.w & 0xFFFFu, cw + hc, cg + hc) ^= bit;
-                    if (code & 8) *F.at32(st.w >> 16, cw + hc, cg + hc) ^= bit;
-                  }
-                }
-              }
-            }
-          }
-          break;
-        }
-        default:
-          done = true;
-          break;
-      }
-      if (kind == SEG_WIN || kind == SEG_END) {
-        __syncthreads();  // every thread is done with this window
-        if (tid == 0) issue(kwin + 2);
-        kwin++;
-        need_window = true;
-        if (kind == SEG_END) break;
-      }
-    }
-    if (failed) break;
-
-    // ---- write the frame back, undoing the x<->z relabels
-    for (uint32_t s = rr; s < a.nslots; s += R) {
-      if (!act) break;
-      const uint32_t q = __ldg(a.slot_qubit + s), sw = __ldg(a.slot_swap + s);
-      uint2* gx = (uint2*)(a.planes + (uint64_t)(2 * q) * pitch + cg);
-      uint2* gz = (uint2*)(a.planes + (uint64_t)(2 * q + 1) * pitch + cg);
-      if (SMEM) {
-        *gx = *F.at2(2 * s + sw, cw, cg);
-        *gz = *F.at2(2 * s + 1 - sw, cw, cg);
-      } else if (sw) {
-        const uint2 x = *gx, z = *gz;
-        *gx = z;
-        *gz = x;
-      }
-    }
-    __syncthreads();
   }
   // no bulk copy may still be in flight when the CTA exits
   if (failed) {
     __syncthreads();
     if (tid == 0)
       for (uint64_t k = kwin; k < kwin + 2 && k < total_win; k++) mbar_wait(&bars[k & 1], (uint32_t)((k >> 1) & 1));
+  }
+}
+
+// ---------------------------------------------------------------- batches
+// Many (program, frame) jobs drained from one persistent launch: the items
+// are (job, tile) pairs in a queue ordered longest first; each CTA (one per
+// SM) takes the next item with an atomic on the queue head.  Thread 0 stages
+// program windows two ahead across item boundaries: when it stages the last
+// window of an item it takes the next item and records it in a ring that the
+// walk reads when it reaches that item.  Every job is fresh (initZ! fused)
+// and in Philox mode, so its results are those of its plain launch.
+struct BatchItem {
+  uint32_t job;
+  uint32_t pad;
+  uint64_t tile;
+};
+
+struct BatchArgs {
+  const WalkArgs* jobs;
+  const BatchItem* items;
+  uint32_t nitems;
+  uint32_t tile_words;  // the largest frame tile of the jobs (words)
+  uint32_t* head;       // next queue item (zero before the launch)
+};
+
+constexpr uint32_t ITEM_NONE = 0xFFFFFFFFu;
+static_assert(sizeof(WalkArgs) % 8 == 0, "WalkArgs is copied in 8-byte words");
+
+__global__ void __launch_bounds__(768, 1) batch_walker_kernel(const BatchArgs b) {
+  extern __shared__ __align__(128) uint32_t sm[];
+  __shared__ uint32_t itemq[8];
+  __shared__ __align__(16) WalkArgs ja;
+  const uint32_t tid = threadIdx.x;
+  uint32_t* win0 = sm + ((b.tile_words + 31) & ~31u);
+  uint32_t* win1 = win0 + PROG_WINDOW_WORDS;
+  uint64_t* bars = (uint64_t*)(win1 + PROG_WINDOW_WORDS);
+  // staging side (thread 0): the item being staged and its next window
+  uint32_t icur = ITEM_NONE, iw = 0, iq = 0;
+  uint64_t issued = 0;
+  auto fetch = [&]() -> uint32_t {
+    const uint32_t i = atomicAdd(b.head, 1u);
+    return i < b.nitems ? i : ITEM_NONE;
+  };
+  auto issue = [&](uint64_t) {
+    if (icur == ITEM_NONE) return;
+    const WalkArgs& J = b.jobs[b.items[icur].job];
+    stage_window((issued & 1) ? win1 : win0, J.prog + (size_t)iw * (PROG_WINDOW_WORDS / 4), PROG_WINDOW_WORDS * 4,
+                 &bars[issued & 1]);
+    issued++;
+    if (++iw == J.nwin) {
+      iw = 0;
+      icur = fetch();
+      iq++;
+      itemq[iq & 7] = icur;
+    }
+  };
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    icur = fetch();
+    itemq[0] = icur;
+    issue(0);
+    issue(1);
+  }
+  __syncthreads();
+  uint64_t kwin = 0;
+  bool failed = false;
+  for (uint32_t wi = 0;; wi++) {
+    const uint32_t it = itemq[wi & 7];  // staged at least one window earlier
+    if (it == ITEM_NONE) break;
+    const BatchItem bi = b.items[it];
+    __syncthreads();  // everyone has read the ring and is done with the previous job
+    for (uint32_t w = tid; w < sizeof(WalkArgs) / 8; w += blockDim.x)
+      ((uint64_t*)&ja)[w] = ((const uint64_t*)(b.jobs + bi.job))[w];
+    __syncthreads();
+    if (!walk_tile<true, true>(ja, sm, win0, win1, bars, kwin, issue, bi.tile)) {
+      failed = true;
+      break;
+    }
+  }
+  // no bulk copy may still be in flight when the CTA exits
+  if (failed) {
+    __syncthreads();
+    if (tid == 0)
+      for (uint64_t k = kwin; k < issued; k++) mbar_wait(&bars[k & 1], (uint32_t)((k >> 1) & 1));
   }
 }
 
@@ -1090,3 +1191,171 @@ int run_program_fresh(qcb_frame* f, const qcb_program* p, uint64_t seed, uint64_
   return run_program(f, p, &n, true, st);
 }
 }  // namespace qcb
+
+// ---------------------------------------------------------------- batches (host)
+namespace qcb {
+
+// The tuner's table: tile width per size class (touched qubits).
+static std::map<uint32_t, uint32_t> g_tuned_tile;
+
+// Widest tile (even, <= 256) whose frame fits one CTA's shared memory next to
+// the staging buffers; 0 when not even 16 columns fit.
+static uint32_t batch_tile_max(const qcb_program* p) {
+  const size_t per_col = (size_t)2 * std::max<uint32_t>(p->nslots, 1) * 4;
+  const size_t stage = (size_t)2 * PROG_WINDOW_WORDS * 4 + 16 + 128 + sizeof(WalkArgs) + 64;
+  const size_t maxsm = (size_t)device_max_smem_optin();
+  const size_t budget = maxsm > stage ? maxsm - stage : 0;
+  uint32_t t = (uint32_t)std::min<size_t>(256, budget / per_col) & ~1u;
+  return t >= 16 ? t : 0;
+}
+
+}  // namespace qcb
+
+struct qcb_batch {
+  std::vector<qcb_frame*> frames;
+  qcb::WalkArgs* d_jobs = nullptr;
+  qcb::BatchItem* d_items = nullptr;
+  uint32_t* d_head = nullptr;
+  uint32_t nitems = 0;
+  uint32_t tile_words = 0;
+  size_t smem_bytes = 0;
+  uint32_t grid = 0;
+};
+
+extern "C" {
+
+int qcb_batch_create(const qcb_batch_job* jobs, size_t n_jobs, qcb_batch** out) {
+  using namespace qcb;
+  if (!out || (n_jobs && !jobs)) return fail(QCB_EARG, "null argument");
+  *out = nullptr;
+  std::vector<WalkArgs> wa(n_jobs);
+  struct Cost { double c; uint32_t job; uint64_t tile; };
+  std::vector<Cost> items;
+  uint32_t tile_words = 0;
+  auto b = std::make_unique<qcb_batch>();
+  for (size_t j = 0; j < n_jobs; j++) {
+    const qcb_batch_job& J = jobs[j];
+    qcb_noise_source n{};
+    n.mode = QCB_NOISE_PHILOX;
+    n.seed = J.seed;
+    n.shot_offset = J.shot_offset;
+    if (int s = check_run(J.frame, J.program, &n)) return s;
+    const uint32_t tmax = batch_tile_max(J.program);
+    if (!tmax) return fail(QCB_EUNSUPPORTED, "batch job " + std::to_string(j) + ": its frame tile does not fit shared memory");
+    uint32_t T = J.tile;
+    if (T && (T % 2 || T < 16 || T > tmax)) return fail(QCB_EARG, "batch job " + std::to_string(j) + ": bad tile width");
+    if (!T) {
+      auto it = g_tuned_tile.find(J.program->nslots);
+      T = it != g_tuned_tile.end() ? std::min(it->second, tmax) : tmax;
+    }
+    const uint64_t ncols = J.frame->ncols;
+    T = (uint32_t)std::min<uint64_t>(T, std::max<uint64_t>(16, (ncols + 1) & ~1ull));
+    WalkArgs& a = wa[j];
+    fill_common(a, J.frame, J.program);
+    a.seed = J.seed;
+    a.col0 = J.shot_offset / 32;
+    a.fresh = 1;
+    a.tile = T;
+    tile_words = std::max(tile_words, 2 * J.program->nslots * T);
+    b->frames.push_back(J.frame);
+    // longest first: a tile walks every record once, its ops over T columns
+    const double cost = (double)J.program->stream_slot.size() * (1.0 + T / 64.0);
+    for (uint64_t t = 0; t * T < ncols; t++) items.push_back({cost, (uint32_t)j, t});
+  }
+  std::stable_sort(items.begin(), items.end(), [](const Cost& x, const Cost& y) { return x.c > y.c; });
+  std::vector<BatchItem> it(items.size());
+  for (size_t i = 0; i < items.size(); i++) it[i] = {items[i].job, 0u, items[i].tile};
+  if (items.size() > 0xFFFFFFF0ull) return fail(QCB_EARG, "too many tiles in one batch");
+  b->nitems = (uint32_t)items.size();
+  b->tile_words = tile_words;
+  b->smem_bytes = (size_t)((tile_words + 31) & ~31u) * 4 + (size_t)2 * PROG_WINDOW_WORDS * 4 + 16;
+  b->grid = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(b->nitems, 1), (uint64_t)device_sm_count());
+  QCB_CUDA(cudaMalloc(&b->d_jobs, std::max<size_t>(wa.size(), 1) * sizeof(WalkArgs)));
+  QCB_CUDA(cudaMalloc(&b->d_items, std::max<size_t>(it.size(), 1) * sizeof(BatchItem)));
+  QCB_CUDA(cudaMalloc(&b->d_head, 4));
+  if (!wa.empty()) QCB_CUDA(cudaMemcpy(b->d_jobs, wa.data(), wa.size() * sizeof(WalkArgs), cudaMemcpyHostToDevice));
+  if (!it.empty()) QCB_CUDA(cudaMemcpy(b->d_items, it.data(), it.size() * sizeof(BatchItem), cudaMemcpyHostToDevice));
+  QCB_CUDA(cudaFuncSetAttribute(batch_walker_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_bytes));
+  *out = b.release();
+  return QCB_OK;
+}
+
+int qcb_batch_run(qcb_batch* b, void* stream) {
+  using namespace qcb;
+  if (!b) return fail(QCB_EARG, "null batch");
+  if (!b->nitems) return QCB_OK;
+  cudaStream_t st = S(stream);
+  QCB_CUDA(cudaMemsetAsync(b->d_head, 0, 4, st));
+  BatchArgs a{b->d_jobs, b->d_items, b->nitems, b->tile_words, b->d_head};
+  batch_walker_kernel<<<b->grid, 768, b->smem_bytes, st>>>(a);
+  QCB_LAUNCHED();
+  return QCB_OK;
+}
+
+int qcb_batch_status(const qcb_batch* b) {
+  if (!b) return fail(QCB_EARG, "null batch");
+  for (qcb_frame* f : b->frames)
+    if (int s = frame_device_status(f)) return s;
+  return QCB_OK;
+}
+
+int qcb_batch_destroy(qcb_batch* b) {
+  if (!b) return QCB_OK;
+  cudaFree(b->d_jobs);
+  cudaFree(b->d_items);
+  cudaFree(b->d_head);
+  delete b;
+  return QCB_OK;
+}
+
+// The autotuner: time candidate tile widths for this program on a scratch
+// frame of two full waves per candidate (fresh Philox runs, CUDA events) and
+// keep the width with the most frame columns per second for the program's
+// size class (its touched qubits); qcb_batch_create uses it.
+int qcb_tune_tile(const qcb_program* p, uint32_t* tile_out, float* us_per_column, void* stream) {
+  using namespace qcb;
+  if (!p) return fail(QCB_EARG, "null program");
+  const uint32_t tmax = batch_tile_max(p);
+  if (!tmax) return fail(QCB_EUNSUPPORTED, "the program's frame tile does not fit shared memory");
+  cudaStream_t st = S(stream);
+  const uint32_t cands[] = {16, 24, 32, 48, 64, 96, 128, 192, 256};
+  const uint64_t nsm = (uint64_t)std::max(device_sm_count(), 1);
+  uint32_t best = 0;
+  float best_us = 0.f;
+  cudaEvent_t e0, e1;
+  QCB_CUDA(cudaEventCreate(&e0));
+  QCB_CUDA(cudaEventCreate(&e1));
+  const uint32_t saved = g_tile_override;
+  int status = QCB_OK;
+  for (uint32_t T : cands) {
+    if (T > tmax) break;
+    const uint64_t ncols = 2 * nsm * T;
+    qcb_frame* f = nullptr;
+    if ((status = qcb_frame_create(ncols * 32, p->nq > 0 ? p->nq - 1 : 0, p->info.nbits, &f))) break;
+    g_tile_override = T;
+    float ms = 0.f;
+    for (int rep = 0; rep < 4 && status == QCB_OK; rep++) {
+      cudaEventRecord(e0, st);
+      status = run_program_fresh(f, p, 0x5EEDull + rep, 0, st);
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) status = fail(QCB_ECUDA, "tuner timing");
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep > 0) ms = rep == 1 ? t : std::min(ms, t);  // rep 0 warms up
+    }
+    qcb_frame_destroy(f);
+    if (status != QCB_OK) break;
+    const float us = ms * 1000.f / (float)ncols;
+    if (!best || us < best_us) { best = T; best_us = us; }
+  }
+  g_tile_override = saved;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (status != QCB_OK) return status;
+  g_tuned_tile[p->nslots] = best;
+  if (tile_out) *tile_out = best;
+  if (us_per_column) *us_per_column = best_us;
+  return QCB_OK;
+}
+
+}  // extern "C"

@@ -309,7 +309,333 @@ __global__ void __launch_bounds__(PROJ_THREADS) project_kernel(const ProjArgs a)
   if (me == 0 && tid == 0) { a.status[0] = PST_OK; a.status[1] = (int32_t)a.k; }
 }
 
-static uint32_t g_proj_cs = 8;
+// ---------------------------------------------------------------------------
+// project_smem_kernel: the same projections with the whole tableau held in
+// the cluster's shared memory (CTA c owns rows [c*RB, c*RB + RB), row stride
+// W+1 words).  Per Pauli there are two cluster barriers: one after every CTA
+// has published the first anticommuting row of each range it owns (every CTA
+// then reads all of them through distributed shared memory and takes the
+// same decision), one after every CTA has fetched the pivot row.  The row
+// products then run on local rows only, and the row copies are done by the
+// rows' owners from their local copies of the pivot and the Pauli (neither
+// row is among the updated ones).  Rows are read from and written back to
+// global memory once per launch.
+struct ProjSmemArgs {
+  ProjArgs a;
+  uint32_t RB;
+};
+
+// Lanes per row: the smallest power of two >= the words of one half, at most 32.
+__device__ __forceinline__ uint32_t group_lanes(uint32_t len) {
+  uint32_t g = 1;
+  while (g < len && g < 32) g <<= 1;
+  return g;
+}
+
+__global__ void __launch_bounds__(PROJ_THREADS) project_smem_kernel(const ProjSmemArgs pa) {
+  const ProjArgs& a = pa.a;
+  cg::cluster_group cl = cg::this_cluster();
+  const uint32_t me = cl.block_rank(), CS = cl.num_blocks();
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t W = a.W, len = W / 2, WS = W + 1, RB = pa.RB;
+  const uint32_t rows = a.rows;
+  const uint32_t r0 = me * RB;
+  const uint32_t nloc = r0 < rows ? min(RB, rows - r0) : 0u;
+  const uint32_t G = group_lanes(len), GPW = 32 / G;  // lanes per row, rows per warp pass
+  const uint32_t gl = lane % G, gi = lane / G;
+
+  extern __shared__ __align__(16) uint64_t smem[];
+  uint64_t* P = smem;                       // W: the Pauli
+  uint64_t* piv = P + W;                    // W: the pivot row / partial product
+  uint64_t* R = piv + W + 1;                // RB * WS: the rows
+  uint8_t* ph = (uint8_t*)(R + (size_t)RB * WS);  // RB
+  uint8_t* fl = ph + RB;                    // RB: comm flags
+  uint32_t* slot = (uint32_t*)(((uintptr_t)(fl + RB) + 15) & ~(uintptr_t)15);  // [2][4]
+  uint32_t* mins = slot + 8;                // 3
+  int32_t* dec = (int32_t*)(mins + 4);      // 8
+
+  auto ROW = [&](uint32_t lr) -> uint64_t* { return R + (size_t)lr * WS; };
+  // (owner CTA, local row) of a global row
+  auto owner_of = [&](uint32_t m) -> uint32_t { return m / RB; };
+
+  for (uint32_t lr = warp; lr < nloc; lr += nwarps)
+    for (uint32_t w = lane; w < W; w += 32) ROW(lr)[w] = a.xzs[(size_t)(r0 + lr) * W + w];
+  for (uint32_t lr = tid; lr < nloc; lr += blockDim.x) ph[lr] = a.ph[r0 + lr];
+  const bool destab = a.kind == QCB_DESTABILIZER || a.kind == QCB_MIXED_DESTABILIZER;
+  const uint32_t nn = destab ? rows / 2 : rows;
+  int32_t r = a.kind == QCB_STABILIZER ? (int32_t)rows : (a.kind == QCB_DESTABILIZER ? (int32_t)(rows / 2) : *a.rank);
+  __syncthreads();
+  cl.sync();
+
+  uint32_t status = PST_OK, jstop = a.k;
+  for (uint32_t j = a.j0; j < a.k; j++) {
+    const uint32_t par = j & 1;
+    const bool single = a.qubits != nullptr;
+    uint32_t wq = 0;
+    uint64_t bq = 0;
+    if (single) {
+      wq = a.qubits[j] >> 6;
+      bq = 1ull << (a.qubits[j] & 63);
+      for (uint32_t w = tid; w < W; w += blockDim.x)
+        P[w] = (((a.basis & 1u) && w == wq) ? bq : 0ull) | (((a.basis & 2u) && w == len + wq) ? bq : 0ull);
+    } else {
+      const uint64_t* pj = a.paulis + (size_t)j * W;
+      for (uint32_t w = tid; w < W; w += blockDim.x) P[w] = pj[w];
+    }
+    if (tid < 3) mins[tid] = 0xFFFFFFFFu;
+    const uint32_t pphase = single ? 0u : a.pph[j];
+    __syncthreads();
+    // 1. comm flags of the local rows and the first anticommuting row of each range
+    auto note = [&](uint32_t m, uint32_t c) {
+      if (!c) return;
+      if (!destab) {
+        if (m < (uint32_t)r) atomicMin(&mins[0], m);
+      } else {
+        if (m >= nn && m < nn + (uint32_t)r) atomicMin(&mins[0], m - nn);
+        if (a.kind == QCB_MIXED_DESTABILIZER) {
+          if (m >= (uint32_t)r && m < nn) atomicMin(&mins[1], m);
+          if (m >= nn + (uint32_t)r) atomicMin(&mins[2], m);
+        }
+      }
+    };
+    if (single) {
+      for (uint32_t lr = tid; lr < nloc; lr += blockDim.x) {
+        const uint64_t* row = ROW(lr);
+        uint32_t c = 0;
+        if (a.basis & 1u) c ^= (uint32_t)((row[len + wq] & bq) != 0);
+        if (a.basis & 2u) c ^= (uint32_t)((row[wq] & bq) != 0);
+        fl[lr] = (uint8_t)c;
+        note(r0 + lr, c);
+      }
+    } else {
+      for (uint32_t base = warp * GPW; base < nloc; base += nwarps * GPW) {
+        const uint32_t lr = base + gi;
+        uint64_t acc = 0;
+        if (lr < nloc) {
+          const uint64_t* row = ROW(lr);
+          for (uint32_t w = gl; w < len; w += G) acc ^= (P[len + w] & row[w]) ^ (P[w] & row[len + w]);
+        }
+        uint32_t c = (uint32_t)__popcll(acc);
+        for (uint32_t off = G >> 1; off; off >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, off);
+        c &= 1u;
+        if (gl == 0 && lr < nloc) {
+          fl[lr] = (uint8_t)c;
+          note(r0 + lr, c);
+        }
+      }
+    }
+    __syncthreads();
+    if (tid < 3) slot[par * 4 + tid] = mins[tid];
+    cl.sync();
+    // 2. the same decision in every CTA
+    if (warp == 0) {
+      uint32_t m0 = 0xFFFFFFFFu, m1 = 0xFFFFFFFFu, m2 = 0xFFFFFFFFu;
+      if (lane < CS) {
+        const uint32_t* rs = cl.map_shared_rank(slot + par * 4, lane);
+        m0 = rs[0]; m1 = rs[1]; m2 = rs[2];
+      }
+      m0 = __reduce_min_sync(0xFFFFFFFFu, m0);
+      m1 = __reduce_min_sync(0xFFFFFFFFu, m1);
+      m2 = __reduce_min_sync(0xFFFFFFFFu, m2);
+      if (lane == 0) {
+        int32_t branch = 0, pivrow = -1, anticom = 0;
+        if (m0 != 0xFFFFFFFFu) {
+          branch = 1;
+          anticom = (int32_t)m0 + 1;
+          pivrow = destab ? (int32_t)nn + anticom - 1 : anticom - 1;
+        } else if (a.kind == QCB_MIXED_DESTABILIZER && (m1 != 0xFFFFFFFFu || m2 != 0xFFFFFFFFu)) {
+          branch = 2;
+          anticom = (int32_t)(m1 != 0xFFFFFFFFu ? m1 : m2) + 1;  // 1-based anticomlog
+          pivrow = (int32_t)nn + r;
+        }
+        dec[0] = branch; dec[1] = pivrow; dec[2] = anticom;
+      }
+    }
+    __syncthreads();
+    const int32_t branch = dec[0];
+    if (branch == 0) {
+      if (!destab) {
+        if (a.keep_result || a.kind == QCB_MIXED_STABILIZER) { status = PST_NEED_CANON; jstop = j; break; }
+        if (me == 0 && tid == 0) { a.anticom[j] = 0; a.result[j] = -1; }
+        continue;
+      }
+      if (a.kind == QCB_DESTABILIZER && nn != a.n) { status = PST_BADSTRUCT; jstop = j; break; }
+      if (!a.keep_result) {
+        if (me == 0 && tid == 0) { a.anticom[j] = 0; a.result[j] = -1; }
+        continue;
+      }
+      // result: the product of the stabilizer rows i < r whose destabilizer
+      // row anticommutes with the Pauli (the stabilizer rows commute, so the
+      // per-CTA partial products can be combined in any order with the exact
+      // phase).  Warp 0 of each CTA multiplies its own stabilizer rows.
+      if (warp == 0) {
+        uint64_t c1 = 0, c2 = 0;
+        uint32_t extra = 0;
+        for (uint32_t w = lane; w < W; w += 32) piv[w] = 0;
+        __syncwarp();
+        for (uint32_t lr = 0; lr < nloc; lr++) {
+          const uint32_t m = r0 + lr;
+          if (m < nn || m >= nn + (uint32_t)r) continue;
+          const uint32_t i = m - nn;  // destabilizer partner row i
+          const uint32_t o = owner_of(i);
+          const uint8_t f = o == me ? fl[i - r0] : *cl.map_shared_rank(fl + (i - o * RB), o);
+          if (!f) continue;
+          const uint64_t* srow = ROW(lr);
+          for (uint32_t w = lane; w < len; w += 32) {
+            uint64_t x2 = piv[w], z2 = piv[len + w];
+            mul_step_p(srow[w], srow[len + w], x2, z2, c1, c2);
+            piv[w] = x2;
+            piv[len + w] = z2;
+          }
+          __syncwarp();
+          extra += ph[lr];
+        }
+        const uint32_t s = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)(__popcll(c1) + 2 * __popcll(c2)) & 3u) & 3u;
+        if (lane == 0) piv[W] = (uint64_t)((s + extra) & 3u);
+      }
+      cl.sync();
+      if (me == 0 && warp == 0) {
+        // combine the CTAs' partial products in CTA order into P's buffer
+        uint64_t c1 = 0, c2 = 0;
+        uint32_t extra = pphase;
+        for (uint32_t w = lane; w < W; w += 32) P[w] = 0;
+        __syncwarp();
+        for (uint32_t q = 0; q < CS; q++) {
+          const uint64_t* pq = q == 0 ? piv : cl.map_shared_rank(piv, q);
+          for (uint32_t w = lane; w < len; w += 32) {
+            uint64_t x2 = P[w], z2 = P[len + w];
+            mul_step_p(pq[w], pq[len + w], x2, z2, c1, c2);
+            P[w] = x2;
+            P[len + w] = z2;
+          }
+          __syncwarp();
+          extra += (uint32_t)pq[W];
+        }
+        const uint32_t s = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)(__popcll(c1) + 2 * __popcll(c2)) & 3u) & 3u;
+        if (lane == 0) {
+          a.anticom[j] = 0;
+          a.result[j] = a.phases ? (int32_t)((s + extra) & 3u) : (int32_t)(pphase & 3u);
+        }
+      }
+      continue;
+    }
+    // 3. MixedDestabilizer logical branch: the row swaps (rare), by CTA 0
+    //    through distributed shared memory
+    if (branch == 2) {
+      if (me == 0) {
+        const uint32_t al = (uint32_t)dec[2];
+        auto swaprow = [&](uint32_t u, uint32_t v) {
+          if (u == v) return;
+          const uint32_t ou = owner_of(u), ov = owner_of(v);
+          uint64_t* ru = cl.map_shared_rank(R + (size_t)(u - ou * RB) * WS, ou);
+          uint64_t* rv = cl.map_shared_rank(R + (size_t)(v - ov * RB) * WS, ov);
+          for (uint32_t w = tid; w < W; w += blockDim.x) { const uint64_t t = ru[w]; ru[w] = rv[w]; rv[w] = t; }
+          if (tid == 0) {
+            uint8_t* pu = cl.map_shared_rank(ph + (u - ou * RB), ou);
+            uint8_t* pv = cl.map_shared_rank(ph + (v - ov * RB), ov);
+            uint8_t t = *pu; *pu = *pv; *pv = t;
+            uint8_t* fu = cl.map_shared_rank(fl + (u - ou * RB), ou);
+            uint8_t* fv = cl.map_shared_rank(fl + (v - ov * RB), ov);
+            t = *fu; *fu = *fv; *fv = t;
+          }
+          __syncthreads();
+        };
+        const uint32_t ru = (uint32_t)r;
+        if (al <= nn) {
+          swaprow(ru + nn, al - 1);
+          if (nn != ru + 1 && al != ru + 1) swaprow(ru, al + nn - 1);
+        } else {
+          swaprow(ru, al - nn - 1);
+          swaprow(ru + nn, al - 1);
+        }
+      }
+      cl.sync();
+    }
+    // 4. every CTA fetches the pivot row, then a barrier before its owner may
+    //    overwrite it
+    const uint32_t pivrow = (uint32_t)dec[1];
+    {
+      const uint32_t o = owner_of(pivrow), lr = pivrow - o * RB;
+      const uint64_t* src = o == me ? ROW(lr) : cl.map_shared_rank(R + (size_t)lr * WS, o);
+      for (uint32_t w = tid; w < W; w += blockDim.x) piv[w] = src[w];
+      if (tid == 0) piv[W] = o == me ? ph[lr] : *cl.map_shared_rank(ph + lr, o);
+    }
+    cl.sync();
+    const uint32_t pph = (uint32_t)piv[W];
+    // 5. row products on local rows (anticomm_update_rows or the Stabilizer loop)
+    const uint32_t ac = branch == 2 ? (uint32_t)r + 1 : (uint32_t)dec[2];
+    const uint32_t ru = branch == 2 ? (uint32_t)r + 1 : (uint32_t)r;
+    for (uint32_t base = warp * GPW; base < nloc; base += nwarps * GPW) {
+      const uint32_t lr = base + gi;
+      const uint32_t m = r0 + lr;
+      int mode = 0;  // 0: skip, 1: with phase, 2: without phase
+      if (lr < nloc && fl[lr] && m != pivrow) {
+        if (!destab) mode = (m >= ac && m < (uint32_t)r) ? 1 : 0;
+        else if (m >= ru && m < nn) mode = 1;
+        else if (m >= nn + ac && m < 2 * nn) mode = 1;
+        else if (m < ru && m != ac - 1) mode = 2;
+      }
+      uint64_t c1 = 0, c2 = 0;
+      if (mode) {
+        uint64_t* row = ROW(lr);
+        for (uint32_t w = gl; w < len; w += G) {
+          uint64_t x2 = row[w], z2 = row[len + w];
+          mul_step_p(piv[w], piv[len + w], x2, z2, c1, c2);
+          row[w] = x2;
+          row[len + w] = z2;
+        }
+      }
+      uint32_t sc = (uint32_t)(__popcll(c1) + 2 * __popcll(c2));
+      for (uint32_t off = G >> 1; off; off >>= 1) sc += __shfl_xor_sync(0xFFFFFFFFu, sc, off);
+      if (gl == 0 && mode == 1 && a.phases) ph[lr] = (uint8_t)((sc + ph[lr] + pph) & 3u);
+    }
+    // 6. row copies by the owners, outputs by CTA 0
+    const int32_t rp = a.rand_ph ? (int32_t)a.rand_ph[j] : -1;
+    if (!destab) {
+      const uint32_t dst = ac - 1;
+      if (owner_of(dst) == me) {
+        const uint32_t lr = dst - r0;
+        for (uint32_t w = tid; w < W; w += blockDim.x) ROW(lr)[w] = P[w];
+        if (tid == 0) ph[lr] = (uint8_t)(rp >= 0 ? rp : (int32_t)pphase);
+      }
+    } else {
+      // destabilizer[ac] = stabilizer[ac] (the pivot row); stabilizer[ac] = pauli
+      const uint32_t dd = ac - 1, ds = nn + ac - 1;
+      if (owner_of(dd) == me) {
+        const uint32_t lr = dd - r0;
+        for (uint32_t w = tid; w < W; w += blockDim.x) ROW(lr)[w] = piv[w];
+        if (tid == 0) ph[lr] = (uint8_t)pph;
+      }
+      if (owner_of(ds) == me) {
+        const uint32_t lr = ds - r0;
+        for (uint32_t w = tid; w < W; w += blockDim.x) ROW(lr)[w] = P[w];
+        if (tid == 0) ph[lr] = (uint8_t)(rp >= 0 ? rp : (int32_t)pphase);
+      }
+      if (branch == 2) r += 1;
+    }
+    if (me == 0 && tid == 0) {
+      a.anticom[j] = (int32_t)ac;
+      a.result[j] = rp;
+    }
+    __syncthreads();
+  }
+  // write the rows back; every CTA is done with remote shared memory first
+  cl.sync();
+  for (uint32_t lr = warp; lr < nloc; lr += nwarps)
+    for (uint32_t w = lane; w < W; w += 32) a.xzs[(size_t)(r0 + lr) * W + w] = ROW(lr)[w];
+  for (uint32_t lr = tid; lr < nloc; lr += blockDim.x) a.ph[r0 + lr] = ph[lr];
+  if (me == 0 && tid == 0) {
+    if (a.kind == QCB_MIXED_STABILIZER || a.kind == QCB_MIXED_DESTABILIZER) *a.rank = r;
+    a.status[0] = (int32_t)status;
+    a.status[1] = (int32_t)jstop;
+  }
+}
+
+static size_t proj_smem_bytes(uint32_t RB, uint32_t W) {
+  return ((size_t)2 * W + 1 + (size_t)RB * (W + 1)) * 8 + 2 * (size_t)RB + 16 + 32 + 16 + 32 + 16;
+}
+
+static uint32_t g_proj_cs = 0;  // tuner override (0 = automatic)
 
 }  // namespace qcb
 
@@ -379,9 +705,28 @@ static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64
   int32_t rank = mixed ? *rank_io : 0;
   QCB_CUDA(cudaMemcpyAsync(d_rank, &rank, 4, cudaMemcpyHostToDevice, st));
 
-  const size_t sm = (size_t)2 * t->W * 8;
-  const uint32_t cs = g_proj_cs;
-  QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(sm, 1024)));
+  // launch shape: the tableau in the cluster's shared memory when it fits
+  // (the smallest cluster with at most 128 rows per CTA, or the tuned size),
+  // else the rows stay in global memory
+  const size_t maxsm = (size_t)device_max_smem_optin();
+  uint32_t cs = 0, RB = 0;
+  bool use_smem = false;
+  for (uint32_t c = 1; c <= 16; c <<= 1) {
+    if (g_proj_cs && c != g_proj_cs) continue;
+    const uint32_t rb = (t->rows + c - 1) / c;
+    if (proj_smem_bytes(rb, W) > maxsm) continue;
+    cs = c; RB = rb; use_smem = true;
+    if (g_proj_cs || rb <= 128) break;
+  }
+  const size_t sm = use_smem ? proj_smem_bytes(RB, W) : std::max<size_t>((size_t)2 * W * 8, 1024);
+  if (!use_smem) cs = g_proj_cs ? g_proj_cs : 8;
+  if (use_smem) {
+    QCB_CUDA(cudaFuncSetAttribute(project_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if (cs > 8) QCB_CUDA(cudaFuncSetAttribute(project_smem_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  } else {
+    QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if (cs > 8) QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  }
   int status = QCB_OK;
   uint32_t j0 = 0;
   std::vector<int32_t> h_anti(k, 0), h_res(k, -1);
@@ -395,7 +740,7 @@ static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(cs);
     cfg.blockDim = dim3(PROJ_THREADS);
-    cfg.dynamicSmemBytes = std::max<size_t>(sm, 1024);
+    cfg.dynamicSmemBytes = sm;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -404,7 +749,12 @@ static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    QCB_CUDA(cudaLaunchKernelEx(&cfg, project_kernel, a));
+    if (use_smem) {
+      ProjSmemArgs pa{a, RB};
+      QCB_CUDA(cudaLaunchKernelEx(&cfg, project_smem_kernel, pa));
+    } else {
+      QCB_CUDA(cudaLaunchKernelEx(&cfg, project_kernel, a));
+    }
     QCB_LAUNCHED();
     int32_t hs[2];
     QCB_CUDA(cudaMemcpyAsync(hs, d_stat, 8, cudaMemcpyDeviceToHost, st));
@@ -531,5 +881,5 @@ int qcb_projectrand(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tablea
 }  // extern "C"
 
 namespace qcb {
-void set_project_cluster(uint32_t cs) { g_proj_cs = cs ? cs : 8; }
+void set_project_cluster(uint32_t cs) { g_proj_cs = cs; }
 }

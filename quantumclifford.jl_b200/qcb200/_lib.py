@@ -91,6 +91,11 @@ class qcb_noise_source(ctypes.Structure):
     ]
 
 
+class qcb_batch_job(ctypes.Structure):
+    _fields_ = [("frame", ctypes.c_void_p), ("program", ctypes.c_void_p), ("seed", ctypes.c_uint64),
+                ("shot_offset", ctypes.c_uint64), ("tile", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
 class qcb_program_info(ctypes.Structure):
     _fields_ = [
         (name, ctypes.c_uint32)
@@ -157,6 +162,11 @@ def lib():
         "qcb_comm": ([vp, u32, vp, u32, vp, vp], ctypes.c_int),
         "qcb_canonicalize": ([vp, u32, u32, ctypes.c_int, P(i32), P(i32), vp], ctypes.c_int),
         "qcb_project": ([vp, ctypes.c_int, P(i32), vp, ctypes.c_int, ctypes.c_int, vp, vp, P(u32), vp], ctypes.c_int),
+        "qcb_batch_create": ([vp, sz, P(vp)], ctypes.c_int),
+        "qcb_batch_run": ([vp, vp], ctypes.c_int),
+        "qcb_batch_status": ([vp], ctypes.c_int),
+        "qcb_batch_destroy": ([vp], ctypes.c_int),
+        "qcb_tune_tile": ([vp, P(u32), P(ctypes.c_float), vp], ctypes.c_int),
         "qcb_frame_measurement_columns": ([vp, vp, sz, vp, vp, vp], ctypes.c_int),
         "qcb_frame_syndrome_rows": ([vp, vp, sz, vp, ctypes.c_int, vp], ctypes.c_int),
         "qcb_evaluate_guesses": ([vp, vp, sz, vp, sz, vp, P(u64), vp], ctypes.c_int),

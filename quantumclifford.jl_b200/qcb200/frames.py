@@ -17,7 +17,7 @@ import numpy as np
 
 from . import ops as _ops
 from ._lib import (
-    EVENT_DTYPE, check, ensure_init, lib, ptr, qcb_noise_source, qcb_program_info,
+    EVENT_DTYPE, check, ensure_init, lib, ptr, qcb_batch_job, qcb_noise_source, qcb_program_info,
 )
 
 QCB_NOISE_PHILOX = 0
@@ -288,3 +288,48 @@ def unpack_record(planes: np.ndarray, frames: int) -> np.ndarray:
     """Shot-packed record planes -> Bool matrix frames x nbits."""
     b = np.unpackbits(planes.view(np.uint8).reshape(planes.shape[0], -1), axis=1, bitorder="little")
     return b[:, :frames].T.astype(bool)
+
+
+class Batch:
+    """Many fresh sampling runs drained from one persistent launch
+    (qcb_batch_*).  ``jobs``: (frame, program, seed[, shot_offset[, tile]])
+    tuples; every frame gets initZ! and its circuit in Philox mode, so each
+    result equals ``pftrajectories`` of that job alone with the same seed.
+    ``run(stream)`` launches (capturable in a CUDA graph); ``status()``
+    synchronises and raises on a device-side timeout."""
+
+    def __init__(self, jobs):
+        ensure_init()
+        self.jobs = list(jobs)
+        arr = (qcb_batch_job * max(len(self.jobs), 1))()
+        for i, j in enumerate(self.jobs):
+            frame, prog, seed = j[0], j[1], j[2]
+            off = j[3] if len(j) > 3 else frame.shot_offset
+            tile = j[4] if len(j) > 4 else 0
+            arr[i] = qcb_batch_job(frame.handle, prog.handle, int(seed) & (2**64 - 1), int(off), int(tile), 0)
+        h = ctypes.c_void_p()
+        check(lib().qcb_batch_create(arr, len(self.jobs), ctypes.byref(h)))
+        self.handle = h
+
+    def run(self, stream=None):
+        check(lib().qcb_batch_run(self.handle, stream))
+        return self
+
+    def status(self):
+        check(lib().qcb_batch_status(self.handle))
+        return self
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            lib().qcb_batch_destroy(h)
+            self.handle = None
+
+
+def tune_tile(program: Program, stream=None):
+    """The autotuner (qcb_tune_tile): the fastest tile width for the program's
+    size class, recorded for later batches.  Returns (tile, us per column)."""
+    t = ctypes.c_uint32()
+    us = ctypes.c_float()
+    check(lib().qcb_tune_tile(program.handle, ctypes.byref(t), ctypes.byref(us), stream))
+    return t.value, us.value

@@ -221,3 +221,25 @@ def test_projectrand_paulis(qcb):
         want.append(r)
     assert res == want and st.rank == rank
     assert np.array_equal(st.tab.xzs, xz) and np.array_equal(st.tab.phases, ph)
+
+
+@pytest.mark.parametrize("kind", ["Destabilizer", "MixedDestabilizer"])
+def test_project_large_tableau_global_rows(qcb, kind):
+    # n = 3000: 6000 rows do not fit the cluster's shared memory, so the
+    # projections run with the rows in global memory
+    n = 3000
+    rng = np.random.default_rng(77)
+    d = dev_random_destabilizer(qcb, n, rng, depth=5)
+    st, tab, rank = make_state(qcb, kind, d, n, n - 5)
+    paulis = _random_paulis(6, n, rng)
+    paulis.xzs[2] = d.tab.xzs[n + 3]  # a stabilizer row: the commuting branch
+    st.to_gpu()
+    _, anti, res = qcb.project_(st, paulis.copy().to_gpu())
+    st.to_cpu()
+    ph, xz = tab.phases.copy(), tab.xzs.copy()
+    outs = []
+    for j in range(6):
+        s_, ph, xz, rank, a, r = oracle.project(kind, ph, xz, n, paulis.xzs[j], paulis.phases[j], rank)
+        outs.append((a, None if r < 0 else r))
+    assert list(zip(anti, res)) == outs
+    assert np.array_equal(st.tab.xzs, xz) and np.array_equal(st.tab.phases, ph)

@@ -385,6 +385,19 @@ int qcb_canonicalize_gott(qcb_tableau* t, int phases, int32_t* r, int32_t* s,
  * (new qubit j is old qubit perm[j], 1-based, nqubits entries); phases stay. */
 int qcb_permutesystems(qcb_tableau* t, const uint32_t* perm, void* stream);
 
+/* Many canonicalize! jobs on Stabilizer tableaux drained by persistent
+ * thread-block clusters (no reference counterpart), each job exactly
+ * qcb_canonicalize on that tableau.  cluster: CTAs per cluster (0 = the
+ * smallest whose shared memory holds the largest tableau).  run launches only
+ * (capturable in a CUDA graph); ranks synchronises and gives each job's rx,
+ * rz in the caller's order.  The tableaux must outlive the batch.         */
+typedef struct qcb_canon_batch qcb_canon_batch;
+int qcb_canon_batch_create(qcb_tableau* const* tabs, size_t n, int phases, uint32_t cluster,
+                           qcb_canon_batch** out);
+int qcb_canon_batch_run(qcb_canon_batch* b, void* stream);
+int qcb_canon_batch_ranks(const qcb_canon_batch* b, int32_t* rx, int32_t* rz);
+int qcb_canon_batch_destroy(qcb_canon_batch* b);
+
 /* generate!(pauli, stabilizer; phases) (src/project_trace_reset.jl:37-81) on
  * a canonical stabilizer.  Writes the remaining Pauli (identity up to phase)
  * back into `pauli`; *ok = 0 when the Pauli cannot be generated.  used_rows

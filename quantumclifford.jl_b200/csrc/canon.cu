@@ -22,6 +22,9 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
 
 #include "qcb_internal.h"
 
@@ -72,7 +75,7 @@ constexpr uint32_t CANON_THREADS = 1024;
 // (canonicalize_rref!).  Compile-time so that canonicalize! runs the lean
 // instance.
 template <bool D, bool DESC>
-__global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a) {
+__device__ __forceinline__ void canon_body(const CanonArgs& a, uint64_t* smem) {
   cg::cluster_group cl = cg::this_cluster();
   const uint32_t me = cl.block_rank();
   const uint32_t CS = cl.num_blocks();
@@ -81,7 +84,6 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a)
   const uint32_t r0 = me * a.RB;
   const uint32_t nloc = r0 < a.rows ? min(a.RB, a.rows - r0) : 0u;
 
-  extern __shared__ __align__(16) uint64_t smem[];
   uint64_t* piv = smem;                                               // W words
   uint64_t* rowsbuf = piv + W + 1;                                    // RB * WS words (smem mode)
   uint64_t* drows = rowsbuf + (a.smem_rows ? (size_t)a.RB * WS : 0);  // RB * WS words (smem mode, D)
@@ -291,6 +293,46 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a)
     a.out[0] = (int32_t)(a.mode == ELIM_BOTH ? rx : npiv);
     a.out[1] = i;
   }
+}
+
+template <bool D, bool DESC>
+__global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a) {
+  extern __shared__ __align__(16) uint64_t smem[];
+  canon_body<D, DESC>(a, smem);
+}
+
+// Many canonicalize! jobs (stabilizer tableaux) drained by persistent
+// clusters: CTA 0 of a cluster takes the next job from the queue (longest
+// first) and the cluster runs it with its rows in shared memory, then the
+// next.  The job's arguments are copied into shared memory.
+struct CanonBatchArgs {
+  const CanonArgs* jobs;
+  uint32_t njobs;
+  uint32_t* head;  // next job (zero before the launch)
+};
+static_assert(sizeof(CanonArgs) % 8 == 0, "CanonArgs is copied in 8-byte words");
+
+__global__ void __launch_bounds__(CANON_THREADS) canon_batch_kernel(const CanonBatchArgs b) {
+  extern __shared__ __align__(16) uint64_t smem[];
+  __shared__ __align__(16) CanonArgs ja;
+  __shared__ uint32_t jobid;
+  cg::cluster_group cl = cg::this_cluster();
+  const uint32_t me = cl.block_rank(), tid = threadIdx.x;
+  while (true) {
+    if (me == 0 && tid == 0) {
+      const uint32_t j = atomicAdd(b.head, 1u);
+      jobid = j < b.njobs ? j : 0xFFFFFFFFu;
+    }
+    cl.sync();
+    const uint32_t j = *cl.map_shared_rank(&jobid, 0);
+    if (j == 0xFFFFFFFFu) break;
+    for (uint32_t w = tid; w < sizeof(CanonArgs) / 8; w += blockDim.x)
+      ((uint64_t*)&ja)[w] = ((const uint64_t*)(b.jobs + j))[w];
+    __syncthreads();
+    canon_body<false, false>(ja, smem);
+    __syncthreads();  // ja is read until the end of the body
+  }
+  cl.sync();  // CTA 0's job slot is read by the cluster until here
 }
 
 // permutesystems!(s, perm) (src/linalg.jl:7-17): every row becomes row[perm]
@@ -787,6 +829,122 @@ int qcb_generate(qcb_tableau* pauli, const qcb_tableau* stab, int phases, int32_
   }
   *ok = hok;
   if (n_used) *n_used = hnu;
+  return QCB_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- batches of canonicalize!
+struct qcb_canon_batch {
+  qcb::CanonArgs* d_jobs = nullptr;
+  uint32_t* d_head = nullptr;
+  int32_t* d_out = nullptr;
+  uint32_t njobs = 0, cs = 1, clusters = 1;
+  size_t smem = 0;
+  std::vector<uint32_t> order;  // queue position -> caller's job index
+};
+
+extern "C" {
+
+int qcb_canon_batch_create(qcb_tableau* const* tabs, size_t n, int phases, uint32_t cluster, qcb_canon_batch** out) {
+  using namespace qcb;
+  if (!out || (n && !tabs)) return fail(QCB_EARG, "null argument");
+  *out = nullptr;
+  if (cluster && (cluster > 16 || (cluster & (cluster - 1)))) return fail(QCB_EARG, "cluster must be 0, 1, 2, 4, 8 or 16");
+  const size_t maxsm = (size_t)device_max_smem_optin() - sizeof(CanonArgs) - 64;
+  uint32_t maxrows = 1, maxW = 2;
+  for (size_t j = 0; j < n; j++) {
+    if (!tabs[j]) return fail(QCB_EARG, "null tableau in the batch");
+    maxrows = std::max(maxrows, tabs[j]->rows);
+    maxW = std::max(maxW, tabs[j]->W);
+  }
+  // the smallest cluster whose shared memory holds the largest job (more
+  // clusters run at once), unless one is given
+  uint32_t cs = 0;
+  for (uint32_t c = 1; c <= 16; c <<= 1) {
+    if (cluster && c != cluster) continue;
+    if (canon_smem(maxrows, maxW, (maxrows + c - 1) / c, true, false) <= maxsm) { cs = c; break; }
+  }
+  if (!cs) return fail(QCB_EUNSUPPORTED, "canonicalize! batch: the largest tableau does not fit the cluster's shared memory");
+  auto b = std::make_unique<qcb_canon_batch>();
+  b->cs = cs;
+  b->njobs = (uint32_t)n;
+  b->order.resize(n);
+  for (size_t j = 0; j < n; j++) b->order[j] = (uint32_t)j;
+  // longest first: about rows^2 * W word operations
+  std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t x, uint32_t y) {
+    const double cx = (double)tabs[x]->rows * tabs[x]->rows * tabs[x]->W;
+    const double cy = (double)tabs[y]->rows * tabs[y]->rows * tabs[y]->W;
+    return cx > cy;
+  });
+  QCB_CUDA(cudaMalloc(&b->d_out, std::max<size_t>(n, 1) * 8));
+  std::vector<CanonArgs> jobs(n);
+  size_t smem = 1024;
+  for (size_t q = 0; q < n; q++) {
+    const uint32_t j = b->order[q];
+    const qcb_tableau* t = tabs[j];
+    CanonArgs& a = jobs[q];
+    std::memset(&a, 0, sizeof(a));
+    a.xzs = t->xzs; a.ph = t->phases; a.rows = t->rows; a.n = t->nqubits; a.W = t->W;
+    a.RB = std::max<uint32_t>(1, (t->rows + cs - 1) / cs);
+    a.phases = phases; a.smem_rows = 1; a.mode = ELIM_BOTH;
+    a.out = b->d_out + 2 * j;
+    smem = std::max(smem, canon_smem(t->rows, t->W, a.RB, true, false));
+  }
+  b->smem = smem;
+  const uint32_t sms = (uint32_t)std::max(device_sm_count(), 1);
+  b->clusters = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)std::max<size_t>(n, 1), sms / cs));
+  QCB_CUDA(cudaMalloc(&b->d_jobs, std::max<size_t>(n, 1) * sizeof(CanonArgs)));
+  QCB_CUDA(cudaMalloc(&b->d_head, 4));
+  if (n) QCB_CUDA(cudaMemcpy(b->d_jobs, jobs.data(), n * sizeof(CanonArgs), cudaMemcpyHostToDevice));
+  QCB_CUDA(cudaFuncSetAttribute(canon_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (cs > 8) QCB_CUDA(cudaFuncSetAttribute(canon_batch_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  *out = b.release();
+  return QCB_OK;
+}
+
+int qcb_canon_batch_run(qcb_canon_batch* b, void* stream) {
+  using namespace qcb;
+  if (!b) return fail(QCB_EARG, "null batch");
+  if (!b->njobs) return QCB_OK;
+  cudaStream_t st = S(stream);
+  QCB_CUDA(cudaMemsetAsync(b->d_head, 0, 4, st));
+  CanonBatchArgs a{b->d_jobs, b->njobs, b->d_head};
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(b->clusters * b->cs);
+  cfg.blockDim = dim3(CANON_THREADS);
+  cfg.dynamicSmemBytes = b->smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = b->cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  QCB_CUDA(cudaLaunchKernelEx(&cfg, canon_batch_kernel, a));
+  QCB_LAUNCHED();
+  return QCB_OK;
+}
+
+int qcb_canon_batch_ranks(const qcb_canon_batch* b, int32_t* rx, int32_t* rz) {
+  using namespace qcb;
+  if (!b) return fail(QCB_EARG, "null batch");
+  std::vector<int32_t> h((size_t)b->njobs * 2);
+  if (b->njobs) QCB_CUDA(cudaMemcpy(h.data(), b->d_out, h.size() * 4, cudaMemcpyDeviceToHost));
+  for (uint32_t j = 0; j < b->njobs; j++) {
+    if (rx) rx[j] = h[2 * j];
+    if (rz) rz[j] = h[2 * j + 1];
+  }
+  return QCB_OK;
+}
+
+int qcb_canon_batch_destroy(qcb_canon_batch* b) {
+  if (!b) return QCB_OK;
+  cudaFree(b->d_jobs);
+  cudaFree(b->d_head);
+  cudaFree(b->d_out);
+  delete b;
   return QCB_OK;
 }
 

@@ -166,6 +166,10 @@ def lib():
         "qcb_batch_run": ([vp, vp], ctypes.c_int),
         "qcb_batch_status": ([vp], ctypes.c_int),
         "qcb_batch_destroy": ([vp], ctypes.c_int),
+        "qcb_canon_batch_create": ([vp, sz, ctypes.c_int, u32, P(vp)], ctypes.c_int),
+        "qcb_canon_batch_run": ([vp, vp], ctypes.c_int),
+        "qcb_canon_batch_ranks": ([vp, vp, vp], ctypes.c_int),
+        "qcb_canon_batch_destroy": ([vp], ctypes.c_int),
         "qcb_tune_tile": ([vp, P(u32), P(ctypes.c_float), vp], ctypes.c_int),
         "qcb_frame_measurement_columns": ([vp, vp, sz, vp, vp, vp], ctypes.c_int),
         "qcb_frame_syndrome_rows": ([vp, vp, sz, vp, ctypes.c_int, vp], ctypes.c_int),

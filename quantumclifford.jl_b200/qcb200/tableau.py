@@ -531,3 +531,36 @@ def tensor_pow(c: CliffordOperator, k: int) -> CliffordOperator:
                 zs[dst, b * m:(b + 1) * m] = zs0[src]
                 ph[dst] = c.tab.phases[src]
     return CliffordOperator(Tableau.from_bits(ph, xs, zs))
+
+
+class CanonBatch:
+    """Many canonicalize! jobs (Stabilizer tableaux on the device) drained by
+    persistent thread-block clusters in one launch (qcb_canon_batch_*); each
+    result equals canonicalize_ of that tableau alone.  ``run(stream)`` is
+    capturable in a CUDA graph; ``ranks()`` returns [(rx, rz)] in order."""
+
+    def __init__(self, states, *, phases: bool = True, cluster: int = 0):
+        self.states = list(states)
+        handles = (ctypes.c_void_p * max(len(self.states), 1))()
+        for i, st in enumerate(self.states):
+            handles[i] = _tab(st)._need_dev().handle
+        h = ctypes.c_void_p()
+        check(lib().qcb_canon_batch_create(handles, len(self.states), int(phases), int(cluster), ctypes.byref(h)))
+        self.handle = h
+
+    def run(self, stream=None):
+        check(lib().qcb_canon_batch_run(self.handle, stream))
+        return self
+
+    def ranks(self):
+        k = len(self.states)
+        rx = np.zeros(max(k, 1), np.int32)
+        rz = np.zeros(max(k, 1), np.int32)
+        check(lib().qcb_canon_batch_ranks(self.handle, ptr(rx), ptr(rz)))
+        return [(int(a), int(b)) for a, b in zip(rx[:k], rz[:k])]
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            lib().qcb_canon_batch_destroy(h)
+            self.handle = None

@@ -95,3 +95,35 @@ def test_batch_rejects_bad_jobs(qcb):
     with pytest.raises(qcb.QCBError):
         qcb.Batch([(small, jobs[0]["prog"], 1, 0)])  # the program needs more qubits
     assert qcb.Batch([]).run().status() is not None
+
+
+@pytest.mark.parametrize("cluster", [0, 8, 16])
+def test_canonicalize_batch_equals_single(qcb, cluster):
+    import oracle
+    from test_gpu_tableau import dev_random_destabilizer
+    from qcb200.tableau import Tableau
+
+    rng = np.random.default_rng(5 + cluster)
+    srcs, states = [], []
+    for k in range(24):
+        n = int(rng.integers(10, 700))
+        d = dev_random_destabilizer(qcb, n, rng, depth=8)
+        rows = n if k % 3 else max(1, n // 2)
+        t = Tableau(d.tab.phases[n:n + rows].copy(), n, d.tab.xzs[n:n + rows].copy())
+        srcs.append(t)
+        states.append(qcb.Stabilizer(t.copy()).to_gpu())
+    b = qcb.CanonBatch(states, cluster=cluster)
+    b.run()
+    ranks = b.ranks()
+    for st, t, (rx, rz) in zip(states, srcs, ranks):
+        st.to_cpu()
+        ph, xz, orx, orz = oracle.canonicalize(t.phases, t.xzs, t.nqubits, True)
+        assert (rx, rz) == (orx, orz)
+        assert np.array_equal(st.tab.xzs, xz) and np.array_equal(st.tab.phases, ph)
+    # a canonical tableau is a fixed point: running the batch again changes nothing
+    b.run()
+    assert b.ranks() == ranks
+    for st in states:
+        before = st.tab.xzs.copy()
+        st.to_cpu()
+        assert np.array_equal(st.tab.xzs, before)

@@ -359,6 +359,145 @@ def bench_tableau(args):
     del graph
 
 
+def bench_batch(args):
+    """The batched mixed workload: 256 rotated surface-code sampling jobs
+    (d uniform in {3,...,15}, rounds = d, p log-uniform in [1e-4, 1e-2], shots
+    log-uniform in [1e3, 1e6]) plus 512 canonicalize! jobs on random
+    stabilizers (n uniform in [100, 2000]), seeded.  Batched: one persistent
+    sampling launch and one persistent canonicalize! launch on two streams,
+    captured together in one CUDA graph, tile widths from the autotuner per
+    size class.  Plain: the same 768 jobs as per-job launches in sequence.
+    The value is frame-gate updates/s of the whole mix (all sampling updates
+    over the time of everything, canonicalize! included)."""
+    import torch
+    import numpy as np
+    import qcb200
+    from qcb200 import circuits, ops as O
+    from qcb200 import tableau as Q
+    from qcb200._lib import check, lib
+
+    qcb200.ensure_init(0)
+    L = lib()
+    rng = np.random.default_rng(0xBA7C4)
+    t_setup = time.perf_counter()
+    jobs = []
+    for k in range(256):
+        d = int(rng.choice([3, 5, 7, 9, 11, 13, 15]))
+        p = float(10 ** rng.uniform(-4, -2))
+        shots = int(round(10 ** rng.uniform(3, 6)))
+        prog = qcb200.Program(circuits.rotated_surface_code_memory(d, d, p))
+        qmax, bmax = O.affected_counts(prog.ops)
+        frame = qcb200.PauliFrame(shots, qmax, bmax, init=False)
+        jobs.append(dict(d=d, p=p, shots=shots, prog=prog, frame=frame, seed=int(rng.integers(0, 2**63))))
+    updates = sum(j["prog"].info["n_updates"] * j["shots"] for j in jobs)
+    # the autotuner: one tile width per size class (code distance)
+    tuned = {}
+    for j in jobs:
+        if j["d"] not in tuned:
+            tuned[j["d"]] = qcb200.tune_tile(j["prog"])[0]
+    fbatch = qcb200.Batch([(j["frame"], j["prog"], j["seed"], 0) for j in jobs])
+    # canonicalize! jobs: random stabilizers from seeded H/S/CNOT circuits
+    canon_n = [int(n) for n in rng.integers(100, 2001, size=512)]
+    pristine, work = [], []
+    for n in canon_n:
+        dst = Q.one_destabilizer(n).to_gpu()
+        Q.apply_(dst, Q.random_clifford_ops(n, 6, rng))
+        dst.to_cpu()
+        t = Q.Tableau(dst.tab.phases[n:].copy(), n, dst.tab.xzs[n:].copy())
+        st = Q.Stabilizer(t).to_gpu()
+        pristine.append(Q.Stabilizer(t.copy()).to_gpu())
+        work.append(st)
+    cbatch = Q.CanonBatch(work)
+    setup_s = time.perf_counter() - t_setup
+
+    def restore():
+        for w, p0 in zip(work, pristine):
+            check(L.qcb_tableau_copy(w.tab.dev.handle, p0.tab.dev.handle, None))
+
+    main = torch.cuda.current_stream()
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    n_cap = L.qcb_launch_count()
+    with torch.cuda.graph(graph):
+        cs = torch.cuda.current_stream()
+        s1.wait_stream(cs)
+        s2.wait_stream(cs)
+        fbatch.run(ctypes.c_void_p(s1.cuda_stream))
+        cbatch.run(ctypes.c_void_p(s2.cuda_stream))
+        cs.wait_stream(s1)
+        cs.wait_stream(s2)
+    torch.cuda.synchronize()
+    launches_per_replay = L.qcb_launch_count() - n_cap  # kernel nodes of the graph
+
+    def timed(fn, steps, warm):
+        ts = []
+        for i in range(warm + steps):
+            restore()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(main)
+            fn()
+            e1.record(main)
+            torch.cuda.synchronize()
+            if i >= warm:
+                ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts), ts
+
+    sp = ctypes.c_void_p(main.cuda_stream)
+
+    def plain():
+        for j in jobs:
+            check(L.qcb_pftrajectories_fresh(j["frame"].handle, j["prog"].handle, j["seed"], 0, sp))
+        for w in work:
+            check(L.qcb_canonicalize(w.tab.dev.handle, 1, len(w.tab), 1, None, None, sp))
+
+    sampler = ClockSampler(0)
+    sampler.start()
+    ms_b, _ = timed(lambda: graph.replay(), args.steps, args.warmup)
+    ms_p, _ = timed(plain, max(3, args.steps // 4), 3)
+    # the two halves alone, for the record
+    ms_f, _ = timed(lambda: fbatch.run(sp), 3, 1)
+    ms_c, _ = timed(lambda: cbatch.run(sp), 3, 1)
+    clocks = sampler.stop()
+    # every job of the last batched replay equals its plain launch: compare a sample
+    restore()
+    graph.replay()
+    torch.cuda.synchronize()
+    fbatch.status()
+    want_rank = cbatch.ranks()
+    for j in jobs[::37]:
+        rec_b = j["frame"].record_planes()
+        check(L.qcb_pftrajectories_fresh(j["frame"].handle, j["prog"].handle, j["seed"], 0, sp))
+        torch.cuda.synchronize()
+        assert np.array_equal(rec_b, j["frame"].record_planes()), "batched record differs from the plain launch"
+    for k in range(0, 512, 97):
+        work[k].to_cpu()
+        got = work[k].tab.xzs.copy()
+        check(L.qcb_tableau_copy(work[k].tab.dev.handle, pristine[k].tab.dev.handle, sp))
+        _, rx, rz = Q.canonicalize_(work[k], ranks=True)
+        work[k].to_cpu()
+        assert np.array_equal(got, work[k].tab.xzs) and (rx, rz) == want_rank[k]
+    v_b = updates / (ms_b / 1e3)
+    v_p = updates / (ms_p / 1e3)
+    out = {"metric": "frame-gate updates/s, batched mixed workload (256 surface-code circuits + 512 canonicalize!)",
+           "value": v_b, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms_b, "higher_is_better": True, "scaling": "none", "vs_baseline": None,
+           "dtype": "u32 bit planes (GF(2)) + u64 bit rows", "data": "synthetic (seeded)",
+           "config": {"workload": "256 rotated surface-code memory circuits, d in {3..15}, rounds = d, p log-U[1e-4,1e-2], "
+                                  "shots log-U[1e3,1e6] + 512 canonicalize! on random stabilizers n ~ U[100,2000]; one "
+                                  "persistent sampling launch + one persistent canonicalize! launch in one CUDA graph",
+                      "frame_updates": updates, "total_shots": sum(j["shots"] for j in jobs),
+                      "tuned_tiles": {str(k): v for k, v in sorted(tuned.items())},
+                      "l2": "no flush: the sampling jobs write ~%.1f GB of records per step" % (
+                          sum(j["prog"].info["nbits"] * j["shots"] for j in jobs) / 8e9)},
+           "gpu_launches": launches_per_replay,
+           "plain": {"value": v_p, "ms_per_step": ms_p, "launches": len(jobs) + len(work)},
+           "speedup_vs_plain": ms_p / ms_b, "sampling_alone_ms": ms_f, "canonicalize_alone_ms": ms_c,
+           "clocks": clocks, "setup_s": setup_s}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -368,7 +507,7 @@ def main():
     ap.add_argument("--shots", type=int, default=SHOTS_PER_GPU)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--walker-tile", type=int, default=0)
-    ap.add_argument("--workload", default="frames", choices=["frames", "tableau"])
+    ap.add_argument("--workload", default="frames", choices=["frames", "tableau", "batch"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -381,6 +520,10 @@ def main():
     if args.workload == "tableau":
         if rank == 0:
             bench_tableau(args)
+        return
+    if args.workload == "batch":
+        if rank == 0:
+            bench_batch(args)
         return
 
     import torch

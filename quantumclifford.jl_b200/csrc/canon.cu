@@ -835,13 +835,25 @@ int qcb_generate(qcb_tableau* pauli, const qcb_tableau* stab, int phases, int32_
 }  // extern "C"
 
 // ---------------------------------------------------------------- batches of canonicalize!
-struct qcb_canon_batch {
+// Jobs are split into size classes by the smallest cluster whose shared
+// memory holds them (a small tableau runs in one CTA with no cluster
+// barrier at all); each class is one persistent launch on its own stream,
+// forked from and joined back to the caller's stream with events, so the
+// classes share the GPU.
+struct CanonClass {
+  uint32_t cs = 1, clusters = 1, njobs = 0;
+  size_t smem = 0;
   qcb::CanonArgs* d_jobs = nullptr;
   uint32_t* d_head = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+};
+
+struct qcb_canon_batch {
+  std::vector<CanonClass> classes;
   int32_t* d_out = nullptr;
-  uint32_t njobs = 0, cs = 1, clusters = 1;
-  size_t smem = 0;
-  std::vector<uint32_t> order;  // queue position -> caller's job index
+  uint32_t njobs = 0;
+  cudaEvent_t fork = nullptr;
 };
 
 extern "C" {
@@ -852,53 +864,64 @@ int qcb_canon_batch_create(qcb_tableau* const* tabs, size_t n, int phases, uint3
   *out = nullptr;
   if (cluster && (cluster > 16 || (cluster & (cluster - 1)))) return fail(QCB_EARG, "cluster must be 0, 1, 2, 4, 8 or 16");
   const size_t maxsm = (size_t)device_max_smem_optin() - sizeof(CanonArgs) - 64;
-  uint32_t maxrows = 1, maxW = 2;
+  // the cluster of every job: the given one, else the smallest that holds it
+  std::vector<uint32_t> cs_of(n, 0);
   for (size_t j = 0; j < n; j++) {
-    if (!tabs[j]) return fail(QCB_EARG, "null tableau in the batch");
-    maxrows = std::max(maxrows, tabs[j]->rows);
-    maxW = std::max(maxW, tabs[j]->W);
-  }
-  // the smallest cluster whose shared memory holds the largest job (more
-  // clusters run at once), unless one is given
-  uint32_t cs = 0;
-  for (uint32_t c = 1; c <= 16; c <<= 1) {
-    if (cluster && c != cluster) continue;
-    if (canon_smem(maxrows, maxW, (maxrows + c - 1) / c, true, false) <= maxsm) { cs = c; break; }
-  }
-  if (!cs) return fail(QCB_EUNSUPPORTED, "canonicalize! batch: the largest tableau does not fit the cluster's shared memory");
-  auto b = std::make_unique<qcb_canon_batch>();
-  b->cs = cs;
-  b->njobs = (uint32_t)n;
-  b->order.resize(n);
-  for (size_t j = 0; j < n; j++) b->order[j] = (uint32_t)j;
-  // longest first: about rows^2 * W word operations
-  std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t x, uint32_t y) {
-    const double cx = (double)tabs[x]->rows * tabs[x]->rows * tabs[x]->W;
-    const double cy = (double)tabs[y]->rows * tabs[y]->rows * tabs[y]->W;
-    return cx > cy;
-  });
-  QCB_CUDA(cudaMalloc(&b->d_out, std::max<size_t>(n, 1) * 8));
-  std::vector<CanonArgs> jobs(n);
-  size_t smem = 1024;
-  for (size_t q = 0; q < n; q++) {
-    const uint32_t j = b->order[q];
     const qcb_tableau* t = tabs[j];
-    CanonArgs& a = jobs[q];
-    std::memset(&a, 0, sizeof(a));
-    a.xzs = t->xzs; a.ph = t->phases; a.rows = t->rows; a.n = t->nqubits; a.W = t->W;
-    a.RB = std::max<uint32_t>(1, (t->rows + cs - 1) / cs);
-    a.phases = phases; a.smem_rows = 1; a.mode = ELIM_BOTH;
-    a.out = b->d_out + 2 * j;
-    smem = std::max(smem, canon_smem(t->rows, t->W, a.RB, true, false));
+    if (!t) return fail(QCB_EARG, "null tableau in the batch");
+    for (uint32_t c = 1; c <= 16; c <<= 1) {
+      if (cluster && c != cluster) continue;
+      if (canon_smem(t->rows, t->W, std::max<uint32_t>(1, (t->rows + c - 1) / c), true, false) <= maxsm) {
+        cs_of[j] = c;
+        break;
+      }
+    }
+    if (!cs_of[j]) return fail(QCB_EUNSUPPORTED, "canonicalize! batch: a tableau does not fit the cluster's shared memory");
   }
-  b->smem = smem;
+  auto b = std::make_unique<qcb_canon_batch>();
+  b->njobs = (uint32_t)n;
+  QCB_CUDA(cudaMalloc(&b->d_out, std::max<size_t>(n, 1) * 8));
+  QCB_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
   const uint32_t sms = (uint32_t)std::max(device_sm_count(), 1);
-  b->clusters = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)std::max<size_t>(n, 1), sms / cs));
-  QCB_CUDA(cudaMalloc(&b->d_jobs, std::max<size_t>(n, 1) * sizeof(CanonArgs)));
-  QCB_CUDA(cudaMalloc(&b->d_head, 4));
-  if (n) QCB_CUDA(cudaMemcpy(b->d_jobs, jobs.data(), n * sizeof(CanonArgs), cudaMemcpyHostToDevice));
-  QCB_CUDA(cudaFuncSetAttribute(canon_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  if (cs > 8) QCB_CUDA(cudaFuncSetAttribute(canon_batch_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  for (uint32_t c = 1; c <= 16; c <<= 1) {
+    std::vector<uint32_t> ids;
+    for (size_t j = 0; j < n; j++)
+      if (cs_of[j] == c) ids.push_back((uint32_t)j);
+    if (ids.empty()) continue;
+    // longest first: about rows^2 * W word operations
+    std::stable_sort(ids.begin(), ids.end(), [&](uint32_t x, uint32_t y) {
+      return (double)tabs[x]->rows * tabs[x]->rows * tabs[x]->W > (double)tabs[y]->rows * tabs[y]->rows * tabs[y]->W;
+    });
+    CanonClass k;
+    k.cs = c;
+    k.njobs = (uint32_t)ids.size();
+    std::vector<CanonArgs> jobs(ids.size());
+    size_t smem = 1024;
+    for (size_t q = 0; q < ids.size(); q++) {
+      const qcb_tableau* t = tabs[ids[q]];
+      CanonArgs& a = jobs[q];
+      std::memset(&a, 0, sizeof(a));
+      a.xzs = t->xzs; a.ph = t->phases; a.rows = t->rows; a.n = t->nqubits; a.W = t->W;
+      a.RB = std::max<uint32_t>(1, (t->rows + c - 1) / c);
+      a.phases = phases; a.smem_rows = 1; a.mode = ELIM_BOTH;
+      a.out = b->d_out + 2 * ids[q];
+      smem = std::max(smem, canon_smem(t->rows, t->W, a.RB, true, false));
+    }
+    k.smem = smem;
+    // as many clusters as fit at once (one CTA per SM at this shared memory)
+    k.clusters = std::max<uint32_t>(1, std::min<uint32_t>(k.njobs, sms / c));
+    QCB_CUDA(cudaMalloc(&k.d_jobs, jobs.size() * sizeof(CanonArgs)));
+    QCB_CUDA(cudaMalloc(&k.d_head, 4));
+    QCB_CUDA(cudaMemcpy(k.d_jobs, jobs.data(), jobs.size() * sizeof(CanonArgs), cudaMemcpyHostToDevice));
+    QCB_CUDA(cudaStreamCreateWithFlags(&k.st, cudaStreamNonBlocking));
+    QCB_CUDA(cudaEventCreateWithFlags(&k.done, cudaEventDisableTiming));
+    b->classes.push_back(k);
+  }
+  size_t smax = 1024;
+  bool big = false;
+  for (auto& k : b->classes) { smax = std::max(smax, k.smem); big |= k.cs > 8; }
+  QCB_CUDA(cudaFuncSetAttribute(canon_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+  if (big) QCB_CUDA(cudaFuncSetAttribute(canon_batch_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   *out = b.release();
   return QCB_OK;
 }
@@ -908,22 +931,28 @@ int qcb_canon_batch_run(qcb_canon_batch* b, void* stream) {
   if (!b) return fail(QCB_EARG, "null batch");
   if (!b->njobs) return QCB_OK;
   cudaStream_t st = S(stream);
-  QCB_CUDA(cudaMemsetAsync(b->d_head, 0, 4, st));
-  CanonBatchArgs a{b->d_jobs, b->njobs, b->d_head};
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(b->clusters * b->cs);
-  cfg.blockDim = dim3(CANON_THREADS);
-  cfg.dynamicSmemBytes = b->smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = b->cs;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  QCB_CUDA(cudaLaunchKernelEx(&cfg, canon_batch_kernel, a));
-  QCB_LAUNCHED();
+  QCB_CUDA(cudaEventRecord(b->fork, st));
+  for (auto& k : b->classes) {
+    QCB_CUDA(cudaStreamWaitEvent(k.st, b->fork, 0));
+    QCB_CUDA(cudaMemsetAsync(k.d_head, 0, 4, k.st));
+    CanonBatchArgs a{k.d_jobs, k.njobs, k.d_head};
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(k.clusters * k.cs);
+    cfg.blockDim = dim3(CANON_THREADS);
+    cfg.dynamicSmemBytes = k.smem;
+    cfg.stream = k.st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = k.cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    QCB_CUDA(cudaLaunchKernelEx(&cfg, canon_batch_kernel, a));
+    QCB_LAUNCHED();
+    QCB_CUDA(cudaEventRecord(k.done, k.st));
+    QCB_CUDA(cudaStreamWaitEvent(st, k.done, 0));
+  }
   return QCB_OK;
 }
 
@@ -931,6 +960,7 @@ int qcb_canon_batch_ranks(const qcb_canon_batch* b, int32_t* rx, int32_t* rz) {
   using namespace qcb;
   if (!b) return fail(QCB_EARG, "null batch");
   std::vector<int32_t> h((size_t)b->njobs * 2);
+  QCB_CUDA(cudaDeviceSynchronize());
   if (b->njobs) QCB_CUDA(cudaMemcpy(h.data(), b->d_out, h.size() * 4, cudaMemcpyDeviceToHost));
   for (uint32_t j = 0; j < b->njobs; j++) {
     if (rx) rx[j] = h[2 * j];
@@ -941,8 +971,13 @@ int qcb_canon_batch_ranks(const qcb_canon_batch* b, int32_t* rx, int32_t* rz) {
 
 int qcb_canon_batch_destroy(qcb_canon_batch* b) {
   if (!b) return QCB_OK;
-  cudaFree(b->d_jobs);
-  cudaFree(b->d_head);
+  for (auto& k : b->classes) {
+    cudaFree(k.d_jobs);
+    cudaFree(k.d_head);
+    if (k.st) cudaStreamDestroy(k.st);
+    if (k.done) cudaEventDestroy(k.done);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
   cudaFree(b->d_out);
   delete b;
   return QCB_OK;

@@ -228,6 +228,32 @@ int qcb_batch_destroy(qcb_batch* b);
  * qcb_batch_create then uses.  Synchronises the device.                     */
 int qcb_tune_tile(const qcb_program* program, uint32_t* tile, float* us_per_column, void* stream);
 
+/* ------------------------------------------------------------ serving
+ * A request loop with continuous batching (no reference counterpart).
+ * Requests (an op list, shots, seed) are submitted at any time from any host
+ * thread; their programs are compiled once per distinct op list and stay
+ * resident.  A scheduler thread admits requests first come, first served as
+ * a slot (a CUDA stream) and the HBM budget (the full record plus one shot
+ * chunk's frame planes from a pool) allow, and runs each as a sequence of
+ * fresh Philox shot chunks of `chunk_shots` (0 = 2^20), so requests overlap
+ * on the device chunk by chunk; every record equals that of one plain run
+ * of the request (qcb_pftrajectories_fresh, same seed, shot_offset 0).
+ * Records stay on the device until qcb_server_release.                   */
+typedef struct qcb_server qcb_server;
+int qcb_server_create(uint64_t hbm_budget_bytes, uint32_t slots, uint64_t chunk_shots, qcb_server** out);
+int qcb_server_submit(qcb_server* s, const qcb_op* ops, size_t n_ops, uint64_t shots, uint64_t seed,
+                      uint64_t* ticket);
+/* state: 0 queued, 1 running, 2 done, 3 failed (the status is then the
+ * request's error); times3 (may be NULL): submit, admit and completion
+ * times in seconds since the server started.                               */
+int qcb_server_query(qcb_server* s, uint64_t ticket, int32_t* state, double* times3);
+int qcb_server_wait(qcb_server* s, uint64_t ticket, double timeout_s);
+/* The record of a finished request: nbits x ceil(shots/32) uint32 planes
+ * (host memory; may be NULL to read *nbits only).                          */
+int qcb_server_result(qcb_server* s, uint64_t ticket, uint32_t* planes, uint32_t* nbits);
+int qcb_server_release(qcb_server* s, uint64_t ticket);
+int qcb_server_destroy(qcb_server* s);
+
 /* The decoder hand-off (src/ecc/decoder_pipeline.jl:163-170).
  * measurements(frame)[:, bits]: the record columns `bits` (1-based, nsel of
  * them) as a Bool matrix S x nsel, column-major (the reference's view of the

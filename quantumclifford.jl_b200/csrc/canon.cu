@@ -534,7 +534,7 @@ static int eliminate(const ElimSpec& e, cudaStream_t st) {
   void (*kern)(const CanonArgs) =
       D ? (e.mode == ELIM_RREF ? canon_kernel<true, true> : canon_kernel<true, false>)
         : (e.mode == ELIM_RREF ? canon_kernel<false, true> : canon_kernel<false, false>);
-  QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_bytes));
+  QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin()));
   if (p.cs > 8) QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(p.cs);

@@ -37,8 +37,9 @@ struct WalkArgs {
   const uint4* prog;        // windowed stream (PROG_WINDOW_WORDS words per window)
   uint32_t nwin;            // windows in the stream
   uint32_t* planes;
-  uint32_t* rec;
+  uint32_t* rec;            // record row b at rec + b * rec_pitch (column 0 of this frame)
   uint64_t pitch;
+  uint64_t rec_pitch;
   uint64_t ncols;
   const uint32_t* slot_qubit;
   const uint32_t* slot_swap;
@@ -314,7 +315,7 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
   const uint32_t tid = threadIdx.x, T = a.tile, TP = T / 2, R = blockDim.x / TP;
   const uint32_t cp = tid % TP, rr = tid / TP, cw = 2 * cp;  // cw: tile column of the pair
   const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
-  const uint64_t pitch = a.pitch;
+  const uint64_t pitch = a.pitch, rpitch = a.rec_pitch;
   const uint64_t c0 = tile * T, cg = c0 + cw;  // the pair's first column in the frame
   const bool act = rr < R && cg < a.ncols;
   const bool two = cg + 1 < a.ncols;          // its second column exists
@@ -462,7 +463,7 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
         const uint2* en = (const uint2*)e;
         for (uint32_t j = rr; j < cnt; j += R) {
           const uint2 o = en[j];
-          *(uint2*)(a.rec + (uint64_t)o.y * pitch + cg) = *F.at2(o.x, cw, cg);
+          *(uint2*)(a.rec + (uint64_t)o.y * rpitch + cg) = *F.at2(o.x, cw, cg);
         }
         break;
       }
@@ -494,7 +495,7 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
               const uint32_t* rp = a.reset_planes + (uint64_t)ent[i].z * a.reset_pitch + cg;
               rb = a.reset_planes ? make_uint2(__ldg(rp), two ? __ldg(rp + 1) : 0u) : make_uint2(0u, 0u);
             }
-            if (ent[i].y != BIT_NONE) *(uint2*)(a.rec + (uint64_t)ent[i].y * pitch + cg) = x;
+            if (ent[i].y != BIT_NONE) *(uint2*)(a.rec + (uint64_t)ent[i].y * rpitch + cg) = x;
             *px = make_uint2(0u, 0u);
             *pz = xor2(z, rb);
           }
@@ -508,8 +509,8 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
           const uint32_t* x = e + 32 * j;  // (store, n, b_0 .. b_{n-1})
           const uint32_t n = min(x[1], XOR_MAX_BITS);
           uint2 v = make_uint2(0u, 0u);
-          for (uint32_t i = 0; i < n; i++) v = xor2(v, *(const uint2*)(a.rec + (uint64_t)x[2 + i] * pitch + cg));
-          *(uint2*)(a.rec + (uint64_t)x[0] * pitch + cg) = v;
+          for (uint32_t i = 0; i < n; i++) v = xor2(v, *(const uint2*)(a.rec + (uint64_t)x[2 + i] * rpitch + cg));
+          *(uint2*)(a.rec + (uint64_t)x[0] * rpitch + cg) = v;
         }
         break;
       }
@@ -952,7 +953,7 @@ int launch_walker(qcb_frame* f, const qcb_program* p, WalkArgs& a, bool philox, 
   if (wc.smem) kern = philox ? walker_kernel<true, true> : walker_kernel<true, false>;
   else kern = philox ? walker_kernel<false, true> : walker_kernel<false, false>;
   if (wc.smem_bytes > 48 * 1024)
-    QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wc.smem_bytes));
+    QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin()));
   kern<<<wc.grid, wc.nth, wc.smem_bytes, st>>>(a);
   QCB_LAUNCHED();
   return QCB_OK;
@@ -964,6 +965,7 @@ static void fill_common(WalkArgs& a, qcb_frame* f, const qcb_program* p) {
   a.planes = f->planes;
   a.rec = f->record;
   a.pitch = f->pitch;
+  a.rec_pitch = f->pitch;
   a.ncols = f->ncols;
   a.slot_qubit = p->d_slot_qubit;
   a.slot_swap = p->d_slot_swap;
@@ -1275,7 +1277,7 @@ int qcb_batch_create(const qcb_batch_job* jobs, size_t n_jobs, qcb_batch** out) 
   QCB_CUDA(cudaMalloc(&b->d_head, 4));
   if (!wa.empty()) QCB_CUDA(cudaMemcpy(b->d_jobs, wa.data(), wa.size() * sizeof(WalkArgs), cudaMemcpyHostToDevice));
   if (!it.empty()) QCB_CUDA(cudaMemcpy(b->d_items, it.data(), it.size() * sizeof(BatchItem), cudaMemcpyHostToDevice));
-  QCB_CUDA(cudaFuncSetAttribute(batch_walker_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_bytes));
+  QCB_CUDA(cudaFuncSetAttribute(batch_walker_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin() - 1024));
   *out = b.release();
   return QCB_OK;
 }
@@ -1359,3 +1361,28 @@ int qcb_tune_tile(const qcb_program* p, uint32_t* tile_out, float* us_per_column
 }
 
 }  // extern "C"
+
+// One shot chunk of a fresh Philox run for the serving loop: `f` holds the
+// chunk's planes (its own record is not used), `ncols` columns of it are
+// walked, and the chunk's record rows go to rec + b * rec_pitch (the chunk's
+// columns of the request's full record).  Counters use the global column,
+// so the chunks of a request give the record of one run over all its shots.
+namespace qcb {
+int run_chunk(qcb_frame* f, uint64_t ncols, const qcb_program* p, uint64_t seed, uint64_t shot_offset, uint32_t* rec,
+              uint64_t rec_pitch, cudaStream_t st) {
+  if (!f || !p || !rec) return fail(QCB_EARG, "null argument");
+  if (p->nq > f->nq1) return fail(QCB_EBOUNDS, "program uses more qubits than the chunk frame has");
+  if (ncols > f->ncols) return fail(QCB_EBOUNDS, "chunk wider than its frame");
+  if (shot_offset % NOISE_GROUP) return fail(QCB_EARG, "chunk shot_offset must be a multiple of 1024");
+  qcb_frame view = *f;
+  view.ncols = ncols;
+  view.frames = ncols * 32;
+  WalkArgs a;
+  fill_common(a, &view, p);
+  a.rec = rec;
+  a.rec_pitch = rec_pitch;
+  a.seed = seed;
+  a.col0 = shot_offset / 32;
+  return launch_walker(&view, p, a, true, true, st);
+}
+}  // namespace qcb

@@ -721,10 +721,10 @@ static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64
   const size_t sm = use_smem ? proj_smem_bytes(RB, W) : std::max<size_t>((size_t)2 * W * 8, 1024);
   if (!use_smem) cs = g_proj_cs ? g_proj_cs : 8;
   if (use_smem) {
-    QCB_CUDA(cudaFuncSetAttribute(project_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    QCB_CUDA(cudaFuncSetAttribute(project_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin()));
     if (cs > 8) QCB_CUDA(cudaFuncSetAttribute(project_smem_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   } else {
-    QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin()));
     if (cs > 8) QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   }
   int status = QCB_OK;

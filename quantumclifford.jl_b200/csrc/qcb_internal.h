@@ -171,6 +171,11 @@ struct qcb_frame {
   int32_t* err;      // device status word of the walker (QCB_ETIMEOUT on a stuck wait)
 };
 
+namespace qcb {
+int run_chunk(qcb_frame* f, uint64_t ncols, const qcb_program* p, uint64_t seed, uint64_t shot_offset, uint32_t* rec,
+              uint64_t rec_pitch, cudaStream_t st);
+}  // namespace qcb
+
 struct qcb_tableau {
   uint32_t rows;
   uint32_t nqubits;

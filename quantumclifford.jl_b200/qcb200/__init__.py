@@ -18,7 +18,7 @@ from .ops import (  # noqa: F401
 )
 from .frames import (  # noqa: F401
     PauliFrame, Program, Masks, sample_masks, pftrajectories, pauliframe_, measurements,
-    pftrajectories_record, unpack_record, evaluate_guesses, Batch, tune_tile,
+    pftrajectories_record, unpack_record, evaluate_guesses, Batch, tune_tile, Server,
 )
 from .tableau import (  # noqa: F401
     Tableau, PauliOperator, Stabilizer, MixedStabilizer, Destabilizer, MixedDestabilizer, CliffordOperator,

@@ -170,6 +170,13 @@ def lib():
         "qcb_canon_batch_run": ([vp, vp], ctypes.c_int),
         "qcb_canon_batch_ranks": ([vp, vp, vp], ctypes.c_int),
         "qcb_canon_batch_destroy": ([vp], ctypes.c_int),
+        "qcb_server_create": ([u64, u32, u64, P(vp)], ctypes.c_int),
+        "qcb_server_submit": ([vp, vp, sz, u64, u64, P(u64)], ctypes.c_int),
+        "qcb_server_query": ([vp, u64, P(i32), vp], ctypes.c_int),
+        "qcb_server_wait": ([vp, u64, ctypes.c_double], ctypes.c_int),
+        "qcb_server_result": ([vp, u64, vp, P(u32)], ctypes.c_int),
+        "qcb_server_release": ([vp, u64], ctypes.c_int),
+        "qcb_server_destroy": ([vp], ctypes.c_int),
         "qcb_tune_tile": ([vp, P(u32), P(ctypes.c_float), vp], ctypes.c_int),
         "qcb_frame_measurement_columns": ([vp, vp, sz, vp, vp, vp], ctypes.c_int),
         "qcb_frame_syndrome_rows": ([vp, vp, sz, vp, ctypes.c_int, vp], ctypes.c_int),

@@ -333,3 +333,53 @@ def tune_tile(program: Program, stream=None):
     us = ctypes.c_float()
     check(lib().qcb_tune_tile(program.handle, ctypes.byref(t), ctypes.byref(us), stream))
     return t.value, us.value
+
+
+class Server:
+    """The serving loop (qcb_server_*): submit sampling requests at any time;
+    a scheduler thread admits them against an HBM budget and a number of
+    slots and runs them chunk by chunk with continuous batching.  Each
+    request's record equals one plain fresh run with the same seed."""
+
+    def __init__(self, hbm_budget_bytes: int, slots: int = 8, chunk_shots: int = 0):
+        ensure_init()
+        h = ctypes.c_void_p()
+        check(lib().qcb_server_create(int(hbm_budget_bytes), int(slots), int(chunk_shots), ctypes.byref(h)))
+        self.handle = h
+
+    def submit(self, circuit, shots: int, seed: int) -> int:
+        arr = _ops.to_array(circuit)
+        t = ctypes.c_uint64()
+        check(lib().qcb_server_submit(self.handle, ptr(arr) if len(arr) else None, len(arr), int(shots),
+                                      int(seed) & (2**64 - 1), ctypes.byref(t)))
+        return t.value
+
+    def query(self, ticket: int):
+        """(state, (t_submit, t_admit, t_done)); state 0 queued, 1 running, 2 done."""
+        st = ctypes.c_int32()
+        times = np.zeros(3, np.float64)
+        check(lib().qcb_server_query(self.handle, int(ticket), ctypes.byref(st), ptr(times)))
+        return st.value, tuple(float(x) for x in times)
+
+    def wait(self, ticket: int, timeout: float = 600.0):
+        check(lib().qcb_server_wait(self.handle, int(ticket), float(timeout)))
+
+    def result(self, ticket: int, shots: int) -> np.ndarray:
+        nb = ctypes.c_uint32()
+        check(lib().qcb_server_result(self.handle, int(ticket), None, ctypes.byref(nb)))
+        out = np.empty((nb.value, (shots + 31) // 32), dtype=np.uint32)
+        if out.size:
+            check(lib().qcb_server_result(self.handle, int(ticket), ptr(out), ctypes.byref(nb)))
+        return out
+
+    def release(self, ticket: int):
+        check(lib().qcb_server_release(self.handle, int(ticket)))
+
+    def close(self):
+        h = getattr(self, "handle", None)
+        if h:
+            lib().qcb_server_destroy(h)
+            self.handle = None
+
+    def __del__(self):
+        self.close()

@@ -1,0 +1,97 @@
+"""GPU tests of the serving loop (qcb_server_*): requests submitted while
+others run are admitted as slots and memory free up, overlap on the device
+chunk by chunk, and each result is bit-identical alone and in the mix (and to
+the plain fresh run of the same request)."""
+import threading
+
+import numpy as np
+import pytest
+
+from qcb200 import circuits, ops as O
+
+pytestmark = pytest.mark.gpu
+
+
+def plain_record(qcb, circ, shots, seed):
+    prog = qcb.Program(circ)
+    qmax, bmax = O.affected_counts(prog.ops)
+    f = qcb.PauliFrame(shots, qmax, bmax, init=False)
+    qcb.check(qcb.lib().qcb_pftrajectories_fresh(f.handle, prog.handle, seed, 0, None))
+    return f.record_planes()
+
+
+def requests(rng, n, dmax=7, smax=5.3):
+    out = []
+    for _ in range(n):
+        d = int(rng.choice([x for x in (3, 5, 7, 9, 11) if x <= dmax]))
+        p = float(10 ** rng.uniform(-4, -2))
+        out.append((circuits.rotated_surface_code_memory(d, d, p), int(10 ** rng.uniform(2, smax)),
+                    int(rng.integers(0, 2**63))))
+    return out
+
+
+def test_results_same_alone_and_in_the_mix(qcb):
+    rng = np.random.default_rng(1)
+    reqs = requests(rng, 12)
+    srv = qcb.Server(hbm_budget_bytes=8 << 30, slots=4, chunk_shots=8192)
+    tickets = [srv.submit(c, s, seed) for c, s, seed in reqs]
+    for t in tickets:
+        srv.wait(t)
+    mixed = [srv.result(t, s) for t, (c, s, seed) in zip(tickets, reqs)]
+    for t in tickets:
+        srv.release(t)
+    # alone: one request at a time through the same server, and the plain launch
+    for (c, s, seed), m in zip(reqs[:5], mixed[:5]):
+        t = srv.submit(c, s, seed)
+        srv.wait(t)
+        assert np.array_equal(srv.result(t, s), m)
+        srv.release(t)
+    for (c, s, seed), m in zip(reqs, mixed):
+        assert np.array_equal(plain_record(qcb, c, s, seed), m)
+    srv.close()
+
+
+def test_admission_waits_for_memory_and_keeps_order(qcb):
+    rng = np.random.default_rng(2)
+    reqs = requests(rng, 6, dmax=5, smax=4.5)
+    # a budget that holds about one request at a time
+    srv = qcb.Server(hbm_budget_bytes=24 << 20, slots=4, chunk_shots=4096)
+    tickets = [srv.submit(c, s, seed) for c, s, seed in reqs]
+    admits = []
+    for t in tickets:
+        srv.wait(t)
+        admits.append(srv.query(t)[1][1])
+        srv.release(t)  # frees the record: the next one can be admitted
+    assert admits == sorted(admits)  # first come, first served
+    srv.close()
+
+
+def test_request_larger_than_budget_fails(qcb):
+    srv = qcb.Server(hbm_budget_bytes=1 << 20, slots=2)
+    t = srv.submit(circuits.rotated_surface_code_memory(5, 5, 1e-3), 200_000, 1)
+    with pytest.raises(qcb.QCBError):
+        srv.wait(t)
+    srv.release(t)
+    srv.close()
+
+
+def test_submissions_from_many_threads(qcb):
+    rng = np.random.default_rng(3)
+    reqs = requests(rng, 16, dmax=5, smax=4.0)
+    srv = qcb.Server(hbm_budget_bytes=4 << 30, slots=6, chunk_shots=2048)
+    tickets = [None] * len(reqs)
+
+    def worker(i):
+        c, s, seed = reqs[i]
+        tickets[i] = srv.submit(c, s, seed)
+
+    ths = [threading.Thread(target=worker, args=(i,)) for i in range(len(reqs))]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    for t, (c, s, seed) in zip(tickets, reqs):
+        srv.wait(t)
+        assert np.array_equal(srv.result(t, s), plain_record(qcb, c, s, seed))
+        srv.release(t)
+    srv.close()

@@ -243,11 +243,16 @@ typedef struct qcb_server qcb_server;
 int qcb_server_create(uint64_t hbm_budget_bytes, uint32_t slots, uint64_t chunk_shots, qcb_server** out);
 int qcb_server_submit(qcb_server* s, const qcb_op* ops, size_t n_ops, uint64_t shots, uint64_t seed,
                       uint64_t* ticket);
+/* Compile an op list into the resident program cache without running it.  */
+int qcb_server_preload(qcb_server* s, const qcb_op* ops, size_t n_ops);
 /* state: 0 queued, 1 running, 2 done, 3 failed (the status is then the
  * request's error); times3 (may be NULL): submit, admit and completion
  * times in seconds since the server started.                               */
 int qcb_server_query(qcb_server* s, uint64_t ticket, int32_t* state, double* times3);
 int qcb_server_wait(qcb_server* s, uint64_t ticket, double timeout_s);
+/* The next request that finished or failed and was not reported yet, in
+ * completion order (blocks up to timeout_s; QCB_ETIMEOUT when none did).    */
+int qcb_server_next_done(qcb_server* s, double timeout_s, uint64_t* ticket, int32_t* state, double* times3);
 /* The record of a finished request: nbits x ceil(shots/32) uint32 planes
  * (host memory; may be NULL to read *nbits only).                          */
 int qcb_server_result(qcb_server* s, uint64_t ticket, uint32_t* planes, uint32_t* nbits);

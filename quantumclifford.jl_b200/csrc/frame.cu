@@ -913,7 +913,7 @@ static uint32_t balanced_tile(uint64_t ncols, uint32_t tmax) {
   return (uint32_t)std::min<uint64_t>(tmax, std::max<uint64_t>(t, 16));
 }
 
-// Shared-memory tile when 2 planes x 32 columns of every touched qubit fit,
+// Shared-memory tile when 2 planes x 16 columns of every touched qubit fit,
 // else the same walker on the HBM planes.
 static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   WalkConfig wc{};
@@ -924,7 +924,7 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   uint32_t T = 0;
   if (g_tile_override && per_col * g_tile_override <= budget) {
     T = g_tile_override;
-  } else if (budget / per_col >= 32) {
+  } else if (budget / per_col >= 16) {
     T = balanced_tile(f->ncols, (uint32_t)std::min<size_t>(256, budget / per_col));
   }
   if (T) {

@@ -6,7 +6,9 @@
 // the op bytes).  Admission is first come, first served against an HBM
 // budget and a number of slots: the head of the queue is admitted as soon as
 // a slot is free and its memory (the full record, plus one chunk's frame
-// planes from a pool) fits the budget.  An admitted request runs on its
+// planes) fits the budget.  Device memory comes from the stream-ordered
+// allocator (cudaMallocAsync / cudaFreeAsync on the slot's stream), so the
+// scheduler thread never waits for the device.  An admitted request runs on its
 // slot's stream as a sequence of shot chunks (fresh Philox runs with the
 // chunk's global shot offset, each writing its columns of the request's
 // record), so requests admitted while others run share the GPU chunk by
@@ -39,7 +41,7 @@ struct Request {
   uint64_t nbits = 0, ncols = 0, rec_pitch = 0;
   uint64_t bytes = 0;           // record + chunk planes charged to the budget
   uint32_t* record = nullptr;
-  qcb_frame* chunk = nullptr;   // from the pool
+  qcb_frame* chunk = nullptr;   // the chunk frame (its planes live while the chunks run)
   int slot = -1;
   cudaEvent_t done = nullptr;
   double t_submit = 0, t_admit = 0, t_done = 0;
@@ -66,9 +68,9 @@ struct qcb_server {
   std::vector<int64_t> slot_req;  // request id per slot, -1 when free
   std::map<uint64_t, std::unique_ptr<qcb::Request>> reqs;
   std::deque<uint64_t> queue;
+  std::deque<uint64_t> completed;  // finished or failed, not yet reported by next_done
   std::unordered_map<uint64_t, qcb_program*> programs;
-  std::multimap<uint32_t, qcb_frame*> pool;  // free chunk frames by qubits + 1
-  uint64_t pool_bytes = 0;
+  int32_t* slot_status = nullptr;  // pinned: each slot's last walker status word
   uint64_t next_id = 1;
   std::mutex mu;
   std::condition_variable cv;   // wakes the scheduler
@@ -117,28 +119,43 @@ static void admit(qcb_server* s) {
       r.msg = "serving: the request needs more device memory than the server's budget";
       r.t_done = s->now();
       s->queue.pop_front();
+      s->completed.push_back(r.id);
       s->done_cv.notify_all();
       continue;
     }
     if (s->used + r.bytes > s->budget) return;  // first come, first served: wait for memory
     const uint32_t nq1 = std::max<uint32_t>(r.prog->nq, 1);
     cudaStream_t st = s->streams[slot];
-    // chunk frame from the pool, else a new one
-    auto pit = s->pool.find(nq1);
-    if (pit != s->pool.end()) {
-      r.chunk = pit->second;
-      s->pool.erase(pit);
-      s->pool_bytes -= chunk_plane_bytes(nq1, s->chunk_cols);
-    } else if (qcb_frame_create(s->chunk_cols * 32, nq1 - 1, 0, &r.chunk) != QCB_OK) {
-      r.chunk = nullptr;
-    }
-    cudaError_t e = r.chunk ? cudaMallocAsync(&r.record, r.nbits * r.rec_pitch * 4, st) : cudaErrorMemoryAllocation;
+    // the chunk frame: planes for one chunk, allocated and freed in stream
+    // order (no device-wide synchronisation on the scheduler thread)
+    qcb_frame* cf = new qcb_frame();
+    cf->frames = s->chunk_cols * 32;
+    cf->qubits = nq1 - 1;
+    cf->nq1 = nq1;
+    cf->nbits = 0;
+    cf->ncols = s->chunk_cols;
+    cf->pitch = std::max<uint64_t>(32, (s->chunk_cols + 31) / 32 * 32);
+    cf->planes = nullptr;
+    cf->record = nullptr;
+    cf->err = nullptr;
+    r.chunk = cf;
+    cudaError_t e = cudaMallocAsync(&cf->planes, (size_t)2 * (nq1 + 1) * cf->pitch * 4, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&cf->err, 16, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cf->err, 0, 16, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&r.record, r.nbits * r.rec_pitch * 4, st);
     if (e == cudaSuccess && !r.done) e = cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming);
     int status = e == cudaSuccess ? QCB_OK : cuda_fail(e, "serving: admission");
     for (uint64_t c0 = 0; status == QCB_OK && c0 < r.ncols; c0 += s->chunk_cols) {
       const uint64_t nc = std::min<uint64_t>(s->chunk_cols, r.ncols - c0);
       status = run_chunk(r.chunk, nc, r.prog, r.seed, c0 * 32, r.record + c0, r.rec_pitch, st);
     }
+    if (status == QCB_OK &&
+        cudaMemcpyAsync(&s->slot_status[slot], cf->err, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      status = fail(QCB_ECUDA, "serving: status copy");
+    if (cf->planes) cudaFreeAsync(cf->planes, st);
+    if (cf->err) cudaFreeAsync(cf->err, st);
+    cf->planes = nullptr;
+    cf->err = nullptr;
     if (status == QCB_OK && cudaEventRecord(r.done, st) != cudaSuccess) status = fail(QCB_ECUDA, "serving: event");
     s->queue.pop_front();
     r.t_admit = s->now();
@@ -146,8 +163,10 @@ static void admit(qcb_server* s) {
       r.msg = last_msg();
       if (r.record) cudaFreeAsync(r.record, st);
       r.record = nullptr;
-      if (r.chunk) { qcb_frame_destroy(r.chunk); r.chunk = nullptr; }
+      delete r.chunk;
+      r.chunk = nullptr;
       r.state = RQ_FAILED; r.status = status; r.t_done = s->now();
+      s->completed.push_back(r.id);
       s->done_cv.notify_all();
       continue;
     }
@@ -159,7 +178,8 @@ static void admit(qcb_server* s) {
 }
 
 // Retire the running requests whose last chunk has finished (lock held):
-// their chunk frames go back to the pool, their records stay until released.
+// their chunk planes were freed in stream order, their records stay until
+// released.
 static void retire(qcb_server* s) {
   for (uint32_t k = 0; k < s->nslots; k++) {
     if (s->slot_req[k] < 0) continue;
@@ -172,32 +192,20 @@ static void retire(qcb_server* s) {
       r.status = cuda_fail(q, "serving: request");
       r.msg = last_msg();
     }
-    int32_t h = 0;
-    if (r.state == RQ_DONE && cudaMemcpy(&h, r.chunk->err, 4, cudaMemcpyDeviceToHost) == cudaSuccess && h) {
+    const int32_t h = *(volatile int32_t*)&s->slot_status[k];  // copied in stream order before the event
+    if (r.state == RQ_DONE && h) {
       r.state = RQ_FAILED;
       r.status = h;
       r.msg = "serving: a device-side wait of the frame walker expired; the record is not valid";
     }
-    const uint32_t nq1 = r.chunk->nq1;
-    if (r.state == RQ_DONE) {
-      s->pool.emplace(nq1, r.chunk);
-      s->pool_bytes += chunk_plane_bytes(nq1, s->chunk_cols);
-    } else {
-      qcb_frame_destroy(r.chunk);
-    }
+    delete r.chunk;
     r.chunk = nullptr;
     // the chunk planes leave the request's charge; the record stays charged
     s->used -= chunk_plane_bytes(std::max<uint32_t>(r.prog->nq, 1), s->chunk_cols);
     r.bytes -= chunk_plane_bytes(std::max<uint32_t>(r.prog->nq, 1), s->chunk_cols);
     s->slot_req[k] = -1;
+    s->completed.push_back(r.id);
     s->done_cv.notify_all();
-  }
-  // pooled chunk frames beyond what the budget leaves free are freed
-  while (!s->pool.empty() && s->used + s->pool_bytes > s->budget) {
-    auto it = s->pool.begin();
-    s->pool_bytes -= chunk_plane_bytes(it->first, s->chunk_cols);
-    qcb_frame_destroy(it->second);
-    s->pool.erase(it);
   }
 }
 
@@ -233,6 +241,8 @@ int qcb_server_create(uint64_t hbm_budget_bytes, uint32_t slots, uint64_t chunk_
   s->nslots = slots;
   s->chunk_cols = (chunk_shots ? chunk_shots : (uint64_t)1 << 20) / 32;
   s->slot_req.assign(slots, -1);
+  QCB_CUDA(cudaHostAlloc(&s->slot_status, 64 * sizeof(int32_t), cudaHostAllocDefault));
+  std::memset(s->slot_status, 0, 64 * sizeof(int32_t));
   for (uint32_t k = 0; k < slots; k++) {
     cudaStream_t st;
     QCB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -288,6 +298,22 @@ int qcb_server_submit(qcb_server* s, const qcb_op* ops, size_t n_ops, uint64_t s
   return QCB_OK;
 }
 
+// Compile a circuit into the resident program cache without running it.
+int qcb_server_preload(qcb_server* s, const qcb_op* ops, size_t n_ops) {
+  if (!s || (n_ops && !ops)) return fail(QCB_EARG, "null argument");
+  std::vector<qcb_op> v(ops, ops + n_ops);
+  const uint64_t h = ops_hash(v);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->programs.count(h)) return QCB_OK;
+  }
+  qcb_program* p = nullptr;
+  if (int st = qcb_program_compile(v.data(), v.size(), &p)) return st;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->programs.emplace(h, p).second) qcb_program_destroy(p);
+  return QCB_OK;
+}
+
 // state: 0 queued, 1 running, 2 done, 3 failed; times (seconds since the
 // server started): submit, admit, done.
 int qcb_server_query(qcb_server* s, uint64_t ticket, int32_t* state, double* times3) {
@@ -299,6 +325,26 @@ int qcb_server_query(qcb_server* s, uint64_t ticket, int32_t* state, double* tim
   if (state) *state = r.state;
   if (times3) { times3[0] = r.t_submit; times3[1] = r.t_admit; times3[2] = r.t_done; }
   return r.state == RQ_FAILED ? fail(r.status, r.msg) : QCB_OK;
+}
+
+// The next request that finished (or failed) and has not been reported yet,
+// in completion order; blocks up to timeout_s.  state and times3 as for
+// qcb_server_query.  QCB_ETIMEOUT when none finished in time.
+int qcb_server_next_done(qcb_server* s, double timeout_s, uint64_t* ticket, int32_t* state, double* times3) {
+  if (!s || !ticket) return fail(QCB_EARG, "null argument");
+  std::unique_lock<std::mutex> lk(s->mu);
+  if (!s->done_cv.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return !s->completed.empty(); }))
+    return fail(QCB_ETIMEOUT, "serving: no request finished within the timeout");
+  const uint64_t id = s->completed.front();
+  s->completed.pop_front();
+  *ticket = id;
+  auto it = s->reqs.find(id);
+  if (it != s->reqs.end()) {
+    const Request& r = *it->second;
+    if (state) *state = r.state;
+    if (times3) { times3[0] = r.t_submit; times3[1] = r.t_admit; times3[2] = r.t_done; }
+  }
+  return QCB_OK;
 }
 
 int qcb_server_wait(qcb_server* s, uint64_t ticket, double timeout_s) {
@@ -344,6 +390,8 @@ int qcb_server_release(qcb_server* s, uint64_t ticket) {
       s->used -= r.bytes;
     }
     if (r.done) cudaEventDestroy(r.done);
+    for (auto c = s->completed.begin(); c != s->completed.end(); ++c)
+      if (*c == ticket) { s->completed.erase(c); break; }  // released without being reported
     s->reqs.erase(it);
   }
   s->cv.notify_all();  // memory freed: the scheduler may admit
@@ -361,10 +409,10 @@ int qcb_server_destroy(qcb_server* s) {
   for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
   for (auto& kv : s->reqs) {
     if (kv.second->record) cudaFree(kv.second->record);
-    if (kv.second->chunk) qcb_frame_destroy(kv.second->chunk);
+    delete kv.second->chunk;
     if (kv.second->done) cudaEventDestroy(kv.second->done);
   }
-  for (auto& kv : s->pool) qcb_frame_destroy(kv.second);
+  if (s->slot_status) cudaFreeHost(s->slot_status);
   for (auto& kv : s->programs) qcb_program_destroy(kv.second);
   for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
   delete s;

@@ -172,7 +172,9 @@ def lib():
         "qcb_canon_batch_destroy": ([vp], ctypes.c_int),
         "qcb_server_create": ([u64, u32, u64, P(vp)], ctypes.c_int),
         "qcb_server_submit": ([vp, vp, sz, u64, u64, P(u64)], ctypes.c_int),
+        "qcb_server_preload": ([vp, vp, sz], ctypes.c_int),
         "qcb_server_query": ([vp, u64, P(i32), vp], ctypes.c_int),
+        "qcb_server_next_done": ([vp, ctypes.c_double, P(u64), P(i32), vp], ctypes.c_int),
         "qcb_server_wait": ([vp, u64, ctypes.c_double], ctypes.c_int),
         "qcb_server_result": ([vp, u64, vp, P(u32)], ctypes.c_int),
         "qcb_server_release": ([vp, u64], ctypes.c_int),

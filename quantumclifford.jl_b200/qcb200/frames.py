@@ -354,12 +354,26 @@ class Server:
                                       int(seed) & (2**64 - 1), ctypes.byref(t)))
         return t.value
 
+    def preload(self, circuit):
+        """Compile a circuit into the resident program cache."""
+        arr = _ops.to_array(circuit)
+        check(lib().qcb_server_preload(self.handle, ptr(arr) if len(arr) else None, len(arr)))
+
     def query(self, ticket: int):
         """(state, (t_submit, t_admit, t_done)); state 0 queued, 1 running, 2 done."""
         st = ctypes.c_int32()
         times = np.zeros(3, np.float64)
         check(lib().qcb_server_query(self.handle, int(ticket), ctypes.byref(st), ptr(times)))
         return st.value, tuple(float(x) for x in times)
+
+    def next_done(self, timeout: float = 600.0):
+        """(ticket, state, (t_submit, t_admit, t_done)) of the next request to
+        finish, in completion order (blocks without holding the GIL)."""
+        t = ctypes.c_uint64()
+        st = ctypes.c_int32()
+        times = np.zeros(3, np.float64)
+        check(lib().qcb_server_next_done(self.handle, float(timeout), ctypes.byref(t), ctypes.byref(st), ptr(times)))
+        return t.value, st.value, tuple(float(x) for x in times)
 
     def wait(self, ticket: int, timeout: float = 600.0):
         check(lib().qcb_server_wait(self.handle, int(ticket), float(timeout)))

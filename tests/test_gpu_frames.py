@@ -145,11 +145,13 @@ def test_classical_xor_chains_bit_exact(qcb):
     assert np.array_equal(coding(f.xzs(), f.qubits + 1), coding(ox, f.qubits + 1))
 
 
-def test_tall_frame_uses_hbm_walker_bit_exact(qcb):
-    # more touched qubits than a shared-memory tile of 64 columns can hold
+@pytest.mark.parametrize("nq", [1200, 3000])
+def test_tall_frames_bit_exact(qcb, nq):
+    # 1200 touched qubits: a narrow shared-memory tile (16..22 columns);
+    # 3000: more than a 16-column tile holds, so the walker runs on the HBM planes
     rng = np.random.default_rng(9)
-    circ = random_circuit(1200, 3000, rng, p=0.02)
-    circ += [O.sCNOT(q, q + 1) for q in range(1, 1200, 2)]
+    circ = random_circuit(nq, 3000, rng, p=0.02)
+    circ += [O.sCNOT(q, q + 1) for q in range(1, nq, 2)]
     f, ox, om = run_mask(qcb, circ, 700, seed=9)
     assert np.array_equal(f.measurements(), om)
     assert np.array_equal(coding(f.xzs(), f.qubits + 1), coding(ox, f.qubits + 1))

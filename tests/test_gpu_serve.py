@@ -95,3 +95,22 @@ def test_submissions_from_many_threads(qcb):
         assert np.array_equal(srv.result(t, s), plain_record(qcb, c, s, seed))
         srv.release(t)
     srv.close()
+
+
+def test_next_done_reports_each_request_once(qcb):
+    rng = np.random.default_rng(6)
+    reqs = requests(rng, 10, dmax=5, smax=4.0)
+    srv = qcb.Server(hbm_budget_bytes=2 << 30, slots=3, chunk_shots=2048)
+    tickets = {srv.submit(c, s, seed): (c, s, seed) for c, s, seed in reqs}
+    seen = []
+    for _ in range(len(reqs)):
+        t, st, times = srv.next_done(60.0)
+        assert st == 2 and times[0] <= times[1] <= times[2]
+        c, s, seed = tickets[t]
+        assert np.array_equal(srv.result(t, s), plain_record(qcb, c, s, seed))
+        srv.release(t)
+        seen.append(t)
+    assert sorted(seen) == sorted(tickets)
+    with pytest.raises(qcb.QCBError):
+        srv.next_done(0.05)  # nothing left to report
+    srv.close()

@@ -221,142 +221,158 @@ def bench_tableau(args):
             out.update(extra)
         print(json.dumps(out), flush=True)
 
+    only = set(x for x in (args.tableau_only or "").split(",") if x)
+
+    def want(name):
+        return not only or name in only
+
     def random_destabilizer(n, depth=12):
         d = Q.one_destabilizer(n).to_gpu()
         Q.apply_(d, Q.random_clifford_ops(n, depth, rng))
         d.to_cpu()
         return d
 
-    # ---- mul_left! of two 1e9-qubit Paulis (HBM: read 2 x 250 MB, write 250 MB)
-    n = 10**9
-    W = Q.nwords(n)
-    rx = rng.integers(0, 2**64, size=(1, W), dtype=np.uint64)
-    lx = rng.integers(0, 2**64, size=(1, W), dtype=np.uint64)
-    r = Q.Tableau(np.array([1], np.uint8), n, rx).to_gpu()
-    l = Q.Tableau(np.array([2], np.uint8), n, lx).to_gpu()
-    ms = device_ms(lambda: check(L.qcb_mul_left_pauli(r.dev.handle, l.dev.handle, 1, None, sp)), args.steps)
-    # correctness of one call against the oracle on a 1e8-qubit slice (X and Z halves)
-    m = 10**8
-    Wm = Q.nwords(m)
-    a = Q.Tableau(np.array([1], np.uint8), m, rx[:, :Wm].copy()).to_gpu()
-    b = Q.Tableau(np.array([2], np.uint8), m, lx[:, :Wm].copy()).to_gpu()
-    Q.mul_left_(a, b)
-    a.to_cpu()
-    ox, oph = oracle.mul_left_pauli(rx[0, :Wm], 1, lx[0, :Wm], 2)
-    assert np.array_equal(a.xzs[0], ox) and int(a.phases[0]) == oph
-    cpu = cpu_ms(lambda: oracle.mul_left_pauli(rx[0, :Wm], 1, lx[0, :Wm], 2)) * (n / m)
-    traffic = 3 * W * 8
-    emit("mul_left! of two 1e9-qubit Paulis", "mul_left", ms,
-         {"workload": "mul_left! r <- l * r, n = 1e9 qubits (250 MB per Pauli), phases on", "l2": "750 MB > L2"},
-         cpu, {"roofline": {"bound": "hbm", "achieved": traffic / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                            "frac": traffic / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
-                            "algorithmic_bytes_per_launch": traffic}})
-    del r, l, a, b
+    if want("mul_left"):
+        # ---- mul_left! of two 1e9-qubit Paulis (HBM: read 2 x 250 MB, write 250 MB)
+        n = 10**9
+        W = Q.nwords(n)
+        rx = rng.integers(0, 2**64, size=(1, W), dtype=np.uint64)
+        lx = rng.integers(0, 2**64, size=(1, W), dtype=np.uint64)
+        r = Q.Tableau(np.array([1], np.uint8), n, rx).to_gpu()
+        l = Q.Tableau(np.array([2], np.uint8), n, lx).to_gpu()
+        ms = device_ms(lambda: check(L.qcb_mul_left_pauli(r.dev.handle, l.dev.handle, 1, None, sp)), args.steps)
+        # correctness of one call against the oracle on a 1e8-qubit slice (X and Z halves)
+        m = 10**8
+        Wm = Q.nwords(m)
+        a = Q.Tableau(np.array([1], np.uint8), m, rx[:, :Wm].copy()).to_gpu()
+        b = Q.Tableau(np.array([2], np.uint8), m, lx[:, :Wm].copy()).to_gpu()
+        Q.mul_left_(a, b)
+        a.to_cpu()
+        ox, oph = oracle.mul_left_pauli(rx[0, :Wm], 1, lx[0, :Wm], 2)
+        assert np.array_equal(a.xzs[0], ox) and int(a.phases[0]) == oph
+        cpu = cpu_ms(lambda: oracle.mul_left_pauli(rx[0, :Wm], 1, lx[0, :Wm], 2)) * (n / m)
+        traffic = 3 * W * 8
+        emit("mul_left! of two 1e9-qubit Paulis", "mul_left", ms,
+             {"workload": "mul_left! r <- l * r, n = 1e9 qubits (250 MB per Pauli), phases on", "l2": "750 MB > L2"},
+             cpu, {"roofline": {"bound": "hbm", "achieved": traffic / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                                "frac": traffic / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+                                "algorithmic_bytes_per_launch": traffic}})
+        del r, l, a, b
 
-    # ---- canonicalize! of random full-rank stabilizers
-    for n in (1000, 2000, 4000):
+    if want("canonicalize"):
+        # ---- canonicalize! of random full-rank stabilizers
+        for n in (1000, 2000, 4000):
+            d = random_destabilizer(n)
+            src = Q.Tableau(d.tab.phases[n:].copy(), n, d.tab.xzs[n:].copy())
+            work = Q.Tableau(src.phases.copy(), n, src.xzs.copy()).to_gpu()
+            pristine = Q.DeviceTableau(n, n)
+            pristine.upload(src.phases, src.xzs)
+            ms = device_ms(lambda: check(L.qcb_canonicalize(work.dev.handle, 1, n, 1, None, None, sp)), args.steps,
+                           setup=lambda: check(L.qcb_tableau_copy(work.dev.handle, pristine.handle, sp)))
+            work.to_cpu()
+            oph, oxz, _, _ = oracle.canonicalize(src.phases, src.xzs, n)
+            assert np.array_equal(work.xzs, oxz) and np.array_equal(work.phases, oph)
+            cpu = cpu_ms(lambda: oracle.canonicalize(src.phases, src.xzs, n), reps=1 if n > 2000 else 3)
+            emit(f"canonicalize! of a random {n}-qubit stabilizer", f"canonicalize_{n}", ms,
+                 {"workload": f"canonicalize!(random_stabilizer({n})), phases on", "rows": n}, cpu)
+
+    if want("project"):
+        # ---- project! of 1000 random Paulis in sequence on a random 1000-qubit Destabilizer
+        n, k = 1000, 1000
+        d = random_destabilizer(n)
+        xs = np.zeros((k, n), bool)
+        zs = np.zeros((k, n), bool)
+        for i in range(k):
+            w = int(rng.integers(1, n + 1))
+            q = rng.choice(n, w, replace=False)
+            kinds = rng.integers(1, 4, size=w)
+            xs[i, q] = kinds & 1 == 1
+            zs[i, q] = kinds & 2 == 2
+        P = Q.Tableau.from_bits(np.zeros(k, np.uint8), xs, zs).to_gpu()
+        state = Q.Destabilizer(Q.Tableau(d.tab.phases.copy(), n, d.tab.xzs.copy())).to_gpu()
+        pristine = Q.DeviceTableau(2 * n, n)
+        pristine.upload(d.tab.phases, d.tab.xzs)
+        rank = ctypes.c_int32(0)
+        anti = np.zeros(k, np.int32)
+        res = np.zeros(k, np.int32)
+        done = ctypes.c_uint32()
+        ms = device_ms(lambda: check(L.qcb_project(state.tab.dev.handle, Q.KIND["Destabilizer"], ctypes.byref(rank),
+                                                   P.dev.handle, 1, 1, ptr(anti), ptr(res), ctypes.byref(done), sp)),
+                       max(3, args.steps // 4), setup=lambda: check(L.qcb_tableau_copy(state.tab.dev.handle, pristine.handle, sp)))
+        # oracle: the same sequence
+        def oracle_chain():
+            ph, xz = d.tab.phases.copy(), d.tab.xzs.copy()
+            outs = []
+            for i in range(k):
+                st, ph, xz, _, a_, r_ = oracle.project("Destabilizer", ph, xz, n, P.xzs[i], 0)
+                outs.append((a_, r_))
+            return outs
+        t0 = time.perf_counter()
+        outs = oracle_chain()
+        cpu = (time.perf_counter() - t0) * 1e3 / k
+        assert [o[0] for o in outs] == list(anti) and [o[1] for o in outs] == list(res)
+        emit("project! of a random Pauli on a random 1000-qubit Destabilizer", "project", ms / k,
+             {"workload": "1000 random Paulis (weight ~ U{1..n}) projected in sequence by one call, per projection",
+              "rows": 2 * n}, cpu)
+
+    if want("dense_apply"):
+        # ---- dense apply! of tensor_pow(tCNOT, 500) to a random 1000-qubit stabilizer
+        n = 1000
         d = random_destabilizer(n)
         src = Q.Tableau(d.tab.phases[n:].copy(), n, d.tab.xzs[n:].copy())
         work = Q.Tableau(src.phases.copy(), n, src.xzs.copy()).to_gpu()
         pristine = Q.DeviceTableau(n, n)
         pristine.upload(src.phases, src.xzs)
-        ms = device_ms(lambda: check(L.qcb_canonicalize(work.dev.handle, 1, n, 1, None, None, sp)), args.steps,
+        c = Q.tensor_pow(Q.tCNOT(), 500).to_gpu()
+        ms = device_ms(lambda: check(L.qcb_apply_dense(work.dev.handle, c.tab.dev.handle, 1, sp)), args.steps,
                        setup=lambda: check(L.qcb_tableau_copy(work.dev.handle, pristine.handle, sp)))
         work.to_cpu()
-        oph, oxz, _, _ = oracle.canonicalize(src.phases, src.xzs, n)
+        oph, oxz = oracle.apply_dense(src.phases, src.xzs, n, c.tab.phases, c.tab.xzs)
         assert np.array_equal(work.xzs, oxz) and np.array_equal(work.phases, oph)
-        cpu = cpu_ms(lambda: oracle.canonicalize(src.phases, src.xzs, n), reps=1 if n > 2000 else 3)
-        emit(f"canonicalize! of a random {n}-qubit stabilizer", f"canonicalize_{n}", ms,
-             {"workload": f"canonicalize!(random_stabilizer({n})), phases on", "rows": n}, cpu)
+        cpu = cpu_ms(lambda: oracle.apply_dense(src.phases, src.xzs, n, c.tab.phases, c.tab.xzs))
+        emit("dense apply! of tensor_pow(tCNOT, 500) to a random 1000-qubit stabilizer", "dense_apply", ms,
+             {"workload": "apply!(random_stabilizer(1000), tensor_pow(tCNOT, 500)), phases on"}, cpu)
 
-    # ---- project! of 1000 random Paulis in sequence on a random 1000-qubit Destabilizer
-    n, k = 1000, 1000
-    d = random_destabilizer(n)
-    xs = np.zeros((k, n), bool)
-    zs = np.zeros((k, n), bool)
-    for i in range(k):
-        w = int(rng.integers(1, n + 1))
-        q = rng.choice(n, w, replace=False)
-        kinds = rng.integers(1, 4, size=w)
-        xs[i, q] = kinds & 1 == 1
-        zs[i, q] = kinds & 2 == 2
-    P = Q.Tableau.from_bits(np.zeros(k, np.uint8), xs, zs).to_gpu()
-    state = Q.Destabilizer(Q.Tableau(d.tab.phases.copy(), n, d.tab.xzs.copy())).to_gpu()
-    pristine = Q.DeviceTableau(2 * n, n)
-    pristine.upload(d.tab.phases, d.tab.xzs)
-    rank = ctypes.c_int32(0)
-    anti = np.zeros(k, np.int32)
-    res = np.zeros(k, np.int32)
-    done = ctypes.c_uint32()
-    ms = device_ms(lambda: check(L.qcb_project(state.tab.dev.handle, Q.KIND["Destabilizer"], ctypes.byref(rank),
-                                               P.dev.handle, 1, 1, ptr(anti), ptr(res), ctypes.byref(done), sp)),
-                   max(3, args.steps // 4), setup=lambda: check(L.qcb_tableau_copy(state.tab.dev.handle, pristine.handle, sp)))
-    # oracle: the same sequence
-    def oracle_chain():
-        ph, xz = d.tab.phases.copy(), d.tab.xzs.copy()
-        outs = []
-        for i in range(k):
-            st, ph, xz, _, a_, r_ = oracle.project("Destabilizer", ph, xz, n, P.xzs[i], 0)
-            outs.append((a_, r_))
-        return outs
-    t0 = time.perf_counter()
-    outs = oracle_chain()
-    cpu = (time.perf_counter() - t0) * 1e3 / k
-    assert [o[0] for o in outs] == list(anti) and [o[1] for o in outs] == list(res)
-    emit("project! of a random Pauli on a random 1000-qubit Destabilizer", "project", ms / k,
-         {"workload": "1000 random Paulis (weight ~ U{1..n}) projected in sequence by one call, per projection",
-          "rows": 2 * n}, cpu)
-
-    # ---- dense apply! of tensor_pow(tCNOT, 500) to a random 1000-qubit stabilizer
-    n = 1000
-    d = random_destabilizer(n)
-    src = Q.Tableau(d.tab.phases[n:].copy(), n, d.tab.xzs[n:].copy())
-    work = Q.Tableau(src.phases.copy(), n, src.xzs.copy()).to_gpu()
-    pristine = Q.DeviceTableau(n, n)
-    pristine.upload(src.phases, src.xzs)
-    c = Q.tensor_pow(Q.tCNOT(), 500).to_gpu()
-    ms = device_ms(lambda: check(L.qcb_apply_dense(work.dev.handle, c.tab.dev.handle, 1, sp)), args.steps,
-                   setup=lambda: check(L.qcb_tableau_copy(work.dev.handle, pristine.handle, sp)))
-    work.to_cpu()
-    oph, oxz = oracle.apply_dense(src.phases, src.xzs, n, c.tab.phases, c.tab.xzs)
-    assert np.array_equal(work.xzs, oxz) and np.array_equal(work.phases, oph)
-    cpu = cpu_ms(lambda: oracle.apply_dense(src.phases, src.xzs, n, c.tab.phases, c.tab.xzs))
-    emit("dense apply! of tensor_pow(tCNOT, 500) to a random 1000-qubit stabilizer", "dense_apply", ms,
-         {"workload": "apply!(random_stabilizer(1000), tensor_pow(tCNOT, 500)), phases on"}, cpu)
-
-    # ---- symbolic sCNOT(32, 504) on a random 1000-qubit stabilizer: the time
-    # per call of a stream of calls (as a repeated apply! is timed on the
-    # CPU), the K launches replayed from one CUDA graph so that the Python
-    # call overhead is not in the timed region; the isolated call, host
-    # overhead included, is reported beside it
-    from qcb200 import ops as O
-    gate = O.to_array([O.sCNOT(32, 504)])
-    check(L.qcb_tableau_copy(work.dev.handle, pristine.handle, sp))
-    single = device_ms(lambda: check(L.qcb_apply_gates(work.dev.handle, ptr(gate), 1, 1, sp)), max(args.steps, 50))
-    check(L.qcb_tableau_copy(work.dev.handle, pristine.handle, sp))
-    torch.cuda.synchronize()
-    K = 1000  # even: sCNOT applied twice is the identity, so the state comes back
-    graph = torch.cuda.CUDAGraph()
-    n_before = L.qcb_launch_count()
-    with torch.cuda.graph(graph):
-        cs = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-        for _ in range(K):
-            check(L.qcb_apply_gates(work.dev.handle, ptr(gate), 1, 1, cs))
-    per_graph = L.qcb_launch_count() - n_before
-    ms = device_ms(lambda: graph.replay(), max(3, args.steps // 4)) / K
-    work.to_cpu()
-    assert np.array_equal(work.xzs, src.xzs) and np.array_equal(work.phases, src.phases)
-    check(L.qcb_apply_gates(work.dev.handle, ptr(gate), 1, 1, sp))
-    work.to_cpu()
-    oph, oxz = oracle.apply_gates(src.phases, src.xzs, n, gate)
-    assert np.array_equal(work.xzs, oxz) and np.array_equal(work.phases, oph)
-    cpu = cpu_ms(lambda: oracle.apply_gates(src.phases, src.xzs, n, gate), reps=20)
-    emit("symbolic apply! of sCNOT(32, 504) to a random 1000-qubit stabilizer", "sCNOT", ms,
-         {"workload": "apply!(random_stabilizer(1000), sCNOT(32, 504)), per call of 1000 calls replayed from one "
-                      "CUDA graph (one kernel launch each)"}, cpu,
-         {"gpu_launches": per_graph, "single_call_ms": single,
-          "single_call_note": "one call between CUDA events, Python ctypes overhead included"})
-    del graph
+    if want("sCNOT"):
+        n = 1000
+        d = random_destabilizer(n)
+        src = Q.Tableau(d.tab.phases[n:].copy(), n, d.tab.xzs[n:].copy())
+        work = Q.Tableau(src.phases.copy(), n, src.xzs.copy()).to_gpu()
+        pristine = Q.DeviceTableau(n, n)
+        pristine.upload(src.phases, src.xzs)
+        # ---- symbolic sCNOT(32, 504) on a random 1000-qubit stabilizer: the time
+        # per call of a stream of calls (as a repeated apply! is timed on the
+        # CPU), the K launches replayed from one CUDA graph so that the Python
+        # call overhead is not in the timed region; the isolated call, host
+        # overhead included, is reported beside it
+        from qcb200 import ops as O
+        gate = O.to_array([O.sCNOT(32, 504)])
+        check(L.qcb_tableau_copy(work.dev.handle, pristine.handle, sp))
+        single = device_ms(lambda: check(L.qcb_apply_gates(work.dev.handle, ptr(gate), 1, 1, sp)), max(args.steps, 50))
+        check(L.qcb_tableau_copy(work.dev.handle, pristine.handle, sp))
+        torch.cuda.synchronize()
+        K = 1000  # even: sCNOT applied twice is the identity, so the state comes back
+        graph = torch.cuda.CUDAGraph()
+        n_before = L.qcb_launch_count()
+        with torch.cuda.graph(graph):
+            cs = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+            for _ in range(K):
+                check(L.qcb_apply_gates(work.dev.handle, ptr(gate), 1, 1, cs))
+        per_graph = L.qcb_launch_count() - n_before
+        ms = device_ms(lambda: graph.replay(), max(3, args.steps // 4)) / K
+        work.to_cpu()
+        assert np.array_equal(work.xzs, src.xzs) and np.array_equal(work.phases, src.phases)
+        check(L.qcb_apply_gates(work.dev.handle, ptr(gate), 1, 1, sp))
+        work.to_cpu()
+        oph, oxz = oracle.apply_gates(src.phases, src.xzs, n, gate)
+        assert np.array_equal(work.xzs, oxz) and np.array_equal(work.phases, oph)
+        cpu = cpu_ms(lambda: oracle.apply_gates(src.phases, src.xzs, n, gate), reps=20)
+        emit("symbolic apply! of sCNOT(32, 504) to a random 1000-qubit stabilizer", "sCNOT", ms,
+             {"workload": "apply!(random_stabilizer(1000), sCNOT(32, 504)), per call of 1000 calls replayed from one "
+                          "CUDA graph (one kernel launch each)"}, cpu,
+             {"gpu_launches": per_graph, "single_call_ms": single,
+              "single_call_note": "one call between CUDA events, Python ctypes overhead included"})
+        del graph
 
 
 def bench_batch(args):
@@ -609,6 +625,7 @@ def main():
     ap.add_argument("--walker-tile", type=int, default=0)
     ap.add_argument("--workload", default="frames", choices=["frames", "tableau", "batch", "serve"])
     ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--tableau-only", default="", help="comma list of mul_left,canonicalize,project,dense_apply,sCNOT")
     ap.add_argument("--serve-rates", default="25,50,100")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -724,7 +724,7 @@ static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64
     QCB_CUDA(cudaFuncSetAttribute(project_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin()));
     if (cs > 8) QCB_CUDA(cudaFuncSetAttribute(project_smem_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   } else {
-    QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin()));
+    QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin() - 1024));  // it has static shared memory too
     if (cs > 8) QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   }
   int status = QCB_OK;

@@ -297,7 +297,8 @@ int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t see
                              uint64_t shot_offset, void* stream);
 
 /* Launch-shape overrides used by the tuner ("walker_tile", "canon_threads",
- * "canon_cluster", "project_cluster"); 0 restores the automatic choice.    */
+ * "canon_cluster", "project_cluster", "canon_blocked": 1 always / 2 never
+ * run canonicalize! by 64-column panels); 0 restores the automatic choice. */
 int qcb_tune_set(const char* key, int64_t value);
 
 /* ------------------------------------------------------------ tableaux    */

@@ -454,6 +454,387 @@ __global__ void __launch_bounds__(1024) generate_kernel(uint64_t* pauli, uint8_t
   for (uint32_t w = tid; w < W; w += blockDim.x) pauli[w] = p[w];
 }
 
+// ---------------------------------------------------------------------------
+// Blocked canonicalize! (X stage then Z stage, no destabilizer rows): the
+// columns are taken in panels of 64.  Per panel:
+//   1. after a cluster barrier every CTA gathers the panel's word of every
+//      row (its own rows from shared memory, the others' through distributed
+//      shared memory) and runs the panel's pivot steps on those words alone,
+//      redundantly in every CTA, so the pivot search needs no cluster
+//      barrier: per column the first row at position >= i with the bit, a
+//      logical row swap, and the panel word of every other row with the bit
+//      XORed with the pivot's.  Each row also keeps which of the panel's
+//      pivot rows (as they were at the panel start) it has absorbed (a
+//      64-bit mask), and each step records the pivot's mask A_t and panel
+//      word;
+//   2. every CTA fetches the panel's pivot rows as they were at the panel
+//      start (full rows) and their phases;
+//   3. after a second cluster barrier every CTA applies the panel to its own
+//      rows: a row's final bits are its start bits XOR the pivot rows of its
+//      mask, and its phase is replayed exactly.  With q = phase + |x & z|
+//      (mod 4) a product L*R has q = q_L + q_R + 2 (z_L . x_R), and z_L . x_R
+//      of two XOR-combinations of start rows is a bilinear form: with
+//      C[a][b] = z_a . x_b over the pivot rows and u_m[a] = z_a . x_m,
+//      z_pivot . x_m = parity(D_t & mask_m) ^ parity(u_m & A_t) where D_t is
+//      the XOR of the C rows in A_t.  The pivots' own q at their steps come
+//      from a triangular recurrence solved by one thread.
+// The row products therefore equal the reference's mul_left! sequence bit
+// for bit, phases included, for any rows (commuting or not).
+constexpr uint32_t PANEL = 64;
+
+struct BlockedLayout {
+  size_t rows_off, pw_off, comb_off, po_off, xt_off, cml_off, c_off, a_off, pwp_off, d_off;  // u64 offsets
+  size_t pos_off, stp_off;                                                                 // u32 offsets
+  size_t bt_off, qo_off, qp_off, lph_off, ql_off;                                          // byte offsets
+  size_t u32_base, u8_base, bytes;
+};
+
+__host__ __device__ inline BlockedLayout blocked_layout(uint32_t rows, uint32_t W, uint32_t RB, bool smem_rows) {
+  BlockedLayout L{};
+  size_t o = 0;
+  L.rows_off = o; o += smem_rows ? (size_t)RB * (W + 1) : 0;
+  L.pw_off = o;
+  L.comb_off = o;
+  L.po_off = o; o += (size_t)PANEL * W;
+  L.xt_off = o; o += (size_t)PANEL * (W / 2);
+  L.cml_off = o; o += RB;
+  L.c_off = o; o += PANEL;
+  L.a_off = o; o += PANEL;
+  L.pwp_off = o; o += PANEL;
+  L.d_off = o; o += PANEL;
+  L.u32_base = o * 8;
+  size_t u = 0;
+  L.pos_off = u; u += rows;
+  L.stp_off = u; u += PANEL;
+  L.u8_base = L.u32_base + u * 4;
+  size_t b = 0;
+  L.bt_off = b; b += PANEL;
+  L.qo_off = b; b += PANEL;
+  L.qp_off = b; b += PANEL;
+  L.lph_off = b; b += RB;
+  L.ql_off = b; b += RB;
+  L.bytes = (L.u8_base + b + 15) / 16 * 16;
+  return L;
+}
+
+template <uint32_t RPT>
+__global__ void __launch_bounds__(CANON_THREADS) canon_blocked_kernel(const CanonArgs a) {
+  cg::cluster_group cl = cg::this_cluster();
+  const uint32_t me = cl.block_rank();
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5, bd = blockDim.x;
+  const uint32_t R = a.rows, n = a.n, W = a.W, len = W / 2, WS = W + 1, RB = a.RB;
+  const uint32_t r0 = me * RB;
+  const uint32_t nloc = r0 < R ? min(RB, R - r0) : 0u;
+  extern __shared__ __align__(16) uint64_t smem[];
+  const BlockedLayout Lo = blocked_layout(R, W, RB, a.smem_rows != 0);
+  uint64_t* rowsbuf = smem + Lo.rows_off;
+  uint64_t* PO = smem + Lo.po_off;
+  uint64_t* XT = smem + Lo.xt_off;   // XT[w * PANEL + t] = X word w of pivot row t
+  uint64_t* cml = smem + Lo.cml_off; // per local row: its mask of pivot rows in this panel
+  uint64_t* C = smem + Lo.c_off;
+  uint64_t* A = smem + Lo.a_off;
+  uint64_t* PWP = smem + Lo.pwp_off;
+  uint64_t* Dt = smem + Lo.d_off;
+  uint32_t* u32b = (uint32_t*)((uint8_t*)smem + Lo.u32_base);
+  uint32_t* pos = u32b + Lo.pos_off;
+  uint32_t* stp = u32b + Lo.stp_off;
+  uint8_t* u8b = (uint8_t*)smem + Lo.u8_base;
+  uint8_t* bt = u8b + Lo.bt_off;
+  uint8_t* qo = u8b + Lo.qo_off;
+  uint8_t* qp = u8b + Lo.qp_off;
+  uint8_t* lph = u8b + Lo.lph_off;
+  uint8_t* ql = u8b + Lo.ql_off;     // per local row: its q after the panel
+
+  // per search warp and column parity: its best (position << 32 | row), that
+  // row's panel word and mask
+  __shared__ uint64_t red2[2][32][3];
+  __shared__ uint32_t shT, shI;     // the search warps' step count and next position
+  __shared__ uint64_t Us[PANEL];   // pivot t's updates before its own step
+  __shared__ uint8_t bases[PANEL];
+  auto ROW = [&](uint32_t lr) -> uint64_t* {
+    return a.smem_rows ? rowsbuf + (size_t)lr * WS : a.xzs + (size_t)(r0 + lr) * W;
+  };
+  // word w of physical row r, wherever it lives
+  auto RWORD = [&](uint32_t r, uint32_t w) -> uint64_t {
+    if (!a.smem_rows) return a.xzs[(size_t)r * W + w];
+    const uint32_t o = r / RB, lr = r - o * RB;
+    const uint64_t* src = rowsbuf + (size_t)lr * WS + w;
+    return o == me ? *src : *cl.map_shared_rank(src, o);
+  };
+
+  for (uint32_t lr = tid; lr < nloc; lr += bd) lph[lr] = a.ph[r0 + lr];
+  if (a.smem_rows)
+    for (uint32_t lr = warp; lr < nloc; lr += nwarps)
+      for (uint32_t w = lane; w < W; w += 32) rowsbuf[(size_t)lr * WS + w] = a.xzs[(size_t)(r0 + lr) * W + w];
+  // the panel's pivot search runs on the first NB warps only, each thread
+  // owning rows tid, tid + nbt, ... (at most RPT) whose positions, panel
+  // words and masks it keeps in registers; named barrier 1 synchronises them
+  const uint32_t NB = min(nwarps, max(1u, (R + 32 * RPT - 1) / (32 * RPT))), nbt = NB * 32;
+  uint32_t rpos[RPT];
+  uint64_t rpw[RPT], rcb[RPT];
+#pragma unroll
+  for (uint32_t k = 0; k < RPT; k++) { rpos[k] = tid + k * nbt; rpw[k] = 0; rcb[k] = 0; }
+
+  uint32_t i = 0, rx = 0;
+  for (uint32_t stage = 0; stage < 2; stage++) {
+    for (uint32_t c0 = 0; c0 < n && i < R; c0 += PANEL) {
+      const uint32_t ncp = min(PANEL, n - c0), wj = stage * len + (c0 >> 6);
+      cl.sync();  // every row is final for this panel (and every CTA is done with the last one)
+      // ---- 1. the panel words of all rows; the panel's pivot steps
+      if (warp < NB) {
+#pragma unroll
+        for (uint32_t k = 0; k < RPT; k++) {
+          const uint32_t r = tid + k * nbt;
+          rpw[k] = r < R ? RWORD(r, wj) : 0ull;
+          rcb[k] = 0;
+        }
+      }
+      // One block barrier per column: every thread evaluates its rows (after
+      // applying the previous step to them), each warp publishes its best
+      // (position, row), and after the barrier every warp reduces the
+      // published pairs itself.  Each row's owner thread moves its own row
+      // (pos[] is per row, nothing else tracks positions); the pivot's owner
+      // records the step for the panel application.
+      uint32_t T = 0;
+      if (warp < NB) {
+        bool prev = false;
+        uint32_t pprev = 0, bprev = 0;
+        uint64_t pwprev = 0, aprev = 0;
+        for (uint32_t b = 0; b < ncp && i < R; b++) {
+          uint32_t bpos = 0xFFFFFFFFu, bk = 0;
+#pragma unroll
+          for (uint32_t k = 0; k < RPT; k++) {
+            const uint32_t r = tid + k * nbt;
+            if (r >= R) continue;
+            if (prev && r != pprev && ((rpw[k] >> bprev) & 1ull)) {  // the previous step's elimination
+              rpw[k] ^= pwprev;
+              rcb[k] ^= aprev;
+            }
+            if (rpos[k] >= i && ((rpw[k] >> b) & 1ull) && rpos[k] < bpos) { bpos = rpos[k]; bk = k; }
+          }
+          {
+            uint64_t mypw = 0, mycb = 0;
+#pragma unroll
+            for (uint32_t k = 0; k < RPT; k++)
+              if (k == bk) { mypw = rpw[k]; mycb = rcb[k]; }
+            const uint32_t m = __reduce_min_sync(0xFFFFFFFFu, bpos);
+            const uint32_t who = __ballot_sync(0xFFFFFFFFu, bpos == m);
+            const uint32_t src = __ffs(who) - 1;
+            const uint32_t row = __shfl_sync(0xFFFFFFFFu, tid + bk * nbt, src);
+            const uint64_t wpw = __shfl_sync(0xFFFFFFFFu, mypw, src);
+            const uint64_t wcb = __shfl_sync(0xFFFFFFFFu, mycb, src);
+            if (lane == 0) {
+              red2[b & 1][warp][0] = ((uint64_t)m << 32) | row;
+              red2[b & 1][warp][1] = wpw;
+              red2[b & 1][warp][2] = wcb;
+            }
+          }
+          // the only barrier of the column: the buffer of column b + 2 is
+          // written after every search warp has passed the barrier of b + 1
+          asm volatile("bar.sync 1, %0;" ::"r"(nbt) : "memory");
+          const uint64_t e = lane < NB ? red2[b & 1][lane][0] : ~0ull;
+          const uint32_t kpos = __reduce_min_sync(0xFFFFFFFFu, (uint32_t)(e >> 32));
+          if (kpos == 0xFFFFFFFFu) {  // no row has the bit: no pivot in this column
+            prev = false;
+            continue;
+          }
+          const uint32_t kw = __ffs(__ballot_sync(0xFFFFFFFFu, (uint32_t)(e >> 32) == kpos)) - 1;
+          const uint32_t pstar = (uint32_t)red2[b & 1][kw][0];
+          pwprev = red2[b & 1][kw][1];
+          aprev = red2[b & 1][kw][2] | (1ull << T);
+          // rowswap!(state, k, i): the rows at positions kpos and i trade places
+#pragma unroll
+          for (uint32_t k = 0; k < RPT; k++) {
+            const uint32_t r = tid + k * nbt;
+            if (r == pstar) rpos[k] = i;
+            else if (r < R && rpos[k] == i) rpos[k] = kpos;
+          }
+          if (tid == 0) {
+            stp[T] = pstar;
+            bt[T] = (uint8_t)b;
+            A[T] = aprev;
+            PWP[T] = pwprev;
+          }
+          prev = true;
+          pprev = pstar;
+          bprev = b;
+          T++;
+          i++;
+        }
+        if (tid == 0) { shT = T; shI = i; }
+      }
+      __syncthreads();  // the step records and the last positions are written
+      T = shT;
+      i = shI;
+      if (T == 0) continue;  // no pivot in this panel: nothing to apply
+      // ---- 2. the pivot rows as they were at the panel start, their q
+      for (uint32_t t = warp; t < T; t += nwarps) {
+        const uint32_t r = stp[t];
+        uint32_t s = 0;
+        for (uint32_t w = lane; w < W; w += 32) {
+          const uint64_t v = RWORD(r, w);
+          PO[(size_t)t * W + w] = v;
+          if (w < len) XT[(size_t)w * PANEL + t] = v;
+        }
+        __syncwarp();
+        for (uint32_t w = lane; w < len; w += 32) s += __popcll(PO[(size_t)t * W + w] & PO[(size_t)t * W + len + w]);
+        s = __reduce_add_sync(0xFFFFFFFFu, s);
+        if (lane == 0) {
+          const uint32_t o = r / RB, lr = r - o * RB;
+          const uint8_t ph0 = o == me ? lph[lr] : *cl.map_shared_rank(lph + lr, o);
+          qo[t] = (uint8_t)((ph0 + s) & 3u);
+        }
+      }
+      __syncthreads();
+      // C[a] bit b = z_a . x_b over the pivot rows: lane b reads the
+      // transposed X words (conflict-free), z_a is a broadcast
+      for (uint32_t t = warp; t < T; t += nwarps) {
+        const uint64_t* za = PO + (size_t)t * W + len;
+        uint32_t p0 = 0, p1 = 0;
+        for (uint32_t w = 0; w < len; w++) {
+          const uint64_t zw = za[w];
+          p0 += __popcll(zw & XT[(size_t)w * PANEL + lane]);
+          p1 += __popcll(zw & XT[(size_t)w * PANEL + lane + 32]);
+        }
+        const uint32_t lo = __ballot_sync(0xFFFFFFFFu, (p0 & 1u) && lane < T);
+        const uint32_t hi = __ballot_sync(0xFFFFFFFFu, (p1 & 1u) && lane + 32 < T);
+        if (lane == 0) C[t] = (uint64_t)lo | ((uint64_t)hi << 32);
+      }
+      __syncthreads();
+      if (a.phases) {
+        // D_t = XOR of the C rows in A_t; then for each pivot its updates
+        // before its own step give q_t = base_t + (sum of q_t' over them)
+        if (tid < T) {
+          uint64_t d = 0;
+          for (uint32_t x = 0; x < T; x++)
+            if ((A[tid] >> x) & 1ull) d ^= C[x];
+          Dt[tid] = d;
+        }
+        __syncthreads();
+        if (tid < T) {
+          const uint32_t t = tid;
+          uint64_t u = 0;  // u[x] = z_x . x_(pivot t) = C[x] bit t
+          for (uint32_t x = 0; x < T; x++) u |= ((C[x] >> t) & 1ull) << x;
+          uint64_t pw = PO[(size_t)t * W + wj], cm = 0, ut = 0;
+          uint32_t cross = 0;
+          for (uint32_t t2 = 0; t2 < t; t2++) {
+            if ((pw >> bt[t2]) & 1ull) {
+              cross += (uint32_t)((__popcll(Dt[t2] & cm) + __popcll(u & A[t2])) & 1);
+              ut |= 1ull << t2;
+              cm ^= A[t2];
+              pw ^= PWP[t2];
+            }
+          }
+          Us[t] = ut;
+          bases[t] = (uint8_t)((qo[t] + 2u * cross) & 3u);
+        }
+        __syncthreads();
+        if (tid == 0) {
+          uint64_t Q1 = 0, Q2 = 0;  // bit t: bit 0 / bit 1 of q_t
+          for (uint32_t t = 0; t < T; t++) {
+            const uint32_t q = (bases[t] + (uint32_t)__popcll(Us[t] & Q1) + 2u * (uint32_t)__popcll(Us[t] & Q2)) & 3u;
+            qp[t] = (uint8_t)q;
+            Q1 |= (uint64_t)(q & 1u) << t;
+            Q2 |= (uint64_t)(q >> 1) << t;
+          }
+        }
+      }
+      cl.sync();  // every CTA is done reading other CTAs' rows
+      // ---- 3. the panel applied to the local rows
+      // (a) per row (warp per row): u[x] = z_x . x_row and q = phase + |x & z|
+      if (a.phases) {
+        for (uint32_t lr = warp; lr < nloc; lr += nwarps) {
+          const uint64_t* row = ROW(lr);
+          uint32_t lo = 0, hi = 0, s = 0;
+          for (uint32_t w = lane; w < len; w += 32) {
+            const uint64_t xw = row[w];
+            s += __popcll(xw & row[len + w]);
+            for (uint32_t x = 0; x < T; x++) {
+              const uint32_t bit = (uint32_t)__popcll(PO[(size_t)x * W + len + w] & xw) & 1u;
+              if (x < 32) lo ^= bit << x; else hi ^= bit << (x - 32);
+            }
+          }
+          s = __reduce_add_sync(0xFFFFFFFFu, s);
+          lo = __reduce_xor_sync(0xFFFFFFFFu, lo);
+          hi = __reduce_xor_sync(0xFFFFFFFFu, hi);
+          if (lane == 0) {
+            cml[lr] = (uint64_t)lo | ((uint64_t)hi << 32);
+            ql[lr] = (uint8_t)((lph[lr] + s) & 3u);
+          }
+        }
+        __syncthreads();
+      }
+      // (b) the steps replayed, one thread per row: its mask and its q
+      for (uint32_t lr = tid; lr < nloc; lr += bd) {
+        const uint32_t r = r0 + lr;
+        uint64_t pw = ROW(lr)[wj], cm = 0;
+        const uint64_t u = a.phases ? cml[lr] : 0;
+        uint32_t q = a.phases ? ql[lr] : 0;
+        for (uint32_t t = 0; t < T; t++) {
+          if (r != stp[t] && ((pw >> bt[t]) & 1ull)) {
+            if (a.phases) q += qp[t] + 2u * (uint32_t)((__popcll(Dt[t] & cm) + __popcll(u & A[t])) & 1);
+            cm ^= A[t];
+            pw ^= PWP[t];
+          }
+        }
+        cml[lr] = cm;
+        ql[lr] = (uint8_t)(q & 3u);
+      }
+      __syncthreads();
+      // (c) the rows (warp per row): start bits XOR the pivot rows of the mask
+      for (uint32_t lr = warp; lr < nloc; lr += nwarps) {
+        const uint64_t cm = cml[lr];
+        if (!cm) continue;
+        uint64_t* row = ROW(lr);
+        uint32_t s = 0;
+        for (uint32_t w = lane; w < len; w += 32) {
+          uint64_t vx = row[w], vz = row[len + w];
+          uint64_t m = cm;
+          while (m) {
+            const uint32_t x = __ffsll(m) - 1;
+            m &= m - 1;
+            vx ^= PO[(size_t)x * W + w];
+            vz ^= PO[(size_t)x * W + len + w];
+          }
+          row[w] = vx;
+          row[len + w] = vz;
+          s += __popcll(vx & vz);
+        }
+        if (a.phases) {
+          s = __reduce_add_sync(0xFFFFFFFFu, s);
+          if (lane == 0) lph[lr] = (uint8_t)((ql[lr] - s) & 3u);
+        }
+      }
+    }
+    if (stage == 0) rx = i;
+  }
+  if (warp < NB) {
+#pragma unroll
+    for (uint32_t k = 0; k < RPT; k++)
+      if (tid + k * nbt < R) pos[tid + k * nbt] = rpos[k];
+  }
+  __syncthreads();
+  cl.sync();
+  // rows to their final positions
+  if (a.smem_rows) {
+    for (uint32_t lr = warp; lr < nloc; lr += nwarps) {
+      const uint32_t p = pos[r0 + lr];
+      for (uint32_t w = lane; w < W; w += 32) a.xzs[(size_t)p * W + w] = rowsbuf[(size_t)lr * WS + w];
+      if (lane == 0 && a.phases) a.ph[p] = lph[lr];
+    }
+  } else {
+    for (uint32_t lr = warp; lr < nloc; lr += nwarps) {
+      const uint32_t p = pos[r0 + lr];
+      for (uint32_t w = lane; w < W; w += 32) a.gtmp[(size_t)p * W + w] = a.xzs[(size_t)(r0 + lr) * W + w];
+      if (lane == 0) a.gtmp_ph[p] = a.phases ? lph[lr] : a.ph[p];
+    }
+  }
+  if (me == 0 && tid == 0) {
+    a.out[0] = (int32_t)rx;
+    a.out[1] = (int32_t)i;
+  }
+}
+
 struct CanonPlan {
   uint32_t cs;
   bool smem_rows;
@@ -509,6 +890,61 @@ struct ElimSpec {
   int32_t* d_out;
 };
 
+static uint32_t g_canon_blocked = 0;  // 0: automatic, 1: always, 2: never
+
+// canonicalize! by panels (canon_blocked_kernel): the cluster (16 CTAs for
+// 256 rows or more, else one CTA) and whether the rows fit its shared memory.
+static int launch_blocked(const ElimSpec& e, cudaStream_t st) {
+  // rows per search thread (registers): 4 up to 4096 rows, else 8
+  void (*kern)(const CanonArgs) = e.rows <= 4096 ? canon_blocked_kernel<4> : canon_blocked_kernel<8>;
+  // the opt-in limit less the kernel's static shared memory
+  cudaFuncAttributes fa{};
+  QCB_CUDA(cudaFuncGetAttributes(&fa, kern));
+  const size_t maxsm = (size_t)device_max_smem_optin() - fa.sharedSizeBytes;
+  uint32_t cs = g_canon_cs ? g_canon_cs : (e.rows >= 256 ? 16 : 1);
+  uint32_t RB = std::max<uint32_t>(1, (e.rows + cs - 1) / cs);
+  bool smem_rows = blocked_layout(e.rows, e.W, RB, true).bytes <= maxsm;
+  if (!smem_rows && !g_canon_cs && cs < 16) {
+    cs = 16;
+    RB = std::max<uint32_t>(1, (e.rows + cs - 1) / cs);
+    smem_rows = blocked_layout(e.rows, e.W, RB, true).bytes <= maxsm;
+  }
+  const size_t bytes = blocked_layout(e.rows, e.W, RB, smem_rows).bytes;
+  if (bytes > maxsm) return fail(QCB_EUNSUPPORTED, "canonicalize!: tableau too tall for the panel bookkeeping");
+  CanonArgs a{};
+  a.xzs = e.xzs; a.ph = e.ph; a.rows = e.rows; a.n = e.n; a.W = e.W; a.RB = RB; a.phases = e.phases;
+  a.smem_rows = smem_rows ? 1 : 0;
+  a.out = e.d_out;
+  a.mode = ELIM_BOTH;
+  if (!smem_rows) {
+    QCB_CUDA(cudaMallocAsync(&a.gtmp, (size_t)e.rows * e.W * 8, st));
+    QCB_CUDA(cudaMallocAsync(&a.gtmp_ph, e.rows, st));
+  }
+  QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxsm));
+  if (cs > 8) QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(cs);
+  cfg.blockDim = dim3(g_canon_threads ? g_canon_threads : CANON_THREADS);
+  cfg.dynamicSmemBytes = bytes;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  QCB_CUDA(cudaLaunchKernelEx(&cfg, kern, a));
+  QCB_LAUNCHED();
+  if (!smem_rows) {
+    QCB_CUDA(cudaMemcpyAsync(e.xzs, a.gtmp, (size_t)e.rows * e.W * 8, cudaMemcpyDeviceToDevice, st));
+    QCB_CUDA(cudaMemcpyAsync(e.ph, a.gtmp_ph, e.rows, cudaMemcpyDeviceToDevice, st));
+    QCB_CUDA(cudaFreeAsync(a.gtmp, st));
+    QCB_CUDA(cudaFreeAsync(a.gtmp_ph, st));
+  }
+  return QCB_OK;
+}
+
 static int eliminate(const ElimSpec& e, cudaStream_t st) {
   if (e.rows == 0) {
     const int32_t h[2] = {0, e.mode == ELIM_RREF ? -1 : (int32_t)e.i0};
@@ -517,6 +953,9 @@ static int eliminate(const ElimSpec& e, cudaStream_t st) {
     return QCB_OK;
   }
   const bool D = e.dxzs != nullptr;
+  // by panels up to 8192 rows (the search keeps at most 8 rows per thread in registers)
+  if (e.mode == ELIM_BOTH && !D && e.rows <= 8192 && g_canon_blocked != 2 && (g_canon_blocked == 1 || e.rows >= 64))
+    return launch_blocked(e, st);
   CanonPlan p = canon_plan(e.rows, e.W, D);
   if (p.smem_bytes > (size_t)device_max_smem_optin())
     return fail(QCB_EUNSUPPORTED, "canonicalize!: tableau too tall for the cluster's bookkeeping");
@@ -627,6 +1066,7 @@ int generate_dev(uint64_t* pauli, uint8_t* pph, const uint64_t* xzs, const uint8
 
 void set_canon_cluster(uint32_t cs) { g_canon_cs = cs; }
 void set_canon_threads(uint32_t n) { g_canon_threads = n; }
+void set_canon_blocked(uint32_t v) { g_canon_blocked = v; }
 
 }  // namespace qcb
 

@@ -243,3 +243,50 @@ def test_project_large_tableau_global_rows(qcb, kind):
         outs.append((a, None if r < 0 else r))
     assert list(zip(anti, res)) == outs
     assert np.array_equal(st.tab.xzs, xz) and np.array_equal(st.tab.phases, ph)
+
+
+@pytest.mark.parametrize("n", [1, 2, 63, 64, 65, 127, 128, 129, 300, 1000])
+@pytest.mark.parametrize("phases", [True, False])
+def test_canonicalize_by_panels_equals_column_steps(qcb, n, phases):
+    # the 64-column panel kernel and the column-by-column kernel on the same
+    # inputs, both against the oracle: full-rank, half-rank, redundant rows,
+    # and rows that do not commute (random bits; the phases still follow the
+    # reference's multiplication order)
+    rng = np.random.default_rng(zlib.crc32(f"panel{n}{phases}".encode()))
+    d = dev_random_destabilizer(qcb, n, rng)
+    stab = Tableau(d.tab.phases[n:].copy(), n, d.tab.xzs[n:].copy())
+    cases = []
+    for rows in sorted({n, max(1, n // 2), n + 3}):
+        t = Tableau.zeros(rows, n)
+        k = min(rows, n)
+        t.phases[:k], t.xzs[:k] = stab.phases[:k], stab.xzs[:k]
+        for r in range(n, rows):
+            t.xzs[r] = t.xzs[r - n] ^ t.xzs[(r - n + 1) % n]
+        cases.append(t)
+    cases.append(Tableau.from_bits(rng.integers(0, 4, n + 5), rng.random((n + 5, n)) < 0.5, rng.random((n + 5, n)) < 0.5))
+    try:
+        for t in cases:
+            ph, xz, orx, orz = oracle.canonicalize(t.phases, t.xzs, n, phases)
+            for mode in (1, 2):
+                qcb.check(qcb.lib().qcb_tune_set(b"canon_blocked", mode))
+                s = qcb.Stabilizer(t.copy()).to_gpu()
+                _, rx, rz = qcb.canonicalize_(s, phases=phases, ranks=True)
+                s.to_cpu()
+                assert (rx, rz) == (orx, orz), mode
+                assert np.array_equal(s.tab.xzs, xz) and np.array_equal(s.tab.phases, ph), mode
+    finally:
+        qcb.check(qcb.lib().qcb_tune_set(b"canon_blocked", 0))
+
+
+def test_canonicalize_by_panels_tall(qcb):
+    # n = 4000: the panel kernel with the rows in global memory
+    n = 4000
+    rng = np.random.default_rng(4000)
+    d = dev_random_destabilizer(qcb, n, rng, depth=6)
+    t = Tableau(d.tab.phases[n:].copy(), n, d.tab.xzs[n:].copy())
+    s = qcb.Stabilizer(t.copy()).to_gpu()
+    _, rx, rz = qcb.canonicalize_(s, ranks=True)
+    s.to_cpu()
+    ph, xz, orx, orz = oracle.canonicalize(t.phases, t.xzs, n, True)
+    assert (rx, rz) == (orx, orz)
+    assert np.array_equal(s.tab.xzs, xz) and np.array_equal(s.tab.phases, ph)

@@ -420,9 +420,11 @@ int qcb_permutesystems(qcb_tableau* t, const uint32_t* perm, void* stream);
 /* Many canonicalize! jobs on Stabilizer tableaux drained by persistent
  * thread-block clusters (no reference counterpart), each job exactly
  * qcb_canonicalize on that tableau.  cluster: CTAs per cluster for every job
- * (0 = per job the smallest cluster whose shared memory holds it; the jobs of
- * one cluster size form a class, one persistent launch per class on its own
- * stream, forked from and joined back to `stream`).  run launches only
+ * (0 = one CTA per job running by 64-column panels, its rows in global memory
+ * when they do not fit; tableaux outside 64..4096 rows by column steps on the
+ * smallest cluster that holds them).  Jobs of one kind and cluster size form
+ * a class, one persistent launch per class on its own stream, forked from and
+ * joined back to `stream`.  run launches only
  * (capturable in a CUDA graph); ranks synchronises the device and gives each
  * job's rx, rz in the caller's order.  The tableaux must outlive the batch. */
 typedef struct qcb_canon_batch qcb_canon_batch;

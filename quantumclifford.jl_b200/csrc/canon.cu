@@ -67,6 +67,8 @@ struct CanonArgs {
   const uint32_t* cols;  // ELIM_RREF columns, 0-based
   uint32_t ncols;
   int32_t* pivcols;      // column of every pivot in order, or null
+  int32_t copy_back;     // global mode in a batch: the body copies gtmp back into the tableau
+  int32_t pad_;
 };
 
 constexpr uint32_t CANON_THREADS = 1024;
@@ -301,40 +303,6 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_kernel(const CanonArgs a)
   canon_body<D, DESC>(a, smem);
 }
 
-// Many canonicalize! jobs (stabilizer tableaux) drained by persistent
-// clusters: CTA 0 of a cluster takes the next job from the queue (longest
-// first) and the cluster runs it with its rows in shared memory, then the
-// next.  The job's arguments are copied into shared memory.
-struct CanonBatchArgs {
-  const CanonArgs* jobs;
-  uint32_t njobs;
-  uint32_t* head;  // next job (zero before the launch)
-};
-static_assert(sizeof(CanonArgs) % 8 == 0, "CanonArgs is copied in 8-byte words");
-
-__global__ void __launch_bounds__(CANON_THREADS) canon_batch_kernel(const CanonBatchArgs b) {
-  extern __shared__ __align__(16) uint64_t smem[];
-  __shared__ __align__(16) CanonArgs ja;
-  __shared__ uint32_t jobid;
-  cg::cluster_group cl = cg::this_cluster();
-  const uint32_t me = cl.block_rank(), tid = threadIdx.x;
-  while (true) {
-    if (me == 0 && tid == 0) {
-      const uint32_t j = atomicAdd(b.head, 1u);
-      jobid = j < b.njobs ? j : 0xFFFFFFFFu;
-    }
-    cl.sync();
-    const uint32_t j = *cl.map_shared_rank(&jobid, 0);
-    if (j == 0xFFFFFFFFu) break;
-    for (uint32_t w = tid; w < sizeof(CanonArgs) / 8; w += blockDim.x)
-      ((uint64_t*)&ja)[w] = ((const uint64_t*)(b.jobs + j))[w];
-    __syncthreads();
-    canon_body<false, false>(ja, smem);
-    __syncthreads();  // ja is read until the end of the body
-  }
-  cl.sync();  // CTA 0's job slot is read by the cluster until here
-}
-
 // permutesystems!(s, perm) (src/linalg.jl:7-17): every row becomes row[perm]
 // (new qubit j is old qubit perm[j], 0-based here); phases stay.  One warp per
 // row, the old row staged in shared memory.
@@ -518,14 +486,13 @@ __host__ __device__ inline BlockedLayout blocked_layout(uint32_t rows, uint32_t 
 }
 
 template <uint32_t RPT>
-__global__ void __launch_bounds__(CANON_THREADS) canon_blocked_kernel(const CanonArgs a) {
+__device__ __forceinline__ void blocked_body(const CanonArgs& a, uint64_t* smem) {
   cg::cluster_group cl = cg::this_cluster();
   const uint32_t me = cl.block_rank();
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5, bd = blockDim.x;
   const uint32_t R = a.rows, n = a.n, W = a.W, len = W / 2, WS = W + 1, RB = a.RB;
   const uint32_t r0 = me * RB;
   const uint32_t nloc = r0 < R ? min(RB, R - r0) : 0u;
-  extern __shared__ __align__(16) uint64_t smem[];
   const BlockedLayout Lo = blocked_layout(R, W, RB, a.smem_rows != 0);
   uint64_t* rowsbuf = smem + Lo.rows_off;
   uint64_t* PO = smem + Lo.po_off;
@@ -828,11 +795,62 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_blocked_kernel(const Cano
       for (uint32_t w = lane; w < W; w += 32) a.gtmp[(size_t)p * W + w] = a.xzs[(size_t)(r0 + lr) * W + w];
       if (lane == 0) a.gtmp_ph[p] = a.phases ? lph[lr] : a.ph[p];
     }
+    if (a.copy_back) {
+      // every CTA has written its rows to their final places in gtmp
+      cl.sync();
+      for (uint32_t lr = warp; lr < nloc; lr += nwarps) {
+        const uint32_t r = r0 + lr;
+        for (uint32_t w = lane; w < W; w += 32) a.xzs[(size_t)r * W + w] = a.gtmp[(size_t)r * W + w];
+        if (lane == 0) a.ph[r] = a.gtmp_ph[r];
+      }
+    }
   }
   if (me == 0 && tid == 0) {
     a.out[0] = (int32_t)rx;
     a.out[1] = (int32_t)i;
   }
+}
+
+template <uint32_t RPT>
+__global__ void __launch_bounds__(CANON_THREADS) canon_blocked_kernel(const CanonArgs a) {
+  extern __shared__ __align__(16) uint64_t smem[];
+  blocked_body<RPT>(a, smem);
+}
+
+// Many canonicalize! jobs (stabilizer tableaux) drained by persistent
+// clusters: CTA 0 of a cluster takes the next job from the queue (longest
+// first) and the cluster runs it (by panels, or by column steps), then the
+// next.  The job's arguments are copied into shared memory.
+struct CanonBatchArgs {
+  const CanonArgs* jobs;
+  uint32_t njobs;
+  uint32_t* head;  // next job (zero before the launch)
+  int blocked;     // 1: the jobs run by panels (blocked_body), else by column steps
+};
+static_assert(sizeof(CanonArgs) % 8 == 0, "CanonArgs is copied in 8-byte words");
+
+__global__ void __launch_bounds__(CANON_THREADS) canon_batch_kernel(const CanonBatchArgs b) {
+  extern __shared__ __align__(16) uint64_t smem[];
+  __shared__ __align__(16) CanonArgs ja;
+  __shared__ uint32_t jobid;
+  cg::cluster_group cl = cg::this_cluster();
+  const uint32_t me = cl.block_rank(), tid = threadIdx.x;
+  while (true) {
+    if (me == 0 && tid == 0) {
+      const uint32_t j = atomicAdd(b.head, 1u);
+      jobid = j < b.njobs ? j : 0xFFFFFFFFu;
+    }
+    cl.sync();
+    const uint32_t j = *cl.map_shared_rank(&jobid, 0);
+    if (j == 0xFFFFFFFFu) break;
+    for (uint32_t w = tid; w < sizeof(CanonArgs) / 8; w += blockDim.x)
+      ((uint64_t*)&ja)[w] = ((const uint64_t*)(b.jobs + j))[w];
+    __syncthreads();
+    if (b.blocked) blocked_body<4>(ja, smem);
+    else canon_body<false, false>(ja, smem);
+    __syncthreads();  // ja is read until the end of the body
+  }
+  cl.sync();  // CTA 0's job slot is read by the cluster until here
 }
 
 struct CanonPlan {
@@ -1275,13 +1293,16 @@ int qcb_generate(qcb_tableau* pauli, const qcb_tableau* stab, int phases, int32_
 }  // extern "C"
 
 // ---------------------------------------------------------------- batches of canonicalize!
-// Jobs are split into size classes by the smallest cluster whose shared
-// memory holds them (a small tableau runs in one CTA with no cluster
-// barrier at all); each class is one persistent launch on its own stream,
-// forked from and joined back to the caller's stream with events, so the
-// classes share the GPU.
+// Jobs are split into classes: by 64-column panels on one CTA each (rows in
+// global memory when they do not fit its shared memory), which takes the
+// least SM time per job at every size measured, else by column steps on the
+// smallest cluster that holds them; each class is one persistent launch on
+// its own stream, forked from and joined back to the caller's stream with
+// events, so the classes share the GPU.
 struct CanonClass {
   uint32_t cs = 1, clusters = 1, njobs = 0;
+  int blocked = 0;                 // by panels (blocked_body) or by column steps
+  std::vector<void*> scratch;      // per-job row buffers of the jobs whose rows stay in global memory
   size_t smem = 0;
   qcb::CanonArgs* d_jobs = nullptr;
   uint32_t* d_head = nullptr;
@@ -1303,64 +1324,89 @@ int qcb_canon_batch_create(qcb_tableau* const* tabs, size_t n, int phases, uint3
   if (!out || (n && !tabs)) return fail(QCB_EARG, "null argument");
   *out = nullptr;
   if (cluster && (cluster > 16 || (cluster & (cluster - 1)))) return fail(QCB_EARG, "cluster must be 0, 1, 2, 4, 8 or 16");
-  const size_t maxsm = (size_t)device_max_smem_optin() - sizeof(CanonArgs) - 64;
-  // the cluster of every job: the given one, else the smallest that holds it
-  std::vector<uint32_t> cs_of(n, 0);
+  cudaFuncAttributes fa{};
+  QCB_CUDA(cudaFuncGetAttributes(&fa, canon_batch_kernel));
+  const size_t maxsm = (size_t)device_max_smem_optin() - fa.sharedSizeBytes;
+  // Per job: by panels on one CTA (the least SM time per job at every size
+  // measured; rows in global memory when they do not fit), or the given
+  // cluster; column steps for tableaux outside the panel kernel's range.
+  struct Plan { uint32_t cs; int blocked; int smem_rows; size_t smem; };
+  std::vector<Plan> plan(n);
   for (size_t j = 0; j < n; j++) {
     const qcb_tableau* t = tabs[j];
     if (!t) return fail(QCB_EARG, "null tableau in the batch");
-    for (uint32_t c = 1; c <= 16; c <<= 1) {
-      if (cluster && c != cluster) continue;
-      if (canon_smem(t->rows, t->W, std::max<uint32_t>(1, (t->rows + c - 1) / c), true, false) <= maxsm) {
-        cs_of[j] = c;
-        break;
+    Plan& pl = plan[j];
+    pl.cs = 0;
+    if (t->rows >= 64 && t->rows <= 4096) {
+      const uint32_t c = cluster ? cluster : 1;
+      const uint32_t RB = std::max<uint32_t>(1, (t->rows + c - 1) / c);
+      const size_t in_smem = blocked_layout(t->rows, t->W, RB, true).bytes;
+      const size_t in_glob = blocked_layout(t->rows, t->W, RB, false).bytes;
+      if (in_smem <= maxsm) pl = {c, 1, 1, in_smem};
+      else if (in_glob <= maxsm) pl = {c, 1, 0, in_glob};
+    }
+    if (!pl.cs) {
+      for (uint32_t c = 1; c <= 16; c <<= 1) {
+        if (cluster && c != cluster) continue;
+        const size_t sm = canon_smem(t->rows, t->W, std::max<uint32_t>(1, (t->rows + c - 1) / c), true, false);
+        if (sm <= maxsm) { pl = {c, 0, 1, sm}; break; }
       }
     }
-    if (!cs_of[j]) return fail(QCB_EUNSUPPORTED, "canonicalize! batch: a tableau does not fit the cluster's shared memory");
+    if (!pl.cs) return fail(QCB_EUNSUPPORTED, "canonicalize! batch: a tableau does not fit the cluster's shared memory");
   }
   auto b = std::make_unique<qcb_canon_batch>();
   b->njobs = (uint32_t)n;
   QCB_CUDA(cudaMalloc(&b->d_out, std::max<size_t>(n, 1) * 8));
   QCB_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
   const uint32_t sms = (uint32_t)std::max(device_sm_count(), 1);
-  for (uint32_t c = 1; c <= 16; c <<= 1) {
-    std::vector<uint32_t> ids;
-    for (size_t j = 0; j < n; j++)
-      if (cs_of[j] == c) ids.push_back((uint32_t)j);
-    if (ids.empty()) continue;
-    // longest first: about rows^2 * W word operations
-    std::stable_sort(ids.begin(), ids.end(), [&](uint32_t x, uint32_t y) {
-      return (double)tabs[x]->rows * tabs[x]->rows * tabs[x]->W > (double)tabs[y]->rows * tabs[y]->rows * tabs[y]->W;
-    });
-    CanonClass k;
-    k.cs = c;
-    k.njobs = (uint32_t)ids.size();
-    std::vector<CanonArgs> jobs(ids.size());
-    size_t smem = 1024;
-    for (size_t q = 0; q < ids.size(); q++) {
-      const qcb_tableau* t = tabs[ids[q]];
-      CanonArgs& a = jobs[q];
-      std::memset(&a, 0, sizeof(a));
-      a.xzs = t->xzs; a.ph = t->phases; a.rows = t->rows; a.n = t->nqubits; a.W = t->W;
-      a.RB = std::max<uint32_t>(1, (t->rows + c - 1) / c);
-      a.phases = phases; a.smem_rows = 1; a.mode = ELIM_BOTH;
-      a.out = b->d_out + 2 * ids[q];
-      smem = std::max(smem, canon_smem(t->rows, t->W, a.RB, true, false));
+  for (int blk = 1; blk >= 0; blk--) {
+    for (uint32_t c = 1; c <= 16; c <<= 1) {
+      std::vector<uint32_t> ids;
+      for (size_t j = 0; j < n; j++)
+        if (plan[j].cs == c && plan[j].blocked == blk) ids.push_back((uint32_t)j);
+      if (ids.empty()) continue;
+      // longest first: about rows^2 * W word operations
+      std::stable_sort(ids.begin(), ids.end(), [&](uint32_t x, uint32_t y) {
+        return (double)tabs[x]->rows * tabs[x]->rows * tabs[x]->W > (double)tabs[y]->rows * tabs[y]->rows * tabs[y]->W;
+      });
+      CanonClass k;
+      k.cs = c;
+      k.blocked = blk;
+      k.njobs = (uint32_t)ids.size();
+      std::vector<CanonArgs> jobs(ids.size());
+      size_t smem = 1024;
+      for (size_t q = 0; q < ids.size(); q++) {
+        const qcb_tableau* t = tabs[ids[q]];
+        const Plan& pl = plan[ids[q]];
+        CanonArgs& a = jobs[q];
+        std::memset(&a, 0, sizeof(a));
+        a.xzs = t->xzs; a.ph = t->phases; a.rows = t->rows; a.n = t->nqubits; a.W = t->W;
+        a.RB = std::max<uint32_t>(1, (t->rows + c - 1) / c);
+        a.phases = phases; a.smem_rows = pl.smem_rows; a.mode = ELIM_BOTH;
+        a.out = b->d_out + 2 * ids[q];
+        if (!pl.smem_rows) {
+          QCB_CUDA(cudaMalloc(&a.gtmp, (size_t)t->rows * t->W * 8));
+          QCB_CUDA(cudaMalloc(&a.gtmp_ph, t->rows));
+          a.copy_back = 1;
+          k.scratch.push_back(a.gtmp);
+          k.scratch.push_back(a.gtmp_ph);
+        }
+        smem = std::max(smem, pl.smem);
+      }
+      k.smem = smem;
+      // as many clusters as fit at once (one CTA per SM at this shared memory)
+      k.clusters = std::max<uint32_t>(1, std::min<uint32_t>(k.njobs, sms / c));
+      QCB_CUDA(cudaMalloc(&k.d_jobs, jobs.size() * sizeof(CanonArgs)));
+      QCB_CUDA(cudaMalloc(&k.d_head, 4));
+      QCB_CUDA(cudaMemcpy(k.d_jobs, jobs.data(), jobs.size() * sizeof(CanonArgs), cudaMemcpyHostToDevice));
+      QCB_CUDA(cudaStreamCreateWithFlags(&k.st, cudaStreamNonBlocking));
+      QCB_CUDA(cudaEventCreateWithFlags(&k.done, cudaEventDisableTiming));
+      b->classes.push_back(k);
     }
-    k.smem = smem;
-    // as many clusters as fit at once (one CTA per SM at this shared memory)
-    k.clusters = std::max<uint32_t>(1, std::min<uint32_t>(k.njobs, sms / c));
-    QCB_CUDA(cudaMalloc(&k.d_jobs, jobs.size() * sizeof(CanonArgs)));
-    QCB_CUDA(cudaMalloc(&k.d_head, 4));
-    QCB_CUDA(cudaMemcpy(k.d_jobs, jobs.data(), jobs.size() * sizeof(CanonArgs), cudaMemcpyHostToDevice));
-    QCB_CUDA(cudaStreamCreateWithFlags(&k.st, cudaStreamNonBlocking));
-    QCB_CUDA(cudaEventCreateWithFlags(&k.done, cudaEventDisableTiming));
-    b->classes.push_back(k);
   }
-  size_t smax = 1024;
   bool big = false;
-  for (auto& k : b->classes) { smax = std::max(smax, k.smem); big |= k.cs > 8; }
-  QCB_CUDA(cudaFuncSetAttribute(canon_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+  for (auto& k : b->classes) big |= k.cs > 8;
+  QCB_CUDA(cudaFuncSetAttribute(canon_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxsm));
   if (big) QCB_CUDA(cudaFuncSetAttribute(canon_batch_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   *out = b.release();
   return QCB_OK;
@@ -1375,7 +1421,7 @@ int qcb_canon_batch_run(qcb_canon_batch* b, void* stream) {
   for (auto& k : b->classes) {
     QCB_CUDA(cudaStreamWaitEvent(k.st, b->fork, 0));
     QCB_CUDA(cudaMemsetAsync(k.d_head, 0, 4, k.st));
-    CanonBatchArgs a{k.d_jobs, k.njobs, k.d_head};
+    CanonBatchArgs a{k.d_jobs, k.njobs, k.d_head, k.blocked};
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(k.clusters * k.cs);
     cfg.blockDim = dim3(CANON_THREADS);
@@ -1412,6 +1458,7 @@ int qcb_canon_batch_ranks(const qcb_canon_batch* b, int32_t* rx, int32_t* rz) {
 int qcb_canon_batch_destroy(qcb_canon_batch* b) {
   if (!b) return QCB_OK;
   for (auto& k : b->classes) {
+    for (void* p : k.scratch) cudaFree(p);
     cudaFree(k.d_jobs);
     cudaFree(k.d_head);
     if (k.st) cudaStreamDestroy(k.st);

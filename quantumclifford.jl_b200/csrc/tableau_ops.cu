@@ -318,6 +318,95 @@ __global__ void __launch_bounds__(256) apply_dense_kernel(uint64_t* xzs, uint8_t
   if (lane == 0) ph[warp] = phases ? (uint8_t)((s + extra + ph[warp]) & 3u) : (uint8_t)0;
 }
 
+// The same product split over G warps per state row (one row per CTA): warp g
+// multiplies the Clifford rows of its share of the qubit words in order into
+// a partial product (bits, counters, phase), and warp 0 then left-multiplies
+// the partials in order.  The Pauli product is associative with exact phases,
+// so P_{G-1} ... P_1 P_0 is the ordered product of all the images, and the
+// row gets G times the warps of the one-warp kernel.
+template <int MAXW, int G>
+__global__ void __launch_bounds__(32 * G) apply_dense_split_kernel(uint64_t* xzs, uint8_t* ph, uint32_t rows,
+                                                                  uint32_t W, uint32_t n,
+                                                                  const uint64_t* __restrict__ c,
+                                                                  const uint8_t* __restrict__ cph, int phases) {
+  __shared__ uint64_t part[G][MAXW];
+  __shared__ uint32_t pph[G];
+  const uint32_t r = blockIdx.x, g = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (r >= rows) return;
+  const uint32_t len = W / 2;
+  constexpr int PER = (MAXW / 2 + 31) / 32;  // words per lane per half
+  uint64_t bx[PER], bz[PER], c1[PER], c2[PER];
+#pragma unroll
+  for (int k = 0; k < PER; k++) { bx[k] = bz[k] = c1[k] = c2[k] = 0; }
+  uint64_t* row = xzs + (uint64_t)r * W;
+  uint32_t extra = 0;  // Clifford-row phases and the -1 of every Y (mod 4)
+  const uint32_t wq0 = g * len / G, wq1 = (g + 1) * len / G;
+  for (uint32_t wq = wq0; wq < wq1; wq++) {
+    const uint64_t xw = row[wq], zw = row[len + wq];  // broadcast loads
+    uint64_t both = xw | zw;
+    while (both) {
+      const uint32_t b = __ffsll((long long)both) - 1;
+      both &= both - 1;
+      const uint32_t q = wq * 64 + b;
+      if (q >= n) break;
+      const bool x = (xw >> b) & 1, z = (zw >> b) & 1;
+      if (x && z) extra += 3;
+      if (x) {
+        const uint64_t* cr = c + (uint64_t)q * W;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+          const uint32_t w = lane + 32 * k;
+          if (w < len) mul_step<uint64_t>(__ldg(cr + w), __ldg(cr + len + w), bx[k], bz[k], c1[k], c2[k]);
+        }
+        extra += cph[q];
+      }
+      if (z) {
+        const uint64_t* cr = c + (uint64_t)(q + n) * W;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+          const uint32_t w = lane + 32 * k;
+          if (w < len) mul_step<uint64_t>(__ldg(cr + w), __ldg(cr + len + w), bx[k], bz[k], c1[k], c2[k]);
+        }
+        extra += cph[q + n];
+      }
+    }
+  }
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < PER; k++) s += cnt_phase(c1[k], c2[k]);
+  s = __reduce_add_sync(0xFFFFFFFFu, s & 3u) & 3u;
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    const uint32_t w = lane + 32 * k;
+    if (w < len) { part[g][w] = bx[k]; part[g][len + w] = bz[k]; }
+  }
+  if (lane == 0) pph[g] = (s + extra) & 3u;
+  __syncthreads();
+  if (g != 0) return;
+  // warp 0: acc = P_0, then acc <- P_g * acc for g = 1 .. G-1
+#pragma unroll
+  for (int k = 0; k < PER; k++) { c1[k] = c2[k] = 0; }
+  uint32_t tot = pph[0];
+  for (uint32_t h = 1; h < G; h++) {
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const uint32_t w = lane + 32 * k;
+      if (w < len) mul_step<uint64_t>(part[h][w], part[h][len + w], bx[k], bz[k], c1[k], c2[k]);
+    }
+    tot += pph[h];
+  }
+  s = 0;
+#pragma unroll
+  for (int k = 0; k < PER; k++) s += cnt_phase(c1[k], c2[k]);
+  s = __reduce_add_sync(0xFFFFFFFFu, s & 3u) & 3u;
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    const uint32_t w = lane + 32 * k;
+    if (w < len) { row[w] = bx[k]; row[len + w] = bz[k]; }
+  }
+  if (lane == 0) ph[r] = phases ? (uint8_t)((s + tot + ph[r]) & 3u) : (uint8_t)0;
+}
+
 // ---------------------------------------------------------------- no-alloc batch
 // Phase accumulators of qcb_mul_left_pauli_batch_noalloc, one per pair.  Zero
 // between calls: the finish kernel clears what it read.
@@ -500,9 +589,23 @@ int qcb_apply_dense(qcb_tableau* t, const qcb_tableau* c, int phases, void* stre
   if (t->nqubits != c->nqubits || c->rows != 2 * c->nqubits)
     return fail(QCB_EDIM, "The tableau and the Clifford operator need to act on the same number of qubits.");
   if (!t->rows) return QCB_OK;
-  const uint32_t threads = 256, blocks = (t->rows * 32 + threads - 1) / threads;
   cudaStream_t st = S(stream);
   const uint32_t W = t->W;
+  // 8 warps per row (one row per CTA) unless the rows alone fill the GPU
+  const bool split = (uint64_t)t->rows < 8ull * 148 * 8 && W >= 16;
+  if (split) {
+    if (W <= 64)
+      apply_dense_split_kernel<64, 8><<<t->rows, 256, 0, st>>>(t->xzs, t->phases, t->rows, W, t->nqubits, c->xzs, c->phases, phases);
+    else if (W <= 128)
+      apply_dense_split_kernel<128, 8><<<t->rows, 256, 0, st>>>(t->xzs, t->phases, t->rows, W, t->nqubits, c->xzs, c->phases, phases);
+    else if (W <= 256)
+      apply_dense_split_kernel<256, 8><<<t->rows, 256, 0, st>>>(t->xzs, t->phases, t->rows, W, t->nqubits, c->xzs, c->phases, phases);
+    else
+      return fail(QCB_EUNSUPPORTED, "qcb_apply_dense: at most 8192 qubits");
+    QCB_LAUNCHED();
+    return QCB_OK;
+  }
+  const uint32_t threads = 256, blocks = (t->rows * 32 + threads - 1) / threads;
   if (W <= 64)
     apply_dense_kernel<64><<<blocks, threads, 0, st>>>(t->xzs, t->phases, t->rows, W, t->nqubits, c->xzs, c->phases, phases);
   else if (W <= 128)

@@ -261,7 +261,7 @@ def test_generate(qcb, n):
             assert out[1] == used and out[0].phases[0] == rph and not out[0].xzs.any()
 
 
-@pytest.mark.parametrize("n", [2, 64, 129, 1000])
+@pytest.mark.parametrize("n", [2, 64, 129, 600, 1000, 1501, 3000])
 def test_dense_apply(qcb, n):
     rng = np.random.default_rng(n)
     d = dev_random_destabilizer(qcb, n, rng)

@@ -33,11 +33,14 @@ __device__ __forceinline__ uint32_t cnt_phase(uint64_t c1, uint64_t c2) {
 
 // Grid-stride mul_left! over two long Paulis.  VEC = 2 uses 128-bit loads
 // (needs len even and 16-byte aligned halves).  Each block adds its phase
-// sum (mod 4) into acc[0].
+// sum (mod 4) into acc[0] and counts itself done in acc[1]; the last block
+// to finish writes r.phase <- (s + r.phase + l.phase) & 3
+// (src/mul_leftright.jl:140) and clears both, so one launch does the call.
 template <int VEC, bool PH>
 __global__ void __launch_bounds__(256) mul_left_long_kernel(uint64_t* __restrict__ r,
                                                             const uint64_t* __restrict__ l,
-                                                            uint64_t len, uint32_t* acc) {
+                                                            uint64_t len, uint32_t* acc,
+                                                            uint8_t* r_phase, const uint8_t* l_phase) {
   uint64_t c1a = 0, c2a = 0, c1b = 0, c2b = 0;
   const uint64_t nvec = len / VEC;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -74,7 +77,16 @@ __global__ void __launch_bounds__(256) mul_left_long_kernel(uint64_t* __restrict
   if (wid == 0) {
     uint32_t s = lane < (blockDim.x >> 5) ? wsum[lane] : 0u;
     s = __reduce_add_sync(0xFFFFFFFFu, s) & 3u;
-    if (lane == 0 && s) atomicAdd(acc, s);
+    if (lane == 0) {
+      if (s) atomicAdd(acc, s);
+      __threadfence();
+      if (atomicAdd(acc + 1, 1u) == gridDim.x - 1) {  // the last block
+        __threadfence();
+        const uint32_t tot = atomicExch(acc, 0u) & 3u;
+        atomicExch(acc + 1, 0u);
+        r_phase[0] = (uint8_t)((tot + r_phase[0] + l_phase[0]) & 3u);
+      }
+    }
   }
 }
 
@@ -488,20 +500,21 @@ int qcb_mul_left_pauli(qcb_tableau* r, const qcb_tableau* l, int phases, uint8_t
   const int sms = device_sm_count();
   const bool vec = (len % 2 == 0);
   const uint64_t work = vec ? len / 2 : len;
-  uint32_t blocks = (uint32_t)std::min<uint64_t>((work + 255) / 256, (uint64_t)sms * 8);
+  // one wave of resident blocks (no tail wave for the grid-stride loop)
+  void (*k)(uint64_t*, const uint64_t*, uint64_t, uint32_t*, uint8_t*, const uint8_t*) =
+      vec ? (phases ? mul_left_long_kernel<2, true> : mul_left_long_kernel<2, false>)
+          : (phases ? mul_left_long_kernel<1, true> : mul_left_long_kernel<1, false>);
+  int per_sm = 0;
+  QCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, 0));
+  uint32_t blocks = (uint32_t)std::min<uint64_t>((work + 255) / 256, (uint64_t)sms * std::max(per_sm, 1));
   if (blocks == 0) blocks = 1;
   if (len) {
-    if (vec) {
-      if (phases) mul_left_long_kernel<2, true><<<blocks, 256, 0, st>>>(r->xzs, l->xzs, len, r->scratch);
-      else mul_left_long_kernel<2, false><<<blocks, 256, 0, st>>>(r->xzs, l->xzs, len, r->scratch);
-    } else {
-      if (phases) mul_left_long_kernel<1, true><<<blocks, 256, 0, st>>>(r->xzs, l->xzs, len, r->scratch);
-      else mul_left_long_kernel<1, false><<<blocks, 256, 0, st>>>(r->xzs, l->xzs, len, r->scratch);
-    }
+    k<<<blocks, 256, 0, st>>>(r->xzs, l->xzs, len, r->scratch, r->phases, l->phases);
+    QCB_LAUNCHED();
+  } else if (phases) {
+    mul_left_finish_kernel<<<1, 1, 0, st>>>(r->phases, l->phases, r->scratch, phases);
     QCB_LAUNCHED();
   }
-  mul_left_finish_kernel<<<1, 1, 0, st>>>(r->phases, l->phases, r->scratch, phases);
-  QCB_LAUNCHED();
   if (phase_out) {
     QCB_CUDA(cudaMemcpyAsync(phase_out, r->phases, 1, cudaMemcpyDeviceToHost, st));
     QCB_CUDA(cudaStreamSynchronize(st));

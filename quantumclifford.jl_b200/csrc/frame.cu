@@ -900,6 +900,7 @@ struct WalkConfig {
 };
 
 static uint32_t g_tile_override = 0;
+static uint32_t g_threads_override = 0;  // threads per CTA (0: 768)
 
 // Tile width (even: threads own column pairs) for ncols columns with tiles of
 // at most tmax columns: the fewest waves of one CTA per SM, then the narrowest
@@ -927,15 +928,16 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   } else if (budget / per_col >= 16) {
     T = balanced_tile(f->ncols, (uint32_t)std::min<size_t>(256, budget / per_col));
   }
+  const uint32_t threads = g_threads_override ? g_threads_override : 768u;
   if (T) {
     wc.smem = true;
     wc.T = T;
-    wc.nth = (768u / (T / 2)) * (T / 2);  // column pairs; the kernel's launch bound is 768
+    wc.nth = (threads / (T / 2)) * (T / 2);  // column pairs; the kernel's launch bound is 768
     wc.smem_bytes = per_col * T + stage;
   } else {
     wc.smem = false;
     wc.T = balanced_tile(f->ncols, 128);
-    wc.nth = (768u / (wc.T / 2)) * (wc.T / 2);
+    wc.nth = (threads / (wc.T / 2)) * (wc.T / 2);
     wc.smem_bytes = (size_t)2 * p->nslots * 4 + stage;
   }
   const uint64_t tiles = (f->ncols + wc.T - 1) / wc.T;
@@ -1184,6 +1186,7 @@ extern "C" int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* p, uint
 // Internal hooks for the batched runner and the tuner.
 namespace qcb {
 void set_walker_tile(uint32_t t) { g_tile_override = t; }
+void set_walker_threads(uint32_t t) { g_threads_override = t; }
 int run_program_fresh(qcb_frame* f, const qcb_program* p, uint64_t seed, uint64_t shot_offset,
                       cudaStream_t st) {
   qcb_noise_source n{};

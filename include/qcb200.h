@@ -434,6 +434,14 @@ int qcb_canon_batch_run(qcb_canon_batch* b, void* stream);
 int qcb_canon_batch_ranks(const qcb_canon_batch* b, int32_t* rx, int32_t* rz);
 int qcb_canon_batch_destroy(qcb_canon_batch* b);
 
+/* expect(p, s) (src/project_trace_reset.jl:743-751) for each of the k
+ * one-row Paulis in `paulis` on the state `t` of the given kind (rank for the
+ * mixed kinds), each on its own copy, in one launch; `t` is not modified.
+ * out[j] = -1 for 0 (the reference's `nothing`), else the phase q of the
+ * result i^q: 0 -> 1, 1 -> im, 2 -> -1, 3 -> -im.                          */
+int qcb_expect(const qcb_tableau* t, int kind, int32_t rank, const qcb_tableau* paulis, int32_t* out,
+               void* stream);
+
 /* generate!(pauli, stabilizer; phases) (src/project_trace_reset.jl:37-81) on
  * a canonical stabilizer.  Writes the remaining Pauli (identity up to phase)
  * back into `pauli`; *ok = 0 when the Pauli cannot be generated.  used_rows

@@ -466,6 +466,27 @@ def project_(state, paulis, *, keep_result: bool = True, phases: bool = True):
     return state, [int(a) for a in anti], results
 
 
+_EXPECT_VALUE = {-1: 0, 0: 1, 1: 1j, 2: -1, 3: -1j}
+
+
+def expect(paulis, state):
+    """expect(p, s) (src/project_trace_reset.jl:743-751): the expectation of
+    a PauliOperator (or of each row of a device Tableau of Paulis, in one
+    launch) on a device state, which is not modified.  Returns 0, 1, -1, 1j or
+    -1j (a list for a Tableau of Paulis)."""
+    dev = _tab(state)._need_dev()
+    kind, rank = _kind_rank(state)
+    single = isinstance(paulis, PauliOperator)
+    pt = _tab(paulis)
+    if pt.dev is None:
+        pt.to_gpu()
+    k = len(pt)
+    out = np.zeros(max(k, 1), np.int32)
+    check(lib().qcb_expect(dev.handle, kind, rank, pt.dev.handle, ptr(out), None))
+    vals = [_EXPECT_VALUE[int(v)] for v in out[:k]]
+    return vals[0] if single else vals
+
+
 def generate_(pauli: PauliOperator, stab, *, phases: bool = True, saveindices: bool = True):
     """generate!(pauli, stabilizer) (src/project_trace_reset.jl:37-81) on device
     objects.  Returns None (nothing) or (pauli, used_indices)."""

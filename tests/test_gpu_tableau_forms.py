@@ -290,3 +290,43 @@ def test_canonicalize_by_panels_tall(qcb):
     ph, xz, orx, orz = oracle.canonicalize(t.phases, t.xzs, n, True)
     assert (rx, rz) == (orx, orz)
     assert np.array_equal(s.tab.xzs, xz) and np.array_equal(s.tab.phases, ph)
+
+
+def oracle_expect(kind, tab, n, p_xz, p_ph, rank=0):
+    st, _, _, _, a, r = oracle.project(kind, tab.phases, tab.xzs, n, p_xz, p_ph, rank)
+    assert st == 0
+    return {-1: 0, 0: 1, 1: 1j, 2: -1, 3: -1j}[r]
+
+
+def test_expect_known_answers_on_device(qcb):
+    # test/test_expect.jl:33-40 (bell() with sX(2): +XX, -ZZ)
+    st = qcb.S("+XX -ZZ").to_gpu()
+    for pauli, want in [("XX", 1), ("ZZ", -1), ("XI", 0), ("ZI", 0), ("II", 1), ("-XX", -1), ("-iXX", -1j)]:
+        assert qcb.expect(qcb.P(pauli), st) == want, pauli
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("n", [1, 5, 64, 65, 300, 1000])
+def test_expect_many_paulis(qcb, kind, n):
+    # random Paulis (mostly 0) and group elements (products of stabilizer rows
+    # with extra signs and factors of i): each against project! on a copy
+    rng = np.random.default_rng(zlib.crc32(f"expect{kind}{n}".encode()))
+    d = dev_random_destabilizer(qcb, n, rng)
+    st, tab, rank = make_state(qcb, kind, d, n, max(1, (2 * n) // 3))
+    k = 48
+    paulis = _random_paulis(k, n, rng)
+    off = n if "Destabilizer" in kind else 0
+    r = rank if kind.startswith("Mixed") else n
+    for j in range(0, k, 2):
+        acc, ph = np.zeros(tab.xzs.shape[1], np.uint64), 0
+        for i in np.nonzero(rng.random(r) < 0.5)[0]:
+            acc, ph = oracle.mul_left_pauli(acc, ph, tab.xzs[off + i], tab.phases[off + i])
+        paulis.xzs[j] = acc
+        paulis.phases[j] = (ph + int(rng.integers(0, 4))) & 3
+    st.to_gpu()
+    got = qcb.expect(paulis.copy().to_gpu(), st)
+    st.to_cpu()
+    assert np.array_equal(st.tab.xzs, tab.xzs) and np.array_equal(st.tab.phases, tab.phases)  # not modified
+    want = [oracle_expect(kind, tab, n, paulis.xzs[j], paulis.phases[j], rank) for j in range(k)]
+    assert got == want
+    assert any(v != 0 for v in want)

@@ -516,3 +516,24 @@ def test_evaluate_guesses_restatement(orc):
     g = rng.random((40, 6)) < 0.5
     f = rng.random((3, 6)) < 0.5
     assert orc.evaluate_guesses((g.astype(int) @ f.T.astype(int)) % 2 == 1, g, f)[1] == 0
+
+
+def oracle_expect(kind, ph, xz, n, p_xz, p_ph, rank=0):
+    """expect(p, s) = project!(copy(s), p) mapped (src/project_trace_reset.jl:743-751)."""
+    st, _, _, _, a, r = orc_mod().project(kind, ph, xz, n, p_xz, p_ph, rank)
+    assert st == 0
+    return {-1: 0, 0: 1, 1: 1j, 2: -1, 3: -1j}[r]
+
+
+def orc_mod():
+    import oracle
+
+    return oracle
+
+
+def test_expect_known_answers(orc):
+    # test/test_expect.jl:33-40: bell() with sX(2) applied is +XX, -ZZ
+    st = S("+XX -ZZ").tab
+    for pauli, want in [("XX", 1), ("ZZ", -1), ("XI", 0), ("ZI", 0), ("II", 1), ("-XX", -1), ("-iXX", -1j)]:
+        p = P(pauli)
+        assert oracle_expect("Stabilizer", st.phases, st.xzs, 2, p.xz, p.phase) == want, pauli

@@ -315,6 +315,43 @@ def bench_tableau(args):
              {"workload": "1000 random Paulis (weight ~ U{1..n}) projected in sequence by one call, per projection",
               "rows": 2 * n}, cpu)
 
+    if want("expect"):
+        # ---- expect of 1000 random Paulis on a random 1000-qubit Destabilizer:
+        # independent projections (each on its own copy), one launch, the
+        # state unchanged; half of them are stabilizer-group elements
+        n, k = 1000, 1000
+        d = random_destabilizer(n)
+        P = Q.Tableau.zeros(k, n)
+        for i in range(k):
+            if i % 2:
+                w = int(rng.integers(1, n + 1))
+                qs = rng.choice(n, w, replace=False)
+                kinds = rng.integers(1, 4, size=w)
+                xs = np.zeros((1, n), bool); zs = np.zeros((1, n), bool)
+                xs[0, qs] = kinds & 1 == 1; zs[0, qs] = kinds & 2 == 2
+                one = Q.Tableau.from_bits([0], xs, zs)
+                P.xzs[i], P.phases[i] = one.xzs[0], 0
+            else:
+                acc, ph = np.zeros(d.tab.xzs.shape[1], np.uint64), 0
+                for r in np.nonzero(rng.random(n) < 0.5)[0][:64]:
+                    acc, ph = oracle.mul_left_pauli(acc, ph, d.tab.xzs[n + r], d.tab.phases[n + r])
+                P.xzs[i], P.phases[i] = acc, ph
+        Pg = P.copy().to_gpu()
+        state = Q.Destabilizer(Q.Tableau(d.tab.phases.copy(), n, d.tab.xzs.copy())).to_gpu()
+        out = np.zeros(k, np.int32)
+        ms = device_ms(lambda: check(L.qcb_expect(state.tab.dev.handle, Q.KIND["Destabilizer"], 0, Pg.dev.handle,
+                                                  ptr(out), sp)), args.steps)
+        t0 = time.perf_counter()
+        expected = []
+        for i in range(k):
+            st_, _, _, _, a_, r_ = oracle.project("Destabilizer", d.tab.phases, d.tab.xzs, n, P.xzs[i], P.phases[i])
+            expected.append(r_)
+        cpu = (time.perf_counter() - t0) * 1e3 / k
+        assert list(out) == expected
+        emit("expect of a random Pauli on a random 1000-qubit Destabilizer (independent projections)", "expect",
+             ms / k, {"workload": "1000 Paulis (half random, half stabilizer-group elements) in one call, per Pauli",
+                      "rows": 2 * n}, cpu)
+
     if want("dense_apply"):
         # ---- dense apply! of tensor_pow(tCNOT, 500) to a random 1000-qubit stabilizer
         n = 1000
@@ -625,7 +662,7 @@ def main():
     ap.add_argument("--walker-tile", type=int, default=0)
     ap.add_argument("--workload", default="frames", choices=["frames", "tableau", "batch", "serve"])
     ap.add_argument("--serve-requests", type=int, default=200)
-    ap.add_argument("--tableau-only", default="", help="comma list of mul_left,canonicalize,project,dense_apply,sCNOT")
+    ap.add_argument("--tableau-only", default="", help="comma list of mul_left,canonicalize,project,expect,dense_apply,sCNOT")
     ap.add_argument("--serve-rates", default="25,50,100")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

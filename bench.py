@@ -708,7 +708,8 @@ def main():
     upd = O.count_updates(arr)
     assert upd == 7601
     shots = args.shots
-    offset = rank * ((shots + 1023) // 1024 * 1024)  # Philox shot groups are 1024 shots
+    from qcb200.shard import max_over_ranks, shard_offset
+    offset = shard_offset(rank, shots)  # Philox shot groups are 1024 shots
     prog = qcb200.Program(arr)
     qmax, bmax = O.affected_counts(arr)
     frame = qcb200.PauliFrame(shots, qmax, bmax, init=False)
@@ -760,9 +761,7 @@ def main():
     clk = clocks.stop()
 
     if world > 1:
-        t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+        ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
 
     total_updates = upd * shots * world
     value = total_updates / (ms / 1e3)

@@ -338,6 +338,16 @@ function project!(s::B200State, p::B200State{<:PauliOperator}; keep_result::Bool
     s, Int(anti[]), res[] < 0 ? nothing : UInt8(res[])
 end
 
+# expect(p, s) (src/project_trace_reset.jl:743-751) on a device state, which
+# is not modified
+function QuantumClifford.expect(p::B200State{<:PauliOperator}, s::B200State)
+    h = s.host
+    out = Ref{Int32}(0)
+    _check(ccall((:qcb_expect, libqcb), Cint, (Ptr{Cvoid}, Cint, Int32, Ptr{Cvoid}, Ref{Int32}, Ptr{Cvoid}),
+                 s.dev.handle, _kind(h), _rank(h), p.dev.handle, out, C_NULL))
+    out[] < 0 ? 0 : (1, im, -1, -im)[out[] + 1]
+end
+
 function apply!(s::B200State, gate::AbstractSymbolicOperator; phases::Bool=true)
     ops = _qcbops(gate)
     _check(ccall((:qcb_apply_gates, libqcb), Cint, (Ptr{Cvoid}, Ptr{QcbOp}, Csize_t, Cint, Ptr{Cvoid}),

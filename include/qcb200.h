@@ -338,6 +338,10 @@ int qcb_mul_left_pauli(qcb_tableau* r, const qcb_tableau* l, int phases,
 int qcb_mul_left_pauli_batch_noalloc(uint64_t* r_xz, uint8_t* r_phases, const uint64_t* l_xz,
                                      const uint8_t* l_phases, uint32_t nqubits, uint32_t count,
                                      int phases, void* stream);
+/* rowswap!(state, i, j; phases) (src/QuantumClifford.jl:899-927): rows i, j
+ * (1-based) of the state's stabilizer view; the Destabilizer kinds swap the
+ * paired destabilizer rows too; phases move only when `phases`.           */
+int qcb_rowswap(qcb_tableau* t, int kind, uint32_t i, uint32_t j, int phases, void* stream);
 /* mul_left!(s::Tableau, m, i; phases) (src/mul_leftright.jl:177-181).      */
 int qcb_mul_left_row(qcb_tableau* s, uint32_t m, uint32_t i, int phases, void* stream);
 /* mul_left!(s::Tableau, p::PauliOperator; phases) (src/mul_leftright.jl:223-229). */

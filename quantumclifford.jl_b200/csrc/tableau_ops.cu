@@ -419,6 +419,22 @@ __global__ void __launch_bounds__(32 * G) apply_dense_split_kernel(uint64_t* xzs
   if (lane == 0) ph[r] = phases ? (uint8_t)((s + tot + ph[r]) & 3u) : (uint8_t)0;
 }
 
+// rowswap!(state, i, j; phases) (src/QuantumClifford.jl:899-927): rows i and
+// j of the view (and their destabilizer rows for the Destabilizer kinds), the
+// phases only when `phases`.  One thread per word.
+__global__ void rowswap_kernel(uint64_t* xzs, uint8_t* ph, uint32_t W, uint32_t i, uint32_t j, uint32_t di,
+                               uint32_t dj, int destab, int phases) {
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < W) {
+    uint64_t t = xzs[(size_t)i * W + w]; xzs[(size_t)i * W + w] = xzs[(size_t)j * W + w]; xzs[(size_t)j * W + w] = t;
+    if (destab) { t = xzs[(size_t)di * W + w]; xzs[(size_t)di * W + w] = xzs[(size_t)dj * W + w]; xzs[(size_t)dj * W + w] = t; }
+  }
+  if (w == 0 && phases) {
+    uint8_t p = ph[i]; ph[i] = ph[j]; ph[j] = p;
+    if (destab) { p = ph[di]; ph[di] = ph[dj]; ph[dj] = p; }
+  }
+}
+
 // ---------------------------------------------------------------- no-alloc batch
 // Phase accumulators of qcb_mul_left_pauli_batch_noalloc, one per pair.  Zero
 // between calls: the finish kernel clears what it read.
@@ -519,6 +535,22 @@ int qcb_mul_left_pauli(qcb_tableau* r, const qcb_tableau* l, int phases, uint8_t
     QCB_CUDA(cudaMemcpyAsync(phase_out, r->phases, 1, cudaMemcpyDeviceToHost, st));
     QCB_CUDA(cudaStreamSynchronize(st));
   }
+  return QCB_OK;
+}
+
+int qcb_rowswap(qcb_tableau* t, int kind, uint32_t i, uint32_t j, int phases, void* stream) {
+  if (!t) return fail(QCB_EARG, "null tableau");
+  if (i == 0 || j == 0) return fail(QCB_EBOUNDS, "rows are 1-based");
+  const bool destab = kind == QCB_DESTABILIZER || kind == QCB_MIXED_DESTABILIZER;
+  if (kind < 0 || kind > 3) return fail(QCB_EARG, "rowswap!: bad state kind");
+  if (destab && t->rows % 2) return fail(QCB_EDIM, "destabilizer tableaux have an even number of rows");
+  const uint32_t nn = destab ? t->rows / 2 : t->rows;
+  if (i > nn || j > nn) return fail(QCB_EBOUNDS, "rowswap!: row out of range");
+  if (i == j) return QCB_OK;
+  const uint32_t off = destab ? nn : 0;
+  rowswap_kernel<<<(t->W + 127) / 128, 128, 0, S(stream)>>>(t->xzs, t->phases, t->W, off + i - 1, off + j - 1, i - 1,
+                                                           j - 1, destab ? 1 : 0, phases);
+  QCB_LAUNCHED();
   return QCB_OK;
 }
 

@@ -25,6 +25,6 @@ from .tableau import (  # noqa: F401
     P, S, T, tCNOT, tensor_pow, one_destabilizer, one_mixed_destabilizer, random_clifford_ops,
     mul_left_, mul_left_row_, prodphase, comm, canonicalize_, project_, generate_, apply_, DeviceTableau,
     canonicalize_rref_, canonicalize_gott_, permutesystems_, projectX_, projectY_, projectZ_,
-    projectrand_, projectXrand_, projectYrand_, projectZrand_, CanonBatch, expect,
+    projectrand_, projectXrand_, projectYrand_, projectZrand_, CanonBatch, expect, rowswap_,
 )
 from . import circuits  # noqa: F401

@@ -183,6 +183,7 @@ def lib():
         "qcb_frame_measurement_columns": ([vp, vp, sz, vp, vp, vp], ctypes.c_int),
         "qcb_frame_syndrome_rows": ([vp, vp, sz, vp, ctypes.c_int, vp], ctypes.c_int),
         "qcb_evaluate_guesses": ([vp, vp, sz, vp, sz, vp, P(u64), vp], ctypes.c_int),
+        "qcb_rowswap": ([vp, ctypes.c_int, u32, u32, ctypes.c_int, vp], ctypes.c_int),
         "qcb_expect": ([vp, ctypes.c_int, i32, vp, vp, vp], ctypes.c_int),
         "qcb_project_qubit": ([vp, ctypes.c_int, P(i32), u32, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, vp, vp,
                                P(u32), vp], ctypes.c_int),

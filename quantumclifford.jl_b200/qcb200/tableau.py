@@ -466,6 +466,16 @@ def project_(state, paulis, *, keep_result: bool = True, phases: bool = True):
     return state, [int(a) for a in anti], results
 
 
+def rowswap_(state, i: int, j: int, *, phases: bool = True):
+    """rowswap!(state, i, j; phases) (src/QuantumClifford.jl:899-927), 1-based
+    rows of the stabilizer view (with the paired destabilizer rows for the
+    Destabilizer kinds)."""
+    dev = _tab(state)._need_dev()
+    kind, _ = _kind_rank(state)
+    check(lib().qcb_rowswap(dev.handle, kind, int(i), int(j), int(phases), None))
+    return state
+
+
 _EXPECT_VALUE = {-1: 0, 0: 1, 1: 1j, 2: -1, 3: -1j}
 
 

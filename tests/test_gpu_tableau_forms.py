@@ -330,3 +330,25 @@ def test_expect_many_paulis(qcb, kind, n):
     want = [oracle_expect(kind, tab, n, paulis.xzs[j], paulis.phases[j], rank) for j in range(k)]
     assert got == want
     assert any(v != 0 for v in want)
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("phases", [True, False])
+def test_rowswap(qcb, kind, phases):
+    # rowswap!(state, i, j; phases) (src/QuantumClifford.jl:899-927)
+    n = 70
+    rng = np.random.default_rng(zlib.crc32(f"swap{kind}{phases}".encode()))
+    d = dev_random_destabilizer(qcb, n, rng)
+    st, tab, rank = make_state(qcb, kind, d, n, 40)
+    st.to_gpu()
+    want_x, want_p = tab.xzs.copy(), tab.phases.copy()
+    off = n if "Destabilizer" in kind else 0
+    for i, j in [(1, 2), (5, 40), (40, 5), (7, 7)]:
+        qcb.rowswap_(st, i, j, phases=phases)
+        rows = [(off + i - 1, off + j - 1)] + ([(i - 1, j - 1)] if off else [])
+        for a, b in rows:
+            want_x[[a, b]] = want_x[[b, a]]
+            if phases:
+                want_p[[a, b]] = want_p[[b, a]]
+    st.to_cpu()
+    assert np.array_equal(st.tab.xzs, want_x) and np.array_equal(st.tab.phases, want_p)

@@ -151,7 +151,7 @@ def run_reference(args, rank, world):
             times.append(r["value"])
             cb = r
     v = statistics.median(times)
-    out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": 7601 * SHOTS_PER_GPU / v * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "u32 bit planes", "data": "synthetic (seeded)", "impl": "reference",
            "config": {"workload": WORKLOAD, "sample": cb["sample"]},

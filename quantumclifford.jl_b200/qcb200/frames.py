@@ -33,6 +33,7 @@ class Program:
         h = ctypes.c_void_p()
         check(lib().qcb_program_compile(ptr(self.ops) if len(self.ops) else None, len(self.ops), ctypes.byref(h)))
         self.handle = h
+        self._destroy = lib().qcb_program_destroy
         info = qcb_program_info()
         check(lib().qcb_program_info_get(self.handle, ctypes.byref(info)))
         self.info = {f: getattr(info, f) for f, _ in info._fields_}
@@ -40,7 +41,7 @@ class Program:
     def __del__(self):
         h = getattr(self, "handle", None)
         if h:
-            lib().qcb_program_destroy(h)
+            self._destroy(h)
             self.handle = None
 
 
@@ -128,6 +129,7 @@ class PauliFrame:
         h = ctypes.c_void_p()
         check(lib().qcb_frame_create(int(frames), int(qubits), int(measurements), ctypes.byref(h)))
         self.handle = h
+        self._destroy = lib().qcb_frame_destroy
         self.frames, self.qubits, self.nbits = int(frames), int(qubits), int(measurements)
         self.shot_offset = int(shot_offset)
         if init:
@@ -136,7 +138,7 @@ class PauliFrame:
     def __del__(self):
         h = getattr(self, "handle", None)
         if h:
-            lib().qcb_frame_destroy(h)
+            self._destroy(h)
             self.handle = None
 
     def __len__(self):
@@ -310,6 +312,7 @@ class Batch:
         h = ctypes.c_void_p()
         check(lib().qcb_batch_create(arr, len(self.jobs), ctypes.byref(h)))
         self.handle = h
+        self._destroy = lib().qcb_batch_destroy
 
     def run(self, stream=None):
         check(lib().qcb_batch_run(self.handle, stream))
@@ -322,7 +325,7 @@ class Batch:
     def __del__(self):
         h = getattr(self, "handle", None)
         if h:
-            lib().qcb_batch_destroy(h)
+            self._destroy(h)
             self.handle = None
 
 
@@ -346,6 +349,7 @@ class Server:
         h = ctypes.c_void_p()
         check(lib().qcb_server_create(int(hbm_budget_bytes), int(slots), int(chunk_shots), ctypes.byref(h)))
         self.handle = h
+        self._destroy = lib().qcb_server_destroy
 
     def submit(self, circuit, shots: int, seed: int) -> int:
         arr = _ops.to_array(circuit)
@@ -392,7 +396,7 @@ class Server:
     def close(self):
         h = getattr(self, "handle", None)
         if h:
-            lib().qcb_server_destroy(h)
+            self._destroy(h)
             self.handle = None
 
     def __del__(self):

@@ -33,12 +33,13 @@ class DeviceTableau:
         h = ctypes.c_void_p()
         check(lib().qcb_tableau_create(int(rows), int(nqubits), ctypes.byref(h)))
         self.handle = h
+        self._destroy = lib().qcb_tableau_destroy
         self.rows, self.nqubits, self.W = int(rows), int(nqubits), nwords(nqubits)
 
     def __del__(self):
         h = getattr(self, "handle", None)
         if h:
-            lib().qcb_tableau_destroy(h)
+            self._destroy(h)
             self.handle = None
 
     def upload(self, phases: np.ndarray, xzs: np.ndarray):
@@ -578,6 +579,7 @@ class CanonBatch:
         h = ctypes.c_void_p()
         check(lib().qcb_canon_batch_create(handles, len(self.states), int(phases), int(cluster), ctypes.byref(h)))
         self.handle = h
+        self._destroy = lib().qcb_canon_batch_destroy
 
     def run(self, stream=None):
         check(lib().qcb_canon_batch_run(self.handle, stream))
@@ -593,5 +595,5 @@ class CanonBatch:
     def __del__(self):
         h = getattr(self, "handle", None)
         if h:
-            lib().qcb_canon_batch_destroy(h)
+            self._destroy(h)
             self.handle = None

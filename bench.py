@@ -742,7 +742,10 @@ def main():
     kernel_ms = ms
 
     # end to end through the public host API: ops from host memory in, record
-    # planes back to pinned host memory, every step.
+    # planes back to pinned host memory, every step.  The host call keeps the
+    # compiled program of the last op list on the device (it compares the op
+    # list each call), so no circuit bytes cross PCIe after the first call;
+    # the record is copied out chunk by chunk while later chunks run.
     words = (shots + 31) // 32
     rec_host = torch.empty((bmax, words), dtype=torch.int32, pin_memory=True)
     ops_host = arr  # numpy, host
@@ -789,8 +792,12 @@ def main():
                    "parallelism": f"shot-sharded x{world}",
                    "l2": "no flush: each step writes 240 MB (record + frame) > 126 MB L2; inputs are the 0.4 MB program"},
         "gpu_launches": int(launches),
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(arr.nbytes),
-                "d2h_bytes_per_step": int(bmax * words * 4), "ms_per_step": e2e_ms},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(bmax * words * 4), "ms_per_step": e2e_ms,
+                "api": "qcb_pftrajectories_host (one call: circuit + shots + seed in, record planes out)",
+                "host_inputs_bytes_per_step": int(arr.nbytes),
+                "inputs": "the op list is read from host memory every call and compared with the cached "
+                          "compiled program; the program crossed PCIe once, before the timed region"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)", "traffic": traffic,
                      "algorithmic_bytes_per_launch": model_bytes,

@@ -296,11 +296,9 @@ int qcb_pftrajectories_host(const qcb_op* ops, size_t n_ops, uint64_t frames,
 int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t seed,
                              uint64_t shot_offset, void* stream);
 
-/* Launch-shape overrides used by the tuner ("walker_tile", "walker_threads",
- * "walker_producers": warps that draw each flush's noise ahead of the walk,
- * 1..16, or -1 for none; "canon_threads", "canon_cluster", "project_cluster",
- * "canon_blocked": 1 always / 2 never run canonicalize! by 64-column
- * panels); 0 restores the automatic choice.                                 */
+/* Launch-shape overrides used by the tuner ("walker_tile", "canon_threads",
+ * "canon_cluster", "project_cluster", "canon_blocked": 1 always / 2 never
+ * run canonicalize! by 64-column panels); 0 restores the automatic choice. */
 int qcb_tune_set(const char* key, int64_t value);
 
 /* ------------------------------------------------------------ tableaux    */

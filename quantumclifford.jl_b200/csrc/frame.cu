@@ -53,10 +53,6 @@ struct WalkArgs {
   uint64_t col0;            // global column index of column 0
   const NoiseClass* classes;
   const uint32_t* cdf;      // Binomial count tables of the sparse classes
-  const uint4* flush_sites; // the FLUSH records' entries, flush by flush
-  const uint32_t* flush_off;  // [nflush + 1]
-  uint32_t nflush;
-  uint32_t nprod;           // producer warps of the warp-specialised walk (0: none)
   double pmax;
   int32_t* err;             // set to QCB_ETIMEOUT when a staging wait gives up
   // mask mode
@@ -223,43 +219,6 @@ constexpr uint32_t NOISE_KREG = 8;
 // in practice; it only bounds the loop).
 constexpr uint32_t NOISE_REDRAWS = 64;
 
-// The count k of one sparse (site, group) and, when k <= NOISE_KREG, its
-// event words w[0..k): word 0 of the stream gives k by inverse CDF against
-// the class's table, event e starts from word 1 + e, and duplicates of an
-// earlier event's position are redrawn from the next unused words k+1, ...
-__device__ __forceinline__ uint32_t sparse_events(const NoiseClass& c, const uint32_t* cdf, uint32_t site,
-                                                  uint32_t glo, uint32_t k0, uint32_t k1,
-                                                  uint32_t w[NOISE_KREG]) {
-  constexpr uint32_t PMASK = NOISE_GROUP - 1;
-  uint32_t o[4];
-  philox4x32_10(site, glo, 0u, TAG_NOISE, k0, k1, o);
-  const uint32_t* tb = cdf + c.cdf_off;
-  uint32_t k = 0;
-  while (k < c.cdf_len && o[0] >= __ldg(tb + k)) k++;
-  if (k == 0 || k > NOISE_KREG) return k;
-  uint32_t next = k + 1;  // next unused word
-#pragma unroll
-  for (uint32_t ev = 0; ev < NOISE_KREG; ev++) {
-    if (ev < k) {
-      if (((ev + 1) & 3) == 0) philox4x32_10(site, glo, (ev + 1) >> 2, TAG_NOISE, k0, k1, o);
-      w[ev] = o[(ev + 1) & 3];
-    }
-  }
-#pragma unroll
-  for (uint32_t ev = 1; ev < NOISE_KREG; ev++) {
-    if (ev < k) {
-      for (uint32_t r = 0; r < NOISE_REDRAWS; r++) {
-        bool dup = false;
-#pragma unroll
-        for (uint32_t j = 0; j < ev; j++) dup |= ((w[ev] ^ w[j]) & PMASK) == 0;
-        if (!dup) break;
-        w[ev] = noise_word(site, glo, next++, k0, k1);
-      }
-    }
-  }
-  return k;
-}
-
 // The events of one noise site on one group of NOISE_GROUP shots (group G of
 // the run, = 32 consecutive shot columns), from the words of noise_word.
 //  sparse: word 0 gives the event count k ~ Binomial(NOISE_GROUP, p_eff) by
@@ -293,16 +252,38 @@ __device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<
     return;
   }
   if (!c.cdf_len) return;
-  uint32_t w[NOISE_KREG];
-  const uint32_t k = sparse_events(c, a.cdf, site, glo, k0, k1, w);
+  philox4x32_10(site, glo, 0u, TAG_NOISE, k0, k1, o);
+  const uint32_t* tb = a.cdf + c.cdf_off;
+  uint32_t k = 0;
+  while (k < c.cdf_len && o[0] >= __ldg(tb + k)) k++;
   if (k == 0) return;
+  uint32_t next = k + 1;  // next unused word
   if (k <= NOISE_KREG) {
+    uint32_t w[NOISE_KREG];
+#pragma unroll
+    for (uint32_t ev = 0; ev < NOISE_KREG; ev++) {
+      if (ev < k) {
+        if (((ev + 1) & 3) == 0) philox4x32_10(site, glo, (ev + 1) >> 2, TAG_NOISE, k0, k1, o);
+        w[ev] = o[(ev + 1) & 3];
+      }
+    }
+#pragma unroll
+    for (uint32_t ev = 1; ev < NOISE_KREG; ev++) {
+      if (ev < k) {
+        for (uint32_t r = 0; r < NOISE_REDRAWS; r++) {
+          bool dup = false;
+#pragma unroll
+          for (uint32_t j = 0; j < ev; j++) dup |= ((w[ev] ^ w[j]) & PMASK) == 0;
+          if (!dup) break;
+          w[ev] = noise_word(site, glo, next++, k0, k1);
+        }
+      }
+    }
 #pragma unroll
     for (uint32_t ev = 0; ev < NOISE_KREG; ev++)
       if (ev < k) apply_code<SMEM>(F, e, sparse_code(kind, c, w[ev] >> 10), lc0, w[ev] & PMASK, c0, a.ncols);
     return;
   }
-  uint32_t next = k + 1;  // next unused word
   uint32_t bm[NOISE_GROUP / 32];  // positions taken so far
   for (uint32_t i = 0; i < NOISE_GROUP / 32; i++) bm[i] = 0;
   for (uint32_t ev = 0; ev < k; ev++) {
@@ -312,137 +293,6 @@ __device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<
     bm[(wv & PMASK) >> 5] |= 1u << (wv & 31);
     apply_code<SMEM>(F, e, sparse_code(kind, c, wv >> 10), lc0, wv & PMASK, c0, a.ncols);
   }
-}
-
-// ---------------------------------------------------------------- flush buffer
-// Warp-specialised walk (shared-memory tile, Philox noise): the last
-// a.nprod warps of the CTA draw the events of flush f + 1 while the other
-// warps apply the gates before it, and write them to a shared-memory buffer
-// as single bit flips of the tile, (plane | column << 16 | bit << 24); at
-// the flush every thread applies the buffer with shared-memory atomics.
-// The buffer holds FLUSH_BUF_WORDS flips; a (site, group) that does not fit
-// (or has a dense class, or more than NOISE_KREG events) is drawn again and
-// applied directly at the flush by its producer thread.  The flips are those
-// of sample_site_group, and XOR commutes, so the frame is the same bit for
-// bit.  Layout after the staging mbarriers: fx[0], fx[1] = buffer fill of
-// even / odd flushes, fx[2] = the walk gave up, fx[3] unused, fx + 4 = the
-// buffer.
-constexpr uint32_t FLUSH_BUF_WORDS = 2048;
-constexpr uint32_t FLUSH_BUF_BYTES = 16 + 4 * FLUSH_BUF_WORDS;
-constexpr uint32_t FLUSH_NONE = 0xFFFFFFFFu;  // a buffer slot without a flip
-
-// Barrier 1: the walking warps only (nc threads); barrier 2: the whole CTA.
-__device__ __forceinline__ void bar_walkers(uint32_t nc) {
-  asm volatile("bar.sync 1, %0;" ::"r"(nc) : "memory");
-}
-__device__ __forceinline__ bool bar_walkers_or(uint32_t nc, bool v) {
-  uint32_t r;
-  asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
-      : "=r"(r)
-      : "r"((uint32_t)v), "r"(nc)
-      : "memory");
-  return r != 0;
-}
-__device__ __forceinline__ void bar_cta() {
-  asm volatile("bar.sync 2, %0;" ::"r"(blockDim.x) : "memory");
-}
-
-// Producer side: the events of one (site, group) into the buffer.  Returns
-// false when the task must be drawn again and applied directly at the flush.
-__device__ __forceinline__ bool buffer_site_group(const WalkArgs& a, const uint4& e, uint64_t G, int32_t lc0,
-                                                  uint64_t c0, uint32_t T, uint32_t* eb, uint32_t* fill) {
-  const uint32_t kind = e.y & 0xFFu;
-  const NoiseClass c = a.classes[e.y >> 8];
-  if (c.dense) return false;
-  if (!c.cdf_len) return true;
-  uint32_t w[NOISE_KREG];
-  const uint32_t k = sparse_events(c, a.cdf, e.x, (uint32_t)G, (uint32_t)a.seed, (uint32_t)(a.seed >> 32), w);
-  if (k == 0) return true;
-  if (k > NOISE_KREG) return false;
-  const uint32_t per = kind == QCB_OP_DEPOL2 ? 4u : 2u;
-  const uint32_t need = k * per;
-  const uint32_t base = atomicAdd(fill, need);
-  if (base >= FLUSH_BUF_WORDS || need > FLUSH_BUF_WORDS - base) {
-    for (uint32_t i = base; i < FLUSH_BUF_WORDS && i < base + need; i++) eb[i] = FLUSH_NONE;
-    return false;
-  }
-#pragma unroll
-  for (uint32_t ev = 0; ev < NOISE_KREG; ev++) {
-    if (ev < k) {
-      const uint32_t code = sparse_code(kind, c, w[ev] >> 10), pos = w[ev] & (NOISE_GROUP - 1);
-      const int32_t lc = lc0 + (int32_t)(pos >> 5);
-      const bool in = lc >= 0 && lc < (int32_t)T && c0 + (uint64_t)lc < a.ncols;
-      const uint32_t at = (((uint32_t)lc & 0xFFu) << 16) | ((pos & 31u) << 24);
-      uint32_t* d = eb + base + ev * per;
-      d[0] = (in && (code & 1u)) ? ((e.z & 0xFFFFu) | at) : FLUSH_NONE;
-      d[1] = (in && (code & 2u)) ? ((e.z >> 16) | at) : FLUSH_NONE;
-      if (per == 4u) {
-        d[2] = (in && (code & 4u)) ? ((e.w & 0xFFFFu) | at) : FLUSH_NONE;
-        d[3] = (in && (code & 8u)) ? ((e.w >> 16) | at) : FLUSH_NONE;
-      }
-    }
-  }
-  return true;
-}
-
-// Every thread: flips [tid, tid + nth, ...) of flush f's buffer.
-__device__ __forceinline__ void apply_flush_buffer(uint32_t* sm, uint32_t T, const uint32_t* fx, uint32_t f) {
-  const uint32_t n = min(fx[f & 1], FLUSH_BUF_WORDS);
-  const uint32_t* eb = fx + 4;
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    const uint32_t v = eb[i];
-    if (v >> 29) continue;  // FLUSH_NONE
-    atomicXor(sm + (v & 0xFFFFu) * T + ((v >> 16) & 0xFFu), 1u << (v >> 24));
-  }
-}
-
-// The producer warps' part of one tile: for each flush, draw its (site,
-// group) tasks into the buffer, meet the walkers at the flush (CTA barrier),
-// apply, apply the tasks left over directly, and release the walkers
-// (second CTA barrier).  A task index j < 32 left over is a bit of `left`;
-// from the first one at j >= 32 on, the thread buffers nothing more in this
-// flush and applies all its later tasks directly.
-__device__ bool produce_tile(const WalkArgs& a, uint32_t* sm, uint32_t* fx, uint64_t tile, uint32_t nc) {
-  const uint32_t ptid = threadIdx.x - nc, npt = blockDim.x - nc, T = a.tile;
-  const uint64_t c0 = tile * T;
-  const uint64_t gc0 = a.col0 + c0;
-  const uint64_t gc1 = a.col0 + min(c0 + T, a.ncols);
-  const uint64_t G0 = gc0 / 32;
-  const uint32_t ng = (uint32_t)((gc1 - 1) / 32 - G0 + 1);
-  const Tile<true> F{sm, a.planes, sm, a.pitch, T};
-  uint32_t* eb = fx + 4;
-  for (uint32_t f = 0; f < a.nflush; f++) {
-    const uint32_t s0 = __ldg(a.flush_off + f), s1 = __ldg(a.flush_off + f + 1);
-    const uint32_t ntask = (s1 - s0) * ng;
-    uint32_t left = 0, left_from = 0xFFFFFFFFu, j = 0;
-    for (uint32_t t = ptid; t < ntask; t += npt, j++) {
-      const uint32_t i = t / ng, gl = t - i * ng;
-      const uint4 e = __ldg(a.flush_sites + s0 + i);
-      const int32_t lc0 = (int32_t)((int64_t)((G0 + gl) * 32) - (int64_t)gc0);
-      if (!buffer_site_group(a, e, G0 + gl, lc0, c0, T, eb, &fx[f & 1])) {
-        if (j < 32) {
-          left |= 1u << j;
-        } else {
-          left_from = j;
-          break;
-        }
-      }
-    }
-    bar_cta();  // the walkers reached flush f: the frame before it is complete
-    apply_flush_buffer(sm, T, fx, f);
-    j = 0;
-    for (uint32_t t = ptid; t < ntask; t += npt, j++) {
-      if (j < 32 ? !((left >> j) & 1u) : j < left_from) continue;
-      const uint32_t i = t / ng, gl = t - i * ng;
-      const uint4 e = __ldg(a.flush_sites + s0 + i);
-      const int32_t lc0 = (int32_t)((int64_t)((G0 + gl) * 32) - (int64_t)gc0);
-      sample_site_group<true>(a, F, e, G0 + gl, lc0, c0);
-    }
-    bar_cta();  // flush f is applied
-  }
-  bar_cta();  // the walkers wrote the tile back
-  return fx[2] == 0;
 }
 
 // ---------------------------------------------------------------- walker
@@ -458,17 +308,11 @@ __device__ __forceinline__ uint2 xor2(uint2 a, uint2 b) { return make_uint2(a.x 
 // two staging buffers (window kwin in buffer kwin & 1); after each window
 // thread 0 calls issue(kwin + 2) for the window two ahead.  Returns false
 // when a staging wait gave up (the job's status word then holds
-// QCB_ETIMEOUT).  SPEC: the last a.nprod warps run produce_tile (the flush
-// buffer above) and the walkers order their records with a barrier of their
-// own; each walker still passes exactly a.nflush flush barrier pairs and the
-// tile-end barrier on every path, so the two sides always meet.
-template <bool SMEM, bool PHILOX, bool SPEC, class Issue>
+// QCB_ETIMEOUT).
+template <bool SMEM, bool PHILOX, class Issue>
 __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint32_t* win0, uint32_t* win1,
-                                          uint64_t* bars, uint32_t* fx, uint64_t& kwin, Issue& issue,
-                                          uint64_t tile) {
-  const uint32_t NC = SPEC ? blockDim.x - 32u * a.nprod : blockDim.x;  // walking threads
-  if (SPEC && threadIdx.x >= NC) return produce_tile(a, sm, fx, tile, NC);
-  const uint32_t tid = threadIdx.x, T = a.tile, TP = T / 2, R = NC / TP;
+                                          uint64_t* bars, uint64_t& kwin, Issue& issue, uint64_t tile) {
+  const uint32_t tid = threadIdx.x, T = a.tile, TP = T / 2, R = blockDim.x / TP;
   const uint32_t cp = tid % TP, rr = tid / TP, cw = 2 * cp;  // cw: tile column of the pair
   const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
   const uint64_t pitch = a.pitch, rpitch = a.rec_pitch;
@@ -521,25 +365,17 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
   const uint32_t* wp = nullptr;
   bool need_window = true;
   bool done = false;
-  uint32_t nfl = 0;  // flushes met (SPEC)
   while (!done) {
     if (need_window) {
       const bool ok = mbar_wait(&bars[kwin & 1], (uint32_t)((kwin >> 1) & 1));
-      const bool gave_up = SPEC ? bar_walkers_or(NC, !ok) : __syncthreads_or(!ok);
-      if (gave_up) {  // every walker takes the same branch
+      if (__syncthreads_or(!ok)) {  // every thread takes the same branch
         if (tid == 0) atomicExch(a.err, QCB_ETIMEOUT);
-        if (SPEC) {  // meet the producers at every flush left and at the tile end
-          if (tid == 0) fx[2] = 1u;
-          for (; nfl < a.nflush; nfl++) { bar_cta(); bar_cta(); }
-          bar_cta();
-        }
         return false;
       }
       wp = (kwin & 1) ? win1 : win0;
       need_window = false;
     }
-    if (SPEC) bar_walkers(NC);
-    else __syncthreads();  // the tile init / the previous record is complete
+    __syncthreads();  // the tile init / the previous record is complete
     const uint4 h = *(const uint4*)wp;
     const uint32_t kind = h.x >> 24, cnt = h.x & 0xFFFFFFu;
     const uint32_t* e = wp + 4;
@@ -681,20 +517,7 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
       case SEG_FLUSH: {
         wp = e + cnt * 4;
         const uint4* en = (const uint4*)e;
-        if (SPEC) {
-          // the producers drew this flush's events; a flush split over
-          // windows is applied at its last part (no gate record between)
-          if (h.y & FLAG_NO_BARRIER) break;
-          if (nfl < a.nflush) {
-            bar_cta();  // the frame before the flush is complete
-            apply_flush_buffer(sm, T, fx, nfl);
-            bar_cta();  // every flip of the flush is applied
-            if (tid == 0) fx[nfl & 1] = 0u;  // refilled only after the next flush's barriers
-            nfl++;
-          } else if (tid == 0) {
-            atomicExch(a.err, QCB_EUNSUPPORTED);  // more flushes than the program lists
-          }
-        } else if (PHILOX) {
+        if (PHILOX) {
           if (a.pmax > 0.0) {
             // (site, shot group) tasks over all threads of the CTA; a group
             // is 32 run columns and may straddle the tile's edges
@@ -745,8 +568,7 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
         break;
     }
     if (kind == SEG_WIN || kind == SEG_END) {
-      if (SPEC) bar_walkers(NC);
-      else __syncthreads();  // every thread is done with this window
+      __syncthreads();  // every thread is done with this window
       if (tid == 0) issue(kwin + 2);
       kwin++;
       need_window = true;
@@ -769,27 +591,20 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
       *gz = x;
     }
   }
-  if (SPEC) {
-    if (nfl < a.nflush && tid == 0) atomicExch(a.err, QCB_EUNSUPPORTED);  // fewer flushes than listed
-    for (; nfl < a.nflush; nfl++) { bar_cta(); bar_cta(); }
-    bar_cta();
-  } else {
-    __syncthreads();
-  }
+  __syncthreads();
   return true;
 }
 
 // The plain launch: one program on one frame, CTA b walking tiles b, b + grid, ...
-template <bool SMEM, bool PHILOX, bool SPEC>
+template <bool SMEM, bool PHILOX>
 __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
   extern __shared__ __align__(128) uint32_t sm[];
   const uint32_t tid = threadIdx.x, T = a.tile;
-  // layout: [frame tile | pmap] [window 0] [window 1] [2 mbarriers] [flush buffer (SPEC)]
+  // layout: [frame tile | pmap] [window 0] [window 1] [2 mbarriers]
   const uint32_t tile_words = SMEM ? 2 * a.nslots * T : 2 * a.nslots;
   uint32_t* win0 = sm + ((tile_words + 31) & ~31u);
   uint32_t* win1 = win0 + PROG_WINDOW_WORDS;
   uint64_t* bars = (uint64_t*)(win1 + PROG_WINDOW_WORDS);
-  uint32_t* fx = (uint32_t*)(bars + 2);
   if (!SMEM)
     for (uint32_t p = tid; p < 2 * a.nslots; p += blockDim.x) sm[p] = 2 * a.slot_qubit[p >> 1] + (p & 1);
   const uint64_t ntiles = (a.ncols + T - 1) / T;
@@ -799,7 +614,6 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    if (SPEC) fx[0] = fx[1] = fx[2] = fx[3] = 0u;
   }
   __syncthreads();
   // window k of the flattened (tile, window) sequence lives in buffer k & 1
@@ -813,7 +627,7 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
   uint64_t kwin = 0;
   bool failed = false;
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    if (!walk_tile<SMEM, PHILOX, SPEC>(a, sm, win0, win1, bars, fx, kwin, issue, tile)) {
+    if (!walk_tile<SMEM, PHILOX>(a, sm, win0, win1, bars, kwin, issue, tile)) {
       failed = true;
       break;
     }
@@ -899,7 +713,7 @@ __global__ void __launch_bounds__(768, 1) batch_walker_kernel(const BatchArgs b)
     for (uint32_t w = tid; w < sizeof(WalkArgs) / 8; w += blockDim.x)
       ((uint64_t*)&ja)[w] = ((const uint64_t*)(b.jobs + bi.job))[w];
     __syncthreads();
-    if (!walk_tile<true, true, false>(ja, sm, win0, win1, bars, nullptr, kwin, issue, bi.tile)) {
+    if (!walk_tile<true, true>(ja, sm, win0, win1, bars, kwin, issue, bi.tile)) {
       failed = true;
       break;
     }
@@ -1079,18 +893,14 @@ namespace qcb {
 // qubits of a tile of >= 64 columns fit, else HBM planes).
 struct WalkConfig {
   bool smem;
-  bool spec;      // warp-specialised (producer warps draw the noise ahead)
   uint32_t T;     // tile columns
   uint32_t nth;   // threads per CTA
-  uint32_t nprod; // producer warps (spec)
   uint32_t grid;
   size_t smem_bytes;
 };
 
 static uint32_t g_tile_override = 0;
 static uint32_t g_threads_override = 0;  // threads per CTA (0: 768)
-static int32_t g_producers = 0;          // producer warps (0: default, < 0: no warp specialisation)
-constexpr uint32_t DEFAULT_PRODUCER_WARPS = 8;
 
 // Tile width (even: threads own column pairs) for ncols columns with tiles of
 // at most tmax columns: the fewest waves of one CTA per SM, then the narrowest
@@ -1105,17 +915,11 @@ static uint32_t balanced_tile(uint64_t ncols, uint32_t tmax) {
 }
 
 // Shared-memory tile when 2 planes x 16 columns of every touched qubit fit,
-// else the same walker on the HBM planes.  A noisy Philox run on a
-// shared-memory tile is warp-specialised: producer warps plus walking
-// threads (whole column-pair rows, rounded up to whole warps).
-static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f, bool philox) {
+// else the same walker on the HBM planes.
+static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   WalkConfig wc{};
-  const uint32_t threads = g_threads_override ? g_threads_override : 768u;
-  const uint32_t np = g_producers > 0 ? (uint32_t)g_producers : DEFAULT_PRODUCER_WARPS;
-  bool spec = philox && p->pmax > 0.0 && p->info.n_flushes > 0 && g_producers >= 0 && 32 * np < threads;
   const size_t per_col = (size_t)2 * std::max<uint32_t>(p->nslots, 1) * 4;
-  // windows, mbarriers, alignment (+ the flush buffer)
-  const size_t stage = (size_t)2 * PROG_WINDOW_WORDS * 4 + 16 + 128 + (spec ? FLUSH_BUF_BYTES : 0);
+  const size_t stage = (size_t)2 * PROG_WINDOW_WORDS * 4 + 16 + 128;  // windows, mbarriers, alignment
   const size_t maxsm = (size_t)device_max_smem_optin();
   const size_t budget = maxsm > stage ? maxsm - stage : 0;
   uint32_t T = 0;
@@ -1124,18 +928,11 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f, bool phi
   } else if (budget / per_col >= 16) {
     T = balanced_tile(f->ncols, (uint32_t)std::min<size_t>(256, budget / per_col));
   }
+  const uint32_t threads = g_threads_override ? g_threads_override : 768u;
   if (T) {
     wc.smem = true;
     wc.T = T;
-    const uint32_t nc = spec ? ((threads - 32 * np) / (T / 2)) * (T / 2) : 0;
-    if (spec && nc > 0) {
-      wc.nth = ((nc + 31) & ~31u) + 32 * np;  // <= threads rounded up to a warp, <= 768
-      wc.nprod = np;
-    } else {
-      spec = false;
-      wc.nth = (threads / (T / 2)) * (T / 2);  // column pairs; the kernel's launch bound is 768
-    }
-    wc.spec = spec;
+    wc.nth = (threads / (T / 2)) * (T / 2);  // column pairs; the kernel's launch bound is 768
     wc.smem_bytes = per_col * T + stage;
   } else {
     wc.smem = false;
@@ -1150,15 +947,13 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f, bool phi
 
 int launch_walker(qcb_frame* f, const qcb_program* p, WalkArgs& a, bool philox, bool fresh,
                   cudaStream_t st) {
-  WalkConfig wc = walk_config(p, f, philox);
+  WalkConfig wc = walk_config(p, f);
   a.fresh = fresh ? 1 : 0;
   a.tile = wc.T;
-  a.nprod = wc.spec ? wc.nprod : 0;
   if (!f->ncols) return QCB_OK;
   void (*kern)(const WalkArgs);
-  if (wc.smem && wc.spec) kern = walker_kernel<true, true, true>;
-  else if (wc.smem) kern = philox ? walker_kernel<true, true, false> : walker_kernel<true, false, false>;
-  else kern = philox ? walker_kernel<false, true, false> : walker_kernel<false, false, false>;
+  if (wc.smem) kern = philox ? walker_kernel<true, true> : walker_kernel<true, false>;
+  else kern = philox ? walker_kernel<false, true> : walker_kernel<false, false>;
   if (wc.smem_bytes > 48 * 1024)
     QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin()));
   kern<<<wc.grid, wc.nth, wc.smem_bytes, st>>>(a);
@@ -1184,9 +979,6 @@ static void fill_common(WalkArgs& a, qcb_frame* f, const qcb_program* p) {
   a.nwin = (uint32_t)(p->stream_slot.size() / PROG_WINDOW_WORDS);
   a.classes = p->d_classes;
   a.cdf = p->d_cdf;
-  a.flush_sites = (const uint4*)p->d_flush_sites;
-  a.flush_off = p->d_flush_off;
-  a.nflush = p->info.n_flushes;
   a.pmax = p->pmax;
   a.err = f->err;
 }
@@ -1458,7 +1250,6 @@ extern "C" int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* p, uint
 namespace qcb {
 void set_walker_tile(uint32_t t) { g_tile_override = t; }
 void set_walker_threads(uint32_t t) { g_threads_override = t; }
-void set_walker_producers(int32_t w) { g_producers = w; }
 int run_program_fresh(qcb_frame* f, const qcb_program* p, uint64_t seed, uint64_t shot_offset,
                       cudaStream_t st) {
   qcb_noise_source n{};

@@ -259,8 +259,6 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
 
   double pmax = 0;
   uint32_t nseg = 0, nflush = 0;
-  P.flush_sites.clear();
-  P.flush_off.assign(1, 0u);
   if (2ull * P.nslots > 65536) return fail(QCB_EUNSUPPORTED, "at most 32768 distinct qubits per program");
 
   // Noise classes: sites of one opcode with equal probabilities share one
@@ -353,9 +351,6 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
       r.w.push_back(pk(s.xa, s.za));
       r.w.push_back(pk(s.xb, s.zb));
     }
-    // the same entries, flush by flush, for warps that sample ahead of the walk
-    P.flush_sites.insert(P.flush_sites.end(), r.w.begin(), r.w.end());
-    P.flush_off.push_back((uint32_t)(P.flush_sites.size() / 4));
     recs.push_back(std::move(r));
     nflush++;
     st.clear();
@@ -501,8 +496,6 @@ int upload(Program& P) {
   if (e == cudaSuccess) e = up(&P.d_qubit_slot, qs);
   std::vector<uint32_t> sw(P.slot_swap.begin(), P.slot_swap.end());
   if (e == cudaSuccess) e = up(&P.d_slot_swap, sw);
-  if (e == cudaSuccess) e = up(&P.d_flush_sites, P.flush_sites);
-  if (e == cudaSuccess) e = up(&P.d_flush_off, P.flush_off);
   if (e != cudaSuccess) return cuda_fail(e, "qcb_program_compile upload");
   return QCB_OK;
 }
@@ -514,9 +507,6 @@ void release(Program& P) {
   cudaFree(P.d_slot_qubit);
   cudaFree(P.d_qubit_slot);
   cudaFree(P.d_slot_swap);
-  cudaFree(P.d_flush_sites);
-  cudaFree(P.d_flush_off);
-  P.d_flush_sites = P.d_flush_off = nullptr;
   P.d_stream_slot = nullptr;
   P.d_classes = nullptr;
   P.d_cdf = nullptr;

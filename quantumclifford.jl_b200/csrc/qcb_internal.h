@@ -143,8 +143,6 @@ struct Program {
   std::vector<uint8_t> slot_swap;     // final x<->z relabel per slot
   std::vector<NoiseClass> classes;
   std::vector<uint32_t> cdf;          // Binomial count thresholds of the sparse classes
-  std::vector<uint32_t> flush_sites;  // the FLUSH records' site entries (4 words each), flush by flush
-  std::vector<uint32_t> flush_off;    // [n_flushes + 1]: first entry of each flush
   double pmax = 0;
   // device copies
   uint32_t* d_stream_slot = nullptr;
@@ -153,8 +151,6 @@ struct Program {
   uint32_t* d_slot_qubit = nullptr;
   uint32_t* d_slot_swap = nullptr;
   uint32_t* d_qubit_slot = nullptr;   // [nq_alloc] qubit -> slot or NONE
-  uint32_t* d_flush_sites = nullptr;
-  uint32_t* d_flush_off = nullptr;
   uint32_t qubit_slot_len = 0;
   uint64_t hash = 0;
 };

@@ -49,7 +49,6 @@ __global__ void philox_probe_kernel(uint4 ctr, uint2 key, uint32_t* out) {
 
 void set_walker_tile(uint32_t t);
 void set_walker_threads(uint32_t t);
-void set_walker_producers(int32_t w);
 void set_canon_cluster(uint32_t cs);
 void set_canon_threads(uint32_t n);
 void set_project_cluster(uint32_t cs);
@@ -107,17 +106,13 @@ uint64_t qcb_launch_count(void) { return g_launches.load(); }
 int qcb_tune_set(const char* key, int64_t value) {
   if (!key) return fail(QCB_EARG, "qcb_tune_set: null key");
   const std::string k(key);
-  if ((value < 0 && !(k == "walker_producers" && value == -1)) || value > 1024)
-    return fail(QCB_EARG, "qcb_tune_set: value out of range");
+  if (value < 0 || value > 1024) return fail(QCB_EARG, "qcb_tune_set: value out of range");
   if (k == "walker_tile") {
     if (value && (value < 8 || value > 256 || value % 2)) return fail(QCB_EARG, "walker_tile must be 0 (automatic) or even, 8..256");
     set_walker_tile((uint32_t)value);
   } else if (k == "walker_threads") {
     if (value && (value < 64 || value > 768 || value % 32)) return fail(QCB_EARG, "walker_threads must be 0 (768) or 64..768, a multiple of 32");
     set_walker_threads((uint32_t)value);
-  } else if (k == "walker_producers") {
-    if (value < -1 || value > 16) return fail(QCB_EARG, "walker_producers must be -1 (off), 0 (default) or 1..16 warps");
-    set_walker_producers((int32_t)value);
   } else if (k == "canon_threads") {
     if (value && (value < 64 || value > 1024 || value % 32)) return fail(QCB_EARG, "canon_threads must be 0 or 64..1024, a multiple of 32");
     set_canon_threads((uint32_t)value);

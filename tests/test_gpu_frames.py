@@ -194,47 +194,6 @@ def test_philox_sparse_noise_any_tile_width(qcb, tile, d, p):
     assert np.array_equal(coding(f.xzs(), qmax + 1), coding(ox, qmax + 1))
 
 
-def _crowded_flush_circuit(n=600, p=0.012):
-    """One flush with n sparse 1q sites (about 12 events per 1024-shot group
-    each) and n/2 two-qubit depolarising sites, then one with a dense site
-    among sparse ones: far more flips than the walker's flush buffer holds."""
-    c = [O.sHadamard(q) for q in range(1, n + 1)]
-    c += O.PauliError(list(range(1, n + 1)), p)
-    for q in range(1, n, 2):
-        c += O.NoiseOp(O.DepolarizationNoise(p), (q, q + 1))
-    c += [O.sCNOT(q, q + 1) for q in range(1, n, 2)]
-    c += O.PauliError(list(range(1, 40)), 0.2)  # dense (p_eff * 1024 > 16)
-    c += O.PauliError(list(range(40, 80)), 1e-3)
-    c += [O.sMZ(q, q) for q in range(1, n + 1)]
-    return c
-
-
-@pytest.mark.parametrize("producers", [-1, 1, 2, 8, 16])
-def test_philox_producer_warps_bit_exact(qcb, producers):
-    """The warp-specialised walker (producer warps draw each flush's events
-    ahead into a shared-memory buffer): any producer count, buffer overflow
-    (tasks applied directly at the flush), more than 32 tasks per producer
-    thread (1-2 warps), dense and sparse sites in one flush; -1 turns the
-    specialisation off."""
-    arr = O.to_array(_crowded_flush_circuit())
-    qmax, bmax = O.affected_counts(arr)
-    sarr = O.to_array(circuits.rotated_surface_code_memory(5, 5, 0.004))
-    sq, sb = O.affected_counts(sarr)
-    frames = 5 * 1024 + 77
-    qcb.check(qcb.lib().qcb_tune_set(b"walker_producers", producers))
-    try:
-        f = qcb.pftrajectories(arr, trajectories=frames, seed=4242)
-        g = qcb.pftrajectories(sarr, trajectories=frames, seed=7)
-    finally:
-        qcb.check(qcb.lib().qcb_tune_set(b"walker_producers", 0))
-    ox, om = oracle.pftrajectories_philox(arr, frames, qmax, bmax, 4242)
-    assert np.array_equal(f.measurements(), om)
-    assert np.array_equal(coding(f.xzs(), qmax + 1), coding(ox, qmax + 1))
-    sx, sm = oracle.pftrajectories_philox(sarr, frames, sq, sb, 7)
-    assert np.array_equal(g.measurements(), sm)
-    assert np.array_equal(coding(g.xzs(), sq + 1), coding(sx, sq + 1))
-
-
 @pytest.mark.parametrize("tile", [16, 40, 106])
 def test_mask_mode_any_tile_width(qcb, tile):
     circ = circuits.rotated_surface_code_memory(3, 3, 0.01)

@@ -451,9 +451,9 @@ __global__ void __launch_bounds__(1024) generate_kernel(uint64_t* pauli, uint8_t
 constexpr uint32_t PANEL = 64;
 
 struct BlockedLayout {
-  size_t rows_off, pw_off, comb_off, po_off, xt_off, cml_off, c_off, a_off, pwp_off, d_off;  // u64 offsets
-  size_t pos_off, stp_off;                                                                 // u32 offsets
-  size_t bt_off, qo_off, qp_off, lph_off, ql_off;                                          // byte offsets
+  size_t rows_off, po_off, xt_off, cml_off, c_off, a_off, pwp_off, d_off;  // u64 offsets
+  size_t pos_off, stp_off;                                                 // u32 offsets
+  size_t bt_off, qo_off, qp_off, lph_off, ql_off;                          // byte offsets
   size_t u32_base, u8_base, bytes;
 };
 
@@ -461,8 +461,6 @@ __host__ __device__ inline BlockedLayout blocked_layout(uint32_t rows, uint32_t 
   BlockedLayout L{};
   size_t o = 0;
   L.rows_off = o; o += smem_rows ? (size_t)RB * (W + 1) : 0;
-  L.pw_off = o;
-  L.comb_off = o;
   L.po_off = o; o += (size_t)PANEL * W;
   L.xt_off = o; o += (size_t)PANEL * (W / 2);
   L.cml_off = o; o += RB;

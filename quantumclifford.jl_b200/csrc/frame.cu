@@ -253,9 +253,19 @@ __device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<
   }
   if (!c.cdf_len) return;
   philox4x32_10(site, glo, 0u, TAG_NOISE, k0, k1, o);
-  const uint32_t* tb = a.cdf + c.cdf_off;
+  // k = number of table entries <= word 0 (the table is non-decreasing, so
+  // this is the inverse CDF), four entries per 16-byte read: one read for
+  // counts below 4
+  const uint4* tb = (const uint4*)(a.cdf + c.cdf_off);
   uint32_t k = 0;
-  while (k < c.cdf_len && o[0] >= __ldg(tb + k)) k++;
+  for (uint32_t b = 0; b < c.cdf_len; b += 4) {
+    const uint4 t = __ldg(tb + (b >> 2));
+    const uint32_t lim = c.cdf_len - b;
+    const uint32_t m = (uint32_t)(o[0] >= t.x) + (uint32_t)(lim > 1 && o[0] >= t.y) +
+                       (uint32_t)(lim > 2 && o[0] >= t.z) + (uint32_t)(lim > 3 && o[0] >= t.w);
+    k += m;
+    if (m < 4) break;
+  }
   if (k == 0) return;
   uint32_t next = k + 1;  // next unused word
   if (k <= NOISE_KREG) {
@@ -526,8 +536,11 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
             const uint64_t G0 = gc0 / 32;
             const uint32_t ng = (uint32_t)((gc1 - 1) / 32 - G0 + 1);
             const uint32_t ntask = cnt * ng;
+            // t / ng as a multiply-high for ng >= 2: ng <= 10 and t < 2^13 (a
+            // record part fits one window), far inside t * (mg * ng - 2^32) < 2^32
+            const uint32_t mg = ng > 1 ? 0xFFFFFFFFu / ng + 1u : 0u;
             for (uint32_t t = tid; t < ntask; t += blockDim.x) {
-              const uint32_t i = t / ng, gl = t - i * ng;
+              const uint32_t i = ng > 1 ? __umulhi(t, mg) : t, gl = t - i * ng;
               const int32_t lc0 = (int32_t)((int64_t)((G0 + gl) * 32) - (int64_t)gc0);
               sample_site_group<SMEM>(a, F, en[i], G0 + gl, lc0, c0);
             }

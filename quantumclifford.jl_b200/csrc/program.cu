@@ -275,6 +275,7 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     if (!c.dense && s.peff > 0.0) {
       auto t = table_of.find(s.peff);
       if (t == table_of.end()) {
+        while (cdf.size() % 4) cdf.push_back(0xFFFFFFFFu);  // tables start on 16 bytes (read 4 at a time)
         const uint32_t off = (uint32_t)cdf.size();
         binomial_count_table(s.peff, cdf);
         t = table_of.emplace(s.peff, std::make_pair(off, (uint32_t)cdf.size() - off)).first;
@@ -468,6 +469,7 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   out.push_back(SEG_END << 24); out.push_back(0); out.push_back(0); out.push_back(0);
   while (out.size() % PROG_WINDOW_WORDS) out.push_back(0);
   P.classes = classes;
+  while (cdf.size() % 4) cdf.push_back(0xFFFFFFFFu);  // the last 4-word read stays inside
   P.cdf = cdf;
   P.info.n_segments = nseg;
   P.info.n_flushes = nflush;

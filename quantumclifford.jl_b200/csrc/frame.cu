@@ -967,8 +967,13 @@ int launch_walker(qcb_frame* f, const qcb_program* p, WalkArgs& a, bool philox, 
   void (*kern)(const WalkArgs);
   if (wc.smem) kern = philox ? walker_kernel<true, true> : walker_kernel<true, false>;
   else kern = philox ? walker_kernel<false, true> : walker_kernel<false, false>;
-  if (wc.smem_bytes > 48 * 1024)
+  if (wc.smem_bytes > 48 * 1024) {
     QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin()));
+    // all of the unified L1 / shared memory as shared memory, so that two
+    // narrow tiles can share an SM when their frames fit side by side
+    QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared));
+  }
   kern<<<wc.grid, wc.nth, wc.smem_bytes, st>>>(a);
   QCB_LAUNCHED();
   return QCB_OK;

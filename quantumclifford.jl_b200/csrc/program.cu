@@ -452,6 +452,12 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   };
   for (auto& r : recs) {
     const uint32_t n = (uint32_t)(r.w.size() / r.entry_words);
+    // A record that fits one window is not split: it starts the next window
+    // when the rest of this one is too small.  Every part of a split record
+    // is one more step of the walk, with a CTA barrier before it and, for a
+    // flush, one more dependent sampling chain; padding costs only words.
+    const size_t whole = 4 + ((r.w.size() + 3) & ~(size_t)3);
+    if (whole <= PROG_WINDOW_WORDS - 4 && whole > room()) next_window();
     uint32_t done = 0;
     while (done < n) {
       if (room() < 4 + ((r.entry_words + 3) & ~3u)) next_window();

@@ -212,8 +212,10 @@ __device__ __forceinline__ uint32_t noise_word(uint32_t site, uint32_t glo, uint
   return sel4(o, i & 3);
 }
 
-// Events with at most this many per (site, group) stay in registers.
-constexpr uint32_t NOISE_KREG = 8;
+// Events with at most this many per (site, group) stay in registers (the
+// rest take the 1024-bit bitmap path, slow enough that a warp with one such
+// lane pays for it: d=11 launch 0.94 / 0.84 / 0.668 / 0.674 ms at 3 / 4 / 6 / 8).
+constexpr uint32_t NOISE_KREG = 6;
 // Redraws of one event's position before its last draw is kept (a collision
 // has probability below k/NOISE_GROUP per draw, so the cap is never reached
 // in practice; it only bounds the loop).

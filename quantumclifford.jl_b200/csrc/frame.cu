@@ -298,8 +298,13 @@ __device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<
   }
   uint32_t bm[NOISE_GROUP / 32];  // positions taken so far
   for (uint32_t i = 0; i < NOISE_GROUP / 32; i++) bm[i] = 0;
+  uint32_t blk = 0;  // o holds Philox block blk of the stream (block 0: the count word and words 1..3)
   for (uint32_t ev = 0; ev < k; ev++) {
-    uint32_t wv = noise_word(site, glo, 1 + ev, k0, k1);
+    if (((1 + ev) >> 2) != blk) {
+      blk = (1 + ev) >> 2;
+      philox4x32_10(site, glo, blk, TAG_NOISE, k0, k1, o);
+    }
+    uint32_t wv = sel4(o, (1 + ev) & 3);  // word 1 + ev, one block per four events
     for (uint32_t r = 0; r < NOISE_REDRAWS && ((bm[(wv & PMASK) >> 5] >> (wv & 31)) & 1u); r++)
       wv = noise_word(site, glo, next++, k0, k1);
     bm[(wv & PMASK) >> 5] |= 1u << (wv & 31);

@@ -63,3 +63,46 @@ def test_relabels_and_noise_interleave():
 def test_classical_xor_chains():
     info = check_circuit(xor_chain_circuit(np.random.default_rng(21)), 150, 4)
     assert info["n_flushes"] >= 1
+
+
+def _records(stream, win=2048):
+    """(kind, count, continued, words) of every record of a device program."""
+    body = {1: lambda c: (2 * c + 3) // 4 * 4, 3: lambda c: (2 * c + 3) // 4 * 4, 4: lambda c: (2 * c + 3) // 4 * 4,
+            6: lambda c: (2 * c + 3) // 4 * 4, 9: lambda c: (2 * c + 3) // 4 * 4, 5: lambda c: 4 * c,
+            7: lambda c: 16 * c, 8: lambda c: 4 * c, 11: lambda c: 32 * c}
+    out, pc = [], 0
+    while pc < len(stream):
+        h = int(stream[pc])
+        kind, cnt = h >> 24, h & 0xFFFFFF
+        if kind == 0:
+            break
+        if kind == 10:  # the stream continues in the next window
+            pc = pc // win * win + win
+            continue
+        n = body[kind](cnt)
+        assert pc // win == (pc + 4 + n - 1) // win, "a record straddles a window"
+        out.append((kind, cnt, int(stream[pc + 1]) & 1, 4 + n))
+        pc += 4 + n
+    return out
+
+
+@pytest.mark.parametrize("d", [3, 5, 11, 25])
+def test_records_that_fit_a_window_are_not_split(d):
+    """A split record is one more barrier-separated step of the walk, so the
+    compiler starts a new window for a record that fits one instead of
+    cutting it at the window edge; only longer records come in parts."""
+    stream, _, _, _, info = stream_emu.dump(circuits.rotated_surface_code_memory(d, d, 1e-3))
+    recs = _records(stream)
+    i = 0
+    while i < len(recs):
+        j = i
+        while recs[j][2]:  # parts of one record: all but the last are marked continued
+            assert recs[j + 1][0] == recs[i][0]
+            j += 1
+        total = 4 + sum(r[3] - 4 for r in recs[i:j + 1])
+        if j > i:
+            assert total > 2048 - 4, (d, i, total)
+        i = j + 1
+    if d <= 11:
+        assert not any(r[2] for r in recs)
+    assert sum(1 for r in recs if r[0] == 8 and not r[2]) == info["n_flushes"]

@@ -284,8 +284,13 @@ int qcb_evaluate_guesses(const qcb_frame* f, const uint32_t* logical_bits, size_
 
 /* pftrajectories(circuit; trajectories) (src/pauli_frames.jl:193-227) as one
  * host call: fresh frame, Philox initZ!, run, record copied back as
- * shot-packed planes [nbits][ceil(frames/32)].  The frame is kept on the
- * device for reuse between calls with the same shape.                       */
+ * shot-packed planes [nbits][ceil(frames/32)]; returns when the record is
+ * in `record_planes` (NULL: run only).  The compiled program of the last op
+ * list and the frame of the last shape stay on the device (the device
+ * current at the first call) for reuse.  Wide runs go as shot chunks whose
+ * record columns are copied out while the next chunk runs; the record is
+ * that of one launch.  Page-locked `record_planes` gets the full PCIe
+ * bandwidth.  Calls are serialised by an internal lock.                     */
 int qcb_pftrajectories_host(const qcb_op* ops, size_t n_ops, uint64_t frames,
                             uint64_t seed, uint64_t shot_offset,
                             uint32_t* record_planes, void* stream);

@@ -34,8 +34,9 @@
 namespace qcb {
 
 struct WalkArgs {
-  const uint4* prog;        // windowed stream (PROG_WINDOW_WORDS words per window)
+  const uint4* prog;        // windowed stream (win_words words per window)
   uint32_t nwin;            // windows in the stream
+  uint32_t win_words;       // words per window (the program's)
   uint32_t* planes;
   uint32_t* rec;            // record row b at rec + b * rec_pitch (column 0 of this frame)
   uint64_t pitch;
@@ -623,8 +624,8 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
   // layout: [frame tile | pmap] [window 0] [window 1] [2 mbarriers]
   const uint32_t tile_words = SMEM ? 2 * a.nslots * T : 2 * a.nslots;
   uint32_t* win0 = sm + ((tile_words + 31) & ~31u);
-  uint32_t* win1 = win0 + PROG_WINDOW_WORDS;
-  uint64_t* bars = (uint64_t*)(win1 + PROG_WINDOW_WORDS);
+  uint32_t* win1 = win0 + a.win_words;
+  uint64_t* bars = (uint64_t*)(win1 + a.win_words);
   if (!SMEM)
     for (uint32_t p = tid; p < 2 * a.nslots; p += blockDim.x) sm[p] = 2 * a.slot_qubit[p >> 1] + (p & 1);
   const uint64_t ntiles = (a.ncols + T - 1) / T;
@@ -640,8 +641,7 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
   auto issue = [&](uint64_t k) {
     if (k >= total_win) return;
     const uint32_t w = (uint32_t)(k % a.nwin);
-    stage_window((k & 1) ? win1 : win0, a.prog + (size_t)w * (PROG_WINDOW_WORDS / 4), PROG_WINDOW_WORDS * 4,
-                 &bars[k & 1]);
+    stage_window((k & 1) ? win1 : win0, a.prog + (size_t)w * (a.win_words / 4), a.win_words * 4, &bars[k & 1]);
   };
   if (tid == 0) { issue(0); issue(1); }
   uint64_t kwin = 0;
@@ -680,6 +680,8 @@ struct BatchArgs {
   uint32_t nitems;
   uint32_t tile_words;  // the largest frame tile of the jobs (words)
   uint32_t* head;       // next queue item (zero before the launch)
+  uint32_t win_words;   // the largest program window of the jobs (words): the staging buffers' size
+  uint32_t pad_;
 };
 
 constexpr uint32_t ITEM_NONE = 0xFFFFFFFFu;
@@ -691,8 +693,8 @@ __global__ void __launch_bounds__(768, 1) batch_walker_kernel(const BatchArgs b)
   __shared__ __align__(16) WalkArgs ja;
   const uint32_t tid = threadIdx.x;
   uint32_t* win0 = sm + ((b.tile_words + 31) & ~31u);
-  uint32_t* win1 = win0 + PROG_WINDOW_WORDS;
-  uint64_t* bars = (uint64_t*)(win1 + PROG_WINDOW_WORDS);
+  uint32_t* win1 = win0 + b.win_words;
+  uint64_t* bars = (uint64_t*)(win1 + b.win_words);
   // staging side (thread 0): the item being staged and its next window
   uint32_t icur = ITEM_NONE, iw = 0, iq = 0;
   uint64_t issued = 0;
@@ -703,7 +705,7 @@ __global__ void __launch_bounds__(768, 1) batch_walker_kernel(const BatchArgs b)
   auto issue = [&](uint64_t) {
     if (icur == ITEM_NONE) return;
     const WalkArgs& J = b.jobs[b.items[icur].job];
-    stage_window((issued & 1) ? win1 : win0, J.prog + (size_t)iw * (PROG_WINDOW_WORDS / 4), PROG_WINDOW_WORDS * 4,
+    stage_window((issued & 1) ? win1 : win0, J.prog + (size_t)iw * (J.win_words / 4), J.win_words * 4,
                  &bars[issued & 1]);
     issued++;
     if (++iw == J.nwin) {
@@ -939,7 +941,7 @@ static uint32_t balanced_tile(uint64_t ncols, uint32_t tmax) {
 static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   WalkConfig wc{};
   const size_t per_col = (size_t)2 * std::max<uint32_t>(p->nslots, 1) * 4;
-  const size_t stage = (size_t)2 * PROG_WINDOW_WORDS * 4 + 16 + 128;  // windows, mbarriers, alignment
+  const size_t stage = (size_t)2 * p->win_words * 4 + 16 + 128;  // windows, mbarriers, alignment
   const size_t maxsm = (size_t)device_max_smem_optin();
   const size_t budget = maxsm > stage ? maxsm - stage : 0;
   uint32_t T = 0;
@@ -1001,7 +1003,8 @@ static void fill_common(WalkArgs& a, qcb_frame* f, const qcb_program* p) {
   a.qubit_slot = p->d_qubit_slot;
   a.qubit_slot_len = p->qubit_slot_len;
   a.prog = (const uint4*)p->d_stream_slot;
-  a.nwin = (uint32_t)(p->stream_slot.size() / PROG_WINDOW_WORDS);
+  a.win_words = p->win_words;
+  a.nwin = (uint32_t)(p->stream_slot.size() / p->win_words);
   a.classes = p->d_classes;
   a.cdf = p->d_cdf;
   a.pmax = p->pmax;
@@ -1292,10 +1295,10 @@ namespace qcb {
 static std::map<uint32_t, uint32_t> g_tuned_tile;
 
 // Widest tile (even, <= 256) whose frame fits one CTA's shared memory next to
-// the staging buffers; 0 when not even 16 columns fit.
-static uint32_t batch_tile_max(const qcb_program* p) {
+// staging buffers of win_words words; 0 when not even 16 columns fit.
+static uint32_t batch_tile_max(const qcb_program* p, uint32_t win_words) {
   const size_t per_col = (size_t)2 * std::max<uint32_t>(p->nslots, 1) * 4;
-  const size_t stage = (size_t)2 * PROG_WINDOW_WORDS * 4 + 16 + 128 + sizeof(WalkArgs) + 64;
+  const size_t stage = (size_t)2 * win_words * 4 + 16 + 128 + sizeof(WalkArgs) + 64;
   const size_t maxsm = (size_t)device_max_smem_optin();
   const size_t budget = maxsm > stage ? maxsm - stage : 0;
   uint32_t t = (uint32_t)std::min<size_t>(256, budget / per_col) & ~1u;
@@ -1311,6 +1314,7 @@ struct qcb_batch {
   uint32_t* d_head = nullptr;
   uint32_t nitems = 0;
   uint32_t tile_words = 0;
+  uint32_t win_words = 0;
   size_t smem_bytes = 0;
   uint32_t grid = 0;
 };
@@ -1326,6 +1330,10 @@ int qcb_batch_create(const qcb_batch_job* jobs, size_t n_jobs, qcb_batch** out) 
   std::vector<Cost> items;
   uint32_t tile_words = 0;
   auto b = std::make_unique<qcb_batch>();
+  // the staging buffers are shared by all jobs: the largest window of any job
+  uint32_t win_words = PROG_WINDOW_WORDS;
+  for (size_t j = 0; j < n_jobs; j++)
+    if (jobs[j].program) win_words = std::max(win_words, jobs[j].program->win_words);
   for (size_t j = 0; j < n_jobs; j++) {
     const qcb_batch_job& J = jobs[j];
     qcb_noise_source n{};
@@ -1333,7 +1341,7 @@ int qcb_batch_create(const qcb_batch_job* jobs, size_t n_jobs, qcb_batch** out) 
     n.seed = J.seed;
     n.shot_offset = J.shot_offset;
     if (int s = check_run(J.frame, J.program, &n)) return s;
-    const uint32_t tmax = batch_tile_max(J.program);
+    const uint32_t tmax = batch_tile_max(J.program, win_words);
     if (!tmax) return fail(QCB_EUNSUPPORTED, "batch job " + std::to_string(j) + ": its frame tile does not fit shared memory");
     uint32_t T = J.tile;
     if (T && (T % 2 || T < 16 || T > tmax)) return fail(QCB_EARG, "batch job " + std::to_string(j) + ": bad tile width");
@@ -1361,7 +1369,8 @@ int qcb_batch_create(const qcb_batch_job* jobs, size_t n_jobs, qcb_batch** out) 
   if (items.size() > 0xFFFFFFF0ull) return fail(QCB_EARG, "too many tiles in one batch");
   b->nitems = (uint32_t)items.size();
   b->tile_words = tile_words;
-  b->smem_bytes = (size_t)((tile_words + 31) & ~31u) * 4 + (size_t)2 * PROG_WINDOW_WORDS * 4 + 16;
+  b->win_words = win_words;
+  b->smem_bytes = (size_t)((tile_words + 31) & ~31u) * 4 + (size_t)2 * win_words * 4 + 16;
   b->grid = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(b->nitems, 1), (uint64_t)device_sm_count());
   QCB_CUDA(cudaMalloc(&b->d_jobs, std::max<size_t>(wa.size(), 1) * sizeof(WalkArgs)));
   QCB_CUDA(cudaMalloc(&b->d_items, std::max<size_t>(it.size(), 1) * sizeof(BatchItem)));
@@ -1379,7 +1388,7 @@ int qcb_batch_run(qcb_batch* b, void* stream) {
   if (!b->nitems) return QCB_OK;
   cudaStream_t st = S(stream);
   QCB_CUDA(cudaMemsetAsync(b->d_head, 0, 4, st));
-  BatchArgs a{b->d_jobs, b->d_items, b->nitems, b->tile_words, b->d_head};
+  BatchArgs a{b->d_jobs, b->d_items, b->nitems, b->tile_words, b->d_head, b->win_words, 0u};
   batch_walker_kernel<<<b->grid, 768, b->smem_bytes, st>>>(a);
   QCB_LAUNCHED();
   return QCB_OK;
@@ -1408,7 +1417,7 @@ int qcb_batch_destroy(qcb_batch* b) {
 int qcb_tune_tile(const qcb_program* p, uint32_t* tile_out, float* us_per_column, void* stream) {
   using namespace qcb;
   if (!p) return fail(QCB_EARG, "null program");
-  const uint32_t tmax = batch_tile_max(p);
+  const uint32_t tmax = batch_tile_max(p, p->win_words);
   if (!tmax) return fail(QCB_EUNSUPPORTED, "the program's frame tile does not fit shared memory");
   cudaStream_t st = S(stream);
   const uint32_t cands[] = {16, 24, 32, 48, 64, 96, 128, 192, 256};

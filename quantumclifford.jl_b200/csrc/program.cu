@@ -438,17 +438,28 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
   close_seg();
   emit_sites(pre);
 
-  // Windowing: the kernel stages the stream into shared memory one window of
-  // PROG_WINDOW_WORDS at a time, so no record may straddle a window.  A record
+  // Windowing: the kernel stages the stream into shared memory one window
+  // (8 or 16 KB, below) at a time, so no record may straddle a window.  A record
   // too long for the space left is split into parts (entries of one segment
   // or flush are independent; every part but the last is marked so that no
   // barrier follows it); a window ends with a WIN record, the stream with END.
+  // Window size: 16 KB for a program with a record longer than an 8 KB
+  // window and a frame of 512..1536 slots (its tiles are narrow, so 8 KB
+  // more staging costs a few columns, while every split record costs a walk
+  // step: d=25 15.2 -> 13.7 ms; up to 1536 slots a 16-column shared-memory
+  // tile still fits next to 16 KB windows), 8 KB otherwise (d=11 keeps its
+  // 106-column tiles).  The WIN record carries the size.
+  size_t longest = 0;
+  for (auto& r : recs) longest = std::max(longest, 4 + ((r.w.size() + 3) & ~(size_t)3));
+  const bool tall = longest > PROG_WINDOW_WORDS - 4 && P.nslots >= 512 && P.nslots <= 1536;
+  const uint32_t W = tall ? PROG_WINDOW_WORDS_TALL : PROG_WINDOW_WORDS;
+  P.win_words = W;
   auto& out = P.stream_slot;
   out.clear();
-  auto room = [&]() { return PROG_WINDOW_WORDS - (uint32_t)(out.size() % PROG_WINDOW_WORDS) - 4; };
+  auto room = [&]() { return W - (uint32_t)(out.size() % W) - 4; };
   auto next_window = [&]() {
-    out.push_back(SEG_WIN << 24); out.push_back(0); out.push_back(0); out.push_back(0);
-    while (out.size() % PROG_WINDOW_WORDS) out.push_back(0);
+    out.push_back((SEG_WIN << 24) | W); out.push_back(0); out.push_back(0); out.push_back(0);
+    while (out.size() % W) out.push_back(0);
   };
   for (auto& r : recs) {
     const uint32_t n = (uint32_t)(r.w.size() / r.entry_words);
@@ -457,7 +468,7 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     // is one more step of the walk, with a CTA barrier before it and, for a
     // flush, one more dependent sampling chain; padding costs only words.
     const size_t whole = 4 + ((r.w.size() + 3) & ~(size_t)3);
-    if (whole <= PROG_WINDOW_WORDS - 4 && whole > room()) next_window();
+    if (whole <= W - 4 && whole > room()) next_window();
     uint32_t done = 0;
     while (done < n) {
       if (room() < 4 + ((r.entry_words + 3) & ~3u)) next_window();
@@ -473,7 +484,7 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     }
   }
   out.push_back(SEG_END << 24); out.push_back(0); out.push_back(0); out.push_back(0);
-  while (out.size() % PROG_WINDOW_WORDS) out.push_back(0);
+  while (out.size() % W) out.push_back(0);
   P.classes = classes;
   while (cdf.size() % 4) cdf.push_back(0xFFFFFFFFu);  // the last 4-word read stays inside
   P.cdf = cdf;

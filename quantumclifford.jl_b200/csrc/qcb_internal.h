@@ -94,7 +94,8 @@ constexpr uint32_t BIT_NONE = 0xFFFFFFFFu;
 constexpr uint32_t MRZ_PAD = 0xFFFFFFFFu;
 constexpr uint32_t FLAG_NO_BARRIER = 1u;
 // Program window staged into shared memory by the walker (words).
-constexpr uint32_t PROG_WINDOW_WORDS = 2048;
+constexpr uint32_t PROG_WINDOW_WORDS = 2048;      // program window (8 KB)
+constexpr uint32_t PROG_WINDOW_WORDS_TALL = 4096; // tall programs with records longer than 8 KB (16 KB)
 
 // Sampling parameters shared by the noise sites of one opcode with equal
 // probabilities, in fixed point so that the device does integer work only.
@@ -137,6 +138,7 @@ struct Program {
   uint32_t nslots;     // distinct qubits referenced (smem slots); scratch = nslots
   std::vector<uint32_t> slot_qubit;   // slot -> 0-based qubit
   std::vector<uint32_t> stream_slot;  // operands in slot space; scratch slot = nslots
+  uint32_t win_words = PROG_WINDOW_WORDS;  // words per window of stream_slot
   std::vector<Site> sites_slot;
   std::vector<int64_t> site_of_op;    // op index -> site (or -1)
   std::vector<uint32_t> site_arity;

@@ -118,8 +118,9 @@ def run_mask(arr, frames, qubits, nbits, masks):
         kind, cnt = int(h[0]) >> 24, int(h[0]) & 0xFFFFFF
         if kind == SEG_END:
             break
-        if kind == SEG_WIN:
-            pc = (pc - 4) // WIN * WIN + WIN
+        if kind == SEG_WIN:  # its count is the program's window size
+            win = cnt or WIN
+            pc = (pc - 4) // win * win + win
             continue
         if kind in (SEG_CNOT, SEG_CZ):
             e = stream[pc: pc + 2 * cnt].reshape(cnt, 2)

@@ -65,25 +65,30 @@ def test_classical_xor_chains():
     assert info["n_flushes"] >= 1
 
 
-def _records(stream, win=2048):
-    """(kind, count, continued, words) of every record of a device program."""
+def _records(stream):
+    """(kind, count, continued, words) of every record of a device program,
+    and the program's window size (carried by its WIN records)."""
     body = {1: lambda c: (2 * c + 3) // 4 * 4, 3: lambda c: (2 * c + 3) // 4 * 4, 4: lambda c: (2 * c + 3) // 4 * 4,
             6: lambda c: (2 * c + 3) // 4 * 4, 9: lambda c: (2 * c + 3) // 4 * 4, 5: lambda c: 4 * c,
             7: lambda c: 16 * c, 8: lambda c: 4 * c, 11: lambda c: 32 * c}
-    out, pc = [], 0
+    out, pc, wins = [], 0, set()
     while pc < len(stream):
         h = int(stream[pc])
         kind, cnt = h >> 24, h & 0xFFFFFF
         if kind == 0:
             break
-        if kind == 10:  # the stream continues in the next window
-            pc = pc // win * win + win
+        if kind == 10:  # the stream continues in the next window; the count is its size
+            wins.add(cnt)
+            pc = pc // cnt * cnt + cnt
             continue
         n = body[kind](cnt)
-        assert pc // win == (pc + 4 + n - 1) // win, "a record straddles a window"
-        out.append((kind, cnt, int(stream[pc + 1]) & 1, 4 + n))
+        out.append((kind, cnt, int(stream[pc + 1]) & 1, 4 + n, pc))
         pc += 4 + n
-    return out
+    assert len(wins) <= 1 and wins <= {2048, 4096}
+    win = wins.pop() if wins else len(stream)
+    for r in out:
+        assert r[4] // win == (r[4] + r[3] - 1) // win, "a record straddles a window"
+    return out, win
 
 
 @pytest.mark.parametrize("d", [3, 5, 11, 25])
@@ -92,7 +97,10 @@ def test_records_that_fit_a_window_are_not_split(d):
     compiler starts a new window for a record that fits one instead of
     cutting it at the window edge; only longer records come in parts."""
     stream, _, _, _, info = stream_emu.dump(circuits.rotated_surface_code_memory(d, d, 1e-3))
-    recs = _records(stream)
+    recs, win = _records(stream)
+    if d >= 11:
+        assert win == (4096 if d == 25 else 2048)  # 16 KB windows for the tall program only
+    assert len(stream) % win == 0
     i = 0
     while i < len(recs):
         j = i
@@ -101,8 +109,18 @@ def test_records_that_fit_a_window_are_not_split(d):
             j += 1
         total = 4 + sum(r[3] - 4 for r in recs[i:j + 1])
         if j > i:
-            assert total > 2048 - 4, (d, i, total)
+            assert total > win - 4, (d, i, total)
         i = j + 1
     if d <= 11:
         assert not any(r[2] for r in recs)
     assert sum(1 for r in recs if r[0] == 8 and not r[2]) == info["n_flushes"]
+
+
+def test_tall_program_runs_in_16k_windows():
+    """A d=25 code (1,250 frame slots, 600-site flushes of 2,400 words) gets
+    16 KB windows; interpreted on the host it reproduces the oracle."""
+    circ = circuits.rotated_surface_code_memory(25, 2, 0.01)
+    stream, _, _, _, _ = stream_emu.dump(circ)
+    recs, win = _records(stream)
+    assert win == 4096 and len(recs) > 10
+    check_circuit(circ, 70, 8)

@@ -175,6 +175,22 @@ def test_philox_mode_bit_exact_against_oracle_replica(qcb, which):
     assert np.array_equal(coding(f.xzs(), qmax + 1), coding(ox, qmax + 1))
 
 
+@pytest.mark.parametrize("mode", ["mask", "philox"])
+def test_tall_program_16k_windows_bit_exact(qcb, mode):
+    """d = 25 (1,250 frame slots, 600-site flushes longer than an 8 KB
+    window): the program runs in 16 KB windows on 18-column tiles."""
+    circ = circuits.rotated_surface_code_memory(25, 2, 0.01)
+    if mode == "mask":
+        f, ox, om = run_mask(qcb, circ, 1500, seed=25)
+    else:
+        arr = O.to_array(circ)
+        qmax, bmax = O.affected_counts(arr)
+        f = qcb.pftrajectories(arr, trajectories=3000, seed=2525)
+        ox, om = oracle.pftrajectories_philox(arr, 3000, qmax, bmax, 2525)
+    assert np.array_equal(f.measurements(), om)
+    assert np.array_equal(coding(f.xzs(), f.qubits + 1), coding(ox, f.qubits + 1))
+
+
 @pytest.mark.parametrize("tile", [0, 16, 40, 106, 256])
 @pytest.mark.parametrize("d,p", [(5, 0.004), (3, 0.015), (3, 1e-4)])
 def test_philox_sparse_noise_any_tile_width(qcb, tile, d, p):

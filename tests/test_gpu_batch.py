@@ -127,3 +127,17 @@ def test_canonicalize_batch_equals_single(qcb, cluster):
         before = st.tab.xzs.copy()
         st.to_cpu()
         assert np.array_equal(st.tab.xzs, before)
+
+
+def test_batch_with_a_tall_program_in_16k_windows(qcb):
+    """A d=25 job (16 KB program windows) in one batch with small jobs
+    (8 KB windows): the staging buffers take the larger size, every job
+    still equals its plain launch."""
+    rng = np.random.default_rng(25)
+    jobs = make_jobs(qcb, rng, 5, dmax=5, smax=3.5)
+    prog = qcb.Program(circuits.rotated_surface_code_memory(25, 2, 0.01))
+    qmax, bmax = O.affected_counts(prog.ops)
+    jobs.insert(2, dict(prog=prog, shots=2100, q=qmax, b=bmax, seed=77, off=2048))
+    frames, b = batched_frames(qcb, jobs)
+    b.run().status()
+    assert_same(qcb, frames, jobs)

@@ -92,13 +92,19 @@ function _qcbops(op::NoiseOp)
     end
     throw(ArgumentError("noise model $(typeof(n)) is not supported on the B200 path"))
 end
-_qcbops(circuit::AbstractVector) = reduce(vcat, (_qcbops(op) for op in circuit); init=QcbOp[])
+# NoisyGate (src/noise.jl:178-190): the gate, then the noise on its qubits
+_qcbops(op::NoisyGate) = vcat(_qcbops(op.gate), _qcbops(NoiseOp(op.noise, collect(QuantumClifford.affectedqubits(op.gate)))))
+# NoiseOpAll (src/noise.jl:173-176, 192-195): the noise on qubits 1..n of the
+# frame (n = nqubits(frame), the hidden ancilla excluded)
+_qcbops(op::NoiseOpAll, n::Integer) = _qcbops(NoiseOp(op.noise, collect(1:n)))
+_qcbops(op, n::Integer) = _qcbops(op)
+_qcbops(circuit::AbstractVector, n::Integer=0) = reduce(vcat, (_qcbops(op, n) for op in circuit); init=QcbOp[])
 
 # ---------------------------------------------------------------- programs
 mutable struct B200Program
     handle::Ptr{Cvoid}
-    function B200Program(circuit)
-        ops = _qcbops(circuit)
+    function B200Program(circuit, n::Integer=0)
+        ops = _qcbops(circuit, n)
         h = Ref{Ptr{Cvoid}}(C_NULL)
         _check(ccall((:qcb_program_compile, libqcb), Cint, (Ptr{QcbOp}, Csize_t, Ref{Ptr{Cvoid}}), ops, length(ops), h))
         p = new(h[])
@@ -107,7 +113,7 @@ mutable struct B200Program
 end
 
 const _programs = IdDict{Any,B200Program}()   # circuits compiled once
-_program(circuit) = get!(() -> B200Program(circuit), _programs, circuit)
+_program(circuit, n::Integer=0) = get!(() -> B200Program(circuit, n), _programs, (circuit, n))
 
 # ---------------------------------------------------------------- frames
 """Device Pauli frame; `to_b200(PauliFrame(...))` or `B200Frame(frames, qubits, bits)`."""
@@ -141,7 +147,7 @@ end
 function pftrajectories(f::B200Frame, circuit)
     src = Ref(NoiseSource(0, 0, f.seed, 0, C_NULL, 0, C_NULL))
     _check(ccall((:qcb_pftrajectories, libqcb), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{NoiseSource}, Ptr{Cvoid}),
-                 f.handle, _program(circuit).handle, src, C_NULL))
+                 f.handle, _program(circuit, f.qubits).handle, src, C_NULL))
     f.seed += 0x9E3779B97F4A7C15   # next call draws fresh randomness
     f
 end

@@ -14,7 +14,7 @@ from .ops import (  # noqa: F401
     Op, OP, sId1, sHadamard, sPhase, sInvPhase, sX, sY, sZ, sSQRTX, sInvSQRTX, sSQRTY, sInvSQRTY,
     sHadamardXY, sHadamardYZ, sCXYZ, sCZYX, SingleQubitOperator, sCNOT, sCPHASE, sSWAP, sZCX, sZCY, sZCZ, sXCX, sXCY, sXCZ,
     sYCX, sYCY, sYCZ, sMZ, sMRZ, sMX, sMRX, ClassicalXOR, PauliMeasurement, PauliError, NoiseOp, PauliNoise, UnbiasedUncorrelatedNoise,
-    DepolarizationNoise, to_array, count_updates, affected_counts,
+    DepolarizationNoise, NoisyGate, NoiseOpAll, to_array, count_updates, affected_counts,
 )
 from .frames import (  # noqa: F401
     PauliFrame, Program, Masks, sample_masks, pftrajectories, pauliframe_, measurements,

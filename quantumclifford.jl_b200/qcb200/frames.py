@@ -27,9 +27,11 @@ QCB_NOISE_MASK = 1
 class Program:
     """A compiled circuit (qcb_program)."""
 
-    def __init__(self, circuit):
+    def __init__(self, circuit, nqubits: Optional[int] = None):
+        """``nqubits``: the frame's qubit count, for NoiseOpAll (default: the
+        highest qubit of the other ops)."""
         ensure_init()
-        self.ops = _ops.to_array(circuit)
+        self.ops = _ops.to_array(circuit, nqubits)
         h = ctypes.c_void_p()
         check(lib().qcb_program_compile(ptr(self.ops) if len(self.ops) else None, len(self.ops), ctypes.byref(h)))
         self.handle = h
@@ -221,7 +223,7 @@ class PauliFrame:
 
     def apply(self, op, *, seed: int = 0, masks: Optional[Masks] = None):
         """apply!(frame, op) for one op or a short op list."""
-        arr = _ops.to_array([op] if isinstance(op, _ops.Op) else op)
+        arr = _ops.to_array([op] if isinstance(op, (_ops.Op, _ops.NoiseOpAll)) else op, self.qubits)
         n = _noise_source(seed, self.shot_offset, masks)
         check(lib().qcb_frame_apply_ops(self.handle, ptr(arr), len(arr), ctypes.byref(n), None))
         return self
@@ -234,7 +236,7 @@ def pftrajectories(frame_or_circuit, circuit=None, *, trajectories: int = 5000, 
     parity; the device path has one schedule."""
     if isinstance(frame_or_circuit, PauliFrame):
         frame = frame_or_circuit
-        prog = program if program is not None else Program(circuit)
+        prog = program if program is not None else Program(circuit, frame.qubits)
     else:
         prog = program if program is not None else Program(frame_or_circuit)
         qmax, bmax = _ops.affected_counts(prog.ops)

@@ -8,7 +8,7 @@ Each constructor returns a record of the C ABI's ``qcb_op`` (1-based qubits,
 from __future__ import annotations
 
 from dataclasses import dataclass
-from typing import Iterable, Sequence
+from typing import Iterable, Optional, Sequence
 
 import numpy as np
 
@@ -257,21 +257,62 @@ def PauliError(qubits, *p) -> list:
     raise TypeError("PauliError(q, p) or PauliError(q, px, py, pz)")
 
 
-def flatten(circuit: Iterable) -> list:
+@dataclass(frozen=True)
+class NoiseOpAll:
+    """NoiseOpAll(noise) (src/noise.jl:173-176, 192-195): the noise on every
+    qubit 1..nqubits(frame) of the frame (hidden ancilla excluded,
+    src/pauli_frames.jl:14).  Lowered by `flatten` once that count is known:
+    `pftrajectories(frame, circuit)` passes the frame's.  Without a frame the
+    highest qubit of the other ops is used, the frame the one-call form makes
+    (the reference's `_create_pauliframe` has no qubit count for NoiseOpAll,
+    src/affectedqubits.jl:22-24, and raises there)."""
+    noise: object
+
+
+def _is_two_qubit(o: Op) -> bool:
+    return OP["CNOT"] <= o.opcode <= OP["YCZ"]
+
+
+def NoisyGate(gate, noise) -> list:
+    """NoisyGate(gate, noise) (src/noise.jl:178-190): the gate, then the
+    noise on its qubits (affectedqubits(gate))."""
+    ops = flatten([gate])
+    if len(ops) != 1 or ops[0].is_noise() or ops[0].opcode in (OP["XOR"], OP["XOR_BITS"]):
+        raise ArgumentError(QCB_EARG, "NoisyGate takes one single- or two-qubit gate or measurement")
+    g = ops[0]
+    return ops + NoiseOp(noise, (g.q1, g.q2) if _is_two_qubit(g) else (g.q1,))
+
+
+def flatten(circuit: Iterable, nqubits: Optional[int] = None) -> list:
+    """The circuit as a flat list of Op; NoiseOpAll becomes one noise op per
+    qubit 1..n (n = nqubits, else the highest qubit of the other ops)."""
     out = []
-    for o in circuit:
-        if isinstance(o, Op):
-            out.append(o)
-        else:
-            out.extend(flatten(o))
-    return out
+
+    def walk(c):
+        for o in c:
+            if isinstance(o, (Op, NoiseOpAll)):
+                out.append(o)
+            else:
+                walk(o)
+
+    walk(circuit)
+    if not any(isinstance(o, NoiseOpAll) for o in out):
+        return out
+    if nqubits is None:
+        rest = [o for o in out if isinstance(o, Op)]
+        nqubits = affected_counts(to_array(rest))[0] if rest else 1
+    res = []
+    for o in out:
+        res.extend(NoiseOp(o.noise, range(1, int(nqubits) + 1)) if isinstance(o, NoiseOpAll) else [o])
+    return res
 
 
-def to_array(circuit: Iterable) -> np.ndarray:
-    """Pack a circuit into a C-contiguous array of qcb_op records."""
+def to_array(circuit: Iterable, nqubits: Optional[int] = None) -> np.ndarray:
+    """Pack a circuit into a C-contiguous array of qcb_op records
+    (``nqubits``: the frame's qubit count, for NoiseOpAll)."""
     if isinstance(circuit, np.ndarray) and circuit.dtype == OP_DTYPE:
         return np.ascontiguousarray(circuit)
-    ops = flatten(circuit)
+    ops = flatten(circuit, nqubits)
     a = np.zeros(len(ops), dtype=OP_DTYPE)
     for i, o in enumerate(ops):
         a[i] = (o.opcode, o.q1, o.q2, o.bit, o.p)

@@ -124,3 +124,22 @@ def test_tall_program_runs_in_16k_windows():
     recs, win = _records(stream)
     assert win == 4096 and len(recs) > 10
     check_circuit(circ, 70, 8)
+
+
+def test_noisy_gate_and_noise_op_all_lowering():
+    """NoisyGate(g, noise) is g then the noise on g's qubits; NoiseOpAll(noise)
+    is the noise on qubits 1..n of the frame (n given, else the highest qubit
+    of the other ops, as _create_pauliframe sizes the frame)."""
+    noise = O.UnbiasedUncorrelatedNoise(0.03)
+    a = O.to_array([O.NoisyGate(O.sCNOT(2, 5), noise), O.NoisyGate(O.sHadamard(3), O.DepolarizationNoise(0.02)),
+                    O.NoiseOpAll(noise), O.sMZ(4, 1)])
+    b = O.to_array([O.sCNOT(2, 5), O.PauliError([2, 5], 0.03), O.sHadamard(3),
+                    O.NoiseOp(O.DepolarizationNoise(0.02), [3]), O.PauliError([1, 2, 3, 4, 5], 0.03), O.sMZ(4, 1)])
+    assert np.array_equal(a, b)
+    c = O.to_array([O.NoiseOpAll(O.PauliNoise(0.01, 0.02, 0.03)), O.sMZ(2, 1)], nqubits=4)
+    assert list(c["q1"][:4]) == [1, 2, 3, 4] and c["p"][0].tolist() == [0.01, 0.02, 0.03]
+    with pytest.raises(qcb200.ArgumentError):
+        O.NoisyGate(O.PauliError(1, 0.1), noise)
+    # through the compiler and the stream emulator, bit for bit against the oracle
+    check_circuit([O.sHadamard(q) for q in range(1, 7)] + [O.NoisyGate(O.sCNOT(1, 4), noise), O.NoiseOpAll(noise)]
+                  + [O.sMZ(q, q) for q in range(1, 7)], 300, 3)

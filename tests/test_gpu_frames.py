@@ -327,3 +327,20 @@ def test_philox_statistics_match_reference_draws(qcb):
     # individual data measurements are uniformly random (initZ! / reset randomisation)
     rec = qcb.unpack_record(planes[-d * d:], frames)
     assert abs(rec.mean() - 0.5) < 0.01
+
+
+def test_noisy_gate_and_noise_op_all_on_frames(qcb):
+    """NoisyGate and NoiseOpAll through pftrajectories(frame, circuit): the
+    frame's qubit count sizes NoiseOpAll (8 here, above the ops' highest
+    qubit 5), bit for bit against the oracle on the lowered circuit."""
+    noise = O.UnbiasedUncorrelatedNoise(0.05)
+    circ = ([O.sHadamard(q) for q in range(1, 6)] + [O.NoisyGate(O.sCNOT(1, 4), noise), O.NoiseOpAll(noise)]
+            + [O.sMZ(q, q) for q in range(1, 6)])
+    masks = qcb.sample_masks(O.to_array(circ, 8), 4096, qubits=8, seed=6)
+    f = qcb.PauliFrame(4096, 8, 5, masks=masks)
+    qcb.pftrajectories(f, circ, masks=masks)
+    arr = O.to_array(circ, 8)
+    assert (arr["opcode"] == O.OP["PAULI_NOISE"]).sum() == 2 + 8
+    ox, om = oracle.pftrajectories_mask(arr, 4096, 8, 5, masks.init_z, masks.reset_planes, masks.events)
+    assert np.array_equal(f.measurements(), om)
+    assert np.array_equal(coding(f.xzs(), 9), coding(ox, 9))

@@ -173,6 +173,9 @@ int qcb_frame_init_z(qcb_frame* f, uint64_t seed, uint64_t shot_offset, void* st
 int qcb_frame_init_z_planes(qcb_frame* f, const uint32_t* z_planes, void* stream);
 /* Zero the x/z bits and the record.                                        */
 int qcb_frame_clear(qcb_frame* f, void* stream);
+/* copy(frame) (src/pauli_frames.jl:17): dst <- src, planes and record, on
+ * the device; both frames have the same shape (QCB_EDIM otherwise).        */
+int qcb_frame_copy(qcb_frame* dst, const qcb_frame* src, void* stream);
 
 /* pftrajectories(frame, circuit) (src/pauli_frames.jl:234-239).            */
 int qcb_pftrajectories(qcb_frame* f, const qcb_program* prog,

@@ -907,6 +907,19 @@ int qcb_frame_clear(qcb_frame* f, void* stream) {
   return QCB_OK;
 }
 
+// copy(frame) (src/pauli_frames.jl:17): planes and record, device to device.
+int qcb_frame_copy(qcb_frame* dst, const qcb_frame* src, void* stream) {
+  if (int st = check_frame(dst)) return st;
+  if (int st = check_frame(src)) return st;
+  if (dst->frames != src->frames || dst->nq1 != src->nq1 || dst->nbits != src->nbits)
+    return fail(QCB_EDIM, "qcb_frame_copy: frames of different shapes");
+  QCB_CUDA(cudaMemcpyAsync(dst->planes, src->planes, (size_t)2 * (src->nq1 + 1) * src->pitch * 4,
+                           cudaMemcpyDeviceToDevice, S(stream)));
+  QCB_CUDA(cudaMemcpyAsync(dst->record, src->record, (size_t)std::max<uint32_t>(src->nbits, 1) * src->pitch * 4,
+                           cudaMemcpyDeviceToDevice, S(stream)));
+  return QCB_OK;
+}
+
 }  // extern "C"
 
 namespace qcb {

@@ -154,6 +154,17 @@ end
 
 apply!(f::B200Frame, op::AbstractOperation) = pftrajectories(f, [op])
 
+# copy(frame) (src/pauli_frames.jl:17): same bits and record on the device;
+# the copy draws its own noise stream from then on
+function Base.copy(f::B200Frame)
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    _check(ccall((:qcb_frame_create, libqcb), Cint, (UInt64, UInt32, UInt32, Ref{Ptr{Cvoid}}), f.frames, f.qubits, f.nbits, h))
+    g = B200Frame(h[], f.frames, f.qubits, f.nbits, rand(UInt64))
+    finalizer(x -> ccall((:qcb_frame_destroy, libqcb), Cint, (Ptr{Cvoid},), x.handle), g)
+    _check(ccall((:qcb_frame_copy, libqcb), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}), g.handle, f.handle, C_NULL))
+    g
+end
+
 function measurements(f::B200Frame)
     m = Matrix{Bool}(undef, f.frames, f.nbits)
     _check(ccall((:qcb_frame_download_measurements, libqcb), Cint, (Ptr{Cvoid}, Ptr{Bool}, Ptr{Cvoid}),

@@ -137,6 +137,7 @@ def lib():
         "qcb_frame_init_z": ([vp, u64, u64, vp], ctypes.c_int),
         "qcb_frame_init_z_planes": ([vp, vp, vp], ctypes.c_int),
         "qcb_frame_clear": ([vp, vp], ctypes.c_int),
+        "qcb_frame_copy": ([vp, vp, vp], ctypes.c_int),
         "qcb_pftrajectories": ([vp, vp, P(qcb_noise_source), vp], ctypes.c_int),
         "qcb_frame_apply_ops": ([vp, vp, sz, P(qcb_noise_source), vp], ctypes.c_int),
         "qcb_frame_download_xzs": ([vp, vp, vp], ctypes.c_int),

@@ -150,6 +150,13 @@ class PauliFrame:
     def words(self) -> int:
         return (self.frames + 31) // 32
 
+    def copy(self) -> "PauliFrame":
+        """copy(frame) (src/pauli_frames.jl:17): a new device frame with the
+        same x/z bits and record."""
+        g = PauliFrame(self.frames, self.qubits, self.nbits, shot_offset=self.shot_offset, init=False)
+        check(lib().qcb_frame_copy(g.handle, self.handle, None))
+        return g
+
     def initZ(self, seed: int = 0, masks: Optional[Masks] = None):
         """initZ! (src/pauli_frames.jl:47-56)."""
         if masks is None:

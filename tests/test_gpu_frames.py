@@ -344,3 +344,18 @@ def test_noisy_gate_and_noise_op_all_on_frames(qcb):
     ox, om = oracle.pftrajectories_mask(arr, 4096, 8, 5, masks.init_z, masks.reset_planes, masks.events)
     assert np.array_equal(f.measurements(), om)
     assert np.array_equal(coding(f.xzs(), 9), coding(ox, 9))
+
+
+def test_frame_copy_is_independent(qcb):
+    """copy(frame): same bits and record; later ops on the copy leave the
+    original as it was."""
+    circ = O.to_array(circuits.rotated_surface_code_memory(3, 3, 0.02))
+    qmax, bmax = O.affected_counts(circ)
+    f = qcb.pftrajectories(circ, trajectories=3000, seed=12)
+    g = f.copy()
+    assert np.array_equal(g.measurements(), f.measurements()) and np.array_equal(g.xzs(), f.xzs())
+    before = f.xzs()
+    g.apply([O.sHadamard(q) for q in range(1, qmax + 1)])
+    assert np.array_equal(f.xzs(), before) and not np.array_equal(g.xzs(), before)
+    with pytest.raises(qcb.DimensionMismatch):
+        qcb.check(qcb.lib().qcb_frame_copy(qcb.PauliFrame(3000, qmax + 1, bmax).handle, f.handle, None))

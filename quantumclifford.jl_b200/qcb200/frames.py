@@ -69,7 +69,7 @@ def sample_masks(circuit, frames: int, qubits: Optional[int] = None, seed: int =
     p a uniform Pauli of the 4^k, identity included), so the file has the
     distribution of the reference's per-frame draws.
     """
-    arr = _ops.to_array(circuit)
+    arr = _ops.to_array(circuit, qubits)  # NoiseOpAll over the frame's qubits
     qmax, _ = _ops.affected_counts(arr)
     nq1 = (qubits if qubits is not None else qmax) + 1
     rng = np.random.default_rng(seed)

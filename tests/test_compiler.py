@@ -143,3 +143,16 @@ def test_noisy_gate_and_noise_op_all_lowering():
     # through the compiler and the stream emulator, bit for bit against the oracle
     check_circuit([O.sHadamard(q) for q in range(1, 7)] + [O.NoisyGate(O.sCNOT(1, 4), noise), O.NoiseOpAll(noise)]
                   + [O.sMZ(q, q) for q in range(1, 7)], 300, 3)
+
+
+def test_sample_masks_lowers_noise_op_all_over_the_frame():
+    """The event file of a circuit with NoiseOpAll refers to the ops of the
+    lowering for the frame's qubit count, as pftrajectories(frame, circuit)
+    compiles it."""
+    noise = O.UnbiasedUncorrelatedNoise(0.3)
+    circ = [O.sHadamard(1), O.NoiseOpAll(noise), O.sMZ(1, 1)]
+    m = qcb200.sample_masks(circ, 256, qubits=6, seed=1)
+    arr = O.to_array(circ, 6)
+    assert len(arr) == 8 and m.init_z.shape[0] == 7
+    assert set(np.unique(m.events["op_index"])) <= set(range(1, 7))
+    assert len(np.unique(m.events["op_index"])) == 6  # p = 0.3 on 256 shots: every qubit's site fires

@@ -114,49 +114,74 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline_run(target_cpu_seconds: float = 15.0):
-    """The oracle port (reference loop structure: one pass over all frames per
-    op, one rand() per frame per noise site, threads over frame slices) timed
-    on the host cores on a bounded sample of the same circuit."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle  # the checker, used here only as the timed CPU baseline
+def _reference_circuit():
     from qcb200 import circuits, ops as O
 
     arr = O.to_array(circuits.rotated_surface_code_memory(D, ROUNDS, P_NOISE))
     qmax, bmax = O.affected_counts(arr)
-    updates_per_shot = O.count_updates(arr)
-    cores = os.cpu_count() or 1
-    shots = 2000
+    return arr, qmax, bmax, O.count_updates(arr)
+
+
+def cpu_reference_step(arr, qmax, bmax, shots, seed, cores):
+    """One step of the CPU path at the full configuration: the oracle port of
+    pftrajectories(circuit; trajectories=shots, threads=true)
+    (src/pauli_frames.jl:193-227: _create_pauliframe, initZ!, one pass over
+    all frames per op, one rand() per frame per noise site, threads over frame
+    slices, nthr = min(cores, shots / 100)), the frame and the Bool record
+    (the reference's column-major Matrix{Bool}, 1.44 GB at 1e6 shots)
+    allocated by the step as the reference allocates them.  Returns seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the checker, used here only as the timed CPU path
+
     t0 = time.perf_counter()
-    oracle.pftrajectories_rng(arr, shots, qmax, bmax, seed=1, threads=1)
-    t1 = time.perf_counter() - t0
-    # size the sample to about target_cpu_seconds of single-core work, spread over all cores
-    sample = int(min(1_000_000, max(cores * 100, shots * target_cpu_seconds / max(t1, 1e-6))))
-    t0 = time.perf_counter()
-    oracle.pftrajectories_rng(arr, sample, qmax, bmax, seed=2, threads=cores)
+    xzs, meas = oracle.pftrajectories_rng(arr, shots, qmax, bmax, seed=seed, threads=cores, as_bool=False)
     dt = time.perf_counter() - t0
-    rate = updates_per_shot * sample / dt
-    threads = max(1, min(cores, sample // 100))
-    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{sample} shots of the d=11 circuit (Xoshiro per-frame draws), {dt:.2f} s wall on {threads} threads"}
+    del xzs, meas
+    return dt
+
+
+def cpu_baseline_run(shots: int = SHOTS_PER_GPU):
+    """The oracle port timed on the host cores over the same workload as the
+    GPU step (all 1e6 shots of the d=11 circuit): one untimed step on a
+    small slice (pages the library in), then one full step."""
+    arr, qmax, bmax, upd = _reference_circuit()
+    cores = os.cpu_count() or 1
+    cpu_reference_step(arr, qmax, bmax, min(shots, 20_000), 1, cores)
+    dt = cpu_reference_step(arr, qmax, bmax, shots, 2, cores)
+    threads = max(1, min(cores, shots // 100))
+    return {"value": upd * shots / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"the full step: {shots} shots of the d=11 circuit (Xoshiro per-frame draws, Bool record "
+                      f"allocated per step as the reference does), {dt:.2f} s wall on {threads} threads"}
 
 
 def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU path (its Julia code cannot run
+    here: no Julia; the oracle port restates it loop for loop) on all host
+    cores, every step the full configuration (1e6 shots of the d=11
+    circuit), W untimed then K timed steps, wall-clock per step."""
     if rank != 0:
         return
-    cb = None
+    arr, qmax, bmax, upd = _reference_circuit()
+    cores = os.cpu_count() or 1
+    threads = max(1, min(cores, SHOTS_PER_GPU // 100))
     times = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline_run(target_cpu_seconds=4.0)
+        dt = cpu_reference_step(arr, qmax, bmax, SHOTS_PER_GPU, 1000 + i, cores)
         if i >= args.warmup:
-            times.append(r["value"])
-            cb = r
-    v = statistics.median(times)
+            times.append(dt)
+    total = sum(times)
+    v = upd * SHOTS_PER_GPU * len(times) / total
+    sample = (f"every step the full configuration: {SHOTS_PER_GPU} shots of the d=11 circuit, Bool record "
+              f"({SHOTS_PER_GPU * bmax / 1e9:.2f} GB) allocated per step; {threads} threads; step times "
+              f"{min(times):.2f}-{max(times):.2f} s")
     out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": 7601 * SHOTS_PER_GPU / v * 1e3, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "u32 bit planes", "data": "synthetic (seeded)", "impl": "reference",
-           "config": {"workload": WORKLOAD, "sample": cb["sample"]},
-           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": cb["kind"], "sample": cb["sample"]},
+           "ms_per_step": total / len(times) * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u64 qubit-packed frame words (the reference layout)",
+           "data": "synthetic (seeded)", "impl": "reference",
+           "config": {"workload": WORKLOAD, "shots_per_step": SHOTS_PER_GPU, "updates_per_shot": upd,
+                      "path": "oracle port of pftrajectories(circuit; trajectories, threads=true); the Julia "
+                              "reference cannot be installed or run here"},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -742,14 +767,17 @@ def main():
     # the walker is the only kernel of a step: its event time is the launch duration
     kernel_ms = ms
 
-    # end to end through the public host API: ops from host memory in, record
-    # planes back to pinned host memory, every step.  The host call keeps the
-    # compiled program of the last op list on the device (it compares the op
-    # list each call), so no circuit bytes cross PCIe after the first call;
-    # the record is copied out chunk by chunk while later chunks run.
+    # end to end through the public host API: the op list from host memory in
+    # (compiled on the host when it changes; the compiled program, 0.2 MB at
+    # d=11, copied host -> device from page-locked memory every call), the
+    # record planes back to pinned host memory every call, copied out chunk by
+    # chunk while later chunks run.
     words = (shots + 31) // 32
     rec_host = torch.empty((bmax, words), dtype=torch.int32, pin_memory=True)
     ops_host = arr  # numpy, host
+    prog_bytes = ctypes.c_uint64()
+    check(L.qcb_program_device_bytes(prog.handle, ctypes.byref(prog_bytes)))
+
     def e2e_step(i):
         check(L.qcb_pftrajectories_host(ptr(ops_host), len(ops_host), shots, 5000 + i, offset,
                                         rec_host.data_ptr(), sp))
@@ -762,10 +790,29 @@ def main():
         e2e_step(10 + i)
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+
+    # end to end through the drop-in output: pftrajectories(frame, circuit)
+    # then measurements(frame), the reference's column-major Matrix{Bool}
+    # (frames x nbits, one byte per bit: 1.44 GB at 1e6 shots) in pinned host
+    # memory, every step
+    bool_host = torch.empty((bmax, shots), dtype=torch.uint8, pin_memory=True)
+
+    def bool_step(i):
+        check(L.qcb_pftrajectories_fresh(frame.handle, prog.handle, 7000 + i, offset, sp))
+        check(L.qcb_frame_download_measurements(frame.handle, ctypes.c_void_p(bool_host.data_ptr()), sp))
+    bool_step(0)
+    torch.cuda.synchronize()
+    bool_steps = max(3, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for i in range(bool_steps):
+        bool_step(1 + i)
+    torch.cuda.synchronize()
+    bool_ms = (time.perf_counter() - t0) * 1e3 / bool_steps
+    del bool_host
     clk = clocks.stop()
 
     if world > 1:
-        ms, e2e_ms = max_over_ranks([ms, e2e_ms], device="cuda")
+        ms, e2e_ms, bool_ms = max_over_ranks([ms, e2e_ms, bool_ms], device="cuda")
 
     total_updates = upd * shots * world
     value = total_updates / (ms / 1e3)
@@ -793,14 +840,24 @@ def main():
                    "parallelism": f"shot-sharded x{world}",
                    "l2": "no flush: each step writes 240 MB (record + frame) > 126 MB L2; inputs are the 0.4 MB program"},
         "gpu_launches": int(launches),
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 0,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(prog_bytes.value),
                 "d2h_bytes_per_step": int(bmax * words * 4), "ms_per_step": e2e_ms,
                 "api": "qcb_pftrajectories_host (one call: circuit + shots + seed in, record planes out)",
-                "host_inputs_bytes_per_step": int(arr.nbytes),
-                "inputs": "the op list is read from host memory every call and compared with the cached "
-                          "compiled program; the program crossed PCIe once, before the timed region"},
+                "inputs": f"the {arr.nbytes}-byte op list is read from host memory and compared with the last "
+                          "call's (compiled on the host when it differs); the compiled program "
+                          f"({prog_bytes.value} bytes) is copied host -> device from page-locked memory every call"},
+        "e2e_measurements": {"value": total_updates / (bool_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": int(bmax * shots), "ms_per_step": bool_ms,
+                             "api": "pftrajectories(frame, circuit) + measurements(frame): qcb_pftrajectories_fresh "
+                                    "then qcb_frame_download_measurements into the reference's column-major "
+                                    "Bool matrix (one byte per bit) in pinned host memory",
+                             "inputs": "the compiled program stays resident (compiled once per circuit, as the "
+                                       "Julia extension caches it); seed per call"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": traffic,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one walker_kernel "
+                                       "launch of this workload (profiles/walker_d11_traffic.json), not measured "
+                                       "in this run",
                      "algorithmic_bytes_per_launch": model_bytes,
                      "basis": "model plane bytes of an op-per-launch schedule (5,175 B/shot); the walker keeps the "
                               "frame on chip, so its compulsory DRAM bytes are the record + final frame",

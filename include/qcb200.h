@@ -67,6 +67,11 @@ enum qcb_opcode {
   QCB_OP_ZCX = 35, QCB_OP_ZCY = 36, QCB_OP_ZCZ = 37,
   QCB_OP_XCX = 38, QCB_OP_XCY = 39, QCB_OP_XCZ = 40,
   QCB_OP_YCX = 41, QCB_OP_YCY = 42, QCB_OP_YCZ = 43,
+  QCB_OP_SWAPCX = 44, QCB_OP_INVSWAPCX = 45, QCB_OP_ISWAP = 46, QCB_OP_INVISWAP = 47,
+  QCB_OP_CZSWAP = 48, QCB_OP_CXSWAP = 49, QCB_OP_ZCRY = 50, QCB_OP_INVZCRY = 51,
+  QCB_OP_SQRTZZ = 52, QCB_OP_INVSQRTZZ = 53, QCB_OP_SQRTXX = 54, QCB_OP_INVSQRTXX = 55,
+  QCB_OP_SQRTYY = 56, QCB_OP_INVSQRTYY = 57,
+  QCB_OP_LAST2Q = 57,  /* two-qubit gates are QCB_OP_CNOT..QCB_OP_LAST2Q */
   /* measurements (frame semantics: src/pauli_frames.jl:74-116) */
   QCB_OP_MZ = 64, QCB_OP_MRZ = 65, QCB_OP_MX = 66, QCB_OP_MRX = 67,
   /* ClassicalXOR(bits, store) (src/misc_ops.jl:198-205; frame semantics
@@ -158,6 +163,10 @@ uint64_t qcb_launch_count(void);
  * Julia constructors do.                                                    */
 int qcb_program_compile(const qcb_op* ops, size_t n_ops, qcb_program** out);
 int qcb_program_info_get(const qcb_program* prog, qcb_program_info* info);
+/* Bytes of the program that the walker reads from device memory (records,
+ * noise classes, Binomial count tables): what qcb_pftrajectories_host copies
+ * host -> device on each call.  No reference counterpart (a size query). */
+int qcb_program_device_bytes(const qcb_program* prog, uint64_t* bytes);
 int qcb_program_destroy(qcb_program* prog);
 
 /* ------------------------------------------------------------ Pauli frames */
@@ -288,9 +297,12 @@ int qcb_evaluate_guesses(const qcb_frame* f, const uint32_t* logical_bits, size_
 /* pftrajectories(circuit; trajectories) (src/pauli_frames.jl:193-227) as one
  * host call: fresh frame, Philox initZ!, run, record copied back as
  * shot-packed planes [nbits][ceil(frames/32)]; returns when the record is
- * in `record_planes` (NULL: run only).  The compiled program of the last op
- * list and the frame of the last shape stay on the device (the device
- * current at the first call) for reuse.  Wide runs go as shot chunks whose
+ * in `record_planes` (NULL: run only).  The op list is compiled on the host
+ * when it differs from the last call's; the compiled program (records,
+ * noise classes, count tables: qcb_program_device_bytes) is copied host ->
+ * device from page-locked memory on every call.  The device buffers of the
+ * program and of the frame of the last shape are kept (on the device current
+ * at the first call) for reuse.  Wide runs go as shot chunks whose
  * record columns are copied out while the next chunk runs; the record is
  * that of one launch.  Page-locked `record_planes` gets the full PCIe
  * bandwidth.  Calls are serialised by an internal lock.                     */

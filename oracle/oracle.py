@@ -237,9 +237,11 @@ def pftrajectories_mask(ops, frames, qubits, nbits, init_z, reset_planes, events
     return xzs, meas.T.astype(bool)
 
 
-def pftrajectories_rng(ops, frames, qubits, nbits, seed=1, threads=1):
+def pftrajectories_rng(ops, frames, qubits, nbits, seed=1, threads=1, as_bool=True):
     """Reference-structured frame run with per-slice Xoshiro draws (the CPU
-    baseline and the statistical comparison)."""
+    baseline and the statistical comparison).  With as_bool=False the record
+    is returned as the uint8 array [nbits, frames], which is the reference's
+    column-major Bool matrix frames x nbits byte for byte (no conversion)."""
     nq1 = qubits + 1
     xzs = np.zeros((frame_words(nq1), frames), dtype=np.uint64)
     meas = np.zeros((nbits, frames), dtype=np.uint8)
@@ -247,7 +249,7 @@ def pftrajectories_rng(ops, frames, qubits, nbits, seed=1, threads=1):
     o = np.ascontiguousarray(ops, dtype=OP_DTYPE)
     L().oracle_pftrajectories(_p(xzs), _p(meas), frames, nq1, nbits, _p(o), len(o), 2, None, 0, None, seed,
                               int(threads))
-    return xzs, meas.T.astype(bool)
+    return xzs, (meas.T.astype(bool) if as_bool else meas)
 
 
 def pftrajectories_philox(ops, frames, qubits, nbits, seed, shot_offset=0):

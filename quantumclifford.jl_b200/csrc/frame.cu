@@ -99,6 +99,15 @@ __device__ __forceinline__ void gate2_xz(uint32_t op, uint32_t& x1, uint32_t& z1
     case QCB_OP_YCX: x1 = a ^ d; z1 = d ^ b; x2 = a ^ b ^ c; break;
     case QCB_OP_YCY: x1 = a ^ d ^ c; z1 = b ^ c ^ d; x2 = a ^ c ^ b; z2 = a ^ b ^ d; break;
     case QCB_OP_YCZ: x1 = a ^ c; z1 = c ^ b; z2 = d ^ a ^ b; break;
+    case QCB_OP_SWAPCX: x1 = c; z1 = d ^ b; x2 = c ^ a; z2 = b; break;
+    case QCB_OP_INVSWAPCX: case QCB_OP_CXSWAP: x1 = c ^ a; z1 = d; x2 = a; z2 = d ^ b; break;
+    case QCB_OP_ISWAP: case QCB_OP_INVISWAP: x1 = c; z1 = a ^ d ^ c; x2 = a; z2 = a ^ c ^ b; break;
+    case QCB_OP_CZSWAP: x1 = c; z1 = d ^ a; x2 = a; z2 = c ^ b; break;
+    case QCB_OP_ZCRY: case QCB_OP_INVZCRY: z1 = a ^ b ^ c ^ d; x2 = a ^ c; z2 = a ^ d; break;
+    case QCB_OP_SQRTZZ: case QCB_OP_INVSQRTZZ: z1 = a ^ c ^ b; z2 = a ^ d ^ c; break;
+    case QCB_OP_SQRTXX: case QCB_OP_INVSQRTXX: x1 = b ^ d ^ a; x2 = b ^ c ^ d; break;
+    case QCB_OP_SQRTYY: case QCB_OP_INVSQRTYY:
+      x1 = b ^ c ^ d; z1 = a ^ d ^ c; x2 = a ^ b ^ d; z2 = a ^ c ^ b; break;
     default: break;
   }
 }
@@ -1187,6 +1196,38 @@ int qcb_frame_download_planes(const qcb_frame* f, uint32_t* xp, uint32_t* zp, vo
 
 namespace qcb {
 
+// Page-locked copy of a compiled program's device image (records, noise
+// classes, count tables) for the one-call host API, which copies it to the
+// device on every call.
+struct HostProgramImage {
+  uint8_t* pinned = nullptr;
+  size_t cap = 0, n_stream = 0, n_classes = 0, n_cdf = 0;
+  int build(const Program& P) {
+    n_stream = P.stream_slot.size() * sizeof(uint32_t);
+    n_classes = P.classes.size() * sizeof(NoiseClass);
+    n_cdf = P.cdf.size() * sizeof(uint32_t);
+    const size_t need = n_stream + n_classes + n_cdf;
+    if (need > cap) {
+      if (pinned) cudaFreeHost(pinned);
+      pinned = nullptr;
+      cap = 0;
+      QCB_CUDA(cudaMallocHost((void**)&pinned, need ? need : 16));
+      cap = need;
+    }
+    if (n_stream) std::memcpy(pinned, P.stream_slot.data(), n_stream);
+    if (n_classes) std::memcpy(pinned + n_stream, P.classes.data(), n_classes);
+    if (n_cdf) std::memcpy(pinned + n_stream + n_classes, P.cdf.data(), n_cdf);
+    return QCB_OK;
+  }
+  int upload(const Program& P, cudaStream_t st) const {
+    if (n_stream) QCB_CUDA(cudaMemcpyAsync(P.d_stream_slot, pinned, n_stream, cudaMemcpyHostToDevice, st));
+    if (n_classes)
+      QCB_CUDA(cudaMemcpyAsync(P.d_classes, pinned + n_stream, n_classes, cudaMemcpyHostToDevice, st));
+    if (n_cdf) QCB_CUDA(cudaMemcpyAsync(P.d_cdf, pinned + n_stream + n_classes, n_cdf, cudaMemcpyHostToDevice, st));
+    return QCB_OK;
+  }
+};
+
 // Copy-out chunks of the one-call host API: the first is one wave of
 // 16-column tiles, each next one twice as wide, the last takes the rest.
 constexpr int HOST_MAX_CHUNKS = 8;
@@ -1229,12 +1270,19 @@ int qcb_pftrajectories_host(const qcb_op* ops, size_t n_ops, uint64_t frames, ui
   static qcb_frame* cframe = nullptr;
   static cudaStream_t copy_stream = nullptr;
   static cudaEvent_t chunk_done[HOST_MAX_CHUNKS + 1] = {};
+  static HostProgramImage image;
   std::lock_guard<std::mutex> lock(mu);
   if (!cprog || cops.size() != n_ops || std::memcmp(cops.data(), ops, n_ops * sizeof(qcb_op)) != 0) {
     if (cprog) { qcb_program_destroy(cprog); cprog = nullptr; }
     if (int st = qcb_program_compile(ops, n_ops, &cprog)) return st;
     cops.assign(ops, ops + n_ops);
+    if (int st = image.build(*cprog)) return st;
   }
+  // The circuit is an input of every call: its compiled records, noise
+  // classes and count tables go host -> device each call, from page-locked
+  // memory, ahead of the walk on the same stream (the host-side compile is
+  // what the op-list comparison saves).
+  if (int st = image.upload(*cprog, S(stream))) return st;
   // _create_pauliframe: qmax / bmax with init = 1 (src/pauli_frames.jl:197-201)
   const uint32_t qmax = std::max<uint32_t>(cprog->info.nqubits, 1);
   const uint32_t bmax = std::max<uint32_t>(cprog->info.nbits, 1);

@@ -34,7 +34,7 @@
 namespace qcb {
 
 static bool is1q(uint32_t o) { return o >= QCB_OP_I && o <= QCB_OP_SQO; }
-static bool is2q(uint32_t o) { return o >= QCB_OP_CNOT && o <= QCB_OP_YCZ; }
+static bool is2q(uint32_t o) { return o >= QCB_OP_CNOT && o <= QCB_OP_LAST2Q; }
 static bool isnoise(uint32_t o) { return o >= QCB_OP_PAULI_NOISE && o <= QCB_OP_DEPOL2; }
 static bool ismeas(uint32_t o) { return o >= QCB_OP_MZ && o <= QCB_OP_MRX; }
 // frame action x <-> z
@@ -577,6 +577,13 @@ int qcb_debug_program_dump(const qcb_op* ops, size_t n_ops, uint32_t* stream, si
 int qcb_program_info_get(const qcb_program* prog, qcb_program_info* info) {
   if (!prog || !info) return fail(QCB_EARG, "null argument");
   *info = prog->info;
+  return QCB_OK;
+}
+
+int qcb_program_device_bytes(const qcb_program* prog, uint64_t* bytes) {
+  if (!prog || !bytes) return fail(QCB_EARG, "null argument");
+  *bytes = prog->stream_slot.size() * sizeof(uint32_t) + prog->classes.size() * sizeof(NoiseClass) +
+           prog->cdf.size() * sizeof(uint32_t);
   return QCB_OK;
 }
 

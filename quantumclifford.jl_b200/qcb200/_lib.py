@@ -130,6 +130,7 @@ def lib():
         "qcb_launch_count": ([], u64),
         "qcb_program_compile": ([vp, sz, P(vp)], ctypes.c_int),
         "qcb_program_info_get": ([vp, P(qcb_program_info)], ctypes.c_int),
+        "qcb_program_device_bytes": ([vp, P(u64)], ctypes.c_int),
         "qcb_program_destroy": ([vp], ctypes.c_int),
         "qcb_frame_create": ([u64, u32, u32, P(vp)], ctypes.c_int),
         "qcb_frame_destroy": ([vp], ctypes.c_int),

@@ -115,30 +115,72 @@ def rotated_surface_code_memory(d: int = 11, rounds: int | None = None, p: float
     return c
 
 
-def surface_code_detectors(record, d: int, rounds: int | None = None):
-    """Z-type detectors of the memory-Z circuit from a Bool record matrix
-    (frames x bits): XOR of consecutive rounds of each Z ancilla, and the
-    final round against the data parity of each Z plaquette.  Returns an
-    int8 matrix frames x n_detectors."""
-    import numpy as np
+def surface_code_detector_bits(d: int, rounds: int | None = None, basis: str = "Z") -> list:
+    """Detectors of the memory-Z circuit as lists of 0-based record bits whose
+    XOR is the detector.
 
+    basis "Z": per Z ancilla its first-round outcome, the XOR of consecutive
+    rounds, and the last round against the data parity of its plaquette
+    (deterministic in the noiseless circuit).  basis "X": per X ancilla the
+    XOR of consecutive rounds (rounds 2..rounds; the first-round X outcome is
+    random in a memory-Z experiment and the data are not measured in X).
+    basis "X1": the first-round X outcomes alone (rate 1/2)."""
     rounds = d if rounds is None else rounds
     plaq = rotated_surface_code_layout(d)
     xs = [pq for pq in plaq if pq[0] == "X"]
     zs = [pq for pq in plaq if pq[0] == "Z"]
     na = len(xs) + len(zs)
-    nd = d * d
+    dets = []
+    if basis == "Z":
+        for k, pq in enumerate(zs):
+            col = len(xs) + k
+            dets.append([col])
+            for r in range(1, rounds):
+                dets.append([na * (r - 1) + col, na * r + col])
+            dets.append([na * (rounds - 1) + col] + [na * rounds + q - 1 for q in pq[3].values()])
+    elif basis == "X":
+        for col in range(len(xs)):
+            for r in range(1, rounds):
+                dets.append([na * (r - 1) + col, na * r + col])
+    elif basis == "X1":
+        dets = [[col] for col in range(len(xs))]
+    else:
+        raise ValueError("basis must be 'Z', 'X' or 'X1'")
+    return dets
+
+
+def surface_code_detectors(record, d: int, rounds: int | None = None, basis: str = "Z"):
+    """Detectors (surface_code_detector_bits) of the memory-Z circuit from a
+    Bool record matrix (frames x bits).  Returns an int8 matrix frames x
+    n_detectors."""
+    import numpy as np
+
     rec = np.asarray(record, dtype=np.int8)
     dets = []
-    for k, pq in enumerate(zs):
-        col = len(xs) + k
-        prev = None
-        for r in range(rounds):
-            cur = rec[:, na * r + col]
-            dets.append(cur if prev is None else cur ^ prev)
-            prev = cur
-        par = np.zeros(rec.shape[0], dtype=np.int8)
-        for q in pq[3].values():
-            par ^= rec[:, na * rounds + q - 1]
-        dets.append(par ^ prev)
+    for bits in surface_code_detector_bits(d, rounds, basis):
+        v = rec[:, bits[0]].copy()
+        for b in bits[1:]:
+            v ^= rec[:, b]
+        dets.append(v)
     return np.stack(dets, axis=1)
+
+
+def detector_counts_from_planes(planes, frames: int, detectors: list):
+    """Number of shots in which each detector fires, from shot-packed record
+    planes (uint32 [nbits, words], bit s%32 of word s//32 = shot s).  Padding
+    shots of the last word are masked off."""
+    import numpy as np
+
+    planes = np.asarray(planes, dtype=np.uint32)
+    words = (frames + 31) // 32
+    mask = np.full(words, 0xFFFFFFFF, dtype=np.uint32)
+    if frames % 32:
+        mask[-1] = np.uint32((1 << (frames % 32)) - 1)
+    out = np.zeros(len(detectors), dtype=np.int64)
+    for i, bits in enumerate(detectors):
+        v = planes[bits[0], :words].copy()
+        for b in bits[1:]:
+            v ^= planes[b, :words]
+        v &= mask
+        out[i] = int(np.unpackbits(v.view(np.uint8)).sum())
+    return out

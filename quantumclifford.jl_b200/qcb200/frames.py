@@ -301,6 +301,17 @@ def unpack_record(planes: np.ndarray, frames: int) -> np.ndarray:
     return b[:, :frames].T.astype(bool)
 
 
+def pack_record(meas: np.ndarray) -> np.ndarray:
+    """Bool matrix frames x nbits -> shot-packed record planes uint32
+    [nbits, ceil(frames/32)] (padding shots zero); inverse of unpack_record."""
+    meas = np.asarray(meas)
+    frames, nbits = meas.shape
+    words = (frames + 31) // 32
+    b = np.zeros((nbits, words * 32), dtype=np.uint8)
+    b[:, :frames] = meas.T
+    return np.packbits(b, axis=1, bitorder="little").view(np.uint32)
+
+
 class Batch:
     """Many fresh sampling runs drained from one persistent launch
     (qcb_batch_*).  ``jobs``: (frame, program, seed[, shot_offset[, tile]])

@@ -153,6 +153,49 @@ static inline u64 gate2(u32 op, u64& x1, u64& z1, u64& x2, u64& z2) {
     case QCB_OP_YCZ:
       x1 = a ^ c; z1 = c ^ b; x2 = c; z2 = d ^ a ^ b;
       ph = c & (a ^ b) & (d ^ a); break;
+    // src/symbolic_cliffords.jl:361-395
+    case QCB_OP_SWAPCX:
+      x1 = c; z1 = d ^ b; x2 = c ^ a; z2 = b;
+      ph = (a & b & c & d) | (~a & b & c & ~d); break;
+    case QCB_OP_INVSWAPCX:
+      x1 = c ^ a; z1 = d; x2 = a; z2 = d ^ b;
+      ph = (a & b & c & d) | (a & ~b & ~c & d); break;
+    case QCB_OP_ISWAP:
+      x1 = c; z1 = a ^ d ^ c; x2 = a; z2 = a ^ c ^ b;
+      ph = (a & b & ~c) | (~a & c & d); break;
+    case QCB_OP_INVISWAP:
+      x1 = c; z1 = a ^ d ^ c; x2 = a; z2 = a ^ c ^ b;
+      ph = (a & ~b & ~c) | (~a & c & ~d); break;
+    case QCB_OP_CZSWAP:
+      x1 = c; z1 = d ^ a; x2 = a; z2 = c ^ b;
+      ph = (a & ~b & c & d) | (a & b & c & ~d); break;
+    case QCB_OP_CXSWAP:
+      x1 = c ^ a; z1 = d; x2 = a; z2 = d ^ b;
+      ph = (a & ~b & ~c & d) | (a & b & c & d); break;
+    case QCB_OP_ZCRY:
+      x1 = a; z1 = a ^ b ^ c ^ d; x2 = a ^ c; z2 = a ^ d;
+      ph = (a & ~b & c) | (a & ~b & ~d) | (a & c & ~d); break;
+    case QCB_OP_INVZCRY:
+      x1 = a; z1 = a ^ b ^ c ^ d; x2 = a ^ c; z2 = a ^ d;
+      ph = (a & b & ~c) | (a & b & d) | (a & ~c & d); break;
+    case QCB_OP_SQRTZZ:
+      x1 = a; z1 = a ^ c ^ b; x2 = c; z2 = a ^ d ^ c;
+      ph = (a & b & ~c) | (~a & c & d); break;
+    case QCB_OP_INVSQRTZZ:
+      x1 = a; z1 = a ^ c ^ b; x2 = c; z2 = a ^ d ^ c;
+      ph = (a & ~b & ~c) | (~a & c & ~d); break;
+    case QCB_OP_SQRTXX:
+      x1 = b ^ d ^ a; z1 = b; x2 = b ^ c ^ d; z2 = d;
+      ph = (~a & b & ~d) | (~b & ~c & d); break;
+    case QCB_OP_INVSQRTXX:
+      x1 = b ^ d ^ a; z1 = b; x2 = b ^ c ^ d; z2 = d;
+      ph = (a & b & ~d) | (~b & c & d); break;
+    case QCB_OP_SQRTYY:
+      x1 = b ^ c ^ d; z1 = a ^ d ^ c; x2 = a ^ b ^ d; z2 = a ^ c ^ b;
+      ph = (~a & ~b & c & ~d) | (a & ~b & ~c & ~d) | (a & ~b & c & d) | (a & b & c & ~d); break;
+    case QCB_OP_INVSQRTYY:
+      x1 = b ^ c ^ d; z1 = a ^ d ^ c; x2 = a ^ b ^ d; z2 = a ^ c ^ b;
+      ph = (a & b & ~c & d) | (~a & b & c & d) | (~a & b & ~c & ~d) | (~a & ~b & ~c & d); break;
     default: break;
   }
   return ph;
@@ -163,7 +206,7 @@ static inline bool is1q(u32 op) { return op >= QCB_OP_I && op <= QCB_OP_SQO; }
 static inline u32 code1(const qcb_op& op) {
   return op.opcode == QCB_OP_SQO ? op.opcode | ((op.q2 & 63u) << 8) : op.opcode;
 }
-static inline bool is2q(u32 op) { return op >= QCB_OP_CNOT && op <= QCB_OP_YCZ; }
+static inline bool is2q(u32 op) { return op >= QCB_OP_CNOT && op <= QCB_OP_LAST2Q; }
 
 // ---------------------------------------------------------------- Pauli rows
 // mul_left!(r, l) on raw words (src/mul_leftright.jl:11-31 / 75-126): r ^= l

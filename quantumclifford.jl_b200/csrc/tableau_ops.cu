@@ -220,6 +220,48 @@ __device__ __forceinline__ uint64_t g2(uint32_t op, uint64_t& x1, uint64_t& z1, 
       x1 = a ^ d ^ c; z1 = b ^ c ^ d; x2 = a ^ c ^ b; z2 = a ^ b ^ d;
       return (a & ~b & ~c & d) | (~a & b & c & ~d);
     case QCB_OP_YCZ: x1 = a ^ c; z1 = c ^ b; z2 = d ^ a ^ b; return c & (a ^ b) & (d ^ a);
+    case QCB_OP_SWAPCX:
+      x1 = c; z1 = d ^ b; x2 = c ^ a; z2 = b;
+      return (a & b & c & d) | (~a & b & c & ~d);
+    case QCB_OP_INVSWAPCX:
+      x1 = c ^ a; z1 = d; x2 = a; z2 = d ^ b;
+      return (a & b & c & d) | (a & ~b & ~c & d);
+    case QCB_OP_ISWAP:
+      x1 = c; z1 = a ^ d ^ c; x2 = a; z2 = a ^ c ^ b;
+      return (a & b & ~c) | (~a & c & d);
+    case QCB_OP_INVISWAP:
+      x1 = c; z1 = a ^ d ^ c; x2 = a; z2 = a ^ c ^ b;
+      return (a & ~b & ~c) | (~a & c & ~d);
+    case QCB_OP_CZSWAP:
+      x1 = c; z1 = d ^ a; x2 = a; z2 = c ^ b;
+      return (a & ~b & c & d) | (a & b & c & ~d);
+    case QCB_OP_CXSWAP:
+      x1 = c ^ a; z1 = d; x2 = a; z2 = d ^ b;
+      return (a & ~b & ~c & d) | (a & b & c & d);
+    case QCB_OP_ZCRY:
+      z1 = a ^ b ^ c ^ d; x2 = a ^ c; z2 = a ^ d;
+      return (a & ~b & c) | (a & ~b & ~d) | (a & c & ~d);
+    case QCB_OP_INVZCRY:
+      z1 = a ^ b ^ c ^ d; x2 = a ^ c; z2 = a ^ d;
+      return (a & b & ~c) | (a & b & d) | (a & ~c & d);
+    case QCB_OP_SQRTZZ:
+      z1 = a ^ c ^ b; z2 = a ^ d ^ c;
+      return (a & b & ~c) | (~a & c & d);
+    case QCB_OP_INVSQRTZZ:
+      z1 = a ^ c ^ b; z2 = a ^ d ^ c;
+      return (a & ~b & ~c) | (~a & c & ~d);
+    case QCB_OP_SQRTXX:
+      x1 = b ^ d ^ a; x2 = b ^ c ^ d;
+      return (~a & b & ~d) | (~b & ~c & d);
+    case QCB_OP_INVSQRTXX:
+      x1 = b ^ d ^ a; x2 = b ^ c ^ d;
+      return (a & b & ~d) | (~b & c & d);
+    case QCB_OP_SQRTYY:
+      x1 = b ^ c ^ d; z1 = a ^ d ^ c; x2 = a ^ b ^ d; z2 = a ^ c ^ b;
+      return (~a & ~b & c & ~d) | (a & ~b & ~c & ~d) | (a & ~b & c & d) | (a & b & c & ~d);
+    case QCB_OP_INVSQRTYY:
+      x1 = b ^ c ^ d; z1 = a ^ d ^ c; x2 = a ^ b ^ d; z2 = a ^ c ^ b;
+      return (a & b & ~c & d) | (~a & b & c & d) | (~a & b & ~c & ~d) | (~a & ~b & ~c & d);
     default: return 0;
   }
 }
@@ -609,7 +651,7 @@ int qcb_apply_gates(qcb_tableau* t, const qcb_op* ops, size_t n_ops, int phases,
   for (size_t k = 0; k < n_ops; k++) {
     const qcb_op& o = ops[k];
     const bool one = o.opcode >= QCB_OP_I && o.opcode <= QCB_OP_SQO;
-    const bool two = o.opcode >= QCB_OP_CNOT && o.opcode <= QCB_OP_YCZ;
+    const bool two = o.opcode >= QCB_OP_CNOT && o.opcode <= QCB_OP_LAST2Q;
     if (!one && !two) return fail(QCB_EUNSUPPORTED, "qcb_apply_gates: op " + std::to_string(k) + " is not a symbolic Clifford gate");
     if (o.q1 == 0 || (two && o.q2 == 0)) return fail(QCB_EZEROQUBIT, "qubit indices start at 1 (NoZeroQubit)");
     if (two && o.q1 == o.q2) return fail(QCB_EARG, "Failed to create a two qubit gate because the two qubits it acts on have the same index. The qubit indices have to be different.");

@@ -46,6 +46,9 @@ const OPC = Dict{DataType,UInt32}(
     sSQRTX => 8, sInvSQRTX => 9, sSQRTY => 10, sInvSQRTY => 11, sHadamardXY => 12, sHadamardYZ => 13,
     sCXYZ => 14, sCZYX => 15, sCNOT => 32, sCPHASE => 33, sSWAP => 34, sZCX => 35, sZCY => 36,
     sZCZ => 37, sXCX => 38, sXCY => 39, sXCZ => 40, sYCX => 41, sYCY => 42, sYCZ => 43,
+    sSWAPCX => 44, sInvSWAPCX => 45, sISWAP => 46, sInvISWAP => 47, sCZSWAP => 48, sCXSWAP => 49,
+    sZCrY => 50, sInvZCrY => 51, sSQRTZZ => 52, sInvSQRTZZ => 53, sSQRTXX => 54, sInvSQRTXX => 55,
+    sSQRTYY => 56, sInvSQRTYY => 57,
     sMZ => 64, sMRZ => 65, sMX => 66, sMRX => 67)
 
 _qcbops(op::AbstractSingleQubitOperator) = [QcbOp(OPC[typeof(op)], op.q, 0, 0, (0.0, 0.0, 0.0))]

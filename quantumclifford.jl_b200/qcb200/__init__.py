@@ -13,12 +13,13 @@ from ._lib import (  # noqa: F401
 from .ops import (  # noqa: F401
     Op, OP, sId1, sHadamard, sPhase, sInvPhase, sX, sY, sZ, sSQRTX, sInvSQRTX, sSQRTY, sInvSQRTY,
     sHadamardXY, sHadamardYZ, sCXYZ, sCZYX, SingleQubitOperator, sCNOT, sCPHASE, sSWAP, sZCX, sZCY, sZCZ, sXCX, sXCY, sXCZ,
-    sYCX, sYCY, sYCZ, sMZ, sMRZ, sMX, sMRX, ClassicalXOR, PauliMeasurement, PauliError, NoiseOp, PauliNoise, UnbiasedUncorrelatedNoise,
+    sYCX, sYCY, sYCZ, sSWAPCX, sInvSWAPCX, sISWAP, sInvISWAP, sCZSWAP, sCXSWAP, sZCrY, sInvZCrY, sSQRTZZ,
+    sInvSQRTZZ, sSQRTXX, sInvSQRTXX, sSQRTYY, sInvSQRTYY, sMZ, sMRZ, sMX, sMRX, ClassicalXOR, PauliMeasurement, PauliError, NoiseOp, PauliNoise, UnbiasedUncorrelatedNoise,
     DepolarizationNoise, NoisyGate, NoiseOpAll, to_array, count_updates, affected_counts,
 )
 from .frames import (  # noqa: F401
     PauliFrame, Program, Masks, sample_masks, pftrajectories, pauliframe_, measurements,
-    pftrajectories_record, unpack_record, evaluate_guesses, Batch, tune_tile, Server,
+    pftrajectories_record, unpack_record, pack_record, evaluate_guesses, Batch, tune_tile, Server,
 )
 from .tableau import (  # noqa: F401
     Tableau, PauliOperator, Stabilizer, MixedStabilizer, Destabilizer, MixedDestabilizer, CliffordOperator,
@@ -28,3 +29,4 @@ from .tableau import (  # noqa: F401
     projectrand_, projectXrand_, projectYrand_, projectZrand_, CanonBatch, expect, rowswap_,
 )
 from . import circuits  # noqa: F401
+from .randoms import random_destabilizer, random_stabilizer, random_clifford, random_paulis  # noqa: F401

@@ -19,6 +19,8 @@ OP = dict(
     NOP=0, I=1, H=2, S=3, SDAG=4, X=5, Y=6, Z=7, SQRTX=8, INVSQRTX=9, SQRTY=10, INVSQRTY=11,
     HXY=12, HYZ=13, CXYZ=14, CZYX=15, SQO=16,
     CNOT=32, CPHASE=33, SWAP=34, ZCX=35, ZCY=36, ZCZ=37, XCX=38, XCY=39, XCZ=40, YCX=41, YCY=42, YCZ=43,
+    SWAPCX=44, INVSWAPCX=45, ISWAP=46, INVISWAP=47, CZSWAP=48, CXSWAP=49, ZCRY=50, INVZCRY=51,
+    SQRTZZ=52, INVSQRTZZ=53, SQRTXX=54, INVSQRTXX=55, SQRTYY=56, INVSQRTYY=57,
     MZ=64, MRZ=65, MX=66, MRX=67, XOR=68, XOR_BITS=69,
     PAULI_NOISE=96, DEPOL1=97, DEPOL2=98,
 )
@@ -186,6 +188,20 @@ sXCZ = _two("XCZ")
 sYCX = _two("YCX")
 sYCY = _two("YCY")
 sYCZ = _two("YCZ")
+sSWAPCX = _two("SWAPCX")
+sInvSWAPCX = _two("INVSWAPCX")
+sISWAP = _two("ISWAP")
+sInvISWAP = _two("INVISWAP")
+sCZSWAP = _two("CZSWAP")
+sCXSWAP = _two("CXSWAP")
+sZCrY = _two("ZCRY")
+sInvZCrY = _two("INVZCRY")
+sSQRTZZ = _two("SQRTZZ")
+sInvSQRTZZ = _two("INVSQRTZZ")
+sSQRTXX = _two("SQRTXX")
+sInvSQRTXX = _two("INVSQRTXX")
+sSQRTYY = _two("SQRTYY")
+sInvSQRTYY = _two("INVSQRTYY")
 
 
 # measurements (src/symbolic_cliffords.jl:515-655)
@@ -270,7 +286,7 @@ class NoiseOpAll:
 
 
 def _is_two_qubit(o: Op) -> bool:
-    return OP["CNOT"] <= o.opcode <= OP["YCZ"]
+    return OP["CNOT"] <= o.opcode <= OP["INVSQRTYY"]
 
 
 def NoisyGate(gate, noise) -> list:
@@ -326,7 +342,7 @@ def affected_counts(arr: np.ndarray) -> tuple[int, int]:
         return 1, 1
     oc = arr["opcode"]
     one_q = ((oc >= OP["I"]) & (oc < OP["XOR"])) | (oc >= OP["PAULI_NOISE"])  # ops with a qubit q1
-    two_q = ((oc >= OP["CNOT"]) & (oc <= OP["YCZ"])) | (oc == OP["DEPOL2"])   # and a second qubit q2
+    two_q = ((oc >= OP["CNOT"]) & (oc <= OP["INVSQRTYY"])) | (oc == OP["DEPOL2"])   # and a second qubit q2
     pay = oc == OP["XOR_BITS"]                                                  # record bits in q1, q2, bit
 
     def top(v):

@@ -78,10 +78,11 @@ class Tableau:
         t = cls.zeros(rows, n)
         t.phases[:] = np.asarray(phases, dtype=np.uint8) & 3
         half = nwords(n) // 2
-        for q in range(n):
-            w, b = q >> 6, np.uint64(1 << (q & 63))
-            t.xzs[xs[:, q], w] |= b
-            t.xzs[zs[:, q], half + w] |= b
+        if rows and n:
+            pad = np.zeros((rows, half * 64), dtype=bool)
+            for k, m in enumerate((xs, zs)):  # bit q of a half -> word q >> 6, bit q & 63
+                pad[:, :n] = m
+                t.xzs[:, k * half:(k + 1) * half] = np.packbits(pad, axis=1, bitorder="little").view("<u8")
         return t
 
     def bits(self):

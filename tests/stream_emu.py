@@ -85,6 +85,22 @@ def gate2(op, a, b, c, d):
         return a ^ d ^ c, b ^ c ^ d, a ^ c ^ b, a ^ b ^ d
     if op == n["YCZ"]:
         return a ^ c, c ^ b, c, d ^ a ^ b
+    if op == n["SWAPCX"]:
+        return c, d ^ b, c ^ a, b
+    if op in (n["INVSWAPCX"], n["CXSWAP"]):
+        return c ^ a, d, a, d ^ b
+    if op in (n["ISWAP"], n["INVISWAP"]):
+        return c, a ^ d ^ c, a, a ^ c ^ b
+    if op == n["CZSWAP"]:
+        return c, d ^ a, a, c ^ b
+    if op in (n["ZCRY"], n["INVZCRY"]):
+        return a, a ^ b ^ c ^ d, a ^ c, a ^ d
+    if op in (n["SQRTZZ"], n["INVSQRTZZ"]):
+        return a, a ^ c ^ b, c, a ^ d ^ c
+    if op in (n["SQRTXX"], n["INVSQRTXX"]):
+        return b ^ d ^ a, b, b ^ c ^ d, d
+    if op in (n["SQRTYY"], n["INVSQRTYY"]):
+        return b ^ c ^ d, a ^ d ^ c, a ^ b ^ d, a ^ c ^ b
     raise ValueError(op)
 
 

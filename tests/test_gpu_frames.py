@@ -71,7 +71,9 @@ def random_sqo(q, rng):
 
 def random_circuit(n, length, rng, p=0.05, nbits_start=1):
     g1 = ["H", "S", "SDAG", "X", "Y", "Z", "SQRTX", "INVSQRTX", "SQRTY", "INVSQRTY", "HXY", "HYZ", "CXYZ", "CZYX", "I"]
-    g2 = ["CNOT", "CPHASE", "SWAP", "ZCX", "ZCY", "ZCZ", "XCX", "XCY", "XCZ", "YCX", "YCY", "YCZ"]
+    g2 = ["CNOT", "CPHASE", "SWAP", "ZCX", "ZCY", "ZCZ", "XCX", "XCY", "XCZ", "YCX", "YCY", "YCZ",
+          "SWAPCX", "INVSWAPCX", "ISWAP", "INVISWAP", "CZSWAP", "CXSWAP", "ZCRY", "INVZCRY", "SQRTZZ", "INVSQRTZZ",
+          "SQRTXX", "INVSQRTXX", "SQRTYY", "INVSQRTYY"]
     c, bit = [], nbits_start
     for _ in range(length):
         k = rng.integers(0, 10)

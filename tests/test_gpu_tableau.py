@@ -93,7 +93,9 @@ def test_symbolic_gates_with_phases(qcb, n):
     t = rand_tab(2 * n, n, rng)
     gates = []
     g1 = ["I", "H", "S", "SDAG", "X", "Y", "Z", "SQRTX", "INVSQRTX", "SQRTY", "INVSQRTY", "HXY", "HYZ", "CXYZ", "CZYX"]
-    g2 = ["CNOT", "CPHASE", "SWAP", "ZCX", "ZCY", "ZCZ", "XCX", "XCY", "XCZ", "YCX", "YCY", "YCZ"]
+    g2 = ["CNOT", "CPHASE", "SWAP", "ZCX", "ZCY", "ZCZ", "XCX", "XCY", "XCZ", "YCX", "YCY", "YCZ",
+          "SWAPCX", "INVSWAPCX", "ISWAP", "INVISWAP", "CZSWAP", "CXSWAP", "ZCRY", "INVZCRY", "SQRTZZ", "INVSQRTZZ",
+          "SQRTXX", "INVSQRTXX", "SQRTYY", "INVSQRTYY"]
     for _ in range(300):
         u = rng.random()
         if u < 0.15:

@@ -246,7 +246,9 @@ def test_canonicalize_against_table_method(orc, n, phases):
 
 
 GATES1 = ["I", "H", "S", "SDAG", "X", "Y", "Z", "SQRTX", "INVSQRTX", "SQRTY", "INVSQRTY", "HXY", "HYZ", "CXYZ", "CZYX"]
-GATES2 = ["CNOT", "CPHASE", "SWAP", "ZCX", "ZCY", "ZCZ", "XCX", "XCY", "XCZ", "YCX", "YCY", "YCZ"]
+GATES2 = ["CNOT", "CPHASE", "SWAP", "ZCX", "ZCY", "ZCZ", "XCX", "XCY", "XCZ", "YCX", "YCY", "YCZ",
+          "SWAPCX", "INVSWAPCX", "ISWAP", "INVISWAP", "CZSWAP", "CXSWAP", "ZCRY", "INVZCRY", "SQRTZZ", "INVSQRTZZ",
+          "SQRTXX", "INVSQRTXX", "SQRTYY", "INVSQRTYY"]
 
 
 @pytest.mark.parametrize("gate", GATES1 + GATES2)

@@ -364,6 +364,28 @@ int qcb_mul_left_pauli_batch_noalloc(uint64_t* r_xz, uint8_t* r_phases, const ui
 int qcb_rowswap(qcb_tableau* t, int kind, uint32_t i, uint32_t j, int phases, void* stream);
 /* mul_left!(s::Tableau, m, i; phases) (src/mul_leftright.jl:177-181).      */
 int qcb_mul_left_row(qcb_tableau* s, uint32_t m, uint32_t i, int phases, void* stream);
+/* The mul_left! / mul_right! family on rows (src/mul_leftright.jl:137-245;
+ * the device methods of ext/QuantumCliffordKAExt/mul_leftright.jl:101-460).
+ * For k < count, target row a = s_row + k of s and source row
+ * b = t_row + k * t_step of t (1-based; t_step 0 repeats one source row):
+ *   right == 0: s[a] <- t[b] * s[a]    (mul_left!)
+ *   right != 0: s[a] <- s[a] * t[b]    (mul_right!)
+ * With `phases`, s.phases[a] <- (extra + s.phases[a] + P) & 3, where P is
+ * t.phases[b] (phase_src 0: the PauliOperator forms, mul_left!(s, p), and the
+ * KA extension's methods) or s.phases[b] (phase_src 1: the reference's
+ * mul_left!(s, m, t, i) / mul_right!(s, m, t, i), which read s.phases[i],
+ * src/mul_leftright.jl:171-175, 183-187).  s and t may be one tableau; then
+ * the source rows must not overlap the target rows (unless they are the same
+ * rows, count > 1).  With count == 1 and phase_out non-NULL the new phase is
+ * written there (the call then synchronises the stream).                    */
+int qcb_mul_rows(qcb_tableau* s, uint32_t s_row, uint32_t count, const qcb_tableau* t, uint32_t t_row,
+                 uint32_t t_step, int right, int phase_src, int phases, uint8_t* phase_out, void* stream);
+/* mul_left!(state, i, j; phases) (src/mul_leftright.jl:194-219), 1-based:
+ * Stabilizer / MixedStabilizer: row i <- row j * row i of the tableau;
+ * Destabilizer / MixedDestabilizer (2n rows): destabilizer j <- destabilizer
+ * i * destabilizer j without phases, then stabilizer i <- stabilizer j *
+ * stabilizer i (rows n+i, n+j) with phases.                                 */
+int qcb_mul_left_state(qcb_tableau* s, int kind, uint32_t i, uint32_t j, int phases, void* stream);
 /* mul_left!(s::Tableau, p::PauliOperator; phases) (src/mul_leftright.jl:223-229). */
 int qcb_mul_left_tableau_pauli(qcb_tableau* s, const qcb_tableau* p, int phases, void* stream);
 /* prodphase / comm of row i of l and row j of r (src/QuantumClifford.jl:723-859). */

@@ -291,6 +291,46 @@ void oracle_mul_left_pauli(u64* r, u8* r_phase, const u64* l, u8 l_phase, size_t
 u8 oracle_prodphase(const u64* l, const u64* r, size_t W) { return row_prodphase(l, r, W); }
 u8 oracle_comm(const u64* l, const u64* r, size_t W) { return row_comm(l, r, W); }
 
+// mul_right!(l, r) on words (src/mul_leftright.jl:128-131): l ^= r through
+// mul_ordered!(l, r) and the phase ((rcnt1 ^ (rcnt2 << 1)) + 2 rcnt1) & 3.
+static inline u8 row_mul_right(u64* l, const u64* r, size_t W, bool phases) {
+  size_t len = W / 2;
+  if (!phases) {
+    for (size_t i = 0; i < W; i++) l[i] ^= r[i];
+    return 0;
+  }
+  u64 cnt1 = 0, cnt2 = 0;
+  for (size_t i = 0; i < len; i++) {
+    u64 x1 = r[i], x2 = l[i], z1 = r[i + len], z2 = l[i + len];
+    u64 newx1 = x1 ^ x2, newz1 = z1 ^ z2;
+    l[i] = newx1; l[i + len] = newz1;
+    u64 x1z2 = x1 & z2;
+    u64 anti = (x2 & z1) ^ x1z2;
+    cnt2 ^= (cnt1 ^ newx1 ^ newz1 ^ x1z2) & anti;
+    cnt1 ^= anti;
+  }
+  int c1 = popc64(cnt1), c2 = popc64(cnt2);
+  return (u8)(((c1 ^ (c2 << 1)) + c1 * 2) & 3);
+}
+
+// The mul_left!/mul_right! family on rows, one reference call per target
+// row, in order (src/mul_leftright.jl:137-245): s[a] <- t[b] * s[a]
+// (right = 0) or s[a] * t[b] (right = 1), a = s_row + k, b = t_row + k*t_step
+// (1-based), phase (extra + s.phases[a] + P) & 3 with P = t.phases[b]
+// (phase_src 0) or s.phases[b] (phase_src 1, :171-175, 183-187).
+void oracle_mul_rows(u64* s_xz, u8* s_ph, const u64* t_xz, const u8* t_ph, size_t W, size_t s_row,
+                     size_t count, size_t t_row, size_t t_step, int right, int phase_src, int phases) {
+  std::vector<u64> src(W);
+  for (size_t k = 0; k < count; k++) {
+    size_t a = s_row - 1 + k, b = t_row - 1 + k * t_step;
+    std::copy(t_xz + b * W, t_xz + (b + 1) * W, src.begin());  // as the reference's view reads it
+    u8 add = phase_src ? s_ph[b] : t_ph[b];
+    u8 e = right ? row_mul_right(s_xz + a * W, src.data(), W, phases != 0)
+                 : row_mul_left(s_xz + a * W, src.data(), W, phases != 0);
+    if (phases) s_ph[a] = (u8)((e + s_ph[a] + add) & 3);
+  }
+}
+
 void oracle_mul_left_row(u64* xzs, u8* ph, size_t W, size_t m, size_t i, int phases) {
   Tab t{xzs, ph, W, 0};
   tab_mul_left(t, m - 1, i - 1, phases != 0);

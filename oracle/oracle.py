@@ -46,6 +46,7 @@ def L():
             "oracle_prodphase": ([vp, vp, sz], u8),
             "oracle_comm": ([vp, vp, sz], u8),
             "oracle_mul_left_row": ([vp, vp, sz, sz, sz, i], None),
+            "oracle_mul_rows": ([vp, vp, vp, vp, sz, sz, sz, sz, sz, i, i, i], None),
             "oracle_mul_left_tableau_pauli": ([vp, vp, sz, sz, vp, u8, i], None),
             "oracle_canonicalize": ([vp, vp, sz, u32, i, P(ctypes.c_int), P(ctypes.c_int)], None),
             "oracle_generate": ([vp, vp, vp, vp, sz, u32, i, vp, P(sz)], i),
@@ -90,6 +91,20 @@ def mul_left_pauli(r_xz, r_phase, l_xz, l_phase, phases=True):
     l = np.ascontiguousarray(l_xz, dtype=np.uint64)
     L().oracle_mul_left_pauli(_p(r), _p(ph), _p(l), int(l_phase), len(r), int(phases))
     return r, int(ph[0])
+
+
+def mul_rows(s_ph, s_xz, t_ph, t_xz, s_row, count, t_row, t_step, right=False, phase_src=0, phases=True):
+    """The mul_left!/mul_right! family on rows (1-based; see oracle.cpp).
+    s is updated on copies: returns (phases, xzs).  Pass t_ph/t_xz = None for
+    t = s (the source rows are read as they are when each target row is done)."""
+    ph = np.array(s_ph, dtype=np.uint8, copy=True)
+    xz = np.array(s_xz, dtype=np.uint64, copy=True)
+    same = t_xz is None
+    tx = xz if same else np.ascontiguousarray(t_xz, dtype=np.uint64)
+    tp = ph if same else np.ascontiguousarray(t_ph, dtype=np.uint8)
+    L().oracle_mul_rows(_p(xz), _p(ph), _p(tx), _p(tp), xz.shape[1], s_row, count, t_row, t_step, int(right),
+                        int(phase_src), int(phases))
+    return ph, xz
 
 
 def prodphase(l_xz, l_ph, r_xz, r_ph):

@@ -31,12 +31,20 @@ __device__ __forceinline__ uint32_t cnt_phase(uint64_t c1, uint64_t c2) {
   return (uint32_t)(__popcll(c1) + 2 * __popcll(c2));
 }
 
+// mul_right!(l, r) runs the word steps of mul_left!(l <- r * l) and adds
+// twice the anticommutation count (src/mul_leftright.jl:128-131): phase
+// (rcnt1 + 2 rcnt2) + 2 rcnt1, i.e. 3 popc(cnt1) + 2 popc(cnt2) per lane.
+template <bool RIGHT>
+__device__ __forceinline__ uint32_t lane_phase(uint64_t c1, uint64_t c2) {
+  return RIGHT ? (uint32_t)(3 * __popcll(c1) + 2 * __popcll(c2)) : cnt_phase(c1, c2);
+}
+
 // Grid-stride mul_left! over two long Paulis.  VEC = 2 uses 128-bit loads
 // (needs len even and 16-byte aligned halves).  Each block adds its phase
 // sum (mod 4) into acc[0] and counts itself done in acc[1]; the last block
 // to finish writes r.phase <- (s + r.phase + l.phase) & 3
 // (src/mul_leftright.jl:140) and clears both, so one launch does the call.
-template <int VEC, bool PH>
+template <int VEC, bool PH, bool RIGHT = false>
 __global__ void __launch_bounds__(256) mul_left_long_kernel(uint64_t* __restrict__ r,
                                                             const uint64_t* __restrict__ l,
                                                             uint64_t len, uint32_t* acc,
@@ -68,7 +76,7 @@ __global__ void __launch_bounds__(256) mul_left_long_kernel(uint64_t* __restrict
     }
   }
   if (!PH) return;
-  uint32_t v = (cnt_phase(c1a, c2a) + cnt_phase(c1b, c2b)) & 3u;
+  uint32_t v = (lane_phase<RIGHT>(c1a, c2a) + lane_phase<RIGHT>(c1b, c2b)) & 3u;
   v = __reduce_add_sync(0xFFFFFFFFu, v) & 3u;
   __shared__ uint32_t wsum[32];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -141,6 +149,37 @@ __global__ void mul_left_row_kernel(uint64_t* xzs, uint8_t* ph, uint32_t W, uint
     if (lane == 0) ph[m] = (uint8_t)((s + ph[m] + ph[i]) & 3u);
   } else {
     warp_mul_left_row<false>(r, l, W / 2, lane);
+  }
+}
+
+// The mul_left!/mul_right! family on rows (src/mul_leftright.jl:137-245,
+// ext/QuantumCliffordKAExt/mul_leftright.jl:101-460): one warp per target row
+// a = s_row + k, source row b = t_row + k * t_step; the added phase is
+// add_ph[b] (t's phases, or s's for the reference's cross-tableau methods).
+template <bool RIGHT, bool PH>
+__global__ void __launch_bounds__(256) mul_rows_kernel(uint64_t* s_xz, uint8_t* s_ph, uint32_t s_row,
+                                                       uint32_t count, const uint64_t* t_xz, uint32_t t_row,
+                                                       uint32_t t_step, uint32_t W, const uint8_t* add_ph) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t len = W / 2;
+  for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < count; k += nwarps) {
+    const uint32_t a = s_row + k, b = t_row + k * t_step;
+    uint64_t* r = s_xz + (uint64_t)a * W;
+    const uint64_t* l = t_xz + (uint64_t)b * W;
+    uint64_t c1 = 0, c2 = 0;
+    for (uint32_t w = lane; w < len; w += 32) {
+      uint64_t rx = r[w], rz = r[len + w];
+      const uint64_t lx = l[w], lz = l[len + w];
+      if (PH) mul_step(lx, lz, rx, rz, c1, c2);
+      else { rx ^= lx; rz ^= lz; }
+      r[w] = rx;
+      r[len + w] = rz;
+    }
+    if (PH) {
+      const uint32_t v = __reduce_add_sync(0xFFFFFFFFu, lane_phase<RIGHT>(c1, c2) & 3u) & 3u;
+      if (lane == 0) s_ph[a] = (uint8_t)((v + s_ph[a] + add_ph[b]) & 3u);
+    }
   }
 }
 
@@ -594,6 +633,79 @@ int qcb_rowswap(qcb_tableau* t, int kind, uint32_t i, uint32_t j, int phases, vo
                                                            j - 1, destab ? 1 : 0, phases);
   QCB_LAUNCHED();
   return QCB_OK;
+}
+
+int qcb_mul_rows(qcb_tableau* s, uint32_t s_row, uint32_t count, const qcb_tableau* t, uint32_t t_row,
+                 uint32_t t_step, int right, int phase_src, int phases, uint8_t* phase_out, void* stream) {
+  if (!s || !t) return fail(QCB_EARG, "null tableau");
+  if (s->nqubits != t->nqubits) return fail(QCB_EDIM, "The two Pauli operators should have the same length!");
+  if (!count) return QCB_OK;
+  const uint64_t last_b = (uint64_t)t_row + (uint64_t)(count - 1) * t_step;
+  if (s_row < 1 || t_row < 1 || (uint64_t)s_row + count - 1 > s->rows || last_b > t->rows)
+    return fail(QCB_EBOUNDS, "row index out of bounds");
+  if (phase_src && last_b > s->rows) return fail(QCB_EBOUNDS, "row index out of bounds (phase taken from s)");
+  if (s == t && count > 1) {  // rows read by one warp must not be written by another
+    const bool same = (t_row == s_row && t_step == 1);
+    const uint64_t b_lo = t_row, b_hi = last_b;
+    const bool disjoint = (b_hi < s_row || b_lo >= (uint64_t)s_row + count);
+    if (!same && !disjoint)
+      return fail(QCB_EARG, "source rows overlap the target rows of the same tableau");
+  }
+  cudaStream_t st = S(stream);
+  const uint8_t* add = phase_src ? s->phases : t->phases;
+  const uint32_t a0 = s_row - 1, b0 = t_row - 1;
+  const uint64_t len = s->W / 2;
+  if (count == 1 && len >= (1u << 15)) {
+    // one long row: the grid-stride kernel of mul_left!(::PauliOperator, ...)
+    const bool vec = (len % 2 == 0);
+    uint64_t* r = s->xzs + (uint64_t)a0 * s->W;
+    const uint64_t* l = t->xzs + (uint64_t)b0 * t->W;
+    const bool aligned = ((uintptr_t)r % 16 == 0) && ((uintptr_t)l % 16 == 0);
+    void (*k)(uint64_t*, const uint64_t*, uint64_t, uint32_t*, uint8_t*, const uint8_t*);
+    if (vec && aligned)
+      k = right ? (phases ? mul_left_long_kernel<2, true, true> : mul_left_long_kernel<2, false, true>)
+                : (phases ? mul_left_long_kernel<2, true> : mul_left_long_kernel<2, false>);
+    else
+      k = right ? (phases ? mul_left_long_kernel<1, true, true> : mul_left_long_kernel<1, false, true>)
+                : (phases ? mul_left_long_kernel<1, true> : mul_left_long_kernel<1, false>);
+    int per_sm = 0;
+    QCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, 0));
+    const uint64_t work = (vec && aligned) ? len / 2 : len;
+    uint32_t blocks = (uint32_t)std::min<uint64_t>((work + 255) / 256,
+                                                   (uint64_t)device_sm_count() * std::max(per_sm, 1));
+    k<<<std::max(blocks, 1u), 256, 0, st>>>(r, l, len, s->scratch, s->phases + a0, add + b0);
+    QCB_LAUNCHED();
+  } else {
+    const uint32_t warps_per_block = 8;
+    const uint32_t blocks = (uint32_t)std::min<uint64_t>((count + warps_per_block - 1) / warps_per_block,
+                                                         (uint64_t)device_sm_count() * 16);
+    void (*k)(uint64_t*, uint8_t*, uint32_t, uint32_t, const uint64_t*, uint32_t, uint32_t, uint32_t,
+              const uint8_t*) = right ? (phases ? mul_rows_kernel<true, true> : mul_rows_kernel<true, false>)
+                                      : (phases ? mul_rows_kernel<false, true> : mul_rows_kernel<false, false>);
+    k<<<blocks, 256, 0, st>>>(s->xzs, s->phases, a0, count, t->xzs, b0, t_step, s->W, add);
+    QCB_LAUNCHED();
+  }
+  if (phase_out) {
+    QCB_CUDA(cudaMemcpyAsync(phase_out, s->phases + a0, 1, cudaMemcpyDeviceToHost, st));
+    QCB_CUDA(cudaStreamSynchronize(st));
+  }
+  return QCB_OK;
+}
+
+int qcb_mul_left_state(qcb_tableau* s, int kind, uint32_t i, uint32_t j, int phases, void* stream) {
+  if (!s) return fail(QCB_EARG, "null tableau");
+  if (kind == QCB_DESTABILIZER || kind == QCB_MIXED_DESTABILIZER) {
+    // src/mul_leftright.jl:200-219: destabilizer j <- destabilizer i * j
+    // without phases (indices flipped), then stabilizer i <- stabilizer j * i
+    if (s->rows % 2) return fail(QCB_EDIM, "a Destabilizer tableau has 2n rows");
+    const uint32_t n = s->rows / 2;
+    if (i < 1 || j < 1 || i > n || j > n) return fail(QCB_EBOUNDS, "row index out of bounds");
+    if (int st = qcb_mul_rows(s, j, 1, s, i, 0, 0, 0, 0, nullptr, stream)) return st;
+    return qcb_mul_rows(s, i + n, 1, s, j + n, 0, 0, 0, phases, nullptr, stream);
+  }
+  if (kind != QCB_STABILIZER && kind != QCB_MIXED_STABILIZER) return fail(QCB_EARG, "unknown state kind");
+  // src/mul_leftright.jl:194-198, 207-211: rows of the tableau
+  return qcb_mul_rows(s, i, 1, s, j, 0, 0, 0, phases, nullptr, stream);
 }
 
 int qcb_mul_left_row(qcb_tableau* s, uint32_t m, uint32_t i, int phases, void* stream) {

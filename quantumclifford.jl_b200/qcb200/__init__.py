@@ -24,7 +24,7 @@ from .frames import (  # noqa: F401
 from .tableau import (  # noqa: F401
     Tableau, PauliOperator, Stabilizer, MixedStabilizer, Destabilizer, MixedDestabilizer, CliffordOperator,
     P, S, T, tCNOT, tensor_pow, one_destabilizer, one_mixed_destabilizer, random_clifford_ops,
-    mul_left_, mul_left_row_, prodphase, comm, canonicalize_, project_, generate_, apply_, DeviceTableau,
+    mul_left_, mul_right_, mul_left_row_, prodphase, comm, canonicalize_, project_, generate_, apply_, DeviceTableau,
     canonicalize_rref_, canonicalize_gott_, permutesystems_, projectX_, projectY_, projectZ_,
     projectrand_, projectXrand_, projectYrand_, projectZrand_, CanonBatch, expect, rowswap_,
 )

@@ -159,6 +159,8 @@ def lib():
         "qcb_mul_left_pauli_batch_noalloc": ([vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp],
                                              ctypes.c_int),
         "qcb_mul_left_row": ([vp, u32, u32, ctypes.c_int, vp], ctypes.c_int),
+        "qcb_mul_rows": ([vp, u32, u32, vp, u32, u32, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp], ctypes.c_int),
+        "qcb_mul_left_state": ([vp, ctypes.c_int, u32, u32, ctypes.c_int, vp], ctypes.c_int),
         "qcb_mul_left_tableau_pauli": ([vp, vp, ctypes.c_int, vp], ctypes.c_int),
         "qcb_prodphase": ([vp, u32, vp, u32, vp, vp], ctypes.c_int),
         "qcb_comm": ([vp, u32, vp, u32, vp, vp], ctypes.c_int),

@@ -16,7 +16,7 @@ from typing import Optional
 import numpy as np
 
 from . import ops as _ops
-from ._lib import check, ensure_init, lib, ptr
+from ._lib import DimensionMismatch, check, ensure_init, lib, ptr
 
 KIND = {"Stabilizer": 0, "MixedStabilizer": 1, "Destabilizer": 2, "MixedDestabilizer": 3}
 
@@ -264,14 +264,67 @@ def _tab(x) -> Tableau:
     return x.tab if isinstance(x, Stabilizer) else x
 
 
-def mul_left_(r, l, *, phases: bool = True):
-    """mul_left!(r, l): r <- l * r for device PauliOperators
-    (src/mul_leftright.jl:137-142).  Returns r."""
-    rt, lt = _tab(r), _tab(l)
+def _mul_rows(s, s_row, count, t, t_row, t_step, right, phase_src, phases):
+    st, tt = _tab(s), _tab(t)
     ph = ctypes.c_uint8()
-    check(lib().qcb_mul_left_pauli(rt._need_dev().handle, lt._need_dev().handle, int(phases), ctypes.byref(ph), None))
-    rt.phases[0] = ph.value if phases else rt.phases[0]
-    return r
+    check(lib().qcb_mul_rows(st._need_dev().handle, int(s_row), int(count), tt._need_dev().handle, int(t_row),
+                             int(t_step), int(right), int(phase_src), int(phases),
+                             ctypes.byref(ph) if count == 1 else None, None))
+    if count == 1 and phases:
+        st.phases[s_row - 1] = ph.value
+    return s
+
+
+def _mul_family(right: bool, a, args, phases: bool):
+    """Method table of src/mul_leftright.jl:137-245 (and the device methods of
+    ext/QuantumCliffordKAExt/mul_leftright.jl:101-460), 1-based rows."""
+    if len(args) == 1 and isinstance(_tab(args[0]), PauliOperator) and not isinstance(_tab(a), PauliOperator):
+        # mul_left!(s, p) / mul_right!(s, p): every row of s with p
+        return _mul_rows(a, 1, len(_tab(a)), args[0], 1, 0, right, 0, phases)
+    if len(args) == 1:  # PauliOperator with PauliOperator
+        if _tab(a).nqubits != _tab(args[0]).nqubits:
+            raise DimensionMismatch("The two Pauli operators should have the same length!")
+        return _mul_rows(a, 1, 1, args[0], 1, 0, right, 0, phases)
+    if len(args) == 2 and not isinstance(args[0], (int, np.integer)):
+        # mul_left!(p::PauliOperator, s::Tableau/Stabilizer, i)
+        return _mul_rows(a, 1, 1, args[0], int(args[1]), 0, right, 0, phases)
+    if len(args) == 2:
+        i, j = int(args[0]), int(args[1])
+        if not right and isinstance(a, (Destabilizer, MixedDestabilizer)):
+            # mul_left!(s::(Mixed)Destabilizer, i, j) (src/mul_leftright.jl:200-219)
+            check(lib().qcb_mul_left_state(_tab(a)._need_dev().handle, KIND[a.kind], i, j, int(phases), None))
+            return a
+        # mul_left!(s, m, i) / mul_right!(s, m, i) on one tableau
+        return _mul_rows(a, i, 1, a, j, 0, right, 0, phases)
+    if len(args) == 3:
+        # mul_left!(s::Tableau, m, t::Tableau, i): the reference adds s.phases[i]
+        # (src/mul_leftright.jl:171-175, 183-187)
+        m, t, i = int(args[0]), args[1], int(args[2])
+        return _mul_rows(a, m, 1, t, i, 0, right, 1, phases)
+    raise TypeError("no mul_left!/mul_right! method for these arguments")
+
+
+def mul_left_(a, *args, phases: bool = True):
+    """mul_left!(...) on device objects (src/mul_leftright.jl:137-229):
+    mul_left!(r, l) (r <- l * r for PauliOperators), mul_left!(p, s, i),
+    mul_left!(s, p) (every row), mul_left!(s, m, i), mul_left!(s, m, t, i),
+    and mul_left!(::Destabilizer/::MixedDestabilizer, i, j).  Rows are
+    1-based.  Returns the first argument."""
+    if len(args) == 1 and isinstance(_tab(a), PauliOperator) and isinstance(_tab(args[0]), PauliOperator):
+        rt, lt = _tab(a), _tab(args[0])
+        ph = ctypes.c_uint8()
+        check(lib().qcb_mul_left_pauli(rt._need_dev().handle, lt._need_dev().handle, int(phases), ctypes.byref(ph),
+                                       None))
+        rt.phases[0] = ph.value if phases else rt.phases[0]
+        return a
+    return _mul_family(False, a, args, phases)
+
+
+def mul_right_(a, *args, phases: bool = True):
+    """mul_right!(...) on device objects (src/mul_leftright.jl:128-245):
+    mul_right!(l, r) (l <- l * r), mul_right!(p, s, i), mul_right!(s, p),
+    mul_right!(s, m, i), mul_right!(s, m, t, i).  Rows are 1-based."""
+    return _mul_family(True, a, args, phases)
 
 
 def mul_left_row_(s, m: int, i: int, *, phases: bool = True):

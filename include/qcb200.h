@@ -318,7 +318,11 @@ int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t see
 
 /* Launch-shape overrides used by the tuner ("walker_tile", "canon_threads",
  * "canon_cluster", "project_cluster", "canon_blocked": 1 always / 2 never
- * run canonicalize! by 64-column panels); 0 restores the automatic choice. */
+ * run canonicalize! by 64-column panels); 0 restores the automatic choice.
+ * Test knob "stage_withhold" k > 0: the plain walker never stages window k of
+ * each CTA's program windows, so its bounded wait expires and the run reports
+ * QCB_ETIMEOUT at the next synchronising call (the kernel returns; nothing
+ * faults); a fresh run or initZ! of the frame clears that status.          */
 int qcb_tune_set(const char* key, int64_t value);
 
 /* ------------------------------------------------------------ tableaux    */

@@ -61,6 +61,9 @@ struct WalkArgs {
   const uint64_t* ev_data;  // (trial << 8) | code, sorted per column
   const uint32_t* reset_planes;
   uint64_t reset_pitch;
+  // test knob: window index (of each CTA's sequence) that is never staged, so
+  // the walker's bounded wait runs out (0: none)
+  uint64_t withhold;
 };
 
 // Bit-sliced single-qubit gate (src/symbolic_cliffords.jl:105-118); frames
@@ -160,17 +163,32 @@ __device__ __forceinline__ void stage_window(uint32_t* dst, const uint4* src, ui
       : "memory");
 }
 
-// Returns false when the wait gave up.
+// Bounded wait for the phase `parity` of an mbarrier: each poll suspends at
+// most WAIT_POLL_NS, and the wait gives up after WAIT_LIMIT_NS of the global
+// timer (or 2^24 polls, whichever comes first).  Returns false when it gave up.
+constexpr uint32_t WAIT_POLL_NS = 2000;
+constexpr uint64_t WAIT_LIMIT_NS = 1000000000ull;  // one second
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   const uint32_t b = smem_addr(bar);
-  for (uint32_t it = 0; it < (1u << 22); it++) {
+  uint64_t t0 = 0;
+  for (uint32_t it = 0; it < (1u << 24); it++) {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(b), "r"(parity)
+        : "r"(b), "r"(parity), "r"(WAIT_POLL_NS)
         : "memory");
     if (ok) return true;
+    const uint64_t now = global_ns();
+    if (it == 0) t0 = now;
+    else if (now - t0 > WAIT_LIMIT_NS) return false;
   }
   return false;
 }
@@ -648,7 +666,7 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
   __syncthreads();
   // window k of the flattened (tile, window) sequence lives in buffer k & 1
   auto issue = [&](uint64_t k) {
-    if (k >= total_win) return;
+    if (k >= total_win || (a.withhold && k == a.withhold)) return;
     const uint32_t w = (uint32_t)(k % a.nwin);
     stage_window((k & 1) ? win1 : win0, a.prog + (size_t)w * (a.win_words / 4), a.win_words * 4, &bars[k & 1]);
   };
@@ -891,6 +909,7 @@ int qcb_frame_init_z(qcb_frame* f, uint64_t seed, uint64_t shot_offset, void* st
   if (int st = check_frame(f)) return st;
   if (shot_offset % 32) return fail(QCB_EARG, "shot_offset must be a multiple of 32");
   if (!f->ncols) return QCB_OK;
+  QCB_CUDA(cudaMemsetAsync(f->err, 0, 4, S(stream)));  // the frame is reinitialised
   uint32_t nt = 256;
   initz_kernel<<<(unsigned)((f->ncols + nt - 1) / nt), nt, 0, S(stream)>>>(
       f->planes, f->pitch, f->ncols, f->nq1, seed, shot_offset / 32);
@@ -901,6 +920,7 @@ int qcb_frame_init_z(qcb_frame* f, uint64_t seed, uint64_t shot_offset, void* st
 int qcb_frame_init_z_planes(qcb_frame* f, const uint32_t* z, void* stream) {
   if (int st = check_frame(f)) return st;
   if (!f->ncols) return QCB_OK;
+  QCB_CUDA(cudaMemsetAsync(f->err, 0, 4, S(stream)));  // the frame is reinitialised
   // x planes to zero, z planes from the caller (strided 2D copy)
   QCB_CUDA(cudaMemset2DAsync(f->planes, 2 * f->pitch * 4, 0, f->ncols * 4, f->nq1, S(stream)));
   QCB_CUDA(cudaMemcpy2DAsync(f->planes + f->pitch, 2 * f->pitch * 4, z, f->ncols * 4,
@@ -911,6 +931,7 @@ int qcb_frame_init_z_planes(qcb_frame* f, const uint32_t* z, void* stream) {
 
 int qcb_frame_clear(qcb_frame* f, void* stream) {
   if (int st = check_frame(f)) return st;
+  QCB_CUDA(cudaMemsetAsync(f->err, 0, 4, S(stream)));
   QCB_CUDA(cudaMemsetAsync(f->planes, 0, (size_t)2 * (f->nq1 + 1) * f->pitch * 4, S(stream)));
   QCB_CUDA(cudaMemsetAsync(f->record, 0, (size_t)std::max<uint32_t>(f->nbits, 1) * f->pitch * 4, S(stream)));
   return QCB_OK;
@@ -944,6 +965,7 @@ struct WalkConfig {
 };
 
 static uint32_t g_tile_override = 0;
+static uint32_t g_stage_withhold = 0;     // test knob, see WalkArgs::withhold
 static uint32_t g_threads_override = 0;  // threads per CTA (0: 768)
 
 // Tile width (even: threads own column pairs) for ncols columns with tiles of
@@ -1031,6 +1053,7 @@ static void fill_common(WalkArgs& a, qcb_frame* f, const qcb_program* p) {
   a.cdf = p->d_cdf;
   a.pmax = p->pmax;
   a.err = f->err;
+  a.withhold = g_stage_withhold;
 }
 
 static int check_run(const qcb_frame* f, const qcb_program* p, const qcb_noise_source* n) {
@@ -1054,6 +1077,8 @@ int run_program(qcb_frame* f, const qcb_program* p, const qcb_noise_source* n, b
   fill_common(a, f, p);
   a.seed = n->seed;
   a.col0 = n->shot_offset / 32;
+  // a fresh run rewrites the whole frame: an earlier expired wait no longer applies
+  if (fresh) QCB_CUDA(cudaMemsetAsync(f->err, 0, 4, st));
   if (n->mode == QCB_NOISE_PHILOX) return launch_walker(f, p, a, true, fresh, st);
 
   // Mask mode: bucket the caller's events per column, sorted by trial.
@@ -1339,6 +1364,7 @@ extern "C" int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* p, uint
 namespace qcb {
 void set_walker_tile(uint32_t t) { g_tile_override = t; }
 void set_walker_threads(uint32_t t) { g_threads_override = t; }
+void set_stage_withhold(uint32_t k) { g_stage_withhold = k; }
 int run_program_fresh(qcb_frame* f, const qcb_program* p, uint64_t seed, uint64_t shot_offset,
                       cudaStream_t st) {
   qcb_noise_source n{};

@@ -49,6 +49,7 @@ __global__ void philox_probe_kernel(uint4 ctr, uint2 key, uint32_t* out) {
 
 void set_walker_tile(uint32_t t);
 void set_walker_threads(uint32_t t);
+void set_stage_withhold(uint32_t k);
 void set_canon_cluster(uint32_t cs);
 void set_canon_threads(uint32_t n);
 void set_project_cluster(uint32_t cs);
@@ -110,6 +111,11 @@ int qcb_tune_set(const char* key, int64_t value) {
   if (k == "walker_tile") {
     if (value && (value < 8 || value > 256 || value % 2)) return fail(QCB_EARG, "walker_tile must be 0 (automatic) or even, 8..256");
     set_walker_tile((uint32_t)value);
+  } else if (k == "stage_withhold") {
+    // test knob: the plain walker never stages window `value` (1-based count
+    // of each CTA's window sequence), so its bounded wait expires and the run
+    // reports QCB_ETIMEOUT; 0 turns it off
+    set_stage_withhold((uint32_t)value);
   } else if (k == "walker_threads") {
     if (value && (value < 64 || value > 768 || value % 32)) return fail(QCB_EARG, "walker_threads must be 0 (768) or 64..768, a multiple of 32");
     set_walker_threads((uint32_t)value);

@@ -269,6 +269,10 @@ int qcb_server_next_done(qcb_server* s, double timeout_s, uint64_t* ticket, int3
  * (host memory; may be NULL to read *nbits only).                          */
 int qcb_server_result(qcb_server* s, uint64_t ticket, uint32_t* planes, uint32_t* nbits);
 int qcb_server_release(qcb_server* s, uint64_t ticket);
+/* Device bytes charged to the budget (records, chunk planes and resident
+ * programs), of which the resident programs, and their number.  No
+ * reference counterpart (the reference has no server).                     */
+int qcb_server_stats(qcb_server* s, uint64_t* used_bytes, uint64_t* program_bytes, uint32_t* n_programs);
 int qcb_server_destroy(qcb_server* s);
 
 /* The decoder hand-off (src/ecc/decoder_pipeline.jl:163-170).
@@ -322,7 +326,10 @@ int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t see
  * Test knob "stage_withhold" k > 0: the plain walker never stages window k of
  * each CTA's program windows, so its bounded wait expires and the run reports
  * QCB_ETIMEOUT at the next synchronising call (the kernel returns; nothing
- * faults); a fresh run or initZ! of the frame clears that status.          */
+ * faults); a fresh run or initZ! of the frame clears that status.  Test
+ * knob "server_hash_bits" b > 0: the serving program cache keeps only b low
+ * bits of its hash, so distinct circuits collide (the byte comparison on a
+ * hit keeps results right).                                                */
 int qcb_tune_set(const char* key, int64_t value);
 
 /* ------------------------------------------------------------ tableaux    */

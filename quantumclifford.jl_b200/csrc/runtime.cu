@@ -50,6 +50,7 @@ __global__ void philox_probe_kernel(uint4 ctr, uint2 key, uint32_t* out) {
 void set_walker_tile(uint32_t t);
 void set_walker_threads(uint32_t t);
 void set_stage_withhold(uint32_t k);
+void set_server_hash_bits(uint32_t b);
 void set_canon_cluster(uint32_t cs);
 void set_canon_threads(uint32_t n);
 void set_project_cluster(uint32_t cs);
@@ -116,6 +117,11 @@ int qcb_tune_set(const char* key, int64_t value) {
     // of each CTA's window sequence), so its bounded wait expires and the run
     // reports QCB_ETIMEOUT; 0 turns it off
     set_stage_withhold((uint32_t)value);
+  } else if (k == "server_hash_bits") {
+    // test knob: the serving program cache keeps only `value` low bits of
+    // its hash (0: all), so that distinct circuits collide
+    if (value > 64) return fail(QCB_EARG, "server_hash_bits must be 0..64");
+    set_server_hash_bits((uint32_t)value);
   } else if (k == "walker_threads") {
     if (value && (value < 64 || value > 768 || value % 32)) return fail(QCB_EARG, "walker_threads must be 0 (768) or 64..768, a multiple of 32");
     set_walker_threads((uint32_t)value);

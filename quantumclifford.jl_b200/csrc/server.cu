@@ -3,7 +3,9 @@
 //
 // A request is a circuit (op list), a shot count and a seed.  Its program is
 // compiled once per distinct op list and stays resident (a cache keyed by
-// the op bytes).  Admission is first come, first served against an HBM
+// the op bytes, compared in full on a hash hit; programs count against the
+// HBM budget, and unused ones are evicted least recently used first when it
+// runs short).  Admission is first come, first served against an HBM
 // budget and a number of slots: the head of the queue is admitted as soon as
 // a slot is free and its memory (the full record, plus one chunk's frame
 // planes) fits the budget.  Device memory comes from the stream-ordered
@@ -33,11 +35,20 @@ namespace qcb {
 
 enum ReqState : int32_t { RQ_QUEUED = 0, RQ_RUNNING = 1, RQ_DONE = 2, RQ_FAILED = 3 };
 
+// A resident compiled program: its op list (compared byte for byte on a hash
+// hit), its device bytes (charged to the budget), the requests holding it.
+struct CachedProgram {
+  std::vector<qcb_op> ops;
+  qcb_program* prog = nullptr;
+  uint64_t hash = 0, bytes = 0, refs = 0, last_use = 0;
+};
+
 struct Request {
   uint64_t id = 0;
   std::vector<qcb_op> ops;
   uint64_t shots = 0, seed = 0;
   qcb_program* prog = nullptr;  // cached, owned by the server
+  CachedProgram* cached = nullptr;
   uint64_t nbits = 0, ncols = 0, rec_pitch = 0;
   uint64_t bytes = 0;           // record + chunk planes charged to the budget
   uint32_t* record = nullptr;
@@ -69,7 +80,9 @@ struct qcb_server {
   std::map<uint64_t, std::unique_ptr<qcb::Request>> reqs;
   std::deque<uint64_t> queue;
   std::deque<uint64_t> completed;  // finished or failed, not yet reported by next_done
-  std::unordered_map<uint64_t, qcb_program*> programs;
+  std::unordered_multimap<uint64_t, std::unique_ptr<qcb::CachedProgram>> programs;
+  uint64_t program_bytes = 0;  // device bytes of the resident programs (inside `used`)
+  uint64_t use_clock = 0;
   int32_t* slot_status = nullptr;  // pinned: each slot's last walker status word
   uint64_t next_id = 1;
   std::mutex mu;
@@ -85,11 +98,73 @@ struct qcb_server {
 
 namespace qcb {
 
+// Test knob: keep only this many low bits of the program hash (0: all 64),
+// so that distinct circuits collide and the byte comparison decides.
+static uint32_t g_hash_bits = 0;
+void set_server_hash_bits(uint32_t b) { g_hash_bits = b; }
+
 static uint64_t ops_hash(const std::vector<qcb_op>& ops) {
   uint64_t h = 1469598103934665603ull;
   const uint8_t* p = (const uint8_t*)ops.data();
   for (size_t i = 0; i < ops.size() * sizeof(qcb_op); i++) { h ^= p[i]; h *= 1099511628211ull; }
-  return h ^ (ops.size() * 0x9E3779B97F4A7C15ull);
+  h ^= ops.size() * 0x9E3779B97F4A7C15ull;
+  return (g_hash_bits && g_hash_bits < 64) ? (h & ((1ull << g_hash_bits) - 1)) : h;
+}
+
+// Device bytes of a compiled program (what it holds resident).
+static uint64_t program_footprint(const qcb_program* p) {
+  return p->stream_slot.size() * 4 + p->classes.size() * sizeof(NoiseClass) + p->cdf.size() * 4 +
+         p->slot_qubit.size() * 4 + (uint64_t)p->qubit_slot_len * 4 + p->slot_swap.size() * 4 + 6 * 16;
+}
+
+// The resident program with exactly these ops, or null (lock held).
+static CachedProgram* find_program(qcb_server* s, uint64_t h, const std::vector<qcb_op>& ops) {
+  auto range = s->programs.equal_range(h);
+  for (auto it = range.first; it != range.second; ++it) {
+    CachedProgram* c = it->second.get();
+    if (c->ops.size() == ops.size() &&
+        (ops.empty() || std::memcmp(c->ops.data(), ops.data(), ops.size() * sizeof(qcb_op)) == 0))
+      return c;
+  }
+  return nullptr;
+}
+
+// Evict unused programs, least recently used first, until `need` more bytes
+// fit the budget (lock held).  Returns whether they fit.
+static bool evict_programs(qcb_server* s, uint64_t need) {
+  while (s->used + need > s->budget) {
+    auto victim = s->programs.end();
+    for (auto it = s->programs.begin(); it != s->programs.end(); ++it)
+      if (!it->second->refs && (victim == s->programs.end() || it->second->last_use < victim->second->last_use))
+        victim = it;
+    if (victim == s->programs.end()) return false;
+    s->used -= victim->second->bytes;
+    s->program_bytes -= victim->second->bytes;
+    qcb_program_destroy(victim->second->prog);  // no request holds it: no work of it is in flight
+    s->programs.erase(victim);
+  }
+  return true;
+}
+
+// Insert a freshly compiled program (lock held) unless an equal one arrived
+// meanwhile; returns the resident one.  Its bytes are charged to the budget,
+// evicting unused programs to make room where possible.
+static CachedProgram* insert_program(qcb_server* s, uint64_t h, std::vector<qcb_op>&& ops, qcb_program* p) {
+  if (CachedProgram* c = find_program(s, h, ops)) {
+    qcb_program_destroy(p);
+    return c;
+  }
+  auto c = std::make_unique<CachedProgram>();
+  c->ops = std::move(ops);
+  c->prog = p;
+  c->hash = h;
+  c->bytes = program_footprint(p);
+  evict_programs(s, c->bytes);
+  s->used += c->bytes;
+  s->program_bytes += c->bytes;
+  CachedProgram* raw = c.get();
+  s->programs.emplace(h, std::move(c));
+  return raw;
 }
 
 static uint64_t chunk_plane_bytes(uint32_t nq1, uint64_t chunk_cols) {
@@ -123,7 +198,21 @@ static void admit(qcb_server* s) {
       s->done_cv.notify_all();
       continue;
     }
-    if (s->used + r.bytes > s->budget) return;  // first come, first served: wait for memory
+    if (s->used + r.bytes > s->budget && !evict_programs(s, r.bytes)) {
+      bool running = false;
+      for (int64_t v : s->slot_req) running |= v >= 0;
+      if (running) return;  // first come, first served: wait for memory
+      // nothing runs and nothing more can be evicted: the resident programs
+      // of queued requests leave no room for this one
+      r.state = RQ_FAILED;
+      r.status = QCB_EBUDGET;
+      r.msg = "serving: the programs of queued requests leave too little of the budget for this request";
+      r.t_done = s->now();
+      s->queue.pop_front();
+      s->completed.push_back(r.id);
+      s->done_cv.notify_all();
+      continue;
+    }
     const uint32_t nq1 = std::max<uint32_t>(r.prog->nq, 1);
     cudaStream_t st = s->streams[slot];
     // the chunk frame: planes for one chunk, allocated and freed in stream
@@ -275,19 +364,23 @@ int qcb_server_submit(qcb_server* s, const qcb_op* ops, size_t n_ops, uint64_t s
   const uint64_t h = ops_hash(r->ops);
   {
     std::lock_guard<std::mutex> lk(s->mu);
-    auto it = s->programs.find(h);
-    if (it != s->programs.end()) r->prog = it->second;
+    if (CachedProgram* c = find_program(s, h, r->ops)) {
+      r->cached = c;
+      c->refs++;  // held from here: eviction skips it
+    }
   }
-  if (!r->prog) {
+  if (!r->cached) {
     qcb_program* p = nullptr;
     if (int st = qcb_program_compile(r->ops.data(), r->ops.size(), &p)) return st;
     std::lock_guard<std::mutex> lk(s->mu);
-    auto ins = s->programs.emplace(h, p);
-    if (!ins.second) qcb_program_destroy(p);
-    r->prog = ins.first->second;
+    std::vector<qcb_op> key(r->ops);
+    r->cached = insert_program(s, h, std::move(key), p);
+    r->cached->refs++;
   }
+  r->prog = r->cached->prog;
   {
     std::lock_guard<std::mutex> lk(s->mu);
+    r->cached->last_use = ++s->use_clock;
     r->id = s->next_id++;
     r->t_submit = t_arrival;
     *ticket = r->id;
@@ -305,12 +398,15 @@ int qcb_server_preload(qcb_server* s, const qcb_op* ops, size_t n_ops) {
   const uint64_t h = ops_hash(v);
   {
     std::lock_guard<std::mutex> lk(s->mu);
-    if (s->programs.count(h)) return QCB_OK;
+    if (CachedProgram* c = find_program(s, h, v)) {
+      c->last_use = ++s->use_clock;
+      return QCB_OK;
+    }
   }
   qcb_program* p = nullptr;
   if (int st = qcb_program_compile(v.data(), v.size(), &p)) return st;
   std::lock_guard<std::mutex> lk(s->mu);
-  if (!s->programs.emplace(h, p).second) qcb_program_destroy(p);
+  insert_program(s, h, std::move(v), p)->last_use = ++s->use_clock;
   return QCB_OK;
 }
 
@@ -390,11 +486,21 @@ int qcb_server_release(qcb_server* s, uint64_t ticket) {
       s->used -= r.bytes;
     }
     if (r.done) cudaEventDestroy(r.done);
+    if (r.cached && r.cached->refs) r.cached->refs--;
     for (auto c = s->completed.begin(); c != s->completed.end(); ++c)
       if (*c == ticket) { s->completed.erase(c); break; }  // released without being reported
     s->reqs.erase(it);
   }
   s->cv.notify_all();  // memory freed: the scheduler may admit
+  return QCB_OK;
+}
+
+int qcb_server_stats(qcb_server* s, uint64_t* used_bytes, uint64_t* program_bytes, uint32_t* n_programs) {
+  if (!s) return fail(QCB_EARG, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (used_bytes) *used_bytes = s->used;
+  if (program_bytes) *program_bytes = s->program_bytes;
+  if (n_programs) *n_programs = (uint32_t)s->programs.size();
   return QCB_OK;
 }
 
@@ -413,7 +519,7 @@ int qcb_server_destroy(qcb_server* s) {
     if (kv.second->done) cudaEventDestroy(kv.second->done);
   }
   if (s->slot_status) cudaFreeHost(s->slot_status);
-  for (auto& kv : s->programs) qcb_program_destroy(kv.second);
+  for (auto& kv : s->programs) qcb_program_destroy(kv.second->prog);
   for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
   delete s;
   return QCB_OK;

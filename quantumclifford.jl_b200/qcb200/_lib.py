@@ -183,6 +183,7 @@ def lib():
         "qcb_server_result": ([vp, u64, vp, P(u32)], ctypes.c_int),
         "qcb_server_release": ([vp, u64], ctypes.c_int),
         "qcb_server_destroy": ([vp], ctypes.c_int),
+        "qcb_server_stats": ([vp, P(u64), P(u64), P(u32)], ctypes.c_int),
         "qcb_tune_tile": ([vp, P(u32), P(ctypes.c_float), vp], ctypes.c_int),
         "qcb_frame_measurement_columns": ([vp, vp, sz, vp, vp, vp], ctypes.c_int),
         "qcb_frame_syndrome_rows": ([vp, vp, sz, vp, ctypes.c_int, vp], ctypes.c_int),

@@ -413,6 +413,14 @@ class Server:
     def release(self, ticket: int):
         check(lib().qcb_server_release(self.handle, int(ticket)))
 
+    def stats(self):
+        """(device bytes charged to the budget, of which resident programs,
+        number of resident programs)."""
+        used, prog = ctypes.c_uint64(), ctypes.c_uint64()
+        n = ctypes.c_uint32()
+        check(lib().qcb_server_stats(self.handle, ctypes.byref(used), ctypes.byref(prog), ctypes.byref(n)))
+        return used.value, prog.value, n.value
+
     def close(self):
         h = getattr(self, "handle", None)
         if h:

@@ -114,3 +114,45 @@ def test_next_done_reports_each_request_once(qcb):
     with pytest.raises(qcb.QCBError):
         srv.next_done(0.05)  # nothing left to report
     srv.close()
+
+
+def test_program_cache_compares_ops_on_hash_collisions(qcb):
+    """With the cache hash cut to one bit every circuit collides; the byte
+    comparison on a hit still gives each request its own program."""
+    rng = np.random.default_rng(7)
+    reqs = requests(rng, 6, dmax=7, smax=4)
+    qcb.check(qcb.lib().qcb_tune_set(b"server_hash_bits", 1))
+    try:
+        srv = qcb.Server(hbm_budget_bytes=4 << 30, slots=3, chunk_shots=4096)
+        tickets = [srv.submit(c, s, seed) for c, s, seed in reqs]
+        for t in tickets:
+            srv.wait(t)
+        got = [srv.result(t, s) for t, (c, s, seed) in zip(tickets, reqs)]
+        assert srv.stats()[2] == len({O.to_array(c).tobytes() for c, _, _ in reqs})
+        for t in tickets:
+            srv.release(t)
+        srv.close()
+    finally:
+        qcb.check(qcb.lib().qcb_tune_set(b"server_hash_bits", 0))
+    for (c, s, seed), m in zip(reqs, got):
+        assert np.array_equal(plain_record(qcb, c, s, seed), m)
+
+
+def test_programs_count_against_the_budget(qcb):
+    """Resident programs are charged to the HBM budget; preloading more than
+    fits evicts the least recently used unused ones, and requests still run."""
+    circs = [circuits.rotated_surface_code_memory(d, d, p) for d in (9, 11, 13) for p in (1e-3, 2e-3, 3e-3)]
+    srv = qcb.Server(hbm_budget_bytes=1 << 20, slots=2, chunk_shots=1024)
+    for c in circs:
+        srv.preload(c)
+        used, prog, n = srv.stats()
+        assert used <= 1 << 20 and prog == used and n >= 1
+    assert srv.stats()[2] < len(circs)  # some were evicted
+    t = srv.submit(circs[0], 2000, 5)
+    srv.wait(t)
+    assert np.array_equal(srv.result(t, 2000), plain_record(qcb, circs[0], 2000, 5))
+    used, prog, _ = srv.stats()
+    assert used > prog  # the record is charged while it is held
+    srv.release(t)
+    assert srv.stats()[0] == srv.stats()[1]
+    srv.close()

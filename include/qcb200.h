@@ -204,6 +204,10 @@ int qcb_frame_upload_xzs(qcb_frame* f, const uint64_t* xzs, void* stream);
 /* measurements(frame) (src/pauli_frames.jl:280): Bool matrix frames x nbits,
  * column-major (one byte per bit).                                         */
 int qcb_frame_download_measurements(const qcb_frame* f, uint8_t* bools, void* stream);
+/* The record from a reference frame's Bool matrix (frames x nbits,
+ * column-major, nonzero = true): PauliFrame(frame, measurements) moved to the
+ * device (the measurements field of src/pauli_frames.jl:9-12).             */
+int qcb_frame_upload_measurements(qcb_frame* f, const uint8_t* bools, void* stream);
 /* The record as shot-packed bit planes [nbits][ceil(frames/32)] uint32.    */
 int qcb_frame_download_record_planes(const qcb_frame* f, uint32_t* planes, void* stream);
 /* x/z planes [qubits+1][ceil(frames/32)] uint32 each (device layout).      */
@@ -364,7 +368,10 @@ int qcb_mul_left_pauli(qcb_tableau* r, const qcb_tableau* l, int phases,
  * at zero.  The first call on a device looks the array up
  * (cudaGetSymbolAddress, with that device current) and clears it, so make it
  * before any latency-critical use.  Calls that overlap in time on one device
- * (other streams or host threads) share the array and race: serialise them. */
+ * (other streams or host threads) share the array and race: serialise them.
+ * The array's address is kept per device for the life of the process: after
+ * a cudaDeviceReset (or a reset of the primary context) of a device, do not
+ * call this entry point on that device again in the same process.          */
 #define QCB_NOALLOC_MAX_PAIRS 4096
 int qcb_mul_left_pauli_batch_noalloc(uint64_t* r_xz, uint8_t* r_phases, const uint64_t* l_xz,
                                      const uint8_t* l_phases, uint32_t nqubits, uint32_t count,

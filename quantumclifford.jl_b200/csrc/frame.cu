@@ -841,6 +841,19 @@ __global__ void record_to_bools_kernel(const uint32_t* rec, uint64_t pitch, uint
   for (uint32_t k = 0; k < 4 && f + k < S; k++) dst[k] = (uint8_t)((word >> (sh + k)) & 1u);
 }
 
+// The inverse: record word (bit b, column c) from 32 Bools of the column-major
+// frames x nbits matrix (bytes other than 0 count as true; padding shots 0).
+__global__ void bools_to_record_kernel(const uint8_t* in, uint64_t S, uint32_t nbits, uint32_t* rec,
+                                       uint64_t pitch, uint64_t ncols) {
+  const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t b = blockIdx.y;
+  if (c >= ncols) return;
+  const uint8_t* src = in + (uint64_t)b * S + c * 32;
+  uint32_t w = 0;
+  for (uint32_t k = 0; k < 32 && c * 32 + k < S; k++) w |= (src[k] ? 1u : 0u) << k;
+  rec[(uint64_t)b * pitch + c] = w;
+}
+
 }  // namespace qcb
 
 using namespace qcb;
@@ -1193,6 +1206,22 @@ int qcb_frame_download_measurements(const qcb_frame* f, uint8_t* bools, void* st
   QCB_CUDA(cudaFreeAsync(d, S(stream)));
   QCB_CUDA(cudaStreamSynchronize(S(stream)));
   return frame_device_status(f);
+}
+
+int qcb_frame_upload_measurements(qcb_frame* f, const uint8_t* bools, void* stream) {
+  if (int st = check_frame(f)) return st;
+  const size_t bytes = (size_t)f->frames * f->nbits;
+  if (!bytes) return QCB_OK;
+  if (!bools) return fail(QCB_EARG, "null measurements");
+  uint8_t* d = nullptr;
+  QCB_CUDA(cudaMallocAsync(&d, bytes, S(stream)));
+  QCB_CUDA(cudaMemcpyAsync(d, bools, bytes, cudaMemcpyHostToDevice, S(stream)));
+  dim3 grid((unsigned)((f->ncols + 255) / 256), f->nbits);
+  bools_to_record_kernel<<<grid, 256, 0, S(stream)>>>(d, f->frames, f->nbits, f->record, f->pitch, f->ncols);
+  QCB_LAUNCHED();
+  QCB_CUDA(cudaFreeAsync(d, S(stream)));
+  QCB_CUDA(cudaStreamSynchronize(S(stream)));  // the caller's buffer may go after the call
+  return QCB_OK;
 }
 
 int qcb_frame_download_record_planes(const qcb_frame* f, uint32_t* planes, void* stream) {

@@ -144,6 +144,7 @@ def lib():
         "qcb_frame_download_xzs": ([vp, vp, vp], ctypes.c_int),
         "qcb_frame_upload_xzs": ([vp, vp, vp], ctypes.c_int),
         "qcb_frame_download_measurements": ([vp, vp, vp], ctypes.c_int),
+        "qcb_frame_upload_measurements": ([vp, vp, vp], ctypes.c_int),
         "qcb_frame_download_record_planes": ([vp, vp, vp], ctypes.c_int),
         "qcb_frame_download_planes": ([vp, vp, vp, vp], ctypes.c_int),
         "qcb_pftrajectories_host": ([vp, sz, u64, u64, u64, vp, vp], ctypes.c_int),

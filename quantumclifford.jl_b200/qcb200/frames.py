@@ -175,6 +175,15 @@ class PauliFrame:
             check(lib().qcb_frame_download_measurements(self.handle, ptr(out), None))
         return out.T.astype(bool)
 
+    def set_measurements(self, meas: np.ndarray):
+        """Load a Bool record matrix (frames x nbits) into the device record."""
+        m = np.asfortranarray(np.asarray(meas, dtype=bool)).astype(np.uint8, order="F")
+        if m.shape != (self.frames, self.nbits):
+            raise ValueError(f"measurements must have shape {(self.frames, self.nbits)}")
+        if m.size:
+            check(lib().qcb_frame_upload_measurements(self.handle, m.ctypes.data, None))
+        return self
+
     def record_planes(self) -> np.ndarray:
         out = np.empty((self.nbits, self.words), dtype=np.uint32)
         if out.size:

@@ -148,6 +148,13 @@ def ClassicalXOR(bits, store) -> list:
     return ops
 
 
+class _PauliMeasurementOps(list):
+    """The lowered ops of one PauliMeasurement; `nqubits` is the length of its
+    Pauli (affectedqubits(::PauliMeasurement) = 1:n, src/affectedqubits.jl:11)."""
+
+    nqubits = 0
+
+
 def PauliMeasurement(pauli, bit: int) -> list:
     """PauliMeasurement(pauli, bit) on a Pauli frame (src/pauli_frames.jl
     :118-134): through the hidden ancilla n+1 of an n-qubit Pauli, sXCZ / sCNOT
@@ -163,7 +170,8 @@ def PauliMeasurement(pauli, bit: int) -> list:
         letters = ["_XZY"[int(x) + 2 * int(z)] for x, z in zip(xs[0], zs[0])]
     n = len(letters)
     anc = n + 1
-    ops = []
+    ops = _PauliMeasurementOps()
+    ops.nqubits = n
     for q, ch in enumerate(letters, start=1):
         if ch == "X":
             ops.append(Op(OP["XCZ"], q, anc))
@@ -291,7 +299,11 @@ def _is_two_qubit(o: Op) -> bool:
 
 def NoisyGate(gate, noise) -> list:
     """NoisyGate(gate, noise) (src/noise.jl:178-190): the gate, then the
-    noise on its qubits (affectedqubits(gate))."""
+    noise on its qubits (affectedqubits(gate): both qubits of a two-qubit
+    gate; 1..n for a PauliMeasurement of an n-qubit Pauli,
+    src/affectedqubits.jl:5, 11)."""
+    if isinstance(gate, _PauliMeasurementOps):
+        return list(gate) + NoiseOp(noise, range(1, gate.nqubits + 1))
     ops = flatten([gate])
     if len(ops) != 1 or ops[0].is_noise() or ops[0].opcode in (OP["XOR"], OP["XOR_BITS"]):
         raise ArgumentError(QCB_EARG, "NoisyGate takes one single- or two-qubit gate or measurement")

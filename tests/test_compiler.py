@@ -156,3 +156,18 @@ def test_sample_masks_lowers_noise_op_all_over_the_frame():
     assert len(arr) == 8 and m.init_z.shape[0] == 7
     assert set(np.unique(m.events["op_index"])) <= set(range(1, 7))
     assert len(np.unique(m.events["op_index"])) == 6  # p = 0.3 on 256 shots: every qubit's site fires
+
+
+def test_noisy_gate_of_a_pauli_measurement():
+    """NoisyGate(PauliMeasurement(P, b), noise): the measurement's ops, then
+    the noise on qubits 1..n of its Pauli (affectedqubits(::PauliMeasurement)
+    = 1:length(pauli), src/affectedqubits.jl:5, 11), as the Julia lowering
+    does; bit for bit against the oracle through the compiler."""
+    noise = O.UnbiasedUncorrelatedNoise(0.05)
+    pm = O.PauliMeasurement("XIZY", 1)
+    a = O.to_array([O.NoisyGate(pm, noise)])
+    b = O.to_array(list(O.PauliMeasurement("XIZY", 1)) + O.PauliError([1, 2, 3, 4], 0.05))
+    assert np.array_equal(a, b)
+    circ = ([O.sHadamard(q) for q in range(1, 5)] + [O.NoisyGate(O.PauliMeasurement("XIZY", 1), noise)]
+            + [O.sMZ(q, q + 1) for q in range(1, 5)])
+    check_circuit(circ, 300, 4)

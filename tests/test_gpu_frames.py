@@ -361,3 +361,19 @@ def test_frame_copy_is_independent(qcb):
     assert np.array_equal(f.xzs(), before) and not np.array_equal(g.xzs(), before)
     with pytest.raises(qcb.DimensionMismatch):
         qcb.check(qcb.lib().qcb_frame_copy(qcb.PauliFrame(3000, qmax + 1, bmax).handle, f.handle, None))
+
+
+@pytest.mark.parametrize("frames,nbits", [(1, 1), (33, 5), (1000, 49), (4096, 3)])
+def test_measurements_upload_roundtrip(qcb, frames, nbits):
+    """A reference frame's Bool record onto the device and back, and the run
+    continues from it: bits the circuit does not write keep their values."""
+    rng = np.random.default_rng(frames)
+    m = rng.random((frames, nbits)) < 0.5
+    f = qcb.PauliFrame(frames, 3, nbits, init=False)
+    f.set_measurements(m)
+    assert np.array_equal(f.measurements(), m)
+    assert np.array_equal(f.record_planes(), qcb.pack_record(m))
+    f.apply([O.sMZ(1, 1)])  # x starts at zero: bit 1 becomes false, the rest stay
+    m2 = m.copy()
+    m2[:, 0] = False
+    assert np.array_equal(f.measurements(), m2)

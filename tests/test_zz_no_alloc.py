@@ -64,6 +64,36 @@ def test_noalloc_batch_matches_mul_left_pauli_two_calls(qcb, n, count, phases):
         assert np.array_equal(gp, ep if phases else rp)
 
 
+def test_noalloc_misaligned_words_and_a_side_stream(qcb):
+    """Word arrays that start 8 bytes past a 16-byte boundary (even word
+    count: the 64-bit load path) and a call on a non-default stream, two
+    calls in a row, against the handle-based entry point."""
+    import torch
+
+    n, count = 640, 33  # 10 words per half: even
+    rng = np.random.default_rng(77)
+    side = torch.cuda.Stream()
+    for _ in range(2):
+        rx, rp = random_pairs(rng, count, n)
+        lx, lp = random_pairs(rng, count, n)
+        ex, ep = expected(rx, rp, lx, lp, n, True)
+        # one spare word in front: the Pauli words start at an 8-byte offset
+        d_rx = torch.zeros(rx.size + 1, dtype=torch.int64, device="cuda")
+        d_lx = torch.zeros(lx.size + 1, dtype=torch.int64, device="cuda")
+        d_rx[1:] = torch.from_numpy(rx.reshape(-1).view(np.int64)).cuda()
+        d_lx[1:] = torch.from_numpy(lx.reshape(-1).view(np.int64)).cuda()
+        d_rp, d_lp = torch.from_numpy(rp).cuda(), torch.from_numpy(lp).cuda()
+        assert (d_rx.data_ptr() + 8) % 16 == 8
+        torch.cuda.synchronize()
+        qcb.check(qcb.lib().qcb_mul_left_pauli_batch_noalloc(
+            ctypes.c_void_p(d_rx.data_ptr() + 8), ctypes.c_void_p(d_rp.data_ptr()), ctypes.c_void_p(d_lx.data_ptr() + 8),
+            ctypes.c_void_p(d_lp.data_ptr()), n, count, 1, ctypes.c_void_p(side.cuda_stream)))
+        side.synchronize()
+        gx = d_rx[1:].cpu().numpy().view(np.uint64).reshape(rx.shape)
+        assert np.array_equal(gx, ex) and np.array_equal(d_rp.cpu().numpy(), ep)
+        assert int(d_rx[0].item()) == 0  # the spare word is untouched
+
+
 def test_noalloc_rejects_batches_above_its_scratch(qcb):
     with pytest.raises(qcb.ArgumentError, match="exceeds the no-alloc scratch"):
         qcb.check(qcb.lib().qcb_mul_left_pauli_batch_noalloc(None, None, None, None, 64, 4097, 1, None))

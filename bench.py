@@ -764,7 +764,9 @@ def main():
     torch.cuda.synchronize()
     launches = L.qcb_launch_count() - n0
     ms = ev0.elapsed_time(ev1) / args.steps
-    # the walker is the only kernel of a step: its event time is the launch duration
+    # a step is two kernels on one stream, the noise pre-sampler and the
+    # walker (plus a memset of the bucket counts); the roofline is taken over
+    # the step's event time (the launch list in profiles/ gives the shares)
     kernel_ms = ms
 
     # end to end through the public host API: the op list from host memory in
@@ -859,6 +861,7 @@ def main():
                                        "launch of this workload (profiles/walker_d11_traffic.json), not measured "
                                        "in this run",
                      "algorithmic_bytes_per_launch": model_bytes,
+                     "timed": "the whole step (presample_kernel + walker_kernel), CUDA events on the launching stream",
                      "basis": "model plane bytes of an op-per-launch schedule (5,175 B/shot); the walker keeps the "
                               "frame on chip, so its compulsory DRAM bytes are the record + final frame",
                      "compulsory_dram_bytes_per_launch": hbm_bytes,

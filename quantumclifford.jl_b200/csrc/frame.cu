@@ -64,6 +64,16 @@ struct WalkArgs {
   // test knob: window index (of each CTA's sequence) that is never staged, so
   // the walker's bounded wait runs out (0: none)
   uint64_t withhold;
+  // pre-sampled noise (null: the walk draws every (site, group) itself):
+  // bucket (group g, flush part j) holds pre_cnt[g * pre_nparts + j] events
+  // at pre_buf + g * pre_capg + pre_capoff[j] (at most pre_capoff[j + 1] -
+  // pre_capoff[j]; a fuller bucket is drawn in the walk); g counts groups
+  // from the run's first column
+  const uint32_t* pre_buf;
+  const uint32_t* pre_cnt;
+  const uint32_t* pre_capoff;
+  uint32_t pre_nparts;
+  uint32_t pre_capg;
 };
 
 // Bit-sliced single-qubit gate (src/symbolic_cliffords.jl:105-118); frames
@@ -261,32 +271,16 @@ constexpr uint32_t NOISE_REDRAWS = 64;
 //          independent: every shot gets an event independently with
 //          probability p_eff, as the reference's per-frame draws.
 //  dense:  word j is the per-shot draw of shot j.
-template <bool SMEM>
-__device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<SMEM>& F, const uint4& e,
-                                                  uint64_t G, int32_t lc0, uint64_t c0) {
-  const uint32_t site = e.x, kind = e.y & 0xFFu;
-  const NoiseClass c = a.classes[e.y >> 8];
-  const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
-  const uint32_t glo = (uint32_t)G;
-  constexpr uint32_t PMASK = NOISE_GROUP - 1;
-  uint32_t o[4];
-  if (c.dense) {
-    for (uint32_t blk = 0; blk < NOISE_GROUP / 4; blk++) {
-      philox4x32_10(site, glo, blk, TAG_NOISE, k0, k1, o);
-#pragma unroll
-      for (uint32_t j = 0; j < 4; j++) {
-        const uint32_t code = dense_code(kind, c, o[j]);
-        if (code) apply_code<SMEM>(F, e, code, lc0, blk * 4 + j, c0, a.ncols);
-      }
-    }
-    return;
-  }
-  if (!c.cdf_len) return;
+// Sparse classes (see sample_site_group): the event count k of (site, group)
+// from Philox block 0, whose words 1..3 `o` keeps for the first events.
+__device__ __forceinline__ uint32_t sparse_count(const NoiseClass& c, const uint32_t* cdf, uint32_t site,
+                                                 uint32_t glo, uint32_t k0, uint32_t k1, uint32_t o[4]) {
+  if (!c.cdf_len) return 0;
   philox4x32_10(site, glo, 0u, TAG_NOISE, k0, k1, o);
   // k = number of table entries <= word 0 (the table is non-decreasing, so
   // this is the inverse CDF), four entries per 16-byte read: one read for
   // counts below 4
-  const uint4* tb = (const uint4*)(a.cdf + c.cdf_off);
+  const uint4* tb = (const uint4*)(cdf + c.cdf_off);
   uint32_t k = 0;
   for (uint32_t b = 0; b < c.cdf_len; b += 4) {
     const uint4 t = __ldg(tb + (b >> 2));
@@ -296,19 +290,29 @@ __device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<
     k += m;
     if (m < 4) break;
   }
-  if (k == 0) return;
+  return k;
+}
+
+// The k events of (site, group) as emit(position, code): event e from word
+// 1 + e, a position already taken redrawn from the next unused word.  Up to
+// KREG events are kept in registers, more in a bitmap; both are the same
+// sequential procedure, so KREG changes the cost and not the events.
+template <uint32_t KREG = NOISE_KREG, class Emit>
+__device__ __forceinline__ void sparse_emit(const NoiseClass& c, uint32_t kind, uint32_t site, uint32_t glo,
+                                            uint32_t k0, uint32_t k1, uint32_t k, uint32_t o[4], Emit emit) {
+  constexpr uint32_t PMASK = NOISE_GROUP - 1;
   uint32_t next = k + 1;  // next unused word
-  if (k <= NOISE_KREG) {
-    uint32_t w[NOISE_KREG];
+  if (k <= KREG) {
+    uint32_t w[KREG];
 #pragma unroll
-    for (uint32_t ev = 0; ev < NOISE_KREG; ev++) {
+    for (uint32_t ev = 0; ev < KREG; ev++) {
       if (ev < k) {
         if (((ev + 1) & 3) == 0) philox4x32_10(site, glo, (ev + 1) >> 2, TAG_NOISE, k0, k1, o);
         w[ev] = o[(ev + 1) & 3];
       }
     }
 #pragma unroll
-    for (uint32_t ev = 1; ev < NOISE_KREG; ev++) {
+    for (uint32_t ev = 1; ev < KREG; ev++) {
       if (ev < k) {
         for (uint32_t r = 0; r < NOISE_REDRAWS; r++) {
           bool dup = false;
@@ -320,8 +324,8 @@ __device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<
       }
     }
 #pragma unroll
-    for (uint32_t ev = 0; ev < NOISE_KREG; ev++)
-      if (ev < k) apply_code<SMEM>(F, e, sparse_code(kind, c, w[ev] >> 10), lc0, w[ev] & PMASK, c0, a.ncols);
+    for (uint32_t ev = 0; ev < KREG; ev++)
+      if (ev < k) emit(w[ev] & PMASK, sparse_code(kind, c, w[ev] >> 10));
     return;
   }
   uint32_t bm[NOISE_GROUP / 32];  // positions taken so far
@@ -336,7 +340,98 @@ __device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<
     for (uint32_t r = 0; r < NOISE_REDRAWS && ((bm[(wv & PMASK) >> 5] >> (wv & 31)) & 1u); r++)
       wv = noise_word(site, glo, next++, k0, k1);
     bm[(wv & PMASK) >> 5] |= 1u << (wv & 31);
-    apply_code<SMEM>(F, e, sparse_code(kind, c, wv >> 10), lc0, wv & PMASK, c0, a.ncols);
+    emit(wv & PMASK, sparse_code(kind, c, wv >> 10));
+  }
+}
+
+template <bool SMEM>
+__device__ __forceinline__ void sample_site_group(const WalkArgs& a, const Tile<SMEM>& F, const uint4& e,
+                                                  uint64_t G, int32_t lc0, uint64_t c0) {
+  const uint32_t site = e.x, kind = e.y & 0xFFu;
+  const NoiseClass c = a.classes[e.y >> 8];
+  const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
+  const uint32_t glo = (uint32_t)G;
+  uint32_t o[4];
+  if (c.dense) {
+    for (uint32_t blk = 0; blk < NOISE_GROUP / 4; blk++) {
+      philox4x32_10(site, glo, blk, TAG_NOISE, k0, k1, o);
+#pragma unroll
+      for (uint32_t j = 0; j < 4; j++) {
+        const uint32_t code = dense_code(kind, c, o[j]);
+        if (code) apply_code<SMEM>(F, e, code, lc0, blk * 4 + j, c0, a.ncols);
+      }
+    }
+    return;
+  }
+  const uint32_t k = sparse_count(c, a.cdf, site, glo, k0, k1, o);
+  if (k == 0) return;
+  sparse_emit(c, kind, site, glo, k0, k1, k, o,
+              [&](uint32_t pos, uint32_t code) { apply_code<SMEM>(F, e, code, lc0, pos, c0, a.ncols); });
+}
+
+// ---------------------------------------------------------------- pre-sampling
+// Every sparse (site, group) of a Philox run drawn before the walk, in a
+// grid of its own (no CTA barriers, full occupancy): thread (entry, group)
+// draws the site's events on the group exactly as sample_site_group would and
+// appends them to the bucket (group, flush part) as words
+// (entry index << 16 | code << 10 | position), the slot from an atomic on the
+// bucket's count.  Event order inside a bucket does not matter (flips are
+// XORs).  A bucket whose count ends above its capacity keeps only part of its
+// events; the walk then draws that bucket itself.
+struct PresampleArgs {
+  const uint4* ent;         // (site, kind | class << 8, part j, entry index i)
+  uint32_t nent;
+  uint32_t nparts;
+  uint64_t g0;              // global group index of the run's first group
+  uint64_t ngroups;
+  const NoiseClass* classes;
+  const uint32_t* cdf;
+  uint64_t seed;
+  uint32_t* cnt;            // [ngroups][nparts], zero before the launch
+  uint32_t* buf;            // [ngroups][capg]
+  const uint32_t* capoff;   // [nparts + 1]
+  uint32_t capg;
+  uint32_t force_overflow;  // test knob: every non-empty bucket reports more than its capacity
+};
+
+__global__ void __launch_bounds__(256) presample_kernel(const PresampleArgs p) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
+  const bool valid = e < p.nent;
+  const uint4 pe = valid ? p.ent[e] : make_uint4(0u, 0u, 0xFFFFFFFFu, 0u);
+  NoiseClass c{};
+  if (valid) c = p.classes[pe.y >> 8];
+  const uint32_t kind = pe.y & 0xFFu, j = pe.z;
+  const uint32_t k0 = (uint32_t)p.seed, k1 = (uint32_t)(p.seed >> 32);
+  const uint32_t off = valid ? p.capoff[j] : 0u, cap = valid ? p.capoff[j + 1] - off : 0u;
+  // The entries are sorted by part, so the lanes of one part form a run
+  // [first, last]: its events take one atomic on the bucket count (by the
+  // run's last lane) and consecutive slots.
+  const uint32_t peers = __match_any_sync(0xFFFFFFFFu, j);
+  const uint32_t first = __ffs(peers) - 1, last = 31 - __clz(peers);
+  const uint32_t tag = pe.w << 16;
+  for (uint64_t g = blockIdx.y; g < p.ngroups; g += gridDim.y) {
+    const uint32_t glo = (uint32_t)(p.g0 + g);
+    uint32_t o[4];
+    const uint32_t k = valid ? sparse_count(c, p.cdf, pe.x, glo, k0, k1, o) : 0u;
+    uint32_t inc = k;  // inclusive prefix of k over the run
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+      if (lane >= first + d) inc += v;
+    }
+    uint32_t base = 0;
+    if (lane == last && inc) base = atomicAdd(p.cnt + g * p.nparts + j, inc + (p.force_overflow ? cap + 1 : 0u));
+    base = __shfl_sync(0xFFFFFFFFu, base, last);
+    if (k == 0) continue;
+    uint32_t* bk = p.buf + g * p.capg + off;
+    uint32_t t = base + inc - k;
+    auto put = [&](uint32_t pos, uint32_t code) {
+      if (t < cap) bk[t] = tag | (code << 10) | pos;
+      t++;
+    };
+    // most counts are below 4 (block 0's words 1..3): a short path for them
+    if (k <= 3) sparse_emit<3>(c, kind, pe.x, glo, k0, k1, k, o, put);
+    else sparse_emit<NOISE_KREG>(c, kind, pe.x, glo, k0, k1, k, o, put);
   }
 }
 
@@ -354,7 +449,7 @@ __device__ __forceinline__ uint2 xor2(uint2 a, uint2 b) { return make_uint2(a.x 
 // thread 0 calls issue(kwin + 2) for the window two ahead.  Returns false
 // when a staging wait gave up (the job's status word then holds
 // QCB_ETIMEOUT).
-template <bool SMEM, bool PHILOX, class Issue>
+template <bool SMEM, bool PHILOX, bool PRE, class Issue>
 __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint32_t* win0, uint32_t* win1,
                                           uint64_t* bars, uint64_t& kwin, Issue& issue, uint64_t tile) {
   const uint32_t tid = threadIdx.x, T = a.tile, TP = T / 2, R = blockDim.x / TP;
@@ -405,6 +500,25 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
     ep[1] = a.ev_off[cg + 1];
     ep[2] = two ? a.ev_off[cg + 2] : ep[1];
   }
+
+  // ---- pre-sampled noise: thread (pgl, pl) takes events pl, pl + pS, ... of
+  // the buckets of its group G0 + pgl of the tile; the count and the first
+  // two events of the next flush part are loaded one part ahead (issued at a
+  // flush, they arrive while the following records run)
+  const uint64_t pG0 = (a.col0 + c0) / 32;
+  const uint32_t png = (uint32_t)((a.col0 + min(c0 + T, a.ncols) - 1) / 32 - pG0 + 1);
+  const uint32_t pS = blockDim.x / png, pgl = tid / pS, pl = tid - pgl * pS;
+  const bool pre = PRE && PHILOX && a.pre_buf != nullptr && pgl < png;
+  const uint32_t* pbase = pre ? a.pre_buf + (pG0 + pgl - a.col0 / 32) * a.pre_capg : nullptr;
+  const uint32_t* pcnt = pre ? a.pre_cnt + (pG0 + pgl - a.col0 / 32) * a.pre_nparts : nullptr;
+  uint32_t pf_tot = 0, pf_e0 = 0, pf_e1 = 0;
+  auto prefetch = [&](uint32_t jn, uint32_t offn) {
+    if (!pre || jn >= a.pre_nparts) return;
+    pf_tot = __ldg(pcnt + jn);
+    pf_e0 = offn + pl < a.pre_capg ? __ldg(pbase + offn + pl) : 0u;
+    pf_e1 = offn + pl + pS < a.pre_capg ? __ldg(pbase + offn + pl + pS) : 0u;
+  };
+  prefetch(0, 0);
 
   // ---- the program, window by window
   const uint32_t* wp = nullptr;
@@ -574,10 +688,39 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
             // t / ng as a multiply-high for ng >= 2: ng <= 10 and t < 2^13 (a
             // record part fits one window), far inside t * (mg * ng - 2^32) < 2^32
             const uint32_t mg = ng > 1 ? 0xFFFFFFFFu / ng + 1u : 0u;
-            for (uint32_t t = tid; t < ntask; t += blockDim.x) {
-              const uint32_t i = ng > 1 ? __umulhi(t, mg) : t, gl = t - i * ng;
-              const int32_t lc0 = (int32_t)((int64_t)((G0 + gl) * 32) - (int64_t)gc0);
-              sample_site_group<SMEM>(a, F, en[i], G0 + gl, lc0, c0);
+            if (PRE && a.pre_buf) {
+              // pre-sampled: bucket (group G0 + pgl, part j), the count and
+              // first events loaded at the previous flush part
+              const uint32_t j = h.z, off = h.w, cap = h.y >> 8;
+              const uint32_t total = pf_tot, ev0 = pf_e0, ev1 = pf_e1;
+              prefetch(j + 1, off + cap);
+              if (pre && cap) {
+                const uint32_t* bk = pbase + off;
+                const int32_t lc0 = (int32_t)((int64_t)((pG0 + pgl) * 32) - (int64_t)gc0);
+                if (total <= cap) {
+                  for (uint32_t m = pl; m < total; m += pS) {
+                    const uint32_t ev = m == pl ? ev0 : m == pl + pS ? ev1 : __ldg(bk + m);
+                    apply_code<SMEM>(F, en[ev >> 16], (ev >> 10) & 15u, lc0, ev & (NOISE_GROUP - 1), c0, a.ncols);
+                  }
+                } else {  // the bucket overflowed: draw its sparse sites here
+                  for (uint32_t i = pl; i < cnt; i += pS)
+                    if (!a.classes[en[i].y >> 8].dense) sample_site_group<SMEM>(a, F, en[i], pG0 + pgl, lc0, c0);
+                }
+              }
+              if (h.y & FLAG_DENSE_SITES) {  // dense sites are drawn in the walk
+                for (uint32_t t = tid; t < ntask; t += blockDim.x) {
+                  const uint32_t i = ng > 1 ? __umulhi(t, mg) : t, gt = t - i * ng;
+                  if (!a.classes[en[i].y >> 8].dense) continue;
+                  const int32_t lc0 = (int32_t)((int64_t)((G0 + gt) * 32) - (int64_t)gc0);
+                  sample_site_group<SMEM>(a, F, en[i], G0 + gt, lc0, c0);
+                }
+              }
+            } else {
+              for (uint32_t t = tid; t < ntask; t += blockDim.x) {
+                const uint32_t i = ng > 1 ? __umulhi(t, mg) : t, gl = t - i * ng;
+                const int32_t lc0 = (int32_t)((int64_t)((G0 + gl) * 32) - (int64_t)gc0);
+                sample_site_group<SMEM>(a, F, en[i], G0 + gl, lc0, c0);
+              }
             }
           }
         } else if (rr == 0 && act) {
@@ -643,9 +786,15 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
   return true;
 }
 
+// Threads of a plain walker CTA at most (its launch bound): 640 leaves 96
+// registers a thread, where the pre-sampled flush and its loads one part
+// ahead fit without spilling (768 left 80 and spilled: d=11 0.69 against
+// 0.59 ms per step).
+constexpr uint32_t WALKER_THREADS = 640;
+
 // The plain launch: one program on one frame, CTA b walking tiles b, b + grid, ...
 template <bool SMEM, bool PHILOX>
-__global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
+__global__ void __launch_bounds__(WALKER_THREADS, 1) walker_kernel(const WalkArgs a) {
   extern __shared__ __align__(128) uint32_t sm[];
   const uint32_t tid = threadIdx.x, T = a.tile;
   // layout: [frame tile | pmap] [window 0] [window 1] [2 mbarriers]
@@ -674,7 +823,7 @@ __global__ void __launch_bounds__(768, 1) walker_kernel(const WalkArgs a) {
   uint64_t kwin = 0;
   bool failed = false;
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    if (!walk_tile<SMEM, PHILOX>(a, sm, win0, win1, bars, kwin, issue, tile)) {
+    if (!walk_tile<SMEM, PHILOX, PHILOX>(a, sm, win0, win1, bars, kwin, issue, tile)) {
       failed = true;
       break;
     }
@@ -762,7 +911,7 @@ __global__ void __launch_bounds__(768, 1) batch_walker_kernel(const BatchArgs b)
     for (uint32_t w = tid; w < sizeof(WalkArgs) / 8; w += blockDim.x)
       ((uint64_t*)&ja)[w] = ((const uint64_t*)(b.jobs + bi.job))[w];
     __syncthreads();
-    if (!walk_tile<true, true>(ja, sm, win0, win1, bars, kwin, issue, bi.tile)) {
+    if (!walk_tile<true, true, false>(ja, sm, win0, win1, bars, kwin, issue, bi.tile)) {
       failed = true;
       break;
     }
@@ -829,16 +978,22 @@ __global__ void xzs_to_planes_kernel(const uint64_t* xzs, uint64_t S, uint32_t W
 }
 
 // record planes -> Bool matrix (frames x nbits, column-major).
-__global__ void record_to_bools_kernel(const uint32_t* rec, uint64_t pitch, uint64_t S,
-                                       uint32_t nbits, uint8_t* out) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;  // 4 frames per thread
-  const uint32_t b = blockIdx.y;
-  const uint64_t f = i * 4;
-  if (f >= S) return;
-  const uint32_t word = __ldg(rec + (uint64_t)b * pitch + (f >> 5));
-  const uint32_t sh = (uint32_t)(f & 31);
-  uint8_t* dst = out + (uint64_t)b * S + f;
-  for (uint32_t k = 0; k < 4 && f + k < S; k++) dst[k] = (uint8_t)((word >> (sh + k)) & 1u);
+// Outputs [o0, o0 + n) of the column-major frames x nbits Bool matrix
+// (output o = bit (o / S), frame (o % S)) into out[0, n): four consecutive
+// outputs per thread, one 32-bit store when all four are in range.
+__global__ void record_to_bools_kernel(const uint32_t* rec, uint64_t pitch, uint64_t S, uint64_t o0,
+                                       uint64_t n, uint8_t* out) {
+  const uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (t >= n) return;
+  uint64_t b = (o0 + t) / S, fr = (o0 + t) - b * S;
+  uint32_t v = 0;
+  const uint32_t m = (uint32_t)(n - t < 4 ? n - t : 4);
+  for (uint32_t k = 0; k < m; k++) {
+    v |= ((__ldg(rec + b * pitch + (fr >> 5)) >> (fr & 31)) & 1u) << (8 * k);
+    if (++fr == S) { fr = 0; b++; }
+  }
+  if (m == 4) *(uint32_t*)(out + t) = v;
+  else for (uint32_t k = 0; k < m; k++) out[t + k] = (uint8_t)(v >> (8 * k));
 }
 
 // The inverse: record word (bit b, column c) from 32 Bools of the column-major
@@ -857,6 +1012,14 @@ __global__ void bools_to_record_kernel(const uint8_t* in, uint64_t S, uint32_t n
 }  // namespace qcb
 
 using namespace qcb;
+
+// Staging of qcb_frame_download_measurements on one device.
+constexpr uint64_t MEAS_STAGE = 32ull << 20;
+struct MeasStage {
+  uint8_t* buf[2] = {nullptr, nullptr};
+  cudaStream_t copy = nullptr;
+  cudaEvent_t expanded[2] = {}, copied[2] = {};
+};
 
 static int check_frame(const qcb_frame* f) {
   if (!f) return fail(QCB_EARG, "null frame");
@@ -884,6 +1047,7 @@ int qcb_frame_create(uint64_t frames, uint32_t qubits, uint32_t nbits, qcb_frame
   f->nbits = nbits;
   f->ncols = (frames + 31) / 32;
   f->pitch = std::max<uint64_t>(32, (f->ncols + 31) / 32 * 32);
+  f->pre_own = true;
   size_t pbytes = (size_t)2 * (f->nq1 + 1) * f->pitch * 4;
   size_t rbytes = (size_t)std::max<uint32_t>(nbits, 1) * f->pitch * 4;
   cudaError_t e = cudaMalloc(&f->planes, pbytes);
@@ -906,6 +1070,7 @@ int qcb_frame_destroy(qcb_frame* f) {
   cudaFree(f->planes);
   cudaFree(f->record);
   cudaFree(f->err);
+  cudaFree(f->pre);
   delete f;
   return QCB_OK;
 }
@@ -979,7 +1144,11 @@ struct WalkConfig {
 
 static uint32_t g_tile_override = 0;
 static uint32_t g_stage_withhold = 0;     // test knob, see WalkArgs::withhold
-static uint32_t g_threads_override = 0;  // threads per CTA (0: 768)
+static uint32_t g_presample = 0;          // 0: automatic, 1: never, 2: every bucket overflows (test)
+// Largest pre-sampler scratch (event buckets + counts) per frame; a run that
+// needs more draws its noise in the walk.
+constexpr uint64_t PRESAMPLE_MAX_BYTES = 512ull << 20;
+static uint32_t g_threads_override = 0;  // threads per CTA (0: WALKER_THREADS)
 
 // Tile width (even: threads own column pairs) for ncols columns with tiles of
 // at most tmax columns: the fewest waves of one CTA per SM, then the narrowest
@@ -1007,11 +1176,11 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   } else if (budget / per_col >= 16) {
     T = balanced_tile(f->ncols, (uint32_t)std::min<size_t>(256, budget / per_col));
   }
-  const uint32_t threads = g_threads_override ? g_threads_override : 768u;
+  const uint32_t threads = g_threads_override ? g_threads_override : WALKER_THREADS;
   if (T) {
     wc.smem = true;
     wc.T = T;
-    wc.nth = (threads / (T / 2)) * (T / 2);  // column pairs; the kernel's launch bound is 768
+    wc.nth = (threads / (T / 2)) * (T / 2);  // column pairs; the kernel's launch bound is WALKER_THREADS
     wc.smem_bytes = per_col * T + stage;
   } else {
     wc.smem = false;
@@ -1024,9 +1193,71 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   return wc;
 }
 
+// Scratch bytes the pre-sampler needs for the frame (0: not used).
+static uint64_t presample_bytes(const qcb_frame* f, const qcb_program* p) {
+  if (g_presample == 1 || p->pre_ent.empty() || p->pmax <= 0.0) return 0;
+  const uint64_t ngroups = (f->ncols + 31) / 32;
+  const uint64_t need = (ngroups * p->pre_capoff.back() + ngroups * p->pre_nparts) * 4;
+  return need <= PRESAMPLE_MAX_BYTES ? need : 0;
+}
+
+// Grow the frame's pre-sampler scratch (frames made by qcb_frame_create only;
+// the first run of a frame allocates, later runs reuse it).
+static int ensure_presample_scratch(qcb_frame* f, const qcb_program* p) {
+  const uint64_t need = presample_bytes(f, p);
+  if (!need || f->pre_bytes >= need || !f->pre_own) return QCB_OK;
+  if (f->pre) QCB_CUDA(cudaFree(f->pre));
+  f->pre = nullptr;
+  f->pre_bytes = 0;
+  QCB_CUDA(cudaMalloc(&f->pre, need));
+  f->pre_bytes = need;
+  return QCB_OK;
+}
+
+// Pre-sample the run's sparse noise into the frame's scratch (counts zeroed,
+// then one presample_kernel launch) and point the walk at it; nothing when
+// the scratch is absent or too small (the walk then draws the noise).
+static int launch_presample(qcb_frame* f, const qcb_program* p, WalkArgs& a, cudaStream_t st) {
+  const uint64_t need = presample_bytes(f, p);
+  if (!need) return QCB_OK;
+  if (int s = ensure_presample_scratch(f, p)) return s;
+  if (f->pre_bytes < need) return QCB_OK;
+  const uint64_t ngroups = (f->ncols + 31) / 32;
+  const uint64_t cnt_words = ngroups * p->pre_nparts;
+  PresampleArgs q{};
+  q.ent = p->d_pre_ent;
+  q.nent = (uint32_t)p->pre_ent.size();
+  q.nparts = p->pre_nparts;
+  q.g0 = a.col0 / 32;
+  q.ngroups = ngroups;
+  q.classes = p->d_classes;
+  q.cdf = p->d_cdf;
+  q.seed = a.seed;
+  q.cnt = f->pre;
+  q.buf = f->pre + cnt_words;
+  q.capoff = p->d_pre_capoff;
+  q.capg = p->pre_capoff.back();
+  q.force_overflow = g_presample == 2 ? 1u : 0u;
+  QCB_CUDA(cudaMemsetAsync(q.cnt, 0, cnt_words * 4, st));
+  // each thread walks groups g, g + grid.y, ...: about 8 CTAs per SM in all
+  const uint32_t gx = (q.nent + 255) / 256;
+  const uint64_t gy = std::max<uint64_t>(1, ((uint64_t)device_sm_count() * 8 + gx - 1) / gx);
+  const dim3 grid(gx, (uint32_t)std::min<uint64_t>(std::min<uint64_t>(ngroups, gy), 65535));
+  presample_kernel<<<grid, 256, 0, st>>>(q);
+  QCB_LAUNCHED();
+  a.pre_buf = q.buf;
+  a.pre_cnt = q.cnt;
+  a.pre_capoff = p->d_pre_capoff;
+  a.pre_nparts = p->pre_nparts;
+  a.pre_capg = q.capg;
+  return QCB_OK;
+}
+
 int launch_walker(qcb_frame* f, const qcb_program* p, WalkArgs& a, bool philox, bool fresh,
                   cudaStream_t st) {
   WalkConfig wc = walk_config(p, f);
+  if (philox && f->ncols)
+    if (int s = launch_presample(f, p, a, st)) return s;
   a.fresh = fresh ? 1 : 0;
   a.tile = wc.T;
   if (!f->ncols) return QCB_OK;
@@ -1195,16 +1426,44 @@ int qcb_frame_upload_xzs(qcb_frame* f, const uint64_t* xzs, void* stream) {
 
 int qcb_frame_download_measurements(const qcb_frame* f, uint8_t* bools, void* stream) {
   if (int st = check_frame(f)) return st;
-  const size_t bytes = (size_t)f->frames * f->nbits;
+  const uint64_t bytes = (uint64_t)f->frames * f->nbits;
   if (!bytes) return QCB_OK;
-  uint8_t* d = nullptr;
-  QCB_CUDA(cudaMallocAsync(&d, bytes, S(stream)));
-  dim3 grid((unsigned)(((f->frames + 3) / 4 + 255) / 256), f->nbits);
-  record_to_bools_kernel<<<grid, 256, 0, S(stream)>>>(f->record, f->pitch, f->frames, f->nbits, d);
-  QCB_LAUNCHED();
-  QCB_CUDA(cudaMemcpyAsync(bools, d, bytes, cudaMemcpyDeviceToHost, S(stream)));
-  QCB_CUDA(cudaFreeAsync(d, S(stream)));
-  QCB_CUDA(cudaStreamSynchronize(S(stream)));
+  // Expanded on the device in chunks of at most MEAS_STAGE bytes into two
+  // staging buffers of the current device (allocated at its first call, kept
+  // for the process), each chunk copied out on a second stream while the next
+  // one expands; calls are serialised by a lock.
+  static std::mutex mu;
+  static std::map<int, MeasStage> stages;
+  std::lock_guard<std::mutex> lock(mu);
+  int dev = 0;
+  QCB_CUDA(cudaGetDevice(&dev));
+  MeasStage& g = stages[dev];
+  if (!g.buf[0]) {
+    QCB_CUDA(cudaMalloc(&g.buf[0], 2 * MEAS_STAGE));
+    g.buf[1] = g.buf[0] + MEAS_STAGE;
+    QCB_CUDA(cudaStreamCreateWithFlags(&g.copy, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; k++) {
+      QCB_CUDA(cudaEventCreateWithFlags(&g.expanded[k], cudaEventDisableTiming));
+      QCB_CUDA(cudaEventCreateWithFlags(&g.copied[k], cudaEventDisableTiming));
+    }
+  }
+  cudaStream_t st = S(stream);
+  uint64_t k = 0;
+  for (uint64_t o0 = 0; o0 < bytes; o0 += MEAS_STAGE, k++) {
+    const uint64_t n = std::min<uint64_t>(MEAS_STAGE, bytes - o0);
+    const int b = (int)(k & 1);
+    if (k >= 2) QCB_CUDA(cudaStreamWaitEvent(st, g.copied[b], 0));  // buffer b is free again
+    const uint64_t threads = (n + 3) / 4;
+    record_to_bools_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(f->record, f->pitch, f->frames, o0, n,
+                                                                             g.buf[b]);
+    QCB_LAUNCHED();
+    QCB_CUDA(cudaEventRecord(g.expanded[b], st));
+    QCB_CUDA(cudaStreamWaitEvent(g.copy, g.expanded[b], 0));
+    QCB_CUDA(cudaMemcpyAsync(bools + o0, g.buf[b], n, cudaMemcpyDeviceToHost, g.copy));
+    QCB_CUDA(cudaEventRecord(g.copied[b], g.copy));
+  }
+  QCB_CUDA(cudaStreamSynchronize(g.copy));
+  QCB_CUDA(cudaStreamSynchronize(st));
   return frame_device_status(f);
 }
 
@@ -1355,9 +1614,12 @@ int qcb_pftrajectories_host(const qcb_op* ops, size_t n_ops, uint64_t frames, ui
     for (cudaEvent_t& e : chunk_done) QCB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   const auto chunks = host_chunks(cframe->ncols);
+  // the chunks share the frame's pre-sampler scratch, sized for the whole run
+  if (int st = ensure_presample_scratch(cframe, cprog)) return st;
   for (size_t k = 0; k < chunks.size(); k++) {
     const uint64_t c0 = chunks[k].first, nc = chunks[k].second;
     qcb_frame view = *cframe;  // columns [c0, c0 + nc) of every plane
+    view.pre_own = false;
     view.planes = cframe->planes + c0;
     view.record = cframe->record + c0;
     view.ncols = nc;
@@ -1394,6 +1656,7 @@ namespace qcb {
 void set_walker_tile(uint32_t t) { g_tile_override = t; }
 void set_walker_threads(uint32_t t) { g_threads_override = t; }
 void set_stage_withhold(uint32_t k) { g_stage_withhold = k; }
+void set_presample(uint32_t v) { g_presample = v; }
 int run_program_fresh(qcb_frame* f, const qcb_program* p, uint64_t seed, uint64_t shot_offset,
                       cudaStream_t st) {
   qcb_noise_source n{};

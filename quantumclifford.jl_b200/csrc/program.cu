@@ -461,6 +461,9 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
     out.push_back((SEG_WIN << 24) | W); out.push_back(0); out.push_back(0); out.push_back(0);
     while (out.size() % W) out.push_back(0);
   };
+  P.pre_ent.clear();
+  P.pre_capoff.assign(1, 0);
+  P.pre_nparts = 0;
   for (auto& r : recs) {
     const uint32_t n = (uint32_t)(r.w.size() / r.entry_words);
     // A record that fits one window is not split: it starts the next window
@@ -476,8 +479,32 @@ int compile(const qcb_op* ops, size_t n_ops, Program& P) {
       // room() - 4 is a multiple of 4 words, so the padded part fits too
       const uint32_t take = std::min(n - done, fit);
       const bool last = done + take == n;
+      uint32_t aux0 = last ? 0u : FLAG_NO_BARRIER, aux1 = 0, aux2 = 0;
+      if (r.kind == SEG_FLUSH) {
+        // flush part j (header word 2); its sparse sites go to the
+        // pre-sampler's entry table, dense ones are drawn in the walk (header
+        // word 3 bit 0).  Bucket capacity per group: the expected event count
+        // Lambda plus 8 standard deviations and a margin (a bucket that
+        // overflows is drawn in the walk instead, so this bounds memory only).
+        const uint32_t j = P.pre_nparts++;
+        double lam = 0;
+        for (uint32_t t = 0; t < take; t++) {
+          const uint32_t* en = &r.w[(size_t)(done + t) * 4];
+          const NoiseClass& c = classes[en[1] >> 8];
+          if (c.dense) { aux0 |= FLAG_DENSE_SITES; continue; }
+          if (!c.cdf_len) continue;
+          P.pre_ent.push_back(make_uint4(en[0], en[1], j, t));
+          lam += P.sites_slot[en[0]].peff * NOISE_GROUP;
+        }
+        const uint32_t cap = lam > 0 ? ((uint32_t)std::ceil(lam + 8.0 * std::sqrt(lam) + 32.0) + 3u) & ~3u : 0u;
+        if (cap >= (1u << 24)) return fail(QCB_EUNSUPPORTED, "noise pre-sampling: a flush part expects too many events");
+        aux0 |= cap << 8;                 // header word 1: flags | bucket capacity << 8
+        aux1 = j;                         // header word 2: the part
+        aux2 = P.pre_capoff.back();       // header word 3: the bucket's offset in a group's events
+        P.pre_capoff.push_back(P.pre_capoff.back() + cap);
+      }
       out.push_back((r.kind << 24) | take);
-      out.push_back(last ? 0u : FLAG_NO_BARRIER); out.push_back(0); out.push_back(0);
+      out.push_back(aux0); out.push_back(aux1); out.push_back(aux2);
       out.insert(out.end(), r.w.begin() + (size_t)done * r.entry_words, r.w.begin() + (size_t)(done + take) * r.entry_words);
       while (out.size() % 4) out.push_back(0);
       done += take;
@@ -515,6 +542,8 @@ int upload(Program& P) {
   if (e == cudaSuccess) e = up(&P.d_qubit_slot, qs);
   std::vector<uint32_t> sw(P.slot_swap.begin(), P.slot_swap.end());
   if (e == cudaSuccess) e = up(&P.d_slot_swap, sw);
+  if (e == cudaSuccess) e = up(&P.d_pre_ent, P.pre_ent);
+  if (e == cudaSuccess) e = up(&P.d_pre_capoff, P.pre_capoff);
   if (e != cudaSuccess) return cuda_fail(e, "qcb_program_compile upload");
   return QCB_OK;
 }
@@ -526,6 +555,10 @@ void release(Program& P) {
   cudaFree(P.d_slot_qubit);
   cudaFree(P.d_qubit_slot);
   cudaFree(P.d_slot_swap);
+  cudaFree(P.d_pre_ent);
+  cudaFree(P.d_pre_capoff);
+  P.d_pre_ent = nullptr;
+  P.d_pre_capoff = nullptr;
   P.d_stream_slot = nullptr;
   P.d_classes = nullptr;
   P.d_cdf = nullptr;

@@ -93,6 +93,10 @@ constexpr uint32_t XOR_MAX_BITS = 30;
 constexpr uint32_t BIT_NONE = 0xFFFFFFFFu;
 constexpr uint32_t MRZ_PAD = 0xFFFFFFFFu;
 constexpr uint32_t FLAG_NO_BARRIER = 1u;
+// FLUSH header word 1: bit 1 = the part has dense sites (drawn in the walk),
+// bits 8.. = the part's pre-sampler bucket capacity; word 2 = the part index,
+// word 3 = the bucket's offset in a group's events.
+constexpr uint32_t FLAG_DENSE_SITES = 2u;
 // Program window staged into shared memory by the walker (words).
 constexpr uint32_t PROG_WINDOW_WORDS = 2048;      // program window (8 KB)
 constexpr uint32_t PROG_WINDOW_WORDS_TALL = 4096; // tall programs with records longer than 8 KB (16 KB)
@@ -146,6 +150,13 @@ struct Program {
   std::vector<NoiseClass> classes;
   std::vector<uint32_t> cdf;          // Binomial count thresholds of the sparse classes
   double pmax = 0;
+  // Pre-sampling of the sparse noise sites (a kernel that draws every (site,
+  // group) before the walk): one entry per sparse site of a flush part,
+  // (site, kind | class << 8, part j, entry index i in the part); per part
+  // the bucket capacity (events per group), cumulative in pre_capoff.
+  std::vector<uint4> pre_ent;
+  std::vector<uint32_t> pre_capoff;   // [nparts + 1]
+  uint32_t pre_nparts = 0;
   // device copies
   uint32_t* d_stream_slot = nullptr;
   NoiseClass* d_classes = nullptr;
@@ -153,6 +164,8 @@ struct Program {
   uint32_t* d_slot_qubit = nullptr;
   uint32_t* d_slot_swap = nullptr;
   uint32_t* d_qubit_slot = nullptr;   // [nq_alloc] qubit -> slot or NONE
+  uint4* d_pre_ent = nullptr;
+  uint32_t* d_pre_capoff = nullptr;
   uint32_t qubit_slot_len = 0;
   uint64_t hash = 0;
 };
@@ -171,6 +184,11 @@ struct qcb_frame {
   uint32_t* planes;  // [(2*(nq1+1))][pitch]: plane 2q = x(q), 2q+1 = z(q); last pair = scratch
   uint32_t* record;  // [nbits][pitch]
   int32_t* err;      // device status word of the walker (QCB_ETIMEOUT on a stuck wait)
+  // scratch of the noise pre-sampler (event buckets and counters), grown on
+  // demand; only frames made by qcb_frame_create own one (pre_own)
+  uint32_t* pre = nullptr;
+  uint64_t pre_bytes = 0;
+  bool pre_own = false;
 };
 
 namespace qcb {

@@ -50,6 +50,7 @@ __global__ void philox_probe_kernel(uint4 ctr, uint2 key, uint32_t* out) {
 void set_walker_tile(uint32_t t);
 void set_walker_threads(uint32_t t);
 void set_stage_withhold(uint32_t k);
+void set_presample(uint32_t v);
 void set_server_hash_bits(uint32_t b);
 void set_canon_cluster(uint32_t cs);
 void set_canon_threads(uint32_t n);
@@ -117,13 +118,19 @@ int qcb_tune_set(const char* key, int64_t value) {
     // of each CTA's window sequence), so its bounded wait expires and the run
     // reports QCB_ETIMEOUT; 0 turns it off
     set_stage_withhold((uint32_t)value);
+  } else if (k == "presample") {
+    // 0: the noise of Philox runs is drawn by the pre-sampler where its
+    // scratch fits; 1: always in the walk; 2 (test): pre-sampled, but every
+    // bucket reports an overflow, so the walk draws them (the fallback path)
+    if (value > 2) return fail(QCB_EARG, "presample must be 0, 1 or 2");
+    set_presample((uint32_t)value);
   } else if (k == "server_hash_bits") {
     // test knob: the serving program cache keeps only `value` low bits of
     // its hash (0: all), so that distinct circuits collide
     if (value > 64) return fail(QCB_EARG, "server_hash_bits must be 0..64");
     set_server_hash_bits((uint32_t)value);
   } else if (k == "walker_threads") {
-    if (value && (value < 64 || value > 768 || value % 32)) return fail(QCB_EARG, "walker_threads must be 0 (768) or 64..768, a multiple of 32");
+    if (value && (value < 64 || value > 640 || value % 32)) return fail(QCB_EARG, "walker_threads must be 0 (640) or 64..640, a multiple of 32");
     set_walker_threads((uint32_t)value);
   } else if (k == "canon_threads") {
     if (value && (value < 64 || value > 1024 || value % 32)) return fail(QCB_EARG, "canon_threads must be 0 or 64..1024, a multiple of 32");

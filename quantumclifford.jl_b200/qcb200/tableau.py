@@ -16,7 +16,7 @@ from typing import Optional
 import numpy as np
 
 from . import ops as _ops
-from ._lib import DimensionMismatch, check, ensure_init, lib, ptr
+from ._lib import QCB_EDIM, DimensionMismatch, check, ensure_init, lib, ptr
 
 KIND = {"Stabilizer": 0, "MixedStabilizer": 1, "Destabilizer": 2, "MixedDestabilizer": 3}
 
@@ -283,7 +283,7 @@ def _mul_family(right: bool, a, args, phases: bool):
         return _mul_rows(a, 1, len(_tab(a)), args[0], 1, 0, right, 0, phases)
     if len(args) == 1:  # PauliOperator with PauliOperator
         if _tab(a).nqubits != _tab(args[0]).nqubits:
-            raise DimensionMismatch("The two Pauli operators should have the same length!")
+            raise DimensionMismatch(QCB_EDIM, "The two Pauli operators should have the same length!")
         return _mul_rows(a, 1, 1, args[0], 1, 0, right, 0, phases)
     if len(args) == 2 and not isinstance(args[0], (int, np.integer)):
         # mul_left!(p::PauliOperator, s::Tableau/Stabilizer, i)

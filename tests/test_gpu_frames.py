@@ -377,3 +377,46 @@ def test_measurements_upload_roundtrip(qcb, frames, nbits):
     m2 = m.copy()
     m2[:, 0] = False
     assert np.array_equal(f.measurements(), m2)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("which", ["d11", "d5_dense_mix", "d25_tall", "random"])
+def test_presampled_noise_bit_exact(qcb, mode, which):
+    """The noise of a Philox run drawn by the pre-sampler (mode 0, the
+    default), in the walk (1), or pre-sampled with every bucket reporting an
+    overflow so that the walk redraws it (2): the same record and frame, bit
+    for bit against the oracle.  d5 at p = 0.02 mixes dense two-qubit sites
+    (drawn in the walk) with sparse ones; d25 runs 16 KB windows."""
+    rng = np.random.default_rng(5)
+    if which == "d11":
+        circ, frames = circuits.rotated_surface_code_memory(11, 3, 2e-3), 20_000
+    elif which == "d5_dense_mix":
+        circ, frames = circuits.rotated_surface_code_memory(5, 5, 0.02), 9 * 1024 + 77
+    elif which == "d25_tall":
+        circ, frames = circuits.rotated_surface_code_memory(25, 2, 0.01), 3000
+    else:
+        circ, frames = random_circuit(40, 500, rng, p=0.1), 3000
+    arr = O.to_array(circ)
+    qmax, bmax = O.affected_counts(arr)
+    qcb.check(qcb.lib().qcb_tune_set(b"presample", mode))
+    try:
+        f = qcb.pftrajectories(arr, trajectories=frames, seed=4242)
+        rec = f.measurements()
+        xzs = f.xzs()
+        planes = qcb.pftrajectories_record(arr, frames, seed=4242)  # the host call, chunked
+    finally:
+        qcb.check(qcb.lib().qcb_tune_set(b"presample", 0))
+    ox, om = oracle.pftrajectories_philox(arr, frames, qmax, bmax, 4242)
+    assert np.array_equal(rec, om)
+    assert np.array_equal(coding(xzs, qmax + 1), coding(ox, qmax + 1))
+    assert np.array_equal(qcb.unpack_record(planes, frames), om)
+
+
+@pytest.mark.parametrize("frames", [1, 31, 4097, 300_001])
+def test_measurements_download_chunks(qcb, frames):
+    """measurements(frame) through the staged download: 32 MB chunks that
+    cut bit rows (300,001 frames x 241 bits = 72 MB), ragged frame counts."""
+    circ = O.to_array(circuits.rotated_surface_code_memory(11, 1, 1e-3))
+    qmax, bmax = O.affected_counts(circ)
+    f = qcb.pftrajectories(circ, trajectories=frames, seed=8)
+    assert np.array_equal(f.measurements(), qcb.unpack_record(f.record_planes(), frames))

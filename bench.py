@@ -196,8 +196,8 @@ def bench_tableau(args):
     """Config-3 tableau kernels, one JSON line each: device time per call
     (CUDA events around the call only; state copies happen outside), the
     result checked against the oracle on the same input, and the oracle
-    single-threaded on the host as cpu_baseline.  Random states come from
-    seeded random H/S/CNOT circuits applied to the identity."""
+    single-threaded on the host as cpu_baseline.  Random states are uniformly
+    random stabilizer states (Bravyi-Maslov sampler, seeded)."""
     import torch
     import numpy as np
     import qcb200
@@ -252,11 +252,9 @@ def bench_tableau(args):
     def want(name):
         return not only or name in only
 
-    def random_destabilizer(n, depth=12):
-        d = Q.one_destabilizer(n).to_gpu()
-        Q.apply_(d, Q.random_clifford_ops(n, depth, rng))
-        d.to_cpu()
-        return d
+    def random_destabilizer(n):
+        # uniformly random (Bravyi-Maslov), as random_destabilizer(n) in the reference
+        return qcb200.random_destabilizer(n, rng)
 
     if want("mul_left"):
         # ---- mul_left! of two 1e9-qubit Paulis (HBM: read 2 x 250 MB, write 250 MB)
@@ -303,43 +301,45 @@ def bench_tableau(args):
                  {"workload": f"canonicalize!(random_stabilizer({n})), phases on", "rows": n}, cpu)
 
     if want("project"):
-        # ---- project! of 1000 random Paulis in sequence on a random 1000-qubit Destabilizer
-        n, k = 1000, 1000
-        d = random_destabilizer(n)
-        xs = np.zeros((k, n), bool)
-        zs = np.zeros((k, n), bool)
-        for i in range(k):
-            w = int(rng.integers(1, n + 1))
-            q = rng.choice(n, w, replace=False)
-            kinds = rng.integers(1, 4, size=w)
-            xs[i, q] = kinds & 1 == 1
-            zs[i, q] = kinds & 2 == 2
-        P = Q.Tableau.from_bits(np.zeros(k, np.uint8), xs, zs).to_gpu()
-        state = Q.Destabilizer(Q.Tableau(d.tab.phases.copy(), n, d.tab.xzs.copy())).to_gpu()
-        pristine = Q.DeviceTableau(2 * n, n)
-        pristine.upload(d.tab.phases, d.tab.xzs)
-        rank = ctypes.c_int32(0)
-        anti = np.zeros(k, np.int32)
-        res = np.zeros(k, np.int32)
-        done = ctypes.c_uint32()
-        ms = device_ms(lambda: check(L.qcb_project(state.tab.dev.handle, Q.KIND["Destabilizer"], ctypes.byref(rank),
-                                                   P.dev.handle, 1, 1, ptr(anti), ptr(res), ctypes.byref(done), sp)),
-                       max(3, args.steps // 4), setup=lambda: check(L.qcb_tableau_copy(state.tab.dev.handle, pristine.handle, sp)))
-        # oracle: the same sequence
-        def oracle_chain():
-            ph, xz = d.tab.phases.copy(), d.tab.xzs.copy()
+        # ---- project! of 1000 random Paulis (weight ~ U{1..n}) in sequence on
+        # random_stabilizer(n), n = 1000 / 2000 / 4000 (Stabilizer kind: the
+        # commuting branch runs canonicalize! + generate!), and on a random
+        # 1000-qubit Destabilizer (the README's case)
+        k = 1000
+        for kind, n in (("Stabilizer", 1000), ("Stabilizer", 2000), ("Stabilizer", 4000), ("Destabilizer", 1000)):
+            d = random_destabilizer(n)
+            if kind == "Stabilizer":
+                ph0, xz0 = d.tab.phases[n:].copy(), d.tab.xzs[n:].copy()
+            else:
+                ph0, xz0 = d.tab.phases.copy(), d.tab.xzs.copy()
+            P = qcb200.random_paulis(k, n, rng).to_gpu()
+            state = (Q.Stabilizer if kind == "Stabilizer" else Q.Destabilizer)(Q.Tableau(ph0.copy(), n, xz0.copy())).to_gpu()
+            pristine = Q.DeviceTableau(len(ph0), n)
+            pristine.upload(ph0, xz0)
+            rank = ctypes.c_int32(0)
+            anti = np.zeros(k, np.int32)
+            res = np.zeros(k, np.int32)
+            done = ctypes.c_uint32()
+            ms = device_ms(lambda: check(L.qcb_project(state.tab.dev.handle, Q.KIND[kind], ctypes.byref(rank),
+                                                       P.dev.handle, 1, 1, ptr(anti), ptr(res), ctypes.byref(done),
+                                                       sp)),
+                           max(3, args.steps // 4),
+                           setup=lambda: check(L.qcb_tableau_copy(state.tab.dev.handle, pristine.handle, sp)))
+            state.to_cpu()
+            # the oracle: the same sequence on the host, one thread
+            t0 = time.perf_counter()
+            ph, xz = ph0.copy(), xz0.copy()
             outs = []
             for i in range(k):
-                st, ph, xz, _, a_, r_ = oracle.project("Destabilizer", ph, xz, n, P.xzs[i], 0)
+                _, ph, xz, _, a_, r_ = oracle.project(kind, ph, xz, n, P.xzs[i], 0)
                 outs.append((a_, r_))
-            return outs
-        t0 = time.perf_counter()
-        outs = oracle_chain()
-        cpu = (time.perf_counter() - t0) * 1e3 / k
-        assert [o[0] for o in outs] == list(anti) and [o[1] for o in outs] == list(res)
-        emit("project! of a random Pauli on a random 1000-qubit Destabilizer", "project", ms / k,
-             {"workload": "1000 random Paulis (weight ~ U{1..n}) projected in sequence by one call, per projection",
-              "rows": 2 * n}, cpu)
+            cpu = (time.perf_counter() - t0) * 1e3 / k
+            assert [o[0] for o in outs] == list(anti) and [o[1] for o in outs] == list(res)
+            assert np.array_equal(state.tab.xzs, xz) and np.array_equal(state.tab.phases, ph)
+            key = "project" if kind == "Destabilizer" else f"project_stab_{n}"
+            emit(f"project! of a random Pauli on a random {n}-qubit {kind}", key, ms / k,
+                 {"workload": f"1000 random Paulis (weight ~ U{{1..n}}) projected in sequence on a random {n}-qubit "
+                              f"{kind} by one call, per projection", "rows": len(ph0)}, cpu)
 
     if want("expect"):
         # ---- expect of 1000 random Paulis on a random 1000-qubit Destabilizer:
@@ -475,14 +475,11 @@ def bench_batch(args):
         if j["d"] not in tuned:
             tuned[j["d"]] = qcb200.tune_tile(j["prog"])[0]
     fbatch = qcb200.Batch([(j["frame"], j["prog"], j["seed"], 0) for j in jobs])
-    # canonicalize! jobs: random stabilizers from seeded H/S/CNOT circuits
+    # canonicalize! jobs: uniformly random stabilizer states (Bravyi-Maslov)
     canon_n = [int(n) for n in rng.integers(100, 2001, size=512)]
     pristine, work = [], []
     for n in canon_n:
-        dst = Q.one_destabilizer(n).to_gpu()
-        Q.apply_(dst, Q.random_clifford_ops(n, 6, rng))
-        dst.to_cpu()
-        t = Q.Tableau(dst.tab.phases[n:].copy(), n, dst.tab.xzs[n:].copy())
+        t = qcb200.random_stabilizer(n, rng).tab
         st = Q.Stabilizer(t).to_gpu()
         pristine.append(Q.Stabilizer(t.copy()).to_gpu())
         work.append(st)
@@ -564,7 +561,7 @@ def bench_batch(args):
            "ms_per_step": ms_b, "higher_is_better": True, "scaling": "none", "vs_baseline": None,
            "dtype": "u32 bit planes (GF(2)) + u64 bit rows", "data": "synthetic (seeded)",
            "config": {"workload": "256 rotated surface-code memory circuits, d in {3..15}, rounds = d, p log-U[1e-4,1e-2], "
-                                  "shots log-U[1e3,1e6] + 512 canonicalize! on random stabilizers n ~ U[100,2000]; one "
+                                  "shots log-U[1e3,1e6] + 512 canonicalize! on uniformly random stabilizers n ~ U[100,2000]; one "
                                   "persistent sampling launch + one persistent canonicalize! launch in one CUDA graph",
                       "frame_updates": updates, "total_shots": sum(j["shots"] for j in jobs),
                       "tuned_tiles": {str(k): v for k, v in sorted(tuned.items())},

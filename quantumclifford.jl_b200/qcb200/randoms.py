@@ -45,14 +45,53 @@ def quantum_mallows(n: int, rng: np.random.Generator):
 
 
 def _mm2(a: np.ndarray, b: np.ndarray) -> np.ndarray:
-    """GF(2) product of 0/1 matrices."""
+    """GF(2) product of 0/1 matrices: an exact floating-point product reduced
+    mod 2 (float64 on a CUDA device when one is present and the product is
+    large -- input generation only -- else float32 BLAS on the host)."""
+    if min(a.shape[0], b.shape[1]) >= 256 and _torch_cuda():
+        import torch
+
+        ta = torch.from_numpy(np.ascontiguousarray(a)).to("cuda", torch.float64)
+        tb = torch.from_numpy(np.ascontiguousarray(b)).to("cuda", torch.float64)
+        return (torch.matmul(ta, tb).to(torch.int64) & 1).to(torch.uint8).cpu().numpy()
     return (np.matmul(a.astype(np.float32), b.astype(np.float32)).astype(np.int64) & 1).astype(np.uint8)
 
 
+_TORCH_CUDA = None
+
+
+def _torch_cuda() -> bool:
+    global _TORCH_CUDA
+    if _TORCH_CUDA is None:
+        try:
+            import torch
+
+            _TORCH_CUDA = bool(torch.cuda.is_available())
+        except ImportError:
+            _TORCH_CUDA = False
+    return _TORCH_CUDA
+
+
 def _unit_lower_inverse(low: np.ndarray) -> np.ndarray:
-    """Inverse over GF(2) of a unit lower-triangular 0/1 matrix, by forward
-    substitution on bit-packed rows: row i of the inverse is e_i XOR the
-    inverse rows j < i with low[i, j] = 1."""
+    """Inverse over GF(2) of a unit lower-triangular 0/1 matrix: by blocks,
+    [[A, 0], [C, D]]^-1 = [[A^-1, 0], [D^-1 C A^-1, D^-1]] (signs vanish mod
+    2), down to blocks of 128 rows done by forward substitution."""
+    n = low.shape[0]
+    if n > 128:
+        h = n // 2
+        ai = _unit_lower_inverse(low[:h, :h])
+        di = _unit_lower_inverse(low[h:, h:])
+        out = np.zeros((n, n), dtype=np.uint8)
+        out[:h, :h] = ai
+        out[h:, h:] = di
+        out[h:, :h] = _mm2(_mm2(di, low[h:, :h]), ai)
+        return out
+    return _unit_lower_inverse_rows(low)
+
+
+def _unit_lower_inverse_rows(low: np.ndarray) -> np.ndarray:
+    """Forward substitution on bit-packed rows: row i of the inverse is e_i
+    XOR the inverse rows j < i with low[i, j] = 1."""
     n = low.shape[0]
     words = (n + 63) // 64
     inv = np.zeros((n, words), dtype=np.uint64)

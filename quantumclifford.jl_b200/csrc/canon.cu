@@ -851,6 +851,330 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_batch_kernel(const CanonB
   cl.sync();  // CTA 0's job slot is read by the cluster until here
 }
 
+// ---------------------------------------------------------------- panels over the whole GPU
+// canonicalize! by 64-column panels with the per-row work spread over every
+// SM: per panel two launches, (1) canon_search_kernel, one CTA: the panel's
+// pivot steps on the panel words of all rows (the same search as
+// blocked_body, positions kept in global memory between panels), the pivot
+// rows as they are at the panel start copied aside, and the panel's phase
+// data (C, D_t, the pivots' q); (2) canon_apply_kernel, a grid over the rows:
+// every row's mask, bits and phase from that record (the same bilinear-form
+// replay as blocked_body).  The launch boundary is the barrier between the
+// two; the rows live in global memory (L2-resident) throughout.
+struct PanelRec {
+  uint32_t T;        // pivots of the panel
+  uint32_t i;        // next pivot position after the panel
+  uint32_t rx;       // pivots of the X stage (kept from the last X-stage panel)
+  uint32_t done;     // every position has a pivot: later panels do nothing
+  uint32_t stp[PANEL];
+  uint8_t bt[PANEL];
+  uint8_t qp[PANEL];
+  uint64_t A[PANEL], PWP[PANEL], Dt[PANEL];
+};
+
+struct PanelArgs {
+  uint64_t* xzs;
+  uint8_t* ph;
+  uint32_t rows, n, W;
+  int phases;
+  uint32_t stage, c0;   // this panel: stage 0 (X) or 1 (Z), first column
+  uint32_t* pos;        // [rows] row -> position (persistent)
+  PanelRec* rec;
+  uint64_t* po;         // [PANEL][W] the pivot rows at the panel start
+  int32_t* out;         // [0] X-stage pivots, [1] next pivot position
+};
+
+template <uint32_t RPT>
+__global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const PanelArgs a) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  PanelRec& g = *a.rec;
+  if (g.done) {  // every position has its pivot: this panel applies nothing
+    if (threadIdx.x == 0) g.T = 0;
+    return;
+  }
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t R = a.rows, W = a.W, len = W / 2, n = a.n;
+  const uint32_t c0 = a.c0, ncp = min(PANEL, n - c0), wj = a.stage * len + (c0 >> 6);
+  uint64_t* XT = sm;                                   // XT[w * PANEL + t] = X word w of pivot t
+  __shared__ uint32_t stp[PANEL];
+  __shared__ uint8_t bt[PANEL], qo[PANEL];
+  __shared__ uint64_t A[PANEL], PWP[PANEL], C[PANEL], Dt[PANEL], Us[PANEL];
+  __shared__ uint8_t bases[PANEL];
+  __shared__ uint64_t red2[2][32][3];
+  __shared__ uint32_t shT, shI;
+  const uint32_t NB = min(nwarps, max(1u, (R + 32 * RPT - 1) / (32 * RPT))), nbt = NB * 32;
+  uint32_t i = g.i;
+  uint32_t rpos[RPT];
+  uint64_t rpw[RPT], rcb[RPT];
+  uint32_t T = 0;
+  if (warp < NB) {
+#pragma unroll
+    for (uint32_t k = 0; k < RPT; k++) {
+      const uint32_t r = tid + k * nbt;
+      rpos[k] = r < R ? a.pos[r] : 0xFFFFFFFFu;
+      rpw[k] = r < R ? a.xzs[(size_t)r * W + wj] : 0ull;
+      rcb[k] = 0;
+    }
+    // the steps (as blocked_body): one named barrier among the search warps per column
+    bool prev = false;
+    uint32_t pprev = 0, bprev = 0;
+    uint64_t pwprev = 0, aprev = 0;
+    for (uint32_t b = 0; b < ncp && i < R; b++) {
+      uint32_t bpos = 0xFFFFFFFFu, bk = 0;
+#pragma unroll
+      for (uint32_t k = 0; k < RPT; k++) {
+        const uint32_t r = tid + k * nbt;
+        if (r >= R) continue;
+        if (prev && r != pprev && ((rpw[k] >> bprev) & 1ull)) {
+          rpw[k] ^= pwprev;
+          rcb[k] ^= aprev;
+        }
+        if (rpos[k] >= i && ((rpw[k] >> b) & 1ull) && rpos[k] < bpos) { bpos = rpos[k]; bk = k; }
+      }
+      {
+        uint64_t mypw = 0, mycb = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < RPT; k++)
+          if (k == bk) { mypw = rpw[k]; mycb = rcb[k]; }
+        const uint32_t m = __reduce_min_sync(0xFFFFFFFFu, bpos);
+        const uint32_t who = __ballot_sync(0xFFFFFFFFu, bpos == m);
+        const uint32_t src = __ffs(who) - 1;
+        const uint32_t row = __shfl_sync(0xFFFFFFFFu, tid + bk * nbt, src);
+        const uint64_t wpw = __shfl_sync(0xFFFFFFFFu, mypw, src);
+        const uint64_t wcb = __shfl_sync(0xFFFFFFFFu, mycb, src);
+        if (lane == 0) {
+          red2[b & 1][warp][0] = ((uint64_t)m << 32) | row;
+          red2[b & 1][warp][1] = wpw;
+          red2[b & 1][warp][2] = wcb;
+        }
+      }
+      asm volatile("bar.sync 1, %0;" ::"r"(nbt) : "memory");
+      const uint64_t e = lane < NB ? red2[b & 1][lane][0] : ~0ull;
+      const uint32_t kpos = __reduce_min_sync(0xFFFFFFFFu, (uint32_t)(e >> 32));
+      if (kpos == 0xFFFFFFFFu) {
+        prev = false;
+        continue;
+      }
+      const uint32_t kw = __ffs(__ballot_sync(0xFFFFFFFFu, (uint32_t)(e >> 32) == kpos)) - 1;
+      const uint32_t pstar = (uint32_t)red2[b & 1][kw][0];
+      pwprev = red2[b & 1][kw][1];
+      aprev = red2[b & 1][kw][2] | (1ull << T);
+#pragma unroll
+      for (uint32_t k = 0; k < RPT; k++) {
+        const uint32_t r = tid + k * nbt;
+        if (r == pstar) rpos[k] = i;
+        else if (r < R && rpos[k] == i) rpos[k] = kpos;
+      }
+      if (tid == 0) {
+        stp[T] = pstar;
+        bt[T] = (uint8_t)b;
+        A[T] = aprev;
+        PWP[T] = pwprev;
+      }
+      prev = true;
+      pprev = pstar;
+      bprev = b;
+      T++;
+      i++;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < RPT; k++) {
+      const uint32_t r = tid + k * nbt;
+      if (r < R) a.pos[r] = rpos[k];
+    }
+    if (tid == 0) { shT = T; shI = i; }
+  }
+  __syncthreads();
+  T = shT;
+  i = shI;
+  // the pivot rows at the panel start, their q = phase + |x & z|, XT
+  for (uint32_t t = warp; t < T; t += nwarps) {
+    const uint32_t r = stp[t];
+    uint32_t s = 0;
+    for (uint32_t w = lane; w < W; w += 32) {
+      const uint64_t v = a.xzs[(size_t)r * W + w];
+      a.po[(size_t)t * W + w] = v;
+      if (w < len) XT[(size_t)w * PANEL + t] = v;
+      if (w >= len) s += __popcll(a.xzs[(size_t)r * W + w - len] & v);
+    }
+    s = __reduce_add_sync(0xFFFFFFFFu, s);
+    if (lane == 0) qo[t] = (uint8_t)((a.ph[r] + s) & 3u);
+  }
+  __syncthreads();
+  if (a.phases && T) {
+    // C[a] bit b = z_a . x_b over the pivot rows (z from global, x transposed)
+    for (uint32_t t = warp; t < T; t += nwarps) {
+      const uint64_t* za = a.xzs + (size_t)stp[t] * W + len;
+      uint32_t p0 = 0, p1 = 0;
+      for (uint32_t w = 0; w < len; w++) {
+        const uint64_t zw = za[w];
+        p0 += __popcll(zw & XT[(size_t)w * PANEL + lane]);
+        p1 += __popcll(zw & XT[(size_t)w * PANEL + lane + 32]);
+      }
+      const uint32_t lo = __ballot_sync(0xFFFFFFFFu, (p0 & 1u) && lane < T);
+      const uint32_t hi = __ballot_sync(0xFFFFFFFFu, (p1 & 1u) && lane + 32 < T);
+      if (lane == 0) C[t] = (uint64_t)lo | ((uint64_t)hi << 32);
+    }
+    __syncthreads();
+    if (tid < T) {
+      uint64_t d = 0;
+      for (uint32_t x = 0; x < T; x++)
+        if ((A[tid] >> x) & 1ull) d ^= C[x];
+      Dt[tid] = d;
+    }
+    __syncthreads();
+    if (tid < T) {
+      const uint32_t t = tid;
+      uint64_t u = 0;
+      for (uint32_t x = 0; x < T; x++) u |= ((C[x] >> t) & 1ull) << x;
+      uint64_t pw = a.po[(size_t)t * W + wj], cm = 0, ut = 0;
+      uint32_t cross = 0;
+      for (uint32_t t2 = 0; t2 < t; t2++) {
+        if ((pw >> bt[t2]) & 1ull) {
+          cross += (uint32_t)((__popcll(Dt[t2] & cm) + __popcll(u & A[t2])) & 1);
+          ut |= 1ull << t2;
+          cm ^= A[t2];
+          pw ^= PWP[t2];
+        }
+      }
+      Us[t] = ut;
+      bases[t] = (uint8_t)((qo[t] + 2u * cross) & 3u);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      uint64_t Q1 = 0, Q2 = 0;
+      for (uint32_t t = 0; t < T; t++) {
+        const uint32_t q = (bases[t] + (uint32_t)__popcll(Us[t] & Q1) + 2u * (uint32_t)__popcll(Us[t] & Q2)) & 3u;
+        g.qp[t] = (uint8_t)q;
+        Q1 |= (uint64_t)(q & 1u) << t;
+        Q2 |= (uint64_t)(q >> 1) << t;
+      }
+    }
+  }
+  // the record for the apply launch
+  for (uint32_t t = tid; t < T; t += blockDim.x) {
+    g.stp[t] = stp[t];
+    g.bt[t] = bt[t];
+    g.A[t] = A[t];
+    g.PWP[t] = PWP[t];
+    g.Dt[t] = a.phases ? Dt[t] : 0ull;
+  }
+  if (tid == 0) {
+    g.T = T;
+    g.i = i;
+    if (a.stage == 0) g.rx = i;
+    if (i >= R) g.done = 1;
+    a.out[0] = (int32_t)g.rx;
+    a.out[1] = (int32_t)i;
+  }
+}
+
+// Rows r0 .. of the grid's share: apply the panel record (as blocked_body's
+// step 3, with rows and phases in global memory).
+__global__ void __launch_bounds__(CANON_THREADS) canon_apply_kernel(const PanelArgs a) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  const PanelRec& g = *a.rec;
+  const uint32_t T = g.T;
+  if (T == 0) return;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5, bd = blockDim.x;
+  const uint32_t R = a.rows, W = a.W, len = W / 2, wj = a.stage * len + (a.c0 >> 6);
+  const uint32_t per = (R + gridDim.x - 1) / gridDim.x, r0 = blockIdx.x * per;
+  const uint32_t nloc = r0 < R ? min(per, R - r0) : 0u;
+  if (!nloc) return;
+  uint64_t* PO = sm;                      // [T][W]
+  uint64_t* cml = PO + (size_t)PANEL * W; // per local row: mask
+  uint8_t* ql = (uint8_t*)(cml + per);    // per local row: q
+  __shared__ uint32_t stp[PANEL];
+  __shared__ uint8_t bt[PANEL], qp[PANEL];
+  __shared__ uint64_t A[PANEL], PWP[PANEL], Dt[PANEL];
+  for (uint32_t t = tid; t < T; t += bd) {
+    stp[t] = g.stp[t]; bt[t] = g.bt[t]; qp[t] = g.qp[t];
+    A[t] = g.A[t]; PWP[t] = g.PWP[t]; Dt[t] = g.Dt[t];
+  }
+  for (size_t w = tid; w < (size_t)T * W; w += bd) PO[w] = a.po[w];
+  __syncthreads();
+  // (a) per row (warp per row): u[x] = z_x . x_row and q = phase + |x & z|
+  if (a.phases) {
+    for (uint32_t lr = warp; lr < nloc; lr += nwarps) {
+      const uint64_t* row = a.xzs + (size_t)(r0 + lr) * W;
+      uint32_t lo = 0, hi = 0, s = 0;
+      for (uint32_t w = lane; w < len; w += 32) {
+        const uint64_t xw = row[w];
+        s += __popcll(xw & row[len + w]);
+        for (uint32_t x = 0; x < T; x++) {
+          const uint32_t bit = (uint32_t)__popcll(PO[(size_t)x * W + len + w] & xw) & 1u;
+          if (x < 32) lo ^= bit << x; else hi ^= bit << (x - 32);
+        }
+      }
+      s = __reduce_add_sync(0xFFFFFFFFu, s);
+      lo = __reduce_xor_sync(0xFFFFFFFFu, lo);
+      hi = __reduce_xor_sync(0xFFFFFFFFu, hi);
+      if (lane == 0) {
+        cml[lr] = (uint64_t)lo | ((uint64_t)hi << 32);
+        ql[lr] = (uint8_t)((a.ph[r0 + lr] + s) & 3u);
+      }
+    }
+    __syncthreads();
+  }
+  // (b) the steps replayed, one thread per row
+  for (uint32_t lr = tid; lr < nloc; lr += bd) {
+    const uint32_t r = r0 + lr;
+    uint64_t pw = a.xzs[(size_t)r * W + wj], cm = 0;
+    const uint64_t u = a.phases ? cml[lr] : 0;
+    uint32_t q = a.phases ? ql[lr] : 0;
+    for (uint32_t t = 0; t < T; t++) {
+      if (r != stp[t] && ((pw >> bt[t]) & 1ull)) {
+        if (a.phases) q += qp[t] + 2u * (uint32_t)((__popcll(Dt[t] & cm) + __popcll(u & A[t])) & 1);
+        cm ^= A[t];
+        pw ^= PWP[t];
+      }
+    }
+    cml[lr] = cm;
+    ql[lr] = (uint8_t)(q & 3u);
+  }
+  __syncthreads();
+  // (c) the rows: start bits XOR the pivot rows of the mask
+  for (uint32_t lr = warp; lr < nloc; lr += nwarps) {
+    const uint64_t cm = cml[lr];
+    if (!cm) continue;
+    uint64_t* row = a.xzs + (size_t)(r0 + lr) * W;
+    uint32_t s = 0;
+    for (uint32_t w = lane; w < len; w += 32) {
+      uint64_t vx = row[w], vz = row[len + w];
+      uint64_t m = cm;
+      while (m) {
+        const uint32_t x = __ffsll(m) - 1;
+        m &= m - 1;
+        vx ^= PO[(size_t)x * W + w];
+        vz ^= PO[(size_t)x * W + len + w];
+      }
+      row[w] = vx;
+      row[len + w] = vz;
+      s += __popcll(vx & vz);
+    }
+    if (a.phases) {
+      s = __reduce_add_sync(0xFFFFFFFFu, s);
+      if (lane == 0) a.ph[r0 + lr] = (uint8_t)((ql[lr] - s) & 3u);
+    }
+  }
+}
+
+// rows to their final positions: out[pos[r]] = row r
+__global__ void canon_place_kernel(const uint64_t* xzs, const uint8_t* ph, const uint32_t* pos, uint32_t rows,
+                                   uint32_t W, uint64_t* out, uint8_t* out_ph) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= rows) return;
+  const uint32_t p = pos[warp];
+  for (uint32_t w = lane; w < W; w += 32) out[(size_t)p * W + w] = xzs[(size_t)warp * W + w];
+  if (lane == 0) out_ph[p] = ph[warp];
+}
+
+__global__ void canon_grid_init_kernel(uint32_t* pos, uint32_t rows, PanelRec* rec) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < rows) pos[r] = r;
+  if (r == 0) { rec->T = 0; rec->i = 0; rec->rx = 0; rec->done = 0; }
+}
+
 struct CanonPlan {
   uint32_t cs;
   bool smem_rows;
@@ -961,6 +1285,61 @@ static int launch_blocked(const ElimSpec& e, cudaStream_t st) {
   return QCB_OK;
 }
 
+static uint32_t g_canon_grid = 0;  // 0: automatic, 1: always, 2: never (panels over the whole GPU)
+// Smallest stabilizer view that runs by panels over the whole GPU (below it,
+// one cluster holds the rows in shared memory).
+constexpr uint32_t CANON_GRID_MIN_ROWS = 1024;
+
+// canonicalize! by panels over the whole GPU (canon_search_kernel +
+// canon_apply_kernel per panel); scratch from the stream-ordered pool.
+static int launch_grid(const ElimSpec& e, cudaStream_t st) {
+  const uint32_t R = e.rows, W = e.W, len = W / 2;
+  uint32_t* pos = nullptr;
+  PanelRec* rec = nullptr;
+  uint64_t *po = nullptr, *gtmp = nullptr;
+  uint8_t* gtmp_ph = nullptr;
+  QCB_CUDA(cudaMallocAsync(&pos, (size_t)R * 4, st));
+  QCB_CUDA(cudaMallocAsync(&rec, sizeof(PanelRec), st));
+  QCB_CUDA(cudaMallocAsync(&po, (size_t)PANEL * W * 8, st));
+  QCB_CUDA(cudaMallocAsync(&gtmp, (size_t)R * W * 8, st));
+  QCB_CUDA(cudaMallocAsync(&gtmp_ph, R, st));
+  canon_grid_init_kernel<<<(R + 255) / 256, 256, 0, st>>>(pos, R, rec);
+  QCB_LAUNCHED();
+  void (*search)(const PanelArgs) = R <= 4096 ? canon_search_kernel<4> : canon_search_kernel<8>;
+  const size_t search_smem = (size_t)len * PANEL * 8;
+  if (search_smem > 48 * 1024)
+    QCB_CUDA(cudaFuncSetAttribute(search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_smem));
+  const uint32_t G = std::max<uint32_t>(1, std::min<uint32_t>((R + 15) / 16, 2 * (uint32_t)device_sm_count()));
+  const uint32_t per = (R + G - 1) / G;
+  const uint32_t threads = std::min<uint32_t>(CANON_THREADS, std::max<uint32_t>(64, 32 * per));
+  const size_t apply_smem = (size_t)PANEL * W * 8 + (size_t)per * 9 + 16;
+  if (apply_smem > 48 * 1024)
+    QCB_CUDA(cudaFuncSetAttribute(canon_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
+  PanelArgs a{};
+  a.xzs = e.xzs; a.ph = e.ph; a.rows = R; a.n = e.n; a.W = W; a.phases = e.phases;
+  a.pos = pos; a.rec = rec; a.po = po; a.out = e.d_out;
+  for (uint32_t stage = 0; stage < 2; stage++) {
+    for (uint32_t c0 = 0; c0 < e.n; c0 += PANEL) {
+      a.stage = stage;
+      a.c0 = c0;
+      search<<<1, CANON_THREADS, search_smem, st>>>(a);
+      QCB_LAUNCHED();
+      canon_apply_kernel<<<G, threads, apply_smem, st>>>(a);
+      QCB_LAUNCHED();
+    }
+  }
+  canon_place_kernel<<<(R * 32 + 255) / 256, 256, 0, st>>>(e.xzs, e.ph, pos, R, W, gtmp, gtmp_ph);
+  QCB_LAUNCHED();
+  QCB_CUDA(cudaMemcpyAsync(e.xzs, gtmp, (size_t)R * W * 8, cudaMemcpyDeviceToDevice, st));
+  QCB_CUDA(cudaMemcpyAsync(e.ph, gtmp_ph, R, cudaMemcpyDeviceToDevice, st));
+  QCB_CUDA(cudaFreeAsync(pos, st));
+  QCB_CUDA(cudaFreeAsync(rec, st));
+  QCB_CUDA(cudaFreeAsync(po, st));
+  QCB_CUDA(cudaFreeAsync(gtmp, st));
+  QCB_CUDA(cudaFreeAsync(gtmp_ph, st));
+  return QCB_OK;
+}
+
 static int eliminate(const ElimSpec& e, cudaStream_t st) {
   if (e.rows == 0) {
     const int32_t h[2] = {0, e.mode == ELIM_RREF ? -1 : (int32_t)e.i0};
@@ -970,6 +1349,9 @@ static int eliminate(const ElimSpec& e, cudaStream_t st) {
   }
   const bool D = e.dxzs != nullptr;
   // by panels up to 8192 rows (the search keeps at most 8 rows per thread in registers)
+  if (e.mode == ELIM_BOTH && !D && e.rows <= 8192 && g_canon_grid != 2 &&
+      (g_canon_grid == 1 || e.rows >= CANON_GRID_MIN_ROWS) && g_canon_blocked != 2 && e.n > 0)
+    return launch_grid(e, st);
   if (e.mode == ELIM_BOTH && !D && e.rows <= 8192 && g_canon_blocked != 2 && (g_canon_blocked == 1 || e.rows >= 64))
     return launch_blocked(e, st);
   CanonPlan p = canon_plan(e.rows, e.W, D);
@@ -1083,6 +1465,7 @@ int generate_dev(uint64_t* pauli, uint8_t* pph, const uint64_t* xzs, const uint8
 void set_canon_cluster(uint32_t cs) { g_canon_cs = cs; }
 void set_canon_threads(uint32_t n) { g_canon_threads = n; }
 void set_canon_blocked(uint32_t v) { g_canon_blocked = v; }
+void set_canon_grid(uint32_t v) { g_canon_grid = v; }
 
 }  // namespace qcb
 

@@ -56,6 +56,7 @@ void set_canon_cluster(uint32_t cs);
 void set_canon_threads(uint32_t n);
 void set_project_cluster(uint32_t cs);
 void set_canon_blocked(uint32_t v);
+void set_canon_grid(uint32_t v);
 
 }  // namespace qcb
 
@@ -141,6 +142,10 @@ int qcb_tune_set(const char* key, int64_t value) {
   } else if (k == "canon_blocked") {
     if (value > 2) return fail(QCB_EARG, "canon_blocked must be 0 (automatic), 1 (always) or 2 (never)");
     set_canon_blocked((uint32_t)value);
+  } else if (k == "canon_grid") {
+    // canonicalize! by panels over the whole GPU: 0 from 1024 rows, 1 always, 2 never
+    if (value > 2) return fail(QCB_EARG, "canon_grid must be 0 (automatic), 1 (always) or 2 (never)");
+    set_canon_grid((uint32_t)value);
   } else if (k == "project_cluster") {
     if (value && (value > 16 || (value & (value - 1)))) return fail(QCB_EARG, "project_cluster must be 1, 2, 4, 8 or 16");
     set_project_cluster((uint32_t)value);

@@ -281,3 +281,30 @@ def test_dense_apply(qcb, n):
         s.to_cpu()
         ph, xz = oracle.apply_dense(state.phases, state.xzs, n, c.tab.phases, c.tab.xzs, phases)
         assert np.array_equal(s.tab.xzs, xz) and np.array_equal(s.tab.phases, ph)
+
+
+@pytest.mark.parametrize("grid", [1, 2])
+@pytest.mark.parametrize("n", [64, 97, 1000, 2100, 4000])
+def test_canonicalize_panels_over_the_gpu(qcb, n, grid):
+    """canonicalize! by panels with the per-row work spread over the GPU
+    (canon_grid 1: a one-CTA search launch and a grid-wide apply launch per
+    panel) and on one cluster (2), on uniformly random stabilizer states, bit
+    for bit with phases and ranks against the oracle; also a rank-deficient
+    view (repeated rows)."""
+    from qcb200 import randoms
+
+    rng = np.random.default_rng(n + grid)
+    t = randoms.random_stabilizer(n, rng).tab
+    if n == 97:  # duplicate rows: rank deficiency, columns without a pivot
+        t.xzs[50:60] = t.xzs[10:20]
+        t.phases[50:60] = t.phases[10:20]
+    qcb.check(qcb.lib().qcb_tune_set(b"canon_grid", grid))
+    try:
+        s = qcb.Stabilizer(t.copy()).to_gpu()
+        _, rx, rz = qcb.canonicalize_(s, ranks=True)
+        s.to_cpu()
+    finally:
+        qcb.check(qcb.lib().qcb_tune_set(b"canon_grid", 0))
+    ph, xz, orx, orz = oracle.canonicalize(t.phases, t.xzs, n, True)
+    assert (rx, rz) == (orx, orz)
+    assert np.array_equal(s.tab.xzs, xz) and np.array_equal(s.tab.phases, ph)

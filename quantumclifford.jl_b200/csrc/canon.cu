@@ -901,18 +901,29 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
   __shared__ uint64_t A[PANEL], PWP[PANEL], C[PANEL], Dt[PANEL], Us[PANEL];
   __shared__ uint8_t bases[PANEL];
   __shared__ uint64_t red2[2][32][3];
-  __shared__ uint32_t shT, shI;
-  const uint32_t NB = min(nwarps, max(1u, (R + 32 * RPT - 1) / (32 * RPT))), nbt = NB * 32;
+  __shared__ uint32_t shT, shI, ncand;
+  uint32_t* cand = (uint32_t*)(XT + (size_t)len * PANEL);  // the candidate rows (position >= i)
   uint32_t i = g.i;
-  uint32_t rpos[RPT];
+  // Only rows at positions >= i can become pivots; the search runs on them
+  // alone (the others' panel words do not matter to it), so it shrinks as
+  // the elimination proceeds.
+  if (tid == 0) ncand = 0;
+  __syncthreads();
+  for (uint32_t r = tid; r < R; r += blockDim.x)
+    if (a.pos[r] >= i) cand[atomicAdd(&ncand, 1u)] = r;
+  __syncthreads();
+  const uint32_t Rc = ncand;
+  const uint32_t NB = min(nwarps, max(1u, (Rc + 32 * RPT - 1) / (32 * RPT))), nbt = NB * 32;
+  uint32_t rrow[RPT], rpos[RPT];
   uint64_t rpw[RPT], rcb[RPT];
   uint32_t T = 0;
   if (warp < NB) {
 #pragma unroll
     for (uint32_t k = 0; k < RPT; k++) {
-      const uint32_t r = tid + k * nbt;
-      rpos[k] = r < R ? a.pos[r] : 0xFFFFFFFFu;
-      rpw[k] = r < R ? a.xzs[(size_t)r * W + wj] : 0ull;
+      const uint32_t j = tid + k * nbt;
+      rrow[k] = j < Rc ? cand[j] : 0xFFFFFFFFu;
+      rpos[k] = j < Rc ? a.pos[rrow[k]] : 0xFFFFFFFFu;
+      rpw[k] = j < Rc ? a.xzs[(size_t)rrow[k] * W + wj] : 0ull;
       rcb[k] = 0;
     }
     // the steps (as blocked_body): one named barrier among the search warps per column
@@ -923,8 +934,8 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
       uint32_t bpos = 0xFFFFFFFFu, bk = 0;
 #pragma unroll
       for (uint32_t k = 0; k < RPT; k++) {
-        const uint32_t r = tid + k * nbt;
-        if (r >= R) continue;
+        const uint32_t r = rrow[k];
+        if (r == 0xFFFFFFFFu) continue;
         if (prev && r != pprev && ((rpw[k] >> bprev) & 1ull)) {
           rpw[k] ^= pwprev;
           rcb[k] ^= aprev;
@@ -939,7 +950,11 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
         const uint32_t m = __reduce_min_sync(0xFFFFFFFFu, bpos);
         const uint32_t who = __ballot_sync(0xFFFFFFFFu, bpos == m);
         const uint32_t src = __ffs(who) - 1;
-        const uint32_t row = __shfl_sync(0xFFFFFFFFu, tid + bk * nbt, src);
+        uint32_t myrow = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < RPT; k++)
+          if (k == bk) myrow = rrow[k];
+        const uint32_t row = __shfl_sync(0xFFFFFFFFu, myrow, src);
         const uint64_t wpw = __shfl_sync(0xFFFFFFFFu, mypw, src);
         const uint64_t wcb = __shfl_sync(0xFFFFFFFFu, mycb, src);
         if (lane == 0) {
@@ -961,9 +976,9 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
       aprev = red2[b & 1][kw][2] | (1ull << T);
 #pragma unroll
       for (uint32_t k = 0; k < RPT; k++) {
-        const uint32_t r = tid + k * nbt;
+        const uint32_t r = rrow[k];
         if (r == pstar) rpos[k] = i;
-        else if (r < R && rpos[k] == i) rpos[k] = kpos;
+        else if (r != 0xFFFFFFFFu && rpos[k] == i) rpos[k] = kpos;
       }
       if (tid == 0) {
         stp[T] = pstar;
@@ -978,10 +993,8 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
       i++;
     }
 #pragma unroll
-    for (uint32_t k = 0; k < RPT; k++) {
-      const uint32_t r = tid + k * nbt;
-      if (r < R) a.pos[r] = rpos[k];
-    }
+    for (uint32_t k = 0; k < RPT; k++)
+      if (rrow[k] != 0xFFFFFFFFu) a.pos[rrow[k]] = rpos[k];
     if (tid == 0) { shT = T; shI = i; }
   }
   __syncthreads();
@@ -1286,6 +1299,8 @@ static int launch_blocked(const ElimSpec& e, cudaStream_t st) {
 }
 
 static uint32_t g_canon_grid = 0;  // 0: automatic, 1: always, 2: never (panels over the whole GPU)
+static uint32_t g_canon_rpt = 0;         // tuner: rows per search thread (0: automatic; 4, 8, 16)
+static uint32_t g_canon_apply_rows = 0;  // tuner: rows per apply CTA (0: automatic)
 // Smallest stabilizer view that runs by panels over the whole GPU (below it,
 // one cluster holds the rows in shared memory).
 constexpr uint32_t CANON_GRID_MIN_ROWS = 1024;
@@ -1305,16 +1320,25 @@ static int launch_grid(const ElimSpec& e, cudaStream_t st) {
   QCB_CUDA(cudaMallocAsync(&gtmp_ph, R, st));
   canon_grid_init_kernel<<<(R + 255) / 256, 256, 0, st>>>(pos, R, rec);
   QCB_LAUNCHED();
-  void (*search)(const PanelArgs) = R <= 4096 ? canon_search_kernel<4> : canon_search_kernel<8>;
-  const size_t search_smem = (size_t)len * PANEL * 8;
-  if (search_smem > 48 * 1024)
-    QCB_CUDA(cudaFuncSetAttribute(search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_smem));
-  const uint32_t G = std::max<uint32_t>(1, std::min<uint32_t>((R + 15) / 16, 2 * (uint32_t)device_sm_count()));
+  // rows per search thread: at least enough for the rows in 1024 threads
+  // (the fewest that fit the 1024 threads: fewer rows a thread was faster,
+  // n = 2000: 4 / 8 / 16 rows 3.10 / 3.72 / 7.00 ms)
+  uint32_t rpt = g_canon_rpt ? g_canon_rpt : 1u;
+  while (rpt * CANON_THREADS < R) rpt *= 2;
+  void (*search)(const PanelArgs) = rpt == 1 ? canon_search_kernel<1>
+                                  : rpt == 2 ? canon_search_kernel<2>
+                                  : rpt == 4 ? canon_search_kernel<4>
+                                  : rpt == 8 ? canon_search_kernel<8> : canon_search_kernel<16>;
+  const size_t search_smem = (size_t)len * PANEL * 8 + (size_t)R * 4;
+  // opt in always: the static shared memory counts against the default 48 KB too
+  QCB_CUDA(cudaFuncSetAttribute(search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_smem));
+  const uint32_t rows_per_cta = g_canon_apply_rows ? g_canon_apply_rows : 16u;
+  const uint32_t G = std::max<uint32_t>(1, std::min<uint32_t>((R + rows_per_cta - 1) / rows_per_cta,
+                                                              2 * (uint32_t)device_sm_count()));
   const uint32_t per = (R + G - 1) / G;
   const uint32_t threads = std::min<uint32_t>(CANON_THREADS, std::max<uint32_t>(64, 32 * per));
   const size_t apply_smem = (size_t)PANEL * W * 8 + (size_t)per * 9 + 16;
-  if (apply_smem > 48 * 1024)
-    QCB_CUDA(cudaFuncSetAttribute(canon_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
+  QCB_CUDA(cudaFuncSetAttribute(canon_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
   PanelArgs a{};
   a.xzs = e.xzs; a.ph = e.ph; a.rows = R; a.n = e.n; a.W = W; a.phases = e.phases;
   a.pos = pos; a.rec = rec; a.po = po; a.out = e.d_out;
@@ -1466,6 +1490,8 @@ void set_canon_cluster(uint32_t cs) { g_canon_cs = cs; }
 void set_canon_threads(uint32_t n) { g_canon_threads = n; }
 void set_canon_blocked(uint32_t v) { g_canon_blocked = v; }
 void set_canon_grid(uint32_t v) { g_canon_grid = v; }
+void set_canon_rpt(uint32_t v) { g_canon_rpt = v; }
+void set_canon_apply_rows(uint32_t v) { g_canon_apply_rows = v; }
 
 }  // namespace qcb
 

@@ -57,6 +57,8 @@ void set_canon_threads(uint32_t n);
 void set_project_cluster(uint32_t cs);
 void set_canon_blocked(uint32_t v);
 void set_canon_grid(uint32_t v);
+void set_canon_rpt(uint32_t v);
+void set_canon_apply_rows(uint32_t v);
 
 }  // namespace qcb
 
@@ -146,6 +148,13 @@ int qcb_tune_set(const char* key, int64_t value) {
     // canonicalize! by panels over the whole GPU: 0 from 1024 rows, 1 always, 2 never
     if (value > 2) return fail(QCB_EARG, "canon_grid must be 0 (automatic), 1 (always) or 2 (never)");
     set_canon_grid((uint32_t)value);
+  } else if (k == "canon_rpt") {
+    if (value && value != 1 && value != 2 && value != 4 && value != 8 && value != 16)
+      return fail(QCB_EARG, "canon_rpt must be 0, 1, 2, 4, 8 or 16");
+    set_canon_rpt((uint32_t)value);
+  } else if (k == "canon_apply_rows") {
+    if (value && (value < 8 || value > 32)) return fail(QCB_EARG, "canon_apply_rows must be 0 or 8..32");
+    set_canon_apply_rows((uint32_t)value);
   } else if (k == "project_cluster") {
     if (value && (value > 16 || (value & (value - 1)))) return fail(QCB_EARG, "project_cluster must be 1, 2, 4, 8 or 16");
     set_project_cluster((uint32_t)value);

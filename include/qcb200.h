@@ -249,11 +249,13 @@ int qcb_tune_tile(const qcb_program* program, uint32_t* tile, float* us_per_colu
  * Requests (an op list, shots, seed) are submitted at any time from any host
  * thread; their programs are compiled once per distinct op list and stay
  * resident.  A scheduler thread admits requests first come, first served as
- * a slot (a CUDA stream) and the HBM budget (the full record plus one shot
- * chunk's frame planes from a pool) allow, and runs each as a sequence of
- * fresh Philox shot chunks of `chunk_shots` (0 = 2^20), so requests overlap
- * on the device chunk by chunk; every record equals that of one plain run
- * of the request (qcb_pftrajectories_fresh, same seed, shot_offset 0).
+ * a slot (a CUDA stream), the HBM budget (the full record plus one shot
+ * chunk's frame planes from a pool) and the GPU's fill allow (the running
+ * requests' remaining walker CTAs leave SMs idle: small requests and the
+ * last chunk of a large one share the GPU, large ones run in arrival order),
+ * and runs each as a sequence of fresh Philox shot chunks of `chunk_shots`
+ * (0 = 2^20), two in flight; every record equals that of one plain run of
+ * the request (qcb_pftrajectories_fresh, same seed, shot_offset 0).
  * Records stay on the device until qcb_server_release.                   */
 typedef struct qcb_server qcb_server;
 int qcb_server_create(uint64_t hbm_budget_bytes, uint32_t slots, uint64_t chunk_shots, qcb_server** out);
@@ -333,7 +335,8 @@ int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t see
  * faults); a fresh run or initZ! of the frame clears that status.  Test
  * knob "server_hash_bits" b > 0: the serving program cache keeps only b low
  * bits of its hash, so distinct circuits collide (the byte comparison on a
- * hit keeps results right).                                                */
+ * hit keeps results right).  Knob "server_fill" (read by qcb_server_create):
+ * 1 (default) admits onto idle SMs only, 0 whenever a slot is free.         */
 int qcb_tune_set(const char* key, int64_t value);
 
 /* ------------------------------------------------------------ tableaux    */

@@ -1847,6 +1847,13 @@ int qcb_tune_tile(const qcb_program* p, uint32_t* tile_out, float* us_per_column
 // columns of the request's full record).  Counters use the global column,
 // so the chunks of a request give the record of one run over all its shots.
 namespace qcb {
+uint32_t chunk_ctas(const qcb_frame* f, const qcb_program* p, uint64_t ncols) {
+  qcb_frame view = *f;
+  view.ncols = ncols;
+  view.frames = ncols * 32;
+  return walk_config(p, &view).grid;
+}
+
 int run_chunk(qcb_frame* f, uint64_t ncols, const qcb_program* p, uint64_t seed, uint64_t shot_offset, uint32_t* rec,
               uint64_t rec_pitch, cudaStream_t st) {
   if (!f || !p || !rec) return fail(QCB_EARG, "null argument");

@@ -194,6 +194,8 @@ struct qcb_frame {
 namespace qcb {
 int run_chunk(qcb_frame* f, uint64_t ncols, const qcb_program* p, uint64_t seed, uint64_t shot_offset, uint32_t* rec,
               uint64_t rec_pitch, cudaStream_t st);
+// CTAs of the walker launch that run_chunk makes for `ncols` columns.
+uint32_t chunk_ctas(const qcb_frame* f, const qcb_program* p, uint64_t ncols);
 }  // namespace qcb
 
 struct qcb_tableau {

@@ -57,6 +57,7 @@ void set_canon_threads(uint32_t n);
 void set_project_cluster(uint32_t cs);
 void set_canon_blocked(uint32_t v);
 void set_canon_grid(uint32_t v);
+void set_server_fill(uint32_t v);
 void set_canon_rpt(uint32_t v);
 void set_canon_apply_rows(uint32_t v);
 
@@ -132,6 +133,11 @@ int qcb_tune_set(const char* key, int64_t value) {
     // its hash (0: all), so that distinct circuits collide
     if (value > 64) return fail(QCB_EARG, "server_hash_bits must be 0..64");
     set_server_hash_bits((uint32_t)value);
+  } else if (k == "server_fill") {
+    // serving admission: 1 (default) onto idle SMs only, 0 whenever a slot is
+    // free; read when a server is created
+    if (value > 1) return fail(QCB_EARG, "server_fill must be 0 or 1");
+    set_server_fill((uint32_t)value);
   } else if (k == "walker_threads") {
     if (value && (value < 64 || value > 640 || value % 32)) return fail(QCB_EARG, "walker_threads must be 0 (640) or 64..640, a multiple of 32");
     set_walker_threads((uint32_t)value);

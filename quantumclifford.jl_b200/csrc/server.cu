@@ -6,17 +6,22 @@
 // the op bytes, compared in full on a hash hit; programs count against the
 // HBM budget, and unused ones are evicted least recently used first when it
 // runs short).  Admission is first come, first served against an HBM
-// budget and a number of slots: the head of the queue is admitted as soon as
-// a slot is free and its memory (the full record, plus one chunk's frame
-// planes) fits the budget.  Device memory comes from the stream-ordered
+// budget, a number of slots and the GPU's fill: the head of the queue is
+// admitted as soon as a slot is free, its memory (the full record, plus one
+// chunk's frame planes) fits the budget and the running requests' remaining
+// walker CTAs leave SMs idle (a request with two or more chunks to go fills
+// the GPU; one on its last chunk leaves the SMs that chunk does not use).  Device memory comes from the stream-ordered
 // allocator (cudaMallocAsync / cudaFreeAsync on the slot's stream), so the
 // scheduler thread never waits for the device.  An admitted request runs on its
 // slot's stream as a sequence of shot chunks (fresh Philox runs with the
 // chunk's global shot offset, each writing its columns of the request's
-// record), so requests admitted while others run share the GPU chunk by
-// chunk, and every record equals that of one plain run of the request.  A
-// scheduler thread admits, launches and retires (CUDA events); the caller
-// polls, waits, copies results out and releases them.
+// record; every record equals that of one plain run of the request), two
+// chunks in flight at a time.  So the oldest requests keep the SMs they fill
+// (first come, first served, as serial execution, which bounds the longest
+// waits) and later ones run beside them only on SMs they leave idle: small
+// requests, and the last chunk of a large one.  A scheduler thread admits,
+// launches chunks and retires (CUDA events); the caller polls, waits, copies
+// results out and releases them.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -54,6 +59,10 @@ struct Request {
   uint32_t* record = nullptr;
   qcb_frame* chunk = nullptr;   // the chunk frame (its planes live while the chunks run)
   int slot = -1;
+  cudaStream_t stream = nullptr;  // the slot's stream
+  uint64_t nchunks = 0, launched = 0, finished = 0;  // chunks: total, launched, seen complete
+  uint32_t ctas_full = 0, ctas_last = 0;             // walker CTAs of a full and of the last chunk
+  cudaEvent_t chunk_ev[2] = {nullptr, nullptr};      // completion of chunk k in chunk_ev[k % 2]
   cudaEvent_t done = nullptr;
   double t_submit = 0, t_admit = 0, t_done = 0;
   int32_t state = RQ_QUEUED;
@@ -75,7 +84,9 @@ struct qcb_server {
   uint64_t budget = 0, used = 0;
   uint32_t nslots = 0;
   uint64_t chunk_cols = 0;  // columns per chunk (a multiple of 32: 1024-shot groups)
-  std::vector<cudaStream_t> streams;
+  std::vector<cudaStream_t> streams;  // one per slot
+  bool fill_gate = true;              // admit only onto idle SMs (false: whenever a slot is free)
+  uint32_t capacity = 0;              // walker CTAs the GPU runs at once (one per SM)
   std::vector<int64_t> slot_req;  // request id per slot, -1 when free
   std::map<uint64_t, std::unique_ptr<qcb::Request>> reqs;
   std::deque<uint64_t> queue;
@@ -97,6 +108,12 @@ struct qcb_server {
 };
 
 namespace qcb {
+
+// Admission policy knob: 1 (default) admits a request only while the running
+// ones leave SMs idle, 0 whenever a slot is free (the GPU's block scheduler
+// then interleaves the requests' chunks).
+static uint32_t g_server_fill = 1;
+void set_server_fill(uint32_t v) { g_server_fill = v; }
 
 // Test knob: keep only this many low bits of the program hash (0: all 64),
 // so that distinct circuits collide and the byte comparison decides.
@@ -172,9 +189,73 @@ static uint64_t chunk_plane_bytes(uint32_t nq1, uint64_t chunk_cols) {
   return (uint64_t)2 * (nq1 + 1) * pitch * 4 + (uint64_t)pitch * 4 + 16;
 }
 
-// Admit the head of the queue while a slot and the budget allow (called
-// with the lock held).  Returns after launching every chunk of each admitted
-// request on its slot's stream.
+// Walker CTAs still to run for a running request: a full chunk's while two or
+// more chunks remain (it fills the GPU as serial execution would), the last
+// chunk's while only that one remains, 0 once every chunk has finished.
+static uint64_t remaining_ctas(const Request& r) {
+  const uint64_t left = r.nchunks - r.finished;
+  return left >= 2 ? r.ctas_full : left == 1 ? r.ctas_last : 0;
+}
+
+// After the last chunk: the walker status word to the slot's pinned word,
+// the chunk planes back to the pool and the request's completion event, all
+// in stream order.
+static int finish_launches(qcb_server* s, Request& r) {
+  qcb_frame* cf = r.chunk;
+  int status = r.status;
+  if (status == QCB_OK && cf->err &&
+      cudaMemcpyAsync(&s->slot_status[r.slot], cf->err, 4, cudaMemcpyDeviceToHost, r.stream) != cudaSuccess)
+    status = fail(QCB_ECUDA, "serving: status copy");
+  if (cf->planes) cudaFreeAsync(cf->planes, r.stream);
+  if (cf->err) cudaFreeAsync(cf->err, r.stream);
+  cf->planes = nullptr;
+  cf->err = nullptr;
+  if (cudaEventRecord(r.done, r.stream) != cudaSuccess && status == QCB_OK) status = fail(QCB_ECUDA, "serving: event");
+  return status;
+}
+
+// Launch the request's next chunk on its stream (lock held); after the last
+// one, finish_launches.  A failure ends the launches: the request retires as
+// failed once its stream has drained.
+static void launch_chunk(qcb_server* s, Request& r) {
+  const uint64_t k = r.launched;
+  const uint64_t c0 = k * s->chunk_cols;
+  const uint64_t nc = std::min<uint64_t>(s->chunk_cols, r.ncols - c0);
+  int status = run_chunk(r.chunk, nc, r.prog, r.seed, c0 * 32, r.record + c0, r.rec_pitch, r.stream);
+  if (status == QCB_OK && cudaEventRecord(r.chunk_ev[k % 2], r.stream) != cudaSuccess)
+    status = fail(QCB_ECUDA, "serving: chunk event");
+  r.launched++;
+  if (status != QCB_OK) {
+    r.status = status;
+    r.msg = last_msg();
+    r.launched = r.nchunks;  // no further chunks
+  }
+  if (r.launched == r.nchunks) {
+    const int st = finish_launches(s, r);
+    if (st != QCB_OK && r.status == QCB_OK) {
+      r.status = st;
+      r.msg = last_msg();
+    }
+  }
+}
+
+// Keep two chunks of every running request in flight (lock held): count the
+// chunks seen complete and launch the next while fewer than two are pending.
+static void advance(qcb_server* s) {
+  for (uint32_t k = 0; k < s->nslots; k++) {
+    if (s->slot_req[k] < 0) continue;
+    Request& r = *s->reqs[(uint64_t)s->slot_req[k]];
+    while (r.finished < r.launched && r.status == QCB_OK) {
+      if (cudaEventQuery(r.chunk_ev[r.finished % 2]) != cudaSuccess) break;
+      r.finished++;
+    }
+    while (r.launched < r.nchunks && r.launched - r.finished < 2) launch_chunk(s, r);
+  }
+}
+
+// Admit the head of the queue while a slot, the budget and the GPU's fill
+// allow (called with the lock held), launching the first two chunks of each
+// admitted request on its slot's stream.
 static void admit(qcb_server* s) {
   while (!s->queue.empty()) {
     int slot = -1;
@@ -198,9 +279,17 @@ static void admit(qcb_server* s) {
       s->done_cv.notify_all();
       continue;
     }
+    bool running = false;
+    uint64_t busy = 0;
+    for (int64_t v : s->slot_req) {
+      if (v < 0) continue;
+      running = true;
+      busy += remaining_ctas(*s->reqs[(uint64_t)v]);
+    }
+    // the SMs are taken (balanced tiles leave a wave a few CTAs short of the
+    // SM count, so fewer than 1/16 idle counts as full): wait, in order
+    if (s->fill_gate && running && busy + s->capacity / 16 > s->capacity) return;
     if (s->used + r.bytes > s->budget && !evict_programs(s, r.bytes)) {
-      bool running = false;
-      for (int64_t v : s->slot_req) running |= v >= 0;
       if (running) return;  // first come, first served: wait for memory
       // nothing runs and nothing more can be evicted: the resident programs
       // of queued requests leave no room for this one
@@ -215,6 +304,8 @@ static void admit(qcb_server* s) {
     }
     const uint32_t nq1 = std::max<uint32_t>(r.prog->nq, 1);
     cudaStream_t st = s->streams[slot];
+    r.stream = st;
+    r.slot = slot;
     // the chunk frame: planes for one chunk, allocated and freed in stream
     // order (no device-wide synchronisation on the scheduler thread)
     qcb_frame* cf = new qcb_frame();
@@ -228,55 +319,53 @@ static void admit(qcb_server* s) {
     cf->record = nullptr;
     cf->err = nullptr;
     r.chunk = cf;
+    r.nchunks = (r.ncols + s->chunk_cols - 1) / s->chunk_cols;
+    r.launched = r.finished = 0;
+    r.ctas_full = chunk_ctas(cf, r.prog, std::min<uint64_t>(s->chunk_cols, r.ncols));
+    r.ctas_last = chunk_ctas(cf, r.prog, r.ncols - (r.nchunks - 1) * s->chunk_cols);
     cudaError_t e = cudaMallocAsync(&cf->planes, (size_t)2 * (nq1 + 1) * cf->pitch * 4, st);
     if (e == cudaSuccess) e = cudaMallocAsync(&cf->err, 16, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(cf->err, 0, 16, st);
     if (e == cudaSuccess) e = cudaMallocAsync(&r.record, r.nbits * r.rec_pitch * 4, st);
+    for (int j = 0; j < 2 && e == cudaSuccess; j++)
+      if (!r.chunk_ev[j]) e = cudaEventCreateWithFlags(&r.chunk_ev[j], cudaEventDisableTiming);
     if (e == cudaSuccess && !r.done) e = cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming);
-    int status = e == cudaSuccess ? QCB_OK : cuda_fail(e, "serving: admission");
-    for (uint64_t c0 = 0; status == QCB_OK && c0 < r.ncols; c0 += s->chunk_cols) {
-      const uint64_t nc = std::min<uint64_t>(s->chunk_cols, r.ncols - c0);
-      status = run_chunk(r.chunk, nc, r.prog, r.seed, c0 * 32, r.record + c0, r.rec_pitch, st);
-    }
-    if (status == QCB_OK &&
-        cudaMemcpyAsync(&s->slot_status[slot], cf->err, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
-      status = fail(QCB_ECUDA, "serving: status copy");
-    if (cf->planes) cudaFreeAsync(cf->planes, st);
-    if (cf->err) cudaFreeAsync(cf->err, st);
-    cf->planes = nullptr;
-    cf->err = nullptr;
-    if (status == QCB_OK && cudaEventRecord(r.done, st) != cudaSuccess) status = fail(QCB_ECUDA, "serving: event");
     s->queue.pop_front();
     r.t_admit = s->now();
-    if (status != QCB_OK) {
+    if (e != cudaSuccess) {
+      r.status = cuda_fail(e, "serving: admission");
       r.msg = last_msg();
+      if (cf->planes) cudaFreeAsync(cf->planes, st);
+      if (cf->err) cudaFreeAsync(cf->err, st);
       if (r.record) cudaFreeAsync(r.record, st);
       r.record = nullptr;
       delete r.chunk;
       r.chunk = nullptr;
-      r.state = RQ_FAILED; r.status = status; r.t_done = s->now();
+      r.slot = -1;
+      r.state = RQ_FAILED; r.t_done = s->now();
       s->completed.push_back(r.id);
       s->done_cv.notify_all();
       continue;
     }
-    r.slot = slot;
     r.state = RQ_RUNNING;
     s->slot_req[slot] = (int64_t)r.id;
     s->used += r.bytes;
+    while (r.launched < r.nchunks && r.launched < 2) launch_chunk(s, r);
   }
 }
 
-// Retire the running requests whose last chunk has finished (lock held):
-// their chunk planes were freed in stream order, their records stay until
-// released.
+// Retire the running requests whose launches have all been made and whose
+// stream has drained (lock held): their chunk planes were freed in stream
+// order, their records stay until released.
 static void retire(qcb_server* s) {
   for (uint32_t k = 0; k < s->nslots; k++) {
     if (s->slot_req[k] < 0) continue;
     Request& r = *s->reqs[(uint64_t)s->slot_req[k]];
+    if (r.launched < r.nchunks) continue;
     const cudaError_t q = cudaEventQuery(r.done);
     if (q == cudaErrorNotReady) continue;
     r.t_done = s->now();
-    r.state = q == cudaSuccess ? RQ_DONE : RQ_FAILED;
+    r.state = q == cudaSuccess && r.status == QCB_OK ? RQ_DONE : RQ_FAILED;
     if (q != cudaSuccess) {
       r.status = cuda_fail(q, "serving: request");
       r.msg = last_msg();
@@ -287,6 +376,8 @@ static void retire(qcb_server* s) {
       r.status = h;
       r.msg = "serving: a device-side wait of the frame walker expired; the record is not valid";
     }
+    s->slot_status[k] = 0;
+    r.finished = r.nchunks;
     delete r.chunk;
     r.chunk = nullptr;
     // the chunk planes leave the request's charge; the record stays charged
@@ -302,6 +393,7 @@ static void scheduler(qcb_server* s) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
   while (!s->stop) {
+    advance(s);
     retire(s);
     admit(s);
     bool running = false;
@@ -337,6 +429,8 @@ int qcb_server_create(uint64_t hbm_budget_bytes, uint32_t slots, uint64_t chunk_
     QCB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     s->streams.push_back(st);
   }
+  s->fill_gate = g_server_fill != 0;
+  s->capacity = (uint32_t)std::max(device_sm_count(), 1);
   // keep freed record memory in the stream-ordered pool up to the budget
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
@@ -482,10 +576,12 @@ int qcb_server_release(qcb_server* s, uint64_t ticket) {
     Request& r = *it->second;
     if (r.state < RQ_DONE) return fail(QCB_EARG, "serving: request still queued or running");
     if (r.record) {
-      cudaFreeAsync(r.record, s->streams[r.slot >= 0 ? r.slot : 0]);  // the request's work is complete
+      cudaFreeAsync(r.record, r.stream ? r.stream : s->streams[0]);  // the request's work is complete
       s->used -= r.bytes;
     }
     if (r.done) cudaEventDestroy(r.done);
+    for (cudaEvent_t ev : r.chunk_ev)
+      if (ev) cudaEventDestroy(ev);
     if (r.cached && r.cached->refs) r.cached->refs--;
     for (auto c = s->completed.begin(); c != s->completed.end(); ++c)
       if (*c == ticket) { s->completed.erase(c); break; }  // released without being reported
@@ -517,6 +613,8 @@ int qcb_server_destroy(qcb_server* s) {
     if (kv.second->record) cudaFree(kv.second->record);
     delete kv.second->chunk;
     if (kv.second->done) cudaEventDestroy(kv.second->done);
+    for (cudaEvent_t ev : kv.second->chunk_ev)
+      if (ev) cudaEventDestroy(ev);
   }
   if (s->slot_status) cudaFreeHost(s->slot_status);
   for (auto& kv : s->programs) qcb_program_destroy(kv.second->prog);

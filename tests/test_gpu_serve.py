@@ -156,3 +156,33 @@ def test_programs_count_against_the_budget(qcb):
     srv.release(t)
     assert srv.stats()[0] == srv.stats()[1]
     srv.close()
+
+
+@pytest.mark.parametrize("fill", [1, 0])
+def test_fill_gate_keeps_large_requests_in_order(qcb, fill):
+    """server_fill 1: a request behind one whose chunks fill the GPU (eight
+    full-width chunks of 2^17 shots, 147 CTAs each) is admitted only when
+    that one has finished; server_fill 0 admits it at once.  Records equal
+    the plain runs either way."""
+    big = circuits.rotated_surface_code_memory(5, 5, 1e-3)
+    small = circuits.rotated_surface_code_memory(3, 3, 1e-3)
+    qcb.check(qcb.lib().qcb_tune_set(b"server_fill", fill))
+    try:
+        srv = qcb.Server(hbm_budget_bytes=8 << 30, slots=4, chunk_shots=1 << 17)
+    finally:
+        qcb.check(qcb.lib().qcb_tune_set(b"server_fill", 1))
+    tb = srv.submit(big, 8 << 17, 5)
+    ts = srv.submit(small, 2000, 6)
+    srv.wait(tb)
+    srv.wait(ts)
+    done_big = srv.query(tb)[1][2]
+    admit_small = srv.query(ts)[1][1]
+    if fill:
+        assert admit_small >= done_big
+    else:
+        assert admit_small < done_big
+    assert np.array_equal(srv.result(tb, 8 << 17), plain_record(qcb, big, 8 << 17, 5))
+    assert np.array_equal(srv.result(ts, 2000), plain_record(qcb, small, 2000, 6))
+    srv.release(tb)
+    srv.release(ts)
+    srv.close()

@@ -1153,13 +1153,38 @@ static uint32_t g_threads_override = 0;  // threads per CTA (0: WALKER_THREADS)
 // Tile width (even: threads own column pairs) for ncols columns with tiles of
 // at most tmax columns: the fewest waves of one CTA per SM, then the narrowest
 // tile that still needs no more waves, so that the last wave is as full as
-// the others.
+// the others.  (The walker on HBM planes.)
 static uint32_t balanced_tile(uint64_t ncols, uint32_t tmax) {
   tmax &= ~1u;
   const uint64_t nsm = (uint64_t)std::max(device_sm_count(), 1);
   const uint64_t waves = std::max<uint64_t>(1, (ncols + nsm * tmax - 1) / (nsm * tmax));
   const uint64_t t = ((ncols + nsm * waves - 1) / (nsm * waves) + 1) & ~1ull;
   return (uint32_t)std::min<uint64_t>(tmax, std::max<uint64_t>(t, 16));
+}
+
+// Tile width of the shared-memory walker: the even width in [16, tmax] with
+// the least waves x (25 + k T), the cost model of a CTA that these launches
+// fit (a fixed part worth about 25 columns, the program's walk, and a part
+// per column), with k = 0.75 for power-of-two widths, whose warps' column
+// pairs cover whole rows of the tile and so meet no shared-memory bank
+// conflicts, 1.1 for 18 columns (nine pairs a row) and 1 otherwise; ties go
+// to the wider tile.  Measured on surface-code memory circuits (2^21 shots,
+// ms): d = 17: 32 columns 4.53, 42 (fewest waves) 5.29; d = 19: 32 5.98, 34
+// 8.02; d = 21: 28 14.36, 16 16.75; d = 23: 22 20.21, 16 20.73; d = 25: 16
+// 24.77, 18 28.69; d = 15 (2^22 shots): 56 7.96, 32 9.90; all of them the
+// model's choice.
+static uint32_t smem_tile(uint64_t ncols, uint32_t tmax) {
+  tmax &= ~1u;
+  const uint64_t nsm = (uint64_t)std::max(device_sm_count(), 1);
+  uint32_t best = 16;
+  uint64_t best_cost = UINT64_MAX;
+  for (uint32_t t = 16; t <= tmax; t += 2) {
+    const uint64_t waves = ((ncols + t - 1) / t + nsm - 1) / nsm;
+    const uint64_t k = (t & (t - 1)) == 0 ? 75 : t == 18 ? 110 : 100;
+    const uint64_t cost = waves * (2500 + k * t);
+    if (cost <= best_cost) { best = t; best_cost = cost; }
+  }
+  return best;
 }
 
 // Shared-memory tile when 2 planes x 16 columns of every touched qubit fit,
@@ -1174,7 +1199,7 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   if (g_tile_override && per_col * g_tile_override <= budget) {
     T = g_tile_override;
   } else if (budget / per_col >= 16) {
-    T = balanced_tile(f->ncols, (uint32_t)std::min<size_t>(256, budget / per_col));
+    T = smem_tile(f->ncols, (uint32_t)std::min<size_t>(256, budget / per_col));
   }
   const uint32_t threads = g_threads_override ? g_threads_override : WALKER_THREADS;
   if (T) {
@@ -1847,11 +1872,20 @@ int qcb_tune_tile(const qcb_program* p, uint32_t* tile_out, float* us_per_column
 // columns of the request's full record).  Counters use the global column,
 // so the chunks of a request give the record of one run over all its shots.
 namespace qcb {
-uint32_t chunk_ctas(const qcb_frame* f, const qcb_program* p, uint64_t ncols) {
-  qcb_frame view = *f;
+uint64_t chunk_presample_bytes(const qcb_program* p, uint64_t ncols) {
+  qcb_frame view{};
   view.ncols = ncols;
   view.frames = ncols * 32;
-  return walk_config(p, &view).grid;
+  return presample_bytes(&view, p);
+}
+
+void chunk_shape(const qcb_program* p, uint64_t ncols, uint32_t* tile, uint32_t* ctas) {
+  qcb_frame view{};
+  view.ncols = ncols;
+  view.frames = ncols * 32;
+  const WalkConfig wc = walk_config(p, &view);
+  if (tile) *tile = wc.T;
+  if (ctas) *ctas = wc.grid;
 }
 
 int run_chunk(qcb_frame* f, uint64_t ncols, const qcb_program* p, uint64_t seed, uint64_t shot_offset, uint32_t* rec,

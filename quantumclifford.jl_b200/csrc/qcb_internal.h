@@ -194,8 +194,13 @@ struct qcb_frame {
 namespace qcb {
 int run_chunk(qcb_frame* f, uint64_t ncols, const qcb_program* p, uint64_t seed, uint64_t shot_offset, uint32_t* rec,
               uint64_t rec_pitch, cudaStream_t st);
-// CTAs of the walker launch that run_chunk makes for `ncols` columns.
-uint32_t chunk_ctas(const qcb_frame* f, const qcb_program* p, uint64_t ncols);
+// Tile width and CTAs of the walker launch that run_chunk makes for `ncols`
+// columns of program p.
+void chunk_shape(const qcb_program* p, uint64_t ncols, uint32_t* tile, uint32_t* ctas);
+// Bytes of noise pre-sampler scratch a chunk of `ncols` columns of program p
+// uses (0: its noise is drawn in the walk); a chunk frame that holds at least
+// that much at `pre` (pre_own false) gets its noise pre-sampled.
+uint64_t chunk_presample_bytes(const qcb_program* p, uint64_t ncols);
 }  // namespace qcb
 
 struct qcb_tableau {

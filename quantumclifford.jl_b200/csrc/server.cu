@@ -60,6 +60,8 @@ struct Request {
   qcb_frame* chunk = nullptr;   // the chunk frame (its planes live while the chunks run)
   int slot = -1;
   cudaStream_t stream = nullptr;  // the slot's stream
+  uint64_t chunk_w = 0;                              // columns per chunk (whole walker waves)
+  uint64_t chunk_bytes = 0;                          // chunk planes + noise pre-sampler scratch
   uint64_t nchunks = 0, launched = 0, finished = 0;  // chunks: total, launched, seen complete
   uint32_t ctas_full = 0, ctas_last = 0;             // walker CTAs of a full and of the last chunk
   cudaEvent_t chunk_ev[2] = {nullptr, nullptr};      // completion of chunk k in chunk_ev[k % 2]
@@ -207,8 +209,11 @@ static int finish_launches(qcb_server* s, Request& r) {
       cudaMemcpyAsync(&s->slot_status[r.slot], cf->err, 4, cudaMemcpyDeviceToHost, r.stream) != cudaSuccess)
     status = fail(QCB_ECUDA, "serving: status copy");
   if (cf->planes) cudaFreeAsync(cf->planes, r.stream);
+  if (cf->pre) cudaFreeAsync(cf->pre, r.stream);
   if (cf->err) cudaFreeAsync(cf->err, r.stream);
   cf->planes = nullptr;
+  cf->pre = nullptr;
+  cf->pre_bytes = 0;
   cf->err = nullptr;
   if (cudaEventRecord(r.done, r.stream) != cudaSuccess && status == QCB_OK) status = fail(QCB_ECUDA, "serving: event");
   return status;
@@ -219,8 +224,8 @@ static int finish_launches(qcb_server* s, Request& r) {
 // failed once its stream has drained.
 static void launch_chunk(qcb_server* s, Request& r) {
   const uint64_t k = r.launched;
-  const uint64_t c0 = k * s->chunk_cols;
-  const uint64_t nc = std::min<uint64_t>(s->chunk_cols, r.ncols - c0);
+  const uint64_t c0 = k * r.chunk_w;
+  const uint64_t nc = std::min<uint64_t>(r.chunk_w, r.ncols - c0);
   int status = run_chunk(r.chunk, nc, r.prog, r.seed, c0 * 32, r.record + c0, r.rec_pitch, r.stream);
   if (status == QCB_OK && cudaEventRecord(r.chunk_ev[k % 2], r.stream) != cudaSuccess)
     status = fail(QCB_ECUDA, "serving: chunk event");
@@ -253,6 +258,20 @@ static void advance(qcb_server* s) {
   }
 }
 
+// Columns per chunk of a request: all of them when they fit the server's
+// chunk width, else the nearest whole number of walker waves (one tile per
+// SM) to it that is a whole number of 1024-shot groups, so that no chunk but
+// the last ends on a mostly empty wave.
+static uint64_t chunk_width(const qcb_server* s, const Request& r) {
+  if (r.ncols <= s->chunk_cols) return r.ncols;
+  uint32_t T = 0;
+  chunk_shape(r.prog, s->chunk_cols, &T, nullptr);
+  uint64_t unit = (uint64_t)s->capacity * std::max<uint32_t>(T, 1);
+  while (unit % 32) unit *= 2;
+  const uint64_t k = std::max<uint64_t>(1, (s->chunk_cols + unit / 2) / unit);
+  return std::min(k * unit, r.ncols);
+}
+
 // Admit the head of the queue while a slot, the budget and the GPU's fill
 // allow (called with the lock held), launching the first two chunks of each
 // admitted request on its slot's stream.
@@ -267,7 +286,10 @@ static void admit(qcb_server* s) {
       r.nbits = std::max<uint32_t>(r.prog->info.nbits, 1);
       r.ncols = (r.shots + 31) / 32;
       r.rec_pitch = std::max<uint64_t>(32, (r.ncols + 31) / 32 * 32);
-      r.bytes = r.nbits * r.rec_pitch * 4 + chunk_plane_bytes(std::max<uint32_t>(r.prog->nq, 1), s->chunk_cols);
+      r.chunk_w = chunk_width(s, r);
+      r.chunk_bytes = chunk_plane_bytes(std::max<uint32_t>(r.prog->nq, 1), r.chunk_w) +
+                      chunk_presample_bytes(r.prog, r.chunk_w);
+      r.bytes = r.nbits * r.rec_pitch * 4 + r.chunk_bytes;
     }
     if (r.bytes > s->budget) {
       r.state = RQ_FAILED;
@@ -309,21 +331,26 @@ static void admit(qcb_server* s) {
     // the chunk frame: planes for one chunk, allocated and freed in stream
     // order (no device-wide synchronisation on the scheduler thread)
     qcb_frame* cf = new qcb_frame();
-    cf->frames = s->chunk_cols * 32;
+    cf->frames = r.chunk_w * 32;
     cf->qubits = nq1 - 1;
     cf->nq1 = nq1;
     cf->nbits = 0;
-    cf->ncols = s->chunk_cols;
-    cf->pitch = std::max<uint64_t>(32, (s->chunk_cols + 31) / 32 * 32);
+    cf->ncols = r.chunk_w;
+    cf->pitch = std::max<uint64_t>(32, (r.chunk_w + 31) / 32 * 32);
     cf->planes = nullptr;
     cf->record = nullptr;
     cf->err = nullptr;
     r.chunk = cf;
-    r.nchunks = (r.ncols + s->chunk_cols - 1) / s->chunk_cols;
+    r.nchunks = (r.ncols + r.chunk_w - 1) / r.chunk_w;
     r.launched = r.finished = 0;
-    r.ctas_full = chunk_ctas(cf, r.prog, std::min<uint64_t>(s->chunk_cols, r.ncols));
-    r.ctas_last = chunk_ctas(cf, r.prog, r.ncols - (r.nchunks - 1) * s->chunk_cols);
+    chunk_shape(r.prog, r.chunk_w, nullptr, &r.ctas_full);
+    chunk_shape(r.prog, r.ncols - (r.nchunks - 1) * r.chunk_w, nullptr, &r.ctas_last);
     cudaError_t e = cudaMallocAsync(&cf->planes, (size_t)2 * (nq1 + 1) * cf->pitch * 4, st);
+    const uint64_t pre = chunk_presample_bytes(r.prog, r.chunk_w);
+    if (e == cudaSuccess && pre) {
+      e = cudaMallocAsync(&cf->pre, pre, st);
+      if (e == cudaSuccess) cf->pre_bytes = pre;
+    }
     if (e == cudaSuccess) e = cudaMallocAsync(&cf->err, 16, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(cf->err, 0, 16, st);
     if (e == cudaSuccess) e = cudaMallocAsync(&r.record, r.nbits * r.rec_pitch * 4, st);
@@ -336,6 +363,7 @@ static void admit(qcb_server* s) {
       r.status = cuda_fail(e, "serving: admission");
       r.msg = last_msg();
       if (cf->planes) cudaFreeAsync(cf->planes, st);
+      if (cf->pre) cudaFreeAsync(cf->pre, st);
       if (cf->err) cudaFreeAsync(cf->err, st);
       if (r.record) cudaFreeAsync(r.record, st);
       r.record = nullptr;
@@ -381,8 +409,8 @@ static void retire(qcb_server* s) {
     delete r.chunk;
     r.chunk = nullptr;
     // the chunk planes leave the request's charge; the record stays charged
-    s->used -= chunk_plane_bytes(std::max<uint32_t>(r.prog->nq, 1), s->chunk_cols);
-    r.bytes -= chunk_plane_bytes(std::max<uint32_t>(r.prog->nq, 1), s->chunk_cols);
+    s->used -= r.chunk_bytes;
+    r.bytes -= r.chunk_bytes;
     s->slot_req[k] = -1;
     s->completed.push_back(r.id);
     s->done_cv.notify_all();
@@ -431,11 +459,25 @@ int qcb_server_create(uint64_t hbm_budget_bytes, uint32_t slots, uint64_t chunk_
   }
   s->fill_gate = g_server_fill != 0;
   s->capacity = (uint32_t)std::max(device_sm_count(), 1);
-  // keep freed record memory in the stream-ordered pool up to the budget
+  // keep this server's budget in the stream-ordered pool (the release
+  // threshold grows by the budget while the server lives) and map it now:
+  // growing the pool during serving maps fresh memory on the scheduler
+  // thread (tens of ms for a multi-GB record) while it holds the lock
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
-    uint64_t thr = hbm_budget_bytes;
+    uint64_t thr = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    thr = thr > UINT64_MAX - hbm_budget_bytes ? UINT64_MAX : thr + hbm_budget_bytes;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const uint64_t reserve = std::min<uint64_t>(hbm_budget_bytes, free_b > (1ull << 30) ? free_b - (1ull << 30) : 0);
+    void* p = nullptr;
+    if (reserve && cudaMallocAsync(&p, reserve, s->streams[0]) == cudaSuccess) {
+      cudaFreeAsync(p, s->streams[0]);
+      cudaStreamSynchronize(s->streams[0]);
+    }
+    cudaGetLastError();  // a reservation that did not fit is not an error
   }
   s->t0 = std::chrono::steady_clock::now();
   qcb_server* raw = s.get();
@@ -619,6 +661,13 @@ int qcb_server_destroy(qcb_server* s) {
   if (s->slot_status) cudaFreeHost(s->slot_status);
   for (auto& kv : s->programs) qcb_program_destroy(kv.second->prog);
   for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+    uint64_t thr = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    thr = thr > s->budget ? thr - s->budget : 0;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
   delete s;
   return QCB_OK;
 }

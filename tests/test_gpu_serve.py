@@ -160,10 +160,10 @@ def test_programs_count_against_the_budget(qcb):
 
 @pytest.mark.parametrize("fill", [1, 0])
 def test_fill_gate_keeps_large_requests_in_order(qcb, fill):
-    """server_fill 1: a request behind one whose chunks fill the GPU (eight
-    full-width chunks of 2^17 shots, 147 CTAs each) is admitted only when
-    that one has finished; server_fill 0 admits it at once.  Records equal
-    the plain runs either way."""
+    """server_fill 1: a request behind one whose chunks fill the GPU (2^20
+    shots in chunks of whole walker waves near 2^17 shots) waits until that
+    one is on its last chunk, which may leave SMs idle; server_fill 0 admits
+    it at once.  Records equal the plain runs either way."""
     big = circuits.rotated_surface_code_memory(5, 5, 1e-3)
     small = circuits.rotated_surface_code_memory(3, 3, 1e-3)
     qcb.check(qcb.lib().qcb_tune_set(b"server_fill", fill))
@@ -175,12 +175,15 @@ def test_fill_gate_keeps_large_requests_in_order(qcb, fill):
     ts = srv.submit(small, 2000, 6)
     srv.wait(tb)
     srv.wait(ts)
-    done_big = srv.query(tb)[1][2]
+    _, admit_big, done_big = srv.query(tb)[1]
     admit_small = srv.query(ts)[1][1]
+    # the big request runs 7 chunks: fill 1 holds the small one for at least
+    # the first six, fill 0 lets it in while the first runs
+    frac = (admit_small - admit_big) / (done_big - admit_big)
     if fill:
-        assert admit_small >= done_big
+        assert frac > 0.5, frac
     else:
-        assert admit_small < done_big
+        assert frac < 0.5, frac
     assert np.array_equal(srv.result(tb, 8 << 17), plain_record(qcb, big, 8 << 17, 5))
     assert np.array_equal(srv.result(ts, 2000), plain_record(qcb, small, 2000, 6))
     srv.release(tb)

@@ -887,6 +887,10 @@ struct PanelArgs {
 template <uint32_t RPT>
 __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const PanelArgs a) {
   extern __shared__ __align__(16) uint64_t sm[];
+  // launched as a programmatic dependent of the previous panel's apply: wait
+  // for it (complete, its writes visible), then let the next launch in
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
   PanelRec& g = *a.rec;
   if (g.done) {  // every position has its pivot: this panel applies nothing
     if (threadIdx.x == 0) g.T = 0;
@@ -896,13 +900,14 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
   const uint32_t R = a.rows, W = a.W, len = W / 2, n = a.n;
   const uint32_t c0 = a.c0, ncp = min(PANEL, n - c0), wj = a.stage * len + (c0 >> 6);
   uint64_t* XT = sm;                                   // XT[w * PANEL + t] = X word w of pivot t
+  uint64_t* ZT = XT + (size_t)len * PANEL;             // ZT[w * PANEL + t] = Z word w of pivot t
   __shared__ uint32_t stp[PANEL];
   __shared__ uint8_t bt[PANEL], qo[PANEL];
   __shared__ uint64_t A[PANEL], PWP[PANEL], C[PANEL], Dt[PANEL], Us[PANEL];
   __shared__ uint8_t bases[PANEL];
   __shared__ uint64_t red2[2][32][3];
   __shared__ uint32_t shT, shI, ncand;
-  uint32_t* cand = (uint32_t*)(XT + (size_t)len * PANEL);  // the candidate rows (position >= i)
+  uint32_t* cand = (uint32_t*)(ZT + (size_t)len * PANEL);  // the candidate rows (position >= i)
   uint32_t i = g.i;
   // Only rows at positions >= i can become pivots; the search runs on them
   // alone (the others' panel words do not matter to it), so it shrinks as
@@ -1000,27 +1005,28 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
   __syncthreads();
   T = shT;
   i = shI;
-  // the pivot rows at the panel start, their q = phase + |x & z|, XT
+  // the pivot rows at the panel start, their q = phase + |x & z|, XT, ZT
   for (uint32_t t = warp; t < T; t += nwarps) {
     const uint32_t r = stp[t];
     uint32_t s = 0;
-    for (uint32_t w = lane; w < W; w += 32) {
-      const uint64_t v = a.xzs[(size_t)r * W + w];
-      a.po[(size_t)t * W + w] = v;
-      if (w < len) XT[(size_t)w * PANEL + t] = v;
-      if (w >= len) s += __popcll(a.xzs[(size_t)r * W + w - len] & v);
+    for (uint32_t w = lane; w < len; w += 32) {
+      const uint64_t vx = a.xzs[(size_t)r * W + w], vz = a.xzs[(size_t)r * W + len + w];
+      a.po[(size_t)t * W + w] = vx;
+      a.po[(size_t)t * W + len + w] = vz;
+      XT[(size_t)w * PANEL + t] = vx;
+      ZT[(size_t)w * PANEL + t] = vz;
+      s += __popcll(vx & vz);
     }
     s = __reduce_add_sync(0xFFFFFFFFu, s);
     if (lane == 0) qo[t] = (uint8_t)((a.ph[r] + s) & 3u);
   }
   __syncthreads();
   if (a.phases && T) {
-    // C[a] bit b = z_a . x_b over the pivot rows (z from global, x transposed)
+    // C[a] bit b = z_a . x_b over the pivot rows (both transposed in shared memory)
     for (uint32_t t = warp; t < T; t += nwarps) {
-      const uint64_t* za = a.xzs + (size_t)stp[t] * W + len;
       uint32_t p0 = 0, p1 = 0;
       for (uint32_t w = 0; w < len; w++) {
-        const uint64_t zw = za[w];
+        const uint64_t zw = ZT[(size_t)w * PANEL + t];
         p0 += __popcll(zw & XT[(size_t)w * PANEL + lane]);
         p1 += __popcll(zw & XT[(size_t)w * PANEL + lane + 32]);
       }
@@ -1086,6 +1092,8 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
 // step 3, with rows and phases in global memory).
 __global__ void __launch_bounds__(CANON_THREADS) canon_apply_kernel(const PanelArgs a) {
   extern __shared__ __align__(16) uint64_t sm[];
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
   const PanelRec& g = *a.rec;
   const uint32_t T = g.T;
   if (T == 0) return;
@@ -1301,9 +1309,30 @@ static int launch_blocked(const ElimSpec& e, cudaStream_t st) {
 static uint32_t g_canon_grid = 0;  // 0: automatic, 1: always, 2: never (panels over the whole GPU)
 static uint32_t g_canon_rpt = 0;         // tuner: rows per search thread (0: automatic; 4, 8, 16)
 static uint32_t g_canon_apply_rows = 0;  // tuner: rows per apply CTA (0: automatic)
+static uint32_t g_canon_pdl = 1;         // panel launches as programmatic dependents (0: plain)
 // Smallest stabilizer view that runs by panels over the whole GPU (below it,
 // one cluster holds the rows in shared memory).
-constexpr uint32_t CANON_GRID_MIN_ROWS = 1024;
+constexpr uint32_t CANON_GRID_MIN_ROWS = 640;
+
+// A panel launch.  With g_canon_pdl it is a programmatic dependent of the
+// launch before it on the stream: its CTAs may be scheduled while that one
+// finishes (each kernel waits for its predecessor with griddepcontrol.wait
+// before touching memory), which hides the launch gap between the ~2 x 63
+// dependent launches of each stage.
+static cudaError_t launch_panel(void (*k)(const PanelArgs), uint32_t grid, uint32_t block, size_t smem,
+                                cudaStream_t st, const PanelArgs& a) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = g_canon_pdl ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, a);
+}
 
 // canonicalize! by panels over the whole GPU (canon_search_kernel +
 // canon_apply_kernel per panel); scratch from the stream-ordered pool.
@@ -1329,7 +1358,7 @@ static int launch_grid(const ElimSpec& e, cudaStream_t st) {
                                   : rpt == 2 ? canon_search_kernel<2>
                                   : rpt == 4 ? canon_search_kernel<4>
                                   : rpt == 8 ? canon_search_kernel<8> : canon_search_kernel<16>;
-  const size_t search_smem = (size_t)len * PANEL * 8 + (size_t)R * 4;
+  const size_t search_smem = (size_t)2 * len * PANEL * 8 + (size_t)R * 4;
   // opt in always: the static shared memory counts against the default 48 KB too
   QCB_CUDA(cudaFuncSetAttribute(search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_smem));
   const uint32_t rows_per_cta = g_canon_apply_rows ? g_canon_apply_rows : 16u;
@@ -1346,16 +1375,15 @@ static int launch_grid(const ElimSpec& e, cudaStream_t st) {
     for (uint32_t c0 = 0; c0 < e.n; c0 += PANEL) {
       a.stage = stage;
       a.c0 = c0;
-      search<<<1, CANON_THREADS, search_smem, st>>>(a);
-      QCB_LAUNCHED();
-      canon_apply_kernel<<<G, threads, apply_smem, st>>>(a);
-      QCB_LAUNCHED();
+      QCB_CUDA(launch_panel(search, 1, CANON_THREADS, search_smem, st, a));
+      QCB_CUDA(launch_panel(canon_apply_kernel, G, threads, apply_smem, st, a));
     }
   }
   canon_place_kernel<<<(R * 32 + 255) / 256, 256, 0, st>>>(e.xzs, e.ph, pos, R, W, gtmp, gtmp_ph);
   QCB_LAUNCHED();
   QCB_CUDA(cudaMemcpyAsync(e.xzs, gtmp, (size_t)R * W * 8, cudaMemcpyDeviceToDevice, st));
-  QCB_CUDA(cudaMemcpyAsync(e.ph, gtmp_ph, R, cudaMemcpyDeviceToDevice, st));
+  // without phases the reference's row swaps leave the phases in place
+  if (e.phases) QCB_CUDA(cudaMemcpyAsync(e.ph, gtmp_ph, R, cudaMemcpyDeviceToDevice, st));
   QCB_CUDA(cudaFreeAsync(pos, st));
   QCB_CUDA(cudaFreeAsync(rec, st));
   QCB_CUDA(cudaFreeAsync(po, st));
@@ -1491,6 +1519,7 @@ void set_canon_threads(uint32_t n) { g_canon_threads = n; }
 void set_canon_blocked(uint32_t v) { g_canon_blocked = v; }
 void set_canon_grid(uint32_t v) { g_canon_grid = v; }
 void set_canon_rpt(uint32_t v) { g_canon_rpt = v; }
+void set_canon_pdl(uint32_t v) { g_canon_pdl = v; }
 void set_canon_apply_rows(uint32_t v) { g_canon_apply_rows = v; }
 
 }  // namespace qcb

@@ -1218,12 +1218,20 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   return wc;
 }
 
-// Scratch bytes the pre-sampler needs for the frame (0: not used).
-static uint64_t presample_bytes(const qcb_frame* f, const qcb_program* p) {
+// Scratch bytes the pre-sampler needs for ncols columns of program p (0:
+// the program has no pre-sampled noise).
+static uint64_t presample_need(const qcb_program* p, uint64_t ncols) {
   if (g_presample == 1 || p->pre_ent.empty() || p->pmax <= 0.0) return 0;
-  const uint64_t ngroups = (f->ncols + 31) / 32;
-  const uint64_t need = (ngroups * p->pre_capoff.back() + ngroups * p->pre_nparts) * 4;
-  return need <= PRESAMPLE_MAX_BYTES ? need : 0;
+  const uint64_t ngroups = (ncols + 31) / 32;
+  return (ngroups * p->pre_capoff.back() + ngroups * p->pre_nparts) * 4;
+}
+
+// Scratch bytes the pre-sampler needs for the frame (0: not used): at most
+// PRESAMPLE_MAX_BYTES, unless the frame was handed a scratch that large.
+static uint64_t presample_bytes(const qcb_frame* f, const qcb_program* p) {
+  const uint64_t need = presample_need(p, f->ncols);
+  if (need <= PRESAMPLE_MAX_BYTES) return need;
+  return (f->pre && !f->pre_own && f->pre_bytes >= need) ? need : 0;
 }
 
 // Grow the frame's pre-sampler scratch (frames made by qcb_frame_create only;
@@ -1872,12 +1880,7 @@ int qcb_tune_tile(const qcb_program* p, uint32_t* tile_out, float* us_per_column
 // columns of the request's full record).  Counters use the global column,
 // so the chunks of a request give the record of one run over all its shots.
 namespace qcb {
-uint64_t chunk_presample_bytes(const qcb_program* p, uint64_t ncols) {
-  qcb_frame view{};
-  view.ncols = ncols;
-  view.frames = ncols * 32;
-  return presample_bytes(&view, p);
-}
+uint64_t chunk_presample_bytes(const qcb_program* p, uint64_t ncols) { return presample_need(p, ncols); }
 
 void chunk_shape(const qcb_program* p, uint64_t ncols, uint32_t* tile, uint32_t* ctas) {
   qcb_frame view{};

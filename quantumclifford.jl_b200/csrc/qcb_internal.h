@@ -198,8 +198,9 @@ int run_chunk(qcb_frame* f, uint64_t ncols, const qcb_program* p, uint64_t seed,
 // columns of program p.
 void chunk_shape(const qcb_program* p, uint64_t ncols, uint32_t* tile, uint32_t* ctas);
 // Bytes of noise pre-sampler scratch a chunk of `ncols` columns of program p
-// uses (0: its noise is drawn in the walk); a chunk frame that holds at least
-// that much at `pre` (pre_own false) gets its noise pre-sampled.
+// needs (0: the program has no pre-sampled noise); a chunk frame that holds at
+// least that much at `pre` (pre_own false) gets its noise pre-sampled, any
+// other chunk draws it in the walk.
 uint64_t chunk_presample_bytes(const qcb_program* p, uint64_t ncols);
 }  // namespace qcb
 

@@ -59,6 +59,7 @@ void set_canon_blocked(uint32_t v);
 void set_canon_grid(uint32_t v);
 void set_server_fill(uint32_t v);
 void set_canon_rpt(uint32_t v);
+void set_canon_pdl(uint32_t v);
 void set_canon_apply_rows(uint32_t v);
 
 }  // namespace qcb
@@ -158,6 +159,10 @@ int qcb_tune_set(const char* key, int64_t value) {
     if (value && value != 1 && value != 2 && value != 4 && value != 8 && value != 16)
       return fail(QCB_EARG, "canon_rpt must be 0, 1, 2, 4, 8 or 16");
     set_canon_rpt((uint32_t)value);
+  } else if (k == "canon_pdl") {
+    // canonicalize! panel launches as programmatic dependents (1, default) or plain (0)
+    if (value > 1) return fail(QCB_EARG, "canon_pdl must be 0 or 1");
+    set_canon_pdl((uint32_t)value);
   } else if (k == "canon_apply_rows") {
     if (value && (value < 8 || value > 32)) return fail(QCB_EARG, "canon_apply_rows must be 0 or 8..32");
     set_canon_apply_rows((uint32_t)value);

@@ -57,11 +57,11 @@ struct Request {
   uint64_t nbits = 0, ncols = 0, rec_pitch = 0;
   uint64_t bytes = 0;           // record + chunk planes charged to the budget
   uint32_t* record = nullptr;
-  qcb_frame* chunk = nullptr;   // the chunk frame (its planes live while the chunks run)
+  qcb_frame* chunk[2] = {nullptr, nullptr};  // chunk frames: chunk k runs in chunk[k & 1] (one for a one-chunk request)
   int slot = -1;
-  cudaStream_t stream = nullptr;  // the slot's stream
+  cudaStream_t stream[2] = {nullptr, nullptr};  // the slot's streams: chunk k runs on stream[k & 1]
   uint64_t chunk_w = 0;                              // columns per chunk (whole walker waves)
-  uint64_t chunk_bytes = 0;                          // chunk planes + noise pre-sampler scratch
+  uint64_t chunk_bytes = 0;                          // chunk frames: planes + noise pre-sampler scratch
   uint64_t nchunks = 0, launched = 0, finished = 0;  // chunks: total, launched, seen complete
   uint32_t ctas_full = 0, ctas_last = 0;             // walker CTAs of a full and of the last chunk
   cudaEvent_t chunk_ev[2] = {nullptr, nullptr};      // completion of chunk k in chunk_ev[k % 2]
@@ -86,7 +86,7 @@ struct qcb_server {
   uint64_t budget = 0, used = 0;
   uint32_t nslots = 0;
   uint64_t chunk_cols = 0;  // columns per chunk (a multiple of 32: 1024-shot groups)
-  std::vector<cudaStream_t> streams;  // one per slot
+  std::vector<cudaStream_t> streams;  // two per slot (slot k: 2k, 2k + 1)
   bool fill_gate = true;              // admit only onto idle SMs (false: whenever a slot is free)
   uint32_t capacity = 0;              // walker CTAs the GPU runs at once (one per SM)
   std::vector<int64_t> slot_req;  // request id per slot, -1 when free
@@ -199,35 +199,50 @@ static uint64_t remaining_ctas(const Request& r) {
   return left >= 2 ? r.ctas_full : left == 1 ? r.ctas_last : 0;
 }
 
-// After the last chunk: the walker status word to the slot's pinned word,
-// the chunk planes back to the pool and the request's completion event, all
-// in stream order.
-static int finish_launches(qcb_server* s, Request& r) {
-  qcb_frame* cf = r.chunk;
-  int status = r.status;
-  if (status == QCB_OK && cf->err &&
-      cudaMemcpyAsync(&s->slot_status[r.slot], cf->err, 4, cudaMemcpyDeviceToHost, r.stream) != cudaSuccess)
-    status = fail(QCB_ECUDA, "serving: status copy");
-  if (cf->planes) cudaFreeAsync(cf->planes, r.stream);
-  if (cf->pre) cudaFreeAsync(cf->pre, r.stream);
-  if (cf->err) cudaFreeAsync(cf->err, r.stream);
+// Free a chunk frame's device buffers in stream order (the status word is
+// shared by the two frames and freed with the first).
+static void free_chunk_frame(qcb_frame* cf, bool err, cudaStream_t st) {
+  if (!cf) return;
+  if (cf->planes) cudaFreeAsync(cf->planes, st);
+  if (cf->pre) cudaFreeAsync(cf->pre, st);
+  if (err && cf->err) cudaFreeAsync(cf->err, st);
   cf->planes = nullptr;
   cf->pre = nullptr;
   cf->pre_bytes = 0;
   cf->err = nullptr;
-  if (cudaEventRecord(r.done, r.stream) != cudaSuccess && status == QCB_OK) status = fail(QCB_ECUDA, "serving: event");
+}
+
+// After the last chunk: stream 0 joins stream 1, then the walker status word
+// to the slot's pinned word, the chunk frames back to the pool and the
+// request's completion event, all in stream order.
+static int finish_launches(qcb_server* s, Request& r) {
+  int status = r.status;
+  if (r.chunk[1] && (cudaEventRecord(r.chunk_ev[1], r.stream[1]) != cudaSuccess ||
+                     cudaStreamWaitEvent(r.stream[0], r.chunk_ev[1], 0) != cudaSuccess) && status == QCB_OK)
+    status = fail(QCB_ECUDA, "serving: stream join");
+  qcb_frame* cf = r.chunk[0];
+  if (status == QCB_OK && cf->err &&
+      cudaMemcpyAsync(&s->slot_status[r.slot], cf->err, 4, cudaMemcpyDeviceToHost, r.stream[0]) != cudaSuccess)
+    status = fail(QCB_ECUDA, "serving: status copy");
+  free_chunk_frame(r.chunk[1], false, r.stream[0]);
+  free_chunk_frame(r.chunk[0], true, r.stream[0]);
+  if (cudaEventRecord(r.done, r.stream[0]) != cudaSuccess && status == QCB_OK)
+    status = fail(QCB_ECUDA, "serving: event");
   return status;
 }
 
-// Launch the request's next chunk on its stream (lock held); after the last
-// one, finish_launches.  A failure ends the launches: the request retires as
-// failed once its stream has drained.
+// Launch the request's next chunk (lock held): chunk k in frame k & 1 on
+// stream k & 1, so that consecutive chunks overlap (the next one's CTAs take
+// the SMs the last wave of this one leaves, instead of one tail per chunk);
+// after the last one, finish_launches.  A failure ends the launches: the
+// request retires as failed once its streams have drained.
 static void launch_chunk(qcb_server* s, Request& r) {
   const uint64_t k = r.launched;
+  const uint32_t j = r.chunk[1] ? (uint32_t)(k & 1) : 0u;
   const uint64_t c0 = k * r.chunk_w;
   const uint64_t nc = std::min<uint64_t>(r.chunk_w, r.ncols - c0);
-  int status = run_chunk(r.chunk, nc, r.prog, r.seed, c0 * 32, r.record + c0, r.rec_pitch, r.stream);
-  if (status == QCB_OK && cudaEventRecord(r.chunk_ev[k % 2], r.stream) != cudaSuccess)
+  int status = run_chunk(r.chunk[j], nc, r.prog, r.seed, c0 * 32, r.record + c0, r.rec_pitch, r.stream[j]);
+  if (status == QCB_OK && cudaEventRecord(r.chunk_ev[k % 2], r.stream[j]) != cudaSuccess)
     status = fail(QCB_ECUDA, "serving: chunk event");
   r.launched++;
   if (status != QCB_OK) {
@@ -258,18 +273,37 @@ static void advance(qcb_server* s) {
   }
 }
 
-// Columns per chunk of a request: all of them when they fit the server's
-// chunk width, else the nearest whole number of walker waves (one tile per
-// SM) to it that is a whole number of 1024-shot groups, so that no chunk but
-// the last ends on a mostly empty wave.
+// Noise pre-sampler scratch per chunk frame: chunks are narrowed (by whole
+// waves) until their scratch fits this, so that strong noise is pre-sampled
+// too (d = 11, 2^20 shots, p = 1e-2: 2.14 ms pre-sampled, 4.82 ms drawn in
+// the walk).
+constexpr uint64_t SERVE_PRESAMPLE_MAX = 1ull << 30;
+
+// Pre-sampler scratch of a chunk frame of `cw` columns (0: drawn in the walk).
+static uint64_t chunk_pre_bytes(const Request& r, uint64_t cw) {
+  const uint64_t need = chunk_presample_bytes(r.prog, cw);
+  return need <= SERVE_PRESAMPLE_MAX ? need : 0;
+}
+
+// Columns per chunk of a request: all of them (one launch) when they fit the
+// server's chunk width, else the nearest whole number of walker waves (one
+// tile per SM) to it that is a whole number of 1024-shot groups, so that no
+// chunk but the last ends on a mostly empty wave; then fewer waves while the
+// chunk's pre-sampler scratch does not fit SERVE_PRESAMPLE_MAX.
 static uint64_t chunk_width(const qcb_server* s, const Request& r) {
-  if (r.ncols <= s->chunk_cols) return r.ncols;
+  if (r.ncols <= s->chunk_cols) return r.ncols;  // one launch
   uint32_t T = 0;
   chunk_shape(r.prog, s->chunk_cols, &T, nullptr);
   uint64_t unit = (uint64_t)s->capacity * std::max<uint32_t>(T, 1);
   while (unit % 32) unit *= 2;
-  const uint64_t k = std::max<uint64_t>(1, (s->chunk_cols + unit / 2) / unit);
-  return std::min(k * unit, r.ncols);
+  const uint64_t k0 = std::max<uint64_t>(1, (s->chunk_cols + unit / 2) / unit);
+  uint64_t cw = std::min(k0 * unit, r.ncols);
+  if (chunk_presample_bytes(r.prog, cw) > SERVE_PRESAMPLE_MAX && cw > unit) {
+    uint64_t k = cw / unit;
+    while (k > 1 && chunk_presample_bytes(r.prog, k * unit) > SERVE_PRESAMPLE_MAX) k--;
+    if (chunk_presample_bytes(r.prog, k * unit) <= SERVE_PRESAMPLE_MAX) cw = k * unit;
+  }
+  return cw;
 }
 
 // Admit the head of the queue while a slot, the budget and the GPU's fill
@@ -287,8 +321,9 @@ static void admit(qcb_server* s) {
       r.ncols = (r.shots + 31) / 32;
       r.rec_pitch = std::max<uint64_t>(32, (r.ncols + 31) / 32 * 32);
       r.chunk_w = chunk_width(s, r);
-      r.chunk_bytes = chunk_plane_bytes(std::max<uint32_t>(r.prog->nq, 1), r.chunk_w) +
-                      chunk_presample_bytes(r.prog, r.chunk_w);
+      r.nchunks = (r.ncols + r.chunk_w - 1) / r.chunk_w;
+      r.chunk_bytes = (r.nchunks > 1 ? 2 : 1) * (chunk_plane_bytes(std::max<uint32_t>(r.prog->nq, 1), r.chunk_w) +
+                                                 chunk_pre_bytes(r, r.chunk_w));
       r.bytes = r.nbits * r.rec_pitch * 4 + r.chunk_bytes;
     }
     if (r.bytes > s->budget) {
@@ -325,50 +360,60 @@ static void admit(qcb_server* s) {
       continue;
     }
     const uint32_t nq1 = std::max<uint32_t>(r.prog->nq, 1);
-    cudaStream_t st = s->streams[slot];
-    r.stream = st;
+    cudaStream_t st = s->streams[2 * (size_t)slot];
+    r.stream[0] = st;
+    r.stream[1] = s->streams[2 * (size_t)slot + 1];
     r.slot = slot;
-    // the chunk frame: planes for one chunk, allocated and freed in stream
-    // order (no device-wide synchronisation on the scheduler thread)
-    qcb_frame* cf = new qcb_frame();
-    cf->frames = r.chunk_w * 32;
-    cf->qubits = nq1 - 1;
-    cf->nq1 = nq1;
-    cf->nbits = 0;
-    cf->ncols = r.chunk_w;
-    cf->pitch = std::max<uint64_t>(32, (r.chunk_w + 31) / 32 * 32);
-    cf->planes = nullptr;
-    cf->record = nullptr;
-    cf->err = nullptr;
-    r.chunk = cf;
-    r.nchunks = (r.ncols + r.chunk_w - 1) / r.chunk_w;
     r.launched = r.finished = 0;
     chunk_shape(r.prog, r.chunk_w, nullptr, &r.ctas_full);
     chunk_shape(r.prog, r.ncols - (r.nchunks - 1) * r.chunk_w, nullptr, &r.ctas_last);
-    cudaError_t e = cudaMallocAsync(&cf->planes, (size_t)2 * (nq1 + 1) * cf->pitch * 4, st);
-    const uint64_t pre = chunk_presample_bytes(r.prog, r.chunk_w);
-    if (e == cudaSuccess && pre) {
-      e = cudaMallocAsync(&cf->pre, pre, st);
-      if (e == cudaSuccess) cf->pre_bytes = pre;
+    // the chunk frames (two when there are two or more chunks): planes for
+    // one chunk and its noise pre-sampler scratch, allocated on stream 0 and
+    // freed in stream order (no device-wide synchronisation on the
+    // scheduler thread); one status word for both
+    const uint64_t pre = chunk_pre_bytes(r, r.chunk_w);
+    cudaError_t e = cudaSuccess;
+    for (uint32_t f = 0; f < (r.nchunks > 1 ? 2u : 1u); f++) {
+      qcb_frame* cf = new qcb_frame();
+      cf->frames = r.chunk_w * 32;
+      cf->qubits = nq1 - 1;
+      cf->nq1 = nq1;
+      cf->nbits = 0;
+      cf->ncols = r.chunk_w;
+      cf->pitch = std::max<uint64_t>(32, (r.chunk_w + 31) / 32 * 32);
+      cf->planes = nullptr;
+      cf->record = nullptr;
+      cf->err = nullptr;
+      r.chunk[f] = cf;
+      if (e == cudaSuccess) e = cudaMallocAsync(&cf->planes, (size_t)2 * (nq1 + 1) * cf->pitch * 4, st);
+      if (e == cudaSuccess && pre) {
+        e = cudaMallocAsync(&cf->pre, pre, st);
+        if (e == cudaSuccess) cf->pre_bytes = pre;
+      }
     }
-    if (e == cudaSuccess) e = cudaMallocAsync(&cf->err, 16, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(cf->err, 0, 16, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&r.chunk[0]->err, 16, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r.chunk[0]->err, 0, 16, st);
+    if (r.chunk[1]) r.chunk[1]->err = r.chunk[0]->err;
     if (e == cudaSuccess) e = cudaMallocAsync(&r.record, r.nbits * r.rec_pitch * 4, st);
-    for (int j = 0; j < 2 && e == cudaSuccess; j++)
-      if (!r.chunk_ev[j]) e = cudaEventCreateWithFlags(&r.chunk_ev[j], cudaEventDisableTiming);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++)
+      if (!r.chunk_ev[k]) e = cudaEventCreateWithFlags(&r.chunk_ev[k], cudaEventDisableTiming);
     if (e == cudaSuccess && !r.done) e = cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming);
+    // stream 1 starts after the allocations made on stream 0
+    if (e == cudaSuccess && r.chunk[1]) e = cudaEventRecord(r.chunk_ev[1], st);
+    if (e == cudaSuccess && r.chunk[1]) e = cudaStreamWaitEvent(r.stream[1], r.chunk_ev[1], 0);
     s->queue.pop_front();
     r.t_admit = s->now();
     if (e != cudaSuccess) {
       r.status = cuda_fail(e, "serving: admission");
       r.msg = last_msg();
-      if (cf->planes) cudaFreeAsync(cf->planes, st);
-      if (cf->pre) cudaFreeAsync(cf->pre, st);
-      if (cf->err) cudaFreeAsync(cf->err, st);
+      free_chunk_frame(r.chunk[1], false, st);
+      free_chunk_frame(r.chunk[0], true, st);
       if (r.record) cudaFreeAsync(r.record, st);
       r.record = nullptr;
-      delete r.chunk;
-      r.chunk = nullptr;
+      for (qcb_frame*& cf : r.chunk) {
+        delete cf;
+        cf = nullptr;
+      }
       r.slot = -1;
       r.state = RQ_FAILED; r.t_done = s->now();
       s->completed.push_back(r.id);
@@ -406,8 +451,10 @@ static void retire(qcb_server* s) {
     }
     s->slot_status[k] = 0;
     r.finished = r.nchunks;
-    delete r.chunk;
-    r.chunk = nullptr;
+    for (qcb_frame*& cf : r.chunk) {
+      delete cf;
+      cf = nullptr;
+    }
     // the chunk planes leave the request's charge; the record stays charged
     s->used -= r.chunk_bytes;
     r.bytes -= r.chunk_bytes;
@@ -452,7 +499,7 @@ int qcb_server_create(uint64_t hbm_budget_bytes, uint32_t slots, uint64_t chunk_
   s->slot_req.assign(slots, -1);
   QCB_CUDA(cudaHostAlloc(&s->slot_status, 64 * sizeof(int32_t), cudaHostAllocDefault));
   std::memset(s->slot_status, 0, 64 * sizeof(int32_t));
-  for (uint32_t k = 0; k < slots; k++) {
+  for (uint32_t k = 0; k < 2 * slots; k++) {
     cudaStream_t st;
     QCB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     s->streams.push_back(st);
@@ -618,7 +665,7 @@ int qcb_server_release(qcb_server* s, uint64_t ticket) {
     Request& r = *it->second;
     if (r.state < RQ_DONE) return fail(QCB_EARG, "serving: request still queued or running");
     if (r.record) {
-      cudaFreeAsync(r.record, r.stream ? r.stream : s->streams[0]);  // the request's work is complete
+      cudaFreeAsync(r.record, r.stream[0] ? r.stream[0] : s->streams[0]);  // the request's work is complete
       s->used -= r.bytes;
     }
     if (r.done) cudaEventDestroy(r.done);
@@ -653,7 +700,7 @@ int qcb_server_destroy(qcb_server* s) {
   for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
   for (auto& kv : s->reqs) {
     if (kv.second->record) cudaFree(kv.second->record);
-    delete kv.second->chunk;
+    for (qcb_frame* cf : kv.second->chunk) delete cf;
     if (kv.second->done) cudaEventDestroy(kv.second->done);
     for (cudaEvent_t ev : kv.second->chunk_ev)
       if (ev) cudaEventDestroy(ev);

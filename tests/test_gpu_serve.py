@@ -160,31 +160,34 @@ def test_programs_count_against_the_budget(qcb):
 
 @pytest.mark.parametrize("fill", [1, 0])
 def test_fill_gate_keeps_large_requests_in_order(qcb, fill):
-    """server_fill 1: a request behind one whose chunks fill the GPU (2^20
+    """server_fill 1: a request behind one whose chunks fill the GPU (2^21
     shots in chunks of whole walker waves near 2^17 shots) waits until that
     one is on its last chunk, which may leave SMs idle; server_fill 0 admits
     it at once.  Records equal the plain runs either way."""
-    big = circuits.rotated_surface_code_memory(5, 5, 1e-3)
+    big = circuits.rotated_surface_code_memory(7, 7, 1e-3)
     small = circuits.rotated_surface_code_memory(3, 3, 1e-3)
+    nbig = 16 << 17
     qcb.check(qcb.lib().qcb_tune_set(b"server_fill", fill))
     try:
         srv = qcb.Server(hbm_budget_bytes=8 << 30, slots=4, chunk_shots=1 << 17)
     finally:
         qcb.check(qcb.lib().qcb_tune_set(b"server_fill", 1))
-    tb = srv.submit(big, 8 << 17, 5)
+    srv.preload(big)
+    srv.preload(small)  # submissions then take no compile time
+    tb = srv.submit(big, nbig, 5)
     ts = srv.submit(small, 2000, 6)
     srv.wait(tb)
     srv.wait(ts)
     _, admit_big, done_big = srv.query(tb)[1]
     admit_small = srv.query(ts)[1][1]
-    # the big request runs 7 chunks: fill 1 holds the small one for at least
-    # the first six, fill 0 lets it in while the first runs
+    # fill 1 holds the small one for all chunks of the big one but the last,
+    # fill 0 lets it in while the first runs
     frac = (admit_small - admit_big) / (done_big - admit_big)
     if fill:
         assert frac > 0.5, frac
     else:
-        assert frac < 0.5, frac
-    assert np.array_equal(srv.result(tb, 8 << 17), plain_record(qcb, big, 8 << 17, 5))
+        assert frac < 0.3, frac
+    assert np.array_equal(srv.result(tb, nbig), plain_record(qcb, big, nbig, 5))
     assert np.array_equal(srv.result(ts, 2000), plain_record(qcb, small, 2000, 6))
     srv.release(tb)
     srv.release(ts)

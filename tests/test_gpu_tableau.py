@@ -285,11 +285,13 @@ def test_dense_apply(qcb, n):
 
 @pytest.mark.parametrize("grid", [1, 2])
 @pytest.mark.parametrize("n", [64, 97, 1000, 2100, 4000])
-def test_canonicalize_panels_over_the_gpu(qcb, n, grid):
+@pytest.mark.parametrize("phases", [True, False])
+def test_canonicalize_panels_over_the_gpu(qcb, n, grid, phases):
     """canonicalize! by panels with the per-row work spread over the GPU
     (canon_grid 1: a one-CTA search launch and a grid-wide apply launch per
     panel) and on one cluster (2), on uniformly random stabilizer states, bit
-    for bit with phases and ranks against the oracle; also a rank-deficient
+    for bit with phases and ranks against the oracle, with phases tracked and
+    not (the row swaps then leave the phases in place); also a rank-deficient
     view (repeated rows)."""
     from qcb200 import randoms
 
@@ -301,10 +303,10 @@ def test_canonicalize_panels_over_the_gpu(qcb, n, grid):
     qcb.check(qcb.lib().qcb_tune_set(b"canon_grid", grid))
     try:
         s = qcb.Stabilizer(t.copy()).to_gpu()
-        _, rx, rz = qcb.canonicalize_(s, ranks=True)
+        _, rx, rz = qcb.canonicalize_(s, phases=phases, ranks=True)
         s.to_cpu()
     finally:
         qcb.check(qcb.lib().qcb_tune_set(b"canon_grid", 0))
-    ph, xz, orx, orz = oracle.canonicalize(t.phases, t.xzs, n, True)
+    ph, xz, orx, orz = oracle.canonicalize(t.phases, t.xzs, n, phases)
     assert (rx, rz) == (orx, orz)
     assert np.array_equal(s.tab.xzs, xz) and np.array_equal(s.tab.phases, ph)

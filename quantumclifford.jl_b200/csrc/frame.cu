@@ -1286,8 +1286,95 @@ static int launch_presample(qcb_frame* f, const qcb_program* p, WalkArgs& a, cud
   return QCB_OK;
 }
 
+static void fill_common(WalkArgs& a, qcb_frame* f, const qcb_program* p);
+int launch_walker(qcb_frame* f, const qcb_program* p, WalkArgs& a, bool philox, bool fresh, cudaStream_t st);
+
+// Largest scratch of a chunked run (two chunks' event buckets).
+constexpr uint64_t CHUNKED_PRESAMPLE_MAX = 4ull << 30;
+
+// Columns per chunk of a Philox run whose pre-sampler scratch would pass
+// PRESAMPLE_MAX_BYTES: whole walker waves (a whole number of 1024-shot
+// groups), as many as fit twice over in PRESAMPLE_MAX_BYTES, at least one
+// (strong noise on tall circuits: d = 21, p = 7.7e-3 needs about 0.5 GB a
+// wave); 0 when two waves' scratch passes CHUNKED_PRESAMPLE_MAX (the run then
+// draws its noise in the walk).
+static uint64_t presample_chunk_cols(const qcb_program* p, const qcb_frame* f) {
+  const uint64_t nsm = (uint64_t)std::max(device_sm_count(), 1);
+  uint64_t unit = nsm * std::max<uint32_t>(walk_config(p, f).T, 1);
+  while (unit % 32) unit *= 2;
+  const uint64_t per = presample_need(p, unit);
+  if (!per || 2 * per > CHUNKED_PRESAMPLE_MAX) return 0;
+  const uint64_t budget = std::max<uint64_t>(PRESAMPLE_MAX_BYTES, 2 * per);
+  uint64_t k = budget / (2 * per);
+  while (k > 1 && 2 * presample_need(p, k * unit) > budget) k--;
+  return k * unit;
+}
+
+// A side stream per device for the chunked runs below.
+static cudaStream_t side_stream() {
+  static std::mutex mu;
+  static cudaStream_t streams[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev >= 0 && dev < 64 && !streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+  return (dev >= 0 && dev < 64) ? streams[dev] : nullptr;
+}
+
+// A Philox run whose pre-sampler scratch would pass PRESAMPLE_MAX_BYTES, as
+// column chunks of cw columns whose noise is pre-sampled (the frame keeps
+// two scratches, one per chunk in flight): chunk k on the caller's stream
+// (k even) or the side stream (k odd), forked from and joined back to the
+// caller's stream, so that a chunk's last wave overlaps the next chunk.
+// Columns are independent in Philox mode and every chunk counts with its
+// global columns, so the frame and record equal those of one launch.
+static int launch_walker_chunked(qcb_frame* f, const qcb_program* p, const WalkArgs& a0, bool fresh,
+                                 cudaStream_t st, uint64_t cw) {
+  const uint64_t half = (presample_need(p, cw) + 15) & ~15ull;
+  if (f->pre_bytes < 2 * half) {
+    if (f->pre) QCB_CUDA(cudaFree(f->pre));
+    f->pre = nullptr;
+    f->pre_bytes = 0;
+    QCB_CUDA(cudaMalloc(&f->pre, 2 * half));
+    f->pre_bytes = 2 * half;
+  }
+  cudaStream_t side = side_stream();
+  if (!side) return fail(QCB_ECUDA, "no side stream for a chunked run");
+  cudaEvent_t fork = nullptr, join = nullptr;
+  QCB_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  QCB_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  int status = QCB_OK;
+  if (cudaEventRecord(fork, st) != cudaSuccess || cudaStreamWaitEvent(side, fork, 0) != cudaSuccess)
+    status = fail(QCB_ECUDA, "chunked run: fork");
+  for (uint64_t c0 = 0, k = 0; status == QCB_OK && c0 < f->ncols; c0 += cw, k++) {
+    const uint64_t nc = std::min(cw, f->ncols - c0);
+    qcb_frame view = *f;  // columns [c0, c0 + nc) of every plane and record row
+    view.planes = f->planes + c0;
+    view.record = f->record ? f->record + c0 : nullptr;
+    view.ncols = nc;
+    view.frames = nc * 32;
+    view.pre = f->pre + (k & 1) * (half / 4);
+    view.pre_bytes = half;
+    view.pre_own = false;
+    WalkArgs a;
+    fill_common(a, &view, p);
+    a.seed = a0.seed;
+    a.col0 = a0.col0 + c0;
+    status = launch_walker(&view, p, a, true, fresh, (k & 1) ? side : st);
+  }
+  if (cudaEventRecord(join, side) != cudaSuccess || cudaStreamWaitEvent(st, join, 0) != cudaSuccess)
+    if (status == QCB_OK) status = fail(QCB_ECUDA, "chunked run: join");
+  cudaEventDestroy(fork);
+  cudaEventDestroy(join);
+  return status;
+}
+
 int launch_walker(qcb_frame* f, const qcb_program* p, WalkArgs& a, bool philox, bool fresh,
                   cudaStream_t st) {
+  if (philox && f->pre_own && f->ncols && presample_need(p, f->ncols) > PRESAMPLE_MAX_BYTES) {
+    const uint64_t cw = presample_chunk_cols(p, f);
+    if (cw && cw < f->ncols) return launch_walker_chunked(f, p, a, fresh, st, cw);
+  }
   WalkConfig wc = walk_config(p, f);
   if (philox && f->ncols)
     if (int s = launch_presample(f, p, a, st)) return s;

@@ -420,3 +420,33 @@ def test_measurements_download_chunks(qcb, frames):
     qmax, bmax = O.affected_counts(circ)
     f = qcb.pftrajectories(circ, trajectories=frames, seed=8)
     assert np.array_equal(f.measurements(), qcb.unpack_record(f.record_planes(), frames))
+
+
+def test_chunked_presampled_run_equals_one_launch(qcb):
+    """A Philox run whose noise pre-sampler scratch would pass its cap (d = 11
+    at p = 1e-2, 2^23 shots: about 1.6 GB of event buckets) runs as column
+    chunks of whole walker waves on two streams, each with its noise
+    pre-sampled; record and frame equal the one-launch run that draws the
+    noise in the walk, bit for bit, and its first 32k shots the oracle."""
+    arr = O.to_array(circuits.rotated_surface_code_memory(11, 11, 1e-2))
+    qmax, bmax = O.affected_counts(arr)
+    shots = 1 << 23
+    prog = qcb.Program(arr)
+    got = []
+    for mode in (0, 1):  # 0: chunked and pre-sampled; 1: one launch, noise in the walk
+        qcb.check(qcb.lib().qcb_tune_set(b"presample", mode))
+        try:
+            f = qcb.PauliFrame(shots, qmax, bmax, init=False)
+            qcb.check(qcb.lib().qcb_pftrajectories_fresh(f.handle, prog.handle, 99, 0, None))
+            got.append((f.record_planes(), f.xzs()))
+            del f
+        finally:
+            qcb.check(qcb.lib().qcb_tune_set(b"presample", 0))
+    (p0, x0), (p1, x1) = got
+    assert np.array_equal(p0, p1)
+    cm = oracle.coding_mask(qmax + 1)[:, None]
+    assert np.array_equal(x0 & cm, x1 & cm)
+    n = 32 * 1024
+    ox, om = oracle.pftrajectories_philox(arr, n, qmax, bmax, 99)
+    assert np.array_equal(p0[:, : n // 32], qcb.pack_record(om))
+    assert np.array_equal(x0[:, :n] & cm, ox & cm)

@@ -931,68 +931,60 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
       rpw[k] = j < Rc ? a.xzs[(size_t)rrow[k] * W + wj] : 0ull;
       rcb[k] = 0;
     }
-    // the steps (as blocked_body): one named barrier among the search warps per column
-    bool prev = false;
-    uint32_t pprev = 0, bprev = 0;
+    // the steps (as blocked_body): one named barrier among the search warps
+    // per column.  Kept short, as the search is instruction-bound on its SM:
+    // rows past the candidates hold a zero word (never a candidate, never
+    // updated); the previous step's pivot is applied lazily at the start of
+    // a step (pwprev = 0 after a column without one), which also zeroes the
+    // pivot row's own word, so it never competes again; positions i and kpos
+    // swap by value; the warp's best row travels with its position and the
+    // winning lane posts it.
+    uint32_t bprev = 0;
     uint64_t pwprev = 0, aprev = 0;
     for (uint32_t b = 0; b < ncp && i < R; b++) {
-      uint32_t bpos = 0xFFFFFFFFu, bk = 0;
+      uint32_t bpos = 0xFFFFFFFFu, brow = 0;
+      uint64_t bpw = 0, bcb = 0;
 #pragma unroll
       for (uint32_t k = 0; k < RPT; k++) {
-        const uint32_t r = rrow[k];
-        if (r == 0xFFFFFFFFu) continue;
-        if (prev && r != pprev && ((rpw[k] >> bprev) & 1ull)) {
+        if ((rpw[k] >> bprev) & 1ull) {
           rpw[k] ^= pwprev;
           rcb[k] ^= aprev;
         }
-        if (rpos[k] >= i && ((rpw[k] >> b) & 1ull) && rpos[k] < bpos) { bpos = rpos[k]; bk = k; }
+        if (((rpw[k] >> b) & 1ull) && rpos[k] < bpos) {
+          bpos = rpos[k];
+          brow = rrow[k];
+          bpw = rpw[k];
+          bcb = rcb[k];
+        }
       }
       {
-        uint64_t mypw = 0, mycb = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < RPT; k++)
-          if (k == bk) { mypw = rpw[k]; mycb = rcb[k]; }
         const uint32_t m = __reduce_min_sync(0xFFFFFFFFu, bpos);
-        const uint32_t who = __ballot_sync(0xFFFFFFFFu, bpos == m);
-        const uint32_t src = __ffs(who) - 1;
-        uint32_t myrow = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < RPT; k++)
-          if (k == bk) myrow = rrow[k];
-        const uint32_t row = __shfl_sync(0xFFFFFFFFu, myrow, src);
-        const uint64_t wpw = __shfl_sync(0xFFFFFFFFu, mypw, src);
-        const uint64_t wcb = __shfl_sync(0xFFFFFFFFu, mycb, src);
-        if (lane == 0) {
-          red2[b & 1][warp][0] = ((uint64_t)m << 32) | row;
-          red2[b & 1][warp][1] = wpw;
-          red2[b & 1][warp][2] = wcb;
+        const uint32_t src = __ffs(__ballot_sync(0xFFFFFFFFu, bpos == m)) - 1;
+        if (lane == src) {
+          red2[b & 1][warp][0] = ((uint64_t)m << 32) | brow;
+          red2[b & 1][warp][1] = bpw;
+          red2[b & 1][warp][2] = bcb;
         }
       }
       asm volatile("bar.sync 1, %0;" ::"r"(nbt) : "memory");
       const uint64_t e = lane < NB ? red2[b & 1][lane][0] : ~0ull;
       const uint32_t kpos = __reduce_min_sync(0xFFFFFFFFu, (uint32_t)(e >> 32));
       if (kpos == 0xFFFFFFFFu) {
-        prev = false;
+        pwprev = 0;
+        aprev = 0;
         continue;
       }
       const uint32_t kw = __ffs(__ballot_sync(0xFFFFFFFFu, (uint32_t)(e >> 32) == kpos)) - 1;
-      const uint32_t pstar = (uint32_t)red2[b & 1][kw][0];
       pwprev = red2[b & 1][kw][1];
       aprev = red2[b & 1][kw][2] | (1ull << T);
 #pragma unroll
-      for (uint32_t k = 0; k < RPT; k++) {
-        const uint32_t r = rrow[k];
-        if (r == pstar) rpos[k] = i;
-        else if (r != 0xFFFFFFFFu && rpos[k] == i) rpos[k] = kpos;
-      }
+      for (uint32_t k = 0; k < RPT; k++) rpos[k] = rpos[k] == kpos ? i : (rpos[k] == i ? kpos : rpos[k]);
       if (tid == 0) {
-        stp[T] = pstar;
+        stp[T] = (uint32_t)red2[b & 1][kw][0];
         bt[T] = (uint8_t)b;
         A[T] = aprev;
         PWP[T] = pwprev;
       }
-      prev = true;
-      pprev = pstar;
       bprev = b;
       T++;
       i++;

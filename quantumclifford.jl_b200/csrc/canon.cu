@@ -1341,10 +1341,11 @@ static int launch_grid(const ElimSpec& e, cudaStream_t st) {
   QCB_CUDA(cudaMallocAsync(&gtmp_ph, R, st));
   canon_grid_init_kernel<<<(R + 255) / 256, 256, 0, st>>>(pos, R, rec);
   QCB_LAUNCHED();
-  // rows per search thread: at least enough for the rows in 1024 threads
-  // (the fewest that fit the 1024 threads: fewer rows a thread was faster,
-  // n = 2000: 4 / 8 / 16 rows 3.10 / 3.72 / 7.00 ms)
-  uint32_t rpt = g_canon_rpt ? g_canon_rpt : 1u;
+  // rows per search thread: 4, or the fewest that fit the rows in 1024
+  // threads (n = 1000: 1 / 2 / 4 / 8 rows 1.225 / 1.233 / 1.223 / 1.333 ms;
+  // n = 2000: 2 / 4 / 8 rows 2.71 / 2.63 / 2.81 ms; n = 4000: 4 / 8 / 16
+  // rows 7.66 / 7.86 / 11.19 ms)
+  uint32_t rpt = g_canon_rpt ? g_canon_rpt : 4u;
   while (rpt * CANON_THREADS < R) rpt *= 2;
   void (*search)(const PanelArgs) = rpt == 1 ? canon_search_kernel<1>
                                   : rpt == 2 ? canon_search_kernel<2>

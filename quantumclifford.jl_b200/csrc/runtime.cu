@@ -152,7 +152,7 @@ int qcb_tune_set(const char* key, int64_t value) {
     if (value > 2) return fail(QCB_EARG, "canon_blocked must be 0 (automatic), 1 (always) or 2 (never)");
     set_canon_blocked((uint32_t)value);
   } else if (k == "canon_grid") {
-    // canonicalize! by panels over the whole GPU: 0 from 1024 rows, 1 always, 2 never
+    // canonicalize! by panels over the whole GPU: 0 from 640 rows, 1 always, 2 never
     if (value > 2) return fail(QCB_EARG, "canon_grid must be 0 (automatic), 1 (always) or 2 (never)");
     set_canon_grid((uint32_t)value);
   } else if (k == "canon_rpt") {

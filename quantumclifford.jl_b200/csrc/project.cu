@@ -635,7 +635,125 @@ static size_t proj_smem_bytes(uint32_t RB, uint32_t W) {
   return ((size_t)2 * W + 1 + (size_t)RB * (W + 1)) * 8 + 2 * (size_t)RB + 16 + 32 + 16 + 32 + 16;
 }
 
+// ---------------------------------------------------------------- the whole GPU
+// project! of a Stabilizer / MixedStabilizer tableau too tall for one
+// cluster's shared memory, on every SM: a cooperative grid (one CTA per SM,
+// all resident) with two grid barriers per Pauli.  Phase 1: comm(pauli, row)
+// for every row (warp per row) and the first anticommuting stabilizer row by
+// a global atomicMin; barrier; phase 2: the same decision in every CTA, then
+// row m <- pivot * row m for the anticommuting rows after the pivot (the
+// loop of src/project_trace_reset.jl:296-305); barrier.  Writing the Pauli
+// into the pivot row is deferred to the next Pauli's phase 1 (CTA 0), whose
+// comm test takes that row from the Pauli kept in shared memory, so no third
+// barrier is needed.  Every wait at a grid barrier is bounded: on expiry the
+// CTA records QCB_ETIMEOUT and returns, and the others give up at their next
+// barrier.
+struct ProjGridArgs {
+  ProjArgs a;
+  uint32_t* bar;   // [0] arrivals, [1] generation
+  uint32_t* gmin;  // [3]: the first anticommuting row of Pauli j at gmin[j % 3]
+  int32_t* err;    // QCB_ETIMEOUT when a grid barrier wait gave up
+};
+
+// Bounded grid barrier; false when this CTA gave up waiting.
+__device__ bool grid_barrier(uint32_t* bar, uint32_t nblocks, int32_t* err) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t* gen = bar + 1;
+    const uint32_t g0 = *gen;
+    __threadfence();
+    ok = 1;
+    if (atomicAdd(bar, 1u) == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      uint32_t it = 0;
+      while (*gen == g0) {
+        if (++it > (1u << 26)) {
+          ok = 0;
+          atomicExch(err, QCB_ETIMEOUT);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+__global__ void __launch_bounds__(PROJ_THREADS) project_grid_kernel(const ProjGridArgs g) {
+  const ProjArgs& a = g.a;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t G = gridDim.x, gw = blockIdx.x * nwarps + warp, NW = G * nwarps;
+  const uint32_t W = a.W, len = W / 2, rows = a.rows;
+  const bool lead = blockIdx.x == 0;
+  extern __shared__ __align__(16) uint64_t smem[];
+  uint64_t* Pb[2] = {smem, smem + W};  // the Pauli of projection j in Pb[j & 1]
+  uint64_t* piv = smem + 2 * W;
+  const uint32_t r = a.kind == QCB_STABILIZER ? rows : (uint32_t)*a.rank;
+  uint32_t pprev = 0xFFFFFFFFu;  // the last pivot row, whose Pauli is not written yet
+  uint8_t phprev = 0;
+  uint32_t j = a.j0;
+  for (; j < a.k; j++) {
+    uint64_t* P = Pb[j & 1];
+    const uint64_t* Pp = Pb[(j + 1) & 1];  // the previous Pauli
+    const uint64_t* pj = a.paulis + (size_t)j * W;
+    for (uint32_t w = tid; w < W; w += blockDim.x) P[w] = pj[w];
+    __syncthreads();
+    if (lead && pprev != 0xFFFFFFFFu) {
+      for (uint32_t w = tid; w < W; w += blockDim.x) a.xzs[(size_t)pprev * W + w] = Pp[w];
+      if (tid == 0) a.ph[pprev] = phprev;
+    }
+    if (lead && tid == 0) g.gmin[(j + 1) % 3] = 0xFFFFFFFFu;  // the slot of Pauli j + 1 (last used by j - 2)
+    // 1. comm flags and the first anticommuting stabilizer row
+    for (uint32_t m = gw; m < rows; m += NW) {
+      const uint64_t* row = m == pprev ? Pp : a.xzs + (size_t)m * W;
+      uint64_t acc = 0;
+      for (uint32_t w = lane; w < len; w += 32) acc ^= (P[len + w] & row[w]) ^ (P[w] & row[len + w]);
+      const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)__popcll(acc)) & 1u;
+      if (lane == 0) {
+        a.flags[m] = (uint8_t)c;
+        if (c && m < r) atomicMin(&g.gmin[j % 3], m);
+      }
+    }
+    if (!grid_barrier(g.bar, G, g.err)) return;
+    // 2. the decision, the same in every CTA
+    const uint32_t p = *(volatile uint32_t*)&g.gmin[j % 3];
+    const int32_t rp = a.rand_ph ? (int32_t)a.rand_ph[j] : -1;
+    if (p == 0xFFFFFFFFu) {
+      // commutes with every stabilizer row
+      pprev = 0xFFFFFFFFu;  // written in this Pauli's phase 1
+      if (a.kind == QCB_STABILIZER && !a.keep_result) {
+        if (lead && tid == 0) { a.anticom[j] = 0; a.result[j] = -1; }
+        continue;  // phase 2 wrote nothing: no barrier needed
+      }
+      if (lead && tid == 0) { a.status[0] = PST_NEED_CANON; a.status[1] = (int32_t)j; }
+      return;
+    }
+    for (uint32_t w = tid; w < W; w += blockDim.x) piv[w] = a.xzs[(size_t)p * W + w];
+    __syncthreads();
+    const uint32_t pph = a.ph[p];
+    for (uint32_t m = p + 1 + gw; m < r; m += NW)
+      if (a.flags[m]) warp_rowmul(a.xzs, a.ph, W, m, piv, pph, a.phases != 0, lane);
+    if (lead && tid == 0) { a.anticom[j] = (int32_t)p + 1; a.result[j] = rp; }
+    phprev = (uint8_t)(rp >= 0 ? rp : (int32_t)a.pph[j]);
+    pprev = p;
+    if (!grid_barrier(g.bar, G, g.err)) return;
+  }
+  if (lead && pprev != 0xFFFFFFFFu) {
+    const uint64_t* Pp = Pb[(j + 1) & 1];
+    for (uint32_t w = tid; w < W; w += blockDim.x) a.xzs[(size_t)pprev * W + w] = Pp[w];
+    if (tid == 0) a.ph[pprev] = phprev;
+  }
+  if (lead && tid == 0) { a.status[0] = PST_OK; a.status[1] = (int32_t)a.k; }
+}
+
 static uint32_t g_proj_cs = 0;  // tuner override (0 = automatic)
+static uint32_t g_proj_grid = 0;  // the whole-GPU kernel: 0 automatic, 1 always (where it applies), 2 never
 
 }  // namespace qcb
 
@@ -727,6 +845,21 @@ static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64
     QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, device_max_smem_optin() - 1024));  // it has static shared memory too
     if (cs > 8) QCB_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   }
+  // generic Paulis on a Stabilizer / MixedStabilizer tableau that does not
+  // fit one cluster's shared memory: the whole GPU (project_grid_kernel)
+  const size_t gsm = (size_t)3 * W * 8;
+  const bool grid = g_proj_grid != 2 && !qubits && (kind == QCB_STABILIZER || kind == QCB_MIXED_STABILIZER) &&
+                    (g_proj_grid == 1 || !use_smem) && gsm <= maxsm;
+  uint32_t G = 0;
+  uint32_t* d_bar = nullptr;  // [0..1] barrier, [2..4] first anticommuting rows, [5] timeout flag
+  if (grid) {
+    if (gsm > 48 * 1024)
+      QCB_CUDA(cudaFuncSetAttribute(project_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
+    int nb = 0;
+    QCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, project_grid_kernel, PROJ_THREADS, gsm));
+    G = (uint32_t)std::max(1, nb) * (uint32_t)std::max(device_sm_count(), 1);
+    QCB_CUDA(cudaMallocAsync(&d_bar, 32, st));
+  }
   int status = QCB_OK;
   uint32_t j0 = 0;
   std::vector<int32_t> h_anti(k, 0), h_res(k, -1);
@@ -749,7 +882,17 @@ static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (use_smem) {
+    int32_t htimeout = 0;
+    if (grid) {
+      QCB_CUDA(cudaMemsetAsync(d_bar, 0, 8, st));
+      QCB_CUDA(cudaMemsetAsync(d_bar + 2, 0xFF, 12, st));
+      QCB_CUDA(cudaMemsetAsync(d_bar + 5, 0, 4, st));
+      QCB_CUDA(cudaMemsetAsync(d_stat, 0xFF, 8, st));
+      ProjGridArgs ga{a, d_bar, d_bar + 2, (int32_t*)(d_bar + 5)};
+      void* args[] = {&ga};
+      QCB_CUDA(cudaLaunchCooperativeKernel((const void*)project_grid_kernel, dim3(G), dim3(PROJ_THREADS), args, gsm,
+                                           st));
+    } else if (use_smem) {
       ProjSmemArgs pa{a, RB};
       QCB_CUDA(cudaLaunchKernelEx(&cfg, project_smem_kernel, pa));
     } else {
@@ -758,7 +901,12 @@ static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64
     QCB_LAUNCHED();
     int32_t hs[2];
     QCB_CUDA(cudaMemcpyAsync(hs, d_stat, 8, cudaMemcpyDeviceToHost, st));
+    if (grid) QCB_CUDA(cudaMemcpyAsync(&htimeout, d_bar + 5, 4, cudaMemcpyDeviceToHost, st));
     QCB_CUDA(cudaStreamSynchronize(st));
+    if (htimeout) {
+      status = fail(QCB_ETIMEOUT, "project!: a grid barrier wait of the whole-GPU kernel expired");
+      break;
+    }
     if (hs[0] == PST_OK) break;
     const uint32_t j = (uint32_t)hs[1];
     if (hs[0] == PST_BADSTRUCT) {
@@ -837,6 +985,7 @@ static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64
   cudaFreeAsync(d_tmp, st); cudaFreeAsync(d_tmpph, st);
   if (d_q) cudaFreeAsync(d_q, st);
   if (d_rand) cudaFreeAsync(d_rand, st);
+  if (d_bar) cudaFreeAsync(d_bar, st);
   cudaStreamSynchronize(st);
   return status;
 }
@@ -882,4 +1031,5 @@ int qcb_projectrand(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tablea
 
 namespace qcb {
 void set_project_cluster(uint32_t cs) { g_proj_cs = cs; }
+void set_project_grid(uint32_t v) { g_proj_grid = v; }
 }

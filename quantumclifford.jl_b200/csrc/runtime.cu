@@ -55,6 +55,7 @@ void set_server_hash_bits(uint32_t b);
 void set_canon_cluster(uint32_t cs);
 void set_canon_threads(uint32_t n);
 void set_project_cluster(uint32_t cs);
+void set_project_grid(uint32_t v);
 void set_canon_blocked(uint32_t v);
 void set_canon_grid(uint32_t v);
 void set_server_fill(uint32_t v);
@@ -166,6 +167,12 @@ int qcb_tune_set(const char* key, int64_t value) {
   } else if (k == "canon_apply_rows") {
     if (value && (value < 8 || value > 32)) return fail(QCB_EARG, "canon_apply_rows must be 0 or 8..32");
     set_canon_apply_rows((uint32_t)value);
+  } else if (k == "project_grid") {
+    // project! of generic Paulis on Stabilizer / MixedStabilizer tableaux on
+    // the whole GPU: 0 when the tableau does not fit one cluster's shared
+    // memory, 1 always, 2 never
+    if (value > 2) return fail(QCB_EARG, "project_grid must be 0, 1 or 2");
+    set_project_grid((uint32_t)value);
   } else if (k == "project_cluster") {
     if (value && (value > 16 || (value & (value - 1)))) return fail(QCB_EARG, "project_cluster must be 1, 2, 4, 8 or 16");
     set_project_cluster((uint32_t)value);

@@ -213,6 +213,48 @@ def test_project_sequences(qcb, kind, n):
         assert st.rank == orank
 
 
+@pytest.mark.parametrize("kind", ["Stabilizer", "MixedStabilizer"])
+@pytest.mark.parametrize("n", [5, 64, 200])
+@pytest.mark.parametrize("keep_result,phases", [(True, True), (False, True), (True, False)])
+def test_project_sequences_whole_gpu(qcb, kind, n, keep_result, phases):
+    """project! of generic Paulis on Stabilizer / MixedStabilizer tableaux by
+    the whole-GPU kernel (project_grid 1: a cooperative grid, two grid
+    barriers per Pauli, the pivot row written one Pauli later), forced on
+    small tableaux; sequences mixing anticommuting Paulis with stabilizer
+    rows and their products (the commuting branch), bit for bit against the
+    oracle."""
+    rng = np.random.default_rng(zlib.crc32(f"grid{kind}{n}{keep_result}{phases}".encode()))
+    d = dev_random_destabilizer(qcb, n, rng)
+    k = 40
+    paulis = _random_paulis(k, n, rng)
+    for j in range(0, k, 5):
+        paulis.xzs[j] = d.tab.xzs[n + (j % n)]
+        paulis.phases[j] = (d.tab.phases[n + (j % n)] + 2 * (j % 2)) & 3
+    for j in range(3, k, 7):  # the Pauli just projected, again
+        paulis.xzs[j], paulis.phases[j] = paulis.xzs[j - 1], paulis.phases[j - 1]
+    rank = 0
+    tab = Tableau(d.tab.phases[n:].copy(), n, d.tab.xzs[n:].copy())
+    if kind == "MixedStabilizer":
+        rank = max(1, n // 2)
+        tab.xzs[rank:] = 0
+        tab.phases[rank:] = 0
+        st = qcb.MixedStabilizer(tab.copy(), rank)
+    else:
+        st = qcb.Stabilizer(tab.copy())
+    st.to_gpu()
+    qcb.check(qcb.lib().qcb_tune_set(b"project_grid", 1))
+    try:
+        _, anti, res = qcb.project_(st, paulis.copy().to_gpu(), keep_result=keep_result, phases=phases)
+    finally:
+        qcb.check(qcb.lib().qcb_tune_set(b"project_grid", 0))
+    st.to_cpu()
+    ph, xz, orank, outs = oracle_project_seq(kind, tab, paulis, n, rank, keep_result, phases)
+    assert list(zip(anti, res)) == outs
+    assert np.array_equal(st.tab.xzs, xz) and np.array_equal(st.tab.phases, ph)
+    if kind == "MixedStabilizer":
+        assert st.rank == orank
+
+
 def test_project_keep_result_false_and_phases_false(qcb):
     n = 50
     rng = np.random.default_rng(8)

@@ -653,6 +653,9 @@ struct ProjGridArgs {
   uint32_t* bar;   // [0] arrivals, [1] generation
   uint32_t* gmin;  // [3]: the first anticommuting row of Pauli j at gmin[j % 3]
   int32_t* err;    // QCB_ETIMEOUT when a grid barrier wait gave up
+  // test knob: CTA 1 leaves before the first barrier, so the others' waits
+  // run out (0: off)
+  uint32_t withhold;
 };
 
 // Bounded grid barrier; false when this CTA gave up waiting.
@@ -671,7 +674,7 @@ __device__ bool grid_barrier(uint32_t* bar, uint32_t nblocks, int32_t* err) {
     } else {
       uint32_t it = 0;
       while (*gen == g0) {
-        if (++it > (1u << 26)) {
+        if (++it > (1u << 24)) {  // about a second
           ok = 0;
           atomicExch(err, QCB_ETIMEOUT);
           break;
@@ -720,6 +723,7 @@ __global__ void __launch_bounds__(PROJ_THREADS) project_grid_kernel(const ProjGr
         if (c && m < r) atomicMin(&g.gmin[j % 3], m);
       }
     }
+    if (g.withhold && blockIdx.x == 1) return;
     if (!grid_barrier(g.bar, G, g.err)) return;
     // 2. the decision, the same in every CTA
     const uint32_t p = *(volatile uint32_t*)&g.gmin[j % 3];
@@ -754,6 +758,7 @@ __global__ void __launch_bounds__(PROJ_THREADS) project_grid_kernel(const ProjGr
 
 static uint32_t g_proj_cs = 0;  // tuner override (0 = automatic)
 static uint32_t g_proj_grid = 0;  // the whole-GPU kernel: 0 automatic, 1 always (where it applies), 2 never
+static uint32_t g_proj_withhold = 0;  // test knob, see ProjGridArgs::withhold
 
 }  // namespace qcb
 
@@ -888,7 +893,7 @@ static int project_impl(qcb_tableau* t, int kind, int32_t* rank_io, const uint64
       QCB_CUDA(cudaMemsetAsync(d_bar + 2, 0xFF, 12, st));
       QCB_CUDA(cudaMemsetAsync(d_bar + 5, 0, 4, st));
       QCB_CUDA(cudaMemsetAsync(d_stat, 0xFF, 8, st));
-      ProjGridArgs ga{a, d_bar, d_bar + 2, (int32_t*)(d_bar + 5)};
+      ProjGridArgs ga{a, d_bar, d_bar + 2, (int32_t*)(d_bar + 5), G > 1 ? g_proj_withhold : 0u};
       void* args[] = {&ga};
       QCB_CUDA(cudaLaunchCooperativeKernel((const void*)project_grid_kernel, dim3(G), dim3(PROJ_THREADS), args, gsm,
                                            st));
@@ -1032,4 +1037,5 @@ int qcb_projectrand(qcb_tableau* t, int kind, int32_t* rank_io, const qcb_tablea
 namespace qcb {
 void set_project_cluster(uint32_t cs) { g_proj_cs = cs; }
 void set_project_grid(uint32_t v) { g_proj_grid = v; }
+void set_project_withhold(uint32_t v) { g_proj_withhold = v; }
 }

@@ -56,6 +56,7 @@ void set_canon_cluster(uint32_t cs);
 void set_canon_threads(uint32_t n);
 void set_project_cluster(uint32_t cs);
 void set_project_grid(uint32_t v);
+void set_project_withhold(uint32_t v);
 void set_canon_blocked(uint32_t v);
 void set_canon_grid(uint32_t v);
 void set_server_fill(uint32_t v);
@@ -173,6 +174,12 @@ int qcb_tune_set(const char* key, int64_t value) {
     // memory, 1 always, 2 never
     if (value > 2) return fail(QCB_EARG, "project_grid must be 0, 1 or 2");
     set_project_grid((uint32_t)value);
+  } else if (k == "project_withhold") {
+    // test knob: one CTA of the whole-GPU project! kernel leaves before the
+    // first grid barrier, so the others' bounded waits run out and the call
+    // returns QCB_ETIMEOUT (nothing faults)
+    if (value > 1) return fail(QCB_EARG, "project_withhold must be 0 or 1");
+    set_project_withhold((uint32_t)value);
   } else if (k == "project_cluster") {
     if (value && (value > 16 || (value & (value - 1)))) return fail(QCB_EARG, "project_cluster must be 1, 2, 4, 8 or 16");
     set_project_cluster((uint32_t)value);

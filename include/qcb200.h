@@ -336,7 +336,20 @@ int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t see
  * knob "server_hash_bits" b > 0: the serving program cache keeps only b low
  * bits of its hash, so distinct circuits collide (the byte comparison on a
  * hit keeps results right).  Knob "server_fill" (read by qcb_server_create):
- * 1 (default) admits onto idle SMs only, 0 whenever a slot is free.         */
+ * 1 (default) admits onto idle SMs only, 0 whenever a slot is free.
+ * canonicalize! by panels over the whole GPU: "canon_grid" 0 (automatic:
+ * stabilizer views of 640..8192 rows) / 1 always / 2 never; "canon_rpt"
+ * rows per pivot-search thread (0: automatic, 1, 2, 4, 8, 16);
+ * "canon_apply_rows" rows per apply CTA (0 or 8..32); "canon_pdl" 1
+ * (default) / 0: the panel launches as programmatic dependent launches or
+ * plain.  project! on the whole GPU: "project_grid" 0 (automatic: generic
+ * Paulis on Stabilizer kinds too tall for one cluster's shared memory) / 1
+ * always where it applies / 2 never.  Test knob "project_withhold" 1: one CTA
+ * of that kernel leaves before the first grid barrier, the others' bounded
+ * waits expire and the call returns QCB_ETIMEOUT (nothing faults).  Noise:
+ * "presample" 0 (automatic) / 1 never (draw in the walk) / 2 every bucket
+ * overflows (test).  "walker_threads" threads per walker CTA (0: 640, or
+ * 64..640 in steps of 32).                                                   */
 int qcb_tune_set(const char* key, int64_t value);
 
 /* ------------------------------------------------------------ tableaux    */

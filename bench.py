@@ -62,6 +62,28 @@ def load_peaks():
     return 6650.0, "fallback 6650 GB/s (no measured hbm_gbs in MEASURED_PEAKS.json)"
 
 
+def clocks_snapshot(device_index: int = 0):
+    """One nvidia-smi reading of the SM clock, its maximum and the throttle
+    reasons (the launch-bound tableau timings are read right after their timed
+    region: a sampler polling during a call of hundreds of launches stalls the
+    launching thread and shows up as idle device time)."""
+    try:
+        r = subprocess.run(["nvidia-smi", "-i", str(device_index), f"--query-gpu={ClockSampler.FIELDS}",
+                            "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=20)
+    except (FileNotFoundError, subprocess.TimeoutExpired):
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "when": "after"}
+    parts = [p.strip() for p in r.stdout.strip().split(",")]
+    if len(parts) < 9:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unreadable"], "when": "after"}
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    try:
+        sm, mx = float(parts[1]), float(parts[2])
+    except ValueError:
+        sm = mx = None
+    return {"sm_mhz": sm, "sm_max_mhz": mx, "reasons": [nm for nm, v in zip(names, parts[5:9]) if v == "Active"],
+            "when": "right after the timed calls"}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -214,9 +236,19 @@ def bench_tableau(args):
     peak, peak_kind = load_peaks()
     rng = np.random.default_rng(2024)
 
-    def device_ms(fn, reps, setup=None, warm=3):
+    def device_ms(fn, reps, setup=None, warm=3, warm_s=0.25):
+        # warm-up: at least `warm` calls and `warm_s` seconds of them, so that
+        # the SM clock is back up after the host-only oracle runs in between
         ts = []
-        for i in range(warm + reps):
+        t0 = time.perf_counter()
+        i = 0
+        while i < warm or (time.perf_counter() - t0 < warm_s and i < 400):
+            if setup:
+                setup()
+            fn()
+            torch.cuda.synchronize()
+            i += 1
+        for _ in range(reps):
             if setup:
                 setup()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -224,8 +256,9 @@ def bench_tableau(args):
             fn()
             e1.record(stream)
             torch.cuda.synchronize()
-            if i >= warm:
-                ts.append(e0.elapsed_time(e1))
+            ts.append(e0.elapsed_time(e1))
+        last_clocks[0] = clocks_snapshot(0)
+        last_spread[0] = {"reps": len(ts), "min_ms": min(ts), "median_ms": statistics.median(ts), "max_ms": max(ts)}
         return statistics.median(ts)
 
     def cpu_ms(fn, reps=3):
@@ -236,6 +269,10 @@ def bench_tableau(args):
             ts.append((time.perf_counter() - t0) * 1e3)
         return statistics.median(ts)
 
+    lines = []  # printed at the end
+    last_clocks = [None]  # the clocks read right after the last timed region
+    last_spread = [None]  # min / median / max of the last timed region's calls
+
     def emit(metric, key, ms, config, cpu, extra=None):
         out = {"metric": metric, "value": ms, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": 3,
                "ms_per_step": ms, "higher_is_better": False, "scaling": "none",
@@ -243,9 +280,11 @@ def bench_tableau(args):
                "data": "synthetic (seeded)", "config": config, "gpu_launches": None,
                "cpu_baseline": {"value": cpu, "unit": "ms", "cores": 1, "kind": "port",
                                 "sample": "the oracle on the same input, one thread"}}
+        out["clocks"] = last_clocks[0]
+        out["spread"] = last_spread[0]
         if extra:
             out.update(extra)
-        print(json.dumps(out), flush=True)
+        lines.append(out)
 
     only = set(x for x in (args.tableau_only or "").split(",") if x)
 
@@ -323,7 +362,7 @@ def bench_tableau(args):
             ms = device_ms(lambda: check(L.qcb_project(state.tab.dev.handle, Q.KIND[kind], ctypes.byref(rank),
                                                        P.dev.handle, 1, 1, ptr(anti), ptr(res), ctypes.byref(done),
                                                        sp)),
-                           max(3, args.steps // 4),
+                           max(7, args.steps // 2),
                            setup=lambda: check(L.qcb_tableau_copy(state.tab.dev.handle, pristine.handle, sp)))
             state.to_cpu()
             # the oracle: the same sequence on the host, one thread
@@ -422,7 +461,7 @@ def bench_tableau(args):
             for _ in range(K):
                 check(L.qcb_apply_gates(work.dev.handle, ptr(gate), 1, 1, cs))
         per_graph = L.qcb_launch_count() - n_before
-        ms = device_ms(lambda: graph.replay(), max(3, args.steps // 4)) / K
+        ms = device_ms(lambda: graph.replay(), max(7, args.steps // 2)) / K
         work.to_cpu()
         assert np.array_equal(work.xzs, src.xzs) and np.array_equal(work.phases, src.phases)
         check(L.qcb_apply_gates(work.dev.handle, ptr(gate), 1, 1, sp))
@@ -436,6 +475,9 @@ def bench_tableau(args):
              {"gpu_launches": per_graph, "single_call_ms": single,
               "single_call_note": "one call between CUDA events, Python ctypes overhead included"})
         del graph
+
+    for out in lines:
+        print(json.dumps(out), flush=True)
 
 
 def bench_batch(args):

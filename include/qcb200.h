@@ -148,6 +148,10 @@ typedef struct qcb_frame qcb_frame;
 typedef struct qcb_tableau qcb_tableau;
 
 /* ------------------------------------------------------------ library     */
+/* Select the device and create its context.  Also raises the release
+ * threshold of the device's default stream-ordered memory pool to at least
+ * 1 GB, so that the per-call scratch of the tableau calls stays in the pool
+ * between calls instead of being mapped through the driver each time.      */
 int qcb_init(int device);
 const char* qcb_version(void);
 int qcb_last_error(char* buf, size_t len);

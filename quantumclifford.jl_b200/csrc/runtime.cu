@@ -76,6 +76,20 @@ int qcb_init(int device) {
   if (device < 0 || device >= n) return fail(QCB_EBOUNDS, "qcb_init: no such device");
   QCB_CUDA(cudaSetDevice(device));
   QCB_CUDA(cudaFree(0));
+  // keep up to 1 GB of freed stream-ordered memory in the device's default
+  // pool: the per-call scratch of the tableau kernels (cudaMallocAsync /
+  // cudaFreeAsync) is then taken from the pool instead of being mapped
+  // through the driver on every call (with the default threshold of 0 the
+  // pool returns it at each synchronisation)
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    if (thr < (1ull << 30)) {
+      thr = 1ull << 30;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  }
   return QCB_OK;
 }
 

@@ -353,7 +353,8 @@ int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t see
  * waits expire and the call returns QCB_ETIMEOUT (nothing faults).  Noise:
  * "presample" 0 (automatic) / 1 never (draw in the walk) / 2 every bucket
  * overflows (test).  "walker_threads" threads per walker CTA (0: 640, or
- * 64..640 in steps of 32).                                                   */
+ * 64..640 in steps of 32); "walker_pdl" 1 (default) / 0: the walker as a
+ * programmatic dependent launch of the noise pre-sampler or plain.          */
 int qcb_tune_set(const char* key, int64_t value);
 
 /* ------------------------------------------------------------ tableaux    */

@@ -395,6 +395,10 @@ struct PresampleArgs {
 };
 
 __global__ void __launch_bounds__(256) presample_kernel(const PresampleArgs p) {
+  // the walker that reads these buckets is a programmatic dependent: let it
+  // launch once every sampler CTA is resident, so that its CTAs take the SMs
+  // of the sampler's last wave as they free up (it waits before its first read)
+  asm volatile("griddepcontrol.launch_dependents;");
   const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
   const bool valid = e < p.nent;
   const uint4 pe = valid ? p.ent[e] : make_uint4(0u, 0u, 0xFFFFFFFFu, 0u);
@@ -518,6 +522,9 @@ __device__ __forceinline__ bool walk_tile(const WalkArgs& a, uint32_t* sm, uint3
     pf_e0 = offn + pl < a.pre_capg ? __ldg(pbase + offn + pl) : 0u;
     pf_e1 = offn + pl + pS < a.pre_capg ? __ldg(pbase + offn + pl + pS) : 0u;
   };
+  // the pre-sampler's buckets are complete from here on (a no-op unless this
+  // launch is its programmatic dependent; the initial frame above overlaps it)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   prefetch(0, 0);
 
   // ---- the program, window by window
@@ -1149,6 +1156,7 @@ static uint32_t g_presample = 0;          // 0: automatic, 1: never, 2: every bu
 // needs more draws its noise in the walk.
 constexpr uint64_t PRESAMPLE_MAX_BYTES = 512ull << 20;
 static uint32_t g_threads_override = 0;  // threads per CTA (0: WALKER_THREADS)
+static uint32_t g_walker_pdl = 1;        // the walker as a programmatic dependent of the pre-sampler
 
 // Tile width (even: threads own column pairs) for ncols columns with tiles of
 // at most tmax columns: the fewest waves of one CTA per SM, then the narrowest
@@ -1391,7 +1399,18 @@ int launch_walker(qcb_frame* f, const qcb_program* p, WalkArgs& a, bool philox, 
     QCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   (int)cudaSharedmemCarveoutMaxShared));
   }
-  kern<<<wc.grid, wc.nth, wc.smem_bytes, st>>>(a);
+  // after the pre-sampler, as its programmatic dependent
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(wc.grid);
+  cfg.blockDim = dim3(wc.nth);
+  cfg.dynamicSmemBytes = wc.smem_bytes;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = (a.pre_buf && g_walker_pdl) ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  QCB_CUDA(cudaLaunchKernelEx(&cfg, kern, (const WalkArgs)a));
   QCB_LAUNCHED();
   return QCB_OK;
 }
@@ -1774,6 +1793,7 @@ extern "C" int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* p, uint
 // Internal hooks for the batched runner and the tuner.
 namespace qcb {
 void set_walker_tile(uint32_t t) { g_tile_override = t; }
+void set_walker_pdl(uint32_t v) { g_walker_pdl = v; }
 void set_walker_threads(uint32_t t) { g_threads_override = t; }
 void set_stage_withhold(uint32_t k) { g_stage_withhold = k; }
 void set_presample(uint32_t v) { g_presample = v; }

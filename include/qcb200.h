@@ -247,6 +247,17 @@ int qcb_batch_destroy(qcb_batch* b);
  * per frame column for the program's size class (its touched qubits), which
  * qcb_batch_create then uses.  Synchronises the device.                     */
 int qcb_tune_tile(const qcb_program* program, uint32_t* tile, float* us_per_column, void* stream);
+/* The plain walker's autotuner: times `program` on a scratch frame of
+ * `frames` shots for the tile widths (the cost model's choice and the
+ * power-of-two widths that fit shared memory) and 448 / 512 / 576 / 640
+ * threads per CTA, and records the fastest pair for the program's size class
+ * (its touched qubits) at that frame width: later fresh runs of exactly that
+ * width take it (results are identical for any launch shape).  Returns the
+ * pair and its time per run.  Synchronises the device.
+ * qcb_tune_walker_clear forgets every recorded pair.                       */
+int qcb_tune_walker(const qcb_program* program, uint64_t frames, uint32_t* tile, uint32_t* threads,
+                    float* ms, void* stream);
+int qcb_tune_walker_clear(void);
 
 /* ------------------------------------------------------------ serving
  * A request loop with continuous batching (no reference counterpart).

@@ -1157,6 +1157,7 @@ static uint32_t g_presample = 0;          // 0: automatic, 1: never, 2: every bu
 constexpr uint64_t PRESAMPLE_MAX_BYTES = 512ull << 20;
 static uint32_t g_threads_override = 0;  // threads per CTA (0: WALKER_THREADS)
 static uint32_t g_walker_pdl = 1;        // the walker as a programmatic dependent of the pre-sampler
+static uint32_t g_walker_narrow = 1;     // 8..14-column shared-memory tiles for tall programs (0: HBM planes)
 
 // Tile width (even: threads own column pairs) for ncols columns with tiles of
 // at most tmax columns: the fewest waves of one CTA per SM, then the narrowest
@@ -1181,12 +1182,12 @@ static uint32_t balanced_tile(uint64_t ncols, uint32_t tmax) {
 // 8.02; d = 21: 28 14.36, 16 16.75; d = 23: 22 20.21, 16 20.73; d = 25: 16
 // 24.77, 18 28.69; d = 15 (2^22 shots): 56 7.96, 32 9.90; all of them the
 // model's choice.
-static uint32_t smem_tile(uint64_t ncols, uint32_t tmax) {
+static uint32_t smem_tile(uint64_t ncols, uint32_t tmax, uint32_t tmin = 16) {
   tmax &= ~1u;
   const uint64_t nsm = (uint64_t)std::max(device_sm_count(), 1);
-  uint32_t best = 16;
+  uint32_t best = tmin;
   uint64_t best_cost = UINT64_MAX;
-  for (uint32_t t = 16; t <= tmax; t += 2) {
+  for (uint32_t t = tmin; t <= tmax; t += 2) {
     const uint64_t waves = ((ncols + t - 1) / t + nsm - 1) / nsm;
     const uint64_t k = (t & (t - 1)) == 0 ? 75 : t == 18 ? 110 : 100;
     const uint64_t cost = waves * (2500 + k * t);
@@ -1194,6 +1195,15 @@ static uint32_t smem_tile(uint64_t ncols, uint32_t tmax) {
   }
   return best;
 }
+
+// The plain walker's autotuner table (qcb_tune_walker): the fastest tile
+// width and threads per CTA measured for a program size class (touched
+// qubits) at a frame width (columns); used by runs of exactly that width.
+struct WalkerTune {
+  uint32_t T, threads;
+};
+static std::map<std::pair<uint32_t, uint64_t>, WalkerTune> g_tuned_walker;
+static std::mutex g_tuned_walker_mu;
 
 // Shared-memory tile when 2 planes x 16 columns of every touched qubit fit,
 // else the same walker on the HBM planes.
@@ -1204,12 +1214,26 @@ static WalkConfig walk_config(const qcb_program* p, const qcb_frame* f) {
   const size_t maxsm = (size_t)device_max_smem_optin();
   const size_t budget = maxsm > stage ? maxsm - stage : 0;
   uint32_t T = 0;
-  if (g_tile_override && per_col * g_tile_override <= budget) {
+  uint32_t tuned_threads = 0;
+  if (!g_tile_override && !g_threads_override) {
+    std::lock_guard<std::mutex> lk(g_tuned_walker_mu);
+    auto it = g_tuned_walker.find({p->nslots, f->ncols});
+    if (it != g_tuned_walker.end() && per_col * it->second.T <= budget) {
+      T = it->second.T;
+      tuned_threads = it->second.threads;
+    }
+  }
+  if (T) {
+  } else if (g_tile_override && per_col * g_tile_override <= budget) {
     T = g_tile_override;
   } else if (budget / per_col >= 16) {
     T = smem_tile(f->ncols, (uint32_t)std::min<size_t>(256, budget / per_col));
+  } else if (g_walker_narrow && budget / per_col >= 8) {
+    // tall programs (d >= 29 surface codes): 8..14-column tiles keep the
+    // frame in shared memory instead of walking the HBM planes
+    T = smem_tile(f->ncols, (uint32_t)(budget / per_col), 8);
   }
-  const uint32_t threads = g_threads_override ? g_threads_override : WALKER_THREADS;
+  const uint32_t threads = g_threads_override ? g_threads_override : tuned_threads ? tuned_threads : WALKER_THREADS;
   if (T) {
     wc.smem = true;
     wc.T = T;
@@ -1794,6 +1818,7 @@ extern "C" int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* p, uint
 namespace qcb {
 void set_walker_tile(uint32_t t) { g_tile_override = t; }
 void set_walker_pdl(uint32_t v) { g_walker_pdl = v; }
+void set_walker_narrow(uint32_t v) { g_walker_narrow = v; }
 void set_walker_threads(uint32_t t) { g_threads_override = t; }
 void set_stage_withhold(uint32_t k) { g_stage_withhold = k; }
 void set_presample(uint32_t v) { g_presample = v; }
@@ -1933,6 +1958,74 @@ int qcb_batch_destroy(qcb_batch* b) {
 // frame of two full waves per candidate (fresh Philox runs, CUDA events) and
 // keep the width with the most frame columns per second for the program's
 // size class (its touched qubits); qcb_batch_create uses it.
+int qcb_tune_walker(const qcb_program* p, uint64_t frames, uint32_t* tile_out, uint32_t* threads_out,
+                    float* ms_out, void* stream) {
+  using namespace qcb;
+  if (!p) return fail(QCB_EARG, "null program");
+  if (!frames) return fail(QCB_EARG, "qcb_tune_walker: frames must be > 0");
+  const size_t per_col = (size_t)2 * std::max<uint32_t>(p->nslots, 1) * 4;
+  const size_t stage = (size_t)2 * p->win_words * 4 + 16 + 128;
+  const size_t maxsm = (size_t)device_max_smem_optin();
+  const uint32_t tmax = maxsm > stage ? (uint32_t)std::min<size_t>(256, (maxsm - stage) / per_col) & ~1u : 0u;
+  if (tmax < 8) return fail(QCB_EUNSUPPORTED, "the program's frame tile does not fit shared memory");
+  const uint64_t ncols = (frames + 31) / 32;
+  const uint32_t tmin = tmax >= 16 ? 16u : 8u;
+  std::vector<uint32_t> tiles = {smem_tile(ncols, tmax, tmin)};
+  for (uint32_t t : {8u, 16u, 32u, 64u, 128u, 256u})
+    if (t >= tmin && t <= tmax && std::find(tiles.begin(), tiles.end(), t) == tiles.end()) tiles.push_back(t);
+  const uint32_t threads[] = {448, 512, 576, 640};
+  cudaStream_t st = S(stream);
+  qcb_frame* f = nullptr;
+  if (int s0 = qcb_frame_create(frames, p->nq > 0 ? p->nq - 1 : 0, p->info.nbits, &f)) return s0;
+  cudaEvent_t e0, e1;
+  QCB_CUDA(cudaEventCreate(&e0));
+  QCB_CUDA(cudaEventCreate(&e1));
+  const uint32_t saved_t = g_tile_override, saved_th = g_threads_override;
+  uint32_t best_t = 0, best_th = 0;
+  float best_ms = 0.f;
+  int status = QCB_OK;
+  for (uint32_t T : tiles) {
+    for (uint32_t th : threads) {
+      if (th / (T / 2) == 0) continue;
+      g_tile_override = T;
+      g_threads_override = th;
+      float ms = 0.f;
+      for (int rep = 0; rep < 4 && status == QCB_OK; rep++) {
+        cudaEventRecord(e0, st);
+        status = run_program_fresh(f, p, 0x5EEDull + rep, 0, st);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) status = fail(QCB_ECUDA, "tuner timing");
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        if (rep > 0) ms = rep == 1 ? t : std::min(ms, t);  // rep 0 warms up
+      }
+      if (status != QCB_OK) break;
+      if (!best_t || ms < best_ms) { best_t = T; best_th = th; best_ms = ms; }
+    }
+    if (status != QCB_OK) break;
+  }
+  g_tile_override = saved_t;
+  g_threads_override = saved_th;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  qcb_frame_destroy(f);
+  if (status != QCB_OK) return status;
+  {
+    std::lock_guard<std::mutex> lk(g_tuned_walker_mu);
+    g_tuned_walker[{p->nslots, ncols}] = WalkerTune{best_t, best_th};
+  }
+  if (tile_out) *tile_out = best_t;
+  if (threads_out) *threads_out = best_th;
+  if (ms_out) *ms_out = best_ms;
+  return QCB_OK;
+}
+
+int qcb_tune_walker_clear(void) {
+  std::lock_guard<std::mutex> lk(qcb::g_tuned_walker_mu);
+  qcb::g_tuned_walker.clear();
+  return QCB_OK;
+}
+
 int qcb_tune_tile(const qcb_program* p, uint32_t* tile_out, float* us_per_column, void* stream) {
   using namespace qcb;
   if (!p) return fail(QCB_EARG, "null program");

@@ -63,6 +63,7 @@ void set_server_fill(uint32_t v);
 void set_canon_rpt(uint32_t v);
 void set_canon_pdl(uint32_t v);
 void set_walker_pdl(uint32_t v);
+void set_walker_narrow(uint32_t v);
 void set_canon_apply_rows(uint32_t v);
 
 }  // namespace qcb
@@ -176,6 +177,11 @@ int qcb_tune_set(const char* key, int64_t value) {
     if (value && value != 1 && value != 2 && value != 4 && value != 8 && value != 16)
       return fail(QCB_EARG, "canon_rpt must be 0, 1, 2, 4, 8 or 16");
     set_canon_rpt((uint32_t)value);
+  } else if (k == "walker_narrow") {
+    // tall programs whose 16-column tile does not fit shared memory: 8..14-
+    // column tiles (1, default) or the walker on the HBM planes (0)
+    if (value > 1) return fail(QCB_EARG, "walker_narrow must be 0 or 1");
+    set_walker_narrow((uint32_t)value);
   } else if (k == "walker_pdl") {
     // the frame walker as a programmatic dependent of the noise pre-sampler (1, default) or plain (0)
     if (value > 1) return fail(QCB_EARG, "walker_pdl must be 0 or 1");

@@ -19,7 +19,8 @@ from .ops import (  # noqa: F401
 )
 from .frames import (  # noqa: F401
     PauliFrame, Program, Masks, sample_masks, pftrajectories, pauliframe_, measurements,
-    pftrajectories_record, unpack_record, pack_record, evaluate_guesses, Batch, tune_tile, Server,
+    pftrajectories_record, unpack_record, pack_record, evaluate_guesses, Batch, tune_tile, tune_walker,
+    tune_walker_clear, Server,
 )
 from .tableau import (  # noqa: F401
     Tableau, PauliOperator, Stabilizer, MixedStabilizer, Destabilizer, MixedDestabilizer, CliffordOperator,

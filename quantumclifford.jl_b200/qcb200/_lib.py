@@ -186,6 +186,8 @@ def lib():
         "qcb_server_destroy": ([vp], ctypes.c_int),
         "qcb_server_stats": ([vp, P(u64), P(u64), P(u32)], ctypes.c_int),
         "qcb_tune_tile": ([vp, P(u32), P(ctypes.c_float), vp], ctypes.c_int),
+        "qcb_tune_walker": ([vp, ctypes.c_uint64, P(u32), P(u32), P(ctypes.c_float), vp], ctypes.c_int),
+        "qcb_tune_walker_clear": ([], ctypes.c_int),
         "qcb_frame_measurement_columns": ([vp, vp, sz, vp, vp, vp], ctypes.c_int),
         "qcb_frame_syndrome_rows": ([vp, vp, sz, vp, ctypes.c_int, vp], ctypes.c_int),
         "qcb_evaluate_guesses": ([vp, vp, sz, vp, sz, vp, P(u64), vp], ctypes.c_int),

@@ -367,6 +367,23 @@ def tune_tile(program: Program, stream=None):
     return t.value, us.value
 
 
+def tune_walker(program: Program, frames: int, stream=None):
+    """The plain walker's autotuner (qcb_tune_walker): the fastest (tile width,
+    threads per CTA) for the program at `frames` shots, recorded for later
+    fresh runs of that width.  Returns (tile, threads, ms per run)."""
+    t = ctypes.c_uint32()
+    th = ctypes.c_uint32()
+    ms = ctypes.c_float()
+    check(lib().qcb_tune_walker(program.handle, int(frames), ctypes.byref(t), ctypes.byref(th), ctypes.byref(ms),
+                                stream))
+    return t.value, th.value, ms.value
+
+
+def tune_walker_clear():
+    """Forget every pair the walker's autotuner recorded."""
+    check(lib().qcb_tune_walker_clear())
+
+
 class Server:
     """The serving loop (qcb_server_*): submit sampling requests at any time;
     a scheduler thread admits them against an HBM budget and a number of

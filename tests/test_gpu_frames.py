@@ -193,12 +193,13 @@ def test_tall_program_16k_windows_bit_exact(qcb, mode):
     assert np.array_equal(coding(f.xzs(), f.qubits + 1), coding(ox, f.qubits + 1))
 
 
-@pytest.mark.parametrize("tile", [0, 16, 40, 106, 256])
+@pytest.mark.parametrize("tile", [0, 8, 12, 16, 40, 106, 256])
 @pytest.mark.parametrize("d,p", [(5, 0.004), (3, 0.015), (3, 1e-4)])
 def test_philox_sparse_noise_any_tile_width(qcb, tile, d, p):
     # sparse sites (p_eff * 1024 <= 16): Binomial counts, distinct positions,
-    # several events per group at p = 0.015; tiles of 16/40/106 columns cut
-    # 1024-shot groups, which both neighbouring tiles draw
+    # several events per group at p = 0.015; tiles of 12/16/40/106 columns cut
+    # 1024-shot groups, which both neighbouring tiles draw; 8-column tiles are
+    # the narrow tiles of tall programs
     arr = O.to_array(circuits.rotated_surface_code_memory(d, d, p))
     qmax, bmax = O.affected_counts(arr)
     frames = 9 * 1024 + 100
@@ -212,7 +213,7 @@ def test_philox_sparse_noise_any_tile_width(qcb, tile, d, p):
     assert np.array_equal(coding(f.xzs(), qmax + 1), coding(ox, qmax + 1))
 
 
-@pytest.mark.parametrize("tile", [16, 40, 106])
+@pytest.mark.parametrize("tile", [8, 12, 16, 40, 106])
 def test_mask_mode_any_tile_width(qcb, tile):
     circ = circuits.rotated_surface_code_memory(3, 3, 0.01)
     qcb.check(qcb.lib().qcb_tune_set(b"walker_tile", tile))
@@ -450,3 +451,47 @@ def test_chunked_presampled_run_equals_one_launch(qcb):
     ox, om = oracle.pftrajectories_philox(arr, n, qmax, bmax, 99)
     assert np.array_equal(p0[:, : n // 32], qcb.pack_record(om))
     assert np.array_equal(x0[:, :n] & cm, ox & cm)
+
+
+@pytest.mark.parametrize("narrow", [1, 0])
+def test_tall_circuit_narrow_tiles(qcb, narrow):
+    """A d = 33 surface code (2,177 qubits): a 16-column tile of every touched
+    qubit does not fit shared memory, so the walker takes 8..14-column tiles
+    (walker_narrow 1, the default) or walks the HBM planes (0); both bit-exact
+    against the oracle, fresh Philox runs with pre-sampled noise."""
+    arr = O.to_array(circuits.rotated_surface_code_memory(33, 2, 2e-3))
+    qmax, bmax = O.affected_counts(arr)
+    frames = 5 * 1024 + 300
+    qcb.check(qcb.lib().qcb_tune_set(b"walker_narrow", narrow))
+    try:
+        f = qcb.pftrajectories(arr, trajectories=frames, seed=33)
+        rec = f.measurements()
+        xzs = f.xzs()
+    finally:
+        qcb.check(qcb.lib().qcb_tune_set(b"walker_narrow", 1))
+    ox, om = oracle.pftrajectories_philox(arr, frames, qmax, bmax, 33)
+    assert np.array_equal(rec, om)
+    assert np.array_equal(coding(xzs, qmax + 1), coding(ox, qmax + 1))
+
+
+def test_walker_autotuner_pairs_and_results(qcb):
+    """qcb_tune_walker times (tile, threads per CTA) pairs for a program at a
+    frame width and records the fastest; later fresh runs of that width take
+    it, and their record and frame are still bit-exact against the oracle
+    (any launch shape walks the same program on the same columns)."""
+    arr = O.to_array(circuits.rotated_surface_code_memory(7, 7, 3e-3))
+    qmax, bmax = O.affected_counts(arr)
+    prog = qcb.Program(arr)
+    frames = 20 * 1024 + 77
+    try:
+        tile, threads, ms = qcb.tune_walker(prog, frames)
+        assert tile % 2 == 0 and 8 <= tile <= 256 and threads in (448, 512, 576, 640) and ms > 0
+        f = qcb.PauliFrame(frames, qmax, bmax, init=False)
+        qcb.check(qcb.lib().qcb_pftrajectories_fresh(f.handle, prog.handle, 71, 0, None))
+        rec = f.measurements()
+        xzs = f.xzs()
+    finally:
+        qcb.tune_walker_clear()
+    ox, om = oracle.pftrajectories_philox(arr, frames, qmax, bmax, 71)
+    assert np.array_equal(rec, om)
+    assert np.array_equal(coding(xzs, qmax + 1), coding(ox, qmax + 1))

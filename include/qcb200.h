@@ -357,7 +357,8 @@ int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t see
  * rows per pivot-search thread (0: automatic, 1, 2, 4, 8, 16);
  * "canon_apply_rows" rows per apply CTA (0 or 8..32); "canon_pdl" 1
  * (default) / 0: the panel launches as programmatic dependent launches or
- * plain.  project! on the whole GPU: "project_grid" 0 (automatic: generic
+ * plain; "canon_lookahead" 1 (default) / 0: each panel's pivot steps run
+ * beside the previous panel's grid-wide apply, or the two in turn.  project! on the whole GPU: "project_grid" 0 (automatic: generic
  * Paulis on Stabilizer kinds too tall for one cluster's shared memory) / 1
  * always where it applies / 2 never.  Test knob "project_withhold" 1: one CTA
  * of that kernel leaves before the first grid barrier, the others' bounded
@@ -365,7 +366,9 @@ int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t see
  * "presample" 0 (automatic) / 1 never (draw in the walk) / 2 every bucket
  * overflows (test).  "walker_threads" threads per walker CTA (0: 640, or
  * 64..640 in steps of 32); "walker_pdl" 1 (default) / 0: the walker as a
- * programmatic dependent launch of the noise pre-sampler or plain.          */
+ * programmatic dependent launch of the noise pre-sampler or plain.
+ * "gates_pdl" 1 (default) / 0: qcb_apply_gates launches as programmatic
+ * dependents of the launch before them on the stream, or plain.            */
 int qcb_tune_set(const char* key, int64_t value);
 
 /* ------------------------------------------------------------ tableaux    */
@@ -546,7 +549,11 @@ int qcb_generate(qcb_tableau* pauli, const qcb_tableau* stab, int phases, int32_
                  int32_t* used_rows, uint32_t cap, uint32_t* n_used, void* stream);
 
 /* apply!(state, gates) for symbolic gates with phases
- * (src/symbolic_cliffords.jl:62-74, 293-316), applied in order.             */
+ * (src/symbolic_cliffords.jl:62-74, 293-316), applied in order.  Each launch
+ * (up to 128 gates) is a programmatic dependent of the launch before it on
+ * the stream, so a stream of single-gate calls overlaps each launch with the
+ * previous kernel; the kernel reads the rows only once its predecessor has
+ * completed, so the order of calls on the stream is kept.                   */
 int qcb_apply_gates(qcb_tableau* t, const qcb_op* ops, size_t n_ops, int phases, void* stream);
 
 /* Dense apply!(state, c::CliffordOperator; phases) (src/dense_cliffords.jl:135-169).

@@ -879,36 +879,47 @@ struct PanelArgs {
   int phases;
   uint32_t stage, c0;   // this panel: stage 0 (X) or 1 (Z), first column
   uint32_t* pos;        // [rows] row -> position (persistent)
-  PanelRec* rec;
+  PanelRec* rec;        // this panel's record
   uint64_t* po;         // [PANEL][W] the pivot rows at the panel start
   int32_t* out;         // [0] X-stage pivots, [1] next pivot position
+  // look-ahead schedule only
+  PanelRec* prev;       // the previous panel's record (its i / rx / done start this panel)
+  uint64_t* po_prev;    // the previous panel's pivot rows
+  uint64_t* nw;         // [rows] each row's word of this panel (of the next one, once written)
+  uint32_t wj_prev;     // word index of the previous panel (UINT32_MAX: none)
+  uint32_t wj_next;     // word index of the next panel (UINT32_MAX: none)
+  uint32_t steps;       // 1: this launch runs this panel's pivot steps
 };
 
+// The word index of a panel's columns in a row (X words, then Z words).
+__host__ __device__ inline uint32_t panel_word(uint32_t stage, uint32_t c0, uint32_t len) {
+  return stage * len + (c0 >> 6);
+}
+
+// (1) The panel's pivot steps on the panel words of the candidate rows
+// (positions >= the next pivot position), word(r) = wsrc[r * wstride]; the
+// positions of those rows are updated in `pos`, and the record g gets the
+// pivot rows, their columns, masks and words (stp, bt, A, PWP) and T, i, rx,
+// done, starting from prev's i / rx / done (prev may be g itself).
 template <uint32_t RPT>
-__global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const PanelArgs a) {
-  extern __shared__ __align__(16) uint64_t sm[];
-  // launched as a programmatic dependent of the previous panel's apply: wait
-  // for it (complete, its writes visible), then let the next launch in
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;");
-  PanelRec& g = *a.rec;
-  if (g.done) {  // every position has its pivot: this panel applies nothing
-    if (threadIdx.x == 0) g.T = 0;
-    return;
-  }
-  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-  const uint32_t R = a.rows, W = a.W, len = W / 2, n = a.n;
-  const uint32_t c0 = a.c0, ncp = min(PANEL, n - c0), wj = a.stage * len + (c0 >> 6);
-  uint64_t* XT = sm;                                   // XT[w * PANEL + t] = X word w of pivot t
-  uint64_t* ZT = XT + (size_t)len * PANEL;             // ZT[w * PANEL + t] = Z word w of pivot t
+__device__ __forceinline__ void panel_steps(const PanelArgs& a, const PanelRec& prev, PanelRec& g,
+                                            const uint64_t* wsrc, uint32_t wstride, uint32_t* cand) {
   __shared__ uint32_t stp[PANEL];
-  __shared__ uint8_t bt[PANEL], qo[PANEL];
-  __shared__ uint64_t A[PANEL], PWP[PANEL], C[PANEL], Dt[PANEL], Us[PANEL];
-  __shared__ uint8_t bases[PANEL];
+  __shared__ uint8_t bt[PANEL];
+  __shared__ uint64_t A[PANEL], PWP[PANEL];
   __shared__ uint64_t red2[2][32][3];
   __shared__ uint32_t shT, shI, ncand;
-  uint32_t* cand = (uint32_t*)(ZT + (size_t)len * PANEL);  // the candidate rows (position >= i)
-  uint32_t i = g.i;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t R = a.rows, n = a.n;
+  const uint32_t c0 = a.c0, ncp = min(PANEL, n - c0);
+  uint32_t i = prev.i;
+  const uint32_t rx0 = prev.rx;
+  if (prev.done) {  // every position has its pivot: this panel applies nothing
+    __syncthreads();  // every thread has read prev before g (maybe prev) is written
+    if (tid == 0) { g.T = 0; g.i = i; g.rx = rx0; g.done = 1; }
+    __syncthreads();
+    return;
+  }
   // Only rows at positions >= i can become pivots; the search runs on them
   // alone (the others' panel words do not matter to it), so it shrinks as
   // the elimination proceeds.
@@ -928,7 +939,7 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
       const uint32_t j = tid + k * nbt;
       rrow[k] = j < Rc ? cand[j] : 0xFFFFFFFFu;
       rpos[k] = j < Rc ? a.pos[rrow[k]] : 0xFFFFFFFFu;
-      rpw[k] = j < Rc ? a.xzs[(size_t)rrow[k] * W + wj] : 0ull;
+      rpw[k] = j < Rc ? wsrc[(size_t)rrow[k] * wstride] : 0ull;
       rcb[k] = 0;
     }
     // the steps (as blocked_body): one named barrier among the search warps
@@ -997,14 +1008,51 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
   __syncthreads();
   T = shT;
   i = shI;
+  for (uint32_t t = tid; t < T; t += blockDim.x) {
+    g.stp[t] = stp[t];
+    g.bt[t] = bt[t];
+    g.A[t] = A[t];
+    g.PWP[t] = PWP[t];
+  }
+  if (tid == 0) {
+    g.T = T;
+    g.i = i;
+    g.rx = a.stage == 0 ? i : rx0;
+    g.done = i >= R ? 1u : 0u;
+    a.out[0] = (int32_t)g.rx;
+    a.out[1] = (int32_t)i;
+  }
+  __syncthreads();  // the record is complete for the whole CTA
+}
+
+// (2) The pivot rows of the record g as they are at the panel start: copied
+// to po, their q = phase + |x & z|, and the panel's phase data (C, D_t and
+// the pivots' q, into g.Dt and g.qp).  wj: the panel's word index.
+__device__ __forceinline__ void panel_post(const PanelArgs& a, PanelRec& g, uint64_t* po, uint32_t wj,
+                                           uint64_t* XT) {
+  __shared__ uint32_t stp[PANEL];
+  __shared__ uint8_t bt[PANEL], qo[PANEL];
+  __shared__ uint64_t A[PANEL], PWP[PANEL], C[PANEL], Dt[PANEL], Us[PANEL];
+  __shared__ uint8_t bases[PANEL];
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t W = a.W, len = W / 2;
+  const uint32_t T = g.T;
+  uint64_t* ZT = XT + (size_t)len * PANEL;  // ZT[w * PANEL + t] = Z word w of pivot t
+  for (uint32_t t = tid; t < T; t += blockDim.x) {
+    stp[t] = g.stp[t];
+    bt[t] = g.bt[t];
+    A[t] = g.A[t];
+    PWP[t] = g.PWP[t];
+  }
+  __syncthreads();
   // the pivot rows at the panel start, their q = phase + |x & z|, XT, ZT
   for (uint32_t t = warp; t < T; t += nwarps) {
     const uint32_t r = stp[t];
     uint32_t s = 0;
     for (uint32_t w = lane; w < len; w += 32) {
       const uint64_t vx = a.xzs[(size_t)r * W + w], vz = a.xzs[(size_t)r * W + len + w];
-      a.po[(size_t)t * W + w] = vx;
-      a.po[(size_t)t * W + len + w] = vz;
+      po[(size_t)t * W + w] = vx;
+      po[(size_t)t * W + len + w] = vz;
       XT[(size_t)w * PANEL + t] = vx;
       ZT[(size_t)w * PANEL + t] = vz;
       s += __popcll(vx & vz);
@@ -1038,7 +1086,7 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
       const uint32_t t = tid;
       uint64_t u = 0;
       for (uint32_t x = 0; x < T; x++) u |= ((C[x] >> t) & 1ull) << x;
-      uint64_t pw = a.po[(size_t)t * W + wj], cm = 0, ut = 0;
+      uint64_t pw = po[(size_t)t * W + wj], cm = 0, ut = 0;
       uint32_t cross = 0;
       for (uint32_t t2 = 0; t2 < t; t2++) {
         if ((pw >> bt[t2]) & 1ull) {
@@ -1062,36 +1110,19 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
       }
     }
   }
-  // the record for the apply launch
-  for (uint32_t t = tid; t < T; t += blockDim.x) {
-    g.stp[t] = stp[t];
-    g.bt[t] = bt[t];
-    g.A[t] = A[t];
-    g.PWP[t] = PWP[t];
-    g.Dt[t] = a.phases ? Dt[t] : 0ull;
-  }
-  if (tid == 0) {
-    g.T = T;
-    g.i = i;
-    if (a.stage == 0) g.rx = i;
-    if (i >= R) g.done = 1;
-    a.out[0] = (int32_t)g.rx;
-    a.out[1] = (int32_t)i;
-  }
+  for (uint32_t t = tid; t < T; t += blockDim.x) g.Dt[t] = a.phases ? Dt[t] : 0ull;
 }
 
-// Rows r0 .. of the grid's share: apply the panel record (as blocked_body's
-// step 3, with rows and phases in global memory).
-__global__ void __launch_bounds__(CANON_THREADS) canon_apply_kernel(const PanelArgs a) {
-  extern __shared__ __align__(16) uint64_t sm[];
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;");
-  const PanelRec& g = *a.rec;
+// (3) Rows of block blk of nblk: apply the record g (pivot rows po at the
+// panel start, word index wj) to every row, as blocked_body's step 3 with
+// rows and phases in global memory.
+__device__ __forceinline__ void panel_apply(const PanelArgs& a, const PanelRec& g, const uint64_t* po,
+                                            uint32_t wj, uint32_t blk, uint32_t nblk, uint64_t* sm) {
   const uint32_t T = g.T;
   if (T == 0) return;
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5, bd = blockDim.x;
-  const uint32_t R = a.rows, W = a.W, len = W / 2, wj = a.stage * len + (a.c0 >> 6);
-  const uint32_t per = (R + gridDim.x - 1) / gridDim.x, r0 = blockIdx.x * per;
+  const uint32_t R = a.rows, W = a.W, len = W / 2;
+  const uint32_t per = (R + nblk - 1) / nblk, r0 = blk * per;
   const uint32_t nloc = r0 < R ? min(per, R - r0) : 0u;
   if (!nloc) return;
   uint64_t* PO = sm;                      // [T][W]
@@ -1104,7 +1135,7 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_apply_kernel(const PanelA
     stp[t] = g.stp[t]; bt[t] = g.bt[t]; qp[t] = g.qp[t];
     A[t] = g.A[t]; PWP[t] = g.PWP[t]; Dt[t] = g.Dt[t];
   }
-  for (size_t w = tid; w < (size_t)T * W; w += bd) PO[w] = a.po[w];
+  for (size_t w = tid; w < (size_t)T * W; w += bd) PO[w] = po[w];
   __syncthreads();
   // (a) per row (warp per row): u[x] = z_x . x_row and q = phase + |x & z|
   if (a.phases) {
@@ -1172,6 +1203,99 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_apply_kernel(const PanelA
   }
 }
 
+// (4) Look-ahead: every row's word wn (the next panel's) after this panel,
+// into a.nw, computed before the panel's apply has run: the row's mask by the
+// same replay as the apply's step (b) on its word wj, then its word wn XOR
+// the pivot rows' words wn of the mask (all read at the panel start).
+__device__ __forceinline__ void panel_next(const PanelArgs& a, const PanelRec& g, uint32_t wj, uint32_t wn,
+                                           uint32_t blk, uint32_t nblk) {
+  __shared__ uint32_t stp[PANEL];
+  __shared__ uint8_t bt[PANEL];
+  __shared__ uint64_t A[PANEL], PWP[PANEL], PN[PANEL];
+  const uint32_t T = g.T, tid = threadIdx.x, R = a.rows, W = a.W;
+  for (uint32_t t = tid; t < T; t += blockDim.x) {
+    stp[t] = g.stp[t]; bt[t] = g.bt[t]; A[t] = g.A[t]; PWP[t] = g.PWP[t];
+    PN[t] = a.xzs[(size_t)g.stp[t] * W + wn];
+  }
+  __syncthreads();
+  for (uint32_t r = blk * blockDim.x + tid; r < R; r += nblk * blockDim.x) {
+    uint64_t pw = a.xzs[(size_t)r * W + wj], cm = 0;
+    for (uint32_t t = 0; t < T; t++) {
+      if (r != stp[t] && ((pw >> bt[t]) & 1ull)) {
+        cm ^= A[t];
+        pw ^= PWP[t];
+      }
+    }
+    uint64_t v = a.xzs[(size_t)r * W + wn];
+    while (cm) {
+      const uint32_t x = __ffsll(cm) - 1;
+      cm &= cm - 1;
+      v ^= PN[x];
+    }
+    a.nw[r] = v;
+  }
+}
+
+// The plain schedule: per panel a one-CTA search launch (steps, then the
+// pivot rows and phase data) and a grid-wide apply launch.
+template <uint32_t RPT>
+__global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const PanelArgs a) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  // launched as a programmatic dependent of the previous panel's apply: wait
+  // for it (complete, its writes visible), then let the next launch in
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  PanelRec& g = *a.rec;
+  const uint32_t len = a.W / 2, wj = panel_word(a.stage, a.c0, len);
+  uint64_t* XT = sm;                                                   // [len][PANEL] X, then Z
+  uint32_t* cand = (uint32_t*)(XT + (size_t)2 * len * PANEL);          // the candidate rows
+  const bool was_done = g.done != 0;
+  panel_steps<RPT>(a, g, g, a.xzs + wj, a.W, cand);
+  if (!was_done) panel_post(a, g, a.po, wj, XT);
+}
+
+__global__ void __launch_bounds__(CANON_THREADS) canon_apply_kernel(const PanelArgs a) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  panel_apply(a, *a.rec, a.po, panel_word(a.stage, a.c0, a.W / 2), blockIdx.x, gridDim.x, sm);
+}
+
+// The look-ahead schedule: per panel p two launches,
+//   L1(p): CTA 0 runs panel p's pivot steps on the words a.nw (panel p's
+//          word of every row as it is after panel p - 1), while CTAs 1..
+//          apply panel p - 1 to the rows;
+//   L2(p): CTA 0 copies panel p's pivot rows (the rows are complete through
+//          panel p - 1 now) and computes its phase data, while CTAs 1..
+//          compute every row's word of panel p + 1 after panel p into a.nw.
+// So the serial part of a panel is the steps and the post-processing; the
+// grid-wide apply runs beside the next panel's steps.  The records and pivot
+// copies alternate between two buffers by panel parity (L1(p)'s apply reads
+// panel p - 1's while its steps write panel p's).
+template <uint32_t RPT>
+__global__ void __launch_bounds__(CANON_THREADS) canon_steps_apply_kernel(const PanelArgs a) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  if (blockIdx.x == 0) {
+    if (a.steps) panel_steps<RPT>(a, *a.prev, *a.rec, a.nw, 1u, (uint32_t*)sm);
+  } else if (a.wj_prev != 0xFFFFFFFFu) {
+    panel_apply(a, *a.prev, a.po_prev, a.wj_prev, blockIdx.x - 1, gridDim.x - 1, sm);
+  }
+}
+
+__global__ void __launch_bounds__(CANON_THREADS) canon_post_next_kernel(const PanelArgs a) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  const uint32_t wj = panel_word(a.stage, a.c0, a.W / 2);
+  if (blockIdx.x == 0) {
+    panel_post(a, *a.rec, a.po, wj, sm);
+  } else if (a.wj_next != 0xFFFFFFFFu) {
+    panel_next(a, *a.rec, wj, a.wj_next, blockIdx.x - 1, gridDim.x - 1);
+  }
+}
+
 // rows to their final positions: out[pos[r]] = row r
 __global__ void canon_place_kernel(const uint64_t* xzs, const uint8_t* ph, const uint32_t* pos, uint32_t rows,
                                    uint32_t W, uint64_t* out, uint8_t* out_ph) {
@@ -1186,6 +1310,18 @@ __global__ void canon_grid_init_kernel(uint32_t* pos, uint32_t rows, PanelRec* r
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r < rows) pos[r] = r;
   if (r == 0) { rec->T = 0; rec->i = 0; rec->rx = 0; rec->done = 0; }
+}
+
+// The look-ahead schedule's start: positions, both records empty, and every
+// row's word of the first panel (X word 0).
+__global__ void canon_look_init_kernel(uint32_t* pos, uint32_t rows, PanelRec* rec, const uint64_t* xzs,
+                                       uint32_t W, uint64_t* nw) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < rows) {
+    pos[r] = r;
+    nw[r] = xzs[(size_t)r * W];
+  }
+  if (r < 2) { rec[r].T = 0; rec[r].i = 0; rec[r].rx = 0; rec[r].done = 0; }
 }
 
 struct CanonPlan {
@@ -1302,6 +1438,7 @@ static uint32_t g_canon_grid = 0;  // 0: automatic, 1: always, 2: never (panels 
 static uint32_t g_canon_rpt = 0;         // tuner: rows per search thread (0: automatic; 4, 8, 16)
 static uint32_t g_canon_apply_rows = 0;  // tuner: rows per apply CTA (0: automatic)
 static uint32_t g_canon_pdl = 1;         // panel launches as programmatic dependents (0: plain)
+static uint32_t g_canon_lookahead = 1;   // the next panel's steps beside this panel's apply (0: in turn)
 // Smallest stabilizer view that runs by panels over the whole GPU (below it,
 // one cluster holds the rows in shared memory).
 constexpr uint32_t CANON_GRID_MIN_ROWS = 640;
@@ -1326,9 +1463,82 @@ static cudaError_t launch_panel(void (*k)(const PanelArgs), uint32_t grid, uint3
   return cudaLaunchKernelEx(&cfg, k, a);
 }
 
+// canonicalize! by panels over the whole GPU with look-ahead
+// (canon_steps_apply_kernel + canon_post_next_kernel per panel, one more
+// canon_steps_apply_kernel for the last panel's apply); scratch from the
+// stream-ordered pool.
+static int launch_grid_lookahead(const ElimSpec& e, cudaStream_t st) {
+  const uint32_t R = e.rows, W = e.W, len = W / 2;
+  uint32_t* pos = nullptr;
+  PanelRec* rec = nullptr;
+  uint64_t *po = nullptr, *nw = nullptr, *gtmp = nullptr;
+  uint8_t* gtmp_ph = nullptr;
+  QCB_CUDA(cudaMallocAsync(&pos, (size_t)R * 4, st));
+  QCB_CUDA(cudaMallocAsync(&rec, 2 * sizeof(PanelRec), st));
+  QCB_CUDA(cudaMallocAsync(&po, (size_t)2 * PANEL * W * 8, st));
+  QCB_CUDA(cudaMallocAsync(&nw, (size_t)R * 8, st));
+  QCB_CUDA(cudaMallocAsync(&gtmp, (size_t)R * W * 8, st));
+  QCB_CUDA(cudaMallocAsync(&gtmp_ph, R, st));
+  canon_look_init_kernel<<<(R + 255) / 256, 256, 0, st>>>(pos, R, rec, e.xzs, W, nw);
+  QCB_LAUNCHED();
+  uint32_t rpt = g_canon_rpt ? g_canon_rpt : 4u;
+  while (rpt * CANON_THREADS < R) rpt *= 2;
+  void (*steps)(const PanelArgs) = rpt == 1 ? canon_steps_apply_kernel<1>
+                                 : rpt == 2 ? canon_steps_apply_kernel<2>
+                                 : rpt == 4 ? canon_steps_apply_kernel<4>
+                                 : rpt == 8 ? canon_steps_apply_kernel<8> : canon_steps_apply_kernel<16>;
+  // CTA 0 of each L1 launch runs the steps on an SM of its own (1024 threads
+  // of up to 64 registers fill an SM's register file); the apply takes the
+  // other SMs, one CTA each
+  const uint32_t nsm = (uint32_t)device_sm_count();
+  const uint32_t rows_per_cta = g_canon_apply_rows ? g_canon_apply_rows : 8u;
+  const uint32_t G = std::max<uint32_t>(1, std::min<uint32_t>((R + rows_per_cta - 1) / rows_per_cta, nsm - 1));
+  const uint32_t per = (R + G - 1) / G;
+  const size_t l1_smem = std::max<size_t>((size_t)R * 4, (size_t)PANEL * W * 8 + (size_t)per * 9 + 16);
+  const size_t l2_smem = (size_t)2 * len * PANEL * 8;
+  const uint32_t G2 = (R + CANON_THREADS - 1) / CANON_THREADS;
+  QCB_CUDA(cudaFuncSetAttribute(steps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l1_smem));
+  QCB_CUDA(cudaFuncSetAttribute(canon_post_next_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l2_smem));
+  std::vector<std::pair<uint32_t, uint32_t>> panels;  // (stage, first column)
+  for (uint32_t stage = 0; stage < 2; stage++)
+    for (uint32_t c0 = 0; c0 < e.n; c0 += PANEL) panels.push_back({stage, c0});
+  const uint32_t P = (uint32_t)panels.size();
+  PanelArgs a{};
+  a.xzs = e.xzs; a.ph = e.ph; a.rows = R; a.n = e.n; a.W = W; a.phases = e.phases;
+  a.pos = pos; a.out = e.d_out; a.nw = nw;
+  for (uint32_t p = 0; p <= P; p++) {
+    // L1(p): panel p's steps (p < P) beside panel p - 1's apply (p > 0)
+    a.steps = p < P ? 1u : 0u;
+    if (p < P) { a.stage = panels[p].first; a.c0 = panels[p].second; }
+    a.rec = rec + (p & 1);
+    a.prev = rec + ((p + 1) & 1);
+    a.po_prev = po + (size_t)((p + 1) & 1) * PANEL * W;
+    a.wj_prev = p > 0 ? panel_word(panels[p - 1].first, panels[p - 1].second, len) : 0xFFFFFFFFu;
+    QCB_CUDA(launch_panel(steps, 1 + G, CANON_THREADS, l1_smem, st, a));
+    if (p == P) break;
+    // L2(p): panel p's pivot rows and phase data beside every row's next word
+    a.po = po + (size_t)(p & 1) * PANEL * W;
+    a.wj_next = p + 1 < P ? panel_word(panels[p + 1].first, panels[p + 1].second, len) : 0xFFFFFFFFu;
+    QCB_CUDA(launch_panel(canon_post_next_kernel, 1 + G2, CANON_THREADS, l2_smem, st, a));
+  }
+  canon_place_kernel<<<(R * 32 + 255) / 256, 256, 0, st>>>(e.xzs, e.ph, pos, R, W, gtmp, gtmp_ph);
+  QCB_LAUNCHED();
+  QCB_CUDA(cudaMemcpyAsync(e.xzs, gtmp, (size_t)R * W * 8, cudaMemcpyDeviceToDevice, st));
+  // without phases the reference's row swaps leave the phases in place
+  if (e.phases) QCB_CUDA(cudaMemcpyAsync(e.ph, gtmp_ph, R, cudaMemcpyDeviceToDevice, st));
+  QCB_CUDA(cudaFreeAsync(pos, st));
+  QCB_CUDA(cudaFreeAsync(rec, st));
+  QCB_CUDA(cudaFreeAsync(po, st));
+  QCB_CUDA(cudaFreeAsync(nw, st));
+  QCB_CUDA(cudaFreeAsync(gtmp, st));
+  QCB_CUDA(cudaFreeAsync(gtmp_ph, st));
+  return QCB_OK;
+}
+
 // canonicalize! by panels over the whole GPU (canon_search_kernel +
 // canon_apply_kernel per panel); scratch from the stream-ordered pool.
 static int launch_grid(const ElimSpec& e, cudaStream_t st) {
+  if (g_canon_lookahead) return launch_grid_lookahead(e, st);
   const uint32_t R = e.rows, W = e.W, len = W / 2;
   uint32_t* pos = nullptr;
   PanelRec* rec = nullptr;
@@ -1517,6 +1727,7 @@ void set_canon_blocked(uint32_t v) { g_canon_blocked = v; }
 void set_canon_grid(uint32_t v) { g_canon_grid = v; }
 void set_canon_rpt(uint32_t v) { g_canon_rpt = v; }
 void set_canon_pdl(uint32_t v) { g_canon_pdl = v; }
+void set_canon_lookahead(uint32_t v) { g_canon_lookahead = v; }
 void set_canon_apply_rows(uint32_t v) { g_canon_apply_rows = v; }
 
 }  // namespace qcb

@@ -62,6 +62,8 @@ void set_canon_grid(uint32_t v);
 void set_server_fill(uint32_t v);
 void set_canon_rpt(uint32_t v);
 void set_canon_pdl(uint32_t v);
+void set_gates_pdl(uint32_t v);
+void set_canon_lookahead(uint32_t v);
 void set_walker_pdl(uint32_t v);
 void set_walker_narrow(uint32_t v);
 void set_canon_apply_rows(uint32_t v);
@@ -190,6 +192,15 @@ int qcb_tune_set(const char* key, int64_t value) {
     // canonicalize! panel launches as programmatic dependents (1, default) or plain (0)
     if (value > 1) return fail(QCB_EARG, "canon_pdl must be 0 or 1");
     set_canon_pdl((uint32_t)value);
+  } else if (k == "canon_lookahead") {
+    // canonicalize! by panels over the whole GPU: the next panel's pivot
+    // steps beside this panel's apply (1, default) or the two in turn (0)
+    if (value > 1) return fail(QCB_EARG, "canon_lookahead must be 0 or 1");
+    set_canon_lookahead((uint32_t)value);
+  } else if (k == "gates_pdl") {
+    // symbolic apply! launches (qcb_apply_gates) as programmatic dependents (1, default) or plain (0)
+    if (value > 1) return fail(QCB_EARG, "gates_pdl must be 0 or 1");
+    set_gates_pdl((uint32_t)value);
   } else if (k == "canon_apply_rows") {
     if (value && (value < 8 || value > 32)) return fail(QCB_EARG, "canon_apply_rows must be 0 or 8..32");
     set_canon_apply_rows((uint32_t)value);

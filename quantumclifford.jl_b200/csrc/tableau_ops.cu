@@ -315,9 +315,15 @@ struct GateBatch {
   GateOp op[GATE_BATCH];
 };
 
-// Thread per row; the batch's gates are applied to that row in order.
+// Thread per row; the batch's gates are applied to that row in order.  The
+// launch may be a programmatic dependent of the launch before it on the
+// stream: the dependents of this one are released at once, and the rows are
+// touched only after griddepcontrol.wait (the predecessor has completed and
+// its writes are visible; a no-op for a plain launch).
 __global__ void apply_gates_kernel(uint64_t* xzs, uint8_t* ph, uint32_t rows, uint32_t W,
                                    const __grid_constant__ GateBatch ops, uint32_t nops, int phases) {
+  asm volatile("griddepcontrol.launch_dependents;");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= rows) return;
   uint64_t* row = xzs + (uint64_t)r * W;
@@ -580,6 +586,9 @@ __global__ void mul_left_batch_finish_kernel(uint8_t* r_phase, const uint8_t* l_
   acc[i] = 0;
 }
 
+static uint32_t g_gates_pdl = 1;  // symbolic gate launches as programmatic dependents (0: plain)
+void set_gates_pdl(uint32_t v) { g_gates_pdl = v; }
+
 }  // namespace qcb
 
 using namespace qcb;
@@ -777,7 +786,19 @@ int qcb_apply_gates(qcb_tableau* t, const qcb_op* ops, size_t n_ops, int phases,
     const uint32_t n = (uint32_t)std::min<size_t>(GATE_BATCH, g.size() - k0);
     GateBatch b{};
     std::copy(g.begin() + k0, g.begin() + k0 + n, b.op);
-    apply_gates_kernel<<<(t->rows + 127) / 128, 128, 0, st>>>(t->xzs, t->phases, t->rows, t->W, b, n, phases);
+    // a programmatic dependent of the previous launch on the stream: in a
+    // stream of single-gate calls each launch is scheduled while the one
+    // before it runs, instead of after it drains
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((t->rows + 127) / 128);
+    cfg.blockDim = dim3(128);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = g_gates_pdl ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    QCB_CUDA(cudaLaunchKernelEx(&cfg, apply_gates_kernel, t->xzs, t->phases, t->rows, t->W, (const GateBatch)b, n, phases));
     QCB_LAUNCHED();
   }
   return QCB_OK;

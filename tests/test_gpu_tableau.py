@@ -325,16 +325,37 @@ def test_dense_apply(qcb, n):
         assert np.array_equal(s.tab.xzs, xz) and np.array_equal(s.tab.phases, ph)
 
 
-@pytest.mark.parametrize("grid", [1, 2])
+def _canonicalize_with(qcb, t, phases, grid, lookahead):
+    lib = qcb.lib()
+    qcb.check(lib.qcb_tune_set(b"canon_grid", grid))
+    qcb.check(lib.qcb_tune_set(b"canon_lookahead", lookahead))
+    try:
+        s = qcb.Stabilizer(t.copy()).to_gpu()
+        _, rx, rz = qcb.canonicalize_(s, phases=phases, ranks=True)
+        s.to_cpu()
+    finally:
+        qcb.check(lib.qcb_tune_set(b"canon_grid", 0))
+        qcb.check(lib.qcb_tune_set(b"canon_lookahead", 1))
+    return s, rx, rz
+
+
+# (canon_grid, canon_lookahead): the whole GPU with look-ahead, the whole GPU
+# with the search and the apply in turn, one cluster
+SCHEDULES = [(1, 1), (1, 0), (2, 1)]
+
+
+@pytest.mark.parametrize("grid,lookahead", SCHEDULES)
 @pytest.mark.parametrize("n", [64, 97, 1000, 2100, 4000])
 @pytest.mark.parametrize("phases", [True, False])
-def test_canonicalize_panels_over_the_gpu(qcb, n, grid, phases):
+def test_canonicalize_panels_over_the_gpu(qcb, n, grid, lookahead, phases):
     """canonicalize! by panels with the per-row work spread over the GPU
-    (canon_grid 1: a one-CTA search launch and a grid-wide apply launch per
-    panel) and on one cluster (2), on uniformly random stabilizer states, bit
-    for bit with phases and ranks against the oracle, with phases tracked and
-    not (the row swaps then leave the phases in place); also a rank-deficient
-    view (repeated rows)."""
+    (canon_grid 1: with look-ahead, per panel one launch of the pivot steps
+    beside the previous panel's grid-wide apply and one of the pivot rows and
+    phase data beside the next panel's words; without, a one-CTA search
+    launch and a grid-wide apply launch per panel) and on one cluster (2), on
+    uniformly random stabilizer states, bit for bit with phases and ranks
+    against the oracle, with phases tracked and not (the row swaps then leave
+    the phases in place); also a rank-deficient view (repeated rows)."""
     from qcb200 import randoms
 
     rng = np.random.default_rng(n + grid)
@@ -342,13 +363,27 @@ def test_canonicalize_panels_over_the_gpu(qcb, n, grid, phases):
     if n == 97:  # duplicate rows: rank deficiency, columns without a pivot
         t.xzs[50:60] = t.xzs[10:20]
         t.phases[50:60] = t.phases[10:20]
-    qcb.check(qcb.lib().qcb_tune_set(b"canon_grid", grid))
-    try:
-        s = qcb.Stabilizer(t.copy()).to_gpu()
-        _, rx, rz = qcb.canonicalize_(s, phases=phases, ranks=True)
-        s.to_cpu()
-    finally:
-        qcb.check(qcb.lib().qcb_tune_set(b"canon_grid", 0))
+    s, rx, rz = _canonicalize_with(qcb, t, phases, grid, lookahead)
     ph, xz, orx, orz = oracle.canonicalize(t.phases, t.xzs, n, phases)
     assert (rx, rz) == (orx, orz)
     assert np.array_equal(s.tab.xzs, xz) and np.array_equal(s.tab.phases, ph)
+
+
+@pytest.mark.parametrize("lookahead", [1, 0])
+@pytest.mark.parametrize("rows,n", [(300, 1000), (1500, 700), (700, 130), (1200, 1200)])
+def test_canonicalize_panels_rectangular_views(qcb, rows, n, lookahead):
+    """Views with fewer or more rows than qubits (random rows, commuting or
+    not; rank-deficient when rows > 2n or rows repeat): the last pivot comes
+    before the last panel, so the remaining panels find every position taken,
+    or columns end without a pivot.  Whole-GPU panels with and without
+    look-ahead, against the oracle."""
+    rng = np.random.default_rng(rows * 7 + n + lookahead)
+    t = rand_tab(rows, n, rng)
+    if rows == 1200:  # low-weight rows and repeats: many panels without pivots
+        t.xzs &= rng.integers(0, 2**63, t.xzs.shape, dtype=np.uint64) & rng.integers(0, 2**63, t.xzs.shape, dtype=np.uint64)
+        t.xzs[600:900] = t.xzs[100:400]
+    for phases in (True, False):
+        s, rx, rz = _canonicalize_with(qcb, t, phases, 1, lookahead)
+        ph, xz, orx, orz = oracle.canonicalize(t.phases, t.xzs, n, phases)
+        assert (rx, rz) == (orx, orz)
+        assert np.array_equal(s.tab.xzs, xz) and np.array_equal(s.tab.phases, ph)

@@ -324,7 +324,8 @@ def bench_tableau(args):
 
     if want("canonicalize"):
         # ---- canonicalize! of random full-rank stabilizers
-        for n in (1000, 2000, 4000):
+        sizes = [int(x) for x in args.canon_sizes.split(",") if x] if args.canon_sizes else [1000, 2000, 4000]
+        for n in sizes:
             d = random_destabilizer(n)
             src = Q.Tableau(d.tab.phases[n:].copy(), n, d.tab.xzs[n:].copy())
             work = Q.Tableau(src.phases.copy(), n, src.xzs.copy()).to_gpu()
@@ -728,6 +729,7 @@ def main():
     ap.add_argument("--workload", default="frames", choices=["frames", "tableau", "batch", "serve"])
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--tableau-only", default="", help="comma list of mul_left,canonicalize,project,expect,dense_apply,sCNOT")
+    ap.add_argument("--canon-sizes", default="", help="comma list of canonicalize! sizes (default 1000,2000,4000)")
     ap.add_argument("--serve-rates", default="25,50,100")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -483,6 +483,45 @@ __host__ __device__ inline BlockedLayout blocked_layout(uint32_t rows, uint32_t 
   return L;
 }
 
+// The lane's part of u[x] = z_x . x_row for one row and the T pivot rows PO
+// ([T][W] in shared memory): the row's X words wb + lane + 32 k, k < K
+// (those below len), against pivot x's Z words, as bit x of lo (x < 32) or
+// hi; s gets the lane's |x & z| of those words.  The products of a pivot's
+// words are XOR-accumulated and counted once (the parity of a sum of
+// popcounts is the parity of the XOR); a lane past len reads word 0 against
+// a zero word, so the pivot loop has no branch.
+template <int K>
+__device__ __forceinline__ void row_parities(const uint64_t* PO, uint32_t W, uint32_t len, uint32_t T,
+                                             uint32_t wb, uint32_t lane, const uint64_t* row, uint32_t& lo,
+                                             uint32_t& hi, uint32_t& s) {
+  uint64_t xw[K];
+  uint32_t off[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const uint32_t w = wb + lane + 32u * k;
+    const bool ok = w < len;
+    off[k] = ok ? w : 0u;
+    xw[k] = ok ? row[w] : 0ull;
+    if (ok) s += __popcll(xw[k] & row[len + w]);
+  }
+  const uint64_t* pz = PO + len;
+  const uint32_t t0 = min(T, 32u);
+#pragma unroll 4
+  for (uint32_t x = 0; x < t0; x++) {
+    uint64_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < K; k++) acc ^= pz[(size_t)x * W + off[k]] & xw[k];
+    lo ^= ((uint32_t)__popc((uint32_t)acc ^ (uint32_t)(acc >> 32)) & 1u) << x;
+  }
+#pragma unroll 4
+  for (uint32_t x = 32; x < T; x++) {
+    uint64_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < K; k++) acc ^= pz[(size_t)x * W + off[k]] & xw[k];
+    hi ^= ((uint32_t)__popc((uint32_t)acc ^ (uint32_t)(acc >> 32)) & 1u) << (x - 32);
+  }
+}
+
 template <uint32_t RPT>
 __device__ __forceinline__ void blocked_body(const CanonArgs& a, uint64_t* smem) {
   cg::cluster_group cl = cg::this_cluster();
@@ -655,14 +694,14 @@ __device__ __forceinline__ void blocked_body(const CanonArgs& a, uint64_t* smem)
       // transposed X words (conflict-free), z_a is a broadcast
       for (uint32_t t = warp; t < T; t += nwarps) {
         const uint64_t* za = PO + (size_t)t * W + len;
-        uint32_t p0 = 0, p1 = 0;
+        uint64_t p0 = 0, p1 = 0;  // XOR-accumulated: the parity is the popcount's
         for (uint32_t w = 0; w < len; w++) {
           const uint64_t zw = za[w];
-          p0 += __popcll(zw & XT[(size_t)w * PANEL + lane]);
-          p1 += __popcll(zw & XT[(size_t)w * PANEL + lane + 32]);
+          p0 ^= zw & XT[(size_t)w * PANEL + lane];
+          p1 ^= zw & XT[(size_t)w * PANEL + lane + 32];
         }
-        const uint32_t lo = __ballot_sync(0xFFFFFFFFu, (p0 & 1u) && lane < T);
-        const uint32_t hi = __ballot_sync(0xFFFFFFFFu, (p1 & 1u) && lane + 32 < T);
+        const uint32_t lo = __ballot_sync(0xFFFFFFFFu, (__popcll(p0) & 1) && lane < T);
+        const uint32_t hi = __ballot_sync(0xFFFFFFFFu, (__popcll(p1) & 1) && lane + 32 < T);
         if (lane == 0) C[t] = (uint64_t)lo | ((uint64_t)hi << 32);
       }
       __syncthreads();
@@ -1062,16 +1101,18 @@ __device__ __forceinline__ void panel_post(const PanelArgs& a, PanelRec& g, uint
   }
   __syncthreads();
   if (a.phases && T) {
-    // C[a] bit b = z_a . x_b over the pivot rows (both transposed in shared memory)
+    // C[a] bit b = z_a . x_b over the pivot rows (both transposed in shared
+    // memory); the parity of a sum of popcounts is the parity of the XOR of
+    // the words, so the words are XOR-accumulated and counted once
     for (uint32_t t = warp; t < T; t += nwarps) {
-      uint32_t p0 = 0, p1 = 0;
+      uint64_t p0 = 0, p1 = 0;
       for (uint32_t w = 0; w < len; w++) {
         const uint64_t zw = ZT[(size_t)w * PANEL + t];
-        p0 += __popcll(zw & XT[(size_t)w * PANEL + lane]);
-        p1 += __popcll(zw & XT[(size_t)w * PANEL + lane + 32]);
+        p0 ^= zw & XT[(size_t)w * PANEL + lane];
+        p1 ^= zw & XT[(size_t)w * PANEL + lane + 32];
       }
-      const uint32_t lo = __ballot_sync(0xFFFFFFFFu, (p0 & 1u) && lane < T);
-      const uint32_t hi = __ballot_sync(0xFFFFFFFFu, (p1 & 1u) && lane + 32 < T);
+      const uint32_t lo = __ballot_sync(0xFFFFFFFFu, (__popcll(p0) & 1) && lane < T);
+      const uint32_t hi = __ballot_sync(0xFFFFFFFFu, (__popcll(p1) & 1) && lane + 32 < T);
       if (lane == 0) C[t] = (uint64_t)lo | ((uint64_t)hi << 32);
     }
     __syncthreads();
@@ -1137,18 +1178,20 @@ __device__ __forceinline__ void panel_apply(const PanelArgs& a, const PanelRec& 
   }
   for (size_t w = tid; w < (size_t)T * W; w += bd) PO[w] = po[w];
   __syncthreads();
-  // (a) per row (warp per row): u[x] = z_x . x_row and q = phase + |x & z|
+  // (a) per row (warp per row): u[x] = z_x . x_row and q = phase + |x & z|;
+  // the lane's X words (up to four at a time) stay in registers, and for
+  // each pivot x their products with z_x are XOR-accumulated and counted
+  // once (parity of the XOR = parity of the popcounts)
   if (a.phases) {
     for (uint32_t lr = warp; lr < nloc; lr += nwarps) {
       const uint64_t* row = a.xzs + (size_t)(r0 + lr) * W;
       uint32_t lo = 0, hi = 0, s = 0;
-      for (uint32_t w = lane; w < len; w += 32) {
-        const uint64_t xw = row[w];
-        s += __popcll(xw & row[len + w]);
-        for (uint32_t x = 0; x < T; x++) {
-          const uint32_t bit = (uint32_t)__popcll(PO[(size_t)x * W + len + w] & xw) & 1u;
-          if (x < 32) lo ^= bit << x; else hi ^= bit << (x - 32);
-        }
+      for (uint32_t wb = 0; wb < len; wb += 128) {
+        const uint32_t kn = min(4u, (len - wb + 31) / 32);  // warp-uniform
+        if (kn == 1) row_parities<1>(PO, W, len, T, wb, lane, row, lo, hi, s);
+        else if (kn == 2) row_parities<2>(PO, W, len, T, wb, lane, row, lo, hi, s);
+        else if (kn == 3) row_parities<3>(PO, W, len, T, wb, lane, row, lo, hi, s);
+        else row_parities<4>(PO, W, len, T, wb, lane, row, lo, hi, s);
       }
       s = __reduce_add_sync(0xFFFFFFFFu, s);
       lo = __reduce_xor_sync(0xFFFFFFFFu, lo);

@@ -11,6 +11,7 @@ import ctypes
 import numpy as np
 import pytest
 
+import oracle
 from qcb200 import tableau as Q
 
 pytestmark = pytest.mark.gpu
@@ -62,6 +63,10 @@ def test_noalloc_batch_matches_mul_left_pauli_two_calls(qcb, n, count, phases):
         gx, gp = noalloc(qcb, rx, rp, lx, lp, n, phases)
         assert np.array_equal(gx, ex)
         assert np.array_equal(gp, ep if phases else rp)
+        # and pinned to the CPU oracle directly, on the first pairs
+        for i in range(min(count, 16)):
+            ox, op = oracle.mul_left_pauli(rx[i], rp[i], lx[i], lp[i], phases)
+            assert np.array_equal(gx[i], ox) and gp[i] == (op if phases else rp[i])
 
 
 def test_noalloc_misaligned_words_and_a_side_stream(qcb):

@@ -1076,7 +1076,10 @@ __device__ __forceinline__ void panel_post(const PanelArgs& a, PanelRec& g, uint
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   const uint32_t W = a.W, len = W / 2;
   const uint32_t T = g.T;
-  uint64_t* ZT = XT + (size_t)len * PANEL;  // ZT[w * PANEL + t] = Z word w of pivot t
+  // XT[w * XS + t] / ZT[w * XS + t]: X / Z word w of pivot t; the odd stride
+  // keeps the transposing stores (lane = word) free of bank conflicts
+  constexpr uint32_t XS = PANEL + 1;
+  uint64_t* ZT = XT + (size_t)len * XS;
   for (uint32_t t = tid; t < T; t += blockDim.x) {
     stp[t] = g.stp[t];
     bt[t] = g.bt[t];
@@ -1092,8 +1095,8 @@ __device__ __forceinline__ void panel_post(const PanelArgs& a, PanelRec& g, uint
       const uint64_t vx = a.xzs[(size_t)r * W + w], vz = a.xzs[(size_t)r * W + len + w];
       po[(size_t)t * W + w] = vx;
       po[(size_t)t * W + len + w] = vz;
-      XT[(size_t)w * PANEL + t] = vx;
-      ZT[(size_t)w * PANEL + t] = vz;
+      XT[(size_t)w * XS + t] = vx;
+      ZT[(size_t)w * XS + t] = vz;
       s += __popcll(vx & vz);
     }
     s = __reduce_add_sync(0xFFFFFFFFu, s);
@@ -1107,9 +1110,9 @@ __device__ __forceinline__ void panel_post(const PanelArgs& a, PanelRec& g, uint
     for (uint32_t t = warp; t < T; t += nwarps) {
       uint64_t p0 = 0, p1 = 0;
       for (uint32_t w = 0; w < len; w++) {
-        const uint64_t zw = ZT[(size_t)w * PANEL + t];
-        p0 ^= zw & XT[(size_t)w * PANEL + lane];
-        p1 ^= zw & XT[(size_t)w * PANEL + lane + 32];
+        const uint64_t zw = ZT[(size_t)w * XS + t];
+        p0 ^= zw & XT[(size_t)w * XS + lane];
+        p1 ^= zw & XT[(size_t)w * XS + lane + 32];
       }
       const uint32_t lo = __ballot_sync(0xFFFFFFFFu, (__popcll(p0) & 1) && lane < T);
       const uint32_t hi = __ballot_sync(0xFFFFFFFFu, (__popcll(p1) & 1) && lane + 32 < T);
@@ -1261,7 +1264,8 @@ __device__ __forceinline__ void panel_next(const PanelArgs& a, const PanelRec& g
     PN[t] = a.xzs[(size_t)g.stp[t] * W + wn];
   }
   __syncthreads();
-  for (uint32_t r = blk * blockDim.x + tid; r < R; r += nblk * blockDim.x) {
+  const uint32_t per = (R + nblk - 1) / nblk, r0 = blk * per, r1 = min(R, r0 + per);
+  for (uint32_t r = r0 + tid; r < r1; r += blockDim.x) {
     uint64_t pw = a.xzs[(size_t)r * W + wj], cm = 0;
     for (uint32_t t = 0; t < T; t++) {
       if (r != stp[t] && ((pw >> bt[t]) & 1ull)) {
@@ -1290,8 +1294,8 @@ __global__ void __launch_bounds__(CANON_THREADS) canon_search_kernel(const Panel
   asm volatile("griddepcontrol.launch_dependents;");
   PanelRec& g = *a.rec;
   const uint32_t len = a.W / 2, wj = panel_word(a.stage, a.c0, len);
-  uint64_t* XT = sm;                                                   // [len][PANEL] X, then Z
-  uint32_t* cand = (uint32_t*)(XT + (size_t)2 * len * PANEL);          // the candidate rows
+  uint64_t* XT = sm;                                                   // [len][PANEL + 1] X, then Z
+  uint32_t* cand = (uint32_t*)(XT + (size_t)2 * len * (PANEL + 1));    // the candidate rows
   const bool was_done = g.done != 0;
   panel_steps<RPT>(a, g, g, a.xzs + wj, a.W, cand);
   if (!was_done) panel_post(a, g, a.po, wj, XT);
@@ -1538,8 +1542,10 @@ static int launch_grid_lookahead(const ElimSpec& e, cudaStream_t st) {
   const uint32_t G = std::max<uint32_t>(1, std::min<uint32_t>((R + rows_per_cta - 1) / rows_per_cta, nsm - 1));
   const uint32_t per = (R + G - 1) / G;
   const size_t l1_smem = std::max<size_t>((size_t)R * 4, (size_t)PANEL * W * 8 + (size_t)per * 9 + 16);
-  const size_t l2_smem = (size_t)2 * len * PANEL * 8;
-  const uint32_t G2 = (R + CANON_THREADS - 1) / CANON_THREADS;
+  const size_t l2_smem = (size_t)2 * len * (PANEL + 1) * 8;
+  // the next words: a share of the rows on every other SM (the replay is a
+  // serial loop over the panel's pivots per row, so the rows are spread thin)
+  const uint32_t G2 = std::max<uint32_t>(1, std::min<uint32_t>(R, nsm - 1));
   QCB_CUDA(cudaFuncSetAttribute(steps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l1_smem));
   QCB_CUDA(cudaFuncSetAttribute(canon_post_next_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l2_smem));
   std::vector<std::pair<uint32_t, uint32_t>> panels;  // (stage, first column)
@@ -1604,7 +1610,7 @@ static int launch_grid(const ElimSpec& e, cudaStream_t st) {
                                   : rpt == 2 ? canon_search_kernel<2>
                                   : rpt == 4 ? canon_search_kernel<4>
                                   : rpt == 8 ? canon_search_kernel<8> : canon_search_kernel<16>;
-  const size_t search_smem = (size_t)2 * len * PANEL * 8 + (size_t)R * 4;
+  const size_t search_smem = (size_t)2 * len * (PANEL + 1) * 8 + (size_t)R * 4;
   // opt in always: the static shared memory counts against the default 48 KB too
   QCB_CUDA(cudaFuncSetAttribute(search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_smem));
   // rows per apply CTA: 8 while that still fits one CTA per SM, else 16

@@ -366,7 +366,9 @@ int qcb_pftrajectories_fresh(qcb_frame* f, const qcb_program* prog, uint64_t see
  * "presample" 0 (automatic) / 1 never (draw in the walk) / 2 every bucket
  * overflows (test).  "walker_threads" threads per walker CTA (0: 640, or
  * 64..640 in steps of 32); "walker_pdl" 1 (default) / 0: the walker as a
- * programmatic dependent launch of the noise pre-sampler or plain.
+ * programmatic dependent launch of the noise pre-sampler or plain;
+ * "walker_narrow" 1 (default) / 0: programs too tall for a 16-column
+ * shared-memory tile run in 8..14-column tiles, or on the HBM planes.
  * "gates_pdl" 1 (default) / 0: qcb_apply_gates launches as programmatic
  * dependents of the launch before them on the stream, or plain.            */
 int qcb_tune_set(const char* key, int64_t value);

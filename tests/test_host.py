@@ -40,6 +40,28 @@ def test_version_string_without_gpu():
     assert b"sm_100a" in qcb200.lib().qcb_version()
 
 
+# every tuning / test knob of qcb_tune_set: (key, its default, a rejected value)
+KNOBS = [("walker_tile", 0, 7), ("stage_withhold", 0, -1), ("presample", 0, 3), ("server_hash_bits", 0, 65),
+         ("server_fill", 1, 2), ("walker_threads", 0, 65), ("canon_threads", 0, 33), ("canon_cluster", 0, 3),
+         ("canon_blocked", 0, 3), ("canon_grid", 0, 3), ("canon_rpt", 0, 3), ("walker_narrow", 1, 2),
+         ("walker_pdl", 1, 2), ("canon_pdl", 1, 2), ("canon_lookahead", 1, 2), ("gates_pdl", 1, 2),
+         ("canon_apply_rows", 0, 7), ("project_grid", 0, 3), ("project_withhold", 0, 2), ("project_cluster", 0, 3)]
+
+
+def test_tune_knobs_validate_without_gpu():
+    """qcb_tune_set only records host settings: each documented knob takes
+    its default back and rejects an out-of-range value with QCB_EARG; an
+    unknown key is rejected too.  No device call is made."""
+    lib = qcb200.lib()
+    hdr = open(os.path.join(ROOT, "include", "qcb200.h")).read()
+    for key, default, bad in KNOBS:
+        assert f'"{key}"' in hdr, key  # documented beside qcb_tune_set
+        assert lib.qcb_tune_set(key.encode(), default) == 0, key
+        assert lib.qcb_tune_set(key.encode(), bad) == 4, (key, bad)  # QCB_EARG
+        assert lib.qcb_tune_set(key.encode(), default) == 0, key
+    assert lib.qcb_tune_set(b"no_such_knob", 0) == 4
+
+
 def test_op_validation_matches_reference_constructors():
     with pytest.raises(ArgumentError):
         O.sCNOT(1, 1)

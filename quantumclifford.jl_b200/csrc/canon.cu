@@ -750,13 +750,12 @@ __device__ __forceinline__ void blocked_body(const CanonArgs& a, uint64_t* smem)
         for (uint32_t lr = warp; lr < nloc; lr += nwarps) {
           const uint64_t* row = ROW(lr);
           uint32_t lo = 0, hi = 0, s = 0;
-          for (uint32_t w = lane; w < len; w += 32) {
-            const uint64_t xw = row[w];
-            s += __popcll(xw & row[len + w]);
-            for (uint32_t x = 0; x < T; x++) {
-              const uint32_t bit = (uint32_t)__popcll(PO[(size_t)x * W + len + w] & xw) & 1u;
-              if (x < 32) lo ^= bit << x; else hi ^= bit << (x - 32);
-            }
+          for (uint32_t wb = 0; wb < len; wb += 128) {
+            const uint32_t kn = min(4u, (len - wb + 31) / 32);  // warp-uniform
+            if (kn == 1) row_parities<1>(PO, W, len, T, wb, lane, row, lo, hi, s);
+            else if (kn == 2) row_parities<2>(PO, W, len, T, wb, lane, row, lo, hi, s);
+            else if (kn == 3) row_parities<3>(PO, W, len, T, wb, lane, row, lo, hi, s);
+            else row_parities<4>(PO, W, len, T, wb, lane, row, lo, hi, s);
           }
           s = __reduce_add_sync(0xFFFFFFFFu, s);
           lo = __reduce_xor_sync(0xFFFFFFFFu, lo);
